@@ -1,0 +1,278 @@
+#!/usr/bin/env python
+"""Direct J+K build benchmark: (H2O)_32 / cc-pVDZ (768 basis functions), Schwarz 1e-12.
+
+One step = one J+K build from a device-resident density D to device-resident J and K (unique
+Schwarz-surviving quartets, all quartet classes).  The reported `value` is unique contracted shell
+quartets per second of the whole job (N GPUs run independent replicas: the path has no collective).
+The default path is the mixed-precision build (quartets with Q_ab Q_cd < 1e-4 in FP32) when it
+meets |dE| <= 1e-8 Eh against the FP64 build of the same run; the FP64 build is always timed and
+reported beside it.  Set-up (basis, E coefficients, Schwarz factors, screening plan) is excluded
+and reported separately.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+"""
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "J+K build s and quartets/s, (H2O)_32 DZ: mixed/batched vs FP64 GPU, |ΔE|≤1e-8 Eh"
+N_WATERS, SEED, OCC = 32, 2024, 160
+SCHWARZ, FP32_THR = 1e-12, 1e-4
+WORKLOAD = {"workload": "direct J+K build, (H2O)_32 water cluster, cc-pVDZ", "n_waters": N_WATERS, "nao": 768,
+            "seed": SEED, "occupied": OCC, "schwarz": SCHWARZ, "fp32_threshold": FP32_THR,
+            "geometry": "5.7 bohr cubic lattice, random rotations, +-0.6 bohr jitter",
+            "l2": "256 MiB buffer rewritten between timed steps"}
+
+
+def env_rank():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("LOCAL_RANK", 0)), int(os.environ.get("WORLD_SIZE", 1))
+
+
+def emit(obj):
+    print(json.dumps(obj), flush=True)
+
+
+def clocks_start(gpu_index):
+    os.makedirs(os.path.join(ROOT, "gpurun_out"), exist_ok=True)
+    path = os.path.join(ROOT, "gpurun_out", f"clocks_{gpu_index}.csv")
+    q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+    try:
+        fh = open(path, "w")
+        p = subprocess.Popen(["nvidia-smi", "-i", str(gpu_index), f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                              "-lms", "200"], stdout=fh, stderr=subprocess.DEVNULL)
+        return p, fh, path
+    except Exception:
+        return None, None, path
+
+
+def clocks_stop(handle):
+    p, fh, path = handle
+    if p is None:
+        return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+    p.terminate()
+    p.wait()
+    fh.close()
+    sm, smax, reasons = [], None, set()
+    names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+    for line in open(path):
+        f = [x.strip() for x in line.split(",")]
+        if len(f) < 9:
+            continue
+        try:
+            sm.append(float(f[1]))
+            smax = float(f[2])
+        except ValueError:
+            continue
+        for n, v in zip(names, f[5:9]):
+            if v.lower() == "active":
+                reasons.add(n)
+    return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+            "samples": len(sm)}
+
+
+def cpu_reference(steps, warmup, Z, xyz, D, target_s=12.0):
+    """The reference's own ERI4Kernel batches digested into J/K on every host core (oracle/_ref),
+    timed on a bounded, class-balanced sample: every `stride`-th bra shell pair of every class pair."""
+    from oracle import ref as R
+    cores = os.cpu_count() or 1
+    R.set_threads(cores)
+    r = R.RefStructure("cc-pvdz", Z, xyz)
+    _, _, nq, sec = r.jk(D, SCHWARZ, 256)
+    stride = max(1, int(math.ceil(256 * sec / target_s)))
+    best = None
+    for _ in range(max(1, steps)):
+        _, _, nq, sec = r.jk(D, SCHWARZ, stride)
+        qps = nq / sec
+        best = qps if best is None else max(best, qps)
+    return best, cores, stride, nq, sec
+
+
+def run_reference(args):
+    rank, local, world = env_rank()
+    if rank != 0:
+        return
+    from lible_b200.workloads import random_density, water_cluster
+    from oracle import ref as R
+    if not R.available():
+        emit({"impl": "reference", "unavailable": "oracle/_ref/liblible_ref.so not built (needs the reference sources)"})
+        return
+    Z, xyz, rng = water_cluster(N_WATERS, SEED)
+    D = random_density(768, OCC, rng)
+    qps, cores, stride, nq, sec = cpu_reference(args.steps, args.warmup, Z, xyz, D)
+    sample = f"every {stride}-th bra shell pair of every class pair ({nq} quartets, {sec:.2f} s per step)"
+    emit({"impl": "reference", "metric": METRIC, "value": qps, "unit": "quartets/s", "n_gpus": args.gpus,
+          "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sec, "higher_is_better": True,
+          "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+          "config": WORKLOAD,
+          "cpu_baseline": {"value": qps, "unit": "quartets/s", "cores": cores, "kind": "reference", "sample": sample},
+          "e2e": {"value": qps, "unit": "quartets/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}})
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+
+    import torch
+    from lible_b200 import ints as L
+    from lible_b200.workloads import random_density, water_cluster
+
+    rank, local, world = env_rank()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    Z, xyz, rng = water_cluster(N_WATERS, SEED)
+    t0 = time.perf_counter()
+    s = L.Structure("cc-pvdz", Z, xyz, units="bohr", device=local)
+    D = random_density(s.nao, OCC, rng)
+    dev = torch.device("cuda", local)
+    Dd = torch.tensor(D, device=dev)
+    J = torch.empty_like(Dd)
+    K = torch.empty_like(Dd)
+    plan64 = L.jk_plan(s, SCHWARZ, "fp64")
+    planmx = L.jk_plan(s, SCHWARZ, "mixed", FP32_THR)
+    setup_s = time.perf_counter() - t0
+    stream = torch.cuda.ExternalStream(L.stream_handle(s), device=dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    dfma, dmma = L.fp64_peak(s)
+
+    def timed(precision, steps, warmup):
+        for _ in range(warmup):
+            L.jk(s, Dd, SCHWARZ, precision, FP32_THR, J=J, K=K)
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        ms = []
+        for _ in range(steps):
+            flush.fill_(1.0)
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            L.jk(s, Dd, SCHWARZ, precision, FP32_THR, J=J, K=K)
+            e1.record(stream)
+            e1.synchronize()
+            ms.append(e0.elapsed_time(e1))
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        return ms
+
+    # accuracy of the mixed path against FP64 (same run)
+    L.jk(s, Dd, SCHWARZ, "fp64", J=J, K=K)
+    J64, K64 = J.double().cpu().numpy(), K.double().cpu().numpy()
+    L.jk(s, Dd, SCHWARZ, "mixed", FP32_THR, J=J, K=K)
+    Jmx, Kmx = J.double().cpu().numpy(), K.double().cpu().numpy()
+    E64 = float(np.sum(D * (0.5 * J64 - 0.25 * K64)))
+    Emx = float(np.sum(D * (0.5 * Jmx - 0.25 * Kmx)))
+    dE = abs(Emx - E64)
+    mixed_ok = dE <= 1e-8
+
+    clk = clocks_start(local)
+    ms64 = timed("fp64", args.steps, args.warmup)
+    msmx = timed("mixed", args.steps, args.warmup)
+    clocks = clocks_stop(clk)
+
+    def agg(ms):
+        t = float(np.mean(ms))
+        if dist:
+            tt = torch.tensor([t], device=dev)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            t = float(tt.item())
+        return t
+
+    t64, tmx = agg(ms64), agg(msmx)
+    head = "mixed" if mixed_ok else "fp64"
+    th = tmx if mixed_ok else t64
+    plan = planmx if mixed_ok else plan64
+    value = world * plan["n_quartets"] / (th * 1e-3)
+
+    # end to end through the public API with host (pinned) buffers: H2D of D, D2H of J and K per step
+    Dh = torch.tensor(D).pin_memory()
+    Jh = torch.empty_like(Dh).pin_memory()
+    Kh = torch.empty_like(Dh).pin_memory()
+    for _ in range(max(1, args.warmup)):
+        L.jk(s, Dh, SCHWARZ, head, FP32_THR, J=Jh, K=Kh)
+    e2e_s = []
+    for _ in range(args.steps):
+        flush.fill_(1.0)
+        torch.cuda.synchronize()
+        a = time.perf_counter()
+        L.jk(s, Dh, SCHWARZ, head, FP32_THR, J=Jh, K=Kh)
+        e2e_s.append(time.perf_counter() - a)
+    e2e_t = float(np.mean(e2e_s))
+    if dist:
+        tt = torch.tensor([e2e_t], device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_t = float(tt.item())
+
+    if rank != 0:
+        if dist:
+            dist.destroy_process_group()
+        return
+
+    cpu = None
+    if world == 1 and not args.no_cpu_baseline:
+        from oracle import ref as R
+        if R.available():
+            qps, cores, stride, nq, sec = cpu_reference(1, 0, Z, xyz, D)
+            cpu = {"value": qps, "unit": "quartets/s", "cores": cores, "kind": "reference",
+                   "sample": f"reference ERI4Kernel + J/K digestion, every {stride}-th bra shell pair of every "
+                             f"class pair: {nq} quartets in {sec:.2f} s"}
+
+    flops64 = plan64["flops_fp64"]
+    achieved64 = flops64 / (t64 * 1e-3) / 1e12
+    out = {
+        "metric": METRIC, "value": value, "unit": "quartets/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": th, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64+f32 (mixed)" if mixed_ok else "f64", "data": "synthetic",
+        "config": dict(WORKLOAD, parallelism=f"replicas x{world}", path=head),
+        "jk_build_s": th * 1e-3,
+        "fp64": {"jk_build_s": t64 * 1e-3, "quartets_per_s": world * plan64["n_quartets"] / (t64 * 1e-3),
+                 "n_quartets": plan64["n_quartets"], "n_prim_quartets": plan64["n_prim_quartets"]},
+        "mixed": {"jk_build_s": tmx * 1e-3, "quartets_per_s": world * planmx["n_quartets"] / (tmx * 1e-3),
+                  "n_fp32_quartets": planmx["n_fp32"], "speedup_vs_fp64": t64 / tmx, "abs_dE_Eh": dE,
+                  "dJ_fro": float(np.linalg.norm(Jmx - J64)), "dK_fro": float(np.linalg.norm(Kmx - K64)),
+                  "meets_1e-8": mixed_ok},
+        "setup_s": setup_s,
+        "roofline": {"bound": "fp64", "achieved": achieved64, "peak": dfma, "unit": "TFLOP/s",
+                     "frac": achieved64 / dfma if dfma else None, "traffic": None,
+                     "scope": "all J/K class kernels of one FP64 build: algorithmic FLOPs / build time",
+                     "peak_source": "measured in this run: register-resident DFMA loop (lible_gpu_fp64_peak)",
+                     "dmma_peak": dmma},
+        "cpu_baseline": cpu,
+        "e2e": {"value": world * plan["n_quartets"] / e2e_t, "unit": "quartets/s",
+                "h2d_bytes_per_step": int(D.nbytes), "d2h_bytes_per_step": int(2 * D.nbytes),
+                "path": "lible_b200.jk -> lible_gpu_jk with pinned host D/J/K"},
+        "gpu_launches": int(plan["n_launches"]) * args.steps,
+        "clocks": clocks,
+    }
+    emit(out)
+    if dist:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

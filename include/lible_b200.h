@@ -1,0 +1,178 @@
+/*
+ * lible_b200: C ABI of the B200 electron-repulsion-integral engine.
+ *
+ * A drop-in for the `lible::ints` calls of MihkuU/Lible that produce 2-, 3- and 4-centre ERIs and
+ * their first nuclear derivatives, plus Schwarz-screened direct J/K, RI-J and the J/K energy
+ * gradient.  Every entry point returns a lible_gpu_status; a human-readable message for the last
+ * failure on a context is available from lible_gpu_last_error().  No C++ exception crosses this
+ * boundary.
+ *
+ * Pointers: every array argument may be a host pointer or a device pointer of the context's GPU;
+ * the library detects which (cudaPointerGetAttributes) and stages host arrays through device memory.
+ * Layouts are row-major, matching the reference's VectorMD (src/lible/vectormd.hpp:24-27).
+ *
+ * Conventions (identical to the reference): coordinates in bohr internally; `units` = 0 means the
+ * caller passes Angstrom, converted with 1/0.5291772083 (src/lible/ints/defs.hpp:9-12); AO order is
+ * atom -> shell (basis-file order) -> m = 0, +1, -1, +2, -2, ...
+ *
+ * Threading: a context owns one CUDA stream; calls on one context must be serialised by the caller.
+ * Different contexts may be used from different threads.
+ */
+#ifndef LIBLE_B200_H
+#define LIBLE_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct lible_gpu_ctx lible_gpu_ctx;
+
+typedef enum lible_gpu_status {
+    LIBLE_GPU_OK = 0,
+    LIBLE_GPU_EINVAL = 1,        /* invalid argument (index out of range, bad size, null pointer) */
+    LIBLE_GPU_ECUDA = 2,         /* CUDA runtime error */
+    LIBLE_GPU_ENOSTRUCT = 3,     /* no structure set on the context */
+    LIBLE_GPU_ENORI = 4,         /* RI call without an auxiliary basis; reference: eri2.cpp:29-30, eri3.cpp:9-10 */
+    LIBLE_GPU_EUNSUPPORTED = 5,  /* angular momentum / class outside the instantiated range */
+    LIBLE_GPU_ETIMEOUT = 6,      /* a bounded device wait gave up */
+    LIBLE_GPU_EINTERNAL = 7
+} lible_gpu_status;
+
+/* ---- context ------------------------------------------------------------------------------ */
+int lible_gpu_create(int device, lible_gpu_ctx **ctx);
+int lible_gpu_destroy(lible_gpu_ctx *ctx);
+const char *lible_gpu_last_error(const lible_gpu_ctx *ctx);
+
+/* ---- structure ------------------------------------------------------------------------------
+ * Replaces lible::ints::Structure(basis_set, [basis_set_aux,] atomic_nrs, coords_angstrom)
+ * (src/lible/ints/structure.hpp:18-27).  Basis files are read from <root>/<family>/<name>.txt in
+ * the reference's text format (src/lible/ints/basis_sets.cpp:214-277).  aux_basis may be NULL. */
+int lible_gpu_set_structure_named(lible_gpu_ctx *ctx, const char *basis_root, const char *basis,
+                                  const char *aux_root, const char *aux_basis, int n_atoms,
+                                  const int *atomic_nrs, const double *xyz, int units);
+
+/* Replaces Structure(basis_atoms_t, [basis_atoms_t,] atomic_nrs, coords) (structure.hpp:29-35):
+ * per-atom shell counts, then per shell l and primitive count, then exponents / coefficients
+ * concatenated.  The aux_* arrays may all be NULL. */
+int lible_gpu_set_structure(lible_gpu_ctx *ctx, int n_atoms, const int *atomic_nrs, const double *xyz,
+                            int units, const int *shells_per_atom, const int *shell_l,
+                            const int *shell_nprim, const double *exps, const double *coeffs,
+                            const int *aux_shells_per_atom, const int *aux_shell_l,
+                            const int *aux_shell_nprim, const double *aux_exps, const double *aux_coeffs);
+
+/* Structure::getDimAO / getDimAOAux / getNAtoms / getMaxL (structure.hpp:70-92). */
+int lible_gpu_dims(lible_gpu_ctx *ctx, long long *nao, long long *naux, int *n_atoms, int *max_l);
+
+/* ---- full tensors ----------------------------------------------------------------------------
+ * vec4d eri4(const Structure&)            (src/lible/ints/ints.hpp:165; twoel/eri4.cpp:38-95)   out[N^4]
+ * vec2d eri4Diagonal(const Structure&)    (ints.hpp:168; eri4.cpp:152-174)                    out[N^2]
+ * vec3d eri3(const Structure&)            (ints.hpp:171; eri3.cpp:7-48)                        out[N*N*Naux]
+ * vec2d eri2(const Structure&)            (ints.hpp:174; eri2.cpp:27-72)                       out[Naux^2]
+ * std::vector<double> eri2Diagonal(...)   (ints.hpp:177; eri2.cpp:74-96)                       out[Naux]   */
+int lible_gpu_eri4(lible_gpu_ctx *ctx, double *out);
+int lible_gpu_eri4_diagonal(lible_gpu_ctx *ctx, double *out);
+int lible_gpu_eri3(lible_gpu_ctx *ctx, double *out);
+int lible_gpu_eri2(lible_gpu_ctx *ctx, double *out);
+int lible_gpu_eri2_diagonal(lible_gpu_ctx *ctx, double *out);
+
+/* ---- kernel API (shell-pair classes) -----------------------------------------------------------
+ * Classes are those of shellPairData(use_symm, structure) (src/lible/ints/shell_pair_data.cpp:294-309)
+ * and shellDataAux(structure) (:280-292), in the same order, with the same pair lists and primitive
+ * screening.  ls[2*i], ls[2*i+1] = (la, lb) of class i. */
+int lible_gpu_pair_classes(lible_gpu_ctx *ctx, int use_symm, int *n_classes, int *ls,
+                           long long *n_pairs, long long *n_ppairs);
+int lible_gpu_aux_classes(lible_gpu_ctx *ctx, int *n_classes, int *ls, long long *n_shells);
+
+/* Batched ERI4Kernel::operator()(ipair_ab, ipair_cd, sp_ab, sp_cd) (twoel/eri_kernels.hpp:60-76):
+ * pairs[2*i], pairs[2*i+1] = (ipair_ab, ipair_cd); out[i] = the vec4d batch [Sa][Sb][Sc][Sd]. */
+int lible_gpu_eri4_batch(lible_gpu_ctx *ctx, int use_symm, int class_ab, int class_cd, long long n,
+                         const unsigned *pairs, double *out);
+/* ERI4D1Kernel (eri_kernels.hpp:114-132): out[i] = 12 blocks [A,B,C,D] x [x,y,z], each [Sa][Sb][Sc][Sd]. */
+int lible_gpu_eri4d1_batch(lible_gpu_ctx *ctx, int use_symm, int class_ab, int class_cd, long long n,
+                           const unsigned *pairs, double *out);
+/* ERI3Kernel (eri_kernels.hpp:78-94): idx[2*i] = ipair_ab, idx[2*i+1] = ishell_c; out[i] = [Sa][Sb][Sc]. */
+int lible_gpu_eri3_batch(lible_gpu_ctx *ctx, int use_symm, int class_ab, int aux_class, long long n,
+                         const unsigned *idx, double *out);
+/* ERI3D1Kernel (eri_kernels.hpp:134-151): out[i] = 9 blocks [A,B,C] x [x,y,z]. */
+int lible_gpu_eri3d1_batch(lible_gpu_ctx *ctx, int use_symm, int class_ab, int aux_class, long long n,
+                           const unsigned *idx, double *out);
+/* ERI2Kernel (eri_kernels.hpp:96-112) and ERI2D1Kernel (:153-169, 6 blocks [A,B] x [x,y,z]). */
+int lible_gpu_eri2_batch(lible_gpu_ctx *ctx, int aux_class_a, int aux_class_b, long long n,
+                         const unsigned *idx, double *out);
+int lible_gpu_eri2d1_batch(lible_gpu_ctx *ctx, int aux_class_a, int aux_class_b, long long n,
+                           const unsigned *idx, double *out);
+
+/* ---- direct Coulomb / exchange (no reference counterpart; built on the eri4 kernels) ----------
+ * J_mn = sum_ls (mn|ls) D_ls,  K_mn = sum_ls (ml|ns) D_ls over Schwarz-surviving unique quartets
+ * (Q_ab Q_cd >= schwarz_threshold, Q_ab = max sqrt|(mn|mn)| over the pair).  precision 0 = FP64;
+ * 1 = quartets with Q_ab Q_cd < fp32_threshold evaluated in FP32 (Boys function and J/K
+ * accumulation stay FP64).  D must be symmetric, N x N. */
+typedef struct lible_gpu_jk_opts {
+    double schwarz_threshold;  /* default 1e-12 */
+    double fp32_threshold;     /* default 1e-4 */
+    int precision;             /* 0 FP64, 1 mixed */
+} lible_gpu_jk_opts;
+
+typedef struct lible_gpu_jk_stats {
+    long long n_quartets;      /* unique contracted shell quartets evaluated */
+    long long n_fp32;          /* of which in FP32 */
+    long long n_launches;      /* kernels launched by the call */
+} lible_gpu_jk_stats;
+
+int lible_gpu_jk(lible_gpu_ctx *ctx, const double *D, double *J, double *K, const lible_gpu_jk_opts *opts,
+                 lible_gpu_jk_stats *stats);
+
+/* Size of the (cached) screening plan for these options: quartets, primitive quartets and the
+ * algorithmic FP64 / FP32 FLOPs one lible_gpu_jk call performs (dense-equivalent count). */
+typedef struct lible_gpu_jk_plan_info {
+    long long n_quartets;
+    long long n_fp32;
+    long long n_prim_quartets;
+    long long n_launches;
+    double flops_fp64;
+    double flops_fp32;
+} lible_gpu_jk_plan_info;
+
+int lible_gpu_jk_plan(lible_gpu_ctx *ctx, const lible_gpu_jk_opts *opts, lible_gpu_jk_plan_info *info);
+
+/* The context's CUDA stream (cudaStream_t), for callers that time or order work around the calls. */
+int lible_gpu_stream(lible_gpu_ctx *ctx, void **stream);
+
+/* Measured FP64 throughput of this GPU (TFLOP/s): a register-resident DFMA loop and a DMMA
+ * (mma.sync m8n8k4 f64) loop; the roofline denominators of the engine's kernels. */
+int lible_gpu_fp64_peak(lible_gpu_ctx *ctx, double *dfma_tflops, double *dmma_tflops);
+
+/* ---- J/K energy and its nuclear gradient (forward / backward pair) ----------------------------
+ * forward:  E = 1/2 Tr(D J) - 1/4 Tr(D K)  (J, K from lible_gpu_jk with opts; J/K may be NULL).
+ * backward: grad[3*atom + x] = dE/dR_{atom,x}, contracting the first-derivative integrals
+ *           (ERI4D1Kernel semantics) with the two-particle density of E on the device. */
+int lible_gpu_jk_energy_forward(lible_gpu_ctx *ctx, const double *D, const lible_gpu_jk_opts *opts,
+                                double *energy, double *J, double *K);
+int lible_gpu_jk_energy_backward(lible_gpu_ctx *ctx, const double *D, double *grad);
+
+/* ---- RI-J ------------------------------------------------------------------------------------
+ * gamma_P = sum_mn (mn|P) D_mn; (P|Q) d = gamma (Cholesky, FP64); J_mn = sum_P (mn|P) d_P.
+ * gamma / dcoef outputs may be NULL. */
+int lible_gpu_rij(lible_gpu_ctx *ctx, const double *D, double *J, double *gamma, double *dcoef);
+/* The two contractions separately (either output may be NULL). */
+int lible_gpu_ri_contract(lible_gpu_ctx *ctx, const double *D, const double *dcoef, double *gamma,
+                          double *J);
+
+/* ---- host-only helpers (no GPU needed) --------------------------------------------------------
+ * The host set-up the kernels consume, exposed for checking against the reference:
+ *  - sphericalTrafo(l) (src/lible/ints/spherical_trafo.cpp:9-690): up to *n (row, cart, value) terms;
+ *  - shell AO norms from the spherical self-overlap (src/lible/ints/shell.cpp:11-46);
+ *  - shell-pair class sizes of shellPairData(use_symm, structure) (shell_pair_data.cpp:73-309);
+ *  - the Boys function F_0..F_n(x) by the engine's grid method (boys_function.cpp:71-118). */
+int lible_host_spherical_trafo(int l, int *n, int *rows, int *carts, double *vals);
+int lible_host_shell_norms(int l, int n_prim, const double *exps, const double *coeffs, double *norms);
+int lible_host_pair_classes(const char *basis_root, const char *basis, int n_atoms, const int *atomic_nrs,
+                            const double *xyz, int units, int use_symm, int *n_classes, int *ls,
+                            long long *n_pairs, long long *n_ppairs);
+int lible_host_boys(int n, double x, double *F);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LIBLE_B200_H */

@@ -1,0 +1,97 @@
+"""Loads liblible_b200.so and declares the C ABI of include/lible_b200.h for ctypes."""
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "liblible_b200.so")
+
+STATUS = {0: "OK", 1: "EINVAL", 2: "ECUDA", 3: "ENOSTRUCT", 4: "ENORI", 5: "EUNSUPPORTED", 6: "ETIMEOUT",
+          7: "EINTERNAL"}
+
+
+class LibleGpuError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"{STATUS.get(code, code)}: {msg}")
+        self.code = code
+
+
+class JKOpts(ctypes.Structure):
+    _fields_ = [("schwarz_threshold", ctypes.c_double), ("fp32_threshold", ctypes.c_double),
+                ("precision", ctypes.c_int)]
+
+
+class JKStats(ctypes.Structure):
+    _fields_ = [("n_quartets", ctypes.c_longlong), ("n_fp32", ctypes.c_longlong), ("n_launches", ctypes.c_longlong)]
+
+
+class JKPlanInfo(ctypes.Structure):
+    _fields_ = [("n_quartets", ctypes.c_longlong), ("n_fp32", ctypes.c_longlong),
+                ("n_prim_quartets", ctypes.c_longlong), ("n_launches", ctypes.c_longlong),
+                ("flops_fp64", ctypes.c_double), ("flops_fp32", ctypes.c_double)]
+
+
+# name -> argument types; every function returns int (status) unless noted
+P = ctypes.c_void_p
+I = ctypes.c_int
+LL = ctypes.c_longlong
+D = ctypes.c_double
+S = ctypes.c_char_p
+SIGNATURES = {
+    "lible_gpu_create": [I, ctypes.POINTER(P)],
+    "lible_gpu_destroy": [P],
+    "lible_gpu_set_structure_named": [P, S, S, S, S, I, P, P, I],
+    "lible_gpu_set_structure": [P, I, P, P, I, P, P, P, P, P, P, P, P, P, P],
+    "lible_gpu_dims": [P, P, P, P, P],
+    "lible_gpu_eri4": [P, P],
+    "lible_gpu_eri4_diagonal": [P, P],
+    "lible_gpu_eri3": [P, P],
+    "lible_gpu_eri2": [P, P],
+    "lible_gpu_eri2_diagonal": [P, P],
+    "lible_gpu_pair_classes": [P, I, P, P, P, P],
+    "lible_gpu_aux_classes": [P, P, P, P],
+    "lible_gpu_eri4_batch": [P, I, I, I, LL, P, P],
+    "lible_gpu_eri4d1_batch": [P, I, I, I, LL, P, P],
+    "lible_gpu_eri3_batch": [P, I, I, I, LL, P, P],
+    "lible_gpu_eri3d1_batch": [P, I, I, I, LL, P, P],
+    "lible_gpu_eri2_batch": [P, I, I, LL, P, P],
+    "lible_gpu_eri2d1_batch": [P, I, I, LL, P, P],
+    "lible_gpu_jk": [P, P, P, P, ctypes.POINTER(JKOpts), ctypes.POINTER(JKStats)],
+    "lible_gpu_jk_energy_forward": [P, P, ctypes.POINTER(JKOpts), P, P, P],
+    "lible_gpu_jk_energy_backward": [P, P, P],
+    "lible_gpu_rij": [P, P, P, P, P],
+    "lible_gpu_jk_plan": [P, ctypes.POINTER(JKOpts), ctypes.POINTER(JKPlanInfo)],
+    "lible_gpu_stream": [P, ctypes.POINTER(P)],
+    "lible_gpu_fp64_peak": [P, ctypes.POINTER(D), ctypes.POINTER(D)],
+    "lible_gpu_ri_contract": [P, P, P, P, P],
+    "lible_host_spherical_trafo": [I, P, P, P, P],
+    "lible_host_shell_norms": [I, I, P, P, P],
+    "lible_host_pair_classes": [S, S, I, P, P, I, I, P, P, P, P],
+    "lible_host_boys": [I, D, P],
+}
+
+_lib = None
+
+
+def load():
+    """Returns the loaded library; raises if the CUDA extension has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"{LIB_PATH} is missing: build it with `python -m lible_b200.build` "
+                           "(there is no CPU fallback)")
+    lib = ctypes.CDLL(LIB_PATH)
+    for name, args in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.argtypes = args
+        fn.restype = ctypes.c_int
+    lib.lible_gpu_last_error.argtypes = [P]
+    lib.lible_gpu_last_error.restype = ctypes.c_char_p
+    _lib = lib
+    return lib
+
+
+def check(ctx, code):
+    if code != 0:
+        msg = load().lible_gpu_last_error(ctx)
+        raise LibleGpuError(code, msg.decode() if msg else "")

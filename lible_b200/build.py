@@ -1,0 +1,92 @@
+"""Builds lible_b200/liblible_b200.so (sm_100a) in-tree with nvcc.
+
+Objects go to lible_b200/_build/; each translation unit is rebuilt when it or any header under
+csrc/ is newer than its object.  Instantiation files are regenerated first.
+
+    python -m lible_b200.build [-j N]
+"""
+import argparse
+import concurrent.futures as cf
+import glob
+import os
+import shutil
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(HERE, "csrc")
+OUT_DIR = os.path.join(HERE, "_build")
+LIB = os.path.join(HERE, "liblible_b200.so")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+NVCC_FLAGS = ARCH + ["-lineinfo", "-O3", "-std=c++17", "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC",
+                     "-Xcompiler", "-O3", "-I" + CSRC]
+
+
+def nvcc():
+    cand = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    if not os.path.exists(cand):
+        raise RuntimeError("nvcc not found")
+    return cand
+
+
+def sources():
+    sys.path.insert(0, CSRC)
+    import gen_instances  # noqa: E402
+    gen_instances.main()
+    srcs = [os.path.join(CSRC, f) for f in ("host_math.cpp", "host_basis.cpp", "engine.cu", "peak.cu", "capi.cpp")]
+    srcs += sorted(glob.glob(os.path.join(CSRC, "gen", "*.cu")))
+    return srcs
+
+
+def newest_header():
+    hdrs = glob.glob(os.path.join(CSRC, "*.hpp")) + glob.glob(os.path.join(CSRC, "*.cuh"))
+    hdrs.append(os.path.join(os.path.dirname(HERE), "include", "lible_b200.h"))
+    return max(os.path.getmtime(h) for h in hdrs if os.path.exists(h))
+
+
+def obj_path(src):
+    rel = os.path.relpath(src, CSRC).replace(os.sep, "_")
+    return os.path.join(OUT_DIR, rel + ".o")
+
+
+def compile_one(src, hdr_time, verbose=False):
+    obj = obj_path(src)
+    if os.path.exists(obj) and os.path.getmtime(obj) >= max(os.path.getmtime(src), hdr_time):
+        return obj, None
+    cmd = [nvcc()] + NVCC_FLAGS + ["-c", src, "-o", obj]
+    if src.endswith(".cpp"):
+        cmd = [nvcc(), "-x", "cu"] + NVCC_FLAGS + ["-c", src, "-o", obj]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        return obj, r.stderr + r.stdout
+    if verbose:
+        print("compiled", os.path.relpath(src, HERE), flush=True)
+    return obj, None
+
+
+def build(jobs=None, verbose=False):
+    os.makedirs(OUT_DIR, exist_ok=True)
+    srcs = sources()
+    hdr = newest_header()
+    jobs = jobs or os.cpu_count() or 4
+    objs, errors = [], []
+    with cf.ThreadPoolExecutor(max_workers=jobs) as ex:
+        for obj, err in ex.map(lambda s: compile_one(s, hdr, verbose), srcs):
+            objs.append(obj)
+            if err:
+                errors.append(err)
+    if errors:
+        raise RuntimeError("nvcc failed:\n" + "\n".join(errors)[:20000])
+    if not os.path.exists(LIB) or os.path.getmtime(LIB) < max(os.path.getmtime(o) for o in objs):
+        cmd = [nvcc()] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart", "-lcusolver"]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError("link failed:\n" + r.stderr + r.stdout)
+    return LIB
+
+
+if __name__ == "__main__":
+    ap = argparse.ArgumentParser()
+    ap.add_argument("-j", type=int, default=None)
+    args = ap.parse_args()
+    print(build(args.j, verbose=True))

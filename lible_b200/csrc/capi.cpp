@@ -1,0 +1,703 @@
+// The C ABI (include/lible_b200.h) over the Engine.  Converts exceptions to status codes and
+// stages host arrays through device memory.
+#include "../../include/lible_b200.h"
+#include "engine_api.hpp"
+
+#include <cuda_runtime.h>
+#include <cusolverDn.h>
+
+#include <cstring>
+#include <memory>
+#include <string>
+
+using namespace lible_b200;
+
+struct lible_gpu_ctx
+{
+    std::unique_ptr<Engine> eng;
+    std::string err;
+};
+
+namespace
+{
+    int fail(lible_gpu_ctx *ctx, int code, const std::string &msg)
+    {
+        if (ctx)
+            ctx->err = msg;
+        return code;
+    }
+
+    template <class F>
+    int guard(lible_gpu_ctx *ctx, F &&f)
+    {
+        if (!ctx || !ctx->eng)
+            return LIBLE_GPU_EINVAL;
+        try
+        {
+            cudaSetDevice(ctx->eng->device());
+            f(*ctx->eng);
+            ctx->err.clear();
+            return LIBLE_GPU_OK;
+        }
+        catch (const EngineError &e)
+        {
+            return fail(ctx, e.code, e.what());
+        }
+        catch (const std::exception &e)
+        {
+            return fail(ctx, LIBLE_GPU_EINTERNAL, e.what());
+        }
+    }
+
+    bool isDevice(const void *p)
+    {
+        if (!p)
+            return false;
+        cudaPointerAttributes at{};
+        if (cudaPointerGetAttributes(&at, p) != cudaSuccess)
+        {
+            cudaGetLastError();
+            return false;
+        }
+        return at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged;
+    }
+
+    // Device view of a caller array: the array itself if it is device memory, else a staged copy.
+    struct DevArray
+    {
+        double *ptr = nullptr;
+        double *user = nullptr;
+        size_t n = 0;
+        bool owned = false;
+        cudaStream_t s = nullptr;
+
+        DevArray(const double *p, size_t count, bool copy_in, cudaStream_t stream)
+            : user(const_cast<double *>(p)), n(count), s(stream)
+        {
+            if (!p)
+                return;
+            if (isDevice(p))
+            {
+                ptr = const_cast<double *>(p);
+                return;
+            }
+            cudaCheck(cudaMalloc(&ptr, std::max<size_t>(n, 1) * sizeof(double)), "cudaMalloc");
+            owned = true;
+            if (copy_in)
+                cudaCheck(cudaMemcpyAsync(ptr, p, n * sizeof(double), cudaMemcpyHostToDevice, s), "H2D");
+        }
+        void copyOut()
+        {
+            if (owned && user)
+            {
+                cudaCheck(cudaMemcpyAsync(user, ptr, n * sizeof(double), cudaMemcpyDeviceToHost, s), "D2H");
+                cudaCheck(cudaStreamSynchronize(s), "D2H");
+            }
+            else
+                cudaCheck(cudaStreamSynchronize(s), "sync");
+        }
+        ~DevArray()
+        {
+            if (owned)
+                cudaFree(ptr);
+        }
+    };
+
+    std::vector<std::array<double, 3>> coords(int n_atoms, const double *xyz, int units)
+    {
+        std::vector<std::array<double, 3>> c(n_atoms);
+        const double f = units == 0 ? kAngstromToBohr : 1.0;
+        for (int a = 0; a < n_atoms; a++)
+            for (int k = 0; k < 3; k++)
+                c[a][k] = xyz[3 * a + k] * f;
+        return c;
+    }
+
+    std::vector<BasisAtom> atomsFromArrays(int n_atoms, const int *Z, const int *nsh, const int *l,
+                                           const int *np, const double *exps, const double *coeffs)
+    {
+        std::vector<BasisAtom> atoms(n_atoms);
+        size_t is = 0, ip = 0;
+        for (int a = 0; a < n_atoms; a++)
+        {
+            atoms[a].z = Z[a];
+            for (int k = 0; k < nsh[a]; k++, is++)
+            {
+                BasisShell s;
+                s.l = l[is];
+                if (np[is] <= 0)
+                    throw EngineError(kStatusInvalid, "shell with no primitives");
+                for (int p = 0; p < np[is]; p++, ip++)
+                {
+                    s.exps.push_back(exps[ip]);
+                    s.coeffs.push_back(coeffs[ip]);
+                }
+                atoms[a].shells.push_back(s);
+            }
+        }
+        return atoms;
+    }
+}
+
+extern "C" {
+
+int lible_host_spherical_trafo(int l, int *n, int *rows, int *carts, double *vals)
+{
+    if (!n || l < 0 || l > 8)
+        return LIBLE_GPU_EINVAL;
+    auto t = sphericalTrafo(l);
+    const int cap = *n;
+    *n = (int)t.size();
+    if (rows && carts && vals)
+        for (int i = 0; i < (int)t.size() && i < cap; i++)
+        {
+            rows[i] = t[i].row;
+            carts[i] = t[i].cart;
+            vals[i] = t[i].val;
+        }
+    return LIBLE_GPU_OK;
+}
+
+int lible_host_shell_norms(int l, int n_prim, const double *exps, const double *coeffs, double *norms)
+{
+    if (l < 0 || l > kMaxL || n_prim <= 0 || !exps || !coeffs || !norms)
+        return LIBLE_GPU_EINVAL;
+    std::vector<double> e(exps, exps + n_prim), c(coeffs, coeffs + n_prim), pn;
+    for (double x : e)
+        pn.push_back(purePrimitiveNorm(l, x));
+    auto v = shellNorms(l, e, c, pn);
+    std::copy(v.begin(), v.end(), norms);
+    return LIBLE_GPU_OK;
+}
+
+int lible_host_pair_classes(const char *basis_root, const char *basis, int n_atoms, const int *atomic_nrs,
+                            const double *xyz, int units, int use_symm, int *n_classes, int *ls, long long *n_pairs,
+                            long long *n_ppairs)
+{
+    if (!basis_root || !basis || n_atoms <= 0 || !atomic_nrs || !xyz || !n_classes)
+        return LIBLE_GPU_EINVAL;
+    try
+    {
+        std::string path = findBasisFile(basis_root, basis);
+        std::vector<BasisAtom> atoms;
+        for (int a = 0; a < n_atoms; a++)
+            atoms.push_back(readBasisAtom(path, atomic_nrs[a]));
+        auto shells = constructShells(atoms, coords(n_atoms, xyz, units));
+        int lmax = 0;
+        for (const auto &s : shells)
+            lmax = std::max(lmax, s.l);
+        auto byL = [&](int l) {
+            std::vector<Shell> v;
+            for (const auto &s : shells)
+                if (s.l == l)
+                    v.push_back(s);
+            return v;
+        };
+        int k = 0;
+        for (int la = 0; la <= lmax; la++)
+            for (int lb = 0; lb <= (use_symm ? la : lmax); lb++, k++)
+            {
+                if (ls)
+                {
+                    PairClass pc = buildPairClass(use_symm != 0, la, lb, byL(la), byL(lb));
+                    ls[2 * k] = la;
+                    ls[2 * k + 1] = lb;
+                    if (n_pairs)
+                        n_pairs[k] = (long long)pc.n_pairs;
+                    if (n_ppairs)
+                        n_ppairs[k] = (long long)pc.n_ppairs;
+                }
+            }
+        *n_classes = k;
+        return LIBLE_GPU_OK;
+    }
+    catch (const EngineError &e)
+    {
+        return e.code;
+    }
+    catch (const std::exception &)
+    {
+        return LIBLE_GPU_EINVAL;
+    }
+}
+
+int lible_host_boys(int n, double x, double *F)
+{
+    if (n < 0 || n >= kBoysCols - 6 || !F || !(x >= 0))
+        return LIBLE_GPU_EINVAL;
+    static const std::vector<double> grid = boysGrid();
+    boysHost(n, x, grid, F);
+    return LIBLE_GPU_OK;
+}
+
+int lible_gpu_create(int device, lible_gpu_ctx **ctx)
+{
+    if (!ctx)
+        return LIBLE_GPU_EINVAL;
+    *ctx = nullptr;
+    auto *c = new lible_gpu_ctx;
+    try
+    {
+        c->eng = std::make_unique<Engine>(device);
+    }
+    catch (const EngineError &e)
+    {
+        delete c;
+        return e.code;
+    }
+    catch (const std::exception &)
+    {
+        delete c;
+        return LIBLE_GPU_EINTERNAL;
+    }
+    *ctx = c;
+    return LIBLE_GPU_OK;
+}
+
+int lible_gpu_destroy(lible_gpu_ctx *ctx)
+{
+    delete ctx;
+    return LIBLE_GPU_OK;
+}
+
+const char *lible_gpu_last_error(const lible_gpu_ctx *ctx)
+{
+    return ctx ? ctx->err.c_str() : "null context";
+}
+
+int lible_gpu_set_structure_named(lible_gpu_ctx *ctx, const char *basis_root, const char *basis,
+                                  const char *aux_root, const char *aux_basis, int n_atoms,
+                                  const int *atomic_nrs, const double *xyz, int units)
+{
+    return guard(ctx, [&](Engine &e) {
+        if (!basis_root || !basis || n_atoms <= 0 || !atomic_nrs || !xyz)
+            throw EngineError(kStatusInvalid, "invalid structure arguments");
+        std::string path = findBasisFile(basis_root, basis);
+        std::vector<BasisAtom> main;
+        for (int a = 0; a < n_atoms; a++)
+            main.push_back(readBasisAtom(path, atomic_nrs[a]));
+        std::vector<BasisAtom> aux;
+        if (aux_basis && aux_basis[0])
+        {
+            std::string apath = findBasisFile(aux_root ? aux_root : basis_root, aux_basis);
+            for (int a = 0; a < n_atoms; a++)
+                aux.push_back(readBasisAtom(apath, atomic_nrs[a]));
+        }
+        e.setStructure(main, (aux_basis && aux_basis[0]) ? &aux : nullptr, coords(n_atoms, xyz, units));
+    });
+}
+
+int lible_gpu_set_structure(lible_gpu_ctx *ctx, int n_atoms, const int *atomic_nrs, const double *xyz, int units,
+                            const int *shells_per_atom, const int *shell_l, const int *shell_nprim,
+                            const double *exps, const double *coeffs, const int *aux_shells_per_atom,
+                            const int *aux_shell_l, const int *aux_shell_nprim, const double *aux_exps,
+                            const double *aux_coeffs)
+{
+    return guard(ctx, [&](Engine &e) {
+        if (n_atoms <= 0 || !atomic_nrs || !xyz || !shells_per_atom || !shell_l || !shell_nprim || !exps || !coeffs)
+            throw EngineError(kStatusInvalid, "invalid structure arguments");
+        auto main = atomsFromArrays(n_atoms, atomic_nrs, shells_per_atom, shell_l, shell_nprim, exps, coeffs);
+        std::vector<BasisAtom> aux;
+        if (aux_shells_per_atom)
+            aux = atomsFromArrays(n_atoms, atomic_nrs, aux_shells_per_atom, aux_shell_l, aux_shell_nprim, aux_exps,
+                                  aux_coeffs);
+        e.setStructure(main, aux_shells_per_atom ? &aux : nullptr, coords(n_atoms, xyz, units));
+    });
+}
+
+int lible_gpu_dims(lible_gpu_ctx *ctx, long long *nao, long long *naux, int *n_atoms, int *max_l)
+{
+    return guard(ctx, [&](Engine &e) {
+        if (nao)
+            *nao = (long long)e.nao();
+        if (naux)
+            *naux = (long long)e.naux();
+        if (n_atoms)
+            *n_atoms = e.nAtoms();
+        if (max_l)
+            *max_l = e.maxL();
+    });
+}
+
+int lible_gpu_eri4(lible_gpu_ctx *ctx, double *out)
+{
+    return guard(ctx, [&](Engine &e) {
+        const size_t n = e.nao();
+        DevArray o(out, n * n * n * n, false, e.stream());
+        e.eri4(o.ptr);
+        o.copyOut();
+    });
+}
+
+int lible_gpu_eri4_diagonal(lible_gpu_ctx *ctx, double *out)
+{
+    return guard(ctx, [&](Engine &e) {
+        const size_t n = e.nao();
+        std::vector<double> h(n * n);
+        e.eri4Diagonal(h.data());
+        if (isDevice(out))
+            cudaCheck(cudaMemcpy(out, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice), "copy");
+        else
+            std::memcpy(out, h.data(), h.size() * sizeof(double));
+    });
+}
+
+int lible_gpu_eri3(lible_gpu_ctx *ctx, double *out)
+{
+    return guard(ctx, [&](Engine &e) {
+        if (!e.hasAux())
+            throw EngineError(kStatusNoAux, "RI approximation is not enabled!");
+        const size_t n = e.nao();
+        DevArray o(out, n * n * e.naux(), false, e.stream());
+        e.eri3(o.ptr);
+        o.copyOut();
+    });
+}
+
+int lible_gpu_eri2(lible_gpu_ctx *ctx, double *out)
+{
+    return guard(ctx, [&](Engine &e) {
+        if (!e.hasAux())
+            throw EngineError(kStatusNoAux, "eri2(): RI approximation is not enabled");
+        DevArray o(out, e.naux() * e.naux(), false, e.stream());
+        e.eri2(o.ptr);
+        o.copyOut();
+    });
+}
+
+int lible_gpu_eri2_diagonal(lible_gpu_ctx *ctx, double *out)
+{
+    return guard(ctx, [&](Engine &e) {
+        if (!e.hasAux())
+            throw EngineError(kStatusNoAux, "eri2Diagonal(): RI approximation is not enabled");
+        std::vector<double> h(e.naux());
+        e.eri2Diagonal(h.data());
+        if (isDevice(out))
+            cudaCheck(cudaMemcpy(out, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice), "copy");
+        else
+            std::memcpy(out, h.data(), h.size() * sizeof(double));
+    });
+}
+
+int lible_gpu_pair_classes(lible_gpu_ctx *ctx, int use_symm, int *n_classes, int *ls, long long *n_pairs,
+                           long long *n_ppairs)
+{
+    return guard(ctx, [&](Engine &e) {
+        auto ci = e.pairClasses(use_symm != 0);
+        if (n_classes)
+            *n_classes = (int)ci.size();
+        for (size_t i = 0; i < ci.size(); i++)
+        {
+            if (ls)
+            {
+                ls[2 * i] = ci[i].la;
+                ls[2 * i + 1] = ci[i].lb;
+            }
+            if (n_pairs)
+                n_pairs[i] = ci[i].n_pairs;
+            if (n_ppairs)
+                n_ppairs[i] = ci[i].n_ppairs;
+        }
+    });
+}
+
+int lible_gpu_aux_classes(lible_gpu_ctx *ctx, int *n_classes, int *ls, long long *n_shells)
+{
+    return guard(ctx, [&](Engine &e) {
+        auto ci = e.auxClasses();
+        if (n_classes)
+            *n_classes = (int)ci.size();
+        for (size_t i = 0; i < ci.size(); i++)
+        {
+            if (ls)
+                ls[i] = ci[i].la;
+            if (n_shells)
+                n_shells[i] = ci[i].n_pairs;
+        }
+    });
+}
+
+static int batch4(lible_gpu_ctx *ctx, int use_symm, int cab, int ccd, long long n, const unsigned *pairs, double *out,
+                  bool d1)
+{
+    return guard(ctx, [&](Engine &e) {
+        if (n < 0 || (n > 0 && (!pairs || !out)))
+            throw EngineError(kStatusInvalid, "invalid batch arguments");
+        auto ci = e.pairClasses(use_symm != 0);
+        if (cab < 0 || ccd < 0 || cab >= (int)ci.size() || ccd >= (int)ci.size())
+            throw EngineError(kStatusInvalid, "class index out of range");
+        const size_t blk = (size_t)nsph(ci[cab].la) * nsph(ci[cab].lb) * nsph(ci[ccd].la) * nsph(ci[ccd].lb);
+        DevArray o(out, (size_t)n * blk * (d1 ? 12 : 1), false, e.stream());
+        e.eri4Batch(use_symm != 0, cab, ccd, n, pairs, o.ptr, d1);
+        o.copyOut();
+    });
+}
+
+int lible_gpu_eri4_batch(lible_gpu_ctx *ctx, int use_symm, int class_ab, int class_cd, long long n,
+                         const unsigned *pairs, double *out)
+{
+    return batch4(ctx, use_symm, class_ab, class_cd, n, pairs, out, false);
+}
+
+int lible_gpu_eri4d1_batch(lible_gpu_ctx *ctx, int use_symm, int class_ab, int class_cd, long long n,
+                           const unsigned *pairs, double *out)
+{
+    return batch4(ctx, use_symm, class_ab, class_cd, n, pairs, out, true);
+}
+
+static int batch3(lible_gpu_ctx *ctx, int use_symm, int cab, int cx, long long n, const unsigned *idx, double *out,
+                  bool d1)
+{
+    return guard(ctx, [&](Engine &e) {
+        if (n < 0 || (n > 0 && (!idx || !out)))
+            throw EngineError(kStatusInvalid, "invalid batch arguments");
+        auto ci = e.pairClasses(use_symm != 0);
+        auto xi = e.auxClasses();
+        if (cab < 0 || cx < 0 || cab >= (int)ci.size() || cx >= (int)xi.size())
+            throw EngineError(kStatusInvalid, "class index out of range");
+        const size_t blk = (size_t)nsph(ci[cab].la) * nsph(ci[cab].lb) * nsph(xi[cx].la);
+        DevArray o(out, (size_t)n * blk * (d1 ? 9 : 1), false, e.stream());
+        e.eri3Batch(use_symm != 0, cab, cx, n, idx, o.ptr, d1);
+        o.copyOut();
+    });
+}
+
+int lible_gpu_eri3_batch(lible_gpu_ctx *ctx, int use_symm, int class_ab, int aux_class, long long n,
+                         const unsigned *idx, double *out)
+{
+    return batch3(ctx, use_symm, class_ab, aux_class, n, idx, out, false);
+}
+
+int lible_gpu_eri3d1_batch(lible_gpu_ctx *ctx, int use_symm, int class_ab, int aux_class, long long n,
+                           const unsigned *idx, double *out)
+{
+    return batch3(ctx, use_symm, class_ab, aux_class, n, idx, out, true);
+}
+
+static int batch2(lible_gpu_ctx *ctx, int ca, int cb, long long n, const unsigned *idx, double *out, bool d1)
+{
+    return guard(ctx, [&](Engine &e) {
+        if (n < 0 || (n > 0 && (!idx || !out)))
+            throw EngineError(kStatusInvalid, "invalid batch arguments");
+        auto xi = e.auxClasses();
+        if (ca < 0 || cb < 0 || ca >= (int)xi.size() || cb >= (int)xi.size())
+            throw EngineError(kStatusInvalid, "class index out of range");
+        const size_t blk = (size_t)nsph(xi[ca].la) * nsph(xi[cb].la);
+        DevArray o(out, (size_t)n * blk * (d1 ? 6 : 1), false, e.stream());
+        e.eri2Batch(ca, cb, n, idx, o.ptr, d1);
+        o.copyOut();
+    });
+}
+
+int lible_gpu_eri2_batch(lible_gpu_ctx *ctx, int a, int b, long long n, const unsigned *idx, double *out)
+{
+    return batch2(ctx, a, b, n, idx, out, false);
+}
+
+int lible_gpu_eri2d1_batch(lible_gpu_ctx *ctx, int a, int b, long long n, const unsigned *idx, double *out)
+{
+    return batch2(ctx, a, b, n, idx, out, true);
+}
+
+static JKOptions toOpts(const lible_gpu_jk_opts *o)
+{
+    JKOptions j;
+    if (o)
+    {
+        j.schwarz = o->schwarz_threshold;
+        j.fp32_threshold = o->fp32_threshold;
+        j.precision = o->precision;
+    }
+    return j;
+}
+
+int lible_gpu_jk(lible_gpu_ctx *ctx, const double *D, double *J, double *K, const lible_gpu_jk_opts *opts,
+                 lible_gpu_jk_stats *stats)
+{
+    return guard(ctx, [&](Engine &e) {
+        if (!D || !J || !K)
+            throw EngineError(kStatusInvalid, "null D/J/K");
+        const size_t n = e.nao();
+        DevArray d(D, n * n, true, e.stream());
+        DevArray j(J, n * n, false, e.stream());
+        DevArray k(K, n * n, false, e.stream());
+        JKStats st;
+        e.jk(d.ptr, j.ptr, k.ptr, toOpts(opts), &st);
+        j.copyOut();
+        k.copyOut();
+        if (stats)
+        {
+            stats->n_quartets = st.n_quartets;
+            stats->n_fp32 = st.n_fp32;
+            stats->n_launches = st.n_launches;
+        }
+    });
+}
+
+int lible_gpu_jk_plan(lible_gpu_ctx *ctx, const lible_gpu_jk_opts *opts, lible_gpu_jk_plan_info *info)
+{
+    return guard(ctx, [&](Engine &e) {
+        if (!info)
+            throw EngineError(kStatusInvalid, "null info");
+        JKPlanInfo p = e.jkPlanInfo(toOpts(opts));
+        info->n_quartets = p.n_quartets;
+        info->n_fp32 = p.n_fp32;
+        info->n_prim_quartets = p.n_prim_quartets;
+        info->n_launches = p.n_launches;
+        info->flops_fp64 = p.flops_fp64;
+        info->flops_fp32 = p.flops_fp32;
+    });
+}
+
+int lible_gpu_stream(lible_gpu_ctx *ctx, void **stream)
+{
+    return guard(ctx, [&](Engine &e) {
+        if (!stream)
+            throw EngineError(kStatusInvalid, "null stream");
+        *stream = (void *)e.stream();
+    });
+}
+
+int lible_gpu_fp64_peak(lible_gpu_ctx *ctx, double *dfma, double *dmma)
+{
+    return guard(ctx, [&](Engine &e) {
+        auto p = measureFp64Peak(e.device(), e.stream());
+        if (dfma)
+            *dfma = p.first;
+        if (dmma)
+            *dmma = p.second;
+    });
+}
+
+int lible_gpu_jk_energy_forward(lible_gpu_ctx *ctx, const double *D, const lible_gpu_jk_opts *opts, double *energy,
+                                double *J, double *K)
+{
+    return guard(ctx, [&](Engine &e) {
+        if (!D || !energy)
+            throw EngineError(kStatusInvalid, "null D/energy");
+        const size_t n = e.nao();
+        DevArray d(D, n * n, true, e.stream());
+        DevArray j(J, n * n, false, e.stream());
+        DevArray k(K, n * n, false, e.stream());
+        double *jp = j.ptr, *kp = k.ptr, *tmp = nullptr;
+        if (!jp || !kp)
+        {
+            cudaCheck(cudaMalloc(&tmp, 2 * n * n * sizeof(double)), "cudaMalloc");
+            if (!jp)
+                jp = tmp;
+            if (!kp)
+                kp = tmp + n * n;
+        }
+        e.jk(d.ptr, jp, kp, toOpts(opts), nullptr);
+        std::vector<double> hd(n * n), hj(n * n), hk(n * n);
+        cudaCheck(cudaMemcpyAsync(hd.data(), d.ptr, n * n * 8, cudaMemcpyDeviceToHost, e.stream()), "D2H");
+        cudaCheck(cudaMemcpyAsync(hj.data(), jp, n * n * 8, cudaMemcpyDeviceToHost, e.stream()), "D2H");
+        cudaCheck(cudaMemcpyAsync(hk.data(), kp, n * n * 8, cudaMemcpyDeviceToHost, e.stream()), "D2H");
+        cudaCheck(cudaStreamSynchronize(e.stream()), "sync");
+        double s = 0.0;
+        for (size_t x = 0; x < n * n; x++)
+            s += hd[x] * (0.5 * hj[x] - 0.25 * hk[x]);
+        *energy = s;
+        if (J)
+            j.copyOut();
+        if (K)
+            k.copyOut();
+        if (tmp)
+            cudaFree(tmp);
+    });
+}
+
+int lible_gpu_jk_energy_backward(lible_gpu_ctx *ctx, const double *D, double *grad)
+{
+    return guard(ctx, [&](Engine &e) {
+        if (!D || !grad)
+            throw EngineError(kStatusInvalid, "null D/grad");
+        const size_t n = e.nao();
+        DevArray d(D, n * n, true, e.stream());
+        DevArray g(grad, 3 * (size_t)e.nAtoms(), false, e.stream());
+        e.jkGradient(d.ptr, g.ptr);
+        g.copyOut();
+    });
+}
+
+int lible_gpu_ri_contract(lible_gpu_ctx *ctx, const double *D, const double *dcoef, double *gamma, double *J)
+{
+    return guard(ctx, [&](Engine &e) {
+        if (!e.hasAux())
+            throw EngineError(kStatusNoAux, "RI approximation is not enabled");
+        const size_t n = e.nao(), na = e.naux();
+        DevArray d(D, n * n, true, e.stream());
+        DevArray c(dcoef, na, true, e.stream());
+        DevArray g(gamma, na, false, e.stream());
+        DevArray j(J, n * n, false, e.stream());
+        if ((gamma && !D) || (J && !dcoef))
+            throw EngineError(kStatusInvalid, "missing input");
+        e.riContract(d.ptr, c.ptr, g.ptr, j.ptr);
+        if (gamma)
+            g.copyOut();
+        if (J)
+            j.copyOut();
+    });
+}
+
+int lible_gpu_rij(lible_gpu_ctx *ctx, const double *D, double *J, double *gamma, double *dcoef)
+{
+    return guard(ctx, [&](Engine &e) {
+        if (!e.hasAux())
+            throw EngineError(kStatusNoAux, "RI approximation is not enabled");
+        if (!D || !J)
+            throw EngineError(kStatusInvalid, "null D/J");
+        const size_t n = e.nao(), na = e.naux();
+        DevArray d(D, n * n, true, e.stream());
+        DevArray j(J, n * n, false, e.stream());
+        double *metric = nullptr, *rhs = nullptr, *work = nullptr;
+        int *info = nullptr;
+        cudaCheck(cudaMalloc(&metric, na * na * sizeof(double)), "cudaMalloc");
+        cudaCheck(cudaMalloc(&rhs, na * sizeof(double)), "cudaMalloc");
+        cudaCheck(cudaMalloc(&info, sizeof(int)), "cudaMalloc");
+        e.riContract(d.ptr, nullptr, rhs, nullptr);
+        if (gamma)
+        {
+            e.sync();
+            if (isDevice(gamma))
+                cudaCheck(cudaMemcpy(gamma, rhs, na * 8, cudaMemcpyDeviceToDevice), "copy");
+            else
+                cudaCheck(cudaMemcpy(gamma, rhs, na * 8, cudaMemcpyDeviceToHost), "copy");
+        }
+        e.eri2(metric);
+        e.sync();
+        cusolverDnHandle_t h;
+        if (cusolverDnCreate(&h) != CUSOLVER_STATUS_SUCCESS)
+            throw EngineError(kStatusCuda, "cusolverDnCreate failed");
+        cusolverDnSetStream(h, e.stream());
+        int lwork = 0;
+        cusolverDnDpotrf_bufferSize(h, CUBLAS_FILL_MODE_LOWER, (int)na, metric, (int)na, &lwork);
+        cudaCheck(cudaMalloc(&work, std::max(lwork, 1) * sizeof(double)), "cudaMalloc");
+        cusolverDnDpotrf(h, CUBLAS_FILL_MODE_LOWER, (int)na, metric, (int)na, work, lwork, info);
+        cusolverDnDpotrs(h, CUBLAS_FILL_MODE_LOWER, (int)na, 1, metric, (int)na, rhs, (int)na, info);
+        int hinfo = 0;
+        cudaCheck(cudaMemcpyAsync(&hinfo, info, sizeof(int), cudaMemcpyDeviceToHost, e.stream()), "info");
+        cudaCheck(cudaStreamSynchronize(e.stream()), "potrs");
+        cusolverDnDestroy(h);
+        cudaFree(work);
+        cudaFree(metric);
+        cudaFree(info);
+        if (hinfo != 0)
+        {
+            cudaFree(rhs);
+            throw EngineError(kStatusInternal, "Cholesky of the RI metric failed (info " + std::to_string(hinfo) + ")");
+        }
+        if (dcoef)
+        {
+            if (isDevice(dcoef))
+                cudaCheck(cudaMemcpy(dcoef, rhs, na * 8, cudaMemcpyDeviceToDevice), "copy");
+            else
+                cudaCheck(cudaMemcpy(dcoef, rhs, na * 8, cudaMemcpyDeviceToHost), "copy");
+        }
+        e.riContract(nullptr, rhs, nullptr, j.ptr);
+        j.copyOut();
+        cudaFree(rhs);
+    });
+}
+
+} // extern "C"

@@ -1,0 +1,1216 @@
+// Host orchestration of the B200 ERI engine: device residency of the pair classes, the
+// E-coefficient kernel, Schwarz screening, the drivers (eri4 / eri4Diagonal / eri3 / eri2 /
+// eri2Diagonal, kernel-API batches, direct J/K, RI-J, J/K gradient) and their support kernels.
+#include "engine_api.hpp"
+#include "eri_launch.cuh"
+
+#include <algorithm>
+#include <chrono>
+#include <cstring>
+#include <numeric>
+#include <stdexcept>
+
+namespace lible_b200
+{
+    // ------------------------------------------------------------------------------------------
+    // Support kernels
+
+    struct SphTables
+    {
+        const int *rc;       // [n][2] row, cart
+        const double *val;   // [n]
+        int ofs[kMaxL + 2];  // first entry of shell l
+    };
+
+    struct EArgs
+    {
+        int la, lb;
+        size_t n_pairs, n_ppairs;
+        const double *exps, *coeffs, *coords, *norms_a, *norms_b;
+        const uint32_t *pofs;
+        SphTables sph;
+        double *pP, *ab, *E, *Et, *E1, *E1t;
+        float *Ef, *Etf;
+    };
+
+    // Hermite E matrices of every primitive pair of one class, with the spherical transforms of both
+    // shells, the AO norms and the contraction coefficients folded in:
+    //   E[mu nu][tuv] = N_mu N_nu d_a d_b sum_{i in mu} sum_{j in nu} T_a T_b E^x_{ij,t} E^y E^z
+    // (src/lible/ints/ecoeffs.cpp:314-403) and its derivative with respect to A - B
+    // (src/lible/ints/ecoeffs.cpp:405-517).  One thread per primitive pair.
+    __global__ void ecoeffKernel(EArgs a)
+    {
+        const size_t ip = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+        if (ip >= a.n_ppairs)
+            return;
+        // owning pair by binary search over the primitive offsets
+        size_t lo = 0, hi = a.n_pairs - 1;
+        while (lo < hi)
+        {
+            size_t mid = (lo + hi + 1) / 2;
+            if (a.pofs[mid] <= ip)
+                lo = mid;
+            else
+                hi = mid - 1;
+        }
+        const size_t ipair = lo;
+        const int la = a.la, lb = a.lb, lab = la + lb;
+        const int sa = nsph(la), sb = nsph(lb), hab = nherm(lab), sab = sa * sb;
+        const double ea = a.exps[2 * ip], eb = a.exps[2 * ip + 1];
+        const double dadb = a.coeffs[2 * ip] * a.coeffs[2 * ip + 1];
+        const double *A = a.coords + 6 * ipair, *B = A + 3;
+        const double p = ea + eb, mu = ea * eb / p;
+        double P[3], Ex[3][128], E1x[3][128];
+        for (int k = 0; k < 3; k++)
+        {
+            P[k] = (ea * A[k] + eb * B[k]) / p;
+            const double kab = exp(-mu * (A[k] - B[k]) * (A[k] - B[k]));
+            hermiteE(la, lb, 1.0 / (2 * p), P[k] - A[k], P[k] - B[k], kab, Ex[k]);
+            if (a.E1)
+                hermiteE1(la, lb, ea, eb, A[k] - B[k], Ex[k], E1x[k]);
+        }
+        a.pP[4 * ip + 0] = p;
+        a.pP[4 * ip + 1] = P[0];
+        a.pP[4 * ip + 2] = P[1];
+        a.pP[4 * ip + 3] = P[2];
+        a.ab[2 * ip + 0] = ea;
+        a.ab[2 * ip + 1] = eb;
+        const int nt = lab + 1;
+        auto ex = [&](const double *E, int i, int j, int t) { return E[(i * (lb + 1) + j) * nt + t]; };
+        const double *na = a.norms_a + ipair * sa, *nb = a.norms_b + ipair * sb;
+        double acc[4][84];
+        for (int m = 0; m < sa; m++)
+            for (int n = 0; n < sb; n++)
+            {
+                for (int x = 0; x < 4; x++)
+                    for (int h = 0; h < hab; h++)
+                        acc[x][h] = 0.0;
+                for (int ta = a.sph.ofs[la]; ta < a.sph.ofs[la + 1]; ta++)
+                {
+                    if (a.sph.rc[2 * ta] != m)
+                        continue;
+                    int ca = a.sph.rc[2 * ta + 1];
+                    // Cartesian exponents of index ca in shell la
+                    int ia = 0, ja = 0, ka = 0;
+                    for (int x = la, c = 0; x >= 0; x--)
+                        for (int y = la - x; y >= 0; y--, c++)
+                            if (c == ca)
+                            {
+                                ia = x;
+                                ja = y;
+                                ka = la - x - y;
+                            }
+                    for (int tb = a.sph.ofs[lb]; tb < a.sph.ofs[lb + 1]; tb++)
+                    {
+                        if (a.sph.rc[2 * tb] != n)
+                            continue;
+                        int cb = a.sph.rc[2 * tb + 1];
+                        int ib = 0, jb = 0, kb = 0;
+                        for (int x = lb, c = 0; x >= 0; x--)
+                            for (int y = lb - x; y >= 0; y--, c++)
+                                if (c == cb)
+                                {
+                                    ib = x;
+                                    jb = y;
+                                    kb = lb - x - y;
+                                }
+                        const double w = a.sph.val[ta] * a.sph.val[tb];
+                        for (int t = 0; t <= ia + ib; t++)
+                            for (int u = 0; u <= ja + jb; u++)
+                                for (int v = 0; v <= ka + kb; v++)
+                                {
+                                    const int h = hermIndex(t, u, v);
+                                    const double gx = ex(Ex[0], ia, ib, t), gy = ex(Ex[1], ja, jb, u),
+                                                 gz = ex(Ex[2], ka, kb, v);
+                                    acc[0][h] += w * gx * gy * gz;
+                                    if (a.E1)
+                                    {
+                                        acc[1][h] += w * ex(E1x[0], ia, ib, t) * gy * gz;
+                                        acc[2][h] += w * gx * ex(E1x[1], ja, jb, u) * gz;
+                                        acc[3][h] += w * gx * gy * ex(E1x[2], ka, kb, v);
+                                    }
+                                }
+                    }
+                }
+                const double s = na[m] * nb[n] * dadb;
+                const int mn = m * sb + n;
+                for (int h = 0; h < hab; h++)
+                {
+                    const double v = s * acc[0][h];
+                    a.E[(ip * sab + mn) * hab + h] = v;
+                    a.Et[(ip * hab + h) * sab + mn] = v;
+                    if (a.Ef)
+                    {
+                        a.Ef[(ip * sab + mn) * hab + h] = (float)v;
+                        a.Etf[(ip * hab + h) * sab + mn] = (float)v;
+                    }
+                    if (a.E1)
+                        for (int x = 0; x < 3; x++)
+                        {
+                            const double v1 = s * acc[1 + x][h];
+                            a.E1[((ip * 3 + x) * sab + mn) * hab + h] = v1;
+                            a.E1t[((ip * 3 + x) * hab + h) * sab + mn] = v1;
+                        }
+                }
+            }
+    }
+
+    // eri4 scatter with 8-fold permutational symmetry (src/lible/ints/twoel/eri4.cpp:70-89).
+    __global__ void scatter4Kernel(const double *batches, const uint32_t *list, long long n_tasks,
+                                   const int32_t *bra_info, const int32_t *ket_info, int sa, int sb,
+                                   int sc, int sd, long long n, double *out)
+    {
+        const long long blk = (long long)sa * sb * sc * sd;
+        const long long total = n_tasks * blk;
+        for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; g < total;
+             g += (long long)gridDim.x * blockDim.x)
+        {
+            const long long t = g / blk;
+            int e = (int)(g % blk);
+            const int l = e % sd;
+            e /= sd;
+            const int k = e % sc;
+            e /= sc;
+            const int j = e % sb;
+            const int i = e / sb;
+            const int32_t *bi = bra_info + 8 * list[2 * t];
+            const int32_t *ki = ket_info + 8 * list[2 * t + 1];
+            const long long m = bi[0] + i, nu = bi[1] + j, ka = ki[0] + k, ta = ki[1] + l;
+            const double v = batches[g];
+            out[((m * n + nu) * n + ka) * n + ta] = v;
+            out[((m * n + nu) * n + ta) * n + ka] = v;
+            out[((nu * n + m) * n + ka) * n + ta] = v;
+            out[((nu * n + m) * n + ta) * n + ka] = v;
+            out[((ka * n + ta) * n + m) * n + nu] = v;
+            out[((ka * n + ta) * n + nu) * n + m] = v;
+            out[((ta * n + ka) * n + m) * n + nu] = v;
+            out[((ta * n + ka) * n + nu) * n + m] = v;
+        }
+    }
+
+    // eri3 scatter: (mn|P) and (nm|P) (src/lible/ints/twoel/eri3.cpp:30-43).  Batches are stored in
+    // the caller orientation [S_a][S_b][S_P].
+    __global__ void scatter3Kernel(const double *batches, const uint32_t *list, long long n_tasks,
+                                   const int32_t *main_info, const int32_t *aux_info, int swap, int sa,
+                                   int sb, int sc, long long n, long long naux, double *out)
+    {
+        const long long blk = (long long)sa * sb * sc;
+        const long long total = n_tasks * blk;
+        for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; g < total;
+             g += (long long)gridDim.x * blockDim.x)
+        {
+            const long long t = g / blk;
+            int e = (int)(g % blk);
+            const int k = e % sc;
+            e /= sc;
+            const int j = e % sb;
+            const int i = e / sb;
+            const uint32_t im = swap ? list[2 * t + 1] : list[2 * t];
+            const uint32_t ix = swap ? list[2 * t] : list[2 * t + 1];
+            const int32_t *mi = main_info + 8 * im;
+            const int32_t *xi = aux_info + 8 * ix;
+            const long long m = mi[0] + i, nu = mi[1] + j, P = xi[0] + k;
+            out[(m * n + nu) * naux + P] = batches[g];
+            out[(nu * n + m) * naux + P] = batches[g];
+        }
+    }
+
+    // eri2 scatter (src/lible/ints/twoel/eri2.cpp:61-66); batches [S_a][S_b] in caller order.
+    __global__ void scatter2Kernel(const double *batches, const uint32_t *list, long long n_tasks,
+                                   const int32_t *a_info, const int32_t *b_info, int swap, int sa, int sb,
+                                   long long naux, double *out)
+    {
+        const long long blk = (long long)sa * sb;
+        const long long total = n_tasks * blk;
+        for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; g < total;
+             g += (long long)gridDim.x * blockDim.x)
+        {
+            const long long t = g / blk;
+            const int e = (int)(g % blk);
+            const int j = e % sb, i = e / sb;
+            const uint32_t ia = swap ? list[2 * t + 1] : list[2 * t];
+            const uint32_t ibb = swap ? list[2 * t] : list[2 * t + 1];
+            const long long P = a_info[8 * ia] + i, Q = b_info[8 * ibb] + j;
+            out[P * naux + Q] = batches[g];
+            out[Q * naux + P] = batches[g];
+        }
+    }
+
+    // X = A + A^T for the unsymmetrised J / K accumulators (in place, n x n).
+    __global__ void symmetrizeKernel(double *A, long long n)
+    {
+        for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; g < n * n;
+             g += (long long)gridDim.x * blockDim.x)
+        {
+            const long long r = g / n, c = g % n;
+            if (c > r)
+                continue;
+            const double v = A[r * n + c] + A[c * n + r];
+            A[r * n + c] = v;
+            A[c * n + r] = v;
+        }
+    }
+
+    // Reorders D1 batches from the internal orientation to the caller's, selecting the caller's
+    // derivative blocks: out[t][slot(c)*3 + x][caller element] = in[t][c*3 + x][internal element].
+    __global__ void reorderD1Kernel(const double *in, long long n_tasks, int sa, int sb, int sc, int sd,
+                                    int flags, int4 slot, int nblk_out, double *out)
+    {
+        const long long blk = (long long)sa * sb * sc * sd;
+        const long long total = n_tasks * 12 * blk;
+        for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; g < total;
+             g += (long long)gridDim.x * blockDim.x)
+        {
+            const long long t = g / (12 * blk);
+            const int bl = (int)((g / blk) % 12);
+            int e = (int)(g % blk);
+            const int centre = bl / 3, x = bl % 3;
+            const int s = centre == 0 ? slot.x : centre == 1 ? slot.y : centre == 2 ? slot.z : slot.w;
+            if (s < 0)
+                continue;
+            const int tt = e % sd;
+            e /= sd;
+            const int k = e % sc;
+            e /= sc;
+            const int nn = e % sb;
+            const int m = e / sb;
+            int b0 = m, b1 = nn, k0 = k, k1 = tt, db0 = sa, db1 = sb, dk0 = sc, dk1 = sd;
+            if (flags & 1)
+            {
+                b0 = nn; b1 = m; db0 = sb; db1 = sa;
+            }
+            if (flags & 2)
+            {
+                k0 = tt; k1 = k; dk0 = sd; dk1 = sc;
+            }
+            const long long d = (flags & 4) ? (((long long)k0 * dk1 + k1) * db0 + b0) * db1 + b1
+                                            : (((long long)b0 * db1 + b1) * dk0 + k0) * dk1 + k1;
+            out[(t * nblk_out + s * 3 + x) * blk + d] = in[g];
+        }
+    }
+
+    // ------------------------------------------------------------------------------------------
+    // Engine
+
+    void cudaCheck(cudaError_t e, const char *what)
+    {
+        if (e != cudaSuccess)
+            throw EngineError(kStatusCuda, std::string(what) + ": " + cudaGetErrorString(e));
+    }
+
+    template <class T>
+    static T *devAlloc(size_t n)
+    {
+        T *p = nullptr;
+        if (n == 0)
+            n = 1;
+        cudaCheck(cudaMalloc(&p, n * sizeof(T)), "cudaMalloc");
+        return p;
+    }
+
+    template <class T>
+    static T *devUpload(const std::vector<T> &v, cudaStream_t s)
+    {
+        T *p = devAlloc<T>(v.size());
+        if (!v.empty())
+            cudaCheck(cudaMemcpyAsync(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, s), "upload");
+        return p;
+    }
+
+    Engine::Engine(int device) : device_(device)
+    {
+        cudaCheck(cudaSetDevice(device), "cudaSetDevice");
+        cudaCheck(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate");
+        cudaDeviceProp prop;
+        cudaCheck(cudaGetDeviceProperties(&prop, device), "cudaGetDeviceProperties");
+        num_sms_ = prop.multiProcessorCount;
+        boys_ = devUpload(boysGrid(), stream_);
+        std::vector<int> rc;
+        std::vector<double> val;
+        sph_ofs_.assign(kMaxL + 2, 0);
+        for (int l = 0; l <= kMaxL; l++)
+        {
+            sph_ofs_[l] = (int)val.size();
+            for (const auto &t : sphericalTrafo(l))
+            {
+                rc.push_back(t.row);
+                rc.push_back(t.cart);
+                val.push_back(t.val);
+            }
+        }
+        sph_ofs_[kMaxL + 1] = (int)val.size();
+        sph_rc_ = devUpload(rc, stream_);
+        sph_val_ = devUpload(val, stream_);
+        cudaCheck(cudaStreamSynchronize(stream_), "init");
+    }
+
+    Engine::~Engine()
+    {
+        cudaSetDevice(device_);
+        clearStructure();
+        for (void *p : persistent_)
+            cudaFree(p);
+        cudaFree(boys_);
+        cudaFree(sph_rc_);
+        cudaFree(sph_val_);
+        cudaStreamDestroy(stream_);
+    }
+
+    void Engine::freeSet(ClassSet &cs)
+    {
+        for (auto &d : cs.dev)
+            for (void *p : {(void *)d.pP, (void *)d.ab, (void *)d.pofs, (void *)d.info, (void *)d.coords,
+                            (void *)d.E, (void *)d.Et, (void *)d.Ef, (void *)d.Etf, (void *)d.E1,
+                            (void *)d.E1t, (void *)d.Q})
+                cudaFree(p);
+        cs = ClassSet();
+    }
+
+    void Engine::clearStructure()
+    {
+        freeSet(symm_);
+        freeSet(nosymm_);
+        freeSet(aux_);
+        for (auto &kv : plans_)
+            freePlan(kv.second);
+        plans_.clear();
+        shells_.clear();
+        aux_shells_.clear();
+        nao_ = naux_ = 0;
+        n_atoms_ = 0;
+        has_structure_ = false;
+    }
+
+    void Engine::setStructure(const std::vector<BasisAtom> &main, const std::vector<BasisAtom> *aux,
+                              const std::vector<std::array<double, 3>> &xyz_bohr)
+    {
+        clearStructure();
+        shells_ = constructShells(main, xyz_bohr);
+        nao_ = 0;
+        max_l_ = 0;
+        for (const auto &s : shells_)
+        {
+            nao_ += nsph(s.l);
+            max_l_ = std::max(max_l_, s.l);
+        }
+        if (max_l_ > 3)
+            throw EngineError(kStatusUnsupported, "main basis shells with l > 3 are not supported");
+        n_atoms_ = (int)xyz_bohr.size();
+        has_aux_ = aux != nullptr;
+        if (aux)
+        {
+            aux_shells_ = constructShells(*aux, xyz_bohr);
+            naux_ = 0;
+            max_l_aux_ = 0;
+            for (const auto &s : aux_shells_)
+            {
+                naux_ += nsph(s.l);
+                max_l_aux_ = std::max(max_l_aux_, s.l);
+            }
+        }
+        has_structure_ = true;
+    }
+
+    std::vector<Shell> Engine::shellsL(const std::vector<Shell> &all, int l)
+    {
+        std::vector<Shell> out;
+        for (const auto &s : all)
+            if (s.l == l)
+                out.push_back(s);
+        return out;
+    }
+
+    void Engine::uploadClass(const PairClass &pc, bool with_d1, bool with_f32, DevPairClass &d)
+    {
+        d.la = pc.la;
+        d.lb = pc.lb;
+        d.single = pc.single;
+        d.n_pairs = pc.n_pairs;
+        d.n_ppairs = pc.n_ppairs;
+        std::vector<int32_t> info(8 * pc.n_pairs, 0);
+        for (size_t i = 0; i < pc.n_pairs; i++)
+        {
+            info[8 * i + 0] = pc.ao_a[i];
+            info[8 * i + 1] = pc.ao_b[i];
+            info[8 * i + 2] = pc.atom_a[i];
+            info[8 * i + 3] = pc.atom_b[i];
+            info[8 * i + 4] = pc.shell_a[i];
+            info[8 * i + 5] = pc.shell_b[i];
+        }
+        d.info = devUpload(info, stream_);
+        d.pofs = devUpload(pc.pofs, stream_);
+        d.coords = devUpload(pc.coords, stream_);
+        const size_t np = std::max<size_t>(pc.n_ppairs, 1);
+        const int sab = nsph(pc.la) * nsph(pc.lb), hab = nherm(pc.la + pc.lb);
+        d.pP = devAlloc<double>(4 * np);
+        d.ab = devAlloc<double>(2 * np);
+        d.E = devAlloc<double>(np * sab * hab);
+        d.Et = devAlloc<double>(np * sab * hab);
+        if (with_f32)
+        {
+            d.Ef = devAlloc<float>(np * sab * hab);
+            d.Etf = devAlloc<float>(np * sab * hab);
+        }
+        if (with_d1)
+        {
+            d.E1 = devAlloc<double>(3 * np * sab * hab);
+            d.E1t = devAlloc<double>(3 * np * sab * hab);
+        }
+        if (pc.n_ppairs == 0)
+            return;
+        double *exps = devUpload(pc.exps, stream_);
+        double *coeffs = devUpload(pc.coeffs, stream_);
+        double *na = devUpload(pc.norms_a, stream_);
+        double *nb = devUpload(pc.norms_b, stream_);
+        EArgs ea{};
+        ea.la = pc.la;
+        ea.lb = pc.lb;
+        ea.n_pairs = pc.n_pairs;
+        ea.n_ppairs = pc.n_ppairs;
+        ea.exps = exps;
+        ea.coeffs = coeffs;
+        ea.coords = d.coords;
+        ea.norms_a = na;
+        ea.norms_b = nb;
+        ea.pofs = d.pofs;
+        ea.sph.rc = sph_rc_;
+        ea.sph.val = sph_val_;
+        for (int l = 0; l <= kMaxL + 1; l++)
+            ea.sph.ofs[l] = sph_ofs_[l];
+        ea.pP = d.pP;
+        ea.ab = d.ab;
+        ea.E = d.E;
+        ea.Et = d.Et;
+        ea.Ef = d.Ef;
+        ea.Etf = d.Etf;
+        ea.E1 = d.E1;
+        ea.E1t = d.E1t;
+        const int bs = 64;
+        ecoeffKernel<<<(unsigned)((pc.n_ppairs + bs - 1) / bs), bs, 0, stream_>>>(ea);
+        cudaCheck(cudaGetLastError(), "ecoeffKernel");
+        cudaCheck(cudaStreamSynchronize(stream_), "ecoeffKernel");
+        cudaFree(exps);
+        cudaFree(coeffs);
+        cudaFree(na);
+        cudaFree(nb);
+    }
+
+    // Reference class order: la = 0..lmax, lb = 0..la (symmetric) or lb = 0..lmax (no symmetry)
+    // (src/lible/ints/utils.cpp:49-73, shell_pair_data.cpp:294-309).
+    Engine::ClassSet &Engine::mainSet(bool use_symm)
+    {
+        requireStructure();
+        ClassSet &cs = use_symm ? symm_ : nosymm_;
+        if (!cs.host.empty() || cs.built)
+            return cs;
+        for (int la = 0; la <= max_l_; la++)
+            for (int lb = 0; lb <= (use_symm ? la : max_l_); lb++)
+            {
+                PairClass pc = buildPairClass(use_symm, la, lb, shellsL(shells_, la), shellsL(shells_, lb));
+                bool swapped = false;
+                if (lb > la)
+                {
+                    // store with the higher angular momentum first; the caller's orientation is
+                    // restored by the epilogue
+                    swapped = true;
+                    for (size_t i = 0; i < pc.n_ppairs; i++)
+                    {
+                        std::swap(pc.exps[2 * i], pc.exps[2 * i + 1]);
+                        std::swap(pc.coeffs[2 * i], pc.coeffs[2 * i + 1]);
+                    }
+                    for (size_t i = 0; i < pc.n_pairs; i++)
+                        for (int k = 0; k < 3; k++)
+                            std::swap(pc.coords[6 * i + k], pc.coords[6 * i + 3 + k]);
+                    std::swap(pc.ao_a, pc.ao_b);
+                    std::swap(pc.atom_a, pc.atom_b);
+                    std::swap(pc.shell_a, pc.shell_b);
+                    std::swap(pc.norms_a, pc.norms_b);
+                    std::swap(pc.la, pc.lb);
+                }
+                cs.host.push_back(std::move(pc));
+                cs.swapped.push_back(swapped);
+                cs.req_l.push_back({la, lb});
+            }
+        cs.dev.resize(cs.host.size());
+        for (size_t c = 0; c < cs.host.size(); c++)
+            uploadClass(cs.host[c], true, use_symm && max_l_ <= 2, cs.dev[c]);
+        cs.built = true;
+        return cs;
+    }
+
+    Engine::ClassSet &Engine::auxSet()
+    {
+        requireStructure();
+        if (!has_aux_)
+            throw EngineError(kStatusNoAux, "RI approximation is not enabled (no auxiliary basis)");
+        if (aux_.built)
+            return aux_;
+        for (int l = 0; l <= max_l_aux_; l++)
+        {
+            aux_.host.push_back(buildSingleClass(l, shellsL(aux_shells_, l)));
+            aux_.swapped.push_back(false);
+            aux_.req_l.push_back({l, 0});
+        }
+        aux_.dev.resize(aux_.host.size());
+        for (size_t c = 0; c < aux_.host.size(); c++)
+            uploadClass(aux_.host[c], true, false, aux_.dev[c]);
+        aux_.built = true;
+        return aux_;
+    }
+
+    void Engine::requireStructure() const
+    {
+        if (!has_structure_)
+            throw EngineError(kStatusNoStructure, "no structure has been set");
+    }
+
+    PairView Engine::view(const DevPairClass &d)
+    {
+        return PairView{d.pP, d.ab, d.pofs, d.info, d.E, d.Et, d.Ef, d.Etf, d.E1, d.E1t};
+    }
+
+    // Runs one class pair over an explicit task list in store mode.  `bra` and `ket` are in the
+    // caller's orientation; the class is launched with the larger pair type in the bra.
+    void Engine::runStore(const DevPairClass &bra, bool bra_swapped, const DevPairClass &ket, bool ket_swapped,
+                          const uint32_t *d_list, long long n, bool d1, double *d_out, bool same_class)
+    {
+        if (n == 0)
+            return;
+        const int tb = pairType(bra.la, bra.lb), tk = pairType(ket.la, ket.lb);
+        const bool swap = tb < tk;
+        QuartetArgs a{};
+        a.bra = view(swap ? ket : bra);
+        a.ket = view(swap ? bra : ket);
+        a.boys = boys_;
+        a.n_tasks = n;
+        a.same_class = same_class ? 1 : 0;
+        a.flags = (bra_swapped ? 1 : 0) | (ket_swapped ? 2 : 0) | (swap ? 4 : 0);
+        if (swap)
+            a.flags = (ket_swapped ? 1 : 0) | (bra_swapped ? 2 : 0) | 4;
+        uint32_t *list = const_cast<uint32_t *>(d_list);
+        if (swap)
+        {
+            // swap the (bra, ket) columns of the task list
+            std::vector<uint32_t> h(2 * n);
+            cudaCheck(cudaMemcpyAsync(h.data(), d_list, 2 * n * sizeof(uint32_t), cudaMemcpyDeviceToHost, stream_), "list");
+            cudaCheck(cudaStreamSynchronize(stream_), "list");
+            for (long long i = 0; i < n; i++)
+                std::swap(h[2 * i], h[2 * i + 1]);
+            list = devUpload(h, stream_);
+        }
+        a.list = list;
+        if (!d1)
+        {
+            a.mode = kStore;
+            a.out = d_out;
+            LaunchFn fn = lookupFwd64(swap ? tk : tb, swap ? tb : tk);
+            if (!fn)
+                throw EngineError(kStatusUnsupported, "quartet class not instantiated");
+            cudaCheck(fn(a, stream_, num_sms_), "eri kernel");
+        }
+        else
+        {
+            const long long blk = (long long)nsph(bra.la) * nsph(bra.lb) * nsph(ket.la) * nsph(ket.lb);
+            double *tmp = devAlloc<double>(n * 12 * blk);
+            a.mode = kD1Store;
+            a.out = tmp;
+            const int flags = a.flags;
+            a.flags = 0;
+            LaunchFn fn = lookupD1(swap ? tk : tb, swap ? tb : tk);
+            if (!fn)
+                throw EngineError(kStatusUnsupported, "quartet class not instantiated");
+            cudaCheck(fn(a, stream_, num_sms_), "eri d1 kernel");
+            // caller slots of the internal centres (A, B | C, D)
+            int s[4] = {0, 1, 2, 3};
+            if (flags & 1)
+                std::swap(s[0], s[1]);
+            if (flags & 2)
+                std::swap(s[2], s[3]);
+            if (flags & 4)
+                for (int &x : s)
+                    x = (x + 2) % 4;
+            // drop the derivative blocks of auxiliary dummy centres; compact the remaining slots
+            const DevPairClass &ib = swap ? ket : bra, &ik = swap ? bra : ket;
+            bool dummy[4] = {false, ib.single, false, ik.single};
+            int callerDummy[4] = {0, 0, 0, 0};
+            for (int c = 0; c < 4; c++)
+                if (dummy[c])
+                    callerDummy[s[c]] = 1;
+            int remap[4], k = 0;
+            for (int c = 0; c < 4; c++)
+                remap[c] = callerDummy[c] ? -1 : k++;
+            int4 slot = make_int4(remap[s[0]], remap[s[1]], remap[s[2]], remap[s[3]]);
+            if (ib.single)
+                slot.y = -1;
+            if (ik.single)
+                slot.w = -1;
+            const int nb = 3 * k;
+            const auto &sb = swap ? ket : bra;
+            const auto &sk = swap ? bra : ket;
+            reorderD1Kernel<<<std::max(1, num_sms_ * 8), 256, 0, stream_>>>(
+                tmp, n, nsph(sb.la), nsph(sb.lb), nsph(sk.la), nsph(sk.lb), flags, slot, nb, d_out);
+            cudaCheck(cudaGetLastError(), "reorder");
+            cudaCheck(cudaStreamSynchronize(stream_), "reorder");
+            cudaFree(tmp);
+        }
+        if (swap)
+        {
+            cudaCheck(cudaStreamSynchronize(stream_), "store");
+            cudaFree(list);
+        }
+    }
+
+    // ------------------------------------------------------------------------------------------
+    // Full tensors
+
+    void Engine::eri4(double *out_dev)
+    {
+        ClassSet &cs = mainSet(true);
+        const long long n = (long long)nao_;
+        cudaCheck(cudaMemsetAsync(out_dev, 0, (size_t)n * n * n * n * sizeof(double), stream_), "memset");
+        for (size_t cb = 0; cb < cs.dev.size(); cb++)
+            for (size_t ck = 0; ck <= cb; ck++)
+            {
+                const auto &B = cs.dev[cb], &K = cs.dev[ck];
+                std::vector<uint32_t> list;
+                for (uint32_t i = 0; i < B.n_pairs; i++)
+                    for (uint32_t j = 0; j < (cb == ck ? i + 1 : K.n_pairs); j++)
+                    {
+                        list.push_back(i);
+                        list.push_back(j);
+                    }
+                const long long nt = (long long)list.size() / 2;
+                if (nt == 0)
+                    continue;
+                uint32_t *dl = devUpload(list, stream_);
+                const int sa = nsph(B.la), sb = nsph(B.lb), sc = nsph(K.la), sd = nsph(K.lb);
+                double *tmp = devAlloc<double>((size_t)nt * sa * sb * sc * sd);
+                runStore(B, false, K, false, dl, nt, false, tmp, cb == ck);
+                scatter4Kernel<<<num_sms_ * 8, 256, 0, stream_>>>(tmp, dl, nt, B.info, K.info, sa, sb, sc, sd, n,
+                                                                   out_dev);
+                cudaCheck(cudaGetLastError(), "scatter4");
+                cudaCheck(cudaStreamSynchronize(stream_), "eri4");
+                cudaFree(tmp);
+                cudaFree(dl);
+            }
+    }
+
+    // Diagonal batches (ab|ab) of every pair of every class (the eri4Diagonal analogue).
+    std::vector<std::vector<double>> Engine::diagonalBatches(ClassSet &cs)
+    {
+        std::vector<std::vector<double>> out(cs.dev.size());
+        for (size_t c = 0; c < cs.dev.size(); c++)
+        {
+            const auto &B = cs.dev[c];
+            if (B.n_pairs == 0)
+                continue;
+            std::vector<uint32_t> list;
+            for (uint32_t i = 0; i < B.n_pairs; i++)
+            {
+                list.push_back(i);
+                list.push_back(i);
+            }
+            uint32_t *dl = devUpload(list, stream_);
+            const size_t sab = (size_t)nsph(B.la) * nsph(B.lb);
+            double *tmp = devAlloc<double>(B.n_pairs * sab * sab);
+            runStore(B, false, B, false, dl, (long long)B.n_pairs, false, tmp, true);
+            out[c].resize(B.n_pairs * sab * sab);
+            cudaCheck(cudaMemcpyAsync(out[c].data(), tmp, out[c].size() * sizeof(double), cudaMemcpyDeviceToHost,
+                                      stream_), "diag");
+            cudaCheck(cudaStreamSynchronize(stream_), "diag");
+            cudaFree(tmp);
+            cudaFree(dl);
+        }
+        return out;
+    }
+
+    void Engine::eri4Diagonal(double *out_host)
+    {
+        ClassSet &cs = mainSet(true);
+        auto batches = diagonalBatches(cs);
+        const size_t n = nao_;
+        std::fill(out_host, out_host + n * n, 0.0);
+        for (size_t c = 0; c < cs.host.size(); c++)
+        {
+            const auto &pc = cs.host[c];
+            const int sa = nsph(pc.la), sb = nsph(pc.lb), sab = sa * sb;
+            for (size_t i = 0; i < pc.n_pairs; i++)
+                for (int x = 0; x < sa; x++)
+                    for (int y = 0; y < sb; y++)
+                    {
+                        const int e = x * sb + y;
+                        const double v = batches[c][(i * sab + e) * sab + e];
+                        const size_t mu = pc.ao_a[i] + x, nu = pc.ao_b[i] + y;
+                        out_host[mu * n + nu] = v;
+                        out_host[nu * n + mu] = v;
+                    }
+        }
+    }
+
+    void Engine::eri3(double *out_dev)
+    {
+        ClassSet &ms = mainSet(true);
+        ClassSet &xs = auxSet();
+        const long long n = (long long)nao_, na = (long long)naux_;
+        cudaCheck(cudaMemsetAsync(out_dev, 0, (size_t)n * n * na * sizeof(double), stream_), "memset");
+        for (size_t cb = 0; cb < ms.dev.size(); cb++)
+            for (size_t cx = 0; cx < xs.dev.size(); cx++)
+            {
+                const auto &B = ms.dev[cb], &X = xs.dev[cx];
+                std::vector<uint32_t> list;
+                for (uint32_t i = 0; i < B.n_pairs; i++)
+                    for (uint32_t j = 0; j < X.n_pairs; j++)
+                    {
+                        list.push_back(i);
+                        list.push_back(j);
+                    }
+                const long long nt = (long long)list.size() / 2;
+                if (nt == 0)
+                    continue;
+                uint32_t *dl = devUpload(list, stream_);
+                const int sa = nsph(B.la), sb = nsph(B.lb), sc = nsph(X.la);
+                double *tmp = devAlloc<double>((size_t)nt * sa * sb * sc);
+                runStore(B, false, X, false, dl, nt, false, tmp, false);
+                scatter3Kernel<<<num_sms_ * 8, 256, 0, stream_>>>(tmp, dl, nt, B.info, X.info, 0, sa, sb, sc, n, na,
+                                                                   out_dev);
+                cudaCheck(cudaGetLastError(), "scatter3");
+                cudaCheck(cudaStreamSynchronize(stream_), "eri3");
+                cudaFree(tmp);
+                cudaFree(dl);
+            }
+    }
+
+    void Engine::eri2(double *out_dev)
+    {
+        ClassSet &xs = auxSet();
+        const long long na = (long long)naux_;
+        cudaCheck(cudaMemsetAsync(out_dev, 0, (size_t)na * na * sizeof(double), stream_), "memset");
+        for (size_t ca = 0; ca < xs.dev.size(); ca++)
+            for (size_t cb = 0; cb <= ca; cb++)
+            {
+                const auto &A = xs.dev[ca], &B = xs.dev[cb];
+                std::vector<uint32_t> list;
+                for (uint32_t i = 0; i < A.n_pairs; i++)
+                    for (uint32_t j = 0; j < (ca == cb ? i + 1 : B.n_pairs); j++)
+                    {
+                        list.push_back(i);
+                        list.push_back(j);
+                    }
+                const long long nt = (long long)list.size() / 2;
+                if (nt == 0)
+                    continue;
+                uint32_t *dl = devUpload(list, stream_);
+                const int sa = nsph(A.la), sb = nsph(B.la);
+                double *tmp = devAlloc<double>((size_t)nt * sa * sb);
+                runStore(A, false, B, false, dl, nt, false, tmp, ca == cb);
+                scatter2Kernel<<<num_sms_ * 8, 256, 0, stream_>>>(tmp, dl, nt, A.info, B.info, 0, sa, sb, na, out_dev);
+                cudaCheck(cudaGetLastError(), "scatter2");
+                cudaCheck(cudaStreamSynchronize(stream_), "eri2");
+                cudaFree(tmp);
+                cudaFree(dl);
+            }
+    }
+
+    void Engine::eri2Diagonal(double *out_host)
+    {
+        ClassSet &xs = auxSet();
+        auto batches = diagonalBatches(xs);
+        std::fill(out_host, out_host + naux_, 0.0);
+        for (size_t c = 0; c < xs.host.size(); c++)
+        {
+            const auto &pc = xs.host[c];
+            const int s = nsph(pc.la);
+            for (size_t i = 0; i < pc.n_pairs; i++)
+                for (int x = 0; x < s; x++)
+                    out_host[pc.ao_a[i] + x] = batches[c][(i * s + x) * s + x];
+        }
+    }
+
+    // ------------------------------------------------------------------------------------------
+    // Kernel-API batches: the caller's classes follow shellPairData(use_symm) / shellDataAux.
+
+    void Engine::eri4Batch(bool use_symm, int cab, int ccd, long long n, const uint32_t *pairs_host, double *out_dev,
+                           bool d1)
+    {
+        ClassSet &cs = mainSet(use_symm);
+        if (cab < 0 || ccd < 0 || cab >= (int)cs.dev.size() || ccd >= (int)cs.dev.size())
+            throw EngineError(kStatusInvalid, "class index out of range");
+        const auto &B = cs.dev[cab], &K = cs.dev[ccd];
+        for (long long i = 0; i < n; i++)
+            if (pairs_host[2 * i] >= B.n_pairs || pairs_host[2 * i + 1] >= K.n_pairs)
+                throw EngineError(kStatusInvalid, "pair index out of range");
+        std::vector<uint32_t> list(pairs_host, pairs_host + 2 * n);
+        uint32_t *dl = devUpload(list, stream_);
+        runStore(B, cs.swapped[cab], K, cs.swapped[ccd], dl, n, d1, out_dev, use_symm && cab == ccd);
+        cudaCheck(cudaStreamSynchronize(stream_), "batch");
+        cudaFree(dl);
+    }
+
+    void Engine::eri3Batch(bool use_symm, int cab, int cx, long long n, const uint32_t *idx_host, double *out_dev,
+                           bool d1)
+    {
+        ClassSet &cs = mainSet(use_symm);
+        ClassSet &xs = auxSet();
+        if (cab < 0 || cx < 0 || cab >= (int)cs.dev.size() || cx >= (int)xs.dev.size())
+            throw EngineError(kStatusInvalid, "class index out of range");
+        const auto &B = cs.dev[cab], &X = xs.dev[cx];
+        for (long long i = 0; i < n; i++)
+            if (idx_host[2 * i] >= B.n_pairs || idx_host[2 * i + 1] >= X.n_pairs)
+                throw EngineError(kStatusInvalid, "index out of range");
+        std::vector<uint32_t> list(idx_host, idx_host + 2 * n);
+        uint32_t *dl = devUpload(list, stream_);
+        runStore(B, cs.swapped[cab], X, false, dl, n, d1, out_dev, false);
+        cudaCheck(cudaStreamSynchronize(stream_), "batch");
+        cudaFree(dl);
+    }
+
+    void Engine::eri2Batch(int ca, int cb, long long n, const uint32_t *idx_host, double *out_dev, bool d1)
+    {
+        ClassSet &xs = auxSet();
+        if (ca < 0 || cb < 0 || ca >= (int)xs.dev.size() || cb >= (int)xs.dev.size())
+            throw EngineError(kStatusInvalid, "class index out of range");
+        const auto &A = xs.dev[ca], &B = xs.dev[cb];
+        for (long long i = 0; i < n; i++)
+            if (idx_host[2 * i] >= A.n_pairs || idx_host[2 * i + 1] >= B.n_pairs)
+                throw EngineError(kStatusInvalid, "index out of range");
+        std::vector<uint32_t> list(idx_host, idx_host + 2 * n);
+        uint32_t *dl = devUpload(list, stream_);
+        runStore(A, false, B, false, dl, n, d1, out_dev, false);
+        cudaCheck(cudaStreamSynchronize(stream_), "batch");
+        cudaFree(dl);
+    }
+
+    // ------------------------------------------------------------------------------------------
+    // Schwarz screening and the direct J/K build
+
+    void Engine::ensureSchwarz(ClassSet &cs)
+    {
+        if (cs.schwarz_done)
+            return;
+        auto batches = diagonalBatches(cs);
+        for (size_t c = 0; c < cs.dev.size(); c++)
+        {
+            auto &d = cs.dev[c];
+            const int sab = nsph(d.la) * nsph(d.lb);
+            d.Qh.assign(d.n_pairs, 0.0);
+            for (size_t i = 0; i < d.n_pairs; i++)
+            {
+                double m = 0.0;
+                for (int e = 0; e < sab; e++)
+                    m = std::max(m, std::fabs(batches[c][(i * sab + e) * sab + e]));
+                d.Qh[i] = std::sqrt(m);
+            }
+            d.Q = devUpload(d.Qh, stream_);
+        }
+        cudaCheck(cudaStreamSynchronize(stream_), "schwarz");
+        cs.schwarz_done = true;
+    }
+
+    void Engine::freePlan(JKPlan &p)
+    {
+        for (auto &cp : p.pairs)
+            for (void *x : {(void *)cp.prefix64, (void *)cp.prefix32, (void *)cp.begin64, (void *)cp.begin32})
+                cudaFree(x);
+        for (void *x : p.orders)
+            cudaFree(x);
+        p = JKPlan();
+    }
+
+    // Unique quartets (ab|cd), cd <= ab, kept iff Q_ab Q_cd >= thr.  Pairs of each class are sorted
+    // by decreasing Q, so the surviving kets of bra position i are a prefix of the ket order and
+    // quartet t of a class pair decodes by a binary search over per-bra prefix sums.  With mixed
+    // precision the prefix is split at Q_ab Q_cd = thr32: FP64 below index n64, FP32 after.
+    Engine::JKPlan &Engine::jkPlan(double thr, double thr32, bool mixed)
+    {
+        ClassSet &cs = mainSet(true);
+        ensureSchwarz(cs);
+        char key[128];
+        snprintf(key, sizeof(key), "%.6e/%.6e/%d", thr, thr32, mixed ? 1 : 0);
+        auto it = plans_.find(key);
+        if (it != plans_.end())
+            return it->second;
+        JKPlan plan;
+        const size_t nc = cs.dev.size();
+        std::vector<std::vector<uint32_t>> order(nc);
+        std::vector<std::vector<double>> qs(nc);
+        for (size_t c = 0; c < nc; c++)
+        {
+            const auto &Q = cs.dev[c].Qh;
+            order[c].resize(Q.size());
+            std::iota(order[c].begin(), order[c].end(), 0u);
+            std::stable_sort(order[c].begin(), order[c].end(), [&](uint32_t x, uint32_t y) { return Q[x] > Q[y]; });
+            qs[c].resize(Q.size());
+            for (size_t i = 0; i < Q.size(); i++)
+                qs[c][i] = Q[order[c][i]];
+            uint32_t *d = devUpload(order[c], stream_);
+            plan.orders.push_back(d);
+        }
+        // primitive-pair counts in sorted order, and their prefix sums
+        std::vector<std::vector<double>> kpre(nc);
+        for (size_t c = 0; c < nc; c++)
+        {
+            kpre[c].assign(order[c].size() + 1, 0.0);
+            for (size_t i = 0; i < order[c].size(); i++)
+            {
+                const uint32_t pi = order[c][i];
+                kpre[c][i + 1] = kpre[c][i] + (cs.host[c].pofs[pi + 1] - cs.host[c].pofs[pi]);
+            }
+        }
+        auto countAbove = [](const std::vector<double> &q, double bound) -> uint32_t {
+            // number of entries with q >= bound (q sorted descending)
+            return (uint32_t)(std::upper_bound(q.begin(), q.end(), bound, [](double b, double v) { return b > v; }) -
+                              q.begin());
+        };
+        for (size_t cb = 0; cb < nc; cb++)
+            for (size_t ck = 0; ck <= cb; ck++)
+            {
+                JKClassPair cp;
+                cp.cb = (int)cb;
+                cp.ck = (int)ck;
+                const size_t nb = qs[cb].size();
+                std::vector<unsigned long long> p64(nb + 1, 0), p32(nb + 1, 0);
+                std::vector<uint32_t> b64(nb, 0), b32(nb, 0);
+                for (size_t i = 0; i < nb; i++)
+                {
+                    const double qi = qs[cb][i];
+                    uint32_t nall = qi > 0 ? countAbove(qs[ck], thr / qi) : 0;
+                    uint32_t n64 = nall;
+                    if (mixed)
+                        n64 = qi > 0 ? std::min(nall, countAbove(qs[ck], thr32 / qi)) : 0;
+                    if (cb == ck)
+                    {
+                        nall = std::min<uint32_t>(nall, (uint32_t)i + 1);
+                        n64 = std::min<uint32_t>(n64, (uint32_t)i + 1);
+                    }
+                    p64[i + 1] = p64[i] + n64;
+                    p32[i + 1] = p32[i] + (nall - n64);
+                    const double ki = kpre[cb][i + 1] - kpre[cb][i];
+                    cp.prim64 += ki * kpre[ck][n64];
+                    cp.prim32 += ki * (kpre[ck][nall] - kpre[ck][n64]);
+                    cp.flops64 += ki * n64;   // bra-side work counted per (bra primitive, ket pair)
+                    cp.flops32 += ki * (nall - n64);
+                    b64[i] = 0;
+                    b32[i] = n64;
+                }
+                cp.n64 = (long long)p64[nb];
+                cp.n32 = (long long)p32[nb];
+                {
+                    const auto &B = cs.host[cb], &K = cs.host[ck];
+                    const int L = B.la + B.lb + K.la + K.lb;
+                    const double hab = nherm(B.la + B.lb), hcd = nherm(K.la + K.lb);
+                    const double sab = nsph(B.la) * nsph(B.lb), scd = nsph(K.la) * nsph(K.lb);
+                    const double per_prim = (20 + 4 * L) + 3.0 * (L + 1) * (L + 2) * (L + 3) * (L + 4) / 24 + hab * hcd +
+                                            2 * hab * hcd * scd;
+                    const double per_bra = 2 * sab * hab * scd;
+                    cp.flops64 = cp.prim64 * per_prim + cp.flops64 * per_bra;
+                    cp.flops32 = cp.prim32 * per_prim + cp.flops32 * per_bra;
+                }
+                cp.n_bra = (int)nb;
+                if (cp.n64 + cp.n32 == 0)
+                    continue;
+                cp.prefix64 = devUpload(p64, stream_);
+                cp.prefix32 = devUpload(p32, stream_);
+                cp.begin64 = devUpload(b64, stream_);
+                cp.begin32 = devUpload(b32, stream_);
+                plan.n_quartets += cp.n64 + cp.n32;
+                plan.n_fp32 += cp.n32;
+                plan.n_prim += cp.prim64 + cp.prim32;
+                plan.flops64 += cp.flops64;
+                plan.flops32 += cp.flops32;
+                plan.pairs.push_back(cp);
+            }
+        // most expensive class pairs first
+        std::stable_sort(plan.pairs.begin(), plan.pairs.end(), [&](const JKClassPair &x, const JKClassPair &y) {
+            auto cost = [&](const JKClassPair &c) {
+                const auto &B = cs.dev[c.cb], &K = cs.dev[c.ck];
+                return (double)(c.n64 + c.n32) * nherm(B.la + B.lb) * nherm(K.la + K.lb) * nsph(K.la) * nsph(K.lb);
+            };
+            return cost(x) > cost(y);
+        });
+        cudaCheck(cudaStreamSynchronize(stream_), "plan");
+        plan.thr = thr;
+        return plans_.emplace(key, std::move(plan)).first->second;
+    }
+
+    void Engine::jk(const double *D_dev, double *J_dev, double *K_dev, const JKOptions &opt, JKStats *stats)
+    {
+        ClassSet &cs = mainSet(true);
+        const bool mixed = opt.precision == 1;
+        if (mixed && max_l_ > 2)
+            throw EngineError(kStatusUnsupported, "mixed precision is instantiated for l <= 2 bases only");
+        JKPlan &plan = jkPlan(opt.schwarz, opt.fp32_threshold, mixed);
+        const size_t n = nao_;
+        cudaCheck(cudaMemsetAsync(J_dev, 0, n * n * sizeof(double), stream_), "memset");
+        cudaCheck(cudaMemsetAsync(K_dev, 0, n * n * sizeof(double), stream_), "memset");
+        for (const auto &cp : plan.pairs)
+        {
+            const auto &B = cs.dev[cp.cb], &K = cs.dev[cp.ck];
+            QuartetArgs a{};
+            a.bra = view(B);
+            a.ket = view(K);
+            a.boys = boys_;
+            a.list = nullptr;
+            a.bra_order = plan.orders[cp.cb];
+            a.ket_order = plan.orders[cp.ck];
+            a.n_bra = cp.n_bra;
+            a.same_class = cp.cb == cp.ck;
+            a.mode = kJK;
+            a.D = D_dev;
+            a.J = J_dev;
+            a.K = K_dev;
+            a.nao = (int)n;
+            const int tb = pairType(B.la, B.lb), tk = pairType(K.la, K.lb);
+            a.n_tasks = cp.n64;
+            a.prefix = cp.prefix64;
+            a.ket_begin = cp.begin64;
+            cudaCheck(lookupFwd64(tb, tk)(a, stream_, num_sms_), "jk kernel");
+            if (cp.n32 > 0)
+            {
+                a.n_tasks = cp.n32;
+                a.prefix = cp.prefix32;
+                a.ket_begin = cp.begin32;
+                cudaCheck(lookupFwd32(tb, tk)(a, stream_, num_sms_), "jk kernel fp32");
+            }
+        }
+        symmetrizeKernel<<<num_sms_ * 4, 256, 0, stream_>>>(J_dev, (long long)n);
+        symmetrizeKernel<<<num_sms_ * 4, 256, 0, stream_>>>(K_dev, (long long)n);
+        cudaCheck(cudaGetLastError(), "symmetrize");
+        if (stats)
+        {
+            stats->n_quartets = plan.n_quartets;
+            stats->n_fp32 = plan.n_fp32;
+            stats->n_launches = 2;
+            for (const auto &cp : plan.pairs)
+                stats->n_launches += 1 + (cp.n32 > 0 ? 1 : 0);
+        }
+    }
+
+    long long Engine::jkLaunchCount(const JKOptions &opt)
+    {
+        JKPlan &plan = jkPlan(opt.schwarz, opt.fp32_threshold, opt.precision == 1);
+        long long c = 2;
+        for (const auto &cp : plan.pairs)
+            c += 1 + (cp.n32 > 0 ? 1 : 0);
+        return c;
+    }
+
+    JKPlanInfo Engine::jkPlanInfo(const JKOptions &opt)
+    {
+        JKPlan &plan = jkPlan(opt.schwarz, opt.fp32_threshold, opt.precision == 1);
+        JKPlanInfo info;
+        info.n_quartets = plan.n_quartets;
+        info.n_fp32 = plan.n_fp32;
+        info.n_prim_quartets = (long long)plan.n_prim;
+        info.flops_fp64 = plan.flops64;
+        info.flops_fp32 = plan.flops32;
+        info.n_launches = jkLaunchCount(opt);
+        return info;
+    }
+
+    // ------------------------------------------------------------------------------------------
+    // J/K energy gradient (adjoint of the J/K build): dE/dR over all unique quartets.
+
+    void Engine::jkGradient(const double *D_dev, double *grad_dev)
+    {
+        ClassSet &cs = mainSet(true);
+        const size_t n = nao_;
+        cudaCheck(cudaMemsetAsync(grad_dev, 0, 3 * n_atoms_ * sizeof(double), stream_), "memset");
+        for (size_t cb = 0; cb < cs.dev.size(); cb++)
+            for (size_t ck = 0; ck <= cb; ck++)
+            {
+                const auto &B = cs.dev[cb], &K = cs.dev[ck];
+                std::vector<uint32_t> list;
+                for (uint32_t i = 0; i < B.n_pairs; i++)
+                    for (uint32_t j = 0; j < (cb == ck ? i + 1 : K.n_pairs); j++)
+                    {
+                        list.push_back(i);
+                        list.push_back(j);
+                    }
+                const long long nt = (long long)list.size() / 2;
+                if (nt == 0)
+                    continue;
+                uint32_t *dl = devUpload(list, stream_);
+                QuartetArgs a{};
+                a.bra = view(B);
+                a.ket = view(K);
+                a.boys = boys_;
+                a.list = dl;
+                a.n_tasks = nt;
+                a.same_class = cb == ck;
+                a.mode = kD1Grad;
+                a.D = D_dev;
+                a.nao = (int)n;
+                a.grad = grad_dev;
+                cudaCheck(lookupD1(pairType(B.la, B.lb), pairType(K.la, K.lb))(a, stream_, num_sms_), "grad kernel");
+                cudaCheck(cudaStreamSynchronize(stream_), "grad");
+                cudaFree(dl);
+            }
+    }
+
+    // ------------------------------------------------------------------------------------------
+    // RI-J pieces: gamma_P = sum_mn (mn|P) D_mn and J_mn = sum_P (mn|P) d_P.
+
+    void Engine::riContract(const double *D_dev, const double *dcoef_dev, double *gamma_dev, double *J_dev)
+    {
+        ClassSet &ms = mainSet(true);
+        ClassSet &xs = auxSet();
+        const size_t n = nao_;
+        if (gamma_dev)
+            cudaCheck(cudaMemsetAsync(gamma_dev, 0, naux_ * sizeof(double), stream_), "memset");
+        if (J_dev)
+            cudaCheck(cudaMemsetAsync(J_dev, 0, n * n * sizeof(double), stream_), "memset");
+        for (size_t cb = 0; cb < ms.dev.size(); cb++)
+            for (size_t cx = 0; cx < xs.dev.size(); cx++)
+            {
+                const auto &B = ms.dev[cb], &X = xs.dev[cx];
+                if (B.n_pairs == 0 || X.n_pairs == 0)
+                    continue;
+                const int tb = pairType(B.la, B.lb), tx = pairType(X.la, X.lb);
+                const bool swap = tb < tx;
+                std::vector<uint32_t> list;
+                for (uint32_t i = 0; i < B.n_pairs; i++)
+                    for (uint32_t j = 0; j < X.n_pairs; j++)
+                    {
+                        list.push_back(swap ? j : i);
+                        list.push_back(swap ? i : j);
+                    }
+                const long long nt = (long long)list.size() / 2;
+                uint32_t *dl = devUpload(list, stream_);
+                QuartetArgs a{};
+                a.bra = view(swap ? X : B);
+                a.ket = view(swap ? B : X);
+                a.boys = boys_;
+                a.list = dl;
+                a.n_tasks = nt;
+                a.aux_side = swap ? 1 : 0;
+                a.D = D_dev;
+                a.dcoef = dcoef_dev;
+                a.gamma = gamma_dev;
+                a.J = J_dev;
+                a.nao = (int)n;
+                LaunchFn fn = lookupFwd64(swap ? tx : tb, swap ? tb : tx);
+                if (gamma_dev)
+                {
+                    a.mode = kRIGamma;
+                    cudaCheck(fn(a, stream_, num_sms_), "ri gamma");
+                }
+                if (J_dev)
+                {
+                    a.mode = kRIJ;
+                    cudaCheck(fn(a, stream_, num_sms_), "ri J");
+                }
+                cudaCheck(cudaStreamSynchronize(stream_), "ri");
+                cudaFree(dl);
+            }
+        if (J_dev)
+        {
+            symmetrizeKernel<<<num_sms_ * 4, 256, 0, stream_>>>(J_dev, (long long)n);
+            cudaCheck(cudaGetLastError(), "symmetrize");
+        }
+    }
+
+    void Engine::sync()
+    {
+        cudaCheck(cudaStreamSynchronize(stream_), "sync");
+    }
+}

@@ -1,0 +1,185 @@
+// The engine object behind the C ABI.
+#pragma once
+
+#include "engine.hpp"
+
+#include <cuda_runtime.h>
+
+#include <map>
+#include <stdexcept>
+#include <string>
+
+namespace lible_b200
+{
+    struct PairView;
+
+    // Status codes returned through the C ABI (mirrors include/lible_b200.h).
+    enum Status : int
+    {
+        kStatusOk = 0,
+        kStatusInvalid = 1,
+        kStatusCuda = 2,
+        kStatusNoStructure = 3,
+        kStatusNoAux = 4,
+        kStatusUnsupported = 5,
+        kStatusTimeout = 6,
+        kStatusInternal = 7,
+    };
+
+    struct EngineError : std::runtime_error
+    {
+        int code;
+        EngineError(int c, const std::string &m) : std::runtime_error(m), code(c) {}
+    };
+
+    void cudaCheck(cudaError_t e, const char *what);
+
+    struct JKOptions
+    {
+        double schwarz = 1e-12;
+        double fp32_threshold = 1e-4;
+        int precision = 0;  // 0 FP64, 1 mixed (FP32 where Q_ab Q_cd < fp32_threshold)
+    };
+
+    struct JKStats
+    {
+        long long n_quartets = 0;
+        long long n_fp32 = 0;
+        long long n_launches = 0;
+    };
+
+    // Size of a J/K plan: unique contracted quartets, primitive quartets and algorithmic FLOPs
+    // (dense-equivalent count per primitive quartet: Boys (20 + 4L), R recursion 3 C(L+4,4) plus
+    // the signed matrix H_ab H_cd, ket contraction 2 H_ab H_cd S_cd, and per bra primitive pair the
+    // bra contraction 2 S_ab H_ab S_cd).
+    struct JKPlanInfo
+    {
+        long long n_quartets = 0, n_fp32 = 0, n_prim_quartets = 0, n_launches = 0;
+        double flops_fp64 = 0, flops_fp32 = 0;
+    };
+
+    std::pair<double, double> measureFp64Peak(int device, cudaStream_t s);
+
+    class Engine
+    {
+    public:
+        explicit Engine(int device);
+        ~Engine();
+        Engine(const Engine &) = delete;
+        Engine &operator=(const Engine &) = delete;
+
+        void setStructure(const std::vector<BasisAtom> &main, const std::vector<BasisAtom> *aux,
+                          const std::vector<std::array<double, 3>> &xyz_bohr);
+        size_t nao() const { return nao_; }
+        size_t naux() const { return naux_; }
+        int nAtoms() const { return n_atoms_; }
+        int maxL() const { return max_l_; }
+        bool hasAux() const { return has_aux_; }
+        cudaStream_t stream() const { return stream_; }
+        int device() const { return device_; }
+
+        // Full tensors (device output pointers) and diagonals (host output).
+        void eri4(double *out_dev);
+        void eri4Diagonal(double *out_host);
+        void eri3(double *out_dev);
+        void eri2(double *out_dev);
+        void eri2Diagonal(double *out_host);
+
+        // Kernel-API batches; classes in the reference's shellPairData / shellDataAux order.
+        struct ClassInfo
+        {
+            int la, lb;
+            long long n_pairs, n_ppairs;
+        };
+        std::vector<ClassInfo> pairClasses(bool use_symm)
+        {
+            auto &cs = mainSet(use_symm);
+            std::vector<ClassInfo> v;
+            for (size_t c = 0; c < cs.host.size(); c++)
+                v.push_back({cs.req_l[c].first, cs.req_l[c].second, (long long)cs.host[c].n_pairs,
+                             (long long)cs.host[c].n_ppairs});
+            return v;
+        }
+        std::vector<ClassInfo> auxClasses()
+        {
+            auto &cs = auxSet();
+            std::vector<ClassInfo> v;
+            for (size_t c = 0; c < cs.host.size(); c++)
+                v.push_back({cs.req_l[c].first, 0, (long long)cs.host[c].n_pairs, (long long)cs.host[c].n_ppairs});
+            return v;
+        }
+        void eri4Batch(bool use_symm, int cab, int ccd, long long n, const uint32_t *pairs_host, double *out_dev,
+                       bool d1);
+        void eri3Batch(bool use_symm, int cab, int cx, long long n, const uint32_t *idx_host, double *out_dev, bool d1);
+        void eri2Batch(int ca, int cb, long long n, const uint32_t *idx_host, double *out_dev, bool d1);
+
+        // Direct J/K (device pointers).  J, K symmetric on return.
+        void jk(const double *D_dev, double *J_dev, double *K_dev, const JKOptions &opt, JKStats *stats);
+        long long jkLaunchCount(const JKOptions &opt);
+        JKPlanInfo jkPlanInfo(const JKOptions &opt);
+        // Gradient of 1/2 Tr(DJ) - 1/4 Tr(DK) with respect to nuclear coordinates, [n_atoms][3].
+        void jkGradient(const double *D_dev, double *grad_dev);
+        // RI-J contractions (either output may be null).
+        void riContract(const double *D_dev, const double *dcoef_dev, double *gamma_dev, double *J_dev);
+
+        void sync();
+
+    private:
+        struct ClassSet
+        {
+            bool built = false;
+            bool schwarz_done = false;
+            std::vector<PairClass> host;
+            std::vector<DevPairClass> dev;
+            std::vector<bool> swapped;
+            std::vector<std::pair<int, int>> req_l;
+        };
+        struct JKClassPair
+        {
+            int cb = 0, ck = 0, n_bra = 0;
+            long long n64 = 0, n32 = 0;
+            double prim64 = 0, prim32 = 0, flops64 = 0, flops32 = 0;
+            unsigned long long *prefix64 = nullptr, *prefix32 = nullptr;
+            uint32_t *begin64 = nullptr, *begin32 = nullptr;
+        };
+        struct JKPlan
+        {
+            double thr = 0;
+            long long n_quartets = 0, n_fp32 = 0;
+            double n_prim = 0, flops64 = 0, flops32 = 0;
+            std::vector<uint32_t *> orders;
+            std::vector<JKClassPair> pairs;
+        };
+
+        void clearStructure();
+        void freeSet(ClassSet &cs);
+        void freePlan(JKPlan &p);
+        void requireStructure() const;
+        static std::vector<Shell> shellsL(const std::vector<Shell> &all, int l);
+        void uploadClass(const PairClass &pc, bool with_d1, bool with_f32, DevPairClass &d);
+        ClassSet &mainSet(bool use_symm);
+        ClassSet &auxSet();
+        static PairView view(const DevPairClass &d);
+        void runStore(const DevPairClass &bra, bool bra_swapped, const DevPairClass &ket, bool ket_swapped,
+                      const uint32_t *d_list, long long n, bool d1, double *d_out, bool same_class);
+        std::vector<std::vector<double>> diagonalBatches(ClassSet &cs);
+        void ensureSchwarz(ClassSet &cs);
+        JKPlan &jkPlan(double thr, double thr32, bool mixed);
+
+        int device_ = 0;
+        int num_sms_ = 0;
+        cudaStream_t stream_ = nullptr;
+        double *boys_ = nullptr;
+        int *sph_rc_ = nullptr;
+        double *sph_val_ = nullptr;
+        std::vector<int> sph_ofs_;
+        std::vector<void *> persistent_;
+
+        bool has_structure_ = false, has_aux_ = false;
+        std::vector<Shell> shells_, aux_shells_;
+        size_t nao_ = 0, naux_ = 0;
+        int n_atoms_ = 0, max_l_ = 0, max_l_aux_ = 0;
+        ClassSet symm_, nosymm_, aux_;
+        std::map<std::string, JKPlan> plans_;
+    };
+}

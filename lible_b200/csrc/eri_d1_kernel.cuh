@@ -1,0 +1,325 @@
+// First nuclear derivatives of contracted shell quartets, one instantiation per class, following
+// the structure of src/lible/ints/twoel/eri_kernel_funs.hpp:350-515:
+//   d/dA = (a/p) E_ab dR/dP E_cd^T + E1_ab R E_cd^T,    d/dB = (b/p) E_ab dR/dP E_cd^T - E1_ab R E_cd^T,
+//   d/dC = E_ab (-(c/q) dR/dP E_cd^T + R E1_cd^T),     d/dD = -(d/dA + d/dB + d/dC),
+// where dR/dP_x is the R matrix shifted by one unit along x (Boys function to L+1) and E1 is the
+// derivative of the Hermite coefficients with respect to the pair separation.
+//
+// The work for one quartet is organised in four passes over the primitive quartets - one per
+// Cartesian direction for the shifted terms plus one for the E1_ab terms - so that only one R
+// matrix and two R.E accumulators are live at a time.  Two epilogues:
+//   kD1Store: the 12 blocks are accumulated straight into the caller's output (each element owned
+//             by exactly one thread, so no atomics);
+//   kD1Grad:  each block is contracted on the fly with the two-particle density of
+//             E = 1/2 Tr(DJ) - 1/4 Tr(DK),  Gamma = f (4 D_ab D_cd - D_ac D_bd - D_ad D_bc),
+//             and the per-atom sums are added to the gradient (the adjoint of the J/K build).
+#pragma once
+
+#include "device_common.cuh"
+
+namespace lible_b200
+{
+    template <int LA, int LB, int LC, int LD>
+    struct ShapeD1
+    {
+        using C = Cls<LA, LB, LC, LD>;
+        static constexpr int HS = C::HAB * C::SCD;
+        static constexpr int G = HS <= 24 * 32 ? 32 : HS <= 24 * 64 ? 64 : HS <= 24 * 128 ? 128 : 256;
+        static constexpr int IK = (HS + G - 1) / G;
+        static constexpr size_t off_rb = 0;                                        // 2 x NR1 doubles
+        static constexpr size_t off_rm = off_rb + 8 * 2 * C::NR1;                  // HCD x HAB
+        static constexpr size_t off_rx = off_rm + 8 * C::HCD * C::HAB;             // 2 x HAB x SCD
+        static constexpr size_t off_gm = off_rx + 8 * 2 * C::HAB * C::SCD;         // SAB x SCD
+        static constexpr size_t off_st = off_gm + 8 * C::SAB * C::SCD;             // HCD x HAB char4
+        static constexpr size_t off_ht = off_st + 4 * C::HCD * C::HAB;             // NR1 char4
+        static constexpr size_t off_rd = (off_ht + 4 * C::NR1 + 15) / 16 * 16;    // 9 x G/32 doubles
+        static constexpr size_t smem = off_rd + 8 * 9 * (G / 32);
+    };
+
+    template <int LA, int LB, int LC, int LD>
+    __global__ void __launch_bounds__(ShapeD1<LA, LB, LC, LD>::G) eriD1Kernel(QuartetArgs a)
+    {
+        using C = Cls<LA, LB, LC, LD>;
+        using S = ShapeD1<LA, LB, LC, LD>;
+        constexpr int G = S::G;
+        constexpr int L1 = C::L + 1;
+        constexpr int blk = C::SAB * C::SCD;
+        extern __shared__ __align__(16) unsigned char smem[];
+        double *rb = reinterpret_cast<double *>(smem + S::off_rb);
+        double *rm = reinterpret_cast<double *>(smem + S::off_rm);
+        double *rx1 = reinterpret_cast<double *>(smem + S::off_rx);
+        double *rx2 = rx1 + C::HAB * C::SCD;
+        double *gm = reinterpret_cast<double *>(smem + S::off_gm);
+        char4 *st = reinterpret_cast<char4 *>(smem + S::off_st);
+        char4 *ht = reinterpret_cast<char4 *>(smem + S::off_ht);
+        const int tid = threadIdx.x;
+
+        for (int e = tid; e < C::NR1; e += G)
+        {
+            int t, u, v;
+            hermTuv(e, t, u, v);
+            ht[e] = make_char4((char)t, (char)u, (char)v, (char)(t + u + v));
+        }
+        for (int e = tid; e < C::HCD * C::HAB; e += G)
+        {
+            const int hp = e / C::HAB, h = e % C::HAB;
+            int t, u, v, tp, up, vp;
+            hermTuv(h, t, u, v);
+            hermTuv(hp, tp, up, vp);
+            st[e] = make_char4((char)(t + tp), (char)(u + up), (char)(v + vp), (char)((tp + up + vp) & 1));
+        }
+        __syncthreads();
+
+        for (long long task = blockIdx.x; task < a.n_tasks; task += gridDim.x)
+        {
+            uint32_t ib, ik;
+            decodeTask(a, task, ib, ik);
+            const int32_t *bi = a.bra.info + 8 * ib;
+            const int32_t *ki = a.ket.info + 8 * ik;
+            double acc[12];
+#pragma unroll
+            for (int x = 0; x < 12; x++)
+                acc[x] = 0.0;
+            double *outq = nullptr;
+            if (a.mode == kD1Store)
+            {
+                outq = a.out + (size_t)task * 12 * blk;
+                for (int e = tid; e < 12 * blk; e += G)
+                    outq[e] = 0.0;
+            }
+            else
+            {
+                const double f = quartetWeight(a, ib, ik);
+                const int n = a.nao;
+                for (int e = tid; e < blk; e += G)
+                {
+                    const int mn = e / C::SCD, kt = e % C::SCD;
+                    const int mu = bi[0] + mn / C::SB, nu = bi[1] + mn % C::SB;
+                    const int ka = ki[0] + kt / C::SD, ta = ki[1] + kt % C::SD;
+                    const double *D = a.D;
+                    gm[e] = f * (4.0 * D[(size_t)mu * n + nu] * D[(size_t)ka * n + ta] -
+                                 D[(size_t)mu * n + ka] * D[(size_t)nu * n + ta] -
+                                 D[(size_t)mu * n + ta] * D[(size_t)nu * n + ka]);
+                }
+            }
+            __syncthreads();
+
+            // Output slot of internal block (centre c, direction x) for kD1Store.
+            auto emit = [&](int centre, int x, int e, double v) {
+                if (a.mode == kD1Store)
+                    outq[(size_t)(centre * 3 + x) * blk + e] += v;
+                else
+                    acc[centre * 3 + x] += gm[e] * v;
+            };
+
+            const uint32_t p0 = a.bra.pofs[ib], p1 = a.bra.pofs[ib + 1];
+            const uint32_t q0 = a.ket.pofs[ik], q1 = a.ket.pofs[ik + 1];
+            for (uint32_t p = p0; p < p1; p++)
+            {
+                const PQ4 P = loadPQ(a.bra.pP, p);
+                const double2 AB = __ldg(reinterpret_cast<const double2 *>(a.bra.ab) + p);
+                const double *eab = a.bra.E + (size_t)p * C::SAB * C::HAB;
+                const double *e1ab = a.bra.E1 + (size_t)p * 3 * C::SAB * C::HAB;
+                for (int pass = 0; pass < 4; pass++)
+                {
+                    double r1[S::IK], r2[S::IK];
+#pragma unroll
+                    for (int k = 0; k < S::IK; k++)
+                        r1[k] = r2[k] = 0.0;
+                    for (uint32_t q = q0; q < q1; q++)
+                    {
+                        const PQ4 Q = loadPQ(a.ket.pP, q);
+                        const double cexp = __ldg(a.ket.ab + 2 * q);
+                        const double pq = P.x + Q.x;
+                        const double alpha = P.x * Q.x / pq;
+                        const double X = P.y - Q.y, Y = P.z - Q.z, Z = P.w - Q.w;
+                        const double fac = 2.0 * 17.493418327624862 / (P.x * Q.x * sqrt(pq));
+                        double F[L1 + 1];
+                        boysF<L1>(alpha * (X * X + Y * Y + Z * Z), a.boys, F);
+                        const double m2a = -2.0 * alpha;
+                        double *cur = rb, *nxt = rb + C::NR1;
+                        if (tid == 0)
+                        {
+                            double pw = 1.0;
+                            for (int k = 0; k < L1; k++)
+                                pw *= m2a;
+                            cur[0] = F[L1] * fac * pw;
+                        }
+                        __syncthreads();
+                        for (int n = L1 - 1; n >= 0; n--)
+                        {
+                            const int cnt = nherm(L1 - n);
+                            for (int e = tid; e < cnt; e += G)
+                            {
+                                double r;
+                                if (e == 0)
+                                {
+                                    double pn = 1.0;
+                                    for (int k = 0; k < n; k++)
+                                        pn *= m2a;
+                                    r = F[n] * fac * pn;
+                                }
+                                else
+                                {
+                                    const char4 tv = ht[e];
+                                    const int t = tv.x, u = tv.y, v = tv.z, m = tv.w;
+                                    if (t > 0)
+                                    {
+                                        r = X * cur[nherm(m - 2) + cartIndex(u, v)];
+                                        if (t > 1)
+                                            r += (t - 1) * cur[nherm(m - 3) + cartIndex(u, v)];
+                                    }
+                                    else if (u > 0)
+                                    {
+                                        r = Y * cur[nherm(m - 2) + cartIndex(u - 1, v)];
+                                        if (u > 1)
+                                            r += (u - 1) * cur[nherm(m - 3) + cartIndex(u - 2, v)];
+                                    }
+                                    else
+                                    {
+                                        r = Z * cur[nherm(m - 2) + cartIndex(0, v - 1)];
+                                        if (v > 1)
+                                            r += (v - 1) * cur[nherm(m - 3) + cartIndex(0, v - 2)];
+                                    }
+                                }
+                                nxt[e] = r;
+                            }
+                            __syncthreads();
+                            double *tmp = cur;
+                            cur = nxt;
+                            nxt = tmp;
+                        }
+                        const double *ecd = a.ket.Et + (size_t)q * C::HCD * C::SCD;
+                        // sub-step 1: shifted (pass < 3) or plain (pass 3) R matrix times E_cd
+                        const int dx = pass == 0, dy = pass == 1, dz = pass == 2;
+                        for (int e = tid; e < C::HCD * C::HAB; e += G)
+                        {
+                            const char4 s4 = st[e];
+                            const double r = cur[hermIndex(s4.x + dx, s4.y + dy, s4.z + dz)];
+                            rm[e] = s4.w ? -r : r;
+                        }
+                        __syncthreads();
+                        const double cq = cexp / Q.x;
+#pragma unroll
+                        for (int k = 0; k < S::IK; k++)
+                        {
+                            const int e = tid + G * k;
+                            if (e < C::HAB * C::SCD)
+                            {
+                                const int h = e / C::SCD, c = e % C::SCD;
+                                double s = 0.0;
+                                for (int hp = 0; hp < C::HCD; hp++)
+                                    s += rm[hp * C::HAB + h] * ecd[hp * C::SCD + c];
+                                r1[k] += s;
+                                if (pass < 3)
+                                    r2[k] -= cq * s;
+                            }
+                        }
+                        __syncthreads();
+                        if (pass < 3)
+                        {
+                            // sub-step 2: plain R matrix times E1_cd along this direction
+                            for (int e = tid; e < C::HCD * C::HAB; e += G)
+                            {
+                                const char4 s4 = st[e];
+                                const double r = cur[hermIndex(s4.x, s4.y, s4.z)];
+                                rm[e] = s4.w ? -r : r;
+                            }
+                            __syncthreads();
+                            const double *e1cd = a.ket.E1t + ((size_t)q * 3 + pass) * C::HCD * C::SCD;
+#pragma unroll
+                            for (int k = 0; k < S::IK; k++)
+                            {
+                                const int e = tid + G * k;
+                                if (e < C::HAB * C::SCD)
+                                {
+                                    const int h = e / C::SCD, c = e % C::SCD;
+                                    double s = 0.0;
+                                    for (int hp = 0; hp < C::HCD; hp++)
+                                        s += rm[hp * C::HAB + h] * e1cd[hp * C::SCD + c];
+                                    r2[k] += s;
+                                }
+                            }
+                            __syncthreads();
+                        }
+                    }
+#pragma unroll
+                    for (int k = 0; k < S::IK; k++)
+                    {
+                        const int e = tid + G * k;
+                        if (e < C::HAB * C::SCD)
+                        {
+                            rx1[e] = r1[k];
+                            rx2[e] = r2[k];
+                        }
+                    }
+                    __syncthreads();
+                    for (int e = tid; e < blk; e += G)
+                    {
+                        const int m = e / C::SCD, c = e % C::SCD;
+                        if (pass < 3)
+                        {
+                            double sp = 0.0, sc = 0.0;
+                            for (int h = 0; h < C::HAB; h++)
+                            {
+                                const double ev = eab[m * C::HAB + h];
+                                sp += ev * rx1[h * C::SCD + c];
+                                sc += ev * rx2[h * C::SCD + c];
+                            }
+                            emit(0, pass, e, (AB.x / P.x) * sp);
+                            emit(1, pass, e, (AB.y / P.x) * sp);
+                            emit(2, pass, e, sc);
+                        }
+                        else
+                        {
+                            for (int x = 0; x < 3; x++)
+                            {
+                                double s = 0.0;
+                                for (int h = 0; h < C::HAB; h++)
+                                    s += e1ab[(x * C::SAB + m) * C::HAB + h] * rx1[h * C::SCD + c];
+                                emit(0, x, e, s);
+                                emit(1, x, e, -s);
+                            }
+                        }
+                    }
+                    __syncthreads();
+                }
+            }
+
+            if (a.mode == kD1Store)
+            {
+                // D by translational invariance; the caller's orientation is applied afterwards by
+                // a separate reorder pass
+                for (int e = tid; e < blk; e += G)
+                    for (int x = 0; x < 3; x++)
+                        outq[(size_t)(9 + x) * blk + e] =
+                            -(outq[(size_t)x * blk + e] + outq[(size_t)(3 + x) * blk + e] + outq[(size_t)(6 + x) * blk + e]);
+            }
+            else
+            {
+                // reduce the 9 independent sums over the block, then add per atom
+                double *red = reinterpret_cast<double *>(smem + S::off_rd);
+                for (int x = 0; x < 9; x++)
+                {
+                    double v = acc[x];
+                    for (int o = 16; o > 0; o >>= 1)
+                        v += __shfl_down_sync(0xffffffffu, v, o);
+                    if ((tid & 31) == 0)
+                        red[(tid >> 5) * 9 + x] = v;
+                }
+                __syncthreads();
+                if (tid < 9)
+                {
+                    double v = 0.0;
+                    for (int w = 0; w < G / 32; w++)
+                        v += red[w * 9 + tid];
+                    const int centre = tid / 3, x = tid % 3;
+                    const int atom = centre == 0 ? bi[2] : centre == 1 ? bi[3] : ki[2];
+                    atomicAdd(a.grad + 3 * atom + x, v);
+                    atomicAdd(a.grad + 3 * ki[3] + x, -v);
+                }
+                __syncthreads();
+            }
+        }
+    }
+}

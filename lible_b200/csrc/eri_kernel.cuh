@@ -1,0 +1,577 @@
+// The quartet-class kernel family: one instantiation per angular-momentum class
+// (la lb | lc ld), computing contracted shell-quartet batches in the SHARK form
+//     (ab|cd) = sum_p sum_q E_ab[p] . R_pq . E_cd[q]^T
+// (src/lible/ints/twoel/eri_kernel_funs.hpp:104-193) and consuming them in a fused epilogue
+// (store, J/K digestion, RI-J).  Three- and two-centre integrals use the same kernels: an
+// auxiliary shell is a "pair" whose second member is a unit s function of exponent 0.
+//
+// Two execution shapes, chosen per class at compile time:
+//  * G = 1  (small classes): one thread owns a whole contracted quartet; R, R.E and the batch live
+//    in registers and every index is a compile-time constant.
+//  * G = 32*W (larger classes): a group of W warps owns one quartet; the R recursion, the signed
+//    R matrix and the staged E tiles live in shared memory and the two contractions are split
+//    over the group's threads.
+#pragma once
+
+#include "device_common.cuh"
+
+namespace lible_b200
+{
+    template <int LA, int LB, int LC, int LD, typename T>
+    struct Shape
+    {
+        using C = Cls<LA, LB, LC, LD>;
+        static constexpr int small_regs = C::SAB * C::SCD + C::HAB * C::SCD + C::NR;
+        static constexpr int W = (small_regs <= 72) ? 0
+                                 : ((C::HAB * C::SCD + C::SAB * C::SCD) <= 64 * 32)     ? 1
+                                 : ((C::HAB * C::SCD + C::SAB * C::SCD) <= 64 * 64)     ? 2
+                                 : ((C::HAB * C::SCD + C::SAB * C::SCD) <= 64 * 128)    ? 4
+                                                                                          : 8;
+        static constexpr int G = W == 0 ? 1 : 32 * W;
+        static constexpr int block = W == 0 ? 128 : G;
+        static constexpr int IK = W == 0 ? 0 : (C::HAB * C::SCD + G - 1) / G;
+        static constexpr int IB = W == 0 ? 0 : (C::SAB * C::SCD + G - 1) / G;
+        // shared-memory carve-up (bytes) for the group shape
+        static constexpr size_t off_rb = 0;                                          // 2 x NR of T
+        static constexpr size_t off_rm = off_rb + sizeof(T) * 2 * C::NR;            // HCD x HAB
+        static constexpr size_t off_ec = off_rm + sizeof(T) * C::HCD * C::HAB;      // HCD x SCD
+        static constexpr size_t off_ea = off_ec + sizeof(T) * C::HCD * C::SCD;      // SAB x HAB
+        static constexpr size_t off_rx = off_ea + sizeof(T) * C::SAB * C::HAB;      // HAB x SCD
+        static constexpr size_t off_ix = off_rx + sizeof(T) * C::HAB * C::SCD;      // HCD x HAB int16
+        static constexpr size_t off_ht = (off_ix + 2 * C::HCD * C::HAB + 15) / 16 * 16; // NR char4
+        static constexpr size_t smem = W == 0 ? 0 : off_ht + 4 * C::NR;
+    };
+
+    __device__ __forceinline__ void groupSync(int G)
+    {
+        if (G == 32)
+            __syncwarp();
+        else
+            __syncthreads();
+    }
+
+    template <typename T>
+    __device__ __forceinline__ const T *braE(const PairView &v);
+    template <>
+    __device__ __forceinline__ const double *braE<double>(const PairView &v) { return v.E; }
+    template <>
+    __device__ __forceinline__ const float *braE<float>(const PairView &v) { return v.Ef; }
+    template <typename T>
+    __device__ __forceinline__ const T *ketE(const PairView &v);
+    template <>
+    __device__ __forceinline__ const double *ketE<double>(const PairView &v) { return v.Et; }
+    template <>
+    __device__ __forceinline__ const float *ketE<float>(const PairView &v) { return v.Etf; }
+
+    // Destination offset of element (m, n, k, t) of a batch for kStore with the caller's
+    // orientation flags.
+    template <int SA, int SB, int SC, int SD>
+    __device__ __forceinline__ size_t storeIndex(int flags, int m, int n, int k, int t)
+    {
+        int b0 = m, b1 = n, k0 = k, k1 = t;
+        int db0 = SA, db1 = SB, dk0 = SC, dk1 = SD;
+        if (flags & 1)
+        {
+            b0 = n; b1 = m; db0 = SB; db1 = SA;
+        }
+        if (flags & 2)
+        {
+            k0 = t; k1 = k; dk0 = SD; dk1 = SC;
+        }
+        if (flags & 4)
+            return (((size_t)k0 * dk1 + k1) * db0 + b0) * db1 + b1;
+        return (((size_t)b0 * db1 + b1) * dk0 + k0) * dk1 + k1;
+    }
+
+    // Generic digestion of one batch V[SAB][SCD] (values read through `val(e)`), with the
+    // thread subset [tid, tid + stride, ...] producing outputs.  Implements
+    //   J_ab += 2 f V D_cd,  J_cd += 2 f V D_ab,
+    //   K_ac += f V D_bd, K_ad += f V D_bc, K_bc += f V D_ad, K_bd += f V D_ac
+    // into the unsymmetrised accumulators (J = A + A^T, K = B + B^T afterwards).
+    template <int SA, int SB, int SC, int SD, bool SERIAL, typename F>
+    __device__ __forceinline__ void digestJK(const QuartetArgs &a, double f, const int32_t *bi,
+                                             const int32_t *ki, F val, int tid, int stride)
+    {
+        if constexpr (SERIAL)
+        {
+            tid = 0;
+            stride = 1;
+        }
+        const int n = a.nao;
+        const int oa = bi[0], ob = bi[1], oc = ki[0], od = ki[1];
+        const double *D = a.D;
+        constexpr int n0 = SA * SB, n1 = n0 + SC * SD, n2 = n1 + SA * SC, n3 = n2 + SA * SD,
+                      n4 = n3 + SB * SC, n5 = n4 + SB * SD;
+#pragma unroll
+        for (int o = tid; o < n5; o += stride)
+        {
+            double s = 0.0;
+            double *dst;
+            double w;
+            if (o < n0)
+            {
+                int m = o / SB, nn = o % SB;
+#pragma unroll
+                for (int k = 0; k < SC; k++)
+#pragma unroll
+                    for (int t = 0; t < SD; t++)
+                        s += val(((m * SB + nn) * SC + k) * SD + t) * __ldg(D + (size_t)(oc + k) * n + od + t);
+                dst = a.J + (size_t)(oa + m) * n + ob + nn;
+                w = 2.0 * f;
+            }
+            else if (o < n1)
+            {
+                int k = (o - n0) / SD, t = (o - n0) % SD;
+#pragma unroll
+                for (int m = 0; m < SA; m++)
+#pragma unroll
+                    for (int nn = 0; nn < SB; nn++)
+                        s += val(((m * SB + nn) * SC + k) * SD + t) * __ldg(D + (size_t)(oa + m) * n + ob + nn);
+                dst = a.J + (size_t)(oc + k) * n + od + t;
+                w = 2.0 * f;
+            }
+            else if (o < n2)
+            {
+                int m = (o - n1) / SC, k = (o - n1) % SC;
+#pragma unroll
+                for (int nn = 0; nn < SB; nn++)
+#pragma unroll
+                    for (int t = 0; t < SD; t++)
+                        s += val(((m * SB + nn) * SC + k) * SD + t) * __ldg(D + (size_t)(ob + nn) * n + od + t);
+                dst = a.K + (size_t)(oa + m) * n + oc + k;
+                w = f;
+            }
+            else if (o < n3)
+            {
+                int m = (o - n2) / SD, t = (o - n2) % SD;
+#pragma unroll
+                for (int nn = 0; nn < SB; nn++)
+#pragma unroll
+                    for (int k = 0; k < SC; k++)
+                        s += val(((m * SB + nn) * SC + k) * SD + t) * __ldg(D + (size_t)(ob + nn) * n + oc + k);
+                dst = a.K + (size_t)(oa + m) * n + od + t;
+                w = f;
+            }
+            else if (o < n4)
+            {
+                int nn = (o - n3) / SC, k = (o - n3) % SC;
+#pragma unroll
+                for (int m = 0; m < SA; m++)
+#pragma unroll
+                    for (int t = 0; t < SD; t++)
+                        s += val(((m * SB + nn) * SC + k) * SD + t) * __ldg(D + (size_t)(oa + m) * n + od + t);
+                dst = a.K + (size_t)(ob + nn) * n + oc + k;
+                w = f;
+            }
+            else
+            {
+                int nn = (o - n4) / SD, t = (o - n4) % SD;
+#pragma unroll
+                for (int m = 0; m < SA; m++)
+#pragma unroll
+                    for (int k = 0; k < SC; k++)
+                        s += val(((m * SB + nn) * SC + k) * SD + t) * __ldg(D + (size_t)(oa + m) * n + oc + k);
+                dst = a.K + (size_t)(ob + nn) * n + od + t;
+                w = f;
+            }
+            atomicAdd(dst, w * s);
+        }
+    }
+
+    // RI-J digestion of a three-centre batch (main pair | aux shell) or (aux | main).
+    template <int SA, int SB, int SC, int SD, bool SERIAL, typename F>
+    __device__ __forceinline__ void digestRI(const QuartetArgs &a, const int32_t *bi, const int32_t *ki,
+                                             F val, int tid, int stride)
+    {
+        if constexpr (SERIAL)
+        {
+            tid = 0;
+            stride = 1;
+        }
+        const int n = a.nao;
+        // main pair (m0, m1) with sizes (S0, S1); aux shell with size SX
+        const bool auxket = a.aux_side == 0;
+        const int32_t *mi = auxket ? bi : ki;
+        const int32_t *xi = auxket ? ki : bi;
+        const int S0 = auxket ? SA : SC, S1 = auxket ? SB : SD, SX = auxket ? SC : SA;
+        const int o0 = mi[0], o1 = mi[1], ox = xi[0];
+        const double fb = (mi[4] == mi[5]) ? 0.5 : 1.0;
+        auto V = [&](int m, int nn, int x) {
+            return auxket ? val((m * SB + nn) * SC * SD + x) : val(x * SC * SD + m * SD + nn);
+        };
+        if (a.mode == kRIGamma)
+        {
+            for (int x = tid; x < SX; x += stride)
+            {
+                double s = 0.0;
+                for (int m = 0; m < S0; m++)
+                    for (int nn = 0; nn < S1; nn++)
+                        s += V(m, nn, x) * __ldg(a.D + (size_t)(o0 + m) * n + o1 + nn);
+                atomicAdd(a.gamma + ox + x, 2.0 * fb * s);
+            }
+        }
+        else
+        {
+            for (int o = tid; o < S0 * S1; o += stride)
+            {
+                int m = o / S1, nn = o % S1;
+                double s = 0.0;
+                for (int x = 0; x < SX; x++)
+                    s += V(m, nn, x) * __ldg(a.dcoef + ox + x);
+                atomicAdd(a.J + (size_t)(o0 + m) * n + o1 + nn, fb * s);
+            }
+        }
+    }
+
+    // ---------------------------------------------------------------------------------------
+    // G = 1: one thread per contracted quartet.
+    template <int LA, int LB, int LC, int LD, typename T>
+    __device__ __forceinline__ void quartetThread(const QuartetArgs &a, uint32_t ib, uint32_t ik, T *V)
+    {
+        using C = Cls<LA, LB, LC, LD>;
+#pragma unroll
+        for (int x = 0; x < C::SAB * C::SCD; x++)
+            V[x] = T(0);
+        const uint32_t p0 = a.bra.pofs[ib], p1 = a.bra.pofs[ib + 1];
+        const uint32_t q0 = a.ket.pofs[ik], q1 = a.ket.pofs[ik + 1];
+        const T *Eb = braE<T>(a.bra);
+        const T *Ek = ketE<T>(a.ket);
+        for (uint32_t p = p0; p < p1; p++)
+        {
+            const PQ4 P = loadPQ(a.bra.pP, p);
+            T RxE[C::HAB * C::SCD];
+#pragma unroll
+            for (int x = 0; x < C::HAB * C::SCD; x++)
+                RxE[x] = T(0);
+            for (uint32_t q = q0; q < q1; q++)
+            {
+                const PQ4 Q = loadPQ(a.ket.pP, q);
+                const double pq = P.x + Q.x;
+                const double alpha = P.x * Q.x / pq;
+                const double X = P.y - Q.y, Y = P.z - Q.z, Z = P.w - Q.w;
+                const double fac = 2.0 * 17.493418327624862 / (P.x * Q.x * sqrt(pq)); // 2 pi^{5/2}
+                double F[C::L + 1];
+                boysF<C::L>(alpha * (X * X + Y * Y + Z * Z), a.boys, F);
+                T Ft[C::L + 1];
+#pragma unroll
+                for (int k = 0; k <= C::L; k++)
+                    Ft[k] = T(F[k] * fac);
+                T R[C::NR];
+                hermiteR<C::L, T>(T(-2.0 * alpha), Ft, T(X), T(Y), T(Z), R);
+                const T *ec = Ek + (size_t)q * C::HCD * C::SCD;
+#pragma unroll
+                for (int hp = 0; hp < C::HCD; hp++)
+                {
+                    int tp = 0, up = 0, vp = 0;
+                    // (t', u', v') of hp, resolved at compile time after unrolling
+#pragma unroll
+                    for (int n = 0, e = 0; n <= C::LCD; n++)
+#pragma unroll
+                        for (int t = n; t >= 0; t--)
+#pragma unroll
+                            for (int u = n - t; u >= 0; u--, e++)
+                                if (e == hp)
+                                {
+                                    tp = t;
+                                    up = u;
+                                    vp = n - t - u;
+                                }
+                    const T sg = ((tp + up + vp) & 1) ? T(-1) : T(1);
+                    T ecv[C::SCD];
+#pragma unroll
+                    for (int c = 0; c < C::SCD; c++)
+                        ecv[c] = ec[hp * C::SCD + c];
+#pragma unroll
+                    for (int h = 0, n = 0; n <= C::LAB; n++)
+#pragma unroll
+                        for (int t = n; t >= 0; t--)
+#pragma unroll
+                            for (int u = n - t; u >= 0; u--, h++)
+                            {
+                                const int v = n - t - u;
+                                const T r = sg * R[hermIndex(t + tp, u + up, v + vp)];
+#pragma unroll
+                                for (int c = 0; c < C::SCD; c++)
+                                    RxE[h * C::SCD + c] += r * ecv[c];
+                            }
+                }
+            }
+            const T *eb = Eb + (size_t)p * C::SAB * C::HAB;
+#pragma unroll
+            for (int m = 0; m < C::SAB; m++)
+#pragma unroll
+                for (int h = 0; h < C::HAB; h++)
+                {
+                    const T e = eb[m * C::HAB + h];
+#pragma unroll
+                    for (int c = 0; c < C::SCD; c++)
+                        V[m * C::SCD + c] += e * RxE[h * C::SCD + c];
+                }
+        }
+    }
+
+    // ---------------------------------------------------------------------------------------
+    // G = 32 W: one thread group (the whole block) per contracted quartet.
+    template <int LA, int LB, int LC, int LD, typename T>
+    __device__ __forceinline__ void quartetGroup(const QuartetArgs &a, uint32_t ib, uint32_t ik,
+                                                 unsigned char *smem, T *vals)
+    {
+        using C = Cls<LA, LB, LC, LD>;
+        using S = Shape<LA, LB, LC, LD, T>;
+        constexpr int G = S::G;
+        const int tid = threadIdx.x;
+        T *rb = reinterpret_cast<T *>(smem + S::off_rb);
+        T *rm = reinterpret_cast<T *>(smem + S::off_rm);
+        T *ecs = reinterpret_cast<T *>(smem + S::off_ec);
+        T *eas = reinterpret_cast<T *>(smem + S::off_ea);
+        T *rxs = reinterpret_cast<T *>(smem + S::off_rx);
+        const short *rix = reinterpret_cast<const short *>(smem + S::off_ix);
+        const char4 *ht = reinterpret_cast<const char4 *>(smem + S::off_ht);
+
+#pragma unroll
+        for (int k = 0; k < S::IB; k++)
+            vals[k] = T(0);
+        const uint32_t p0 = a.bra.pofs[ib], p1 = a.bra.pofs[ib + 1];
+        const uint32_t q0 = a.ket.pofs[ik], q1 = a.ket.pofs[ik + 1];
+        const T *Eb = braE<T>(a.bra);
+        const T *Ek = ketE<T>(a.ket);
+        for (uint32_t p = p0; p < p1; p++)
+        {
+            const PQ4 P = loadPQ(a.bra.pP, p);
+            for (int e = tid; e < C::SAB * C::HAB; e += G)
+                eas[e] = Eb[(size_t)p * C::SAB * C::HAB + e];
+            T rxe[S::IK];
+#pragma unroll
+            for (int k = 0; k < S::IK; k++)
+                rxe[k] = T(0);
+            for (uint32_t q = q0; q < q1; q++)
+            {
+                const PQ4 Q = loadPQ(a.ket.pP, q);
+                const double pq = P.x + Q.x;
+                const double alpha = P.x * Q.x / pq;
+                const double X = P.y - Q.y, Y = P.z - Q.z, Z = P.w - Q.w;
+                const double fac = 2.0 * 17.493418327624862 / (P.x * Q.x * sqrt(pq));
+                double F[C::L + 1];
+                boysF<C::L>(alpha * (X * X + Y * Y + Z * Z), a.boys, F);
+                const double m2a = -2.0 * alpha;
+                // level L
+                T *cur = rb, *nxt = rb + C::NR;
+                double pw = 1.0;
+                for (int k = 0; k < C::L; k++)
+                    pw *= m2a;
+                if (tid == 0)
+                    cur[0] = T(F[C::L] * fac * pw);
+                groupSync(G);
+                for (int n = C::L - 1; n >= 0; n--)
+                {
+                    const int cnt = nherm(C::L - n);
+                    for (int e = tid; e < cnt; e += G)
+                    {
+                        T r;
+                        if (e == 0)
+                        {
+                            double pn = 1.0;
+                            for (int k = 0; k < n; k++)
+                                pn *= m2a;
+                            r = T(F[n] * fac * pn);
+                        }
+                        else
+                        {
+                            const char4 tv = ht[e];
+                            const int t = tv.x, u = tv.y, v = tv.z, m = tv.w;
+                            if (t > 0)
+                            {
+                                r = T(X) * cur[nherm(m - 2) + cartIndex(u, v)];
+                                if (t > 1)
+                                    r += T(t - 1) * cur[nherm(m - 3) + cartIndex(u, v)];
+                            }
+                            else if (u > 0)
+                            {
+                                r = T(Y) * cur[nherm(m - 2) + cartIndex(u - 1, v)];
+                                if (u > 1)
+                                    r += T(u - 1) * cur[nherm(m - 3) + cartIndex(u - 2, v)];
+                            }
+                            else
+                            {
+                                r = T(Z) * cur[nherm(m - 2) + cartIndex(0, v - 1)];
+                                if (v > 1)
+                                    r += T(v - 1) * cur[nherm(m - 3) + cartIndex(0, v - 2)];
+                            }
+                        }
+                        nxt[e] = r;
+                    }
+                    groupSync(G);
+                    T *tmp = cur;
+                    cur = nxt;
+                    nxt = tmp;
+                }
+                // signed R matrix [h'][h] and the staged ket E[q] [h'][cd]
+                for (int e = tid; e < C::HCD * C::HAB; e += G)
+                {
+                    const short ix = rix[e];
+                    const T r = cur[ix & 0x7fff];
+                    rm[e] = (ix & 0x8000) ? -r : r;
+                }
+                for (int e = tid; e < C::HCD * C::SCD; e += G)
+                    ecs[e] = Ek[(size_t)q * C::HCD * C::SCD + e];
+                groupSync(G);
+#pragma unroll
+                for (int k = 0; k < S::IK; k++)
+                {
+                    const int e = tid + G * k;
+                    if (e < C::HAB * C::SCD)
+                    {
+                        const int h = e / C::SCD, c = e % C::SCD;
+                        T s = rxe[k];
+#pragma unroll 5
+                        for (int hp = 0; hp < C::HCD; hp++)
+                            s += rm[hp * C::HAB + h] * ecs[hp * C::SCD + c];
+                        rxe[k] = s;
+                    }
+                }
+                groupSync(G);
+            }
+#pragma unroll
+            for (int k = 0; k < S::IK; k++)
+            {
+                const int e = tid + G * k;
+                if (e < C::HAB * C::SCD)
+                    rxs[e] = rxe[k];
+            }
+            groupSync(G);
+#pragma unroll
+            for (int k = 0; k < S::IB; k++)
+            {
+                const int e = tid + G * k;
+                if (e < C::SAB * C::SCD)
+                {
+                    const int m = e / C::SCD, c = e % C::SCD;
+                    T s = vals[k];
+#pragma unroll 5
+                    for (int h = 0; h < C::HAB; h++)
+                        s += eas[m * C::HAB + h] * rxs[h * C::SCD + c];
+                    vals[k] = s;
+                }
+            }
+            groupSync(G);
+        }
+    }
+
+    // Builds the per-block tables of the group shape: Hermite (t,u,v,order) list and the signed
+    // combined index of (h + h') for the R matrix.
+    template <int LA, int LB, int LC, int LD, typename T>
+    __device__ __forceinline__ void buildGroupTables(unsigned char *smem)
+    {
+        using C = Cls<LA, LB, LC, LD>;
+        using S = Shape<LA, LB, LC, LD, T>;
+        short *rix = reinterpret_cast<short *>(smem + S::off_ix);
+        char4 *ht = reinterpret_cast<char4 *>(smem + S::off_ht);
+        for (int e = threadIdx.x; e < C::NR; e += blockDim.x)
+        {
+            int t, u, v;
+            hermTuv(e, t, u, v);
+            ht[e] = make_char4((char)t, (char)u, (char)v, (char)(t + u + v));
+        }
+        for (int e = threadIdx.x; e < C::HCD * C::HAB; e += blockDim.x)
+        {
+            const int hp = e / C::HAB, h = e % C::HAB;
+            int t, u, v, tp, up, vp;
+            hermTuv(h, t, u, v);
+            hermTuv(hp, tp, up, vp);
+            int ix = hermIndex(t + tp, u + up, v + vp);
+            if ((tp + up + vp) & 1)
+                ix |= 0x8000;
+            rix[e] = (short)ix;
+        }
+        __syncthreads();
+    }
+
+    // Forward kernel: every mode except the derivative ones.
+    template <int LA, int LB, int LC, int LD, typename T>
+    __global__ void __launch_bounds__(Shape<LA, LB, LC, LD, T>::block)
+    eriKernel(QuartetArgs a)
+    {
+        using C = Cls<LA, LB, LC, LD>;
+        using S = Shape<LA, LB, LC, LD, T>;
+        constexpr int blk = C::SAB * C::SCD;
+        if constexpr (S::W == 0)
+        {
+            const long long stride = (long long)gridDim.x * blockDim.x;
+            for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < a.n_tasks; t += stride)
+            {
+                uint32_t ib, ik;
+                decodeTask(a, t, ib, ik);
+                T V[blk];
+                quartetThread<LA, LB, LC, LD, T>(a, ib, ik, V);
+                const int32_t *bi = a.bra.info + 8 * ib;
+                const int32_t *ki = a.ket.info + 8 * ik;
+                auto val = [&](int e) { return (double)V[e]; };
+                if (a.mode == kStore)
+                {
+#pragma unroll
+                    for (int m = 0; m < C::SA; m++)
+#pragma unroll
+                        for (int n = 0; n < C::SB; n++)
+#pragma unroll
+                            for (int k = 0; k < C::SC; k++)
+#pragma unroll
+                                for (int l = 0; l < C::SD; l++)
+                                    a.out[(size_t)t * blk + storeIndex<C::SA, C::SB, C::SC, C::SD>(a.flags, m, n, k, l)] =
+                                        (double)V[((m * C::SB + n) * C::SC + k) * C::SD + l];
+                }
+                else if (a.mode == kJK)
+                    digestJK<C::SA, C::SB, C::SC, C::SD, true>(a, quartetWeight(a, ib, ik), bi, ki, val, 0, 1);
+                else
+                    digestRI<C::SA, C::SB, C::SC, C::SD, true>(a, bi, ki, val, 0, 1);
+            }
+        }
+        else
+        {
+            extern __shared__ __align__(16) unsigned char smem[];
+            buildGroupTables<LA, LB, LC, LD, T>(smem);
+            T *vs = reinterpret_cast<T *>(smem + S::off_rx);
+            for (long long t = blockIdx.x; t < a.n_tasks; t += gridDim.x)
+            {
+                uint32_t ib, ik;
+                decodeTask(a, t, ib, ik);
+                T vals[S::IB];
+                quartetGroup<LA, LB, LC, LD, T>(a, ib, ik, smem, vals);
+                if (a.mode == kStore)
+                {
+#pragma unroll
+                    for (int k = 0; k < S::IB; k++)
+                    {
+                        const int e = threadIdx.x + S::G * k;
+                        if (e < blk)
+                        {
+                            const int mn = e / C::SCD, kt = e % C::SCD;
+                            a.out[(size_t)t * blk + storeIndex<C::SA, C::SB, C::SC, C::SD>(
+                                                        a.flags, mn / C::SB, mn % C::SB, kt / C::SD, kt % C::SD)] =
+                                (double)vals[k];
+                        }
+                    }
+                }
+                else
+                {
+#pragma unroll
+                    for (int k = 0; k < S::IB; k++)
+                    {
+                        const int e = threadIdx.x + S::G * k;
+                        if (e < blk)
+                            vs[e] = vals[k];
+                    }
+                    __syncthreads();
+                    const int32_t *bi = a.bra.info + 8 * ib;
+                    const int32_t *ki = a.ket.info + 8 * ik;
+                    auto val = [&](int e) { return (double)vs[e]; };
+                    if (a.mode == kJK)
+                        digestJK<C::SA, C::SB, C::SC, C::SD, false>(a, quartetWeight(a, ib, ik), bi, ki, val,
+                                                                    threadIdx.x, S::G);
+                    else
+                        digestRI<C::SA, C::SB, C::SC, C::SD, false>(a, bi, ki, val, threadIdx.x, S::G);
+                }
+                __syncthreads();
+            }
+        }
+    }
+}

@@ -1,0 +1,77 @@
+// Launch wrappers and the dispatch table that maps a quartet class to its kernel instantiation.
+#pragma once
+
+#include "eri_kernel.cuh"
+#include "eri_d1_kernel.cuh"
+
+#include <algorithm>
+
+namespace lible_b200
+{
+    using LaunchFn = cudaError_t (*)(const QuartetArgs &, cudaStream_t, int num_sms);
+
+    // Pair types in canonical order; a quartet class is instantiated with the larger type in the
+    // bra.  Index: la*(la+1)/2 + lb for la <= 3, then (4,0) -> 10, (5,0) -> 11.
+    constexpr int kNumPairTypes = 12;
+    inline int pairType(int la, int lb)
+    {
+        if (la <= 3)
+            return la * (la + 1) / 2 + lb;
+        return la == 4 ? 10 : 11;
+    }
+
+    template <int LA, int LB, int LC, int LD, typename T>
+    cudaError_t launchFwd(const QuartetArgs &a, cudaStream_t s, int num_sms)
+    {
+        using S = Shape<LA, LB, LC, LD, T>;
+        if (a.n_tasks <= 0)
+            return cudaSuccess;
+        auto kern = eriKernel<LA, LB, LC, LD, T>;
+        long long grid;
+        if constexpr (S::W == 0)
+            grid = std::min<long long>((a.n_tasks + S::block - 1) / S::block, (long long)num_sms * 64);
+        else
+        {
+            if (S::smem > 48 * 1024)
+            {
+                cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::smem);
+                if (e != cudaSuccess)
+                    return e;
+            }
+            int occ = 0;
+            cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, S::block, S::smem);
+            if (e != cudaSuccess)
+                return e;
+            grid = std::min<long long>(a.n_tasks, (long long)num_sms * std::max(occ, 1) * 4);
+        }
+        kern<<<(unsigned)grid, S::block, S::smem, s>>>(a);
+        return cudaGetLastError();
+    }
+
+    template <int LA, int LB, int LC, int LD>
+    cudaError_t launchD1(const QuartetArgs &a, cudaStream_t s, int num_sms)
+    {
+        using S = ShapeD1<LA, LB, LC, LD>;
+        if (a.n_tasks <= 0)
+            return cudaSuccess;
+        auto kern = eriD1Kernel<LA, LB, LC, LD>;
+        if (S::smem > 48 * 1024)
+        {
+            cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::smem);
+            if (e != cudaSuccess)
+                return e;
+        }
+        int occ = 0;
+        cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, S::G, S::smem);
+        if (e != cudaSuccess)
+            return e;
+        long long grid = std::min<long long>(a.n_tasks, (long long)num_sms * std::max(occ, 1) * 4);
+        kern<<<(unsigned)grid, S::G, S::smem, s>>>(a);
+        return cudaGetLastError();
+    }
+
+    // Implemented by the generated instantiation files.
+    LaunchFn lookupFwd64(int bra_type, int ket_type);
+    LaunchFn lookupFwd32(int bra_type, int ket_type);
+    LaunchFn lookupD1(int bra_type, int ket_type);
+}

@@ -1,0 +1,12 @@
+// Generated by gen_instances.py: class kernels with bra pair type (2,0).
+#include "../eri_launch.cuh"
+
+namespace lible_b200
+{
+    extern const LaunchFn k_d1_03[4] = {
+        &launchD1<2,0,0,0>,
+        &launchD1<2,0,1,0>,
+        &launchD1<2,0,1,1>,
+        &launchD1<2,0,2,0>,
+    };
+}

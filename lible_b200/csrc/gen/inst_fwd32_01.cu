@@ -1,0 +1,10 @@
+// Generated by gen_instances.py: class kernels with bra pair type (1,0).
+#include "../eri_launch.cuh"
+
+namespace lible_b200
+{
+    extern const LaunchFn k_fwd32_01[2] = {
+        &launchFwd<1,0,0,0,float>,
+        &launchFwd<1,0,1,0,float>,
+    };
+}

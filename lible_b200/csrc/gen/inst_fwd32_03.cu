@@ -1,0 +1,12 @@
+// Generated by gen_instances.py: class kernels with bra pair type (2,0).
+#include "../eri_launch.cuh"
+
+namespace lible_b200
+{
+    extern const LaunchFn k_fwd32_03[4] = {
+        &launchFwd<2,0,0,0,float>,
+        &launchFwd<2,0,1,0,float>,
+        &launchFwd<2,0,1,1,float>,
+        &launchFwd<2,0,2,0,float>,
+    };
+}

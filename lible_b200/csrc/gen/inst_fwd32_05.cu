@@ -1,0 +1,14 @@
+// Generated by gen_instances.py: class kernels with bra pair type (2,2).
+#include "../eri_launch.cuh"
+
+namespace lible_b200
+{
+    extern const LaunchFn k_fwd32_05[6] = {
+        &launchFwd<2,2,0,0,float>,
+        &launchFwd<2,2,1,0,float>,
+        &launchFwd<2,2,1,1,float>,
+        &launchFwd<2,2,2,0,float>,
+        &launchFwd<2,2,2,1,float>,
+        &launchFwd<2,2,2,2,float>,
+    };
+}

@@ -1,0 +1,9 @@
+// Generated by gen_instances.py: class kernels with bra pair type (0,0).
+#include "../eri_launch.cuh"
+
+namespace lible_b200
+{
+    extern const LaunchFn k_fwd64_00[1] = {
+        &launchFwd<0,0,0,0,double>,
+    };
+}

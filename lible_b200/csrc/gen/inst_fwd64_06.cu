@@ -1,0 +1,15 @@
+// Generated by gen_instances.py: class kernels with bra pair type (3,0).
+#include "../eri_launch.cuh"
+
+namespace lible_b200
+{
+    extern const LaunchFn k_fwd64_06[7] = {
+        &launchFwd<3,0,0,0,double>,
+        &launchFwd<3,0,1,0,double>,
+        &launchFwd<3,0,1,1,double>,
+        &launchFwd<3,0,2,0,double>,
+        &launchFwd<3,0,2,1,double>,
+        &launchFwd<3,0,2,2,double>,
+        &launchFwd<3,0,3,0,double>,
+    };
+}

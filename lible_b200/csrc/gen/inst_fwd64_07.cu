@@ -1,0 +1,16 @@
+// Generated by gen_instances.py: class kernels with bra pair type (3,1).
+#include "../eri_launch.cuh"
+
+namespace lible_b200
+{
+    extern const LaunchFn k_fwd64_07[8] = {
+        &launchFwd<3,1,0,0,double>,
+        &launchFwd<3,1,1,0,double>,
+        &launchFwd<3,1,1,1,double>,
+        &launchFwd<3,1,2,0,double>,
+        &launchFwd<3,1,2,1,double>,
+        &launchFwd<3,1,2,2,double>,
+        &launchFwd<3,1,3,0,double>,
+        &launchFwd<3,1,3,1,double>,
+    };
+}

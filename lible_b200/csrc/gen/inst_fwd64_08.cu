@@ -1,0 +1,17 @@
+// Generated by gen_instances.py: class kernels with bra pair type (3,2).
+#include "../eri_launch.cuh"
+
+namespace lible_b200
+{
+    extern const LaunchFn k_fwd64_08[9] = {
+        &launchFwd<3,2,0,0,double>,
+        &launchFwd<3,2,1,0,double>,
+        &launchFwd<3,2,1,1,double>,
+        &launchFwd<3,2,2,0,double>,
+        &launchFwd<3,2,2,1,double>,
+        &launchFwd<3,2,2,2,double>,
+        &launchFwd<3,2,3,0,double>,
+        &launchFwd<3,2,3,1,double>,
+        &launchFwd<3,2,3,2,double>,
+    };
+}

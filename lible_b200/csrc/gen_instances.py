@@ -1,0 +1,65 @@
+"""Writes the per-class kernel instantiation files under lible_b200/csrc/gen/.
+
+One file per (kernel kind, bra pair type) keeps each nvcc invocation small so the build can run
+in parallel.  A quartet class is always instantiated with the larger pair type in the bra; the
+host swaps bra and ket (and transposes the output) for the other orientation.
+"""
+import os
+
+PAIR_TYPES = [(0, 0), (1, 0), (1, 1), (2, 0), (2, 1), (2, 2), (3, 0), (3, 1), (3, 2), (3, 3), (4, 0), (5, 0)]
+FP32_MAX_TYPE = 5  # mixed precision is instantiated for the l <= 2 classes
+
+
+def kinds():
+    yield "fwd64", "launchFwd<{la},{lb},{lc},{ld},double>", len(PAIR_TYPES)
+    yield "fwd32", "launchFwd<{la},{lb},{lc},{ld},float>", FP32_MAX_TYPE + 1
+    yield "d1", "launchD1<{la},{lb},{lc},{ld}>", len(PAIR_TYPES)
+
+
+def main():
+    here = os.path.dirname(os.path.abspath(__file__))
+    out = os.path.join(here, "gen")
+    os.makedirs(out, exist_ok=True)
+    written = []
+    table = ['// Generated by gen_instances.py: lookup of class kernels.',
+             '#include "../eri_launch.cuh"', '', 'namespace lible_b200', '{']
+    for kind, tmpl, ntypes in kinds():
+        for bt in range(ntypes):
+            la, lb = PAIR_TYPES[bt]
+            entries = []
+            for kt in range(bt + 1):
+                lc, ld = PAIR_TYPES[kt]
+                entries.append("&" + tmpl.format(la=la, lb=lb, lc=lc, ld=ld))
+            name = f"inst_{kind}_{bt:02d}.cu"
+            body = ['// Generated by gen_instances.py: class kernels with bra pair type '
+                    f'({la},{lb}).', '#include "../eri_launch.cuh"', '', 'namespace lible_b200', '{',
+                    f'    extern const LaunchFn k_{kind}_{bt:02d}[{bt + 1}] = {{']
+            body += [f'        {e},' for e in entries]
+            body += ['    };', '}', '']
+            path = os.path.join(out, name)
+            text = "\n".join(body)
+            if not os.path.exists(path) or open(path).read() != text:
+                with open(path, "w") as fh:
+                    fh.write(text)
+            written.append(name)
+            table.append(f'    extern const LaunchFn k_{kind}_{bt:02d}[{bt + 1}];')
+        table.append(f'    static const LaunchFn *const k_{kind}[{ntypes}] = {{' +
+                     ", ".join(f"k_{kind}_{bt:02d}" for bt in range(ntypes)) + '};')
+    for kind, _, ntypes in kinds():
+        fn = {"fwd64": "lookupFwd64", "fwd32": "lookupFwd32", "d1": "lookupD1"}[kind]
+        table += [f'    LaunchFn {fn}(int bt, int kt)', '    {',
+                  f'        if (bt < 0 || bt >= {ntypes} || kt < 0 || kt > bt)',
+                  '            return nullptr;', f'        return k_{kind}[bt][kt];', '    }']
+    table += ['}', '']
+    path = os.path.join(out, "inst_table.cu")
+    text = "\n".join(table)
+    if not os.path.exists(path) or open(path).read() != text:
+        with open(path, "w") as fh:
+            fh.write(text)
+    written.append("inst_table.cu")
+    return [os.path.join(out, w) for w in written]
+
+
+if __name__ == "__main__":
+    for p in main():
+        print(p)

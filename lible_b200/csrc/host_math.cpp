@@ -1,0 +1,130 @@
+// Host-side tables: real solid-harmonic (spherical) transformation and the Boys-function grid.
+#include "engine.hpp"
+
+#include <stdexcept>
+
+namespace lible_b200
+{
+    namespace
+    {
+        double binom(int n, int k)
+        {
+            if (k < 0 || k > n)
+                return 0.0;
+            double r = 1.0;
+            for (int i = 1; i <= k; i++)
+                r = r * (n - k + i) / i;
+            return r;
+        }
+
+        double factorial(int n)
+        {
+            double r = 1.0;
+            for (int i = 2; i <= n; i++)
+                r *= i;
+            return r;
+        }
+    }
+
+    // Cartesian -> real solid harmonic coefficients for shell l, built from the closed form of
+    // Helgaker, Jorgensen, Olsen, Molecular Electronic-Structure Theory, eqs. 6.4.47-6.4.50:
+    //   S_lm = N_lm sum_t sum_u sum_v C^{lm}_{tuv} x^{2t+|m|-2(u+v)} y^{2(u+v)} z^{l-2t-|m|}
+    // with C = (-1)^{t+v-v_m} (1/4)^t binom(l,t) binom(l-t,|m|+t) binom(t,u) binom(|m|,2v),
+    // v_m = 0 (m >= 0) or 1/2 (m < 0), N_lm = sqrt(2 (l+|m|)! (l-|m|)! / 2^{delta_m0}) / (2^|m| l!).
+    // Rows are ordered m = 0, +1, -1, +2, -2, ... as in the reference
+    // (src/lible/ints/spherical_trafo.cpp:9-690, whose printed values are these to 14 decimals).
+    std::vector<SphTerm> sphericalTrafo(int l)
+    {
+        if (l < 0 || l > 8)
+            throw std::runtime_error("sphericalTrafo(): angular momentum out of range");
+        std::vector<SphTerm> out;
+        for (int row = 0; row < 2 * l + 1; row++)
+        {
+            int m = (row == 0) ? 0 : ((row % 2 == 1) ? (row + 1) / 2 : -(row / 2));
+            int am = m < 0 ? -m : m;
+            double nlm = std::sqrt(2.0 * factorial(l + am) * factorial(l - am) / (m == 0 ? 2.0 : 1.0)) /
+                         (std::pow(2.0, am) * factorial(l));
+            // accumulate per Cartesian component
+            std::vector<double> coef(ncart(l), 0.0);
+            for (int t = 0; t <= (l - am) / 2; t++)
+                for (int u = 0; u <= t; u++)
+                {
+                    // 2v runs over even values (m >= 0) or odd values (m < 0) up to |m|
+                    for (int two_v = (m < 0 ? 1 : 0); two_v <= am; two_v += 2)
+                    {
+                        int vv = two_v / 2;  // integer part; exponent of y uses 2(u+v)
+                        double sign_exp = t + (m < 0 ? (two_v - 1) / 2 : two_v / 2);
+                        double c = ((int)sign_exp % 2 == 0 ? 1.0 : -1.0) * std::pow(0.25, t) * binom(l, t) *
+                                   binom(l - t, am + t) * binom(t, u) * binom(am, two_v);
+                        int py = 2 * u + two_v;
+                        int px = 2 * t + am - 2 * u - two_v;
+                        int pz = l - 2 * t - am;
+                        (void)vv;
+                        if (px < 0 || py < 0 || pz < 0)
+                            continue;
+                        coef[cartIndex(py, pz)] += nlm * c;
+                    }
+                }
+            for (int c = 0; c < ncart(l); c++)
+                if (coef[c] != 0.0)
+                    out.push_back({row, c, coef[c]});
+        }
+        return out;
+    }
+
+    // Boys function F_n(x) on the grid x_k = 0.01 k, k = 0..3000, n = 0..kBoysCols-1.
+    // Top column by the convergent series F_N(x) = e^{-x} sum_i x^i / ((N+1/2)(N+3/2)...(N+i+1/2))
+    // stopped when a term falls below 1e-16, lower columns by downward recursion
+    // F_n = (2x F_{n+1} + e^{-x}) / (2n+1).  Same published method (Helgaker, Jorgensen, Olsen,
+    // eqs. 9.8.11-9.8.14) and constants as src/lible/ints/boys_function.cpp:40-69.
+    // Host evaluation with the same method as the device boysF<N>() (device_common.cuh).
+    void boysHost(int n, double x, const std::vector<double> &grid, double *F)
+    {
+        if (x > kBoysLargeX)
+        {
+            F[0] = 0.5 * std::sqrt(M_PI / x);
+            for (int k = 1; k <= n; k++)
+                F[k] = F[k - 1] * (k - 0.5) / x;
+            return;
+        }
+        const int iv = (int)(x / kBoysStep);
+        const double dx = x - iv * kBoysStep;
+        const double *row = grid.data() + (size_t)iv * kBoysCols + n;
+        double s = row[0], pk = 1.0, fact = 1.0;
+        for (int k = 1; k < 7; k++)
+        {
+            pk *= -dx;
+            fact *= k;
+            s += row[k] * pk / fact;
+        }
+        F[n] = s;
+        const double ex = std::exp(-x);
+        for (int k = n - 1; k >= 0; k--)
+            F[k] = (2.0 * x * F[k + 1] + ex) / (2 * k + 1);
+    }
+
+    std::vector<double> boysGrid()
+    {
+        std::vector<double> g((size_t)kBoysRows * kBoysCols);
+        const int nmax = kBoysCols - 1;
+        for (int k = 0; k < kBoysRows; k++)
+        {
+            double x = k * kBoysStep;
+            double term = 1.0 / (2.0 * nmax + 1.0);
+            double sum = term;
+            for (int i = 1;; i++)
+            {
+                term *= x / (nmax + 0.5 + i);
+                sum += term;
+                if (std::fabs(term) < 1e-16)
+                    break;
+            }
+            double ex = std::exp(-x);
+            double *row = &g[(size_t)k * kBoysCols];
+            row[nmax] = ex * sum;
+            for (int n = nmax - 1; n >= 0; n--)
+                row[n] = (2.0 * x * row[n + 1] + ex) / (2 * n + 1);
+        }
+        return g;
+    }
+}

@@ -1,0 +1,118 @@
+// Index conventions and small recurrences shared by host and device code.
+//
+// Conventions (identical to the reference, because they decide per-integral parity):
+//  * Cartesian order of a shell with angular momentum l: x-major descending,
+//    (l,0,0), (l-1,1,0), (l-1,0,1), ... (src/lible/ints/utils.cpp:33-47);
+//    index(i,j,k) = (j+k)(j+k+1)/2 + k (src/lible/ints/utils.hpp:27-31).
+//  * Hermite order for a pair of total angular momentum L: by n = t+u+v ascending, then the
+//    Cartesian order inside one n (src/lible/ints/utils.cpp:92-104, rints.hpp:58-69).  This order
+//    does not depend on L, so one "combined" index serves every class.
+//  * Spherical order inside a shell: m = 0, +1, -1, +2, -2, ... (src/lible/ints/spherical_trafo.cpp:13-60).
+#pragma once
+
+#include <cmath>
+#include <cstddef>
+
+#if defined(__CUDACC__)
+#define LB_HD __host__ __device__ __forceinline__
+#else
+#define LB_HD inline
+#endif
+
+namespace lible_b200
+{
+    constexpr int kMaxL = 5;          // highest shell angular momentum handled (aux h shells)
+    constexpr int kMaxLPair = 2 * kMaxL;
+    constexpr int kMaxLTotal = 14;    // highest L of a quartet (+1 for first derivatives)
+    constexpr int kBoysRows = 3001;   // grid x = 0, 0.01, ..., 30 (src/lible/ints/boys_function.hpp:112-122)
+    constexpr int kBoysCols = 24;     // F_n for n = 0 .. 23 (highest n needed: kMaxLTotal + 6)
+    constexpr double kBoysStep = 0.01;
+    constexpr double kBoysLargeX = 30.0;
+    constexpr double kPrimitiveThreshold = 1e-15;   // src/lible/ints/shell_pair_data.hpp:57
+    constexpr double kBohrToAngstrom = 0.5291772083; // src/lible/ints/defs.hpp:9
+    constexpr double kAngstromToBohr = 1.0 / kBohrToAngstrom;
+
+    LB_HD constexpr int nsph(int l) { return 2 * l + 1; }
+    LB_HD constexpr int ncart(int l) { return (l + 1) * (l + 2) / 2; }
+    // Number of Hermite functions with t+u+v <= l.
+    LB_HD constexpr int nherm(int l) { return l < 0 ? 0 : (l + 1) * (l + 2) * (l + 3) / 6; }
+    LB_HD constexpr int cartIndex(int j, int k) { return (j + k) * (j + k + 1) / 2 + k; }
+    // Combined Hermite index of (t, u, v).
+    LB_HD constexpr int hermIndex(int t, int u, int v)
+    {
+        return nherm(t + u + v - 1) + cartIndex(u, v);
+    }
+
+    // Hermite expansion coefficients of a primitive pair along one axis, McMurchie-Davidson
+    // recurrences (Helgaker, Jorgensen, Olsen, Molecular Electronic-Structure Theory, 9.5.6-9.5.7).
+    // E[i][j][t] is stored at E[(i * (lb + 1) + j) * (la + lb + 1) + t].  `one_o_2p` = 1/(2p),
+    // `pa` = P - A, `pb` = P - B, `kab` = exp(-mu (A-B)^2) on this axis.
+    // Follows src/lible/ints/ecoeffs.cpp:33-68.
+    LB_HD void hermiteE(int la, int lb, double one_o_2p, double pa, double pb, double kab, double *E)
+    {
+        const int nt = la + lb + 1;
+        for (int x = 0; x < (la + 1) * (lb + 1) * nt; x++)
+            E[x] = 0.0;
+        auto at = [&](int i, int j, int t) -> double & { return E[(i * (lb + 1) + j) * nt + t]; };
+        at(0, 0, 0) = kab;
+        for (int i = 1; i <= la; i++)
+            for (int t = 0; t <= i; t++)
+            {
+                double v = pa * at(i - 1, 0, t);
+                if (t > 0)
+                    v += one_o_2p * at(i - 1, 0, t - 1);
+                if (t + 1 <= i - 1)
+                    v += (t + 1) * at(i - 1, 0, t + 1);
+                at(i, 0, t) = v;
+            }
+        for (int j = 1; j <= lb; j++)
+            for (int i = 0; i <= la; i++)
+                for (int t = 0; t <= i + j; t++)
+                {
+                    double v = pb * at(i, j - 1, t);
+                    if (t > 0)
+                        v += one_o_2p * at(i, j - 1, t - 1);
+                    if (t + 1 <= i + j - 1)
+                        v += (t + 1) * at(i, j - 1, t + 1);
+                    at(i, j, t) = v;
+                }
+    }
+
+    // Derivative of E[i][j][t] with respect to the separation R = A - B on this axis, at fixed
+    // exponents.  With PA = -(b/p) R, PB = (a/p) R and K = exp(-mu R^2) the product rule applied
+    // to the recurrences above gives the same three-term form plus the derivative of PA / PB.
+    // Follows src/lible/ints/ecoeffs.cpp:70-111.
+    LB_HD void hermiteE1(int la, int lb, double a, double b, double rab, const double *E, double *E1)
+    {
+        const double p = a + b;
+        const double one_o_2p = 0.5 / p;
+        const double pa = -(b / p) * rab, pb = (a / p) * rab;
+        const int nt = la + lb + 1;
+        for (int x = 0; x < (la + 1) * (lb + 1) * nt; x++)
+            E1[x] = 0.0;
+        auto e0 = [&](int i, int j, int t) -> double { return E[(i * (lb + 1) + j) * nt + t]; };
+        auto at = [&](int i, int j, int t) -> double & { return E1[(i * (lb + 1) + j) * nt + t]; };
+        at(0, 0, 0) = -2.0 * (a * b / p) * rab * e0(0, 0, 0);
+        for (int i = 1; i <= la; i++)
+            for (int t = 0; t <= i; t++)
+            {
+                double v = pa * at(i - 1, 0, t) - (b / p) * e0(i - 1, 0, t);
+                if (t > 0)
+                    v += one_o_2p * at(i - 1, 0, t - 1);
+                if (t + 1 <= i - 1)
+                    v += (t + 1) * at(i - 1, 0, t + 1);
+                at(i, 0, t) = v;
+            }
+        for (int j = 1; j <= lb; j++)
+            for (int i = 0; i <= la; i++)
+                for (int t = 0; t <= i + j; t++)
+                {
+                    double v = pb * at(i, j - 1, t) + (a / p) * e0(i, j - 1, t);
+                    if (t > 0)
+                        v += one_o_2p * at(i, j - 1, t - 1);
+                    if (t + 1 <= i + j - 1)
+                        v += (t + 1) * at(i, j - 1, t + 1);
+                    at(i, j, t) = v;
+                }
+    }
+}

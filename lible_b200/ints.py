@@ -1,0 +1,333 @@
+"""Python mirror of the `lible::ints` calls this engine replaces (src/lible/ints/ints.hpp of the
+reference), running on the B200 through the C ABI of include/lible_b200.h.
+
+    s = Structure("cc-pvdz", [8, 1, 1], coords_angstrom)
+    V = eri4(s)                       # lible::ints::eri4          -> (N, N, N, N)
+    d = eri4Diagonal(s)               # lible::ints::eri4Diagonal  -> (N, N)
+    sp = shellPairData(True, s)       # lible::ints::shellPairData
+    k = ERI4Kernel(sp[1], sp[0]); b = k(0, 0, sp[1], sp[0])
+    J, K, st = jk(s, D)               # direct Coulomb / exchange (new)
+
+Array arguments may be numpy arrays (host) or CUDA torch tensors (device); outputs are numpy
+unless `out=` device tensors are given.  Errors raise LibleGpuError with the library's message.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+from ._lib import JKOpts, JKPlanInfo, JKStats, LibleGpuError, check, load
+
+BASIS_ROOT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "basis", "main")
+AUX_BASIS_ROOT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "basis", "aux")
+ANG_TO_BOHR = 1.0 / 0.5291772083
+
+
+def _ptr(a):
+    if a is None:
+        return None
+    if hasattr(a, "data_ptr"):
+        return ctypes.c_void_p(a.data_ptr())
+    return ctypes.c_void_p(a.ctypes.data)
+
+
+def _i32(x):
+    return np.ascontiguousarray(np.asarray(x, dtype=np.int32))
+
+
+def _f64(x):
+    return np.ascontiguousarray(np.asarray(x, dtype=np.float64))
+
+
+class Structure:
+    """lible::ints::Structure (src/lible/ints/structure.hpp:18-62).
+
+    `basis_set` is a basis name (read from `basis_root`, default the shipped subset) or a
+    basis_atoms list: one list per atom of (l, exps, coeffs) shells.  Coordinates are Angstrom
+    unless units="bohr"."""
+
+    def __init__(self, basis_set, atomic_nrs, coords, basis_set_aux=None, *, units="angstrom",
+                 basis_root=None, aux_root=None, device=0):
+        self._lib = load()
+        ctx = ctypes.c_void_p()
+        check(None, self._lib.lible_gpu_create(device, ctypes.byref(ctx)))
+        self._ctx = ctx
+        Z = _i32(atomic_nrs)
+        xyz = _f64(coords).reshape(-1, 3)
+        if len(Z) != len(xyz):
+            raise ValueError("number of atomic numbers does not match the number of coordinates")
+        u = 0 if units == "angstrom" else 1
+        if isinstance(basis_set, str):
+            rc = self._lib.lible_gpu_set_structure_named(
+                ctx, (basis_root or BASIS_ROOT).encode(), basis_set.encode(),
+                (aux_root or AUX_BASIS_ROOT).encode(), basis_set_aux.encode() if basis_set_aux else None,
+                len(Z), _ptr(Z), _ptr(xyz), u)
+        else:
+            main = self._flatten(basis_set)
+            aux = self._flatten(basis_set_aux) if basis_set_aux is not None else (None,) * 5
+            self._keep = (main, aux)
+            rc = self._lib.lible_gpu_set_structure(ctx, len(Z), _ptr(Z), _ptr(xyz), u, *[_ptr(x) for x in main],
+                                                   *[_ptr(x) for x in aux])
+        check(ctx, rc)
+        nao, naux, nat, maxl = ctypes.c_longlong(), ctypes.c_longlong(), ctypes.c_int(), ctypes.c_int()
+        check(ctx, self._lib.lible_gpu_dims(ctx, ctypes.byref(nao), ctypes.byref(naux), ctypes.byref(nat),
+                                            ctypes.byref(maxl)))
+        self.nao, self.naux, self.n_atoms, self.max_l = nao.value, naux.value, nat.value, maxl.value
+        self.use_ri = basis_set_aux is not None
+
+    @staticmethod
+    def _flatten(basis_atoms):
+        nsh, ls, nps, ex, co = [], [], [], [], []
+        for atom in basis_atoms:
+            nsh.append(len(atom))
+            for (l, exps, coeffs) in atom:
+                ls.append(l)
+                nps.append(len(exps))
+                ex.extend(exps)
+                co.extend(coeffs)
+        return _i32(nsh), _i32(ls), _i32(nps), _f64(ex), _f64(co)
+
+    def __del__(self):
+        ctx = getattr(self, "_ctx", None)
+        if ctx is not None and ctx.value:
+            self._lib.lible_gpu_destroy(ctx)
+            self._ctx = None
+
+    @property
+    def ctx(self):
+        return self._ctx
+
+    def getDimAO(self):
+        return self.nao
+
+    def getDimAOAux(self):
+        return self.naux
+
+    def getNAtoms(self):
+        return self.n_atoms
+
+    def getMaxL(self):
+        return self.max_l
+
+    def getUseRI(self):
+        return self.use_ri
+
+
+def _call(s, name, *args):
+    check(s.ctx, getattr(load(), name)(s.ctx, *args))
+
+
+def eri4(structure, out=None):
+    n = structure.nao
+    out = np.empty((n, n, n, n)) if out is None else out
+    _call(structure, "lible_gpu_eri4", _ptr(out))
+    return out
+
+
+def eri4Diagonal(structure):
+    n = structure.nao
+    out = np.empty((n, n))
+    _call(structure, "lible_gpu_eri4_diagonal", _ptr(out))
+    return out
+
+
+def eri3(structure, out=None):
+    out = np.empty((structure.nao, structure.nao, structure.naux)) if out is None else out
+    _call(structure, "lible_gpu_eri3", _ptr(out))
+    return out
+
+
+def eri2(structure, out=None):
+    out = np.empty((structure.naux, structure.naux)) if out is None else out
+    _call(structure, "lible_gpu_eri2", _ptr(out))
+    return out
+
+
+def eri2Diagonal(structure):
+    out = np.empty(structure.naux)
+    _call(structure, "lible_gpu_eri2_diagonal", _ptr(out))
+    return out
+
+
+class ShellPairData:
+    """Handle of one shell-pair class of shellPairData(use_symm, structure): (la, lb), number of
+    pairs and primitive pairs (src/lible/ints/shell_pair_data.hpp:50-120)."""
+
+    def __init__(self, structure, use_symm, index, la, lb, n_pairs, n_ppairs):
+        self.structure, self.uses_symm, self.index = structure, use_symm, index
+        self.la_, self.lb_, self.n_pairs_, self.n_ppairs_ = la, lb, n_pairs, n_ppairs
+
+    def getLPair(self):
+        return self.la_, self.lb_
+
+
+class ShellData:
+    """Handle of one auxiliary shell class of shellDataAux(structure) (shell_pair_data.hpp:8-45)."""
+
+    def __init__(self, structure, index, l, n_shells):
+        self.structure, self.index, self.l_, self.n_shells_ = structure, index, l, n_shells
+
+
+def shellPairData(use_symm, structure):
+    n = ctypes.c_int()
+    _call(structure, "lible_gpu_pair_classes", int(bool(use_symm)), ctypes.byref(n), None, None, None)
+    ls = np.zeros(2 * n.value, np.int32)
+    npairs = np.zeros(n.value, np.int64)
+    nppairs = np.zeros(n.value, np.int64)
+    _call(structure, "lible_gpu_pair_classes", int(bool(use_symm)), ctypes.byref(n), _ptr(ls), _ptr(npairs),
+          _ptr(nppairs))
+    return [ShellPairData(structure, bool(use_symm), i, int(ls[2 * i]), int(ls[2 * i + 1]), int(npairs[i]),
+                          int(nppairs[i])) for i in range(n.value)]
+
+
+def shellDataAux(structure):
+    if not structure.use_ri:
+        raise LibleGpuError(4, "shellDataAux(): RI approximation is not enabled!")
+    n = ctypes.c_int()
+    _call(structure, "lible_gpu_aux_classes", ctypes.byref(n), None, None)
+    ls = np.zeros(n.value, np.int32)
+    nsh = np.zeros(n.value, np.int64)
+    _call(structure, "lible_gpu_aux_classes", ctypes.byref(n), _ptr(ls), _ptr(nsh))
+    return [ShellData(structure, i, int(ls[i]), int(nsh[i])) for i in range(n.value)]
+
+
+def _nsph(l):
+    return 2 * l + 1
+
+
+class _Kernel:
+    _fn = None
+    _nblk = 1
+
+    def _dims(self):
+        raise NotImplementedError
+
+    def batch(self, idx):
+        """Evaluates many (i, j) index pairs at once: idx is (n, 2); returns (n, *block_shape)."""
+        idx = np.ascontiguousarray(np.asarray(idx, dtype=np.uint32).reshape(-1, 2))
+        shape = self._dims()
+        out = np.empty((len(idx), self._nblk) + shape) if self._nblk > 1 else np.empty((len(idx),) + shape)
+        self._run(len(idx), idx, out)
+        return out
+
+    def __call__(self, i, j, *_):
+        r = self.batch([[i, j]])[0]
+        return list(r) if self._nblk > 1 else r
+
+
+class ERI4Kernel(_Kernel):
+    """lible::ints::ERI4Kernel (src/lible/ints/twoel/eri_kernels.hpp:60-76)."""
+    _fn, _nblk = "lible_gpu_eri4_batch", 1
+
+    def __init__(self, sp_ab, sp_cd):
+        self.ab, self.cd, self.s = sp_ab, sp_cd, sp_ab.structure
+
+    def _dims(self):
+        return (_nsph(self.ab.la_), _nsph(self.ab.lb_), _nsph(self.cd.la_), _nsph(self.cd.lb_))
+
+    def _run(self, n, idx, out):
+        _call(self.s, self._fn, int(self.ab.uses_symm), self.ab.index, self.cd.index, n, _ptr(idx), _ptr(out))
+
+
+class ERI4D1Kernel(ERI4Kernel):
+    """lible::ints::ERI4D1Kernel (eri_kernels.hpp:114-132): 12 blocks [A, B, C, D] x [x, y, z]."""
+    _fn, _nblk = "lible_gpu_eri4d1_batch", 12
+
+
+class ERI3Kernel(_Kernel):
+    """lible::ints::ERI3Kernel (eri_kernels.hpp:78-94)."""
+    _fn, _nblk = "lible_gpu_eri3_batch", 1
+
+    def __init__(self, sp_ab, sh_c):
+        self.ab, self.c, self.s = sp_ab, sh_c, sp_ab.structure
+
+    def _dims(self):
+        return (_nsph(self.ab.la_), _nsph(self.ab.lb_), _nsph(self.c.l_))
+
+    def _run(self, n, idx, out):
+        _call(self.s, self._fn, int(self.ab.uses_symm), self.ab.index, self.c.index, n, _ptr(idx), _ptr(out))
+
+
+class ERI3D1Kernel(ERI3Kernel):
+    """lible::ints::ERI3D1Kernel (eri_kernels.hpp:134-151): 9 blocks [A, B, C] x [x, y, z]."""
+    _fn, _nblk = "lible_gpu_eri3d1_batch", 9
+
+
+class ERI2Kernel(_Kernel):
+    """lible::ints::ERI2Kernel (eri_kernels.hpp:96-112)."""
+    _fn, _nblk = "lible_gpu_eri2_batch", 1
+
+    def __init__(self, sh_a, sh_b):
+        self.a, self.b, self.s = sh_a, sh_b, sh_a.structure
+
+    def _dims(self):
+        return (_nsph(self.a.l_), _nsph(self.b.l_))
+
+    def _run(self, n, idx, out):
+        _call(self.s, self._fn, self.a.index, self.b.index, n, _ptr(idx), _ptr(out))
+
+
+class ERI2D1Kernel(ERI2Kernel):
+    """lible::ints::ERI2D1Kernel (eri_kernels.hpp:153-169): 6 blocks [A, B] x [x, y, z]."""
+    _fn, _nblk = "lible_gpu_eri2d1_batch", 6
+
+
+def _opts(schwarz, precision, fp32_threshold):
+    return JKOpts(float(schwarz), float(fp32_threshold), 1 if precision in (1, "mixed") else 0)
+
+
+def jk(structure, D, schwarz=1e-12, precision="fp64", fp32_threshold=1e-4, J=None, K=None):
+    """Direct Coulomb and exchange matrices for a symmetric density D (N x N)."""
+    n = structure.nao
+    Dh = D if hasattr(D, "data_ptr") else _f64(D)
+    J = np.empty((n, n)) if J is None else J
+    K = np.empty((n, n)) if K is None else K
+    st = JKStats()
+    opts = _opts(schwarz, precision, fp32_threshold)
+    _call(structure, "lible_gpu_jk", _ptr(Dh), _ptr(J), _ptr(K), ctypes.byref(opts), ctypes.byref(st))
+    return J, K, {"n_quartets": st.n_quartets, "n_fp32": st.n_fp32, "n_launches": st.n_launches}
+
+
+def jk_energy_forward(structure, D, schwarz=1e-12, precision="fp64", fp32_threshold=1e-4):
+    """E = 1/2 Tr(DJ) - 1/4 Tr(DK)."""
+    e = ctypes.c_double()
+    opts = _opts(schwarz, precision, fp32_threshold)
+    _call(structure, "lible_gpu_jk_energy_forward", _ptr(_f64(D)), ctypes.byref(opts), ctypes.byref(e), None, None)
+    return e.value
+
+
+def jk_energy_backward(structure, D):
+    """dE/dR of E = 1/2 Tr(DJ) - 1/4 Tr(DK), shape (n_atoms, 3), in Eh/bohr."""
+    g = np.empty((structure.n_atoms, 3))
+    _call(structure, "lible_gpu_jk_energy_backward", _ptr(_f64(D)), _ptr(g))
+    return g
+
+
+def rij(structure, D):
+    """RI-J: returns J, gamma, d with (P|Q) d = gamma."""
+    n, na = structure.nao, structure.naux
+    J, g, d = np.empty((n, n)), np.empty(na), np.empty(na)
+    _call(structure, "lible_gpu_rij", _ptr(_f64(D)), _ptr(J), _ptr(g), _ptr(d))
+    return J, g, d
+
+
+def jk_plan(structure, schwarz=1e-12, precision="fp64", fp32_threshold=1e-4):
+    """Quartet / primitive-quartet counts and algorithmic FLOPs of one J/K build with these options."""
+    info = JKPlanInfo()
+    opts = _opts(schwarz, precision, fp32_threshold)
+    _call(structure, "lible_gpu_jk_plan", ctypes.byref(opts), ctypes.byref(info))
+    return {k: getattr(info, k) for k, _ in JKPlanInfo._fields_}
+
+
+def stream_handle(structure):
+    """The cudaStream_t the structure's calls run on (integer handle)."""
+    p = ctypes.c_void_p()
+    _call(structure, "lible_gpu_stream", ctypes.byref(p))
+    return p.value or 0
+
+
+def fp64_peak(structure):
+    """Measured (DFMA, DMMA) FP64 TFLOP/s of the structure's GPU."""
+    a, b = ctypes.c_double(), ctypes.c_double()
+    _call(structure, "lible_gpu_fp64_peak", ctypes.byref(a), ctypes.byref(b))
+    return a.value, b.value

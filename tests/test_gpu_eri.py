@@ -1,0 +1,188 @@
+"""Parity of the CUDA path (through the C ABI) with the reference's own CPU integrals.
+
+Tolerances: 1e-12 absolute per integral for FP64 integrals (the bar the reference's tests use,
+test/tests_ints.cpp:15, applied element-wise against the reference's own output).  The reference's
+golden sums (sum of |values| over whole tensors of up to 3.6e6 elements, test/tests_ints.cpp) are
+checked to 1e-13 relative: last-bit differences of individual integrals, which any independent
+implementation has, accumulate to ~1e-14 relative in such a sum."""
+import numpy as np
+import pytest
+
+from lible_b200 import ints as L
+from lible_b200.workloads import WATER_BOHR, WATER_Z, random_density, water_cluster
+from oracle import ref as R
+
+pytestmark = pytest.mark.gpu
+
+O3_ANG = [[0, 0, 0], [0, 1, 1], [0, 0, 2]]
+H2O_ANG = [[0.0, 0.0, 0.0], [0.757, 0.586, 0.0], [-0.757, 0.586, 0.0]]
+
+
+def golden(value, expected):
+    return abs(value - expected) <= 1e-13 * abs(expected)
+
+
+def seqsum(x):
+    """Sum of |x| in storage order, accumulated sequentially like the reference's tests."""
+    return float(np.cumsum(np.abs(np.asarray(x)).ravel())[-1])
+
+
+@pytest.fixture(scope="module")
+def water_dz():
+    return L.Structure("cc-pvdz", WATER_Z, WATER_BOHR, units="bohr")
+
+
+def test_eri4_water_ccpvdz_elementwise(water_dz):
+    V = L.eri4(water_dz)
+    ref = R.RefStructure("cc-pvdz", WATER_Z, WATER_BOHR).eri4()
+    assert V.shape == (24,) * 4
+    assert np.abs(V - ref).max() <= 1e-12
+
+
+def test_eri4_golden_o3_def2svp():
+    s = L.Structure("def2-svp", [8, 8, 8], O3_ANG)
+    V = L.eri4(s)
+    assert golden(seqsum(V), 8246.711763196334)
+    ref = R.RefStructure("def2-svp", [8, 8, 8], O3_ANG, units="angstrom").eri4()
+    assert np.abs(V - ref).max() <= 1e-12
+
+
+def test_eri4_diagonal_golden_o3_def2tzvp():
+    s = L.Structure("def2-tzvp", [8, 8, 8], O3_ANG)
+    d = L.eri4Diagonal(s)
+    assert golden(seqsum(d), 306.806419250122)
+    ref = R.RefStructure("def2-tzvp", [8, 8, 8], O3_ANG, units="angstrom").eri4_diagonal()
+    assert np.abs(d - ref).max() <= 1e-12
+
+
+def test_eri3_golden_o3():
+    s = L.Structure("def2-tzvp", [8, 8, 8], O3_ANG, "def2-qzvp-rifit")
+    v = L.eri3(s)
+    assert golden(seqsum(v), 25854.105851585416531)
+    ref = R.RefStructure("def2-tzvp", [8, 8, 8], O3_ANG, aux="def2-qzvp-rifit", units="angstrom").eri3()
+    assert np.abs(v - ref).max() <= 1e-12
+
+
+def test_eri2_golden_h2o():
+    s = L.Structure("def2-svp", [8, 1, 1], H2O_ANG, "def2-qzvp-rifit")
+    v = L.eri2(s)
+    assert golden(seqsum(v), 8801.334703460838)
+    ref = R.RefStructure("def2-svp", [8, 1, 1], H2O_ANG, aux="def2-qzvp-rifit", units="angstrom").eri2()
+    assert np.abs(v - ref).max() <= 1e-12
+
+
+def test_eri2_diagonal_golden_h2o():
+    s = L.Structure("def2-svp", [8, 1, 1], H2O_ANG, "def2-universal-jkfit")
+    d = L.eri2Diagonal(s)
+    assert golden(seqsum(d), 830.788976485982)
+
+
+def test_ri_required_errors():
+    s = L.Structure("def2-svp", [8, 1, 1], H2O_ANG)
+    with pytest.raises(L.LibleGpuError) as e:
+        L.eri3(s)
+    assert e.value.code == 4
+
+
+def _deploy4(s, use_symm, d1=False):
+    sp = L.shellPairData(use_symm, s)
+    total = 0.0
+    parts = []
+    for a in sp:
+        for c in sp:
+            k = (L.ERI4D1Kernel if d1 else L.ERI4Kernel)(a, c)
+            idx = [(i, j) for i in range(a.n_pairs_) for j in range(c.n_pairs_)]
+            if idx:
+                parts.append(k.batch(idx).ravel())
+    return seqsum(np.concatenate(parts))
+
+
+def test_deploy_eri4_kernel_golden():
+    s = L.Structure("def2-svp", [8, 8, 8], O3_ANG)
+    assert golden(_deploy4(s, False), 8246.711763197583)
+
+
+def test_deploy_eri4d1_kernel_golden():
+    s = L.Structure("def2-svp", [8, 8, 8], O3_ANG)
+    assert golden(_deploy4(s, True, d1=True), 30546.780073140635)
+
+
+def test_eri4_class_batches_elementwise():
+    s = L.Structure("def2-svp", [8, 8, 8], O3_ANG)
+    r = R.RefStructure("def2-svp", [8, 8, 8], O3_ANG, units="angstrom")
+    for use_symm in (False, True):
+        sp = L.shellPairData(use_symm, s)
+        assert [(x.la_, x.lb_, x.n_pairs_, x.n_ppairs_) for x in sp] == r.pair_classes(use_symm)
+        for a in sp:
+            for c in sp:
+                idx = [(i, j) for i in range(a.n_pairs_) for j in range(c.n_pairs_)]
+                got = L.ERI4Kernel(a, c).batch(idx).reshape(a.n_pairs_, c.n_pairs_, -1)
+                want = r.eri4_class(use_symm, a.index, c.index).reshape(a.n_pairs_, c.n_pairs_, -1)
+                assert np.abs(got - want).max() <= 1e-12, (a.getLPair(), c.getLPair())
+
+
+def test_eri4d1_class_batches_elementwise():
+    s = L.Structure("def2-svp", [8, 1, 1], H2O_ANG)
+    r = R.RefStructure("def2-svp", [8, 1, 1], H2O_ANG, units="angstrom")
+    sp = L.shellPairData(True, s)
+    for a in sp:
+        for c in sp:
+            idx = [(i, j) for i in range(a.n_pairs_) for j in range(c.n_pairs_)]
+            got = L.ERI4D1Kernel(a, c).batch(idx).reshape(a.n_pairs_, c.n_pairs_, 12, -1)
+            want = r.eri4_class(True, a.index, c.index, d1=True).reshape(a.n_pairs_, c.n_pairs_, 12, -1)
+            assert np.abs(got - want).max() <= 1e-11, (a.getLPair(), c.getLPair())
+
+
+def test_deploy_eri3_eri2_golden():
+    s = L.Structure("def2-svp", [8, 8, 8], O3_ANG, "def2-universal-jkfit")
+    sp = L.shellPairData(False, s)
+    aux = L.shellDataAux(s)
+    parts3, parts3d, parts2, parts2d = [], [], [], []
+    for a in sp:
+        for c in aux:
+            idx = [(i, j) for i in range(a.n_pairs_) for j in range(c.n_shells_)]
+            parts3.append(L.ERI3Kernel(a, c).batch(idx).ravel())
+            parts3d.append(L.ERI3D1Kernel(a, c).batch(idx).ravel())
+    for a in aux:
+        for b in aux:
+            idx = [(i, j) for i in range(a.n_shells_) for j in range(b.n_shells_)]
+            parts2.append(L.ERI2Kernel(a, b).batch(idx).ravel())
+            parts2d.append(L.ERI2D1Kernel(a, b).batch(idx).ravel())
+    assert golden(seqsum(np.concatenate(parts3)), 12350.130354189232)
+    assert golden(seqsum(np.concatenate(parts2)), 21014.512841176023)
+    assert golden(seqsum(np.concatenate(parts3d)), 78466.360848033844)
+    assert golden(seqsum(np.concatenate(parts2d)), 39949.218421684251)
+
+
+def test_jk_water_dimer_vs_reference_kernels():
+    Z, xyz, rng = water_cluster(2, seed=7)
+    s = L.Structure("cc-pvdz", Z, xyz, units="bohr")
+    D = random_density(s.nao, 10, rng)
+    r = R.RefStructure("cc-pvdz", Z, xyz)
+    J, K, st = L.jk(s, D, schwarz=0.0)
+    Jr, Kr, nq, _ = r.jk(D, schwarz=0.0)
+    assert st["n_quartets"] == nq
+    assert np.abs(J - Jr).max() <= 1e-11
+    assert np.abs(K - Kr).max() <= 1e-11
+    J2, K2, st2 = L.jk(s, D, schwarz=1e-12)
+    assert np.abs(J2 - Jr).max() <= 1e-9
+    assert np.abs(K2 - Kr).max() <= 1e-9
+
+
+def test_jk_gradient_vs_reference_and_fd():
+    Z, xyz, rng = water_cluster(2, seed=3)
+    s = L.Structure("cc-pvdz", Z, xyz, units="bohr")
+    D = random_density(s.nao, 10, rng)
+    g = L.jk_energy_backward(s, D)
+    gr = R.RefStructure("cc-pvdz", Z, xyz).jk_grad(D)
+    assert np.abs(g - gr).max() <= 1e-10
+    # central finite differences of the forward energy on two coordinates
+    h = 1e-4
+    for atom, x in [(0, 0), (4, 2)]:
+        e = []
+        for sgn in (1, -1):
+            c = xyz.copy()
+            c[atom, x] += sgn * h
+            e.append(L.jk_energy_forward(L.Structure("cc-pvdz", Z, c, units="bohr"), D, schwarz=0.0))
+        fd = (e[0] - e[1]) / (2 * h)
+        assert abs(fd - g[atom, x]) <= 1e-6

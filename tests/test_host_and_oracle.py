@@ -1,0 +1,149 @@
+"""CPU tests: the oracle against the reference's golden vectors and the reference itself, the
+engine's host-side set-up against the reference, and the C ABI's exported symbol set.
+
+Golden sums are the reference's own test constants (test/tests_ints.cpp), compared at 1e-13
+relative (see tests/test_gpu_eri.py for why); element-wise comparisons are absolute."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+from lible_b200 import _lib
+from lible_b200.workloads import WATER_BOHR, WATER_Z, random_density, water_cluster
+from oracle import port, ref
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+O3_BOHR = np.array([[0, 0, 0], [0, 1, 1], [0, 0, 2]], float) / 0.5291772083
+needs_ref = pytest.mark.skipif(not ref.available(), reason="reference library not built")
+
+
+def seqsum(x):
+    return float(np.cumsum(np.abs(np.asarray(x)).ravel())[-1])
+
+
+def test_capi_exports_every_declared_symbol():
+    header = open(os.path.join(ROOT, "include", "lible_b200.h")).read()
+    declared = set(re.findall(r"\b(lible_(?:gpu|host)_\w+)\s*\(", header))
+    assert len(declared) >= 30
+    lib = ctypes.CDLL(_lib.LIB_PATH)
+    missing = [n for n in sorted(declared) if not hasattr(lib, n)]
+    assert not missing, missing
+    # and the Python mirror declares a signature for each of them
+    assert declared - {"lible_gpu_last_error"} <= set(_lib.SIGNATURES)
+
+
+def test_port_boys_golden():
+    # calcBoysF(n=5, x=2.5), sum of values: test/tests_ints.cpp:1296-1313
+    assert abs(seqsum(port.boys(5, 2.5)) - 0.728561124180) < 1e-12
+
+
+def test_host_boys_matches_port_and_golden():
+    lib = _lib.load()
+    for n, x in [(5, 2.5), (0, 0.0), (8, 1e-3), (12, 17.3), (13, 29.999), (4, 31.0), (10, 250.0)]:
+        F = np.empty(n + 1)
+        assert lib.lible_host_boys(n, x, F.ctypes.data) == 0
+        assert np.allclose(F, port.boys(n, x), rtol=1e-14, atol=1e-300)
+    F = np.empty(6)
+    lib.lible_host_boys(5, 2.5, F.ctypes.data)
+    assert abs(seqsum(F) - 0.728561124180) < 1e-12
+
+
+def test_host_spherical_trafo_golden():
+    # sphericalTrafo(8): sum |val| + i + j = 7005.923248093791 (test/tests_ints.cpp:856-871)
+    lib = _lib.load()
+    n = ctypes.c_int(1000)
+    rows, carts, vals = np.zeros(1000, np.int32), np.zeros(1000, np.int32), np.zeros(1000)
+    assert lib.lible_host_spherical_trafo(8, ctypes.byref(n), rows.ctypes.data, carts.ctypes.data,
+                                          vals.ctypes.data) == 0
+    k = n.value
+    assert abs(np.sum(np.abs(vals[:k]) + rows[:k] + carts[:k]) - 7005.923248093791) < 1e-9
+
+
+def test_host_shell_norms_normalise_overlap():
+    # A normalised contracted s shell: cc-pVDZ O 1s coefficients (norm close to 1 by construction)
+    lib = _lib.load()
+    atoms = port.read_basis("cc-pvdz", [8])[0]
+    for l, e, c in atoms:
+        norms = np.empty(2 * l + 1)
+        assert lib.lible_host_shell_norms(l, len(e), np.asarray(e).ctypes.data, np.asarray(c).ctypes.data,
+                                          norms.ctypes.data) == 0
+        assert np.all(norms > 0.5) and np.all(norms < 3.0)
+
+
+@needs_ref
+@pytest.mark.parametrize("basis,Z,xyz", [("def2-svp", [8, 8, 8], O3_BOHR), ("cc-pvtz", WATER_Z, WATER_BOHR)])
+def test_host_pair_classes_match_reference(basis, Z, xyz):
+    lib = _lib.load()
+    r = ref.RefStructure(basis, Z, xyz)
+    for use_symm in (0, 1):
+        n = ctypes.c_int()
+        ls = np.zeros(64, np.int32)
+        npr, npp = np.zeros(32, np.int64), np.zeros(32, np.int64)
+        Zs = np.asarray(Z, np.int32)
+        x = np.ascontiguousarray(xyz, float)
+        assert lib.lible_host_pair_classes(os.path.join(ROOT, "lible_b200", "basis", "main").encode(), basis.encode(),
+                                           len(Z), Zs.ctypes.data, x.ctypes.data, 1, use_symm, ctypes.byref(n),
+                                           ls.ctypes.data, npr.ctypes.data, npp.ctypes.data) == 0
+        mine = [(int(ls[2 * i]), int(ls[2 * i + 1]), int(npr[i]), int(npp[i])) for i in range(n.value)]
+        assert mine == r.pair_classes(bool(use_symm))
+
+
+@needs_ref
+def test_reference_golden_sums():
+    r = ref.RefStructure("def2-svp", [8, 8, 8], O3_BOHR)
+    assert abs(seqsum(r.eri4()) - 8246.711763196334) < 1e-12
+    assert abs(r.deploy_sum(0) - 8246.711763197583) < 1e-12
+
+
+def test_port_golden_eri4_o3():
+    V = port.PortMolecule("def2-svp", [8, 8, 8], O3_BOHR).eri4()
+    assert abs(seqsum(V) - 8246.711763196334) <= 1e-13 * 8246.711763196334
+
+
+@needs_ref
+def test_port_matches_reference_elementwise():
+    V = port.PortMolecule("cc-pvdz", WATER_Z, WATER_BOHR).eri4()
+    Vr = ref.RefStructure("cc-pvdz", WATER_Z, WATER_BOHR).eri4()
+    assert np.abs(V - Vr).max() <= 1e-12
+
+
+@needs_ref
+def test_port_jk_and_gradient_match_reference():
+    Z, xyz, rng = water_cluster(2, seed=5)
+    D = random_density(48, 10, rng)
+    m = port.PortMolecule("cc-pvdz", Z, xyz)
+    r = ref.RefStructure("cc-pvdz", Z, xyz)
+    J, K, nq = m.jk(D, 1e-12)
+    Jr, Kr, nqr, _ = r.jk(D, 1e-12)
+    assert nq == nqr
+    assert np.abs(J - Jr).max() <= 1e-11 and np.abs(K - Kr).max() <= 1e-11
+    assert np.abs(m.jk_grad(D) - r.jk_grad(D)).max() <= 1e-11
+
+
+def test_port_gradient_matches_finite_differences():
+    Z, xyz, rng = water_cluster(1, seed=9)
+    D = random_density(24, 5, rng)
+    g = port.PortMolecule("cc-pvdz", Z, xyz).jk_grad(D)
+    h = 1e-4
+
+    def energy(c):
+        J, K, _ = port.PortMolecule("cc-pvdz", Z, c).jk(D, 0.0)
+        return float(np.sum(D * (0.5 * J - 0.25 * K)))
+
+    for atom, x in [(0, 1), (2, 0)]:
+        cp, cm = xyz.copy(), xyz.copy()
+        cp[atom, x] += h
+        cm[atom, x] -= h
+        assert abs((energy(cp) - energy(cm)) / (2 * h) - g[atom, x]) <= 1e-6
+
+
+def test_water_cluster_generator_is_seeded():
+    Z1, x1, _ = water_cluster(32, 2024)
+    Z2, x2, _ = water_cluster(32, 2024)
+    assert Z1 == Z2 and np.array_equal(x1, x2)
+    assert len(Z1) == 96
+    # rigid waters: O-H distances preserved
+    d = np.linalg.norm(x1[1::3] - x1[0::3], axis=1)
+    assert np.allclose(d, np.linalg.norm([1.4305, 1.1093, 0.0]))
