@@ -135,6 +135,11 @@ typedef struct lible_gpu_jk_plan_info {
 
 int lible_gpu_jk_plan(lible_gpu_ctx *ctx, const lible_gpu_jk_opts *opts, lible_gpu_jk_plan_info *info);
 
+/* Per class pair of that plan, in launch order: ls[4*i..4*i+3] = (la, lb, lc, ld), quartets in
+ * FP64 / FP32, primitive quartets, algorithmic FLOPs.  Call with ls == NULL to get *n only. */
+int lible_gpu_jk_plan_classes(lible_gpu_ctx *ctx, const lible_gpu_jk_opts *opts, int *n, int *ls,
+                              long long *n64, long long *n32, double *n_prim, double *flops);
+
 /* The context's CUDA stream (cudaStream_t), for callers that time or order work around the calls. */
 int lible_gpu_stream(lible_gpu_ctx *ctx, void **stream);
 

@@ -61,6 +61,7 @@ SIGNATURES = {
     "lible_gpu_rij": [P, P, P, P, P],
     "lible_gpu_jk_plan": [P, ctypes.POINTER(JKOpts), ctypes.POINTER(JKPlanInfo)],
     "lible_gpu_stream": [P, ctypes.POINTER(P)],
+    "lible_gpu_jk_plan_classes": [P, ctypes.POINTER(JKOpts), P, P, P, P, P, P],
     "lible_gpu_fp64_peak": [P, ctypes.POINTER(D), ctypes.POINTER(D)],
     "lible_gpu_ri_contract": [P, P, P, P, P],
     "lible_host_spherical_trafo": [I, P, P, P, P],

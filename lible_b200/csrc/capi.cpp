@@ -223,7 +223,7 @@ int lible_host_pair_classes(const char *basis_root, const char *basis, int n_ato
 
 int lible_host_boys(int n, double x, double *F)
 {
-    if (n < 0 || n >= kBoysCols - 6 || !F || !(x >= 0))
+    if (n < 0 || n > kBoysMaxN || !F || !(x >= 0))
         return LIBLE_GPU_EINVAL;
     static const std::vector<double> grid = boysGrid();
     boysHost(n, x, grid, F);
@@ -546,6 +546,32 @@ int lible_gpu_jk_plan(lible_gpu_ctx *ctx, const lible_gpu_jk_opts *opts, lible_g
         info->n_launches = p.n_launches;
         info->flops_fp64 = p.flops_fp64;
         info->flops_fp32 = p.flops_fp32;
+    });
+}
+
+int lible_gpu_jk_plan_classes(lible_gpu_ctx *ctx, const lible_gpu_jk_opts *opts, int *n, int *ls, long long *n64,
+                              long long *n32, double *n_prim, double *flops)
+{
+    return guard(ctx, [&](Engine &e) {
+        if (!n)
+            throw EngineError(kStatusInvalid, "null n");
+        auto v = e.jkPlanClasses(toOpts(opts));
+        *n = (int)v.size();
+        if (!ls)
+            return;
+        for (size_t i = 0; i < v.size(); i++)
+        {
+            for (int k = 0; k < 4; k++)
+                ls[4 * i + k] = v[i].l[k];
+            if (n64)
+                n64[i] = v[i].n64;
+            if (n32)
+                n32[i] = v[i].n32;
+            if (n_prim)
+                n_prim[i] = v[i].prim;
+            if (flops)
+                flops[i] = v[i].flops;
+        }
     });
 }
 

@@ -23,7 +23,7 @@ namespace lible_b200
     // Views of one pair class in device memory (see DevPairClass).
     struct PairView
     {
-        const double *pP;      // [ppair][4] p, Px, Py, Pz
+        const double *pP;      // [ppair][8] p, Px, Py, Pz, 1/p, a, b, 0
         const double *ab;      // [ppair][2] a, b
         const uint32_t *pofs;  // [pair + 1]
         const int32_t *info;   // [pair][8] ao_a, ao_b, atom_a, atom_b, shell_a, shell_b
@@ -48,15 +48,19 @@ namespace lible_b200
     struct QuartetArgs
     {
         PairView bra, ket;
-        const double *boys;               // Boys grid [kBoysRows][kBoysCols]
-        // task enumeration: explicit (bra pair, ket pair) list, or implicit Schwarz prefix form
+        const double *boys;               // Boys tables [kBoysMaxN + 1][kBoysRows][kBoysTerms]
+        // task enumeration: explicit (bra pair, ket pair) list, or the implicit Schwarz prefix form:
+        // task t belongs to major position i with prefix[i] <= t < prefix[i+1] and pairs with
+        // minor position minor_begin[i] + (t - prefix[i]).  major_ket = 1 enumerates ket-major
+        // (consecutive tasks share the ket pair), 0 bra-major.
         const uint32_t *list;             // [n_tasks][2] or null
         long long n_tasks;
-        const unsigned long long *prefix; // [n_bra + 1]
-        const uint32_t *bra_order;        // bra pair index of bra position i
-        const uint32_t *ket_order;        // ket pair index of ket position j
-        const uint32_t *ket_begin;        // first ket position of bra position i
-        int n_bra;
+        const unsigned long long *prefix; // [n_major + 1]
+        const uint32_t *major_order;      // pair index of major position i
+        const uint32_t *minor_order;      // pair index of minor position j
+        const uint32_t *minor_begin;      // first minor position of major position i
+        int n_major;
+        int major_ket;
         int same_class;                   // bra and ket classes are the same pair list
         // epilogue
         int mode;
@@ -73,17 +77,68 @@ namespace lible_b200
         int *status;                      // error word (non-zero = failure)
     };
 
-    // Primitive-pair record: total exponent p and centre P = (x, y, z) in bohr (named w for z).
+    // Primitive-pair record as stored in DevPairClass::pP: [p, Px, Py, Pz, 1/p, a, b, 0].
+    // x = p, (y, z, w) = P, ip = 1/p.
     struct PQ4
     {
-        double x, y, z, w;
+        double x, y, z, w, ip;
     };
 
     __device__ __forceinline__ PQ4 loadPQ(const double *pP, uint32_t i)
     {
-        const double2 *v = reinterpret_cast<const double2 *>(pP) + 2 * (size_t)i;
-        const double2 lo = __ldg(v), hi = __ldg(v + 1);
-        return {lo.x, lo.y, hi.x, hi.y};
+        const double2 *v = reinterpret_cast<const double2 *>(pP + 8 * (size_t)i);
+        const double2 a = __ldg(v), b = __ldg(v + 1), c = __ldg(v + 2);
+        return {a.x, a.y, b.x, b.y, c.x};
+    }
+
+    // Largest major position i >= lo with prefix[i] <= t, given prefix[lo] <= t: gallops forward
+    // from the caller's cursor, so walking consecutive tasks costs a load or two, not a full search.
+    __device__ __forceinline__ int advanceMajor(const QuartetArgs &a, long long t, int lo)
+    {
+        const unsigned long long ut = (unsigned long long)t;
+        if (lo + 1 >= a.n_major || __ldg(a.prefix + lo + 1) > ut)
+            return lo;
+        int step = 1, hi = lo + 1;
+        while (hi < a.n_major && __ldg(a.prefix + hi) <= ut)
+        {
+            lo = hi;
+            step <<= 1;
+            hi = lo + step;
+        }
+        if (hi > a.n_major - 1)
+            hi = a.n_major - 1;
+        while (lo < hi)
+        {
+            int mid = (lo + hi + 1) >> 1;
+            if (__ldg(a.prefix + mid) <= ut)
+                lo = mid;
+            else
+                hi = mid - 1;
+        }
+        return lo;
+    }
+
+    // Task t decoded with a known major position (implicit enumeration only).
+    __device__ __forceinline__ void decodeAt(const QuartetArgs &a, long long t, int lo, uint32_t &ib, uint32_t &ik)
+    {
+        const uint32_t maj = __ldg(a.major_order + lo);
+        const uint32_t mnr = __ldg(a.minor_order + __ldg(a.minor_begin + lo) +
+                                   (uint32_t)((unsigned long long)t - __ldg(a.prefix + lo)));
+        ib = a.major_ket ? mnr : maj;
+        ik = a.major_ket ? maj : mnr;
+    }
+
+    // Cursor-based decode: explicit lists index directly; implicit ones advance `cur`.
+    __device__ __forceinline__ void decodeCursor(const QuartetArgs &a, long long t, int &cur, uint32_t &ib, uint32_t &ik)
+    {
+        if (a.list)
+        {
+            ib = a.list[2 * t];
+            ik = a.list[2 * t + 1];
+            return;
+        }
+        cur = advanceMajor(a, t, cur);
+        decodeAt(a, t, cur, ib, ik);
     }
 
     __device__ __forceinline__ void decodeTask(const QuartetArgs &a, long long t, uint32_t &ib, uint32_t &ik)
@@ -94,17 +149,20 @@ namespace lible_b200
             ik = a.list[2 * t + 1];
             return;
         }
-        int lo = 0, hi = a.n_bra - 1;
+        int lo = 0, hi = a.n_major - 1;
         while (lo < hi)
         {
             int mid = (lo + hi + 1) >> 1;
-            if (a.prefix[mid] <= (unsigned long long)t)
+            if (__ldg(a.prefix + mid) <= (unsigned long long)t)
                 lo = mid;
             else
                 hi = mid - 1;
         }
-        ib = a.bra_order[lo];
-        ik = a.ket_order[a.ket_begin[lo] + (uint32_t)((unsigned long long)t - a.prefix[lo])];
+        const uint32_t maj = __ldg(a.major_order + lo);
+        const uint32_t mnr = __ldg(a.minor_order + __ldg(a.minor_begin + lo) +
+                                   (uint32_t)((unsigned long long)t - __ldg(a.prefix + lo)));
+        ib = a.major_ket ? mnr : maj;
+        ik = a.major_ket ? maj : mnr;
     }
 
     // Degeneracy weight of a unique quartet: 1/2 for each coinciding shell pair / pair pair.
@@ -122,39 +180,80 @@ namespace lible_b200
         return f;
     }
 
-    // Boys function F_n(x), n = 0..N: Taylor expansion of F_N about the nearest lower grid point
-    // (7 terms, step 0.01) followed by downward recursion; exact at x = 0; for x > 30 the
-    // asymptotic F_0 = sqrt(pi/x)/2 and upward recursion.  Same method and constants as
-    // src/lible/ints/boys_function.hpp:68-109.
+    // e^{-x} for 0 <= x <= 700 using only FP64 FMAs and integer adds (no special-function or
+    // conversion instructions): Cody-Waite reduction x = k ln2 - r with k = round(x / ln2) taken
+    // from the low mantissa bits of x/ln2 + 1.5*2^52, e^{-r} by its degree-13 Taylor polynomial
+    // (|r| <= ln2/2, truncation < 2e-17), and 2^-k applied to the exponent field.  Within ~1 ulp
+    // of exp().
+    __device__ __forceinline__ double expNeg(double x)
+    {
+        constexpr double kMagic = 6755399441055744.0;  // 1.5 * 2^52
+        const double t = fma(-x, 1.4426950408889634074, kMagic);
+        const double kd = t - kMagic;
+        const long long k = __double_as_longlong(t) - __double_as_longlong(kMagic);
+        double r = fma(kd, -0.6931471805599453094, -x);
+        r = fma(kd, -2.319046813846299558e-17, r);
+        double p = 1.0 / 6227020800.0;  // 1/13!
+        p = fma(p, r, 1.0 / 479001600.0);
+        p = fma(p, r, 1.0 / 39916800.0);
+        p = fma(p, r, 1.0 / 3628800.0);
+        p = fma(p, r, 1.0 / 362880.0);
+        p = fma(p, r, 1.0 / 40320.0);
+        p = fma(p, r, 1.0 / 5040.0);
+        p = fma(p, r, 1.0 / 720.0);
+        p = fma(p, r, 1.0 / 120.0);
+        p = fma(p, r, 1.0 / 24.0);
+        p = fma(p, r, 1.0 / 6.0);
+        p = fma(p, r, 0.5);
+        p = fma(p, r, 1.0);
+        p = fma(p, r, 1.0);
+        return __longlong_as_double(__double_as_longlong(p) + k * 4503599627370496LL);
+    }
+
+    // Boys function F_n(x), n = 0..N.  Reference method (src/lible/ints/boys_function.hpp:68-109):
+    // Taylor expansion of F_N about a grid point (7 terms, step 0.01) followed by downward
+    // recursion, and for x > 30 the asymptotic F_0 = sqrt(pi/x)/2 with upward recursion.
+    // Here the expansion point is the nearest grid point (|x - x_i| <= 0.005, half the reference's
+    // truncation interval), found with the 1.5*2^52 rounding trick, and e^{-x} comes from expNeg(),
+    // so the only special-function instruction on this path is the asymptote's rsqrt.
     template <int N>
     __device__ __forceinline__ void boysF(double x, const double *__restrict__ grid, double *F)
     {
         if (x > kBoysLargeX)
         {
-            F[0] = 0.5 * sqrt(M_PI / x);
-            const double rx = 1.0 / x;
+            // sqrt(pi)/2 * x^{-1/2}, then F_k = F_{k-1} (k - 1/2) / x
+            const double rs = rsqrt(x);
+            const double rx = rs * rs;
+            F[0] = 0.88622692545275801365 * rs;
 #pragma unroll
             for (int k = 1; k <= N; k++)
-                F[k] = F[k - 1] * (k - 0.5) * rx;
+                F[k] = F[k - 1] * ((k - 0.5) * rx);
             return;
         }
-        const int iv = (int)(x / kBoysStep);
-        const double dx = x - iv * kBoysStep;
-        const double *row = grid + (size_t)iv * kBoysCols + N;
-        double s = __ldg(row);
-        double pk = 1.0, fact = 1.0;
-#pragma unroll
-        for (int k = 1; k < 7; k++)
-        {
-            pk *= -dx;
-            fact *= k;
-            s += __ldg(row + k) * pk / fact;
-        }
+        constexpr double kMagic = 6755399441055744.0;  // 1.5 * 2^52
+        const double t = fma(x, 1.0 / kBoysStep, kMagic);
+        const long long iv = __double_as_longlong(t) - __double_as_longlong(kMagic);
+        const double m = fma(t - kMagic, kBoysStep, -x);  // x_i - x
+        // row of 10 coefficients F_{N+k}(x_i)/k! (80 bytes, 16-byte aligned)
+        const double2 *row = reinterpret_cast<const double2 *>(grid + ((size_t)N * kBoysRows + iv) * kBoysTerms);
+        static_assert(kBoysTerms == 10, "row load below assumes 10 terms");
+        const double2 c01 = __ldg(row), c23 = __ldg(row + 1), c45 = __ldg(row + 2), c67 = __ldg(row + 3),
+                      c89 = __ldg(row + 4);
+        double s = fma(c89.y, m, c89.x);
+        s = fma(s, m, c67.y);
+        s = fma(s, m, c67.x);
+        s = fma(s, m, c45.y);
+        s = fma(s, m, c45.x);
+        s = fma(s, m, c23.y);
+        s = fma(s, m, c23.x);
+        s = fma(s, m, c01.y);
+        s = fma(s, m, c01.x);
         F[N] = s;
-        const double ex = exp(-x);
+        const double ex = expNeg(x);
+        const double x2 = 2.0 * x;
 #pragma unroll
         for (int k = N - 1; k >= 0; k--)
-            F[k] = (2.0 * x * F[k + 1] + ex) / (2 * k + 1);
+            F[k] = (x2 * F[k + 1] + ex) * (1.0 / (2 * k + 1));
     }
 
     // Hermite Coulomb integrals R_{tuv} = R^{(0)}_{tuv} for t+u+v <= L in registers, by the

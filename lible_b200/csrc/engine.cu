@@ -69,10 +69,14 @@ namespace lible_b200
             if (a.E1)
                 hermiteE1(la, lb, ea, eb, A[k] - B[k], Ex[k], E1x[k]);
         }
-        a.pP[4 * ip + 0] = p;
-        a.pP[4 * ip + 1] = P[0];
-        a.pP[4 * ip + 2] = P[1];
-        a.pP[4 * ip + 3] = P[2];
+        a.pP[8 * ip + 0] = p;
+        a.pP[8 * ip + 1] = P[0];
+        a.pP[8 * ip + 2] = P[1];
+        a.pP[8 * ip + 3] = P[2];
+        a.pP[8 * ip + 4] = 1.0 / p;
+        a.pP[8 * ip + 5] = ea;
+        a.pP[8 * ip + 6] = eb;
+        a.pP[8 * ip + 7] = 0.0;
         a.ab[2 * ip + 0] = ea;
         a.ab[2 * ip + 1] = eb;
         const int nt = lab + 1;
@@ -442,7 +446,7 @@ namespace lible_b200
         d.coords = devUpload(pc.coords, stream_);
         const size_t np = std::max<size_t>(pc.n_ppairs, 1);
         const int sab = nsph(pc.la) * nsph(pc.lb), hab = nherm(pc.la + pc.lb);
-        d.pP = devAlloc<double>(4 * np);
+        d.pP = devAlloc<double>(8 * np);
         d.ab = devAlloc<double>(2 * np);
         d.E = devAlloc<double>(np * sab * hab);
         d.Et = devAlloc<double>(np * sab * hab);
@@ -909,17 +913,22 @@ namespace lible_b200
     void Engine::freePlan(JKPlan &p)
     {
         for (auto &cp : p.pairs)
-            for (void *x : {(void *)cp.prefix64, (void *)cp.prefix32, (void *)cp.begin64, (void *)cp.begin32})
+            for (void *x : {(void *)cp.prefix64, (void *)cp.prefix32, (void *)cp.begin64, (void *)cp.begin32,
+                            (void *)cp.majors})
                 cudaFree(x);
         for (void *x : p.orders)
             cudaFree(x);
         p = JKPlan();
     }
 
-    // Unique quartets (ab|cd), cd <= ab, kept iff Q_ab Q_cd >= thr.  Pairs of each class are sorted
-    // by decreasing Q, so the surviving kets of bra position i are a prefix of the ket order and
-    // quartet t of a class pair decodes by a binary search over per-bra prefix sums.  With mixed
-    // precision the prefix is split at Q_ab Q_cd = thr32: FP64 below index n64, FP32 after.
+    // Unique quartets (ab|cd), cd <= ab, kept iff Q_ab Q_cd >= thr.  The pairs of each class are
+    // grouped by their number of primitive pairs K and sorted by decreasing Q inside a group, so the
+    // surviving bras of a ket are a prefix of each bra group.  Tasks are enumerated ket-major per
+    // (bra group, ket group) segment: "major" entries m = (ket pair, bra group) own the task range
+    // [prefix[m], prefix[m+1]) whose bras are minor_order[minor_begin[m] + (t - prefix[m])].  All
+    // quartets of a segment have the same K_ab and K_cd, so a warp's primitive loops run in lock
+    // step.  With mixed precision a second (prefix, begin) pair covers the FP32 part of each range
+    // (Q_ab Q_cd < thr32).
     Engine::JKPlan &Engine::jkPlan(double thr, double thr32, bool mixed)
     {
         ClassSet &cs = mainSet(true);
@@ -931,35 +940,41 @@ namespace lible_b200
             return it->second;
         JKPlan plan;
         const size_t nc = cs.dev.size();
+        struct Group
+        {
+            uint32_t k, start, end;
+        };
         std::vector<std::vector<uint32_t>> order(nc);
         std::vector<std::vector<double>> qs(nc);
-        for (size_t c = 0; c < nc; c++)
-        {
-            const auto &Q = cs.dev[c].Qh;
-            order[c].resize(Q.size());
-            std::iota(order[c].begin(), order[c].end(), 0u);
-            std::stable_sort(order[c].begin(), order[c].end(), [&](uint32_t x, uint32_t y) { return Q[x] > Q[y]; });
-            qs[c].resize(Q.size());
-            for (size_t i = 0; i < Q.size(); i++)
-                qs[c][i] = Q[order[c][i]];
-            uint32_t *d = devUpload(order[c], stream_);
-            plan.orders.push_back(d);
-        }
-        // primitive-pair counts in sorted order, and their prefix sums
+        std::vector<std::vector<Group>> groups(nc);
         std::vector<std::vector<double>> kpre(nc);
         for (size_t c = 0; c < nc; c++)
         {
-            kpre[c].assign(order[c].size() + 1, 0.0);
-            for (size_t i = 0; i < order[c].size(); i++)
+            const auto &Q = cs.dev[c].Qh;
+            const auto &pofs = cs.host[c].pofs;
+            auto K = [&](uint32_t x) { return pofs[x + 1] - pofs[x]; };
+            order[c].resize(Q.size());
+            std::iota(order[c].begin(), order[c].end(), 0u);
+            std::stable_sort(order[c].begin(), order[c].end(), [&](uint32_t x, uint32_t y) {
+                return K(x) != K(y) ? K(x) < K(y) : Q[x] > Q[y];
+            });
+            qs[c].resize(Q.size());
+            kpre[c].assign(Q.size() + 1, 0.0);
+            for (size_t i = 0; i < Q.size(); i++)
             {
-                const uint32_t pi = order[c][i];
-                kpre[c][i + 1] = kpre[c][i] + (cs.host[c].pofs[pi + 1] - cs.host[c].pofs[pi]);
+                qs[c][i] = Q[order[c][i]];
+                kpre[c][i + 1] = kpre[c][i] + K(order[c][i]);
+                if (groups[c].empty() || groups[c].back().k != K(order[c][i]))
+                    groups[c].push_back({K(order[c][i]), (uint32_t)i, (uint32_t)i});
+                groups[c].back().end = (uint32_t)i + 1;
             }
+            plan.orders.push_back(devUpload(order[c], stream_));
         }
-        auto countAbove = [](const std::vector<double> &q, double bound) -> uint32_t {
-            // number of entries with q >= bound (q sorted descending)
-            return (uint32_t)(std::upper_bound(q.begin(), q.end(), bound, [](double b, double v) { return b > v; }) -
-                              q.begin());
+        // number of entries >= bound in the descending range q[b, e)
+        auto countAbove = [](const std::vector<double> &q, uint32_t b, uint32_t e, double bound) -> uint32_t {
+            return (uint32_t)(std::upper_bound(q.begin() + b, q.begin() + e, bound,
+                                               [](double x, double v) { return x > v; }) -
+                              (q.begin() + b));
         };
         for (size_t cb = 0; cb < nc; cb++)
             for (size_t ck = 0; ck <= cb; ck++)
@@ -967,33 +982,44 @@ namespace lible_b200
                 JKClassPair cp;
                 cp.cb = (int)cb;
                 cp.ck = (int)ck;
-                const size_t nb = qs[cb].size();
-                std::vector<unsigned long long> p64(nb + 1, 0), p32(nb + 1, 0);
-                std::vector<uint32_t> b64(nb, 0), b32(nb, 0);
-                for (size_t i = 0; i < nb; i++)
-                {
-                    const double qi = qs[cb][i];
-                    uint32_t nall = qi > 0 ? countAbove(qs[ck], thr / qi) : 0;
-                    uint32_t n64 = nall;
-                    if (mixed)
-                        n64 = qi > 0 ? std::min(nall, countAbove(qs[ck], thr32 / qi)) : 0;
-                    if (cb == ck)
+                std::vector<uint32_t> majors, b64, b32;
+                std::vector<unsigned long long> p64(1, 0), p32(1, 0);
+                double bra_prims64 = 0, bra_prims32 = 0;
+                for (size_t gb = 0; gb < groups[cb].size(); gb++)
+                    for (size_t gc = 0; gc < groups[ck].size(); gc++)
                     {
-                        nall = std::min<uint32_t>(nall, (uint32_t)i + 1);
-                        n64 = std::min<uint32_t>(n64, (uint32_t)i + 1);
+                        if (cb == ck && gb < gc)
+                            continue;
+                        const Group &B = groups[cb][gb], &C = groups[ck][gc];
+                        for (uint32_t j = C.start; j < C.end; j++)
+                        {
+                            const double qj = qs[ck][j];
+                            const uint32_t lo = (cb == ck && gb == gc) ? j - C.start : 0u;
+                            uint32_t nall = qj > 0 ? countAbove(qs[cb], B.start, B.end, thr / qj) : 0;
+                            uint32_t n64 = nall;
+                            if (mixed)
+                                n64 = qj > 0 ? std::min(nall, countAbove(qs[cb], B.start, B.end, thr32 / qj)) : 0;
+                            nall = std::max(nall, lo);
+                            n64 = std::max(n64, lo);
+                            if (nall == lo)
+                                continue;
+                            majors.push_back(order[ck][j]);
+                            b64.push_back(B.start + lo);
+                            b32.push_back(B.start + n64);
+                            p64.push_back(p64.back() + (n64 - lo));
+                            p32.push_back(p32.back() + (nall - n64));
+                            const double kj = C.k;
+                            const double pr64 = kpre[cb][B.start + n64] - kpre[cb][B.start + lo];
+                            const double pr32 = kpre[cb][B.start + nall] - kpre[cb][B.start + n64];
+                            cp.prim64 += kj * pr64;
+                            cp.prim32 += kj * pr32;
+                            // bra-side work is counted per (bra primitive, ket pair)
+                            bra_prims64 += pr64;
+                            bra_prims32 += pr32;
+                        }
                     }
-                    p64[i + 1] = p64[i] + n64;
-                    p32[i + 1] = p32[i] + (nall - n64);
-                    const double ki = kpre[cb][i + 1] - kpre[cb][i];
-                    cp.prim64 += ki * kpre[ck][n64];
-                    cp.prim32 += ki * (kpre[ck][nall] - kpre[ck][n64]);
-                    cp.flops64 += ki * n64;   // bra-side work counted per (bra primitive, ket pair)
-                    cp.flops32 += ki * (nall - n64);
-                    b64[i] = 0;
-                    b32[i] = n64;
-                }
-                cp.n64 = (long long)p64[nb];
-                cp.n32 = (long long)p32[nb];
+                cp.n64 = (long long)p64.back();
+                cp.n32 = (long long)p32.back();
                 {
                     const auto &B = cs.host[cb], &K = cs.host[ck];
                     const int L = B.la + B.lb + K.la + K.lb;
@@ -1002,12 +1028,13 @@ namespace lible_b200
                     const double per_prim = (20 + 4 * L) + 3.0 * (L + 1) * (L + 2) * (L + 3) * (L + 4) / 24 + hab * hcd +
                                             2 * hab * hcd * scd;
                     const double per_bra = 2 * sab * hab * scd;
-                    cp.flops64 = cp.prim64 * per_prim + cp.flops64 * per_bra;
-                    cp.flops32 = cp.prim32 * per_prim + cp.flops32 * per_bra;
+                    cp.flops64 = cp.prim64 * per_prim + bra_prims64 * per_bra;
+                    cp.flops32 = cp.prim32 * per_prim + bra_prims32 * per_bra;
                 }
-                cp.n_bra = (int)nb;
+                cp.n_bra = (int)majors.size();
                 if (cp.n64 + cp.n32 == 0)
                     continue;
+                cp.majors = devUpload(majors, stream_);
                 cp.prefix64 = devUpload(p64, stream_);
                 cp.prefix32 = devUpload(p32, stream_);
                 cp.begin64 = devUpload(b64, stream_);
@@ -1020,17 +1047,13 @@ namespace lible_b200
                 plan.pairs.push_back(cp);
             }
         // most expensive class pairs first
-        std::stable_sort(plan.pairs.begin(), plan.pairs.end(), [&](const JKClassPair &x, const JKClassPair &y) {
-            auto cost = [&](const JKClassPair &c) {
-                const auto &B = cs.dev[c.cb], &K = cs.dev[c.ck];
-                return (double)(c.n64 + c.n32) * nherm(B.la + B.lb) * nherm(K.la + K.lb) * nsph(K.la) * nsph(K.lb);
-            };
-            return cost(x) > cost(y);
-        });
+        std::stable_sort(plan.pairs.begin(), plan.pairs.end(),
+                         [](const JKClassPair &x, const JKClassPair &y) { return x.flops64 + x.flops32 > y.flops64 + y.flops32; });
         cudaCheck(cudaStreamSynchronize(stream_), "plan");
         plan.thr = thr;
         return plans_.emplace(key, std::move(plan)).first->second;
     }
+
 
     void Engine::jk(const double *D_dev, double *J_dev, double *K_dev, const JKOptions &opt, JKStats *stats)
     {
@@ -1050,9 +1073,10 @@ namespace lible_b200
             a.ket = view(K);
             a.boys = boys_;
             a.list = nullptr;
-            a.bra_order = plan.orders[cp.cb];
-            a.ket_order = plan.orders[cp.ck];
-            a.n_bra = cp.n_bra;
+            a.major_ket = 1;
+            a.major_order = cp.majors;
+            a.minor_order = plan.orders[cp.cb];
+            a.n_major = cp.n_bra;
             a.same_class = cp.cb == cp.ck;
             a.mode = kJK;
             a.D = D_dev;
@@ -1062,13 +1086,13 @@ namespace lible_b200
             const int tb = pairType(B.la, B.lb), tk = pairType(K.la, K.lb);
             a.n_tasks = cp.n64;
             a.prefix = cp.prefix64;
-            a.ket_begin = cp.begin64;
+            a.minor_begin = cp.begin64;
             cudaCheck(lookupFwd64(tb, tk)(a, stream_, num_sms_), "jk kernel");
             if (cp.n32 > 0)
             {
                 a.n_tasks = cp.n32;
                 a.prefix = cp.prefix32;
-                a.ket_begin = cp.begin32;
+                a.minor_begin = cp.begin32;
                 cudaCheck(lookupFwd32(tb, tk)(a, stream_, num_sms_), "jk kernel fp32");
             }
         }
@@ -1105,6 +1129,19 @@ namespace lible_b200
         info.flops_fp32 = plan.flops32;
         info.n_launches = jkLaunchCount(opt);
         return info;
+    }
+
+    std::vector<Engine::JKClassInfo> Engine::jkPlanClasses(const JKOptions &opt)
+    {
+        JKPlan &plan = jkPlan(opt.schwarz, opt.fp32_threshold, opt.precision == 1);
+        ClassSet &cs = mainSet(true);
+        std::vector<JKClassInfo> v;
+        for (const auto &cp : plan.pairs)
+        {
+            const auto &B = cs.dev[cp.cb], &K = cs.dev[cp.ck];
+            v.push_back({{B.la, B.lb, K.la, K.lb}, cp.n64, cp.n32, cp.prim64 + cp.prim32, cp.flops64 + cp.flops32});
+        }
+        return v;
     }
 
     // ------------------------------------------------------------------------------------------

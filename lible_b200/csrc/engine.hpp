@@ -88,7 +88,7 @@ namespace lible_b200
         int la = 0, lb = 0;
         bool single = false;
         size_t n_pairs = 0, n_ppairs = 0;
-        double *pP = nullptr;       // [n_ppairs][4]: p, Px, Py, Pz
+        double *pP = nullptr;       // [n_ppairs][8]: p, Px, Py, Pz, 1/p, a, b, 0
         double *ab = nullptr;       // [n_ppairs][2]: a, b
         uint32_t *pofs = nullptr;   // [n_pairs + 1]
         int32_t *info = nullptr;    // [n_pairs][8]: ao_a, ao_b, atom_a, atom_b, shell_a, shell_b, 0, 0

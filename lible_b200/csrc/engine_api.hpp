@@ -117,6 +117,13 @@ namespace lible_b200
         void jk(const double *D_dev, double *J_dev, double *K_dev, const JKOptions &opt, JKStats *stats);
         long long jkLaunchCount(const JKOptions &opt);
         JKPlanInfo jkPlanInfo(const JKOptions &opt);
+        struct JKClassInfo
+        {
+            int l[4];
+            long long n64, n32;
+            double prim, flops;
+        };
+        std::vector<JKClassInfo> jkPlanClasses(const JKOptions &opt);
         // Gradient of 1/2 Tr(DJ) - 1/4 Tr(DK) with respect to nuclear coordinates, [n_atoms][3].
         void jkGradient(const double *D_dev, double *grad_dev);
         // RI-J contractions (either output may be null).
@@ -140,7 +147,7 @@ namespace lible_b200
             long long n64 = 0, n32 = 0;
             double prim64 = 0, prim32 = 0, flops64 = 0, flops32 = 0;
             unsigned long long *prefix64 = nullptr, *prefix32 = nullptr;
-            uint32_t *begin64 = nullptr, *begin32 = nullptr;
+            uint32_t *begin64 = nullptr, *begin32 = nullptr, *majors = nullptr;
         };
         struct JKPlan
         {

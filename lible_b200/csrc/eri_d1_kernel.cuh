@@ -130,10 +130,10 @@ namespace lible_b200
                     {
                         const PQ4 Q = loadPQ(a.ket.pP, q);
                         const double cexp = __ldg(a.ket.ab + 2 * q);
-                        const double pq = P.x + Q.x;
-                        const double alpha = P.x * Q.x / pq;
+                        const double rs = rsqrt(P.x + Q.x);
+                        const double alpha = P.x * Q.x * (rs * rs);
                         const double X = P.y - Q.y, Y = P.z - Q.z, Z = P.w - Q.w;
-                        const double fac = 2.0 * 17.493418327624862 / (P.x * Q.x * sqrt(pq));
+                        const double fac = 34.986836655249725 * rs * P.ip * Q.ip;
                         double F[L1 + 1];
                         boysF<L1>(alpha * (X * X + Y * Y + Z * Z), a.boys, F);
                         const double m2a = -2.0 * alpha;

@@ -17,18 +17,35 @@
 
 namespace lible_b200
 {
+    // Register-path group size: the smallest g dividing S_cd (g <= 32) for which one thread's share
+    // of the batch (S_ab x S_cd/g), of R.E (H_ab x S_cd/g) and the R vector fit the register
+    // budget; 0 when no split fits (the class then uses the shared-memory group path).
+    constexpr int kRegBudget = 104;
+    constexpr int pickRegGroup(int sab, int scd, int hab, int nr)
+    {
+        for (int g = 1; g <= 32; g++)
+            if (scd % g == 0 && sab * (scd / g) + hab * (scd / g) + nr <= kRegBudget)
+                return g;
+        return 0;
+    }
+
     template <int LA, int LB, int LC, int LD, typename T>
     struct Shape
     {
         using C = Cls<LA, LB, LC, LD>;
-        static constexpr int small_regs = C::SAB * C::SCD + C::HAB * C::SCD + C::NR;
-        static constexpr int W = (small_regs <= 72) ? 0
+        // register path: GT threads per quartet, each owning CW consecutive ket columns
+        static constexpr int GT = pickRegGroup(C::SAB, C::SCD, C::HAB, C::NR);
+        static constexpr int CW = GT ? C::SCD / GT : 0;
+        static constexpr int QPW = GT ? 32 / GT : 0;           // quartets per warp
+        static constexpr int W = GT ? 0
                                  : ((C::HAB * C::SCD + C::SAB * C::SCD) <= 64 * 32)     ? 1
                                  : ((C::HAB * C::SCD + C::SAB * C::SCD) <= 64 * 64)     ? 2
                                  : ((C::HAB * C::SCD + C::SAB * C::SCD) <= 64 * 128)    ? 4
                                                                                           : 8;
         static constexpr int G = W == 0 ? 1 : 32 * W;
         static constexpr int block = W == 0 ? 128 : G;
+        // register path: per-warp staging of finished batches for the digestion epilogue
+        static constexpr size_t reg_smem = (GT > 1) ? sizeof(double) * (block / 32) * QPW * C::SAB * C::SCD : 0;
         static constexpr int IK = W == 0 ? 0 : (C::HAB * C::SCD + G - 1) / G;
         static constexpr int IB = W == 0 ? 0 : (C::SAB * C::SCD + G - 1) / G;
         // shared-memory carve-up (bytes) for the group shape
@@ -39,7 +56,7 @@ namespace lible_b200
         static constexpr size_t off_rx = off_ea + sizeof(T) * C::SAB * C::HAB;      // HAB x SCD
         static constexpr size_t off_ix = off_rx + sizeof(T) * C::HAB * C::SCD;      // HCD x HAB int16
         static constexpr size_t off_ht = (off_ix + 2 * C::HCD * C::HAB + 15) / 16 * 16; // NR char4
-        static constexpr size_t smem = W == 0 ? 0 : off_ht + 4 * C::NR;
+        static constexpr size_t smem = W == 0 ? reg_smem : off_ht + 4 * C::NR;
     };
 
     __device__ __forceinline__ void groupSync(int G)
@@ -88,9 +105,12 @@ namespace lible_b200
     //   J_ab += 2 f V D_cd,  J_cd += 2 f V D_ab,
     //   K_ac += f V D_bd, K_ad += f V D_bc, K_bc += f V D_ad, K_bd += f V D_ac
     // into the unsymmetrised accumulators (J = A + A^T, K = B + B^T afterwards).
+    // `ket_uniform` (serial form only): every lane of the warp holds a quartet with the same ket
+    // pair, so the J_cd sums are reduced across the warp and added once.
     template <int SA, int SB, int SC, int SD, bool SERIAL, typename F>
     __device__ __forceinline__ void digestJK(const QuartetArgs &a, double f, const int32_t *bi,
-                                             const int32_t *ki, F val, int tid, int stride)
+                                             const int32_t *ki, F val, int tid, int stride,
+                                             bool ket_uniform = false)
     {
         if constexpr (SERIAL)
         {
@@ -174,7 +194,19 @@ namespace lible_b200
                 dst = a.K + (size_t)(ob + nn) * n + od + t;
                 w = f;
             }
-            atomicAdd(dst, w * s);
+            double v = w * s;
+            if constexpr (SERIAL)
+            {
+                if (ket_uniform && o >= n0 && o < n1)
+                {
+#pragma unroll
+                    for (int sh = 16; sh > 0; sh >>= 1)
+                        v += __shfl_xor_sync(0xffffffffu, v, sh);
+                    if ((threadIdx.x & 31) != 0)
+                        continue;
+                }
+            }
+            atomicAdd(dst, v);
         }
     }
 
@@ -224,32 +256,37 @@ namespace lible_b200
     }
 
     // ---------------------------------------------------------------------------------------
-    // G = 1: one thread per contracted quartet.
+    // Register path: a group of GT threads per contracted quartet, thread `member` owning the ket
+    // columns [c0, c0 + CW) of the batch (c0 = member * CW).  Each thread evaluates the Boys
+    // function and the R vector itself, so the group never synchronises; every index into R, the
+    // R.E accumulator and the batch is a compile-time constant.
     template <int LA, int LB, int LC, int LD, typename T>
-    __device__ __forceinline__ void quartetThread(const QuartetArgs &a, uint32_t ib, uint32_t ik, T *V)
+    __device__ __forceinline__ void quartetThread(const QuartetArgs &a, uint32_t ib, uint32_t ik, int c0, T *V)
     {
         using C = Cls<LA, LB, LC, LD>;
+        constexpr int CW = Shape<LA, LB, LC, LD, T>::CW;
 #pragma unroll
-        for (int x = 0; x < C::SAB * C::SCD; x++)
+        for (int x = 0; x < C::SAB * CW; x++)
             V[x] = T(0);
         const uint32_t p0 = a.bra.pofs[ib], p1 = a.bra.pofs[ib + 1];
         const uint32_t q0 = a.ket.pofs[ik], q1 = a.ket.pofs[ik + 1];
         const T *Eb = braE<T>(a.bra);
-        const T *Ek = ketE<T>(a.ket);
+        const T *Ek = ketE<T>(a.ket) + c0;
         for (uint32_t p = p0; p < p1; p++)
         {
             const PQ4 P = loadPQ(a.bra.pP, p);
-            T RxE[C::HAB * C::SCD];
+            T RxE[C::HAB * CW];
 #pragma unroll
-            for (int x = 0; x < C::HAB * C::SCD; x++)
+            for (int x = 0; x < C::HAB * CW; x++)
                 RxE[x] = T(0);
             for (uint32_t q = q0; q < q1; q++)
             {
                 const PQ4 Q = loadPQ(a.ket.pP, q);
-                const double pq = P.x + Q.x;
-                const double alpha = P.x * Q.x / pq;
+                // alpha = pq/(p+q) and the prefactor 2 pi^{5/2} / (p q sqrt(p+q)) from one rsqrt
+                const double rs = rsqrt(P.x + Q.x);
+                const double alpha = P.x * Q.x * (rs * rs);
                 const double X = P.y - Q.y, Y = P.z - Q.z, Z = P.w - Q.w;
-                const double fac = 2.0 * 17.493418327624862 / (P.x * Q.x * sqrt(pq)); // 2 pi^{5/2}
+                const double fac = 34.986836655249725 * rs * P.ip * Q.ip;
                 double F[C::L + 1];
                 boysF<C::L>(alpha * (X * X + Y * Y + Z * Z), a.boys, F);
                 T Ft[C::L + 1];
@@ -276,11 +313,10 @@ namespace lible_b200
                                     up = u;
                                     vp = n - t - u;
                                 }
-                    const T sg = ((tp + up + vp) & 1) ? T(-1) : T(1);
-                    T ecv[C::SCD];
+                    T ecv[CW];
 #pragma unroll
-                    for (int c = 0; c < C::SCD; c++)
-                        ecv[c] = ec[hp * C::SCD + c];
+                    for (int c = 0; c < CW; c++)
+                        ecv[c] = ((tp + up + vp) & 1) ? -ec[hp * C::SCD + c] : ec[hp * C::SCD + c];
 #pragma unroll
                     for (int h = 0, n = 0; n <= C::LAB; n++)
 #pragma unroll
@@ -289,10 +325,10 @@ namespace lible_b200
                             for (int u = n - t; u >= 0; u--, h++)
                             {
                                 const int v = n - t - u;
-                                const T r = sg * R[hermIndex(t + tp, u + up, v + vp)];
+                                const T r = R[hermIndex(t + tp, u + up, v + vp)];
 #pragma unroll
-                                for (int c = 0; c < C::SCD; c++)
-                                    RxE[h * C::SCD + c] += r * ecv[c];
+                                for (int c = 0; c < CW; c++)
+                                    RxE[h * CW + c] += r * ecv[c];
                             }
                 }
             }
@@ -304,8 +340,8 @@ namespace lible_b200
                 {
                     const T e = eb[m * C::HAB + h];
 #pragma unroll
-                    for (int c = 0; c < C::SCD; c++)
-                        V[m * C::SCD + c] += e * RxE[h * C::SCD + c];
+                    for (int c = 0; c < CW; c++)
+                        V[m * CW + c] += e * RxE[h * CW + c];
                 }
         }
     }
@@ -347,10 +383,10 @@ namespace lible_b200
             for (uint32_t q = q0; q < q1; q++)
             {
                 const PQ4 Q = loadPQ(a.ket.pP, q);
-                const double pq = P.x + Q.x;
-                const double alpha = P.x * Q.x / pq;
+                const double rs = rsqrt(P.x + Q.x);
+                const double alpha = P.x * Q.x * (rs * rs);
                 const double X = P.y - Q.y, Y = P.z - Q.z, Z = P.w - Q.w;
-                const double fac = 2.0 * 17.493418327624862 / (P.x * Q.x * sqrt(pq));
+                const double fac = 34.986836655249725 * rs * P.ip * Q.ip;
                 double F[C::L + 1];
                 boysF<C::L>(alpha * (X * X + Y * Y + Z * Z), a.boys, F);
                 const double m2a = -2.0 * alpha;
@@ -496,33 +532,97 @@ namespace lible_b200
         constexpr int blk = C::SAB * C::SCD;
         if constexpr (S::W == 0)
         {
-            const long long stride = (long long)gridDim.x * blockDim.x;
-            for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < a.n_tasks; t += stride)
+            constexpr int GT = S::GT, CW = S::CW, QPW = S::QPW;
+            const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+            const int slot = lane / GT, member = lane % GT;
+            const long long warps = (long long)gridDim.x * (blockDim.x >> 5);
+            const long long gw = (long long)blockIdx.x * (blockDim.x >> 5) + warp;
+            extern __shared__ __align__(16) unsigned char smem[];
+            double *vs = reinterpret_cast<double *>(smem) + ((size_t)warp * QPW + slot) * blk;
+            // each warp walks chunks of consecutive tasks (QPW per iteration); consecutive tasks
+            // share the major pair, so the task cursor rarely moves
+            constexpr long long CH = 8 * QPW;
+            const long long n_chunks = (a.n_tasks + CH - 1) / CH;
+            for (long long chunk = gw; chunk < n_chunks; chunk += warps)
             {
-                uint32_t ib, ik;
-                decodeTask(a, t, ib, ik);
-                T V[blk];
-                quartetThread<LA, LB, LC, LD, T>(a, ib, ik, V);
+            const long long end = (chunk + 1) * CH < a.n_tasks ? (chunk + 1) * CH : a.n_tasks;
+            int cur = 0;
+            if (!a.list)
+                cur = advanceMajor(a, chunk * CH, 0);
+            for (long long base = chunk * CH; base < end; base += QPW)
+            {
+                const long long t = base + slot;
+                const bool valid = slot < QPW && t < end;
+                uint32_t ib = 0, ik = 0;
+                T V[C::SAB * CW];
+                if (valid)
+                {
+                    int my = cur;
+                    decodeCursor(a, t, my, ib, ik);
+                    quartetThread<LA, LB, LC, LD, T>(a, ib, ik, member * CW, V);
+                }
+                if (!a.list)
+                    cur = advanceMajor(a, base + QPW < end ? base + QPW : end - 1, cur);
                 const int32_t *bi = a.bra.info + 8 * ib;
                 const int32_t *ki = a.ket.info + 8 * ik;
-                auto val = [&](int e) { return (double)V[e]; };
                 if (a.mode == kStore)
                 {
+                    if (valid)
+                    {
 #pragma unroll
-                    for (int m = 0; m < C::SA; m++)
+                        for (int m = 0; m < C::SAB; m++)
 #pragma unroll
-                        for (int n = 0; n < C::SB; n++)
-#pragma unroll
-                            for (int k = 0; k < C::SC; k++)
-#pragma unroll
-                                for (int l = 0; l < C::SD; l++)
-                                    a.out[(size_t)t * blk + storeIndex<C::SA, C::SB, C::SC, C::SD>(a.flags, m, n, k, l)] =
-                                        (double)V[((m * C::SB + n) * C::SC + k) * C::SD + l];
+                            for (int c = 0; c < CW; c++)
+                            {
+                                const int kt = member * CW + c;
+                                a.out[(size_t)t * blk + storeIndex<C::SA, C::SB, C::SC, C::SD>(
+                                                            a.flags, m / C::SB, m % C::SB, kt / C::SD, kt % C::SD)] =
+                                    (double)V[m * CW + c];
+                            }
+                    }
                 }
-                else if (a.mode == kJK)
-                    digestJK<C::SA, C::SB, C::SC, C::SD, true>(a, quartetWeight(a, ib, ik), bi, ki, val, 0, 1);
+                else if constexpr (GT == 1)
+                {
+                    auto val = [&](int e) { return (double)V[e]; };
+                    // ket-major enumeration: usually the whole warp shares one ket pair
+                    const unsigned vmask = __ballot_sync(0xffffffffu, valid);
+                    const uint32_t ik0 = __shfl_sync(0xffffffffu, ik, 0);
+                    const bool uniform = vmask == 0xffffffffu && __all_sync(0xffffffffu, ik == ik0);
+                    if (a.mode == kJK)
+                    {
+                        if (uniform)
+                            digestJK<C::SA, C::SB, C::SC, C::SD, true>(a, quartetWeight(a, ib, ik), bi, ki, val, 0, 1,
+                                                                       true);
+                        else if (valid)
+                            digestJK<C::SA, C::SB, C::SC, C::SD, true>(a, quartetWeight(a, ib, ik), bi, ki, val, 0, 1);
+                    }
+                    else if (valid)
+                        digestRI<C::SA, C::SB, C::SC, C::SD, true>(a, bi, ki, val, 0, 1);
+                }
                 else
-                    digestRI<C::SA, C::SB, C::SC, C::SD, true>(a, bi, ki, val, 0, 1);
+                {
+                    // gather the quartet's columns in shared memory, then digest with the group
+                    if (valid)
+                    {
+#pragma unroll
+                        for (int m = 0; m < C::SAB; m++)
+#pragma unroll
+                            for (int c = 0; c < CW; c++)
+                                vs[m * C::SCD + member * CW + c] = (double)V[m * CW + c];
+                    }
+                    __syncwarp();
+                    if (valid)
+                    {
+                        auto val = [&](int e) { return vs[e]; };
+                        if (a.mode == kJK)
+                            digestJK<C::SA, C::SB, C::SC, C::SD, false>(a, quartetWeight(a, ib, ik), bi, ki, val,
+                                                                        member, GT);
+                        else
+                            digestRI<C::SA, C::SB, C::SC, C::SD, false>(a, bi, ki, val, member, GT);
+                    }
+                    __syncwarp();
+                }
+            }
             }
         }
         else
@@ -530,10 +630,15 @@ namespace lible_b200
             extern __shared__ __align__(16) unsigned char smem[];
             buildGroupTables<LA, LB, LC, LD, T>(smem);
             T *vs = reinterpret_cast<T *>(smem + S::off_rx);
-            for (long long t = blockIdx.x; t < a.n_tasks; t += gridDim.x)
+            // blocks walk chunks of consecutive tasks with a cursor over the major positions
+            constexpr long long CHB = 8;
+            const long long n_chunks = (a.n_tasks + CHB - 1) / CHB;
+            long long chunk = blockIdx.x;
+            int cur = 0;
+            for (long long t = chunk * CHB; chunk < n_chunks;)
             {
                 uint32_t ib, ik;
-                decodeTask(a, t, ib, ik);
+                decodeCursor(a, t, cur, ib, ik);
                 T vals[S::IB];
                 quartetGroup<LA, LB, LC, LD, T>(a, ib, ik, smem, vals);
                 if (a.mode == kStore)
@@ -571,6 +676,14 @@ namespace lible_b200
                         digestRI<C::SA, C::SB, C::SC, C::SD, false>(a, bi, ki, val, threadIdx.x, S::G);
                 }
                 __syncthreads();
+                // next task: the rest of this chunk, then the block's next chunk
+                t++;
+                if (t >= (chunk + 1) * CHB || t >= a.n_tasks)
+                {
+                    chunk += gridDim.x;
+                    t = chunk * CHB;
+                    cur = 0;
+                }
             }
         }
     }

@@ -29,7 +29,17 @@ namespace lible_b200
         auto kern = eriKernel<LA, LB, LC, LD, T>;
         long long grid;
         if constexpr (S::W == 0)
-            grid = std::min<long long>((a.n_tasks + S::block - 1) / S::block, (long long)num_sms * 64);
+        {
+            // one chunk of 8 warp-iterations per warp, at most 32 blocks per SM in flight
+            const long long chunks = (a.n_tasks + 8LL * S::QPW - 1) / (8LL * S::QPW);
+            grid = std::min<long long>((chunks + S::block / 32 - 1) / (S::block / 32), (long long)num_sms * 32);
+            if (S::smem > 48 * 1024)
+            {
+                cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::smem);
+                if (e != cudaSuccess)
+                    return e;
+            }
+        }
         else
         {
             if (S::smem > 48 * 1024)
@@ -42,7 +52,7 @@ namespace lible_b200
             cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, S::block, S::smem);
             if (e != cudaSuccess)
                 return e;
-            grid = std::min<long long>(a.n_tasks, (long long)num_sms * std::max(occ, 1) * 4);
+            grid = std::min<long long>((a.n_tasks + 7) / 8, (long long)num_sms * std::max(occ, 1) * 4);
         }
         kern<<<(unsigned)grid, S::block, S::smem, s>>>(a);
         return cudaGetLastError();

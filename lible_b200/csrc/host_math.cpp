@@ -72,13 +72,8 @@ namespace lible_b200
         return out;
     }
 
-    // Boys function F_n(x) on the grid x_k = 0.01 k, k = 0..3000, n = 0..kBoysCols-1.
-    // Top column by the convergent series F_N(x) = e^{-x} sum_i x^i / ((N+1/2)(N+3/2)...(N+i+1/2))
-    // stopped when a term falls below 1e-16, lower columns by downward recursion
-    // F_n = (2x F_{n+1} + e^{-x}) / (2n+1).  Same published method (Helgaker, Jorgensen, Olsen,
-    // eqs. 9.8.11-9.8.14) and constants as src/lible/ints/boys_function.cpp:40-69.
-    // Host evaluation with the same method as the device boysF<N>() (device_common.cuh).
-    void boysHost(int n, double x, const std::vector<double> &grid, double *F)
+    // Host evaluation with the same method and tables as the device boysF<N>() (device_common.cuh).
+    void boysHost(int n, double x, const std::vector<double> &tables, double *F)
     {
         if (x > kBoysLargeX)
         {
@@ -87,43 +82,54 @@ namespace lible_b200
                 F[k] = F[k - 1] * (k - 0.5) / x;
             return;
         }
-        const int iv = (int)(x / kBoysStep);
-        const double dx = x - iv * kBoysStep;
-        const double *row = grid.data() + (size_t)iv * kBoysCols + n;
-        double s = row[0], pk = 1.0, fact = 1.0;
-        for (int k = 1; k < 7; k++)
-        {
-            pk *= -dx;
-            fact *= k;
-            s += row[k] * pk / fact;
-        }
+        const int iv = (int)std::nearbyint(x / kBoysStep);
+        const double m = iv * kBoysStep - x;
+        const double *row = tables.data() + ((size_t)n * kBoysRows + iv) * kBoysTerms;
+        double s = row[kBoysTerms - 1];
+        for (int k = kBoysTerms - 2; k >= 0; k--)
+            s = s * m + row[k];
         F[n] = s;
         const double ex = std::exp(-x);
         for (int k = n - 1; k >= 0; k--)
             F[k] = (2.0 * x * F[k + 1] + ex) / (2 * k + 1);
     }
 
+    // Boys function tables (layout in lible_math.hpp).  At each grid point F_n(x_i) for
+    // n = 0..kBoysCols-1 is computed as the reference builds its grid: the top order by the
+    // convergent series F_N(x) = e^{-x} sum_i x^i / ((N+1/2)(N+3/2)...(N+i+1/2)) stopped when a term
+    // falls below 1e-16, lower orders by downward recursion F_n = (2x F_{n+1} + e^{-x}) / (2n+1)
+    // (Helgaker, Jorgensen, Olsen, eqs. 9.8.11-9.8.14; src/lible/ints/boys_function.cpp:40-69).
     std::vector<double> boysGrid()
     {
-        std::vector<double> g((size_t)kBoysRows * kBoysCols);
+        std::vector<double> g((size_t)(kBoysMaxN + 1) * kBoysRows * kBoysTerms);
         const int nmax = kBoysCols - 1;
-        for (int k = 0; k < kBoysRows; k++)
+        std::vector<double> col(kBoysCols);
+        for (int i = 0; i < kBoysRows; i++)
         {
-            double x = k * kBoysStep;
+            const double x = i * kBoysStep;
             double term = 1.0 / (2.0 * nmax + 1.0);
             double sum = term;
-            for (int i = 1;; i++)
+            for (int k = 1;; k++)
             {
-                term *= x / (nmax + 0.5 + i);
+                term *= x / (nmax + 0.5 + k);
                 sum += term;
                 if (std::fabs(term) < 1e-16)
                     break;
             }
-            double ex = std::exp(-x);
-            double *row = &g[(size_t)k * kBoysCols];
-            row[nmax] = ex * sum;
+            const double ex = std::exp(-x);
+            col[nmax] = ex * sum;
             for (int n = nmax - 1; n >= 0; n--)
-                row[n] = (2.0 * x * row[n + 1] + ex) / (2 * n + 1);
+                col[n] = (2.0 * x * col[n + 1] + ex) / (2 * n + 1);
+            for (int N = 0; N <= kBoysMaxN; N++)
+            {
+                double fact = 1.0;
+                for (int k = 0; k < kBoysTerms; k++)
+                {
+                    if (k > 0)
+                        fact *= k;
+                    g[((size_t)N * kBoysRows + i) * kBoysTerms + k] = col[N + k] / fact;
+                }
+            }
         }
         return g;
     }

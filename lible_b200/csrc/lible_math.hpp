@@ -24,9 +24,17 @@ namespace lible_b200
     constexpr int kMaxL = 5;          // highest shell angular momentum handled (aux h shells)
     constexpr int kMaxLPair = 2 * kMaxL;
     constexpr int kMaxLTotal = 14;    // highest L of a quartet (+1 for first derivatives)
-    constexpr int kBoysRows = 3001;   // grid x = 0, 0.01, ..., 30 (src/lible/ints/boys_function.hpp:112-122)
-    constexpr int kBoysCols = 24;     // F_n for n = 0 .. 23 (highest n needed: kMaxLTotal + 6)
-    constexpr double kBoysStep = 0.01;
+    // Boys tables: for every order N = 0..kBoysMaxN a table over x = 0, 0.05, ..., 30 whose row i
+    // holds F_{N+k}(x_i) / k!, k = 0..kBoysTerms-1, the Taylor coefficients of F_N about x_i.
+    // Expanding about the nearest grid point (|x - x_i| <= 0.025) with 10 terms truncates at
+    // 0.025^10/10! < 3e-23 relative; one table is 48 KB and stays resident in L1.  The reference
+    // grid is finer (step 0.01, 7 terms about the lower point, src/lible/ints/boys_function.hpp:112-122);
+    // both are accurate to the last bits.
+    constexpr int kBoysMaxN = 14;
+    constexpr int kBoysTerms = 10;
+    constexpr double kBoysStep = 0.05;
+    constexpr int kBoysRows = 601;
+    constexpr int kBoysCols = 24;     // F_n for n = 0 .. 23 computed when building the tables
     constexpr double kBoysLargeX = 30.0;
     constexpr double kPrimitiveThreshold = 1e-15;   // src/lible/ints/shell_pair_data.hpp:57
     constexpr double kBohrToAngstrom = 0.5291772083; // src/lible/ints/defs.hpp:9

@@ -331,3 +331,18 @@ def fp64_peak(structure):
     a, b = ctypes.c_double(), ctypes.c_double()
     _call(structure, "lible_gpu_fp64_peak", ctypes.byref(a), ctypes.byref(b))
     return a.value, b.value
+
+
+def jk_plan_classes(structure, schwarz=1e-12, precision="fp64", fp32_threshold=1e-4):
+    """Per class pair of the J/K plan (launch order): (la, lb, lc, ld), n_fp64, n_fp32, primitive
+    quartets, algorithmic FLOPs."""
+    opts = _opts(schwarz, precision, fp32_threshold)
+    n = ctypes.c_int()
+    _call(structure, "lible_gpu_jk_plan_classes", ctypes.byref(opts), ctypes.byref(n), None, None, None, None, None)
+    k = n.value
+    ls, n64, n32 = np.zeros(4 * k, np.int32), np.zeros(k, np.int64), np.zeros(k, np.int64)
+    prim, fl = np.zeros(k), np.zeros(k)
+    _call(structure, "lible_gpu_jk_plan_classes", ctypes.byref(opts), ctypes.byref(n), _ptr(ls), _ptr(n64), _ptr(n32),
+          _ptr(prim), _ptr(fl))
+    return [(tuple(int(x) for x in ls[4 * i:4 * i + 4]), int(n64[i]), int(n32[i]), float(prim[i]), float(fl[i]))
+            for i in range(k)]
