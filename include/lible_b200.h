@@ -90,6 +90,19 @@ int lible_gpu_eri4_batch(lible_gpu_ctx *ctx, int use_symm, int class_ab, int cla
 /* ERI4D1Kernel (eri_kernels.hpp:114-132): out[i] = 12 blocks [A,B,C,D] x [x,y,z], each [Sa][Sb][Sc][Sd]. */
 int lible_gpu_eri4d1_batch(lible_gpu_ctx *ctx, int use_symm, int class_ab, int class_cd, long long n,
                            const unsigned *pairs, double *out);
+/* lible_gpu_eri4_batch for callers that cannot allocate device memory (no counterpart in the
+ * reference).  A host program that has handed all free device memory to its own pool allocator, or
+ * that overlaps work on other streams and cannot accept the device-wide synchronisation cudaFree
+ * implies, can call this instead: it performs no cudaMalloc, cudaFree or other allocating call.
+ * The pair list is staged in a fixed 8 MiB buffer inside the library's device image (held on every
+ * GPU that loads the library until the process exits), so n may be at most 1048576 pairs; larger n
+ * returns LIBLE_GPU_EINVAL.  pairs must be host memory, out device memory of the context's GPU.
+ * The shell-pair classes must already be on the device: call lible_gpu_pair_classes(ctx, use_symm,
+ * ...) once first.  The first call on a device also looks up the buffer's device address
+ * (cudaGetSymbolAddress); make that first call before any stream capture.  All calls share the
+ * buffer: calls whose GPU work overlaps (other streams or contexts on the same device) race. */
+int lible_gpu_eri4_batch_noalloc(lible_gpu_ctx *ctx, int use_symm, int class_ab, int class_cd, long long n,
+                                 const unsigned *pairs, double *out);
 /* ERI3Kernel (eri_kernels.hpp:78-94): idx[2*i] = ipair_ab, idx[2*i+1] = ishell_c; out[i] = [Sa][Sb][Sc]. */
 int lible_gpu_eri3_batch(lible_gpu_ctx *ctx, int use_symm, int class_ab, int aux_class, long long n,
                          const unsigned *idx, double *out);

@@ -51,6 +51,7 @@ SIGNATURES = {
     "lible_gpu_aux_classes": [P, P, P, P],
     "lible_gpu_eri4_batch": [P, I, I, I, LL, P, P],
     "lible_gpu_eri4d1_batch": [P, I, I, I, LL, P, P],
+    "lible_gpu_eri4_batch_noalloc": [P, I, I, I, LL, P, P],
     "lible_gpu_eri3_batch": [P, I, I, I, LL, P, P],
     "lible_gpu_eri3d1_batch": [P, I, I, I, LL, P, P],
     "lible_gpu_eri2_batch": [P, I, I, LL, P, P],

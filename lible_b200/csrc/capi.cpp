@@ -12,6 +12,12 @@
 
 using namespace lible_b200;
 
+namespace lible_b200
+{
+    // noalloc.cu: device address of the allocation-free call's staging buffer on `device`.
+    uint32_t *noAllocScratch(int device, long long *max_pairs);
+}
+
 struct lible_gpu_ctx
 {
     std::unique_ptr<Engine> eng;
@@ -443,6 +449,25 @@ int lible_gpu_eri4d1_batch(lible_gpu_ctx *ctx, int use_symm, int class_ab, int c
                            const unsigned *pairs, double *out)
 {
     return batch4(ctx, use_symm, class_ab, class_cd, n, pairs, out, true);
+}
+
+int lible_gpu_eri4_batch_noalloc(lible_gpu_ctx *ctx, int use_symm, int class_ab, int class_cd, long long n,
+                                 const unsigned *pairs, double *out)
+{
+    return guard(ctx, [&](Engine &e) {
+        if (n < 0 || (n > 0 && (!pairs || !out)))
+            throw EngineError(kStatusInvalid, "invalid batch arguments");
+        long long max_pairs = 0;
+        uint32_t *scratch = noAllocScratch(e.device(), &max_pairs);
+        if (n > max_pairs)
+            throw EngineError(kStatusInvalid, "eri4 batch without allocation: n = " + std::to_string(n) +
+                                                  " exceeds the maximum of " + std::to_string(max_pairs) + " pairs");
+        if (n > 0 && !isDevice(out))
+            throw EngineError(kStatusInvalid, "eri4 batch without allocation: out must be device memory");
+        if (n > 0 && isDevice(pairs))
+            throw EngineError(kStatusInvalid, "eri4 batch without allocation: pairs must be host memory");
+        e.eri4BatchNoAlloc(use_symm != 0, class_ab, class_cd, n, pairs, out, scratch, max_pairs);
+    });
 }
 
 static int batch3(lible_gpu_ctx *ctx, int use_symm, int cab, int cx, long long n, const unsigned *idx, double *out,

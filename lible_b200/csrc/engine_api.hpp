@@ -112,6 +112,11 @@ namespace lible_b200
                        bool d1);
         void eri3Batch(bool use_symm, int cab, int cx, long long n, const uint32_t *idx_host, double *out_dev, bool d1);
         void eri2Batch(int ca, int cb, long long n, const uint32_t *idx_host, double *out_dev, bool d1);
+        // eri4Batch without any device allocation: the pair list is staged in `scratch` (device
+        // memory the caller owns, room for 2 * max_pairs indices); `out_dev` must be device memory.
+        // The class set must already exist on the device (built by an earlier pairClasses call).
+        void eri4BatchNoAlloc(bool use_symm, int cab, int ccd, long long n, const uint32_t *pairs_host,
+                              double *out_dev, uint32_t *scratch, long long max_pairs);
 
         // Direct J/K (device pointers).  J, K symmetric on return.
         void jk(const double *D_dev, double *J_dev, double *K_dev, const JKOptions &opt, JKStats *stats);
