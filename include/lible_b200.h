@@ -163,18 +163,23 @@ int lible_gpu_fp64_peak(lible_gpu_ctx *ctx, double *dfma_tflops, double *dmma_tf
 /* ---- J/K energy and its nuclear gradient (forward / backward pair) ----------------------------
  * forward:  E = 1/2 Tr(D J) - 1/4 Tr(D K)  (J, K from lible_gpu_jk with opts; J/K may be NULL).
  * backward: grad[3*atom + x] = dE/dR_{atom,x}, contracting the first-derivative integrals
- *           (ERI4D1Kernel semantics) with the two-particle density of E on the device. */
+ *           (ERI4D1Kernel semantics) with the two-particle density of E on the device, over the
+ *           same Schwarz-surviving quartets as the FP64 forward pass with opts->schwarz_threshold
+ *           (opts->precision is ignored: the gradient is FP64). */
 int lible_gpu_jk_energy_forward(lible_gpu_ctx *ctx, const double *D, const lible_gpu_jk_opts *opts,
                                 double *energy, double *J, double *K);
-int lible_gpu_jk_energy_backward(lible_gpu_ctx *ctx, const double *D, double *grad);
+int lible_gpu_jk_energy_backward(lible_gpu_ctx *ctx, const double *D, const lible_gpu_jk_opts *opts,
+                                 double *grad);
 
 /* ---- RI-J ------------------------------------------------------------------------------------
  * gamma_P = sum_mn (mn|P) D_mn; (P|Q) d = gamma (Cholesky, FP64); J_mn = sum_P (mn|P) d_P.
+ * Three-centre quartets with Q_mn Q_P < schwarz_threshold are skipped (Q_P = sqrt (P|P)).
  * gamma / dcoef outputs may be NULL. */
-int lible_gpu_rij(lible_gpu_ctx *ctx, const double *D, double *J, double *gamma, double *dcoef);
+int lible_gpu_rij(lible_gpu_ctx *ctx, const double *D, double schwarz_threshold, double *J, double *gamma,
+                  double *dcoef);
 /* The two contractions separately (either output may be NULL). */
-int lible_gpu_ri_contract(lible_gpu_ctx *ctx, const double *D, const double *dcoef, double *gamma,
-                          double *J);
+int lible_gpu_ri_contract(lible_gpu_ctx *ctx, const double *D, const double *dcoef, double schwarz_threshold,
+                          double *gamma, double *J);
 
 /* ---- host-only helpers (no GPU needed) --------------------------------------------------------
  * The host set-up the kernels consume, exposed for checking against the reference:

@@ -58,13 +58,13 @@ SIGNATURES = {
     "lible_gpu_eri2d1_batch": [P, I, I, LL, P, P],
     "lible_gpu_jk": [P, P, P, P, ctypes.POINTER(JKOpts), ctypes.POINTER(JKStats)],
     "lible_gpu_jk_energy_forward": [P, P, ctypes.POINTER(JKOpts), P, P, P],
-    "lible_gpu_jk_energy_backward": [P, P, P],
-    "lible_gpu_rij": [P, P, P, P, P],
+    "lible_gpu_jk_energy_backward": [P, P, ctypes.POINTER(JKOpts), P],
+    "lible_gpu_rij": [P, P, D, P, P, P],
     "lible_gpu_jk_plan": [P, ctypes.POINTER(JKOpts), ctypes.POINTER(JKPlanInfo)],
     "lible_gpu_stream": [P, ctypes.POINTER(P)],
     "lible_gpu_jk_plan_classes": [P, ctypes.POINTER(JKOpts), P, P, P, P, P, P],
     "lible_gpu_fp64_peak": [P, ctypes.POINTER(D), ctypes.POINTER(D)],
-    "lible_gpu_ri_contract": [P, P, P, P, P],
+    "lible_gpu_ri_contract": [P, P, P, D, P, P],
     "lible_host_spherical_trafo": [I, P, P, P, P],
     "lible_host_shell_norms": [I, I, P, P, P],
     "lible_host_pair_classes": [S, S, I, P, P, I, I, P, P, P, P],

@@ -658,7 +658,7 @@ int lible_gpu_jk_energy_forward(lible_gpu_ctx *ctx, const double *D, const lible
     });
 }
 
-int lible_gpu_jk_energy_backward(lible_gpu_ctx *ctx, const double *D, double *grad)
+int lible_gpu_jk_energy_backward(lible_gpu_ctx *ctx, const double *D, const lible_gpu_jk_opts *opts, double *grad)
 {
     return guard(ctx, [&](Engine &e) {
         if (!D || !grad)
@@ -666,12 +666,13 @@ int lible_gpu_jk_energy_backward(lible_gpu_ctx *ctx, const double *D, double *gr
         const size_t n = e.nao();
         DevArray d(D, n * n, true, e.stream());
         DevArray g(grad, 3 * (size_t)e.nAtoms(), false, e.stream());
-        e.jkGradient(d.ptr, g.ptr);
+        e.jkGradient(d.ptr, g.ptr, toOpts(opts).schwarz);
         g.copyOut();
     });
 }
 
-int lible_gpu_ri_contract(lible_gpu_ctx *ctx, const double *D, const double *dcoef, double *gamma, double *J)
+int lible_gpu_ri_contract(lible_gpu_ctx *ctx, const double *D, const double *dcoef, double schwarz_threshold,
+                          double *gamma, double *J)
 {
     return guard(ctx, [&](Engine &e) {
         if (!e.hasAux())
@@ -683,7 +684,7 @@ int lible_gpu_ri_contract(lible_gpu_ctx *ctx, const double *D, const double *dco
         DevArray j(J, n * n, false, e.stream());
         if ((gamma && !D) || (J && !dcoef))
             throw EngineError(kStatusInvalid, "missing input");
-        e.riContract(d.ptr, c.ptr, g.ptr, j.ptr);
+        e.riContract(d.ptr, c.ptr, g.ptr, j.ptr, schwarz_threshold);
         if (gamma)
             g.copyOut();
         if (J)
@@ -691,7 +692,8 @@ int lible_gpu_ri_contract(lible_gpu_ctx *ctx, const double *D, const double *dco
     });
 }
 
-int lible_gpu_rij(lible_gpu_ctx *ctx, const double *D, double *J, double *gamma, double *dcoef)
+int lible_gpu_rij(lible_gpu_ctx *ctx, const double *D, double schwarz_threshold, double *J, double *gamma,
+                  double *dcoef)
 {
     return guard(ctx, [&](Engine &e) {
         if (!e.hasAux())
@@ -706,7 +708,7 @@ int lible_gpu_rij(lible_gpu_ctx *ctx, const double *D, double *J, double *gamma,
         cudaCheck(cudaMalloc(&metric, na * na * sizeof(double)), "cudaMalloc");
         cudaCheck(cudaMalloc(&rhs, na * sizeof(double)), "cudaMalloc");
         cudaCheck(cudaMalloc(&info, sizeof(int)), "cudaMalloc");
-        e.riContract(d.ptr, nullptr, rhs, nullptr);
+        e.riContract(d.ptr, nullptr, rhs, nullptr, schwarz_threshold);
         if (gamma)
         {
             e.sync();
@@ -745,7 +747,7 @@ int lible_gpu_rij(lible_gpu_ctx *ctx, const double *D, double *J, double *gamma,
             else
                 cudaCheck(cudaMemcpy(dcoef, rhs, na * 8, cudaMemcpyDeviceToHost), "copy");
         }
-        e.riContract(nullptr, rhs, nullptr, j.ptr);
+        e.riContract(nullptr, rhs, nullptr, j.ptr, schwarz_threshold);
         j.copyOut();
         cudaFree(rhs);
     });

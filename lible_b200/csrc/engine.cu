@@ -367,6 +367,8 @@ namespace lible_b200
                             (void *)d.E, (void *)d.Et, (void *)d.Ef, (void *)d.Etf, (void *)d.E1,
                             (void *)d.E1t, (void *)d.Q})
                 cudaFree(p);
+        for (auto &o : cs.orders)
+            cudaFree(o.d_order);
         cs = ClassSet();
     }
 
@@ -378,6 +380,9 @@ namespace lible_b200
         for (auto &kv : plans_)
             freePlan(kv.second);
         plans_.clear();
+        for (auto &kv : ri_plans_)
+            freePlan(kv.second);
+        ri_plans_.clear();
         shells_.clear();
         aux_shells_.clear();
         nao_ = naux_ = 0;
@@ -887,11 +892,14 @@ namespace lible_b200
     // ------------------------------------------------------------------------------------------
     // Schwarz screening and the direct J/K build
 
+    // Schwarz factors Q_ab = max sqrt|(mn|mn)| of every pair, and the per-class Schwarz order:
+    // pairs grouped by their number of primitive pairs K, decreasing Q inside a group.
     void Engine::ensureSchwarz(ClassSet &cs)
     {
         if (cs.schwarz_done)
             return;
         auto batches = diagonalBatches(cs);
+        cs.orders.resize(cs.dev.size());
         for (size_t c = 0; c < cs.dev.size(); c++)
         {
             auto &d = cs.dev[c];
@@ -905,6 +913,26 @@ namespace lible_b200
                 d.Qh[i] = std::sqrt(m);
             }
             d.Q = devUpload(d.Qh, stream_);
+            const auto &Q = d.Qh;
+            const auto &pofs = cs.host[c].pofs;
+            auto K = [&](uint32_t x) { return pofs[x + 1] - pofs[x]; };
+            ClassOrder &o = cs.orders[c];
+            o.order.resize(Q.size());
+            std::iota(o.order.begin(), o.order.end(), 0u);
+            std::stable_sort(o.order.begin(), o.order.end(), [&](uint32_t x, uint32_t y) {
+                return K(x) != K(y) ? K(x) < K(y) : Q[x] > Q[y];
+            });
+            o.q.resize(Q.size());
+            o.kpre.assign(Q.size() + 1, 0.0);
+            for (size_t i = 0; i < Q.size(); i++)
+            {
+                o.q[i] = Q[o.order[i]];
+                o.kpre[i + 1] = o.kpre[i] + K(o.order[i]);
+                if (o.groups.empty() || o.groups.back().k != K(o.order[i]))
+                    o.groups.push_back({K(o.order[i]), (uint32_t)i, (uint32_t)i});
+                o.groups.back().end = (uint32_t)i + 1;
+            }
+            o.d_order = devUpload(o.order, stream_);
         }
         cudaCheck(cudaStreamSynchronize(stream_), "schwarz");
         cs.schwarz_done = true;
@@ -916,19 +944,91 @@ namespace lible_b200
             for (void *x : {(void *)cp.prefix64, (void *)cp.prefix32, (void *)cp.begin64, (void *)cp.begin32,
                             (void *)cp.majors})
                 cudaFree(x);
-        for (void *x : p.orders)
-            cudaFree(x);
         p = JKPlan();
     }
 
-    // Unique quartets (ab|cd), cd <= ab, kept iff Q_ab Q_cd >= thr.  The pairs of each class are
-    // grouped by their number of primitive pairs K and sorted by decreasing Q inside a group, so the
+    // Surviving quartets of one class pair, kept iff Q_bra Q_ket >= thr (and, with `triangle`, only
+    // the unique ones of a class paired with itself).  Both classes are in their Schwarz order, so the
     // surviving bras of a ket are a prefix of each bra group.  Tasks are enumerated ket-major per
     // (bra group, ket group) segment: "major" entries m = (ket pair, bra group) own the task range
     // [prefix[m], prefix[m+1]) whose bras are minor_order[minor_begin[m] + (t - prefix[m])].  All
     // quartets of a segment have the same K_ab and K_cd, so a warp's primitive loops run in lock
     // step.  With mixed precision a second (prefix, begin) pair covers the FP32 part of each range
-    // (Q_ab Q_cd < thr32).
+    // (Q_bra Q_ket < thr32).
+    Engine::JKClassPair Engine::buildClassPair(const ClassSet &bs, int cb, const ClassSet &ks, int ck, bool triangle,
+                                               double thr, double thr32, bool mixed)
+    {
+        const ClassOrder &ob = bs.orders[cb], &ok = ks.orders[ck];
+        // number of entries >= bound in the descending range q[b, e)
+        auto countAbove = [](const std::vector<double> &q, uint32_t b, uint32_t e, double bound) -> uint32_t {
+            return (uint32_t)(std::upper_bound(q.begin() + b, q.begin() + e, bound,
+                                               [](double x, double v) { return x > v; }) -
+                              (q.begin() + b));
+        };
+        JKClassPair cp;
+        cp.cb = cb;
+        cp.ck = ck;
+        std::vector<uint32_t> majors, b64, b32;
+        std::vector<unsigned long long> p64(1, 0), p32(1, 0);
+        double bra_prims64 = 0, bra_prims32 = 0;
+        for (size_t gb = 0; gb < ob.groups.size(); gb++)
+            for (size_t gc = 0; gc < ok.groups.size(); gc++)
+            {
+                if (triangle && gb < gc)
+                    continue;
+                const auto &B = ob.groups[gb], &C = ok.groups[gc];
+                for (uint32_t j = C.start; j < C.end; j++)
+                {
+                    const double qj = ok.q[j];
+                    const uint32_t lo = (triangle && gb == gc) ? j - C.start : 0u;
+                    uint32_t nall = qj > 0 ? countAbove(ob.q, B.start, B.end, thr / qj) : 0;
+                    if (thr <= 0)
+                        nall = B.end - B.start;
+                    uint32_t n64 = nall;
+                    if (mixed)
+                        n64 = qj > 0 ? std::min(nall, countAbove(ob.q, B.start, B.end, thr32 / qj)) : 0;
+                    nall = std::max(nall, lo);
+                    n64 = std::max(n64, lo);
+                    if (nall == lo)
+                        continue;
+                    majors.push_back(ok.order[j]);
+                    b64.push_back(B.start + lo);
+                    b32.push_back(B.start + n64);
+                    p64.push_back(p64.back() + (n64 - lo));
+                    p32.push_back(p32.back() + (nall - n64));
+                    const double kj = C.k;
+                    const double pr64 = ob.kpre[B.start + n64] - ob.kpre[B.start + lo];
+                    const double pr32 = ob.kpre[B.start + nall] - ob.kpre[B.start + n64];
+                    cp.prim64 += kj * pr64;
+                    cp.prim32 += kj * pr32;
+                    // bra-side work is counted per (bra primitive, ket pair)
+                    bra_prims64 += pr64;
+                    bra_prims32 += pr32;
+                }
+            }
+        cp.n64 = (long long)p64.back();
+        cp.n32 = (long long)p32.back();
+        const auto &B = bs.host[cb], &K = ks.host[ck];
+        const int L = B.la + B.lb + K.la + K.lb;
+        const double hab = nherm(B.la + B.lb), hcd = nherm(K.la + K.lb);
+        const double sab = nsph(B.la) * nsph(B.lb), scd = nsph(K.la) * nsph(K.lb);
+        const double per_prim =
+            (20 + 4 * L) + 3.0 * (L + 1) * (L + 2) * (L + 3) * (L + 4) / 24 + hab * hcd + 2 * hab * hcd * scd;
+        const double per_bra = 2 * sab * hab * scd;
+        cp.flops64 = cp.prim64 * per_prim + bra_prims64 * per_bra;
+        cp.flops32 = cp.prim32 * per_prim + bra_prims32 * per_bra;
+        cp.n_bra = (int)majors.size();
+        if (cp.n64 + cp.n32 == 0)
+            return cp;
+        cp.majors = devUpload(majors, stream_);
+        cp.prefix64 = devUpload(p64, stream_);
+        cp.prefix32 = devUpload(p32, stream_);
+        cp.begin64 = devUpload(b64, stream_);
+        cp.begin32 = devUpload(b32, stream_);
+        return cp;
+    }
+
+    // Unique quartets (ab|cd), class cd <= class ab, kept iff Q_ab Q_cd >= thr.
     Engine::JKPlan &Engine::jkPlan(double thr, double thr32, bool mixed)
     {
         ClassSet &cs = mainSet(true);
@@ -940,105 +1040,12 @@ namespace lible_b200
             return it->second;
         JKPlan plan;
         const size_t nc = cs.dev.size();
-        struct Group
-        {
-            uint32_t k, start, end;
-        };
-        std::vector<std::vector<uint32_t>> order(nc);
-        std::vector<std::vector<double>> qs(nc);
-        std::vector<std::vector<Group>> groups(nc);
-        std::vector<std::vector<double>> kpre(nc);
-        for (size_t c = 0; c < nc; c++)
-        {
-            const auto &Q = cs.dev[c].Qh;
-            const auto &pofs = cs.host[c].pofs;
-            auto K = [&](uint32_t x) { return pofs[x + 1] - pofs[x]; };
-            order[c].resize(Q.size());
-            std::iota(order[c].begin(), order[c].end(), 0u);
-            std::stable_sort(order[c].begin(), order[c].end(), [&](uint32_t x, uint32_t y) {
-                return K(x) != K(y) ? K(x) < K(y) : Q[x] > Q[y];
-            });
-            qs[c].resize(Q.size());
-            kpre[c].assign(Q.size() + 1, 0.0);
-            for (size_t i = 0; i < Q.size(); i++)
-            {
-                qs[c][i] = Q[order[c][i]];
-                kpre[c][i + 1] = kpre[c][i] + K(order[c][i]);
-                if (groups[c].empty() || groups[c].back().k != K(order[c][i]))
-                    groups[c].push_back({K(order[c][i]), (uint32_t)i, (uint32_t)i});
-                groups[c].back().end = (uint32_t)i + 1;
-            }
-            plan.orders.push_back(devUpload(order[c], stream_));
-        }
-        // number of entries >= bound in the descending range q[b, e)
-        auto countAbove = [](const std::vector<double> &q, uint32_t b, uint32_t e, double bound) -> uint32_t {
-            return (uint32_t)(std::upper_bound(q.begin() + b, q.begin() + e, bound,
-                                               [](double x, double v) { return x > v; }) -
-                              (q.begin() + b));
-        };
         for (size_t cb = 0; cb < nc; cb++)
             for (size_t ck = 0; ck <= cb; ck++)
             {
-                JKClassPair cp;
-                cp.cb = (int)cb;
-                cp.ck = (int)ck;
-                std::vector<uint32_t> majors, b64, b32;
-                std::vector<unsigned long long> p64(1, 0), p32(1, 0);
-                double bra_prims64 = 0, bra_prims32 = 0;
-                for (size_t gb = 0; gb < groups[cb].size(); gb++)
-                    for (size_t gc = 0; gc < groups[ck].size(); gc++)
-                    {
-                        if (cb == ck && gb < gc)
-                            continue;
-                        const Group &B = groups[cb][gb], &C = groups[ck][gc];
-                        for (uint32_t j = C.start; j < C.end; j++)
-                        {
-                            const double qj = qs[ck][j];
-                            const uint32_t lo = (cb == ck && gb == gc) ? j - C.start : 0u;
-                            uint32_t nall = qj > 0 ? countAbove(qs[cb], B.start, B.end, thr / qj) : 0;
-                            uint32_t n64 = nall;
-                            if (mixed)
-                                n64 = qj > 0 ? std::min(nall, countAbove(qs[cb], B.start, B.end, thr32 / qj)) : 0;
-                            nall = std::max(nall, lo);
-                            n64 = std::max(n64, lo);
-                            if (nall == lo)
-                                continue;
-                            majors.push_back(order[ck][j]);
-                            b64.push_back(B.start + lo);
-                            b32.push_back(B.start + n64);
-                            p64.push_back(p64.back() + (n64 - lo));
-                            p32.push_back(p32.back() + (nall - n64));
-                            const double kj = C.k;
-                            const double pr64 = kpre[cb][B.start + n64] - kpre[cb][B.start + lo];
-                            const double pr32 = kpre[cb][B.start + nall] - kpre[cb][B.start + n64];
-                            cp.prim64 += kj * pr64;
-                            cp.prim32 += kj * pr32;
-                            // bra-side work is counted per (bra primitive, ket pair)
-                            bra_prims64 += pr64;
-                            bra_prims32 += pr32;
-                        }
-                    }
-                cp.n64 = (long long)p64.back();
-                cp.n32 = (long long)p32.back();
-                {
-                    const auto &B = cs.host[cb], &K = cs.host[ck];
-                    const int L = B.la + B.lb + K.la + K.lb;
-                    const double hab = nherm(B.la + B.lb), hcd = nherm(K.la + K.lb);
-                    const double sab = nsph(B.la) * nsph(B.lb), scd = nsph(K.la) * nsph(K.lb);
-                    const double per_prim = (20 + 4 * L) + 3.0 * (L + 1) * (L + 2) * (L + 3) * (L + 4) / 24 + hab * hcd +
-                                            2 * hab * hcd * scd;
-                    const double per_bra = 2 * sab * hab * scd;
-                    cp.flops64 = cp.prim64 * per_prim + bra_prims64 * per_bra;
-                    cp.flops32 = cp.prim32 * per_prim + bra_prims32 * per_bra;
-                }
-                cp.n_bra = (int)majors.size();
+                JKClassPair cp = buildClassPair(cs, (int)cb, cs, (int)ck, cb == ck, thr, thr32, mixed);
                 if (cp.n64 + cp.n32 == 0)
                     continue;
-                cp.majors = devUpload(majors, stream_);
-                cp.prefix64 = devUpload(p64, stream_);
-                cp.prefix32 = devUpload(p32, stream_);
-                cp.begin64 = devUpload(b64, stream_);
-                cp.begin32 = devUpload(b32, stream_);
                 plan.n_quartets += cp.n64 + cp.n32;
                 plan.n_fp32 += cp.n32;
                 plan.n_prim += cp.prim64 + cp.prim32;
@@ -1047,13 +1054,47 @@ namespace lible_b200
                 plan.pairs.push_back(cp);
             }
         // most expensive class pairs first
-        std::stable_sort(plan.pairs.begin(), plan.pairs.end(),
-                         [](const JKClassPair &x, const JKClassPair &y) { return x.flops64 + x.flops32 > y.flops64 + y.flops32; });
+        std::stable_sort(plan.pairs.begin(), plan.pairs.end(), [](const JKClassPair &x, const JKClassPair &y) {
+            return x.flops64 + x.flops32 > y.flops64 + y.flops32;
+        });
         cudaCheck(cudaStreamSynchronize(stream_), "plan");
         plan.thr = thr;
         return plans_.emplace(key, std::move(plan)).first->second;
     }
 
+    // Three-centre (mn|P) quartets of every main pair class with every auxiliary shell class, kept iff
+    // Q_mn Q_P >= thr; the larger pair type is the bra (`swap` when that is the auxiliary class).
+    Engine::JKPlan &Engine::riPlan(double thr)
+    {
+        ClassSet &ms = mainSet(true);
+        ClassSet &xs = auxSet();
+        ensureSchwarz(ms);
+        ensureSchwarz(xs);
+        char key[64];
+        snprintf(key, sizeof(key), "%.6e", thr);
+        auto it = ri_plans_.find(key);
+        if (it != ri_plans_.end())
+            return it->second;
+        JKPlan plan;
+        for (size_t cb = 0; cb < ms.dev.size(); cb++)
+            for (size_t cx = 0; cx < xs.dev.size(); cx++)
+            {
+                const auto &B = ms.dev[cb], &X = xs.dev[cx];
+                const bool swap = pairType(B.la, B.lb) < pairType(X.la, X.lb);
+                JKClassPair cp = swap ? buildClassPair(xs, (int)cx, ms, (int)cb, false, thr, 0.0, false)
+                                      : buildClassPair(ms, (int)cb, xs, (int)cx, false, thr, 0.0, false);
+                cp.swap = swap;
+                if (cp.n64 == 0)
+                    continue;
+                plan.n_quartets += cp.n64;
+                plan.n_prim += cp.prim64;
+                plan.flops64 += cp.flops64;
+                plan.pairs.push_back(cp);
+            }
+        cudaCheck(cudaStreamSynchronize(stream_), "plan");
+        plan.thr = thr;
+        return ri_plans_.emplace(key, std::move(plan)).first->second;
+    }
 
     void Engine::jk(const double *D_dev, double *J_dev, double *K_dev, const JKOptions &opt, JKStats *stats)
     {
@@ -1075,7 +1116,7 @@ namespace lible_b200
             a.list = nullptr;
             a.major_ket = 1;
             a.major_order = cp.majors;
-            a.minor_order = plan.orders[cp.cb];
+            a.minor_order = cs.orders[cp.cb].d_order;
             a.n_major = cp.n_bra;
             a.same_class = cp.cb == cp.ck;
             a.mode = kJK;
@@ -1147,103 +1188,95 @@ namespace lible_b200
     // ------------------------------------------------------------------------------------------
     // J/K energy gradient (adjoint of the J/K build): dE/dR over all unique quartets.
 
-    void Engine::jkGradient(const double *D_dev, double *grad_dev)
+    // The quartets are those of the FP64 J/K plan with the same Schwarz threshold, so the gradient
+    // is the exact derivative of the energy lible_gpu_jk_energy_forward computes with that threshold.
+    void Engine::jkGradient(const double *D_dev, double *grad_dev, double schwarz)
     {
         ClassSet &cs = mainSet(true);
+        JKPlan &plan = jkPlan(schwarz, 0.0, false);
         const size_t n = nao_;
         cudaCheck(cudaMemsetAsync(grad_dev, 0, 3 * n_atoms_ * sizeof(double), stream_), "memset");
-        for (size_t cb = 0; cb < cs.dev.size(); cb++)
-            for (size_t ck = 0; ck <= cb; ck++)
-            {
-                const auto &B = cs.dev[cb], &K = cs.dev[ck];
-                std::vector<uint32_t> list;
-                for (uint32_t i = 0; i < B.n_pairs; i++)
-                    for (uint32_t j = 0; j < (cb == ck ? i + 1 : K.n_pairs); j++)
-                    {
-                        list.push_back(i);
-                        list.push_back(j);
-                    }
-                const long long nt = (long long)list.size() / 2;
-                if (nt == 0)
-                    continue;
-                uint32_t *dl = devUpload(list, stream_);
-                QuartetArgs a{};
-                a.bra = view(B);
-                a.ket = view(K);
-                a.boys = boys_;
-                a.list = dl;
-                a.n_tasks = nt;
-                a.same_class = cb == ck;
-                a.mode = kD1Grad;
-                a.D = D_dev;
-                a.nao = (int)n;
-                a.grad = grad_dev;
-                cudaCheck(lookupD1(pairType(B.la, B.lb), pairType(K.la, K.lb))(a, stream_, num_sms_), "grad kernel");
-                cudaCheck(cudaStreamSynchronize(stream_), "grad");
-                cudaFree(dl);
-            }
+        for (const auto &cp : plan.pairs)
+        {
+            const auto &B = cs.dev[cp.cb], &K = cs.dev[cp.ck];
+            QuartetArgs a{};
+            a.bra = view(B);
+            a.ket = view(K);
+            a.boys = boys_;
+            a.list = nullptr;
+            a.major_ket = 1;
+            a.major_order = cp.majors;
+            a.minor_order = cs.orders[cp.cb].d_order;
+            a.minor_begin = cp.begin64;
+            a.prefix = cp.prefix64;
+            a.n_major = cp.n_bra;
+            a.n_tasks = cp.n64;
+            a.same_class = cp.cb == cp.ck;
+            a.mode = kD1Grad;
+            a.D = D_dev;
+            a.nao = (int)n;
+            a.grad = grad_dev;
+            cudaCheck(lookupD1(pairType(B.la, B.lb), pairType(K.la, K.lb))(a, stream_, num_sms_), "grad kernel");
+        }
+        cudaCheck(cudaStreamSynchronize(stream_), "grad");
     }
 
     // ------------------------------------------------------------------------------------------
     // RI-J pieces: gamma_P = sum_mn (mn|P) D_mn and J_mn = sum_P (mn|P) d_P.
 
-    void Engine::riContract(const double *D_dev, const double *dcoef_dev, double *gamma_dev, double *J_dev)
+    void Engine::riContract(const double *D_dev, const double *dcoef_dev, double *gamma_dev, double *J_dev,
+                            double schwarz)
     {
         ClassSet &ms = mainSet(true);
         ClassSet &xs = auxSet();
+        JKPlan &plan = riPlan(schwarz);
         const size_t n = nao_;
         if (gamma_dev)
             cudaCheck(cudaMemsetAsync(gamma_dev, 0, naux_ * sizeof(double), stream_), "memset");
         if (J_dev)
             cudaCheck(cudaMemsetAsync(J_dev, 0, n * n * sizeof(double), stream_), "memset");
-        for (size_t cb = 0; cb < ms.dev.size(); cb++)
-            for (size_t cx = 0; cx < xs.dev.size(); cx++)
+        for (const auto &cp : plan.pairs)
+        {
+            // cp.cb / cp.ck index the bra / ket sets: (aux, main) when cp.swap, else (main, aux)
+            const ClassSet &bs = cp.swap ? xs : ms;
+            const auto &B = bs.dev[cp.cb];
+            const auto &K = (cp.swap ? ms : xs).dev[cp.ck];
+            QuartetArgs a{};
+            a.bra = view(B);
+            a.ket = view(K);
+            a.boys = boys_;
+            a.list = nullptr;
+            a.major_ket = 1;
+            a.major_order = cp.majors;
+            a.minor_order = bs.orders[cp.cb].d_order;
+            a.minor_begin = cp.begin64;
+            a.prefix = cp.prefix64;
+            a.n_major = cp.n_bra;
+            a.n_tasks = cp.n64;
+            a.aux_side = cp.swap ? 1 : 0;
+            a.D = D_dev;
+            a.dcoef = dcoef_dev;
+            a.gamma = gamma_dev;
+            a.J = J_dev;
+            a.nao = (int)n;
+            LaunchFn fn = lookupFwd64(pairType(B.la, B.lb), pairType(K.la, K.lb));
+            if (gamma_dev)
             {
-                const auto &B = ms.dev[cb], &X = xs.dev[cx];
-                if (B.n_pairs == 0 || X.n_pairs == 0)
-                    continue;
-                const int tb = pairType(B.la, B.lb), tx = pairType(X.la, X.lb);
-                const bool swap = tb < tx;
-                std::vector<uint32_t> list;
-                for (uint32_t i = 0; i < B.n_pairs; i++)
-                    for (uint32_t j = 0; j < X.n_pairs; j++)
-                    {
-                        list.push_back(swap ? j : i);
-                        list.push_back(swap ? i : j);
-                    }
-                const long long nt = (long long)list.size() / 2;
-                uint32_t *dl = devUpload(list, stream_);
-                QuartetArgs a{};
-                a.bra = view(swap ? X : B);
-                a.ket = view(swap ? B : X);
-                a.boys = boys_;
-                a.list = dl;
-                a.n_tasks = nt;
-                a.aux_side = swap ? 1 : 0;
-                a.D = D_dev;
-                a.dcoef = dcoef_dev;
-                a.gamma = gamma_dev;
-                a.J = J_dev;
-                a.nao = (int)n;
-                LaunchFn fn = lookupFwd64(swap ? tx : tb, swap ? tb : tx);
-                if (gamma_dev)
-                {
-                    a.mode = kRIGamma;
-                    cudaCheck(fn(a, stream_, num_sms_), "ri gamma");
-                }
-                if (J_dev)
-                {
-                    a.mode = kRIJ;
-                    cudaCheck(fn(a, stream_, num_sms_), "ri J");
-                }
-                cudaCheck(cudaStreamSynchronize(stream_), "ri");
-                cudaFree(dl);
+                a.mode = kRIGamma;
+                cudaCheck(fn(a, stream_, num_sms_), "ri gamma");
             }
+            if (J_dev)
+            {
+                a.mode = kRIJ;
+                cudaCheck(fn(a, stream_, num_sms_), "ri J");
+            }
+        }
         if (J_dev)
         {
             symmetrizeKernel<<<num_sms_ * 4, 256, 0, stream_>>>(J_dev, (long long)n);
             cudaCheck(cudaGetLastError(), "symmetrize");
         }
+        cudaCheck(cudaStreamSynchronize(stream_), "ri");
     }
 
     void Engine::sync()

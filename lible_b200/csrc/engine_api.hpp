@@ -130,13 +130,27 @@ namespace lible_b200
         };
         std::vector<JKClassInfo> jkPlanClasses(const JKOptions &opt);
         // Gradient of 1/2 Tr(DJ) - 1/4 Tr(DK) with respect to nuclear coordinates, [n_atoms][3].
-        void jkGradient(const double *D_dev, double *grad_dev);
+        void jkGradient(const double *D_dev, double *grad_dev, double schwarz);
         // RI-J contractions (either output may be null).
-        void riContract(const double *D_dev, const double *dcoef_dev, double *gamma_dev, double *J_dev);
+        void riContract(const double *D_dev, const double *dcoef_dev, double *gamma_dev, double *J_dev,
+                        double schwarz);
 
         void sync();
 
     private:
+        // Schwarz order of one class: pairs grouped by primitive-pair count K, decreasing Q inside
+        // a group (see jkPlan).
+        struct ClassOrder
+        {
+            struct Group
+            {
+                uint32_t k, start, end;
+            };
+            std::vector<uint32_t> order;
+            std::vector<double> q, kpre;
+            std::vector<Group> groups;
+            uint32_t *d_order = nullptr;
+        };
         struct ClassSet
         {
             bool built = false;
@@ -145,10 +159,12 @@ namespace lible_b200
             std::vector<DevPairClass> dev;
             std::vector<bool> swapped;
             std::vector<std::pair<int, int>> req_l;
+            std::vector<ClassOrder> orders;
         };
         struct JKClassPair
         {
             int cb = 0, ck = 0, n_bra = 0;
+            bool swap = false;  // RI plans: bra is the auxiliary class
             long long n64 = 0, n32 = 0;
             double prim64 = 0, prim32 = 0, flops64 = 0, flops32 = 0;
             unsigned long long *prefix64 = nullptr, *prefix32 = nullptr;
@@ -159,9 +175,13 @@ namespace lible_b200
             double thr = 0;
             long long n_quartets = 0, n_fp32 = 0;
             double n_prim = 0, flops64 = 0, flops32 = 0;
-            std::vector<uint32_t *> orders;
             std::vector<JKClassPair> pairs;
         };
+        // One class pair of a plan: bra class cb of set bs, ket class ck of set ks; `triangle`
+        // keeps only unique pairs when both are the same class of the same set.
+        JKClassPair buildClassPair(const ClassSet &bs, int cb, const ClassSet &ks, int ck, bool triangle,
+                                   double thr, double thr32, bool mixed);
+        JKPlan &riPlan(double thr);
 
         void clearStructure();
         void freeSet(ClassSet &cs);
@@ -192,6 +212,6 @@ namespace lible_b200
         size_t nao_ = 0, naux_ = 0;
         int n_atoms_ = 0, max_l_ = 0, max_l_aux_ = 0;
         ClassSet symm_, nosymm_, aux_;
-        std::map<std::string, JKPlan> plans_;
+        std::map<std::string, JKPlan> plans_, ri_plans_;
     };
 }

@@ -292,23 +292,36 @@ def jk_energy_forward(structure, D, schwarz=1e-12, precision="fp64", fp32_thresh
     """E = 1/2 Tr(DJ) - 1/4 Tr(DK)."""
     e = ctypes.c_double()
     opts = _opts(schwarz, precision, fp32_threshold)
-    _call(structure, "lible_gpu_jk_energy_forward", _ptr(_f64(D)), ctypes.byref(opts), ctypes.byref(e), None, None)
+    Dh = D if hasattr(D, "data_ptr") else _f64(D)
+    _call(structure, "lible_gpu_jk_energy_forward", _ptr(Dh), ctypes.byref(opts), ctypes.byref(e), None, None)
     return e.value
 
 
-def jk_energy_backward(structure, D):
-    """dE/dR of E = 1/2 Tr(DJ) - 1/4 Tr(DK), shape (n_atoms, 3), in Eh/bohr."""
+def jk_energy_backward(structure, D, schwarz=1e-12):
+    """dE/dR of E = 1/2 Tr(DJ) - 1/4 Tr(DK), shape (n_atoms, 3), in Eh/bohr, over the quartets the
+    FP64 forward pass keeps with the same Schwarz threshold."""
     g = np.empty((structure.n_atoms, 3))
-    _call(structure, "lible_gpu_jk_energy_backward", _ptr(_f64(D)), _ptr(g))
+    opts = _opts(schwarz, "fp64", 1e-4)
+    _call(structure, "lible_gpu_jk_energy_backward", _ptr(_f64(D)), ctypes.byref(opts), _ptr(g))
     return g
 
 
-def rij(structure, D):
+def rij(structure, D, schwarz=1e-12):
     """RI-J: returns J, gamma, d with (P|Q) d = gamma."""
     n, na = structure.nao, structure.naux
     J, g, d = np.empty((n, n)), np.empty(na), np.empty(na)
-    _call(structure, "lible_gpu_rij", _ptr(_f64(D)), _ptr(J), _ptr(g), _ptr(d))
+    _call(structure, "lible_gpu_rij", _ptr(_f64(D)), float(schwarz), _ptr(J), _ptr(g), _ptr(d))
     return J, g, d
+
+
+def ri_contract(structure, D=None, dcoef=None, schwarz=1e-12):
+    """gamma_P = sum (mn|P) D_mn (if D is given) and J_mn = sum_P (mn|P) d_P (if dcoef is given)."""
+    n, na = structure.nao, structure.naux
+    g = np.empty(na) if D is not None else None
+    J = np.empty((n, n)) if dcoef is not None else None
+    _call(structure, "lible_gpu_ri_contract", _ptr(_f64(D)) if D is not None else None,
+          _ptr(_f64(dcoef)) if dcoef is not None else None, float(schwarz), _ptr(g), _ptr(J))
+    return g, J
 
 
 def jk_plan(structure, schwarz=1e-12, precision="fp64", fp32_threshold=1e-4):

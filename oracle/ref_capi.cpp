@@ -707,6 +707,8 @@ int ref_rij_j(void *h, const double *dcoef, double *J)
                 const int nc = lints::numSphericals(c.l_);
                 for (size_t i = 0; i < ab.n_pairs_; i++)
                 {
+                    // a diagonal shell pair's batch already holds both (m, n) and (n, m)
+                    bool diag = ab.shell_idxs_[2 * i] == ab.shell_idxs_[2 * i + 1];
                     size_t oa = ab.offsets_sph_[2 * i], ob = ab.offsets_sph_[2 * i + 1];
                     for (size_t j = 0; j < c.n_shells_; j++)
                     {
@@ -718,8 +720,9 @@ int ref_rij_j(void *h, const double *dcoef, double *J)
                                 double s = 0;
                                 for (int z = 0; z < nc; z++)
                                     s += b(x, y, z) * dcoef[oc + z];
-                                J[(oa + x) * n + ob + y] = s;
-                                J[(ob + y) * n + oa + x] = s;
+                                J[(oa + x) * n + ob + y] += s;
+                                if (!diag)
+                                    J[(ob + y) * n + oa + x] += s;
                             }
                     }
                 }

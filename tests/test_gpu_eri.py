@@ -173,7 +173,7 @@ def test_jk_gradient_vs_reference_and_fd():
     Z, xyz, rng = water_cluster(2, seed=3)
     s = L.Structure("cc-pvdz", Z, xyz, units="bohr")
     D = random_density(s.nao, 10, rng)
-    g = L.jk_energy_backward(s, D)
+    g = L.jk_energy_backward(s, D, schwarz=0.0)
     gr = R.RefStructure("cc-pvdz", Z, xyz).jk_grad(D)
     assert np.abs(g - gr).max() <= 1e-10
     # central finite differences of the forward energy on two coordinates
@@ -186,3 +186,53 @@ def test_jk_gradient_vs_reference_and_fd():
             e.append(L.jk_energy_forward(L.Structure("cc-pvdz", Z, c, units="bohr"), D, schwarz=0.0))
         fd = (e[0] - e[1]) / (2 * h)
         assert abs(fd - g[atom, x]) <= 1e-6
+
+
+def test_jk_gradient_screened_matches_screened_energy():
+    # the backward pass keeps exactly the quartets of the forward pass at the same threshold
+    Z, xyz, rng = water_cluster(3, seed=4)
+    s = L.Structure("cc-pvdz", Z, xyz, units="bohr")
+    D = random_density(s.nao, 15, rng)
+    thr = 1e-10
+    g = L.jk_energy_backward(s, D, schwarz=thr)
+    h = 1e-4
+    for atom, x in [(1, 1), (6, 0)]:
+        e = []
+        for sgn in (1, -1):
+            c = xyz.copy()
+            c[atom, x] += sgn * h
+            e.append(L.jk_energy_forward(L.Structure("cc-pvdz", Z, c, units="bohr"), D, schwarz=thr))
+        assert abs((e[0] - e[1]) / (2 * h) - g[atom, x]) <= 1e-6
+
+
+def test_ri_contractions_vs_reference_kernels():
+    Z, xyz, rng = water_cluster(2, seed=8)
+    aux = "def2-universal-jkfit"
+    s = L.Structure("cc-pvdz", Z, xyz, aux, units="bohr")
+    r = R.RefStructure("cc-pvdz", Z, xyz, aux=aux)
+    D = random_density(s.nao, 10, rng)
+    g, _ = L.ri_contract(s, D=D, schwarz=0.0)
+    gr = r.rij_gamma(D)
+    assert np.abs(g - gr).max() <= 1e-11
+    d = np.random.default_rng(1).standard_normal(s.naux)
+    _, J = L.ri_contract(s, dcoef=d, schwarz=0.0)
+    assert np.abs(J - r.rij_j(d)).max() <= 1e-11
+    # full RI-J against a CPU solve of the reference's metric
+    J, gamma, dc = L.rij(s, D, schwarz=0.0)
+    M = r.eri2()
+    dref = np.linalg.solve(M, gr)
+    assert np.abs(dc - dref).max() <= 1e-7 * max(1.0, np.abs(dref).max())
+    assert np.abs(J - r.rij_j(dref)).max() <= 1e-8
+
+
+def test_mixed_precision_jk_error_small():
+    Z, xyz, rng = water_cluster(4, seed=12)
+    s = L.Structure("cc-pvdz", Z, xyz, units="bohr")
+    D = random_density(s.nao, 20, rng)
+    J, K, st = L.jk(s, D, 1e-12, "fp64")
+    Jm, Km, stm = L.jk(s, D, 1e-12, "mixed", 1e-4)
+    assert stm["n_fp32"] > 0
+    E = np.sum(D * (0.5 * J - 0.25 * K))
+    Em = np.sum(D * (0.5 * Jm - 0.25 * Km))
+    assert abs(E - Em) <= 1e-8
+    assert np.linalg.norm(Jm - J) <= 1e-6 and np.linalg.norm(Km - K) <= 1e-6
