@@ -48,7 +48,8 @@ namespace lible_b200
     struct QuartetArgs
     {
         PairView bra, ket;
-        const double *boys;               // Boys tables [kBoysMaxN + 1][kBoysRows][kBoysTerms]
+        const double *boys;               // Boys tables [kBoysMaxN + 1][kBoysTerms][kBoysPitch]
+        const float *boys_f;              // FP32 Boys tables [kBoysMaxN + 1][kBoysTermsF][kBoysPitch]
         // task enumeration: explicit (bra pair, ket pair) list, or the implicit Schwarz prefix form:
         // task t belongs to major position i with prefix[i] <= t < prefix[i+1] and pairs with
         // minor position minor_begin[i] + (t - prefix[i]).  major_ket = 1 enumerates ket-major
@@ -62,6 +63,11 @@ namespace lible_b200
         int n_major;
         int major_ket;
         int same_class;                   // bra and ket classes are the same pair list
+        // work queue (optional): chunk c covers tasks [chunks[c], chunks[c+1]); workers claim chunk
+        // indices from *counter (zeroed before the launch) until n_chunks is reached
+        const unsigned long long *chunks;
+        long long n_chunks;
+        unsigned long long *counter;
         // epilogue
         int mode;
         int flags;                        // kStore: bit0 swap bra shells, bit1 swap ket shells, bit2 swap bra/ket
@@ -210,14 +216,45 @@ namespace lible_b200
         return __longlong_as_double(__double_as_longlong(p) + k * 4503599627370496LL);
     }
 
+    // Shared-memory load of a double / float (explicit ld.shared, so table lookups never fall back
+    // to generic addressing).
+    __device__ __forceinline__ double ldsD(const double *p)
+    {
+        double v;
+        asm volatile("ld.shared.f64 %0, [%1];" : "=d"(v) : "r"((unsigned)__cvta_generic_to_shared(p)));
+        return v;
+    }
+    __device__ __forceinline__ float ldsF(const float *p)
+    {
+        float v;
+        asm volatile("ld.shared.f32 %0, [%1];" : "=f"(v) : "r"((unsigned)__cvta_generic_to_shared(p)));
+        return v;
+    }
+
+    // Copies the order-N Boys table (kBoysTerms x kBoysPitch doubles, or the FP32 one) into shared
+    // memory; the caller synchronises the block afterwards.
+    __device__ __forceinline__ void stageBoys(const double *__restrict__ tables, int N, double *dst)
+    {
+        const double *src = tables + (size_t)N * kBoysTerms * kBoysPitch;
+        for (int e = threadIdx.x; e < kBoysTerms * kBoysPitch; e += blockDim.x)
+            dst[e] = __ldg(src + e);
+    }
+    __device__ __forceinline__ void stageBoys(const float *__restrict__ tables, int N, float *dst)
+    {
+        const float *src = tables + (size_t)N * kBoysTermsF * kBoysPitch;
+        for (int e = threadIdx.x; e < kBoysTermsF * kBoysPitch; e += blockDim.x)
+            dst[e] = __ldg(src + e);
+    }
+
     // Boys function F_n(x), n = 0..N.  Reference method (src/lible/ints/boys_function.hpp:68-109):
-    // Taylor expansion of F_N about a grid point (7 terms, step 0.01) followed by downward
-    // recursion, and for x > 30 the asymptotic F_0 = sqrt(pi/x)/2 with upward recursion.
-    // Here the expansion point is the nearest grid point (|x - x_i| <= 0.005, half the reference's
-    // truncation interval), found with the 1.5*2^52 rounding trick, and e^{-x} comes from expNeg(),
-    // so the only special-function instruction on this path is the asymptote's rsqrt.
-    template <int N>
-    __device__ __forceinline__ void boysF(double x, const double *__restrict__ grid, double *F)
+    // Taylor expansion of F_N about a grid point followed by downward recursion, and for x > 30 the
+    // asymptotic F_0 = sqrt(pi/x)/2 with upward recursion.  Here the expansion point is the nearest
+    // integer (|x - x_i| <= 1/2, 16 terms; table layout in lible_math.hpp), found with the
+    // 1.5*2^52 rounding trick, and e^{-x} comes from expNeg(), so the only special-function
+    // instruction on this path is the asymptote's rsqrt.  `tab` is the order-N table, in shared
+    // memory when SMEM (staged by stageBoys), else in global memory (a.boys + N * terms * pitch).
+    template <int N, bool SMEM>
+    __device__ __forceinline__ void boysF(double x, const double *__restrict__ tab, double *F)
     {
         if (x > kBoysLargeX)
         {
@@ -231,29 +268,55 @@ namespace lible_b200
             return;
         }
         constexpr double kMagic = 6755399441055744.0;  // 1.5 * 2^52
-        const double t = fma(x, 1.0 / kBoysStep, kMagic);
-        const long long iv = __double_as_longlong(t) - __double_as_longlong(kMagic);
-        const double m = fma(t - kMagic, kBoysStep, -x);  // x_i - x
-        // row of 10 coefficients F_{N+k}(x_i)/k! (80 bytes, 16-byte aligned)
-        const double2 *row = reinterpret_cast<const double2 *>(grid + ((size_t)N * kBoysRows + iv) * kBoysTerms);
-        static_assert(kBoysTerms == 10, "row load below assumes 10 terms");
-        const double2 c01 = __ldg(row), c23 = __ldg(row + 1), c45 = __ldg(row + 2), c67 = __ldg(row + 3),
-                      c89 = __ldg(row + 4);
-        double s = fma(c89.y, m, c89.x);
-        s = fma(s, m, c67.y);
-        s = fma(s, m, c67.x);
-        s = fma(s, m, c45.y);
-        s = fma(s, m, c45.x);
-        s = fma(s, m, c23.y);
-        s = fma(s, m, c23.x);
-        s = fma(s, m, c01.y);
-        s = fma(s, m, c01.x);
+        const double t = x + kMagic;                    // nearest integer, exactly
+        const int iv = (int)(__double_as_longlong(t) - __double_as_longlong(kMagic));
+        const double m = (t - kMagic) - x;              // x_i - x
+        const double *c = tab + iv;
+        double s = SMEM ? ldsD(c + (kBoysTerms - 1) * kBoysPitch) : __ldg(c + (kBoysTerms - 1) * kBoysPitch);
+#pragma unroll
+        for (int k = kBoysTerms - 2; k >= 0; k--)
+            s = fma(s, m, SMEM ? ldsD(c + k * kBoysPitch) : __ldg(c + k * kBoysPitch));
         F[N] = s;
         const double ex = expNeg(x);
         const double x2 = 2.0 * x;
 #pragma unroll
         for (int k = N - 1; k >= 0; k--)
             F[k] = (x2 * F[k + 1] + ex) * (1.0 / (2 * k + 1));
+    }
+
+    // The same function for quartets evaluated in FP32: the large-x asymptote and the downward
+    // recursion stay FP64, while the Taylor sum of F_N (10 float terms from the shared-memory FP32
+    // table) and e^{-x} (MUFU ex2) are single precision, so every F_k carries FP32 relative accuracy.
+    template <int N>
+    __device__ __forceinline__ void boysF32(double x, const float *__restrict__ tabf, double *F)
+    {
+        if (x > kBoysLargeX)
+        {
+            const double rs = rsqrt(x);
+            const double rx = rs * rs;
+            F[0] = 0.88622692545275801365 * rs;
+#pragma unroll
+            for (int k = 1; k <= N; k++)
+                F[k] = F[k - 1] * ((k - 0.5) * rx);
+            return;
+        }
+        const float xf = (float)x;
+        const int iv = __float2int_rn(xf);
+        const float m = (float)iv - xf;
+        const float *c = tabf + iv;
+        float s = ldsF(c + (kBoysTermsF - 1) * kBoysPitch);
+#pragma unroll
+        for (int k = kBoysTermsF - 2; k >= 0; k--)
+            s = fmaf(s, m, ldsF(c + k * kBoysPitch));
+        F[N] = (double)s;
+        if constexpr (N > 0)
+        {
+            const double ex = (double)__expf(-xf);
+            const double x2 = 2.0 * x;
+#pragma unroll
+            for (int k = N - 1; k >= 0; k--)
+                F[k] = (x2 * F[k + 1] + ex) * (1.0 / (2 * k + 1));
+        }
     }
 
     // Hermite Coulomb integrals R_{tuv} = R^{(0)}_{tuv} for t+u+v <= L in registers, by the

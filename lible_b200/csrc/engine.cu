@@ -329,6 +329,7 @@ namespace lible_b200
         cudaCheck(cudaGetDeviceProperties(&prop, device), "cudaGetDeviceProperties");
         num_sms_ = prop.multiProcessorCount;
         boys_ = devUpload(boysGrid(), stream_);
+        boys_f_ = devUpload(boysGridF(), stream_);
         std::vector<int> rc;
         std::vector<double> val;
         sph_ofs_.assign(kMaxL + 2, 0);
@@ -355,6 +356,7 @@ namespace lible_b200
         for (void *p : persistent_)
             cudaFree(p);
         cudaFree(boys_);
+        cudaFree(boys_f_);
         cudaFree(sph_rc_);
         cudaFree(sph_val_);
         cudaStreamDestroy(stream_);
@@ -591,6 +593,7 @@ namespace lible_b200
         a.bra = view(swap ? ket : bra);
         a.ket = view(swap ? bra : ket);
         a.boys = boys_;
+        a.boys_f = boys_f_;
         a.n_tasks = n;
         a.same_class = same_class ? 1 : 0;
         a.flags = (bra_swapped ? 1 : 0) | (ket_swapped ? 2 : 0) | (swap ? 4 : 0);
@@ -942,9 +945,57 @@ namespace lible_b200
     {
         for (auto &cp : p.pairs)
             for (void *x : {(void *)cp.prefix64, (void *)cp.prefix32, (void *)cp.begin64, (void *)cp.begin32,
-                            (void *)cp.majors})
+                            (void *)cp.majors, (void *)cp.chunks64, (void *)cp.chunks32})
                 cudaFree(x);
+        cudaFree(p.counters);
         p = JKPlan();
+    }
+
+    // Cuts a task sequence into work-queue chunks.  Tasks come in runs (major entries) of n[i] tasks
+    // costing c[i] each (primitive quartets plus a fixed per-quartet overhead).  A chunk closes once
+    // it holds the cost of `unit` tasks of the most expensive run (one full worker step of the
+    // heaviest quartets) or `max_tasks` tasks, whichever comes first; with the heaviest runs first
+    // in the task order and chunks claimed dynamically, the last chunks to finish are cheap ones.
+    static std::vector<unsigned long long> costChunks(const std::vector<unsigned long long> &n,
+                                                      const std::vector<double> &c, int unit, int max_tasks)
+    {
+        double cmax = 0;
+        for (size_t i = 0; i < n.size(); i++)
+            if (n[i])
+                cmax = std::max(cmax, c[i]);
+        const double C = (double)std::max(unit, 1) * cmax;
+        std::vector<unsigned long long> ch(1, 0);
+        unsigned long long pos = 0, cnt = 0;
+        double acc = 0;
+        for (size_t i = 0; i < n.size(); i++)
+        {
+            unsigned long long left = n[i];
+            while (left > 0)
+            {
+                const unsigned long long by_cost =
+                    std::max<unsigned long long>(1, (unsigned long long)std::ceil((C - acc) / c[i]));
+                const unsigned long long by_count = (unsigned long long)max_tasks - cnt;
+                const unsigned long long k = std::min(by_cost, by_count);
+                if (k > left)
+                {
+                    acc += (double)left * c[i];
+                    cnt += left;
+                    pos += left;
+                    left = 0;
+                }
+                else
+                {
+                    pos += k;
+                    left -= k;
+                    ch.push_back(pos);
+                    acc = 0;
+                    cnt = 0;
+                }
+            }
+        }
+        if (ch.back() != pos)
+            ch.push_back(pos);
+        return ch;
     }
 
     // Surviving quartets of one class pair, kept iff Q_bra Q_ket >= thr (and, with `triangle`, only
@@ -954,7 +1005,8 @@ namespace lible_b200
     // [prefix[m], prefix[m+1]) whose bras are minor_order[minor_begin[m] + (t - prefix[m])].  All
     // quartets of a segment have the same K_ab and K_cd, so a warp's primitive loops run in lock
     // step.  With mixed precision a second (prefix, begin) pair covers the FP32 part of each range
-    // (Q_bra Q_ket < thr32).
+    // (Q_bra Q_ket < thr32).  Segments are visited heaviest first (decreasing K_ab K_cd) and each task
+    // sequence is cut into work-queue chunks (costChunks) that the kernels claim dynamically.
     Engine::JKClassPair Engine::buildClassPair(const ClassSet &bs, int cb, const ClassSet &ks, int ck, bool triangle,
                                                double thr, double thr32, bool mixed)
     {
@@ -970,10 +1022,14 @@ namespace lible_b200
         cp.ck = ck;
         std::vector<uint32_t> majors, b64, b32;
         std::vector<unsigned long long> p64(1, 0), p32(1, 0);
+        std::vector<unsigned long long> run64, run32;  // tasks per major entry
+        std::vector<double> cost;                      // primitive quartets per task of the entry
         double bra_prims64 = 0, bra_prims32 = 0;
-        for (size_t gb = 0; gb < ob.groups.size(); gb++)
-            for (size_t gc = 0; gc < ok.groups.size(); gc++)
+        // groups are in increasing K; walk them backwards so the heaviest segments come first
+        for (size_t gbr = ob.groups.size(); gbr-- > 0;)
+            for (size_t gcr = ok.groups.size(); gcr-- > 0;)
             {
+                const size_t gb = gbr, gc = gcr;
                 if (triangle && gb < gc)
                     continue;
                 const auto &B = ob.groups[gb], &C = ok.groups[gc];
@@ -996,6 +1052,9 @@ namespace lible_b200
                     b32.push_back(B.start + n64);
                     p64.push_back(p64.back() + (n64 - lo));
                     p32.push_back(p32.back() + (nall - n64));
+                    run64.push_back(n64 - lo);
+                    run32.push_back(nall - n64);
+                    cost.push_back((double)C.k * B.k + 4.0);
                     const double kj = C.k;
                     const double pr64 = ob.kpre[B.start + n64] - ob.kpre[B.start + lo];
                     const double pr32 = ob.kpre[B.start + nall] - ob.kpre[B.start + n64];
@@ -1025,6 +1084,17 @@ namespace lible_b200
         cp.prefix32 = devUpload(p32, stream_);
         cp.begin64 = devUpload(b64, stream_);
         cp.begin32 = devUpload(b32, stream_);
+        const int tb = pairType(B.la, B.lb), tk = pairType(K.la, K.lb);
+        for (int fp32 = 0; fp32 < 2; fp32++)
+        {
+            const long long n = fp32 ? cp.n32 : cp.n64;
+            const int unit = unitFwd(tb, tk, fp32 == 1);
+            if (n == 0 || unit == 0)
+                continue;
+            auto ch = costChunks(fp32 ? run32 : run64, cost, unit, 8 * unit);
+            (fp32 ? cp.n_chunks32 : cp.n_chunks64) = (long long)ch.size() - 1;
+            (fp32 ? cp.chunks32 : cp.chunks64) = devUpload(ch, stream_);
+        }
         return cp;
     }
 
@@ -1057,6 +1127,7 @@ namespace lible_b200
         std::stable_sort(plan.pairs.begin(), plan.pairs.end(), [](const JKClassPair &x, const JKClassPair &y) {
             return x.flops64 + x.flops32 > y.flops64 + y.flops32;
         });
+        plan.counters = devAlloc<unsigned long long>(2 * std::max<size_t>(plan.pairs.size(), 1));
         cudaCheck(cudaStreamSynchronize(stream_), "plan");
         plan.thr = thr;
         return plans_.emplace(key, std::move(plan)).first->second;
@@ -1091,6 +1162,7 @@ namespace lible_b200
                 plan.flops64 += cp.flops64;
                 plan.pairs.push_back(cp);
             }
+        plan.counters = devAlloc<unsigned long long>(2 * std::max<size_t>(plan.pairs.size(), 1));
         cudaCheck(cudaStreamSynchronize(stream_), "plan");
         plan.thr = thr;
         return ri_plans_.emplace(key, std::move(plan)).first->second;
@@ -1106,13 +1178,17 @@ namespace lible_b200
         const size_t n = nao_;
         cudaCheck(cudaMemsetAsync(J_dev, 0, n * n * sizeof(double), stream_), "memset");
         cudaCheck(cudaMemsetAsync(K_dev, 0, n * n * sizeof(double), stream_), "memset");
-        for (const auto &cp : plan.pairs)
+        cudaCheck(cudaMemsetAsync(plan.counters, 0, 2 * plan.pairs.size() * sizeof(unsigned long long), stream_),
+                  "memset");
+        for (size_t ip = 0; ip < plan.pairs.size(); ip++)
         {
+            const auto &cp = plan.pairs[ip];
             const auto &B = cs.dev[cp.cb], &K = cs.dev[cp.ck];
             QuartetArgs a{};
             a.bra = view(B);
             a.ket = view(K);
             a.boys = boys_;
+            a.boys_f = boys_f_;
             a.list = nullptr;
             a.major_ket = 1;
             a.major_order = cp.majors;
@@ -1128,12 +1204,18 @@ namespace lible_b200
             a.n_tasks = cp.n64;
             a.prefix = cp.prefix64;
             a.minor_begin = cp.begin64;
+            a.chunks = cp.chunks64;
+            a.n_chunks = cp.n_chunks64;
+            a.counter = plan.counters + 2 * ip;
             cudaCheck(lookupFwd64(tb, tk)(a, stream_, num_sms_), "jk kernel");
             if (cp.n32 > 0)
             {
                 a.n_tasks = cp.n32;
                 a.prefix = cp.prefix32;
                 a.minor_begin = cp.begin32;
+                a.chunks = cp.chunks32;
+                a.n_chunks = cp.n_chunks32;
+                a.counter = plan.counters + 2 * ip + 1;
                 cudaCheck(lookupFwd32(tb, tk)(a, stream_, num_sms_), "jk kernel fp32");
             }
         }
@@ -1203,6 +1285,7 @@ namespace lible_b200
             a.bra = view(B);
             a.ket = view(K);
             a.boys = boys_;
+            a.boys_f = boys_f_;
             a.list = nullptr;
             a.major_ket = 1;
             a.major_order = cp.majors;
@@ -1235,8 +1318,11 @@ namespace lible_b200
             cudaCheck(cudaMemsetAsync(gamma_dev, 0, naux_ * sizeof(double), stream_), "memset");
         if (J_dev)
             cudaCheck(cudaMemsetAsync(J_dev, 0, n * n * sizeof(double), stream_), "memset");
-        for (const auto &cp : plan.pairs)
+        cudaCheck(cudaMemsetAsync(plan.counters, 0, 2 * plan.pairs.size() * sizeof(unsigned long long), stream_),
+                  "memset");
+        for (size_t ip = 0; ip < plan.pairs.size(); ip++)
         {
+            const auto &cp = plan.pairs[ip];
             // cp.cb / cp.ck index the bra / ket sets: (aux, main) when cp.swap, else (main, aux)
             const ClassSet &bs = cp.swap ? xs : ms;
             const auto &B = bs.dev[cp.cb];
@@ -1245,6 +1331,7 @@ namespace lible_b200
             a.bra = view(B);
             a.ket = view(K);
             a.boys = boys_;
+            a.boys_f = boys_f_;
             a.list = nullptr;
             a.major_ket = 1;
             a.major_order = cp.majors;
@@ -1260,13 +1347,17 @@ namespace lible_b200
             a.J = J_dev;
             a.nao = (int)n;
             LaunchFn fn = lookupFwd64(pairType(B.la, B.lb), pairType(K.la, K.lb));
+            a.chunks = cp.chunks64;
+            a.n_chunks = cp.n_chunks64;
             if (gamma_dev)
             {
+                a.counter = plan.counters + 2 * ip;
                 a.mode = kRIGamma;
                 cudaCheck(fn(a, stream_, num_sms_), "ri gamma");
             }
             if (J_dev)
             {
+                a.counter = plan.counters + 2 * ip + 1;
                 a.mode = kRIJ;
                 cudaCheck(fn(a, stream_, num_sms_), "ri J");
             }

@@ -24,6 +24,7 @@ namespace lible_b200
 
     std::vector<SphTerm> sphericalTrafo(int l);
     std::vector<double> boysGrid();
+    std::vector<float> boysGridF();
     void boysHost(int n, double x, const std::vector<double> &grid, double *F);
 
     struct BasisShell

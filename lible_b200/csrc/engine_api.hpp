@@ -169,6 +169,9 @@ namespace lible_b200
             double prim64 = 0, prim32 = 0, flops64 = 0, flops32 = 0;
             unsigned long long *prefix64 = nullptr, *prefix32 = nullptr;
             uint32_t *begin64 = nullptr, *begin32 = nullptr, *majors = nullptr;
+            // work-queue chunks of about equal primitive-quartet cost (task boundaries)
+            unsigned long long *chunks64 = nullptr, *chunks32 = nullptr;
+            long long n_chunks64 = 0, n_chunks32 = 0;
         };
         struct JKPlan
         {
@@ -176,6 +179,7 @@ namespace lible_b200
             long long n_quartets = 0, n_fp32 = 0;
             double n_prim = 0, flops64 = 0, flops32 = 0;
             std::vector<JKClassPair> pairs;
+            unsigned long long *counters = nullptr;  // two work-queue counters per class pair
         };
         // One class pair of a plan: bra class cb of set bs, ket class ck of set ks; `triangle`
         // keeps only unique pairs when both are the same class of the same set.
@@ -202,6 +206,7 @@ namespace lible_b200
         int num_sms_ = 0;
         cudaStream_t stream_ = nullptr;
         double *boys_ = nullptr;
+        float *boys_f_ = nullptr;
         int *sph_rc_ = nullptr;
         double *sph_val_ = nullptr;
         std::vector<int> sph_ofs_;

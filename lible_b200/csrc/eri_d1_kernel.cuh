@@ -135,7 +135,7 @@ namespace lible_b200
                         const double X = P.y - Q.y, Y = P.z - Q.z, Z = P.w - Q.w;
                         const double fac = 34.986836655249725 * rs * P.ip * Q.ip;
                         double F[L1 + 1];
-                        boysF<L1>(alpha * (X * X + Y * Y + Z * Z), a.boys, F);
+                        boysF<L1, false>(alpha * (X * X + Y * Y + Z * Z), a.boys + L1 * kBoysTerms * kBoysPitch, F);
                         const double m2a = -2.0 * alpha;
                         double *cur = rb, *nxt = rb + C::NR1;
                         if (tid == 0)

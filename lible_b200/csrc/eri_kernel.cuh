@@ -46,6 +46,10 @@ namespace lible_b200
         static constexpr int block = W == 0 ? 128 : G;
         // register path: per-warp staging of finished batches for the digestion epilogue
         static constexpr size_t reg_smem = (GT > 1) ? sizeof(double) * (block / 32) * QPW * C::SAB * C::SCD : 0;
+        // register path: the order-L Boys table, staged once per block
+        static constexpr size_t off_boys = (reg_smem + 15) / 16 * 16;
+        static constexpr size_t boys_bytes = sizeof(T) == 8 ? sizeof(double) * kBoysTerms * kBoysPitch
+                                                            : sizeof(float) * kBoysTermsF * kBoysPitch;
         static constexpr int IK = W == 0 ? 0 : (C::HAB * C::SCD + G - 1) / G;
         static constexpr int IB = W == 0 ? 0 : (C::SAB * C::SCD + G - 1) / G;
         // shared-memory carve-up (bytes) for the group shape
@@ -56,7 +60,7 @@ namespace lible_b200
         static constexpr size_t off_rx = off_ea + sizeof(T) * C::SAB * C::HAB;      // HAB x SCD
         static constexpr size_t off_ix = off_rx + sizeof(T) * C::HAB * C::SCD;      // HCD x HAB int16
         static constexpr size_t off_ht = (off_ix + 2 * C::HCD * C::HAB + 15) / 16 * 16; // NR char4
-        static constexpr size_t smem = W == 0 ? reg_smem : off_ht + 4 * C::NR;
+        static constexpr size_t smem = W == 0 ? off_boys + boys_bytes : off_ht + 4 * C::NR;
     };
 
     __device__ __forceinline__ void groupSync(int G)
@@ -261,7 +265,8 @@ namespace lible_b200
     // function and the R vector itself, so the group never synchronises; every index into R, the
     // R.E accumulator and the batch is a compile-time constant.
     template <int LA, int LB, int LC, int LD, typename T>
-    __device__ __forceinline__ void quartetThread(const QuartetArgs &a, uint32_t ib, uint32_t ik, int c0, T *V)
+    __device__ __forceinline__ void quartetThread(const QuartetArgs &a, uint32_t ib, uint32_t ik, int c0, T *V,
+                                                  const T *btab)
     {
         using C = Cls<LA, LB, LC, LD>;
         constexpr int CW = Shape<LA, LB, LC, LD, T>::CW;
@@ -288,7 +293,10 @@ namespace lible_b200
                 const double X = P.y - Q.y, Y = P.z - Q.z, Z = P.w - Q.w;
                 const double fac = 34.986836655249725 * rs * P.ip * Q.ip;
                 double F[C::L + 1];
-                boysF<C::L>(alpha * (X * X + Y * Y + Z * Z), a.boys, F);
+                if constexpr (sizeof(T) == 8)
+                    boysF<C::L, true>(alpha * (X * X + Y * Y + Z * Z), reinterpret_cast<const double *>(btab), F);
+                else
+                    boysF32<C::L>(alpha * (X * X + Y * Y + Z * Z), reinterpret_cast<const float *>(btab), F);
                 T Ft[C::L + 1];
 #pragma unroll
                 for (int k = 0; k <= C::L; k++)
@@ -388,7 +396,7 @@ namespace lible_b200
                 const double X = P.y - Q.y, Y = P.z - Q.z, Z = P.w - Q.w;
                 const double fac = 34.986836655249725 * rs * P.ip * Q.ip;
                 double F[C::L + 1];
-                boysF<C::L>(alpha * (X * X + Y * Y + Z * Z), a.boys, F);
+                boysF<C::L, false>(alpha * (X * X + Y * Y + Z * Z), a.boys + C::L * kBoysTerms * kBoysPitch, F);
                 const double m2a = -2.0 * alpha;
                 // level L
                 T *cur = rb, *nxt = rb + C::NR;
@@ -539,17 +547,20 @@ namespace lible_b200
             const long long gw = (long long)blockIdx.x * (blockDim.x >> 5) + warp;
             extern __shared__ __align__(16) unsigned char smem[];
             double *vs = reinterpret_cast<double *>(smem) + ((size_t)warp * QPW + slot) * blk;
+            T *btab = reinterpret_cast<T *>(smem + S::off_boys);
+            if constexpr (sizeof(T) == 8)
+                stageBoys(a.boys, C::L, reinterpret_cast<double *>(btab));
+            else
+                stageBoys(a.boys_f, C::L, reinterpret_cast<float *>(btab));
+            __syncthreads();
             // each warp walks chunks of consecutive tasks (QPW per iteration); consecutive tasks
             // share the major pair, so the task cursor rarely moves
-            constexpr long long CH = 8 * QPW;
-            const long long n_chunks = (a.n_tasks + CH - 1) / CH;
-            for (long long chunk = gw; chunk < n_chunks; chunk += warps)
-            {
-            const long long end = (chunk + 1) * CH < a.n_tasks ? (chunk + 1) * CH : a.n_tasks;
+            // tasks [start, end) of one chunk, QPW quartets per warp step
+            auto processRange = [&](long long start, long long end) {
             int cur = 0;
             if (!a.list)
-                cur = advanceMajor(a, chunk * CH, 0);
-            for (long long base = chunk * CH; base < end; base += QPW)
+                cur = advanceMajor(a, start, 0);
+            for (long long base = start; base < end; base += QPW)
             {
                 const long long t = base + slot;
                 const bool valid = slot < QPW && t < end;
@@ -559,7 +570,7 @@ namespace lible_b200
                 {
                     int my = cur;
                     decodeCursor(a, t, my, ib, ik);
-                    quartetThread<LA, LB, LC, LD, T>(a, ib, ik, member * CW, V);
+                    quartetThread<LA, LB, LC, LD, T>(a, ib, ik, member * CW, V, btab);
                 }
                 if (!a.list)
                     cur = advanceMajor(a, base + QPW < end ? base + QPW : end - 1, cur);
@@ -623,6 +634,28 @@ namespace lible_b200
                     __syncwarp();
                 }
             }
+            };
+            if (a.chunks)
+            {
+                // work queue: lane 0 claims the next chunk for the whole warp
+                for (;;)
+                {
+                    unsigned long long c = 0;
+                    if (lane == 0)
+                        c = atomicAdd(a.counter, 1ULL);
+                    c = __shfl_sync(0xffffffffu, c, 0);
+                    if (c >= (unsigned long long)a.n_chunks)
+                        break;
+                    processRange((long long)__ldg(a.chunks + c), (long long)__ldg(a.chunks + c + 1));
+                }
+            }
+            else
+            {
+                // static chunks of 8 warp steps, strided over the grid's warps
+                constexpr long long CH = 8 * QPW;
+                const long long n_chunks = (a.n_tasks + CH - 1) / CH;
+                for (long long chunk = gw; chunk < n_chunks; chunk += warps)
+                    processRange(chunk * CH, (chunk + 1) * CH < a.n_tasks ? (chunk + 1) * CH : a.n_tasks);
             }
         }
         else
@@ -630,12 +663,10 @@ namespace lible_b200
             extern __shared__ __align__(16) unsigned char smem[];
             buildGroupTables<LA, LB, LC, LD, T>(smem);
             T *vs = reinterpret_cast<T *>(smem + S::off_rx);
-            // blocks walk chunks of consecutive tasks with a cursor over the major positions
-            constexpr long long CHB = 8;
-            const long long n_chunks = (a.n_tasks + CHB - 1) / CHB;
-            long long chunk = blockIdx.x;
+            // one quartet at a time for the whole block, tasks [start, end) of a chunk
+            auto processRange = [&](long long start, long long end) {
             int cur = 0;
-            for (long long t = chunk * CHB; chunk < n_chunks;)
+            for (long long t = start; t < end; t++)
             {
                 uint32_t ib, ik;
                 decodeCursor(a, t, cur, ib, ik);
@@ -676,14 +707,30 @@ namespace lible_b200
                         digestRI<C::SA, C::SB, C::SC, C::SD, false>(a, bi, ki, val, threadIdx.x, S::G);
                 }
                 __syncthreads();
-                // next task: the rest of this chunk, then the block's next chunk
-                t++;
-                if (t >= (chunk + 1) * CHB || t >= a.n_tasks)
+            }
+            };
+            if (a.chunks)
+            {
+                __shared__ unsigned long long claimed;
+                for (;;)
                 {
-                    chunk += gridDim.x;
-                    t = chunk * CHB;
-                    cur = 0;
+                    if (threadIdx.x == 0)
+                        claimed = atomicAdd(a.counter, 1ULL);
+                    __syncthreads();
+                    const unsigned long long c = claimed;
+                    __syncthreads();
+                    if (c >= (unsigned long long)a.n_chunks)
+                        break;
+                    processRange((long long)__ldg(a.chunks + c), (long long)__ldg(a.chunks + c + 1));
                 }
+            }
+            else
+            {
+                // static chunks of 8 consecutive tasks, strided over the grid's blocks
+                constexpr long long CHB = 8;
+                const long long n_chunks = (a.n_tasks + CHB - 1) / CHB;
+                for (long long chunk = blockIdx.x; chunk < n_chunks; chunk += gridDim.x)
+                    processRange(chunk * CHB, (chunk + 1) * CHB < a.n_tasks ? (chunk + 1) * CHB : a.n_tasks);
             }
         }
     }

@@ -20,6 +20,16 @@ namespace lible_b200
         return la == 4 ? 10 : 11;
     }
 
+    // Quartets a worker processes side by side: QPW per warp on the register path, one per block on
+    // the group path.  Work-queue chunks are cut so that each holds at least one unit of the most
+    // expensive quartets.
+    template <int LA, int LB, int LC, int LD, typename T>
+    constexpr int workUnit()
+    {
+        using S = Shape<LA, LB, LC, LD, T>;
+        return S::W == 0 ? S::QPW : 1;
+    }
+
     template <int LA, int LB, int LC, int LD, typename T>
     cudaError_t launchFwd(const QuartetArgs &a, cudaStream_t s, int num_sms)
     {
@@ -28,7 +38,25 @@ namespace lible_b200
             return cudaSuccess;
         auto kern = eriKernel<LA, LB, LC, LD, T>;
         long long grid;
-        if constexpr (S::W == 0)
+        if (a.chunks)
+        {
+            // persistent grid: every resident block pulls chunks from the work queue
+            if (S::smem > 48 * 1024)
+            {
+                cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::smem);
+                if (e != cudaSuccess)
+                    return e;
+            }
+            int occ = 0;
+            cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, S::block, S::smem);
+            if (e != cudaSuccess)
+                return e;
+            const long long workers_per_block = S::W == 0 ? S::block / 32 : 1;
+            grid = std::min<long long>((a.n_chunks + workers_per_block - 1) / workers_per_block,
+                                       (long long)num_sms * std::max(occ, 1));
+            grid = std::max<long long>(grid, 1);
+        }
+        else if constexpr (S::W == 0)
         {
             // one chunk of 8 warp-iterations per warp, at most 32 blocks per SM in flight
             const long long chunks = (a.n_tasks + 8LL * S::QPW - 1) / (8LL * S::QPW);
@@ -84,4 +112,5 @@ namespace lible_b200
     LaunchFn lookupFwd64(int bra_type, int ket_type);
     LaunchFn lookupFwd32(int bra_type, int ket_type);
     LaunchFn lookupD1(int bra_type, int ket_type);
+    int unitFwd(int bra_type, int ket_type, bool fp32);
 }

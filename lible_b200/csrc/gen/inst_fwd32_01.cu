@@ -7,4 +7,8 @@ namespace lible_b200
         &launchFwd<1,0,0,0,float>,
         &launchFwd<1,0,1,0,float>,
     };
+    extern const int u_fwd32_01[2] = {
+        workUnit<1,0,0,0,float>(),
+        workUnit<1,0,1,0,float>(),
+    };
 }

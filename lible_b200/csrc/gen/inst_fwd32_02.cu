@@ -8,4 +8,9 @@ namespace lible_b200
         &launchFwd<1,1,1,0,float>,
         &launchFwd<1,1,1,1,float>,
     };
+    extern const int u_fwd32_02[3] = {
+        workUnit<1,1,0,0,float>(),
+        workUnit<1,1,1,0,float>(),
+        workUnit<1,1,1,1,float>(),
+    };
 }

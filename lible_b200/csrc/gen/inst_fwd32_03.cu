@@ -9,4 +9,10 @@ namespace lible_b200
         &launchFwd<2,0,1,1,float>,
         &launchFwd<2,0,2,0,float>,
     };
+    extern const int u_fwd32_03[4] = {
+        workUnit<2,0,0,0,float>(),
+        workUnit<2,0,1,0,float>(),
+        workUnit<2,0,1,1,float>(),
+        workUnit<2,0,2,0,float>(),
+    };
 }

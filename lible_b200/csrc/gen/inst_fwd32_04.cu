@@ -10,4 +10,11 @@ namespace lible_b200
         &launchFwd<2,1,2,0,float>,
         &launchFwd<2,1,2,1,float>,
     };
+    extern const int u_fwd32_04[5] = {
+        workUnit<2,1,0,0,float>(),
+        workUnit<2,1,1,0,float>(),
+        workUnit<2,1,1,1,float>(),
+        workUnit<2,1,2,0,float>(),
+        workUnit<2,1,2,1,float>(),
+    };
 }

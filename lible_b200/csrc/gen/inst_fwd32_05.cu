@@ -11,4 +11,12 @@ namespace lible_b200
         &launchFwd<2,2,2,1,float>,
         &launchFwd<2,2,2,2,float>,
     };
+    extern const int u_fwd32_05[6] = {
+        workUnit<2,2,0,0,float>(),
+        workUnit<2,2,1,0,float>(),
+        workUnit<2,2,1,1,float>(),
+        workUnit<2,2,2,0,float>(),
+        workUnit<2,2,2,1,float>(),
+        workUnit<2,2,2,2,float>(),
+    };
 }

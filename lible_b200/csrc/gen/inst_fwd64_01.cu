@@ -7,4 +7,8 @@ namespace lible_b200
         &launchFwd<1,0,0,0,double>,
         &launchFwd<1,0,1,0,double>,
     };
+    extern const int u_fwd64_01[2] = {
+        workUnit<1,0,0,0,double>(),
+        workUnit<1,0,1,0,double>(),
+    };
 }

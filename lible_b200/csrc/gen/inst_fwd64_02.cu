@@ -8,4 +8,9 @@ namespace lible_b200
         &launchFwd<1,1,1,0,double>,
         &launchFwd<1,1,1,1,double>,
     };
+    extern const int u_fwd64_02[3] = {
+        workUnit<1,1,0,0,double>(),
+        workUnit<1,1,1,0,double>(),
+        workUnit<1,1,1,1,double>(),
+    };
 }

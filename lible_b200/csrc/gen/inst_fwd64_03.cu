@@ -9,4 +9,10 @@ namespace lible_b200
         &launchFwd<2,0,1,1,double>,
         &launchFwd<2,0,2,0,double>,
     };
+    extern const int u_fwd64_03[4] = {
+        workUnit<2,0,0,0,double>(),
+        workUnit<2,0,1,0,double>(),
+        workUnit<2,0,1,1,double>(),
+        workUnit<2,0,2,0,double>(),
+    };
 }

@@ -10,4 +10,11 @@ namespace lible_b200
         &launchFwd<2,1,2,0,double>,
         &launchFwd<2,1,2,1,double>,
     };
+    extern const int u_fwd64_04[5] = {
+        workUnit<2,1,0,0,double>(),
+        workUnit<2,1,1,0,double>(),
+        workUnit<2,1,1,1,double>(),
+        workUnit<2,1,2,0,double>(),
+        workUnit<2,1,2,1,double>(),
+    };
 }

@@ -11,4 +11,12 @@ namespace lible_b200
         &launchFwd<2,2,2,1,double>,
         &launchFwd<2,2,2,2,double>,
     };
+    extern const int u_fwd64_05[6] = {
+        workUnit<2,2,0,0,double>(),
+        workUnit<2,2,1,0,double>(),
+        workUnit<2,2,1,1,double>(),
+        workUnit<2,2,2,0,double>(),
+        workUnit<2,2,2,1,double>(),
+        workUnit<2,2,2,2,double>(),
+    };
 }

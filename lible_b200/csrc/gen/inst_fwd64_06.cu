@@ -12,4 +12,13 @@ namespace lible_b200
         &launchFwd<3,0,2,2,double>,
         &launchFwd<3,0,3,0,double>,
     };
+    extern const int u_fwd64_06[7] = {
+        workUnit<3,0,0,0,double>(),
+        workUnit<3,0,1,0,double>(),
+        workUnit<3,0,1,1,double>(),
+        workUnit<3,0,2,0,double>(),
+        workUnit<3,0,2,1,double>(),
+        workUnit<3,0,2,2,double>(),
+        workUnit<3,0,3,0,double>(),
+    };
 }

@@ -14,4 +14,15 @@ namespace lible_b200
         &launchFwd<3,2,3,1,double>,
         &launchFwd<3,2,3,2,double>,
     };
+    extern const int u_fwd64_08[9] = {
+        workUnit<3,2,0,0,double>(),
+        workUnit<3,2,1,0,double>(),
+        workUnit<3,2,1,1,double>(),
+        workUnit<3,2,2,0,double>(),
+        workUnit<3,2,2,1,double>(),
+        workUnit<3,2,2,2,double>(),
+        workUnit<3,2,3,0,double>(),
+        workUnit<3,2,3,1,double>(),
+        workUnit<3,2,3,2,double>(),
+    };
 }

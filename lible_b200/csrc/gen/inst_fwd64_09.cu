@@ -15,4 +15,16 @@ namespace lible_b200
         &launchFwd<3,3,3,2,double>,
         &launchFwd<3,3,3,3,double>,
     };
+    extern const int u_fwd64_09[10] = {
+        workUnit<3,3,0,0,double>(),
+        workUnit<3,3,1,0,double>(),
+        workUnit<3,3,1,1,double>(),
+        workUnit<3,3,2,0,double>(),
+        workUnit<3,3,2,1,double>(),
+        workUnit<3,3,2,2,double>(),
+        workUnit<3,3,3,0,double>(),
+        workUnit<3,3,3,1,double>(),
+        workUnit<3,3,3,2,double>(),
+        workUnit<3,3,3,3,double>(),
+    };
 }

@@ -16,4 +16,17 @@ namespace lible_b200
         &launchFwd<4,0,3,3,double>,
         &launchFwd<4,0,4,0,double>,
     };
+    extern const int u_fwd64_10[11] = {
+        workUnit<4,0,0,0,double>(),
+        workUnit<4,0,1,0,double>(),
+        workUnit<4,0,1,1,double>(),
+        workUnit<4,0,2,0,double>(),
+        workUnit<4,0,2,1,double>(),
+        workUnit<4,0,2,2,double>(),
+        workUnit<4,0,3,0,double>(),
+        workUnit<4,0,3,1,double>(),
+        workUnit<4,0,3,2,double>(),
+        workUnit<4,0,3,3,double>(),
+        workUnit<4,0,4,0,double>(),
+    };
 }

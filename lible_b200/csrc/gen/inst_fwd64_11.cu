@@ -17,4 +17,18 @@ namespace lible_b200
         &launchFwd<5,0,4,0,double>,
         &launchFwd<5,0,5,0,double>,
     };
+    extern const int u_fwd64_11[12] = {
+        workUnit<5,0,0,0,double>(),
+        workUnit<5,0,1,0,double>(),
+        workUnit<5,0,1,1,double>(),
+        workUnit<5,0,2,0,double>(),
+        workUnit<5,0,2,1,double>(),
+        workUnit<5,0,2,2,double>(),
+        workUnit<5,0,3,0,double>(),
+        workUnit<5,0,3,1,double>(),
+        workUnit<5,0,3,2,double>(),
+        workUnit<5,0,3,3,double>(),
+        workUnit<5,0,4,0,double>(),
+        workUnit<5,0,5,0,double>(),
+    };
 }

@@ -4,24 +4,44 @@
 namespace lible_b200
 {
     extern const LaunchFn k_fwd64_00[1];
+    extern const int u_fwd64_00[1];
     extern const LaunchFn k_fwd64_01[2];
+    extern const int u_fwd64_01[2];
     extern const LaunchFn k_fwd64_02[3];
+    extern const int u_fwd64_02[3];
     extern const LaunchFn k_fwd64_03[4];
+    extern const int u_fwd64_03[4];
     extern const LaunchFn k_fwd64_04[5];
+    extern const int u_fwd64_04[5];
     extern const LaunchFn k_fwd64_05[6];
+    extern const int u_fwd64_05[6];
     extern const LaunchFn k_fwd64_06[7];
+    extern const int u_fwd64_06[7];
     extern const LaunchFn k_fwd64_07[8];
+    extern const int u_fwd64_07[8];
     extern const LaunchFn k_fwd64_08[9];
+    extern const int u_fwd64_08[9];
     extern const LaunchFn k_fwd64_09[10];
+    extern const int u_fwd64_09[10];
     extern const LaunchFn k_fwd64_10[11];
+    extern const int u_fwd64_10[11];
     extern const LaunchFn k_fwd64_11[12];
+    extern const int u_fwd64_11[12];
+    static const int *const u_fwd64[12] = {u_fwd64_00, u_fwd64_01, u_fwd64_02, u_fwd64_03, u_fwd64_04, u_fwd64_05, u_fwd64_06, u_fwd64_07, u_fwd64_08, u_fwd64_09, u_fwd64_10, u_fwd64_11};
     static const LaunchFn *const k_fwd64[12] = {k_fwd64_00, k_fwd64_01, k_fwd64_02, k_fwd64_03, k_fwd64_04, k_fwd64_05, k_fwd64_06, k_fwd64_07, k_fwd64_08, k_fwd64_09, k_fwd64_10, k_fwd64_11};
     extern const LaunchFn k_fwd32_00[1];
+    extern const int u_fwd32_00[1];
     extern const LaunchFn k_fwd32_01[2];
+    extern const int u_fwd32_01[2];
     extern const LaunchFn k_fwd32_02[3];
+    extern const int u_fwd32_02[3];
     extern const LaunchFn k_fwd32_03[4];
+    extern const int u_fwd32_03[4];
     extern const LaunchFn k_fwd32_04[5];
+    extern const int u_fwd32_04[5];
     extern const LaunchFn k_fwd32_05[6];
+    extern const int u_fwd32_05[6];
+    static const int *const u_fwd32[6] = {u_fwd32_00, u_fwd32_01, u_fwd32_02, u_fwd32_03, u_fwd32_04, u_fwd32_05};
     static const LaunchFn *const k_fwd32[6] = {k_fwd32_00, k_fwd32_01, k_fwd32_02, k_fwd32_03, k_fwd32_04, k_fwd32_05};
     extern const LaunchFn k_d1_00[1];
     extern const LaunchFn k_d1_01[2];
@@ -53,5 +73,11 @@ namespace lible_b200
         if (bt < 0 || bt >= 12 || kt < 0 || kt > bt)
             return nullptr;
         return k_d1[bt][kt];
+    }
+    int unitFwd(int bt, int kt, bool fp32)
+    {
+        if (bt < 0 || kt < 0 || kt > bt || bt >= (fp32 ? 6 : 12))
+            return 0;
+        return fp32 ? u_fwd32[bt][kt] : u_fwd64[bt][kt];
     }
 }

@@ -35,7 +35,15 @@ def main():
                     f'({la},{lb}).', '#include "../eri_launch.cuh"', '', 'namespace lible_b200', '{',
                     f'    extern const LaunchFn k_{kind}_{bt:02d}[{bt + 1}] = {{']
             body += [f'        {e},' for e in entries]
-            body += ['    };', '}', '']
+            body += ['    };']
+            if kind.startswith("fwd"):
+                T = "double" if kind == "fwd64" else "float"
+                body += [f'    extern const int u_{kind}_{bt:02d}[{bt + 1}] = {{']
+                for kt in range(bt + 1):
+                    lc, ld = PAIR_TYPES[kt]
+                    body.append(f'        workUnit<{la},{lb},{lc},{ld},{T}>(),')
+                body += ['    };']
+            body += ['}', '']
             path = os.path.join(out, name)
             text = "\n".join(body)
             if not os.path.exists(path) or open(path).read() != text:
@@ -43,6 +51,11 @@ def main():
                     fh.write(text)
             written.append(name)
             table.append(f'    extern const LaunchFn k_{kind}_{bt:02d}[{bt + 1}];')
+            if kind.startswith("fwd"):
+                table.append(f'    extern const int u_{kind}_{bt:02d}[{bt + 1}];')
+        if kind.startswith("fwd"):
+            table.append(f'    static const int *const u_{kind}[{ntypes}] = {{' +
+                         ", ".join(f"u_{kind}_{bt:02d}" for bt in range(ntypes)) + '};')
         table.append(f'    static const LaunchFn *const k_{kind}[{ntypes}] = {{' +
                      ", ".join(f"k_{kind}_{bt:02d}" for bt in range(ntypes)) + '};')
     for kind, _, ntypes in kinds():
@@ -50,6 +63,9 @@ def main():
         table += [f'    LaunchFn {fn}(int bt, int kt)', '    {',
                   f'        if (bt < 0 || bt >= {ntypes} || kt < 0 || kt > bt)',
                   '            return nullptr;', f'        return k_{kind}[bt][kt];', '    }']
+    table += ['    int unitFwd(int bt, int kt, bool fp32)', '    {',
+              '        if (bt < 0 || kt < 0 || kt > bt || bt >= (fp32 ? %d : %d))' % (FP32_MAX_TYPE + 1, len(PAIR_TYPES)),
+              '            return 0;', '        return fp32 ? u_fwd32[bt][kt] : u_fwd64[bt][kt];', '    }']
     table += ['}', '']
     path = os.path.join(out, "inst_table.cu")
     text = "\n".join(table)

@@ -1,6 +1,7 @@
 // Host-side tables: real solid-harmonic (spherical) transformation and the Boys-function grid.
 #include "engine.hpp"
 
+#include <algorithm>
 #include <stdexcept>
 
 namespace lible_b200
@@ -82,38 +83,38 @@ namespace lible_b200
                 F[k] = F[k - 1] * (k - 0.5) / x;
             return;
         }
-        const int iv = (int)std::nearbyint(x / kBoysStep);
-        const double m = iv * kBoysStep - x;
-        const double *row = tables.data() + ((size_t)n * kBoysRows + iv) * kBoysTerms;
-        double s = row[kBoysTerms - 1];
+        const int iv = (int)std::nearbyint(x);
+        const double m = iv - x;
+        const double *c = tables.data() + (size_t)n * kBoysTerms * kBoysPitch + iv;
+        double s = c[(kBoysTerms - 1) * kBoysPitch];
         for (int k = kBoysTerms - 2; k >= 0; k--)
-            s = s * m + row[k];
+            s = std::fma(s, m, c[k * kBoysPitch]);
         F[n] = s;
         const double ex = std::exp(-x);
         for (int k = n - 1; k >= 0; k--)
             F[k] = (2.0 * x * F[k + 1] + ex) / (2 * k + 1);
     }
 
-    // Boys function tables (layout in lible_math.hpp).  At each grid point F_n(x_i) for
+    // Boys function tables (layout in lible_math.hpp).  At each integer x_i, F_n(x_i) for
     // n = 0..kBoysCols-1 is computed as the reference builds its grid: the top order by the
     // convergent series F_N(x) = e^{-x} sum_i x^i / ((N+1/2)(N+3/2)...(N+i+1/2)) stopped when a term
-    // falls below 1e-16, lower orders by downward recursion F_n = (2x F_{n+1} + e^{-x}) / (2n+1)
+    // falls below 1e-17 of the sum, lower orders by downward recursion F_n = (2x F_{n+1} + e^{-x}) / (2n+1)
     // (Helgaker, Jorgensen, Olsen, eqs. 9.8.11-9.8.14; src/lible/ints/boys_function.cpp:40-69).
     std::vector<double> boysGrid()
     {
-        std::vector<double> g((size_t)(kBoysMaxN + 1) * kBoysRows * kBoysTerms);
+        std::vector<double> g((size_t)(kBoysMaxN + 1) * kBoysTerms * kBoysPitch, 0.0);
         const int nmax = kBoysCols - 1;
         std::vector<double> col(kBoysCols);
-        for (int i = 0; i < kBoysRows; i++)
+        for (int i = 0; i < kBoysPitch; i++)
         {
-            const double x = i * kBoysStep;
+            const double x = std::min(i, kBoysRows - 1);
             double term = 1.0 / (2.0 * nmax + 1.0);
             double sum = term;
             for (int k = 1;; k++)
             {
                 term *= x / (nmax + 0.5 + k);
                 sum += term;
-                if (std::fabs(term) < 1e-16)
+                if (std::fabs(term) < 1e-17 * sum)
                     break;
             }
             const double ex = std::exp(-x);
@@ -127,10 +128,23 @@ namespace lible_b200
                 {
                     if (k > 0)
                         fact *= k;
-                    g[((size_t)N * kBoysRows + i) * kBoysTerms + k] = col[N + k] / fact;
+                    g[((size_t)N * kBoysTerms + k) * kBoysPitch + i] = col[N + k] / fact;
                 }
             }
         }
         return g;
+    }
+
+    // The FP32 tables: the first kBoysTermsF coefficients of every order, rounded to float.
+    std::vector<float> boysGridF()
+    {
+        const std::vector<double> g = boysGrid();
+        std::vector<float> f((size_t)(kBoysMaxN + 1) * kBoysTermsF * kBoysPitch);
+        for (int N = 0; N <= kBoysMaxN; N++)
+            for (int k = 0; k < kBoysTermsF; k++)
+                for (int i = 0; i < kBoysPitch; i++)
+                    f[((size_t)N * kBoysTermsF + k) * kBoysPitch + i] =
+                        (float)g[((size_t)N * kBoysTerms + k) * kBoysPitch + i];
+        return f;
     }
 }

@@ -24,17 +24,21 @@ namespace lible_b200
     constexpr int kMaxL = 5;          // highest shell angular momentum handled (aux h shells)
     constexpr int kMaxLPair = 2 * kMaxL;
     constexpr int kMaxLTotal = 14;    // highest L of a quartet (+1 for first derivatives)
-    // Boys tables: for every order N = 0..kBoysMaxN a table over x = 0, 0.05, ..., 30 whose row i
-    // holds F_{N+k}(x_i) / k!, k = 0..kBoysTerms-1, the Taylor coefficients of F_N about x_i.
-    // Expanding about the nearest grid point (|x - x_i| <= 0.025) with 10 terms truncates at
-    // 0.025^10/10! < 3e-23 relative; one table is 48 KB and stays resident in L1.  The reference
-    // grid is finer (step 0.01, 7 terms about the lower point, src/lible/ints/boys_function.hpp:112-122);
-    // both are accurate to the last bits.
+    // Boys tables: for every order N = 0..kBoysMaxN a table of Taylor coefficients of F_N about
+    // the integers x_i = 0, 1, ..., 30: c_N[k][i] = F_{N+k}(x_i) / k!, k = 0..kBoysTerms-1, stored
+    // term-major with a row pitch of kBoysPitch (index k * kBoysPitch + i; entry 31 repeats 30).
+    // Expanding about the nearest integer (|x - x_i| <= 1/2) with 16 terms truncates below
+    // 0.5^16/16! < 1e-18 relative.  One order is 4 KB, small enough to be staged in shared memory,
+    // and the 31 possible rows of a warp's lookups fall on few distinct words (mostly broadcasts).
+    // The reference grid is finer (step 0.01, 7 terms about the lower point,
+    // src/lible/ints/boys_function.hpp:112-122); both are accurate to the last bits.
+    // The FP32 tables hold the first kBoysTermsF coefficients as floats (truncation 0.5^10/10! < 3e-10).
     constexpr int kBoysMaxN = 14;
-    constexpr int kBoysTerms = 10;
-    constexpr double kBoysStep = 0.05;
-    constexpr int kBoysRows = 601;
-    constexpr int kBoysCols = 24;     // F_n for n = 0 .. 23 computed when building the tables
+    constexpr int kBoysTerms = 16;
+    constexpr int kBoysTermsF = 10;
+    constexpr int kBoysPitch = 32;
+    constexpr int kBoysRows = 31;
+    constexpr int kBoysCols = 32;     // F_n for n = 0 .. 31 computed when building the tables
     constexpr double kBoysLargeX = 30.0;
     constexpr double kPrimitiveThreshold = 1e-15;   // src/lible/ints/shell_pair_data.hpp:57
     constexpr double kBohrToAngstrom = 0.5291772083; // src/lible/ints/defs.hpp:9

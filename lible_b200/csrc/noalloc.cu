@@ -82,6 +82,7 @@ namespace lible_b200
         a.bra = view(swap ? ket : bra);
         a.ket = view(swap ? bra : ket);
         a.boys = boys_;
+        a.boys_f = boys_f_;
         a.list = scratch;
         a.n_tasks = n;
         a.same_class = (use_symm && cab == ccd) ? 1 : 0;

@@ -1,0 +1,52 @@
+"""Runs direct J/K builds of a seeded water cluster and prints the screening plan and timings.
+
+    python -m lible_b200.jk_run --waters 8 --basis cc-pvdz --precision fp64 --repeat 2
+
+The cluster and density follow lible_b200.workloads (5.7 bohr lattice, random rotations, +-0.6 bohr
+jitter, D = C C^T with occupation 5 per water unless --occ is given).  Every build is a separate
+lible_gpu_jk call on the structure's stream; the first one also builds the Schwarz factors and the
+screening plan.  Small cases of this command are what kernel profiles are taken on.
+"""
+import argparse
+import json
+import sys
+import time
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--waters", type=int, default=8)
+    ap.add_argument("--basis", default="cc-pvdz")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--schwarz", type=float, default=1e-12)
+    ap.add_argument("--fp32-threshold", type=float, default=1e-4)
+    ap.add_argument("--occ", type=int, default=None)
+    ap.add_argument("--seed", type=int, default=2024)
+    ap.add_argument("--repeat", type=int, default=2)
+    args = ap.parse_args(argv)
+
+    import torch
+
+    from . import ints as L
+    from .workloads import random_density, water_cluster
+
+    Z, xyz, rng = water_cluster(args.waters, args.seed)
+    s = L.Structure(args.basis, Z, xyz, units="bohr")
+    D = random_density(s.nao, args.occ or 5 * args.waters, rng)
+    Dd = torch.tensor(D, device="cuda")
+    J, K = torch.empty_like(Dd), torch.empty_like(Dd)
+    times = []
+    for _ in range(args.repeat):
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        L.jk(s, Dd, args.schwarz, args.precision, args.fp32_threshold, J=J, K=K)
+        torch.cuda.synchronize()
+        times.append(time.perf_counter() - t)
+    plan = L.jk_plan(s, args.schwarz, args.precision, args.fp32_threshold)
+    print(json.dumps({"waters": args.waters, "basis": args.basis, "nao": s.nao, "precision": args.precision,
+                      "plan": plan, "wall_s": times}))
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())
