@@ -119,6 +119,72 @@ def run_reference(args):
           "e2e": {"value": qps, "unit": "quartets/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}})
 
 
+def run_batch(steps, warmup, dev):
+    """The heterogeneous batch: 64 water clusters (1..12 waters, half cc-pVDZ, half cc-pVTZ), FP64,
+    Schwarz 1e-12.  Times the batched build (one work-queue launch per quartet class for all
+    molecules, replayed from a CUDA graph) against the same molecules built one after another
+    through the single-structure path."""
+    import torch
+
+    from lible_b200 import ints as L
+    from lible_b200.workloads import batch_clusters
+
+    specs = batch_clusters()
+    t0 = time.perf_counter()
+    b = L.Batch([(bs, Z, xyz) for bs, Z, xyz, _ in specs], device=dev.index or 0)
+    Ds = [f(int(b.nao[m])) for m, (_, _, _, f) in enumerate(specs)]
+    Dp = torch.tensor(b.pack(Ds), device=dev)
+    J, K = torch.empty_like(Dp), torch.empty_like(Dp)
+    plan = L.jk_plan(b, SCHWARZ, "fp64")
+    setup_s = time.perf_counter() - t0
+    stream = torch.cuda.ExternalStream(L.stream_handle(b), device=dev)
+
+    def time_batch(use_graph):
+        for _ in range(warmup):
+            L.jk(b, Dp, SCHWARZ, "fp64", J=J, K=K, use_graph=use_graph)
+        torch.cuda.synchronize()
+        ms = []
+        for _ in range(steps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            L.jk(b, Dp, SCHWARZ, "fp64", J=J, K=K, use_graph=use_graph)
+            e1.record(stream)
+            e1.synchronize()
+            ms.append(e0.elapsed_time(e1))
+        return float(np.mean(ms))
+
+    t_direct = time_batch(False)
+    t_graph = time_batch(True)
+    flops = plan["flops_fp64"]
+    Jb = J.cpu().numpy()
+    # the same molecules one by one through the single-structure path
+    singles = [L.Structure(bs, Z, xyz, units="bohr", device=dev.index or 0) for bs, Z, xyz, _ in specs]
+    Dd = [torch.tensor(D, device=dev) for D in Ds]
+    Jm = [torch.empty_like(x) for x in Dd]
+    Km = [torch.empty_like(x) for x in Dd]
+    for s, D_, J_, K_ in zip(singles, Dd, Jm, Km):
+        L.jk(s, D_, SCHWARZ, "fp64", J=J_, K=K_)
+    torch.cuda.synchronize()
+    err = max(float(np.abs(b.unpack(Jb)[m] - Jm[m].cpu().numpy()).max()) for m in range(len(specs)))
+    seq = []
+    for _ in range(steps):
+        torch.cuda.synchronize()
+        a = time.perf_counter()
+        for s, D_, J_, K_ in zip(singles, Dd, Jm, Km):
+            L.jk(s, D_, SCHWARZ, "fp64", J=J_, K=K_)
+        torch.cuda.synchronize()
+        seq.append(time.perf_counter() - a)
+    t_seq = 1e3 * float(np.mean(seq))
+    nq = plan["n_quartets"]
+    return {"workload": "64 water clusters, 1..12 waters, half cc-pVDZ / half cc-pVTZ, FP64, Schwarz 1e-12",
+            "n_molecules": len(specs), "n_quartets": nq, "n_prim_quartets": plan["n_prim_quartets"],
+            "packed_elements": int(b.packed), "setup_s": setup_s,
+            "batched_graph_ms": t_graph, "batched_direct_ms": t_direct, "sequential_single_ms": t_seq,
+            "quartets_per_s": nq / (t_graph * 1e-3), "speedup_vs_sequential": t_seq / t_graph,
+            "algorithmic_fp64_tflops": flops / (t_graph * 1e-3) / 1e12,
+            "max_abs_dJ_vs_single": err}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -126,6 +192,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batch", action="store_true", help="skip the 64-molecule batched measurement")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
@@ -228,6 +295,9 @@ def main():
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         e2e_t = float(tt.item())
 
+    # the batch is seconds per build: two timed steps after one warm-up keep the run short
+    batch = None if args.no_batch else run_batch(min(args.steps, 2), 1, dev)
+
     if rank != 0:
         if dist:
             dist.destroy_process_group()
@@ -266,6 +336,7 @@ def main():
         "e2e": {"value": world * plan["n_quartets"] / e2e_t, "unit": "quartets/s",
                 "h2d_bytes_per_step": int(D.nbytes), "d2h_bytes_per_step": int(2 * D.nbytes),
                 "path": "lible_b200.jk -> lible_gpu_jk with pinned host D/J/K"},
+        "batch": batch,
         "gpu_launches": int(plan["n_launches"]) * args.steps,
         "clocks": clocks,
     }

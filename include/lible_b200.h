@@ -124,6 +124,9 @@ typedef struct lible_gpu_jk_opts {
     double schwarz_threshold;  /* default 1e-12 */
     double fp32_threshold;     /* default 1e-4 */
     int precision;             /* 0 FP64, 1 mixed */
+    int use_graph;             /* 1: capture the launch sequence once per (plan, D, J, K) in a CUDA graph
+                                  and replay it; the first call per buffer set must not be inside a
+                                  caller's stream capture */
 } lible_gpu_jk_opts;
 
 typedef struct lible_gpu_jk_stats {
@@ -134,6 +137,29 @@ typedef struct lible_gpu_jk_stats {
 
 int lible_gpu_jk(lible_gpu_ctx *ctx, const double *D, double *J, double *K, const lible_gpu_jk_opts *opts,
                  lible_gpu_jk_stats *stats);
+
+/* ---- batches of molecules (no reference counterpart) -------------------------------------------
+ * A context can hold a batch of molecules instead of one structure: their J/K are built together,
+ * every quartet class of every molecule going through one persistent work-queue launch per class,
+ * and lible_gpu_jk with use_graph replays the whole sequence as one CUDA graph.  Molecule m has
+ * n_atoms[m] atoms (atomic_nrs and xyz concatenated over molecules, xyz as 3 per atom) and the basis
+ * basis[m], read from basis_root like lible_gpu_set_structure_named.  D, J and K are then packed:
+ * molecule m's N_m x N_m row-major matrix starts at element base[m] (lible_gpu_batch_layout), and
+ * lible_gpu_jk / lible_gpu_jk_energy_forward / lible_gpu_jk_plan* / lible_gpu_jk_autotune take
+ * packed arrays of *packed elements.  Other calls return LIBLE_GPU_EUNSUPPORTED for a batch. */
+int lible_gpu_set_batch(lible_gpu_ctx *ctx, int n_mol, const char *basis_root, const char *const *basis,
+                        const int *n_atoms, const int *atomic_nrs, const double *xyz, int units);
+int lible_gpu_batch_layout(lible_gpu_ctx *ctx, int *n_mol, long long *nao, long long *base, long long *packed);
+
+/* Autotuner of the J/K class launches: for every class pair of the plan for opts, times each
+ * candidate launch shape (resident blocks per SM: all or half; work-queue chunks of 2, 8 or 32
+ * work units) on D/J/K with CUDA events and keeps the fastest.  J and K are overwritten with
+ * meaningless values.  When cache_path is non-empty the choices are appended to that text file;
+ * lible_gpu_set_tune_cache(ctx, path) makes later plans start from a cache.  summary (may be NULL)
+ * receives one line per class pair. */
+int lible_gpu_jk_autotune(lible_gpu_ctx *ctx, const double *D, double *J, double *K, const lible_gpu_jk_opts *opts,
+                          const char *cache_path, char *summary, int summary_len);
+int lible_gpu_set_tune_cache(lible_gpu_ctx *ctx, const char *path);
 
 /* Size of the (cached) screening plan for these options: quartets, primitive quartets and the
  * algorithmic FP64 / FP32 FLOPs one lible_gpu_jk call performs (dense-equivalent count). */

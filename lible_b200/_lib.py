@@ -17,7 +17,7 @@ class LibleGpuError(RuntimeError):
 
 class JKOpts(ctypes.Structure):
     _fields_ = [("schwarz_threshold", ctypes.c_double), ("fp32_threshold", ctypes.c_double),
-                ("precision", ctypes.c_int)]
+                ("precision", ctypes.c_int), ("use_graph", ctypes.c_int)]
 
 
 class JKStats(ctypes.Structure):
@@ -61,6 +61,10 @@ SIGNATURES = {
     "lible_gpu_jk_energy_backward": [P, P, ctypes.POINTER(JKOpts), P],
     "lible_gpu_rij": [P, P, D, P, P, P],
     "lible_gpu_jk_plan": [P, ctypes.POINTER(JKOpts), ctypes.POINTER(JKPlanInfo)],
+    "lible_gpu_set_batch": [P, I, S, P, P, P, P, I],
+    "lible_gpu_batch_layout": [P, P, P, P, P],
+    "lible_gpu_jk_autotune": [P, P, P, P, ctypes.POINTER(JKOpts), S, P, I],
+    "lible_gpu_set_tune_cache": [P, S],
     "lible_gpu_stream": [P, ctypes.POINTER(P)],
     "lible_gpu_jk_plan_classes": [P, ctypes.POINTER(JKOpts), P, P, P, P, P, P],
     "lible_gpu_fp64_peak": [P, ctypes.POINTER(D), ctypes.POINTER(D)],

@@ -8,6 +8,7 @@
 
 #include <cstring>
 #include <memory>
+#include <map>
 #include <string>
 
 using namespace lible_b200;
@@ -532,6 +533,7 @@ static JKOptions toOpts(const lible_gpu_jk_opts *o)
         j.schwarz = o->schwarz_threshold;
         j.fp32_threshold = o->fp32_threshold;
         j.precision = o->precision;
+        j.use_graph = o->use_graph;
     }
     return j;
 }
@@ -542,10 +544,10 @@ int lible_gpu_jk(lible_gpu_ctx *ctx, const double *D, double *J, double *K, cons
     return guard(ctx, [&](Engine &e) {
         if (!D || !J || !K)
             throw EngineError(kStatusInvalid, "null D/J/K");
-        const size_t n = e.nao();
-        DevArray d(D, n * n, true, e.stream());
-        DevArray j(J, n * n, false, e.stream());
-        DevArray k(K, n * n, false, e.stream());
+        const size_t n2 = (size_t)e.packedSize();
+        DevArray d(D, n2, true, e.stream());
+        DevArray j(J, n2, false, e.stream());
+        DevArray k(K, n2, false, e.stream());
         JKStats st;
         e.jk(d.ptr, j.ptr, k.ptr, toOpts(opts), &st);
         j.copyOut();
@@ -555,6 +557,79 @@ int lible_gpu_jk(lible_gpu_ctx *ctx, const double *D, double *J, double *K, cons
             stats->n_quartets = st.n_quartets;
             stats->n_fp32 = st.n_fp32;
             stats->n_launches = st.n_launches;
+        }
+    });
+}
+
+int lible_gpu_set_batch(lible_gpu_ctx *ctx, int n_mol, const char *basis_root, const char *const *basis,
+                        const int *n_atoms, const int *atomic_nrs, const double *xyz, int units)
+{
+    return guard(ctx, [&](Engine &e) {
+        if (n_mol <= 0 || !basis_root || !basis || !n_atoms || !atomic_nrs || !xyz)
+            throw EngineError(kStatusInvalid, "invalid batch arguments");
+        std::vector<std::vector<BasisAtom>> mols;
+        std::vector<std::vector<std::array<double, 3>>> xyzs;
+        std::map<std::string, std::string> paths;
+        long long at = 0;
+        for (int m = 0; m < n_mol; m++)
+        {
+            if (!basis[m] || n_atoms[m] <= 0)
+                throw EngineError(kStatusInvalid, "invalid batch molecule " + std::to_string(m));
+            auto it = paths.find(basis[m]);
+            if (it == paths.end())
+                it = paths.emplace(basis[m], findBasisFile(basis_root, basis[m])).first;
+            std::vector<BasisAtom> atoms;
+            for (int a = 0; a < n_atoms[m]; a++)
+                atoms.push_back(readBasisAtom(it->second, atomic_nrs[at + a]));
+            mols.push_back(std::move(atoms));
+            xyzs.push_back(coords(n_atoms[m], xyz + 3 * at, units));
+            at += n_atoms[m];
+        }
+        e.setBatch(mols, xyzs);
+    });
+}
+
+int lible_gpu_batch_layout(lible_gpu_ctx *ctx, int *n_mol, long long *nao, long long *base, long long *packed)
+{
+    return guard(ctx, [&](Engine &e) {
+        const auto &na = e.molNao(), &mb = e.molBase();
+        if (n_mol)
+            *n_mol = (int)na.size();
+        for (size_t m = 0; m < na.size(); m++)
+        {
+            if (nao)
+                nao[m] = na[m];
+            if (base)
+                base[m] = mb[m];
+        }
+        if (packed)
+            *packed = e.packedSize();
+    });
+}
+
+int lible_gpu_set_tune_cache(lible_gpu_ctx *ctx, const char *path)
+{
+    return guard(ctx, [&](Engine &e) { e.setTuneCache(path ? path : ""); });
+}
+
+int lible_gpu_jk_autotune(lible_gpu_ctx *ctx, const double *D, double *J, double *K, const lible_gpu_jk_opts *opts,
+                          const char *cache_path, char *summary, int summary_len)
+{
+    return guard(ctx, [&](Engine &e) {
+        if (!D || !J || !K)
+            throw EngineError(kStatusInvalid, "null D/J/K");
+        const size_t n2 = (size_t)e.packedSize();
+        DevArray d(D, n2, true, e.stream());
+        DevArray j(J, n2, false, e.stream());
+        DevArray k(K, n2, false, e.stream());
+        std::string s = e.jkAutotune(d.ptr, j.ptr, k.ptr, toOpts(opts), cache_path ? cache_path : "");
+        j.copyOut();
+        k.copyOut();
+        if (summary && summary_len > 0)
+        {
+            const size_t c = std::min<size_t>(s.size(), (size_t)summary_len - 1);
+            std::memcpy(summary, s.data(), c);
+            summary[c] = 0;
         }
     });
 }
@@ -626,27 +701,27 @@ int lible_gpu_jk_energy_forward(lible_gpu_ctx *ctx, const double *D, const lible
     return guard(ctx, [&](Engine &e) {
         if (!D || !energy)
             throw EngineError(kStatusInvalid, "null D/energy");
-        const size_t n = e.nao();
-        DevArray d(D, n * n, true, e.stream());
-        DevArray j(J, n * n, false, e.stream());
-        DevArray k(K, n * n, false, e.stream());
+        const size_t nn = (size_t)e.packedSize();
+        DevArray d(D, nn, true, e.stream());
+        DevArray j(J, nn, false, e.stream());
+        DevArray k(K, nn, false, e.stream());
         double *jp = j.ptr, *kp = k.ptr, *tmp = nullptr;
         if (!jp || !kp)
         {
-            cudaCheck(cudaMalloc(&tmp, 2 * n * n * sizeof(double)), "cudaMalloc");
+            cudaCheck(cudaMalloc(&tmp, 2 * nn * sizeof(double)), "cudaMalloc");
             if (!jp)
                 jp = tmp;
             if (!kp)
-                kp = tmp + n * n;
+                kp = tmp + nn;
         }
         e.jk(d.ptr, jp, kp, toOpts(opts), nullptr);
-        std::vector<double> hd(n * n), hj(n * n), hk(n * n);
-        cudaCheck(cudaMemcpyAsync(hd.data(), d.ptr, n * n * 8, cudaMemcpyDeviceToHost, e.stream()), "D2H");
-        cudaCheck(cudaMemcpyAsync(hj.data(), jp, n * n * 8, cudaMemcpyDeviceToHost, e.stream()), "D2H");
-        cudaCheck(cudaMemcpyAsync(hk.data(), kp, n * n * 8, cudaMemcpyDeviceToHost, e.stream()), "D2H");
+        std::vector<double> hd(nn), hj(nn), hk(nn);
+        cudaCheck(cudaMemcpyAsync(hd.data(), d.ptr, nn * 8, cudaMemcpyDeviceToHost, e.stream()), "D2H");
+        cudaCheck(cudaMemcpyAsync(hj.data(), jp, nn * 8, cudaMemcpyDeviceToHost, e.stream()), "D2H");
+        cudaCheck(cudaMemcpyAsync(hk.data(), kp, nn * 8, cudaMemcpyDeviceToHost, e.stream()), "D2H");
         cudaCheck(cudaStreamSynchronize(e.stream()), "sync");
         double s = 0.0;
-        for (size_t x = 0; x < n * n; x++)
+        for (size_t x = 0; x < nn; x++)
             s += hd[x] * (0.5 * hj[x] - 0.25 * hk[x]);
         *energy = s;
         if (J)

@@ -68,6 +68,7 @@ namespace lible_b200
         const unsigned long long *chunks;
         long long n_chunks;
         unsigned long long *counter;
+        int grid_div;                     // persistent grid: resident blocks per SM / grid_div
         // epilogue
         int mode;
         int flags;                        // kStore: bit0 swap bra shells, bit1 swap ket shells, bit2 swap bra/ket

@@ -6,6 +6,8 @@
 
 #include <algorithm>
 #include <chrono>
+#include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <numeric>
 #include <stdexcept>
@@ -255,6 +257,24 @@ namespace lible_b200
         }
     }
 
+    // A_m <- A_m + A_m^T for every packed block m = blockIdx.y (blocks[2m] = first element,
+    // blocks[2m+1] = N_m).
+    __global__ void symmetrizeBlocksKernel(double *A, const long long *blocks)
+    {
+        const long long base = blocks[2 * blockIdx.y], n = blocks[2 * blockIdx.y + 1];
+        double *M = A + base;
+        for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; g < n * n;
+             g += (long long)gridDim.x * blockDim.x)
+        {
+            const long long r = g / n, c = g % n;
+            if (c > r)
+                continue;
+            const double v = M[r * n + c] + M[c * n + r];
+            M[r * n + c] = v;
+            M[c * n + r] = v;
+        }
+    }
+
     // Reorders D1 batches from the internal orientation to the caller's, selecting the caller's
     // derivative blocks: out[t][slot(c)*3 + x][caller element] = in[t][c*3 + x][internal element].
     __global__ void reorderD1Kernel(const double *in, long long n_tasks, int sa, int sb, int sc, int sd,
@@ -328,6 +348,13 @@ namespace lible_b200
         cudaDeviceProp prop;
         cudaCheck(cudaGetDeviceProperties(&prop, device), "cudaGetDeviceProperties");
         num_sms_ = prop.multiProcessorCount;
+        gpu_name_ = prop.name;
+        for (int b = 0; b < kBranches; b++)
+        {
+            cudaCheck(cudaStreamCreateWithFlags(&branch_[b], cudaStreamNonBlocking), "cudaStreamCreate");
+            cudaCheck(cudaEventCreateWithFlags(&join_[b], cudaEventDisableTiming), "cudaEventCreate");
+        }
+        cudaCheck(cudaEventCreateWithFlags(&fork_, cudaEventDisableTiming), "cudaEventCreate");
         boys_ = devUpload(boysGrid(), stream_);
         boys_f_ = devUpload(boysGridF(), stream_);
         std::vector<int> rc;
@@ -359,7 +386,21 @@ namespace lible_b200
         cudaFree(boys_f_);
         cudaFree(sph_rc_);
         cudaFree(sph_val_);
+        for (int b = 0; b < kBranches; b++)
+        {
+            cudaStreamDestroy(branch_[b]);
+            cudaEventDestroy(join_[b]);
+        }
+        cudaEventDestroy(fork_);
         cudaStreamDestroy(stream_);
+    }
+
+    void Engine::releaseGraph()
+    {
+        if (graph_exec_)
+            cudaGraphExecDestroy(graph_exec_);
+        graph_exec_ = nullptr;
+        graph_key_.clear();
     }
 
     void Engine::freeSet(ClassSet &cs)
@@ -376,6 +417,14 @@ namespace lible_b200
 
     void Engine::clearStructure()
     {
+        releaseGraph();
+        cudaFree(d_blocks_);
+        d_blocks_ = nullptr;
+        batch_ = false;
+        mol_shells_.clear();
+        mol_nao_.clear();
+        mol_base_.clear();
+        packed_ = 0;
         freeSet(symm_);
         freeSet(nosymm_);
         freeSet(aux_);
@@ -419,6 +468,56 @@ namespace lible_b200
                 max_l_aux_ = std::max(max_l_aux_, s.l);
             }
         }
+        mol_nao_ = {(long long)nao_};
+        mol_base_ = {0};
+        packed_ = (long long)(nao_ * nao_);
+        d_blocks_ = devUpload(std::vector<long long>{0, (long long)nao_}, stream_);
+        cudaCheck(cudaStreamSynchronize(stream_), "upload");
+        has_structure_ = true;
+    }
+
+    void Engine::setBatch(const std::vector<std::vector<BasisAtom>> &mols,
+                          const std::vector<std::vector<std::array<double, 3>>> &xyz_bohr)
+    {
+        clearStructure();
+        if (mols.empty() || mols.size() != xyz_bohr.size())
+            throw EngineError(kStatusInvalid, "a batch needs one coordinate set per molecule");
+        size_t shell_ofs = 0, atom_ofs = 0;
+        std::vector<long long> blocks;
+        max_l_ = 0;
+        nao_ = 0;
+        for (size_t m = 0; m < mols.size(); m++)
+        {
+            auto sh = constructShells(mols[m], xyz_bohr[m]);
+            long long n = 0;
+            for (auto &x : sh)
+            {
+                x.mol = (int)m;
+                x.idx += shell_ofs;
+                x.atom += atom_ofs;
+                n += nsph(x.l);
+                max_l_ = std::max(max_l_, x.l);
+            }
+            shell_ofs += sh.size();
+            atom_ofs += xyz_bohr[m].size();
+            mol_nao_.push_back(n);
+            mol_base_.push_back(packed_);
+            blocks.push_back(packed_);
+            blocks.push_back(n);
+            packed_ += n * n;
+            nao_ += (size_t)n;
+            shells_.insert(shells_.end(), sh.begin(), sh.end());
+            mol_shells_.push_back(std::move(sh));
+        }
+        if (max_l_ > 3)
+            throw EngineError(kStatusUnsupported, "main basis shells with l > 3 are not supported");
+        if (packed_ >= (1LL << 31))
+            throw EngineError(kStatusInvalid, "batch too large: packed matrices exceed 2^31 elements");
+        n_atoms_ = (int)atom_ofs;
+        has_aux_ = false;
+        batch_ = true;
+        d_blocks_ = devUpload(blocks, stream_);
+        cudaCheck(cudaStreamSynchronize(stream_), "upload");
         has_structure_ = true;
     }
 
@@ -447,6 +546,8 @@ namespace lible_b200
             info[8 * i + 3] = pc.atom_b[i];
             info[8 * i + 4] = pc.shell_a[i];
             info[8 * i + 5] = pc.shell_b[i];
+            info[8 * i + 6] = pc.mat_base.empty() ? 0 : pc.mat_base[i];
+            info[8 * i + 7] = pc.mat_n.empty() ? (int32_t)nao_ : pc.mat_n[i];
         }
         d.info = devUpload(info, stream_);
         d.pofs = devUpload(pc.pofs, stream_);
@@ -517,7 +618,23 @@ namespace lible_b200
         for (int la = 0; la <= max_l_; la++)
             for (int lb = 0; lb <= (use_symm ? la : max_l_); lb++)
             {
-                PairClass pc = buildPairClass(use_symm, la, lb, shellsL(shells_, la), shellsL(shells_, lb));
+                PairClass pc;
+                if (batch_)
+                {
+                    // pairs only within a molecule, tagged with the molecule's packed block
+                    for (size_t m = 0; m < mol_shells_.size(); m++)
+                        appendPairClass(pc, buildPairClass(use_symm, la, lb, shellsL(mol_shells_[m], la),
+                                                           shellsL(mol_shells_[m], lb)),
+                                        (int32_t)mol_base_[m], (int32_t)mol_nao_[m]);
+                    if (pc.pofs.empty())
+                    {
+                        pc.la = la;
+                        pc.lb = lb;
+                        pc.pofs.push_back(0);
+                    }
+                }
+                else
+                    pc = buildPairClass(use_symm, la, lb, shellsL(shells_, la), shellsL(shells_, lb));
                 bool swapped = false;
                 if (lb > la)
                 {
@@ -573,6 +690,13 @@ namespace lible_b200
     {
         if (!has_structure_)
             throw EngineError(kStatusNoStructure, "no structure has been set");
+    }
+
+    void Engine::requireSingle() const
+    {
+        requireStructure();
+        if (batch_)
+            throw EngineError(kStatusUnsupported, "this call takes a single structure, not a batch");
     }
 
     PairView Engine::view(const DevPairClass &d)
@@ -677,6 +801,7 @@ namespace lible_b200
 
     void Engine::eri4(double *out_dev)
     {
+        requireSingle();
         ClassSet &cs = mainSet(true);
         const long long n = (long long)nao_;
         cudaCheck(cudaMemsetAsync(out_dev, 0, (size_t)n * n * n * n * sizeof(double), stream_), "memset");
@@ -738,6 +863,7 @@ namespace lible_b200
 
     void Engine::eri4Diagonal(double *out_host)
     {
+        requireSingle();
         ClassSet &cs = mainSet(true);
         auto batches = diagonalBatches(cs);
         const size_t n = nao_;
@@ -761,6 +887,7 @@ namespace lible_b200
 
     void Engine::eri3(double *out_dev)
     {
+        requireSingle();
         ClassSet &ms = mainSet(true);
         ClassSet &xs = auxSet();
         const long long n = (long long)nao_, na = (long long)naux_;
@@ -794,6 +921,7 @@ namespace lible_b200
 
     void Engine::eri2(double *out_dev)
     {
+        requireSingle();
         ClassSet &xs = auxSet();
         const long long na = (long long)naux_;
         cudaCheck(cudaMemsetAsync(out_dev, 0, (size_t)na * na * sizeof(double), stream_), "memset");
@@ -825,6 +953,7 @@ namespace lible_b200
 
     void Engine::eri2Diagonal(double *out_host)
     {
+        requireSingle();
         ClassSet &xs = auxSet();
         auto batches = diagonalBatches(xs);
         std::fill(out_host, out_host + naux_, 0.0);
@@ -844,6 +973,7 @@ namespace lible_b200
     void Engine::eri4Batch(bool use_symm, int cab, int ccd, long long n, const uint32_t *pairs_host, double *out_dev,
                            bool d1)
     {
+        requireSingle();
         ClassSet &cs = mainSet(use_symm);
         if (cab < 0 || ccd < 0 || cab >= (int)cs.dev.size() || ccd >= (int)cs.dev.size())
             throw EngineError(kStatusInvalid, "class index out of range");
@@ -861,6 +991,7 @@ namespace lible_b200
     void Engine::eri3Batch(bool use_symm, int cab, int cx, long long n, const uint32_t *idx_host, double *out_dev,
                            bool d1)
     {
+        requireSingle();
         ClassSet &cs = mainSet(use_symm);
         ClassSet &xs = auxSet();
         if (cab < 0 || cx < 0 || cab >= (int)cs.dev.size() || cx >= (int)xs.dev.size())
@@ -878,6 +1009,7 @@ namespace lible_b200
 
     void Engine::eri2Batch(int ca, int cb, long long n, const uint32_t *idx_host, double *out_dev, bool d1)
     {
+        requireSingle();
         ClassSet &xs = auxSet();
         if (ca < 0 || cb < 0 || ca >= (int)xs.dev.size() || cb >= (int)xs.dev.size())
             throw EngineError(kStatusInvalid, "class index out of range");
@@ -918,21 +1050,26 @@ namespace lible_b200
             d.Q = devUpload(d.Qh, stream_);
             const auto &Q = d.Qh;
             const auto &pofs = cs.host[c].pofs;
+            const auto &mb = cs.host[c].mat_base;
             auto K = [&](uint32_t x) { return pofs[x + 1] - pofs[x]; };
+            auto M = [&](uint32_t x) { return mb.empty() ? 0 : mb[x]; };
             ClassOrder &o = cs.orders[c];
             o.order.resize(Q.size());
             std::iota(o.order.begin(), o.order.end(), 0u);
             std::stable_sort(o.order.begin(), o.order.end(), [&](uint32_t x, uint32_t y) {
+                if (M(x) != M(y))
+                    return M(x) < M(y);
                 return K(x) != K(y) ? K(x) < K(y) : Q[x] > Q[y];
             });
             o.q.resize(Q.size());
             o.kpre.assign(Q.size() + 1, 0.0);
             for (size_t i = 0; i < Q.size(); i++)
             {
-                o.q[i] = Q[o.order[i]];
-                o.kpre[i + 1] = o.kpre[i] + K(o.order[i]);
-                if (o.groups.empty() || o.groups.back().k != K(o.order[i]))
-                    o.groups.push_back({K(o.order[i]), (uint32_t)i, (uint32_t)i});
+                const uint32_t x = o.order[i];
+                o.q[i] = Q[x];
+                o.kpre[i + 1] = o.kpre[i] + K(x);
+                if (o.groups.empty() || o.groups.back().k != K(x) || o.groups.back().mol != M(x))
+                    o.groups.push_back({K(x), (uint32_t)i, (uint32_t)i, M(x)});
                 o.groups.back().end = (uint32_t)i + 1;
             }
             o.d_order = devUpload(o.order, stream_);
@@ -1022,16 +1159,22 @@ namespace lible_b200
         cp.ck = ck;
         std::vector<uint32_t> majors, b64, b32;
         std::vector<unsigned long long> p64(1, 0), p32(1, 0);
-        std::vector<unsigned long long> run64, run32;  // tasks per major entry
-        std::vector<double> cost;                      // primitive quartets per task of the entry
+        auto &run64 = cp.run64, &run32 = cp.run32;  // tasks per major entry
+        auto &cost = cp.cost;                       // primitive quartets (+ overhead) per task
         double bra_prims64 = 0, bra_prims32 = 0;
-        // groups are in increasing K; walk them backwards so the heaviest segments come first
-        for (size_t gbr = ob.groups.size(); gbr-- > 0;)
-            for (size_t gcr = ok.groups.size(); gcr-- > 0;)
+        // segments (bra group, ket group) of the same molecule, heaviest (largest K_b K_k) first
+        std::vector<std::pair<uint32_t, uint32_t>> segs;
+        for (uint32_t gb = 0; gb < (uint32_t)ob.groups.size(); gb++)
+            for (uint32_t gc = 0; gc < (uint32_t)ok.groups.size(); gc++)
+                if (!(triangle && gb < gc) && ob.groups[gb].mol == ok.groups[gc].mol)
+                    segs.push_back({gb, gc});
+        std::stable_sort(segs.begin(), segs.end(), [&](const auto &x, const auto &y) {
+            return (double)ob.groups[x.first].k * ok.groups[x.second].k >
+                   (double)ob.groups[y.first].k * ok.groups[y.second].k;
+        });
+        for (const auto &sg : segs)
             {
-                const size_t gb = gbr, gc = gcr;
-                if (triangle && gb < gc)
-                    continue;
+                const size_t gb = sg.first, gc = sg.second;
                 const auto &B = ob.groups[gb], &C = ok.groups[gc];
                 for (uint32_t j = C.start; j < C.end; j++)
                 {
@@ -1068,6 +1211,8 @@ namespace lible_b200
         cp.n64 = (long long)p64.back();
         cp.n32 = (long long)p32.back();
         const auto &B = bs.host[cb], &K = ks.host[ck];
+        cp.tb = pairType(B.la, B.lb);
+        cp.tk = pairType(K.la, K.lb);
         const int L = B.la + B.lb + K.la + K.lb;
         const double hab = nherm(B.la + B.lb), hcd = nherm(K.la + K.lb);
         const double sab = nsph(B.la) * nsph(B.lb), scd = nsph(K.la) * nsph(K.lb);
@@ -1084,18 +1229,31 @@ namespace lible_b200
         cp.prefix32 = devUpload(p32, stream_);
         cp.begin64 = devUpload(b64, stream_);
         cp.begin32 = devUpload(b32, stream_);
-        const int tb = pairType(B.la, B.lb), tk = pairType(K.la, K.lb);
-        for (int fp32 = 0; fp32 < 2; fp32++)
-        {
-            const long long n = fp32 ? cp.n32 : cp.n64;
-            const int unit = unitFwd(tb, tk, fp32 == 1);
-            if (n == 0 || unit == 0)
-                continue;
-            auto ch = costChunks(fp32 ? run32 : run64, cost, unit, 8 * unit);
-            (fp32 ? cp.n_chunks32 : cp.n_chunks64) = (long long)ch.size() - 1;
-            (fp32 ? cp.chunks32 : cp.chunks64) = devUpload(ch, stream_);
-        }
+        rebuildChunks(cp, false, cp.chunk_mult64);
+        rebuildChunks(cp, true, cp.chunk_mult32);
         return cp;
+    }
+
+    // (Re)cuts the FP64 or FP32 task sequence of a class pair into work-queue chunks of at most
+    // `mult` work units.
+    void Engine::rebuildChunks(JKClassPair &cp, bool fp32, int mult)
+    {
+        const long long n = fp32 ? cp.n32 : cp.n64;
+        unsigned long long *&dev = fp32 ? cp.chunks32 : cp.chunks64;
+        cudaFree(dev);
+        dev = nullptr;
+        (fp32 ? cp.n_chunks32 : cp.n_chunks64) = 0;
+        (fp32 ? cp.chunk_mult32 : cp.chunk_mult64) = mult;
+        if (n == 0)
+            return;
+        // bra / ket classes of the launch: the bra set is the auxiliary one for swapped RI pairs
+        const int tb = cp.tb, tk = cp.tk;
+        const int unit = unitFwd(tb, tk, fp32);
+        if (unit == 0)
+            return;
+        auto ch = costChunks(fp32 ? cp.run32 : cp.run64, cp.cost, unit, mult * unit);
+        (fp32 ? cp.n_chunks32 : cp.n_chunks64) = (long long)ch.size() - 1;
+        dev = devUpload(ch, stream_);
     }
 
     // Unique quartets (ab|cd), class cd <= class ab, kept iff Q_ab Q_cd >= thr.
@@ -1128,9 +1286,106 @@ namespace lible_b200
             return x.flops64 + x.flops32 > y.flops64 + y.flops32;
         });
         plan.counters = devAlloc<unsigned long long>(2 * std::max<size_t>(plan.pairs.size(), 1));
+        plan.key = key;
+        applyTuneCache(plan);
+        assignBranches(plan);
         cudaCheck(cudaStreamSynchronize(stream_), "plan");
         plan.thr = thr;
         return plans_.emplace(key, std::move(plan)).first->second;
+    }
+
+    // Longest-processing-time assignment of the class pairs (already in decreasing cost) to the
+    // stream branches of the fork/join launch sequence, so the tail of one class kernel overlaps
+    // the next ones.
+    void Engine::assignBranches(JKPlan &plan)
+    {
+        double load[kBranches] = {};
+        for (auto &cp : plan.pairs)
+        {
+            int b = 0;
+            for (int i = 1; i < kBranches; i++)
+                if (load[i] < load[b])
+                    b = i;
+            cp.branch = b;
+            load[b] += cp.flops64 + 0.5 * cp.flops32 + 1e6;
+        }
+    }
+
+    // Launches one J/K build of `plan` (memsets, class kernels over the stream branches, block
+    // symmetrisation) on stream_; usable inside a stream capture.
+    void Engine::enqueueJK(JKPlan &plan, const double *D, double *J, double *K, bool mixed)
+    {
+        ClassSet &cs = mainSet(true);
+        const size_t n = (size_t)packed_;
+        cudaCheck(cudaMemsetAsync(J, 0, n * sizeof(double), stream_), "memset");
+        cudaCheck(cudaMemsetAsync(K, 0, n * sizeof(double), stream_), "memset");
+        cudaCheck(cudaMemsetAsync(plan.counters, 0, 2 * plan.pairs.size() * sizeof(unsigned long long), stream_),
+                  "memset");
+        cudaCheck(cudaEventRecord(fork_, stream_), "fork");
+        bool used[kBranches] = {};
+        for (const auto &cp : plan.pairs)
+            used[cp.branch] = true;
+        for (int b = 0; b < kBranches; b++)
+            if (used[b])
+                cudaCheck(cudaStreamWaitEvent(branch_[b], fork_, 0), "fork");
+        for (size_t ip = 0; ip < plan.pairs.size(); ip++)
+        {
+            const auto &cp = plan.pairs[ip];
+            const auto &B = cs.dev[cp.cb], &Kc = cs.dev[cp.ck];
+            cudaStream_t st = branch_[cp.branch];
+            QuartetArgs a{};
+            a.bra = view(B);
+            a.ket = view(Kc);
+            a.boys = boys_;
+            a.boys_f = boys_f_;
+            a.list = nullptr;
+            a.major_ket = 1;
+            a.major_order = cp.majors;
+            a.minor_order = cs.orders[cp.cb].d_order;
+            a.n_major = cp.n_bra;
+            a.same_class = cp.cb == cp.ck;
+            a.mode = kJK;
+            a.D = D;
+            a.J = J;
+            a.K = K;
+            a.nao = (int)nao_;
+            a.n_tasks = cp.n64;
+            a.prefix = cp.prefix64;
+            a.minor_begin = cp.begin64;
+            a.chunks = cp.chunks64;
+            a.n_chunks = cp.n_chunks64;
+            a.counter = plan.counters + 2 * ip;
+            a.grid_div = cp.grid_div64;
+            LaunchFn f64 = lookupFwd64(cp.tb, cp.tk);
+            if (!f64)
+                throw EngineError(kStatusUnsupported, "quartet class not instantiated");
+            cudaCheck(f64(a, st, num_sms_), "jk kernel");
+            if (mixed && cp.n32 > 0)
+            {
+                a.n_tasks = cp.n32;
+                a.prefix = cp.prefix32;
+                a.minor_begin = cp.begin32;
+                a.chunks = cp.chunks32;
+                a.n_chunks = cp.n_chunks32;
+                a.counter = plan.counters + 2 * ip + 1;
+                a.grid_div = cp.grid_div32;
+                LaunchFn f32 = lookupFwd32(cp.tb, cp.tk);
+                if (!f32)
+                    throw EngineError(kStatusUnsupported, "FP32 quartet class not instantiated");
+                cudaCheck(f32(a, st, num_sms_), "jk kernel fp32");
+            }
+        }
+        for (int b = 0; b < kBranches; b++)
+            if (used[b])
+            {
+                cudaCheck(cudaEventRecord(join_[b], branch_[b]), "join");
+                cudaCheck(cudaStreamWaitEvent(stream_, join_[b], 0), "join");
+            }
+        const dim3 grid((unsigned)std::max(1, num_sms_ * 4 / (int)std::max<size_t>(mol_nao_.size(), 1)),
+                        (unsigned)mol_nao_.size());
+        symmetrizeBlocksKernel<<<grid, 256, 0, stream_>>>(J, d_blocks_);
+        symmetrizeBlocksKernel<<<grid, 256, 0, stream_>>>(K, d_blocks_);
+        cudaCheck(cudaGetLastError(), "symmetrize");
     }
 
     // Three-centre (mn|P) quartets of every main pair class with every auxiliary shell class, kept iff
@@ -1170,58 +1425,41 @@ namespace lible_b200
 
     void Engine::jk(const double *D_dev, double *J_dev, double *K_dev, const JKOptions &opt, JKStats *stats)
     {
-        ClassSet &cs = mainSet(true);
         const bool mixed = opt.precision == 1;
         if (mixed && max_l_ > 2)
             throw EngineError(kStatusUnsupported, "mixed precision is instantiated for l <= 2 bases only");
         JKPlan &plan = jkPlan(opt.schwarz, opt.fp32_threshold, mixed);
-        const size_t n = nao_;
-        cudaCheck(cudaMemsetAsync(J_dev, 0, n * n * sizeof(double), stream_), "memset");
-        cudaCheck(cudaMemsetAsync(K_dev, 0, n * n * sizeof(double), stream_), "memset");
-        cudaCheck(cudaMemsetAsync(plan.counters, 0, 2 * plan.pairs.size() * sizeof(unsigned long long), stream_),
-                  "memset");
-        for (size_t ip = 0; ip < plan.pairs.size(); ip++)
+        if (opt.use_graph)
         {
-            const auto &cp = plan.pairs[ip];
-            const auto &B = cs.dev[cp.cb], &K = cs.dev[cp.ck];
-            QuartetArgs a{};
-            a.bra = view(B);
-            a.ket = view(K);
-            a.boys = boys_;
-            a.boys_f = boys_f_;
-            a.list = nullptr;
-            a.major_ket = 1;
-            a.major_order = cp.majors;
-            a.minor_order = cs.orders[cp.cb].d_order;
-            a.n_major = cp.n_bra;
-            a.same_class = cp.cb == cp.ck;
-            a.mode = kJK;
-            a.D = D_dev;
-            a.J = J_dev;
-            a.K = K_dev;
-            a.nao = (int)n;
-            const int tb = pairType(B.la, B.lb), tk = pairType(K.la, K.lb);
-            a.n_tasks = cp.n64;
-            a.prefix = cp.prefix64;
-            a.minor_begin = cp.begin64;
-            a.chunks = cp.chunks64;
-            a.n_chunks = cp.n_chunks64;
-            a.counter = plan.counters + 2 * ip;
-            cudaCheck(lookupFwd64(tb, tk)(a, stream_, num_sms_), "jk kernel");
-            if (cp.n32 > 0)
+            char key[256];
+            snprintf(key, sizeof(key), "%s|%p|%p|%p", plan.key.c_str(), (const void *)D_dev, (void *)J_dev,
+                     (void *)K_dev);
+            if (!graph_exec_ || graph_key_ != key)
             {
-                a.n_tasks = cp.n32;
-                a.prefix = cp.prefix32;
-                a.minor_begin = cp.begin32;
-                a.chunks = cp.chunks32;
-                a.n_chunks = cp.n_chunks32;
-                a.counter = plan.counters + 2 * ip + 1;
-                cudaCheck(lookupFwd32(tb, tk)(a, stream_, num_sms_), "jk kernel fp32");
+                releaseGraph();
+                cudaGraph_t g = nullptr;
+                cudaCheck(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "capture");
+                try
+                {
+                    enqueueJK(plan, D_dev, J_dev, K_dev, mixed);
+                }
+                catch (...)
+                {
+                    cudaStreamEndCapture(stream_, &g);
+                    if (g)
+                        cudaGraphDestroy(g);
+                    throw;
+                }
+                cudaCheck(cudaStreamEndCapture(stream_, &g), "capture");
+                cudaError_t e = cudaGraphInstantiate(&graph_exec_, g, 0);
+                cudaGraphDestroy(g);
+                cudaCheck(e, "cudaGraphInstantiate");
+                graph_key_ = key;
             }
+            cudaCheck(cudaGraphLaunch(graph_exec_, stream_), "cudaGraphLaunch");
         }
-        symmetrizeKernel<<<num_sms_ * 4, 256, 0, stream_>>>(J_dev, (long long)n);
-        symmetrizeKernel<<<num_sms_ * 4, 256, 0, stream_>>>(K_dev, (long long)n);
-        cudaCheck(cudaGetLastError(), "symmetrize");
+        else
+            enqueueJK(plan, D_dev, J_dev, K_dev, mixed);
         if (stats)
         {
             stats->n_quartets = plan.n_quartets;
@@ -1230,6 +1468,166 @@ namespace lible_b200
             for (const auto &cp : plan.pairs)
                 stats->n_launches += 1 + (cp.n32 > 0 ? 1 : 0);
         }
+    }
+
+    // ------------------------------------------------------------------------------------------
+    // Autotuning of the class-pair launches.  The tunable "tile" of a persistent class kernel is
+    // its occupancy (resident blocks per SM divided by grid_div) and the granularity of its work
+    // queue (chunks of at most chunk_mult work units); every candidate is timed on the caller's
+    // buffers with CUDA events and the fastest is kept.  Results are keyed by GPU name, quartet
+    // class and the size bucket floor(log2(tasks)), and appended to a plain-text cache:
+    //     <gpu>|<la> <lb> <lc> <ld>|<fp32>|<bucket>|<grid_div> <chunk_mult>
+
+    static int sizeBucket(long long n)
+    {
+        int b = 0;
+        while ((1LL << (b + 1)) <= n)
+            b++;
+        return b;
+    }
+
+    void Engine::applyTuneCache(JKPlan &plan)
+    {
+        if (tune_cache_.empty())
+            return;
+        FILE *f = fopen(tune_cache_.c_str(), "r");
+        if (!f)
+            return;
+        std::map<std::string, std::pair<int, int>> entries;
+        char line[512];
+        while (fgets(line, sizeof(line), f))
+        {
+            std::string l(line);
+            const size_t bar = l.rfind('|');
+            if (bar == std::string::npos)
+                continue;
+            int gd = 0, cm = 0;
+            if (sscanf(l.c_str() + bar + 1, "%d %d", &gd, &cm) == 2 && gd > 0 && cm > 0)
+                entries[l.substr(0, bar)] = {gd, cm};
+        }
+        fclose(f);
+        ClassSet &cs = mainSet(true);
+        for (auto &cp : plan.pairs)
+            for (int fp32 = 0; fp32 < 2; fp32++)
+            {
+                const long long n = fp32 ? cp.n32 : cp.n64;
+                if (n == 0)
+                    continue;
+                const auto &B = cs.host[cp.cb], &K = cs.host[cp.ck];
+                char key[256];
+                snprintf(key, sizeof(key), "%s|%d %d %d %d|%d|%d", gpu_name_.c_str(), B.la, B.lb, K.la, K.lb, fp32,
+                         sizeBucket(n));
+                auto it = entries.find(key);
+                if (it == entries.end())
+                    continue;
+                (fp32 ? cp.grid_div32 : cp.grid_div64) = it->second.first;
+                if (it->second.second != (fp32 ? cp.chunk_mult32 : cp.chunk_mult64))
+                    rebuildChunks(cp, fp32 == 1, it->second.second);
+                plan.tuned = true;
+            }
+    }
+
+    std::string Engine::jkAutotune(const double *D, double *J, double *K, const JKOptions &opt,
+                                   const std::string &cache)
+    {
+        const bool mixed = opt.precision == 1;
+        if (mixed && max_l_ > 2)
+            throw EngineError(kStatusUnsupported, "mixed precision is instantiated for l <= 2 bases only");
+        if (!cache.empty())
+            tune_cache_ = cache;
+        JKPlan &plan = jkPlan(opt.schwarz, opt.fp32_threshold, mixed);
+        releaseGraph();
+        ClassSet &cs = mainSet(true);
+        cudaEvent_t e0, e1;
+        cudaCheck(cudaEventCreate(&e0), "event");
+        cudaCheck(cudaEventCreate(&e1), "event");
+        std::string summary;
+        FILE *out = cache.empty() ? nullptr : fopen(cache.c_str(), "a");
+        const int grid_divs[] = {1, 2};
+        const int mults[] = {2, 8, 32};
+        for (size_t ip = 0; ip < plan.pairs.size(); ip++)
+        {
+            JKClassPair &cp = plan.pairs[ip];
+            const auto &B = cs.dev[cp.cb], &Kc = cs.dev[cp.ck];
+            for (int fp32 = 0; fp32 < (mixed ? 2 : 1); fp32++)
+            {
+                const long long n = fp32 ? cp.n32 : cp.n64;
+                if (n == 0)
+                    continue;
+                LaunchFn fn = fp32 ? lookupFwd32(cp.tb, cp.tk) : lookupFwd64(cp.tb, cp.tk);
+                if (!fn)
+                    throw EngineError(kStatusUnsupported, "quartet class not instantiated");
+                float best = 1e30f;
+                int best_gd = 1, best_cm = 8;
+                for (int cm : mults)
+                {
+                    rebuildChunks(cp, fp32 == 1, cm);
+                    for (int gd : grid_divs)
+                    {
+                        QuartetArgs a{};
+                        a.bra = view(B);
+                        a.ket = view(Kc);
+                        a.boys = boys_;
+                        a.boys_f = boys_f_;
+                        a.major_ket = 1;
+                        a.major_order = cp.majors;
+                        a.minor_order = cs.orders[cp.cb].d_order;
+                        a.n_major = cp.n_bra;
+                        a.same_class = cp.cb == cp.ck;
+                        a.mode = kJK;
+                        a.D = D;
+                        a.J = J;
+                        a.K = K;
+                        a.nao = (int)nao_;
+                        a.n_tasks = n;
+                        a.prefix = fp32 ? cp.prefix32 : cp.prefix64;
+                        a.minor_begin = fp32 ? cp.begin32 : cp.begin64;
+                        a.chunks = fp32 ? cp.chunks32 : cp.chunks64;
+                        a.n_chunks = fp32 ? cp.n_chunks32 : cp.n_chunks64;
+                        a.counter = plan.counters + 2 * ip + fp32;
+                        a.grid_div = gd;
+                        float t_min = 1e30f;
+                        for (int rep = 0; rep < 2; rep++)
+                        {
+                            cudaCheck(cudaMemsetAsync(a.counter, 0, sizeof(unsigned long long), stream_), "memset");
+                            cudaCheck(cudaEventRecord(e0, stream_), "event");
+                            cudaCheck(fn(a, stream_, num_sms_), "autotune kernel");
+                            cudaCheck(cudaEventRecord(e1, stream_), "event");
+                            cudaCheck(cudaEventSynchronize(e1), "event");
+                            float ms = 0;
+                            cudaCheck(cudaEventElapsedTime(&ms, e0, e1), "event");
+                            t_min = std::min(t_min, ms);
+                        }
+                        if (t_min < best)
+                        {
+                            best = t_min;
+                            best_gd = gd;
+                            best_cm = cm;
+                        }
+                    }
+                }
+                if (best_cm != (fp32 ? cp.chunk_mult32 : cp.chunk_mult64))
+                    rebuildChunks(cp, fp32 == 1, best_cm);
+                (fp32 ? cp.grid_div32 : cp.grid_div64) = best_gd;
+                const auto &Bh = cs.host[cp.cb], &Kh = cs.host[cp.ck];
+                char line[320];
+                snprintf(line, sizeof(line), "%s|%d %d %d %d|%d|%d|%d %d\n", gpu_name_.c_str(), Bh.la, Bh.lb, Kh.la,
+                         Kh.lb, fp32, sizeBucket(n), best_gd, best_cm);
+                if (out)
+                    fputs(line, out);
+                char info[160];
+                snprintf(info, sizeof(info), "(%d%d|%d%d) %s tasks=%lld grid_div=%d chunk_mult=%d %.3f ms\n", Bh.la,
+                         Bh.lb, Kh.la, Kh.lb, fp32 ? "fp32" : "fp64", n, best_gd, best_cm, best);
+                summary += info;
+            }
+        }
+        if (out)
+            fclose(out);
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        cudaCheck(cudaStreamSynchronize(stream_), "autotune");
+        plan.tuned = true;
+        return summary;
     }
 
     long long Engine::jkLaunchCount(const JKOptions &opt)
@@ -1274,6 +1672,7 @@ namespace lible_b200
     // is the exact derivative of the energy lible_gpu_jk_energy_forward computes with that threshold.
     void Engine::jkGradient(const double *D_dev, double *grad_dev, double schwarz)
     {
+        requireSingle();
         ClassSet &cs = mainSet(true);
         JKPlan &plan = jkPlan(schwarz, 0.0, false);
         const size_t n = nao_;
@@ -1310,6 +1709,7 @@ namespace lible_b200
     void Engine::riContract(const double *D_dev, const double *dcoef_dev, double *gamma_dev, double *J_dev,
                             double schwarz)
     {
+        requireSingle();
         ClassSet &ms = mainSet(true);
         ClassSet &xs = auxSet();
         JKPlan &plan = riPlan(schwarz);

@@ -49,6 +49,7 @@ namespace lible_b200
     struct Shell
     {
         int l = 0, z = 0;
+        int mol = 0;                 // molecule of a batch (0 for a single structure)
         size_t idx = 0, atom = 0, ofs_sph = 0;
         double xyz[3] = {0, 0, 0};
         std::vector<double> exps, coeffs, prim_norms, norms;  // norms: one per spherical AO
@@ -77,7 +78,13 @@ namespace lible_b200
         std::vector<int32_t> atom_a, atom_b;
         std::vector<int32_t> shell_a, shell_b;  // shell indices (for degeneracy factors)
         std::vector<double> norms_a, norms_b;   // [n_pairs * S_a], [n_pairs * S_b]
+        // batches: per pair, the first element of its molecule's packed N_m x N_m matrices and N_m
+        // (empty for a single structure: base 0, stride N)
+        std::vector<int32_t> mat_base, mat_n;
     };
+
+    // Appends the pairs of `src` to `dst` (same la, lb), tagging them with a packed-matrix block.
+    void appendPairClass(PairClass &dst, const PairClass &src, int32_t mat_base, int32_t mat_n);
 
     PairClass buildPairClass(bool use_symm, int la, int lb, const std::vector<Shell> &sa,
                              const std::vector<Shell> &sb, double thr = kPrimitiveThreshold);

@@ -39,6 +39,7 @@ namespace lible_b200
         double schwarz = 1e-12;
         double fp32_threshold = 1e-4;
         int precision = 0;  // 0 FP64, 1 mixed (FP32 where Q_ab Q_cd < fp32_threshold)
+        int use_graph = 0;  // replay the launch sequence from a captured CUDA graph
     };
 
     struct JKStats
@@ -118,8 +119,26 @@ namespace lible_b200
         void eri4BatchNoAlloc(bool use_symm, int cab, int ccd, long long n, const uint32_t *pairs_host,
                               double *out_dev, uint32_t *scratch, long long max_pairs);
 
-        // Direct J/K (device pointers).  J, K symmetric on return.
+        // A batch of molecules whose J/K are built together: every class pair of every molecule goes
+        // through one launch per quartet class.  D, J and K are packed: molecule m's N_m x N_m
+        // matrix starts at element molBase()[m].  Only the J/K calls accept a batch.
+        void setBatch(const std::vector<std::vector<BasisAtom>> &mols,
+                      const std::vector<std::vector<std::array<double, 3>>> &xyz_bohr);
+        bool isBatch() const { return batch_; }
+        // Autotune cache read when J/K plans are built (empty: none).
+        void setTuneCache(const std::string &path) { tune_cache_ = path; }
+        const std::vector<long long> &molNao() const { return mol_nao_; }
+        const std::vector<long long> &molBase() const { return mol_base_; }
+        long long packedSize() const { return packed_; }
+
+        // Direct J/K (device pointers).  J, K symmetric on return.  With opt.use_graph the launch
+        // sequence is captured once per (plan, D, J, K) into a CUDA graph and replayed.
         void jk(const double *D_dev, double *J_dev, double *K_dev, const JKOptions &opt, JKStats *stats);
+        // Times the candidate launch parameters of every class pair of the plan for `opt` on the
+        // given buffers, keeps the fastest and appends them to `cache` (if non-empty).  Returns a
+        // one-line summary per class pair.
+        std::string jkAutotune(const double *D_dev, double *J_dev, double *K_dev, const JKOptions &opt,
+                               const std::string &cache);
         long long jkLaunchCount(const JKOptions &opt);
         JKPlanInfo jkPlanInfo(const JKOptions &opt);
         struct JKClassInfo
@@ -145,6 +164,7 @@ namespace lible_b200
             struct Group
             {
                 uint32_t k, start, end;
+                int32_t mol;  // packed-matrix base of the group's molecule (batches)
             };
             std::vector<uint32_t> order;
             std::vector<double> q, kpre;
@@ -169,9 +189,16 @@ namespace lible_b200
             double prim64 = 0, prim32 = 0, flops64 = 0, flops32 = 0;
             unsigned long long *prefix64 = nullptr, *prefix32 = nullptr;
             uint32_t *begin64 = nullptr, *begin32 = nullptr, *majors = nullptr;
-            // work-queue chunks of about equal primitive-quartet cost (task boundaries)
+            // work-queue chunks (task boundaries) and the runs they are cut from
             unsigned long long *chunks64 = nullptr, *chunks32 = nullptr;
             long long n_chunks64 = 0, n_chunks32 = 0;
+            std::vector<unsigned long long> run64, run32;
+            std::vector<double> cost;
+            // launch parameters (autotuned): resident blocks per SM divided by grid_div, chunks of
+            // at most chunk_mult work units
+            int grid_div64 = 1, grid_div32 = 1, chunk_mult64 = 8, chunk_mult32 = 8;
+            int branch = 0;  // stream branch of the fork/join launch sequence
+            int tb = 0, tk = 0;  // pair types of the launched (bra, ket) classes
         };
         struct JKPlan
         {
@@ -180,6 +207,8 @@ namespace lible_b200
             double n_prim = 0, flops64 = 0, flops32 = 0;
             std::vector<JKClassPair> pairs;
             unsigned long long *counters = nullptr;  // two work-queue counters per class pair
+            std::string key;
+            bool tuned = false;
         };
         // One class pair of a plan: bra class cb of set bs, ket class ck of set ks; `triangle`
         // keeps only unique pairs when both are the same class of the same set.
@@ -187,6 +216,12 @@ namespace lible_b200
                                    double thr, double thr32, bool mixed);
         JKPlan &riPlan(double thr);
 
+        void rebuildChunks(JKClassPair &cp, bool fp32, int mult);
+        void assignBranches(JKPlan &plan);
+        void enqueueJK(JKPlan &plan, const double *D, double *J, double *K, bool mixed);
+        void applyTuneCache(JKPlan &plan);
+        void requireSingle() const;
+        void releaseGraph();
         void clearStructure();
         void freeSet(ClassSet &cs);
         void freePlan(JKPlan &p);
@@ -211,6 +246,20 @@ namespace lible_b200
         double *sph_val_ = nullptr;
         std::vector<int> sph_ofs_;
         std::vector<void *> persistent_;
+
+        static constexpr int kBranches = 4;
+        cudaStream_t branch_[kBranches] = {};
+        cudaEvent_t fork_ = nullptr, join_[kBranches] = {};
+        cudaGraphExec_t graph_exec_ = nullptr;
+        std::string graph_key_;
+        std::string tune_cache_;
+        std::string gpu_name_;
+
+        bool batch_ = false;
+        std::vector<std::vector<Shell>> mol_shells_;
+        std::vector<long long> mol_nao_, mol_base_;
+        long long packed_ = 0;
+        long long *d_blocks_ = nullptr;  // [n_mol][2] packed base, N_m
 
         bool has_structure_ = false, has_aux_ = false;
         std::vector<Shell> shells_, aux_shells_;

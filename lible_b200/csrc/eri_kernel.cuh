@@ -121,9 +121,14 @@ namespace lible_b200
             tid = 0;
             stride = 1;
         }
-        const int n = a.nao;
+        // the quartet's molecule block of the packed D, J, K (bra and ket share it): first element
+        // and dimension from the bra pair's info record
+        const int n = bi[7];
+        const size_t base = (uint32_t)bi[6];
         const int oa = bi[0], ob = bi[1], oc = ki[0], od = ki[1];
-        const double *D = a.D;
+        const double *D = a.D + base;
+        double *const Jm = a.J + base;
+        double *const Km = a.K + base;
         constexpr int n0 = SA * SB, n1 = n0 + SC * SD, n2 = n1 + SA * SC, n3 = n2 + SA * SD,
                       n4 = n3 + SB * SC, n5 = n4 + SB * SD;
 #pragma unroll
@@ -140,7 +145,7 @@ namespace lible_b200
 #pragma unroll
                     for (int t = 0; t < SD; t++)
                         s += val(((m * SB + nn) * SC + k) * SD + t) * __ldg(D + (size_t)(oc + k) * n + od + t);
-                dst = a.J + (size_t)(oa + m) * n + ob + nn;
+                dst = Jm + (size_t)(oa + m) * n + ob + nn;
                 w = 2.0 * f;
             }
             else if (o < n1)
@@ -151,7 +156,7 @@ namespace lible_b200
 #pragma unroll
                     for (int nn = 0; nn < SB; nn++)
                         s += val(((m * SB + nn) * SC + k) * SD + t) * __ldg(D + (size_t)(oa + m) * n + ob + nn);
-                dst = a.J + (size_t)(oc + k) * n + od + t;
+                dst = Jm + (size_t)(oc + k) * n + od + t;
                 w = 2.0 * f;
             }
             else if (o < n2)
@@ -162,7 +167,7 @@ namespace lible_b200
 #pragma unroll
                     for (int t = 0; t < SD; t++)
                         s += val(((m * SB + nn) * SC + k) * SD + t) * __ldg(D + (size_t)(ob + nn) * n + od + t);
-                dst = a.K + (size_t)(oa + m) * n + oc + k;
+                dst = Km + (size_t)(oa + m) * n + oc + k;
                 w = f;
             }
             else if (o < n3)
@@ -173,7 +178,7 @@ namespace lible_b200
 #pragma unroll
                     for (int k = 0; k < SC; k++)
                         s += val(((m * SB + nn) * SC + k) * SD + t) * __ldg(D + (size_t)(ob + nn) * n + oc + k);
-                dst = a.K + (size_t)(oa + m) * n + od + t;
+                dst = Km + (size_t)(oa + m) * n + od + t;
                 w = f;
             }
             else if (o < n4)
@@ -184,7 +189,7 @@ namespace lible_b200
 #pragma unroll
                     for (int t = 0; t < SD; t++)
                         s += val(((m * SB + nn) * SC + k) * SD + t) * __ldg(D + (size_t)(oa + m) * n + od + t);
-                dst = a.K + (size_t)(ob + nn) * n + oc + k;
+                dst = Km + (size_t)(ob + nn) * n + oc + k;
                 w = f;
             }
             else
@@ -195,7 +200,7 @@ namespace lible_b200
 #pragma unroll
                     for (int k = 0; k < SC; k++)
                         s += val(((m * SB + nn) * SC + k) * SD + t) * __ldg(D + (size_t)(oa + m) * n + oc + k);
-                dst = a.K + (size_t)(ob + nn) * n + od + t;
+                dst = Km + (size_t)(ob + nn) * n + od + t;
                 w = f;
             }
             double v = w * s;

@@ -53,7 +53,7 @@ namespace lible_b200
                 return e;
             const long long workers_per_block = S::W == 0 ? S::block / 32 : 1;
             grid = std::min<long long>((a.n_chunks + workers_per_block - 1) / workers_per_block,
-                                       (long long)num_sms * std::max(occ, 1));
+                                       (long long)num_sms * std::max(occ / std::max(a.grid_div, 1), 1));
             grid = std::max<long long>(grid, 1);
         }
         else if constexpr (S::W == 0)

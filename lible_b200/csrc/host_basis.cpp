@@ -225,6 +225,37 @@ namespace lible_b200
         return pc;
     }
 
+    void appendPairClass(PairClass &dst, const PairClass &src, int32_t mat_base, int32_t mat_n)
+    {
+        if (dst.pofs.empty())
+        {
+            dst.la = src.la;
+            dst.lb = src.lb;
+            dst.single = src.single;
+            dst.pofs.push_back(0);
+        }
+        if (dst.la != src.la || dst.lb != src.lb)
+            throw std::runtime_error("appendPairClass(): class mismatch");
+        const uint32_t p0 = dst.pofs.back();
+        dst.exps.insert(dst.exps.end(), src.exps.begin(), src.exps.end());
+        dst.coeffs.insert(dst.coeffs.end(), src.coeffs.begin(), src.coeffs.end());
+        dst.coords.insert(dst.coords.end(), src.coords.begin(), src.coords.end());
+        for (size_t i = 1; i < src.pofs.size(); i++)
+            dst.pofs.push_back(p0 + src.pofs[i]);
+        dst.ao_a.insert(dst.ao_a.end(), src.ao_a.begin(), src.ao_a.end());
+        dst.ao_b.insert(dst.ao_b.end(), src.ao_b.begin(), src.ao_b.end());
+        dst.atom_a.insert(dst.atom_a.end(), src.atom_a.begin(), src.atom_a.end());
+        dst.atom_b.insert(dst.atom_b.end(), src.atom_b.begin(), src.atom_b.end());
+        dst.shell_a.insert(dst.shell_a.end(), src.shell_a.begin(), src.shell_a.end());
+        dst.shell_b.insert(dst.shell_b.end(), src.shell_b.begin(), src.shell_b.end());
+        dst.norms_a.insert(dst.norms_a.end(), src.norms_a.begin(), src.norms_a.end());
+        dst.norms_b.insert(dst.norms_b.end(), src.norms_b.begin(), src.norms_b.end());
+        dst.mat_base.insert(dst.mat_base.end(), src.n_pairs, mat_base);
+        dst.mat_n.insert(dst.mat_n.end(), src.n_pairs, mat_n);
+        dst.n_pairs = dst.ao_a.size();
+        dst.n_ppairs = dst.pofs.back();
+    }
+
     PairClass buildSingleClass(int l, const std::vector<Shell> &s)
     {
         PairClass pc;

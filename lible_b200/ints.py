@@ -272,27 +272,103 @@ class ERI2D1Kernel(ERI2Kernel):
     _fn, _nblk = "lible_gpu_eri2d1_batch", 6
 
 
-def _opts(schwarz, precision, fp32_threshold):
-    return JKOpts(float(schwarz), float(fp32_threshold), 1 if precision in (1, "mixed") else 0)
+class Batch:
+    """A batch of molecules whose J/K are built together (no reference counterpart).
+
+    `molecules` is a list of (basis name, atomic numbers, coordinates).  D, J and K are packed 1-D
+    arrays of `packed` elements: molecule m's N_m x N_m matrix starts at `base[m]` (see pack() and
+    unpack()).  Every quartet class of every molecule goes through one work-queue launch per class;
+    jk(batch, D, use_graph=True) replays the whole build as one CUDA graph."""
+
+    def __init__(self, molecules, *, units="bohr", basis_root=None, device=0):
+        self._lib = load()
+        ctx = ctypes.c_void_p()
+        check(None, self._lib.lible_gpu_create(device, ctypes.byref(ctx)))
+        self._ctx = ctx
+        names = [m[0].encode() for m in molecules]
+        arr = (ctypes.c_char_p * len(names))(*names)
+        n_atoms = _i32([len(m[1]) for m in molecules])
+        Z = _i32(np.concatenate([np.asarray(m[1], dtype=np.int32) for m in molecules]))
+        xyz = _f64(np.vstack([np.asarray(m[2], dtype=float).reshape(-1, 3) for m in molecules]))
+        u = 0 if units == "angstrom" else 1
+        check(ctx, self._lib.lible_gpu_set_batch(ctx, len(molecules), (basis_root or BASIS_ROOT).encode(),
+                                                 ctypes.cast(arr, ctypes.c_void_p), _ptr(n_atoms), _ptr(Z),
+                                                 _ptr(xyz), u))
+        nm = ctypes.c_int()
+        nao = np.zeros(len(molecules), np.int64)
+        base = np.zeros(len(molecules), np.int64)
+        packed = ctypes.c_longlong()
+        check(ctx, self._lib.lible_gpu_batch_layout(ctx, ctypes.byref(nm), _ptr(nao), _ptr(base), ctypes.byref(packed)))
+        self.nao, self.base, self.packed = nao, base, packed.value
+        self.n_molecules = nm.value
+
+    def __del__(self):
+        ctx = getattr(self, "_ctx", None)
+        if ctx is not None and ctx.value:
+            self._lib.lible_gpu_destroy(ctx)
+            self._ctx = None
+
+    @property
+    def ctx(self):
+        return self._ctx
+
+    def pack(self, mats):
+        """Packs per-molecule N_m x N_m matrices into one array."""
+        out = np.empty(self.packed)
+        for m, M in enumerate(mats):
+            n = self.nao[m]
+            out[self.base[m]:self.base[m] + n * n] = np.asarray(M, dtype=float).reshape(-1)
+        return out
+
+    def unpack(self, arr):
+        """Splits a packed array (numpy or torch) into per-molecule N_m x N_m views."""
+        return [arr[self.base[m]:self.base[m] + self.nao[m] ** 2].reshape(int(self.nao[m]), int(self.nao[m]))
+                for m in range(self.n_molecules)]
 
 
-def jk(structure, D, schwarz=1e-12, precision="fp64", fp32_threshold=1e-4, J=None, K=None):
-    """Direct Coulomb and exchange matrices for a symmetric density D (N x N)."""
-    n = structure.nao
+def _opts(schwarz, precision, fp32_threshold, use_graph=False):
+    return JKOpts(float(schwarz), float(fp32_threshold), 1 if precision in (1, "mixed") else 0, 1 if use_graph else 0)
+
+
+def _jk_shape(structure):
+    return (structure.packed,) if isinstance(structure, Batch) else (structure.nao, structure.nao)
+
+
+def jk(structure, D, schwarz=1e-12, precision="fp64", fp32_threshold=1e-4, J=None, K=None, use_graph=False):
+    """Direct Coulomb and exchange matrices for a symmetric density D (N x N, or packed for a Batch).
+    With use_graph the launch sequence is captured once per (plan, D, J, K) and replayed."""
     Dh = D if hasattr(D, "data_ptr") else _f64(D)
-    J = np.empty((n, n)) if J is None else J
-    K = np.empty((n, n)) if K is None else K
+    J = np.empty(_jk_shape(structure)) if J is None else J
+    K = np.empty(_jk_shape(structure)) if K is None else K
     st = JKStats()
-    opts = _opts(schwarz, precision, fp32_threshold)
+    opts = _opts(schwarz, precision, fp32_threshold, use_graph)
     _call(structure, "lible_gpu_jk", _ptr(Dh), _ptr(J), _ptr(K), ctypes.byref(opts), ctypes.byref(st))
     return J, K, {"n_quartets": st.n_quartets, "n_fp32": st.n_fp32, "n_launches": st.n_launches}
+
+
+def jk_autotune(structure, D, schwarz=1e-12, precision="fp64", fp32_threshold=1e-4, cache=None, J=None, K=None):
+    """Autotunes the class launches of the J/K plan on D (J and K are overwritten); returns the
+    per-class summary.  With `cache`, the choices are appended to that file."""
+    Dh = D if hasattr(D, "data_ptr") else _f64(D)
+    J = np.empty(_jk_shape(structure)) if J is None else J
+    K = np.empty(_jk_shape(structure)) if K is None else K
+    buf = ctypes.create_string_buffer(1 << 16)
+    opts = _opts(schwarz, precision, fp32_threshold)
+    _call(structure, "lible_gpu_jk_autotune", _ptr(Dh), _ptr(J), _ptr(K), ctypes.byref(opts),
+          cache.encode() if cache else None, buf, len(buf))
+    return buf.value.decode()
+
+
+def set_tune_cache(structure, path):
+    """Later J/K plans of this structure start from the autotune cache at `path`."""
+    _call(structure, "lible_gpu_set_tune_cache", path.encode() if path else None)
 
 
 def jk_energy_forward(structure, D, schwarz=1e-12, precision="fp64", fp32_threshold=1e-4):
     """E = 1/2 Tr(DJ) - 1/4 Tr(DK)."""
     e = ctypes.c_double()
     opts = _opts(schwarz, precision, fp32_threshold)
-    Dh = D if hasattr(D, "data_ptr") else _f64(D)
+    Dh = D if hasattr(D, "data_ptr") else _f64(D)  # N x N, or packed for a Batch
     _call(structure, "lible_gpu_jk_energy_forward", _ptr(Dh), ctypes.byref(opts), ctypes.byref(e), None, None)
     return e.value
 

@@ -45,3 +45,18 @@ def even_tempered_aux(Z, lmax=3, n_exp=12, base=0.1, ratio=2.5):
     """Per-atom auxiliary basis of uncontracted shells l = 0..lmax with exponents base*ratio^k."""
     shells = [(l, [base * ratio ** k], [1.0]) for l in range(lmax + 1) for k in range(n_exp)]
     return [list(shells) for _ in Z]
+
+
+def batch_clusters(n_mol=64, seed=7, n_max=12):
+    """The heterogeneous batch: n_mol water clusters with n drawn uniformly from 1..n_max, even
+    index cc-pVDZ and odd index cc-pVTZ; each cluster and its density (occupation 5n) come from
+    their own generator seeded with (seed, index).  Returns [(basis, Z, xyz, D_factory)], where
+    D_factory(nao) draws the density."""
+    rng = np.random.default_rng(seed)
+    sizes = rng.integers(1, n_max + 1, size=n_mol)
+    out = []
+    for i, n in enumerate(sizes):
+        Z, xyz, r = water_cluster(int(n), seed * 1000 + i)
+        basis = "cc-pvdz" if i % 2 == 0 else "cc-pvtz"
+        out.append((basis, Z, xyz, (lambda nao, r=r, n=int(n): random_density(nao, 5 * n, r))))
+    return out
