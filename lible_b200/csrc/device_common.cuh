@@ -69,6 +69,12 @@ namespace lible_b200
         long long n_chunks;
         unsigned long long *counter;
         int grid_div;                     // persistent grid: resident blocks per SM / grid_div
+        // bra-side structure-of-arrays copies indexed by the task's minor (Schwarz) position
+        // (implicit ket-major enumeration only; null = read the per-pair records)
+        const uint4 *bra_soa;
+        const double *bra_pPs;
+        const double *bra_Es;
+        const float *bra_Efs;
         // epilogue
         int mode;
         int flags;                        // kStore: bit0 swap bra shells, bit1 swap ket shells, bit2 swap bra/ket
@@ -125,19 +131,23 @@ namespace lible_b200
         return lo;
     }
 
-    // Task t decoded with a known major position (implicit enumeration only).
-    __device__ __forceinline__ void decodeAt(const QuartetArgs &a, long long t, int lo, uint32_t &ib, uint32_t &ik)
+    // Task t decoded with a known major position (implicit enumeration only); `pos` receives the
+    // minor (Schwarz) position.
+    __device__ __forceinline__ void decodeAt(const QuartetArgs &a, long long t, int lo, uint32_t &ib, uint32_t &ik,
+                                             uint32_t &pos)
     {
         const uint32_t maj = __ldg(a.major_order + lo);
-        const uint32_t mnr = __ldg(a.minor_order + __ldg(a.minor_begin + lo) +
-                                   (uint32_t)((unsigned long long)t - __ldg(a.prefix + lo)));
+        pos = __ldg(a.minor_begin + lo) + (uint32_t)((unsigned long long)t - __ldg(a.prefix + lo));
+        const uint32_t mnr = __ldg(a.minor_order + pos);
         ib = a.major_ket ? mnr : maj;
         ik = a.major_ket ? maj : mnr;
     }
 
     // Cursor-based decode: explicit lists index directly; implicit ones advance `cur`.
-    __device__ __forceinline__ void decodeCursor(const QuartetArgs &a, long long t, int &cur, uint32_t &ib, uint32_t &ik)
+    __device__ __forceinline__ void decodeCursor(const QuartetArgs &a, long long t, int &cur, uint32_t &ib, uint32_t &ik,
+                                                 uint32_t &pos)
     {
+        pos = 0;
         if (a.list)
         {
             ib = a.list[2 * t];
@@ -145,7 +155,12 @@ namespace lible_b200
             return;
         }
         cur = advanceMajor(a, t, cur);
-        decodeAt(a, t, cur, ib, ik);
+        decodeAt(a, t, cur, ib, ik, pos);
+    }
+    __device__ __forceinline__ void decodeCursor(const QuartetArgs &a, long long t, int &cur, uint32_t &ib, uint32_t &ik)
+    {
+        uint32_t pos;
+        decodeCursor(a, t, cur, ib, ik, pos);
     }
 
     __device__ __forceinline__ void decodeTask(const QuartetArgs &a, long long t, uint32_t &ib, uint32_t &ik)

@@ -257,6 +257,32 @@ namespace lible_b200
         }
     }
 
+    // Builds the bra-side structure-of-arrays copies of one class in Schwarz order (layout in
+    // DevPairClass): block-strided over positions, threads over (primitive, field).
+    __global__ void soaGatherKernel(const double *E, const float *Ef, const double *pP, const uint32_t *pofs,
+                                    const uint32_t *order, const uint4 *soa, long long n_pos, int sabhab, double *Es,
+                                    float *Efs, double *pPs)
+    {
+        for (long long j = blockIdx.x; j < n_pos; j += gridDim.x)
+        {
+            const uint32_t pair = order[j], p0 = pofs[pair], K = pofs[pair + 1] - p0;
+            const uint4 sv = soa[j];
+            const size_t n = sv.z;
+            for (int idx = threadIdx.x; idx < (int)K * sabhab; idx += blockDim.x)
+            {
+                const size_t src = (size_t)p0 * sabhab + idx;
+                Es[sv.y + (size_t)idx * n] = E[src];
+                if (Efs)
+                    Efs[sv.y + (size_t)idx * n] = Ef[src];
+            }
+            for (int idx = threadIdx.x; idx < (int)K * 5; idx += blockDim.x)
+            {
+                const int k = idx / 5, f = idx % 5;
+                pPs[sv.x + (size_t)idx * n] = pP[8 * ((size_t)p0 + k) + (f < 4 ? f : 4)];
+            }
+        }
+    }
+
     // A_m <- A_m + A_m^T for every packed block m = blockIdx.y (blocks[2m] = first element,
     // blocks[2m+1] = N_m).
     __global__ void symmetrizeBlocksKernel(double *A, const long long *blocks)
@@ -408,7 +434,8 @@ namespace lible_b200
         for (auto &d : cs.dev)
             for (void *p : {(void *)d.pP, (void *)d.ab, (void *)d.pofs, (void *)d.info, (void *)d.coords,
                             (void *)d.E, (void *)d.Et, (void *)d.Ef, (void *)d.Etf, (void *)d.E1,
-                            (void *)d.E1t, (void *)d.Q})
+                            (void *)d.E1t, (void *)d.Q, (void *)d.pPs, (void *)d.Es, (void *)d.Efs,
+                            (void *)d.soa})
                 cudaFree(p);
         for (auto &o : cs.orders)
             cudaFree(o.d_order);
@@ -1073,6 +1100,31 @@ namespace lible_b200
                 o.groups.back().end = (uint32_t)i + 1;
             }
             o.d_order = devUpload(o.order, stream_);
+            // bra-side structure-of-arrays copies in this order
+            const int sabhab = nsph(d.la) * nsph(d.lb) * nherm(d.la + d.lb);
+            std::vector<uint4> soa(Q.size());
+            size_t base_p = 0, base_e = 0;
+            for (const auto &g : o.groups)
+            {
+                const uint32_t ng = g.end - g.start;
+                for (uint32_t i = 0; i < ng; i++)
+                    soa[g.start + i] = make_uint4((unsigned)(base_p + i), (unsigned)(base_e + i), ng, 0);
+                base_p += (size_t)g.k * 5 * ng;
+                base_e += (size_t)g.k * sabhab * ng;
+            }
+            if (base_e >= (1ULL << 32) || base_p >= (1ULL << 32))
+                throw EngineError(kStatusInvalid, "pair class too large for 32-bit structure-of-arrays offsets");
+            if (!soa.empty())
+            {
+                d.soa = devUpload(soa, stream_);
+                d.pPs = devAlloc<double>(std::max<size_t>(base_p, 1));
+                d.Es = devAlloc<double>(std::max<size_t>(base_e, 1));
+                if (d.Ef)
+                    d.Efs = devAlloc<float>(std::max<size_t>(base_e, 1));
+                soaGatherKernel<<<(unsigned)std::min<size_t>(soa.size(), 65535), 128, 0, stream_>>>(
+                    d.E, d.Ef, d.pP, d.pofs, o.d_order, d.soa, (long long)soa.size(), sabhab, d.Es, d.Efs, d.pPs);
+                cudaCheck(cudaGetLastError(), "soaGatherKernel");
+            }
         }
         cudaCheck(cudaStreamSynchronize(stream_), "schwarz");
         cs.schwarz_done = true;
@@ -1356,6 +1408,10 @@ namespace lible_b200
             a.n_chunks = cp.n_chunks64;
             a.counter = plan.counters + 2 * ip;
             a.grid_div = cp.grid_div64;
+            a.bra_soa = B.soa;
+            a.bra_pPs = B.pPs;
+            a.bra_Es = B.Es;
+            a.bra_Efs = B.Efs;
             LaunchFn f64 = lookupFwd64(cp.tb, cp.tk);
             if (!f64)
                 throw EngineError(kStatusUnsupported, "quartet class not instantiated");
@@ -1586,6 +1642,10 @@ namespace lible_b200
                         a.n_chunks = fp32 ? cp.n_chunks32 : cp.n_chunks64;
                         a.counter = plan.counters + 2 * ip + fp32;
                         a.grid_div = gd;
+                        a.bra_soa = B.soa;
+                        a.bra_pPs = B.pPs;
+                        a.bra_Es = B.Es;
+                        a.bra_Efs = B.Efs;
                         float t_min = 1e30f;
                         for (int rep = 0; rep < 2; rep++)
                         {
@@ -1747,6 +1807,10 @@ namespace lible_b200
             a.J = J_dev;
             a.nao = (int)n;
             LaunchFn fn = lookupFwd64(pairType(B.la, B.lb), pairType(K.la, K.lb));
+            a.bra_soa = B.soa;
+            a.bra_pPs = B.pPs;
+            a.bra_Es = B.Es;
+            a.bra_Efs = B.Efs;
             a.chunks = cp.chunks64;
             a.n_chunks = cp.n_chunks64;
             if (gamma_dev)

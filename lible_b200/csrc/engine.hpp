@@ -7,6 +7,8 @@
 
 #include "lible_math.hpp"
 
+#include <vector_types.h>
+
 #include <array>
 #include <cstdint>
 #include <memory>
@@ -109,5 +111,13 @@ namespace lible_b200
         double *E1t = nullptr;      // [n_ppairs][3][H_ab][S_ab]
         double *Q = nullptr;        // [n_pairs] Schwarz factors
         std::vector<double> Qh;     // host copy
+        // Bra-side copies in Schwarz order, structure of arrays per (molecule, K) group g of n_g
+        // pairs: element (prim k, field f) of the pair at group offset i sits at
+        // base_g + (k * F + f) * n_g + i, so lanes holding consecutive Schwarz positions read
+        // consecutive words.  soa[position] = (pP base + i, E base + i, n_g, 0).
+        double *pPs = nullptr;      // F = 5: p, Px, Py, Pz, 1/p
+        double *Es = nullptr;       // F = S_ab H_ab
+        float *Efs = nullptr;
+        uint4 *soa = nullptr;
     };
 }

@@ -269,9 +269,17 @@ namespace lible_b200
     // columns [c0, c0 + CW) of the batch (c0 = member * CW).  Each thread evaluates the Boys
     // function and the R vector itself, so the group never synchronises; every index into R, the
     // R.E accumulator and the batch is a compile-time constant.
+    template <typename T>
+    __device__ __forceinline__ const T *braEs(const QuartetArgs &a);
+    template <>
+    __device__ __forceinline__ const double *braEs<double>(const QuartetArgs &a) { return a.bra_Es; }
+    template <>
+    __device__ __forceinline__ const float *braEs<float>(const QuartetArgs &a) { return a.bra_Efs; }
+
+    // `sv` is the bra's structure-of-arrays entry (sv.z = 0: read the per-pair records instead).
     template <int LA, int LB, int LC, int LD, typename T>
     __device__ __forceinline__ void quartetThread(const QuartetArgs &a, uint32_t ib, uint32_t ik, int c0, T *V,
-                                                  const T *btab)
+                                                  const T *btab, uint4 sv)
     {
         using C = Cls<LA, LB, LC, LD>;
         constexpr int CW = Shape<LA, LB, LC, LD, T>::CW;
@@ -282,9 +290,17 @@ namespace lible_b200
         const uint32_t q0 = a.ket.pofs[ik], q1 = a.ket.pofs[ik + 1];
         const T *Eb = braE<T>(a.bra);
         const T *Ek = ketE<T>(a.ket) + c0;
+        const size_t sn = sv.z;
         for (uint32_t p = p0; p < p1; p++)
         {
-            const PQ4 P = loadPQ(a.bra.pP, p);
+            PQ4 P;
+            if (sn)
+            {
+                const double *pp = a.bra_pPs + sv.x + (size_t)(p - p0) * 5 * sn;
+                P = {__ldg(pp), __ldg(pp + sn), __ldg(pp + 2 * sn), __ldg(pp + 3 * sn), __ldg(pp + 4 * sn)};
+            }
+            else
+                P = loadPQ(a.bra.pP, p);
             T RxE[C::HAB * CW];
 #pragma unroll
             for (int x = 0; x < C::HAB * CW; x++)
@@ -345,13 +361,15 @@ namespace lible_b200
                             }
                 }
             }
-            const T *eb = Eb + (size_t)p * C::SAB * C::HAB;
+            const T *eb = sn ? braEs<T>(a) + sv.y + (size_t)(p - p0) * C::SAB * C::HAB * sn
+                             : Eb + (size_t)p * C::SAB * C::HAB;
+            const size_t es = sn ? sn : 1;
 #pragma unroll
             for (int m = 0; m < C::SAB; m++)
 #pragma unroll
                 for (int h = 0; h < C::HAB; h++)
                 {
-                    const T e = eb[m * C::HAB + h];
+                    const T e = __ldg(eb + (m * C::HAB + h) * es);
 #pragma unroll
                     for (int c = 0; c < CW; c++)
                         V[m * CW + c] += e * RxE[h * CW + c];
@@ -574,8 +592,10 @@ namespace lible_b200
                 if (valid)
                 {
                     int my = cur;
-                    decodeCursor(a, t, my, ib, ik);
-                    quartetThread<LA, LB, LC, LD, T>(a, ib, ik, member * CW, V, btab);
+                    uint32_t pos;
+                    decodeCursor(a, t, my, ib, ik, pos);
+                    const uint4 sv = a.bra_soa ? __ldg(a.bra_soa + pos) : make_uint4(0, 0, 0, 0);
+                    quartetThread<LA, LB, LC, LD, T>(a, ib, ik, member * CW, V, btab, sv);
                 }
                 if (!a.list)
                     cur = advanceMajor(a, base + QPW < end ? base + QPW : end - 1, cur);
