@@ -29,6 +29,22 @@ namespace lible_b200
         return 0;
     }
 
+    // Shared-memory pitches (in doubles) of the DMMA operand tiles.  Fragments read either 4 rows x 8
+    // consecutive elements (k-major: R, E_ket, R.E) or 8 rows x 4 (m-major: E_bra); a pitch of 8
+    // (resp. 4) modulo 16 spreads those rows over all 32 banks.
+    constexpr int kPitch(int x)
+    {
+        const int p = (x + 7) / 8 * 8;
+        return p % 16 == 0 ? p + 8 : p;
+    }
+    constexpr int mPitch(int x)
+    {
+        int p = (x + 3) / 4 * 4;
+        while (p % 16 != 4)
+            p += 4;
+        return p;
+    }
+
     template <int LA, int LB, int LC, int LD, typename T>
     struct Shape
     {
@@ -37,7 +53,25 @@ namespace lible_b200
         static constexpr int GT = pickRegGroup(C::SAB, C::SCD, C::HAB, C::NR);
         static constexpr int CW = GT ? C::SCD / GT : 0;
         static constexpr int QPW = GT ? 32 / GT : 0;           // quartets per warp
+        // group path in FP64: both contractions on the DMMA pipe (mma.m8n8k4.f64) in 8x8 tiles of
+        // R.E_ket^T [H_ab x S_cd] (K = H_cd) and of the batch [S_ab x S_cd] (K = H_ab)
+        static constexpr bool MMA = GT == 0 && sizeof(T) == 8;
+        static constexpr int MT = (C::HAB + 7) / 8, NT = (C::SCD + 7) / 8, KT = (C::HCD + 3) / 4;
+        static constexpr int MT2 = (C::SAB + 7) / 8, KT2 = (C::HAB + 3) / 4;
+        static constexpr int TILES = MT * NT, TILES2 = MT2 * NT;
+        static constexpr int WM = (TILES + 5) / 6 < 1 ? 1 : ((TILES + 5) / 6 > 8 ? 8 : (TILES + 5) / 6);
+        static constexpr int TPW = (TILES + WM - 1) / WM, TPW2 = (TILES2 + WM - 1) / WM;
+        static constexpr int P_RM = kPitch(C::HAB), P_EC = kPitch(C::SCD), P_EA = mPitch(C::HAB);
+        static constexpr size_t m_off_rb = 0;                                            // 2 x NR
+        static constexpr size_t m_off_rm = m_off_rb + 8 * 2 * C::NR;                     // KT*4 x P_RM
+        static constexpr size_t m_off_ec = m_off_rm + 8 * (size_t)KT * 4 * P_RM;         // KT*4 x P_EC
+        static constexpr size_t m_off_ea = m_off_ec + 8 * (size_t)KT * 4 * P_EC;         // MT2*8 x P_EA
+        static constexpr size_t m_off_rx = m_off_ea + 8 * (size_t)MT2 * 8 * P_EA;        // MT*8 x P_EC
+        static constexpr size_t m_off_ix = m_off_rx + 8 * (size_t)MT * 8 * P_EC;         // HCD x HAB int16
+        static constexpr size_t m_off_ht = (m_off_ix + 2 * C::HCD * C::HAB + 15) / 16 * 16; // NR char4
+        static constexpr size_t m_smem = m_off_ht + 4 * C::NR;
         static constexpr int W = GT ? 0
+                                 : MMA ? WM
                                  : ((C::HAB * C::SCD + C::SAB * C::SCD) <= 64 * 32)     ? 1
                                  : ((C::HAB * C::SCD + C::SAB * C::SCD) <= 64 * 64)     ? 2
                                  : ((C::HAB * C::SCD + C::SAB * C::SCD) <= 64 * 128)    ? 4
@@ -60,8 +94,18 @@ namespace lible_b200
         static constexpr size_t off_rx = off_ea + sizeof(T) * C::SAB * C::HAB;      // HAB x SCD
         static constexpr size_t off_ix = off_rx + sizeof(T) * C::HAB * C::SCD;      // HCD x HAB int16
         static constexpr size_t off_ht = (off_ix + 2 * C::HCD * C::HAB + 15) / 16 * 16; // NR char4
-        static constexpr size_t smem = W == 0 ? off_boys + boys_bytes : off_ht + 4 * C::NR;
+        static constexpr size_t smem = W == 0 ? off_boys + boys_bytes : MMA ? m_smem : off_ht + 4 * C::NR;
+        static_assert(!MMA || m_smem <= 227 * 1024, "DMMA shared-memory layout exceeds 227 KB");
     };
+
+    // D += A B for one 8x8x4 FP64 tile (PTX mma.sync.aligned.m8n8k4.row.col.f64): lane l holds
+    // A[l/4][l%4], B[l%4][l/4] and D[l/4][2(l%4) + {0,1}].
+    __device__ __forceinline__ void dmma8x8x4(double &d0, double &d1, double a, double b)
+    {
+        asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+                     : "+d"(d0), "+d"(d1)
+                     : "d"(a), "d"(b));
+    }
 
     __device__ __forceinline__ void groupSync(int G)
     {
@@ -524,6 +568,197 @@ namespace lible_b200
         }
     }
 
+    // ---------------------------------------------------------------------------------------
+    // FP64 group path on the DMMA pipe.  Per primitive quartet the block builds R (recursion in
+    // shared memory), writes the signed R matrix rm[h'][h] and stages E_ket[q] ec[h'][c], both into
+    // zero-padded tiles; every warp then accumulates its 8x8 tiles of R.E_ket^T over the ket
+    // primitives in registers (acc).  Per bra primitive the R.E tiles go to shared memory and the
+    // warps accumulate their 8x8 tiles of E_bra . (R.E) into `v`.  Padded rows and columns of the
+    // operand tiles are zeroed once per block and never written afterwards.
+    template <int LA, int LB, int LC, int LD>
+    __device__ __forceinline__ void quartetGroupMMA(const QuartetArgs &a, uint32_t ib, uint32_t ik,
+                                                    unsigned char *smem, double (&v)[Shape<LA, LB, LC, LD, double>::TPW2][2])
+    {
+        using C = Cls<LA, LB, LC, LD>;
+        using S = Shape<LA, LB, LC, LD, double>;
+        constexpr int G = S::G;
+        const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, r8 = lane >> 2, k4 = lane & 3;
+        double *rb = reinterpret_cast<double *>(smem + S::m_off_rb);
+        double *rm = reinterpret_cast<double *>(smem + S::m_off_rm);
+        double *ec = reinterpret_cast<double *>(smem + S::m_off_ec);
+        double *ea = reinterpret_cast<double *>(smem + S::m_off_ea);
+        double *rx = reinterpret_cast<double *>(smem + S::m_off_rx);
+        const short *rix = reinterpret_cast<const short *>(smem + S::m_off_ix);
+        const char4 *ht = reinterpret_cast<const char4 *>(smem + S::m_off_ht);
+
+#pragma unroll
+        for (int i = 0; i < S::TPW2; i++)
+            v[i][0] = v[i][1] = 0.0;
+        const uint32_t p0 = a.bra.pofs[ib], p1 = a.bra.pofs[ib + 1];
+        const uint32_t q0 = a.ket.pofs[ik], q1 = a.ket.pofs[ik + 1];
+        for (uint32_t p = p0; p < p1; p++)
+        {
+            const PQ4 P = loadPQ(a.bra.pP, p);
+            for (int e = tid; e < C::SAB * C::HAB; e += G)
+                ea[(e / C::HAB) * S::P_EA + e % C::HAB] = __ldg(a.bra.E + (size_t)p * C::SAB * C::HAB + e);
+            double acc[S::TPW][2];
+#pragma unroll
+            for (int i = 0; i < S::TPW; i++)
+                acc[i][0] = acc[i][1] = 0.0;
+            for (uint32_t q = q0; q < q1; q++)
+            {
+                const PQ4 Q = loadPQ(a.ket.pP, q);
+                const double rs = rsqrt(P.x + Q.x);
+                const double alpha = P.x * Q.x * (rs * rs);
+                const double X = P.y - Q.y, Y = P.z - Q.z, Z = P.w - Q.w;
+                const double fac = 34.986836655249725 * rs * P.ip * Q.ip;
+                double F[C::L + 1];
+                boysF<C::L, false>(alpha * (X * X + Y * Y + Z * Z), a.boys + C::L * kBoysTerms * kBoysPitch, F);
+                const double m2a = -2.0 * alpha;
+                double *cur = rb, *nxt = rb + C::NR;
+                double pw = 1.0;
+                for (int k = 0; k < C::L; k++)
+                    pw *= m2a;
+                if (tid == 0)
+                    cur[0] = F[C::L] * fac * pw;
+                groupSync(G);
+                // levels unrolled (L is a compile-time constant) so F[n] stays in registers
+#pragma unroll
+                for (int n = C::L - 1; n >= 0; n--)
+                {
+                    const int cnt = nherm(C::L - n);
+                    for (int e = tid; e < cnt; e += G)
+                    {
+                        double r;
+                        if (e == 0)
+                        {
+                            double pn = 1.0;
+                            for (int k = 0; k < n; k++)
+                                pn *= m2a;
+                            r = F[n] * fac * pn;
+                        }
+                        else
+                        {
+                            const char4 tv = ht[e];
+                            const int t = tv.x, u = tv.y, vv = tv.z, m = tv.w;
+                            if (t > 0)
+                            {
+                                r = X * cur[nherm(m - 2) + cartIndex(u, vv)];
+                                if (t > 1)
+                                    r += (t - 1) * cur[nherm(m - 3) + cartIndex(u, vv)];
+                            }
+                            else if (u > 0)
+                            {
+                                r = Y * cur[nherm(m - 2) + cartIndex(u - 1, vv)];
+                                if (u > 1)
+                                    r += (u - 1) * cur[nherm(m - 3) + cartIndex(u - 2, vv)];
+                            }
+                            else
+                            {
+                                r = Z * cur[nherm(m - 2) + cartIndex(0, vv - 1)];
+                                if (vv > 1)
+                                    r += (vv - 1) * cur[nherm(m - 3) + cartIndex(0, vv - 2)];
+                            }
+                        }
+                        nxt[e] = r;
+                    }
+                    groupSync(G);
+                    double *tmp = cur;
+                    cur = nxt;
+                    nxt = tmp;
+                }
+                // signed R matrix rm[h'][h] and the staged ket E[q] ec[h'][c]
+                for (int e = tid; e < C::HCD * C::HAB; e += G)
+                {
+                    const short ix = rix[e];
+                    const double r = cur[ix & 0x7fff];
+                    rm[(e / C::HAB) * S::P_RM + e % C::HAB] = (ix & 0x8000) ? -r : r;
+                }
+                for (int e = tid; e < C::HCD * C::SCD; e += G)
+                    ec[(e / C::SCD) * S::P_EC + e % C::SCD] = __ldg(a.ket.Et + (size_t)q * C::HCD * C::SCD + e);
+                groupSync(G);
+                // acc[tile] += R^T[h][h'] E_ket[h'][c] over h' (A = rm viewed transposed, row-major)
+#pragma unroll
+                for (int i = 0; i < S::TPW; i++)
+                {
+                    const int t = warp + i * S::WM;
+                    if (t < S::TILES)
+                    {
+                        const int mt = t / S::NT, nt = t % S::NT;
+                        const double *A = rm + k4 * S::P_RM + mt * 8 + r8;
+                        const double *B = ec + k4 * S::P_EC + nt * 8 + r8;
+#pragma unroll 4
+                        for (int ks = 0; ks < S::KT; ks++)
+                            dmma8x8x4(acc[i][0], acc[i][1], A[ks * 4 * S::P_RM], B[ks * 4 * S::P_EC]);
+                    }
+                }
+                groupSync(G);
+            }
+            // R.E tiles to shared memory (rows h, columns c; padded entries are zero)
+#pragma unroll
+            for (int i = 0; i < S::TPW; i++)
+            {
+                const int t = warp + i * S::WM;
+                if (t < S::TILES)
+                {
+                    const int mt = t / S::NT, nt = t % S::NT;
+                    double *o = rx + (mt * 8 + r8) * S::P_EC + nt * 8 + 2 * k4;
+                    o[0] = acc[i][0];
+                    o[1] = acc[i][1];
+                }
+            }
+            groupSync(G);
+            // v[tile] += E_bra[m][h] (R.E)[h][c] over h
+#pragma unroll
+            for (int i = 0; i < S::TPW2; i++)
+            {
+                const int t = warp + i * S::WM;
+                if (t < S::TILES2)
+                {
+                    const int mt = t / S::NT, nt = t % S::NT;
+                    const double *A = ea + (mt * 8 + r8) * S::P_EA + k4;
+                    const double *B = rx + k4 * S::P_EC + nt * 8 + r8;
+#pragma unroll 4
+                    for (int ks = 0; ks < S::KT2; ks++)
+                        dmma8x8x4(v[i][0], v[i][1], A[ks * 4], B[ks * 4 * S::P_EC]);
+                }
+            }
+            groupSync(G);
+        }
+    }
+
+    // Tables and zero padding of the DMMA layout (once per block).
+    template <int LA, int LB, int LC, int LD>
+    __device__ __forceinline__ void buildGroupTablesMMA(unsigned char *smem)
+    {
+        using C = Cls<LA, LB, LC, LD>;
+        using S = Shape<LA, LB, LC, LD, double>;
+        double *z = reinterpret_cast<double *>(smem + S::m_off_rm);
+        const int nz = (int)((S::m_off_ix - S::m_off_rm) / 8);
+        for (int e = threadIdx.x; e < nz; e += blockDim.x)
+            z[e] = 0.0;
+        short *rix = reinterpret_cast<short *>(smem + S::m_off_ix);
+        char4 *ht = reinterpret_cast<char4 *>(smem + S::m_off_ht);
+        for (int e = threadIdx.x; e < C::NR; e += blockDim.x)
+        {
+            int t, u, v;
+            hermTuv(e, t, u, v);
+            ht[e] = make_char4((char)t, (char)u, (char)v, (char)(t + u + v));
+        }
+        for (int e = threadIdx.x; e < C::HCD * C::HAB; e += blockDim.x)
+        {
+            const int hp = e / C::HAB, h = e % C::HAB;
+            int t, u, v, tp, up, vp;
+            hermTuv(h, t, u, v);
+            hermTuv(hp, tp, up, vp);
+            int ix = hermIndex(t + tp, u + up, v + vp);
+            if ((tp + up + vp) & 1)
+                ix |= 0x8000;
+            rix[e] = (short)ix;
+        }
+        __syncthreads();
+    }
+
     // Builds the per-block tables of the group shape: Hermite (t,u,v,order) list and the signed
     // combined index of (h + h') for the R matrix.
     template <int LA, int LB, int LC, int LD, typename T>
@@ -681,6 +916,83 @@ namespace lible_b200
                 const long long n_chunks = (a.n_tasks + CH - 1) / CH;
                 for (long long chunk = gw; chunk < n_chunks; chunk += warps)
                     processRange(chunk * CH, (chunk + 1) * CH < a.n_tasks ? (chunk + 1) * CH : a.n_tasks);
+            }
+        }
+        else if constexpr (S::MMA)
+        {
+            extern __shared__ __align__(16) unsigned char smem[];
+            buildGroupTablesMMA<LA, LB, LC, LD>(smem);
+            double *vs = reinterpret_cast<double *>(smem + S::m_off_rx);
+            const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, r8 = lane >> 2, k4 = lane & 3;
+            // one quartet at a time for the whole block, tasks [start, end) of a chunk
+            auto processRange = [&](long long start, long long end) {
+            int cur = 0;
+            for (long long t = start; t < end; t++)
+            {
+                uint32_t ib, ik;
+                decodeCursor(a, t, cur, ib, ik);
+                double v[S::TPW2][2];
+                quartetGroupMMA<LA, LB, LC, LD>(a, ib, ik, smem, v);
+                // element (m, c) of the batch held by this thread: tile rows / columns
+#pragma unroll
+                for (int i = 0; i < S::TPW2; i++)
+                {
+                    const int tt = warp + i * S::WM;
+                    if (tt < S::TILES2)
+                    {
+                        const int m = (tt / S::NT) * 8 + r8;
+#pragma unroll
+                        for (int j = 0; j < 2; j++)
+                        {
+                            const int c = (tt % S::NT) * 8 + 2 * k4 + j;
+                            if (m < C::SAB && c < C::SCD)
+                            {
+                                if (a.mode == kStore)
+                                    a.out[(size_t)t * blk + storeIndex<C::SA, C::SB, C::SC, C::SD>(
+                                                                a.flags, m / C::SB, m % C::SB, c / C::SD, c % C::SD)] =
+                                        v[i][j];
+                                else
+                                    vs[m * C::SCD + c] = v[i][j];
+                            }
+                        }
+                    }
+                }
+                if (a.mode != kStore)
+                {
+                    __syncthreads();
+                    const int32_t *bi = a.bra.info + 8 * ib;
+                    const int32_t *ki = a.ket.info + 8 * ik;
+                    auto val = [&](int e) { return vs[e]; };
+                    if (a.mode == kJK)
+                        digestJK<C::SA, C::SB, C::SC, C::SD, false>(a, quartetWeight(a, ib, ik), bi, ki, val,
+                                                                    threadIdx.x, S::G);
+                    else
+                        digestRI<C::SA, C::SB, C::SC, C::SD, false>(a, bi, ki, val, threadIdx.x, S::G);
+                }
+                __syncthreads();
+            }
+            };
+            if (a.chunks)
+            {
+                __shared__ unsigned long long claimed;
+                for (;;)
+                {
+                    if (threadIdx.x == 0)
+                        claimed = atomicAdd(a.counter, 1ULL);
+                    __syncthreads();
+                    const unsigned long long c = claimed;
+                    __syncthreads();
+                    if (c >= (unsigned long long)a.n_chunks)
+                        break;
+                    processRange((long long)__ldg(a.chunks + c), (long long)__ldg(a.chunks + c + 1));
+                }
+            }
+            else
+            {
+                constexpr long long CHB = 8;
+                const long long n_chunks = (a.n_tasks + CHB - 1) / CHB;
+                for (long long chunk = blockIdx.x; chunk < n_chunks; chunk += gridDim.x)
+                    processRange(chunk * CHB, (chunk + 1) * CHB < a.n_tasks ? (chunk + 1) * CHB : a.n_tasks);
             }
         }
         else
