@@ -161,6 +161,15 @@ int lible_gpu_jk_autotune(lible_gpu_ctx *ctx, const double *D, double *J, double
                           const char *cache_path, char *summary, int summary_len);
 int lible_gpu_set_tune_cache(lible_gpu_ctx *ctx, const char *path);
 
+/* Per-launch timing of one J/K build (no reference counterpart; the reference's only timing hook
+ * is eri4Benchmark, src/lible/ints/twoel/eri4.cpp:97-150): every class launch runs serialised on
+ * the context stream between two CUDA events.  On entry *n is the capacity of the arrays (any of
+ * which may be NULL); on return *n is the number of launches.  Per launch: ls[4i..4i+3] = (la, lb,
+ * lc, ld), fp32[i], ms[i], algorithmic FLOPs flops[i] and quartets tasks[i].  J, K receive the
+ * build's result. */
+int lible_gpu_jk_profile(lible_gpu_ctx *ctx, const double *D, double *J, double *K, const lible_gpu_jk_opts *opts,
+                         int *n, int *ls, int *fp32, double *ms, double *flops, long long *tasks);
+
 /* Size of the (cached) screening plan for these options: quartets, primitive quartets and the
  * algorithmic FP64 / FP32 FLOPs one lible_gpu_jk call performs (dense-equivalent count). */
 typedef struct lible_gpu_jk_plan_info {

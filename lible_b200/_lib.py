@@ -65,6 +65,7 @@ SIGNATURES = {
     "lible_gpu_batch_layout": [P, P, P, P, P],
     "lible_gpu_jk_autotune": [P, P, P, P, ctypes.POINTER(JKOpts), S, P, I],
     "lible_gpu_set_tune_cache": [P, S],
+    "lible_gpu_jk_profile": [P, P, P, P, ctypes.POINTER(JKOpts), P, P, P, P, P, P],
     "lible_gpu_stream": [P, ctypes.POINTER(P)],
     "lible_gpu_jk_plan_classes": [P, ctypes.POINTER(JKOpts), P, P, P, P, P, P],
     "lible_gpu_fp64_peak": [P, ctypes.POINTER(D), ctypes.POINTER(D)],

@@ -70,15 +70,19 @@ namespace
     }
 
     // Device view of a caller array: the array itself if it is device memory, else a staged copy.
+    // With an engine and a slot, host arrays are staged in the context's cached buffer of that slot
+    // (grow-only, kept until the context is destroyed), so repeated calls allocate nothing and the
+    // device addresses stay stable (which keeps captured CUDA graphs valid).
     struct DevArray
     {
         double *ptr = nullptr;
         double *user = nullptr;
         size_t n = 0;
-        bool owned = false;
+        bool owned = false, staged = false;
         cudaStream_t s = nullptr;
 
-        DevArray(const double *p, size_t count, bool copy_in, cudaStream_t stream)
+        DevArray(const double *p, size_t count, bool copy_in, cudaStream_t stream, Engine *eng = nullptr,
+                 int slot = -1)
             : user(const_cast<double *>(p)), n(count), s(stream)
         {
             if (!p)
@@ -88,14 +92,20 @@ namespace
                 ptr = const_cast<double *>(p);
                 return;
             }
-            cudaCheck(cudaMalloc(&ptr, std::max<size_t>(n, 1) * sizeof(double)), "cudaMalloc");
-            owned = true;
+            staged = true;
+            if (eng && slot >= 0)
+                ptr = eng->staging(slot, std::max<size_t>(n, 1));
+            else
+            {
+                cudaCheck(cudaMalloc(&ptr, std::max<size_t>(n, 1) * sizeof(double)), "cudaMalloc");
+                owned = true;
+            }
             if (copy_in)
                 cudaCheck(cudaMemcpyAsync(ptr, p, n * sizeof(double), cudaMemcpyHostToDevice, s), "H2D");
         }
         void copyOut()
         {
-            if (owned && user)
+            if (staged && user)
             {
                 cudaCheck(cudaMemcpyAsync(user, ptr, n * sizeof(double), cudaMemcpyDeviceToHost, s), "D2H");
                 cudaCheck(cudaStreamSynchronize(s), "D2H");
@@ -545,9 +555,9 @@ int lible_gpu_jk(lible_gpu_ctx *ctx, const double *D, double *J, double *K, cons
         if (!D || !J || !K)
             throw EngineError(kStatusInvalid, "null D/J/K");
         const size_t n2 = (size_t)e.packedSize();
-        DevArray d(D, n2, true, e.stream());
-        DevArray j(J, n2, false, e.stream());
-        DevArray k(K, n2, false, e.stream());
+        DevArray d(D, n2, true, e.stream(), &e, 0);
+        DevArray j(J, n2, false, e.stream(), &e, 1);
+        DevArray k(K, n2, false, e.stream(), &e, 2);
         JKStats st;
         e.jk(d.ptr, j.ptr, k.ptr, toOpts(opts), &st);
         j.copyOut();
@@ -607,6 +617,39 @@ int lible_gpu_batch_layout(lible_gpu_ctx *ctx, int *n_mol, long long *nao, long 
     });
 }
 
+int lible_gpu_jk_profile(lible_gpu_ctx *ctx, const double *D, double *J, double *K, const lible_gpu_jk_opts *opts,
+                         int *n, int *ls, int *fp32, double *ms, double *flops, long long *tasks)
+{
+    return guard(ctx, [&](Engine &e) {
+        if (!D || !J || !K || !n)
+            throw EngineError(kStatusInvalid, "null argument");
+        const size_t n2 = (size_t)e.packedSize();
+        DevArray d(D, n2, true, e.stream(), &e, 0);
+        DevArray j(J, n2, false, e.stream(), &e, 1);
+        DevArray k(K, n2, false, e.stream(), &e, 2);
+        auto v = e.jkProfile(d.ptr, j.ptr, k.ptr, toOpts(opts));
+        j.copyOut();
+        k.copyOut();
+        const int cap = *n;
+        *n = (int)v.size();
+        if (!ls)
+            return;
+        for (int i = 0; i < std::min(cap, (int)v.size()); i++)
+        {
+            for (int q = 0; q < 4; q++)
+                ls[4 * i + q] = v[i].l[q];
+            if (fp32)
+                fp32[i] = v[i].fp32;
+            if (ms)
+                ms[i] = v[i].ms;
+            if (flops)
+                flops[i] = v[i].flops;
+            if (tasks)
+                tasks[i] = v[i].tasks;
+        }
+    });
+}
+
 int lible_gpu_set_tune_cache(lible_gpu_ctx *ctx, const char *path)
 {
     return guard(ctx, [&](Engine &e) { e.setTuneCache(path ? path : ""); });
@@ -619,9 +662,9 @@ int lible_gpu_jk_autotune(lible_gpu_ctx *ctx, const double *D, double *J, double
         if (!D || !J || !K)
             throw EngineError(kStatusInvalid, "null D/J/K");
         const size_t n2 = (size_t)e.packedSize();
-        DevArray d(D, n2, true, e.stream());
-        DevArray j(J, n2, false, e.stream());
-        DevArray k(K, n2, false, e.stream());
+        DevArray d(D, n2, true, e.stream(), &e, 0);
+        DevArray j(J, n2, false, e.stream(), &e, 1);
+        DevArray k(K, n2, false, e.stream(), &e, 2);
         std::string s = e.jkAutotune(d.ptr, j.ptr, k.ptr, toOpts(opts), cache_path ? cache_path : "");
         j.copyOut();
         k.copyOut();
@@ -702,9 +745,9 @@ int lible_gpu_jk_energy_forward(lible_gpu_ctx *ctx, const double *D, const lible
         if (!D || !energy)
             throw EngineError(kStatusInvalid, "null D/energy");
         const size_t nn = (size_t)e.packedSize();
-        DevArray d(D, nn, true, e.stream());
-        DevArray j(J, nn, false, e.stream());
-        DevArray k(K, nn, false, e.stream());
+        DevArray d(D, nn, true, e.stream(), &e, 0);
+        DevArray j(J, nn, false, e.stream(), &e, 1);
+        DevArray k(K, nn, false, e.stream(), &e, 2);
         double *jp = j.ptr, *kp = k.ptr, *tmp = nullptr;
         if (!jp || !kp)
         {

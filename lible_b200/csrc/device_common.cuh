@@ -33,6 +33,7 @@ namespace lible_b200
         const float *Etf;
         const double *E1;      // [ppair][3][S_ab][H_ab]
         const double *E1t;     // [ppair][3][H_ab][S_ab]
+        const float *pPf;      // [ppair][8] p, 1/p, P hi, P lo (FP32 classes only)
     };
 
     enum EpilogueMode : int
@@ -49,7 +50,7 @@ namespace lible_b200
     {
         PairView bra, ket;
         const double *boys;               // Boys tables [kBoysMaxN + 1][kBoysTerms][kBoysPitch]
-        const float *boys_f;              // FP32 Boys tables [kBoysMaxN + 1][kBoysTermsF][kBoysPitch]
+        const float *boys_f;              // FP32 Boys table [kBoysMaxN + kBoysTermsF][kBoysPitch], F_j(x_i)
         // task enumeration: explicit (bra pair, ket pair) list, or the implicit Schwarz prefix form:
         // task t belongs to major position i with prefix[i] <= t < prefix[i+1] and pairs with
         // minor position minor_begin[i] + (t - prefix[i]).  major_ket = 1 enumerates ket-major
@@ -75,6 +76,20 @@ namespace lible_b200
         const double *bra_pPs;
         const double *bra_Es;
         const float *bra_Efs;
+        const float *bra_pPfs;
+        // per-position bra fields (x = first AO of a, y = first AO of b, z = packed-block base,
+        // w = block dimension | K << 16 | (a and b the same shell) << 31) and the D_ab blocks gathered
+        // in Schwarz order ([mn][position]); J/K launches only
+        const int4 *bra_soa2;
+        const double *bra_Dab;
+        int bra_npos;
+        // Schwarz window of implicit enumerations: a task whose Q_bra Q_ket falls outside
+        // [q_lo, q_hi) is skipped (plans hand out whole bra groups and leave the test to the
+        // kernels); Q by Schwarz position (bra_qpos) or by pair index; ket_qpair null = no test
+        const double *bra_qpos;
+        const double *bra_qpair;
+        const double *ket_qpair;
+        double q_lo, q_hi;
         // epilogue
         int mode;
         int flags;                        // kStore: bit0 swap bra shells, bit1 swap ket shells, bit2 swap bra/ket
@@ -187,7 +202,29 @@ namespace lible_b200
         ik = a.major_ket ? maj : mnr;
     }
 
+    // Whether task (bra pair ib at Schwarz position pos, ket pair ik) lies in the launch's window.
+    __device__ __forceinline__ bool inWindow(const QuartetArgs &a, uint32_t ib, uint32_t ik, uint32_t pos, bool by_pos)
+    {
+        if (!a.ket_qpair)
+            return true;
+        const double qb = (by_pos && a.bra_qpos) ? __ldg(a.bra_qpos + pos) : __ldg(a.bra_qpair + ib);
+        const double qq = qb * __ldg(a.ket_qpair + ik);
+        return qq >= a.q_lo && qq < a.q_hi;
+    }
+
     // Degeneracy weight of a unique quartet: 1/2 for each coinciding shell pair / pair pair.
+    __device__ __forceinline__ double quartetWeight(const QuartetArgs &a, bool bra_same_shell, uint32_t ib,
+                                                    uint32_t ik)
+    {
+        const int32_t *ki = a.ket.info + 8 * ik;
+        double f = bra_same_shell ? 0.5 : 1.0;
+        if (ki[4] == ki[5])
+            f *= 0.5;
+        if (a.same_class && ib == ik)
+            f *= 0.5;
+        return f;
+    }
+
     __device__ __forceinline__ double quartetWeight(const QuartetArgs &a, uint32_t ib, uint32_t ik)
     {
         const int32_t *bi = a.bra.info + 8 * ib;
@@ -255,11 +292,11 @@ namespace lible_b200
         for (int e = threadIdx.x; e < kBoysTerms * kBoysPitch; e += blockDim.x)
             dst[e] = __ldg(src + e);
     }
-    __device__ __forceinline__ void stageBoys(const float *__restrict__ tables, int N, float *dst)
+    // FP32: rows F_0 .. F_{N + kBoysTermsF - 1} of the unscaled table.
+    __device__ __forceinline__ void stageBoys(const float *__restrict__ table, int N, float *dst)
     {
-        const float *src = tables + (size_t)N * kBoysTermsF * kBoysPitch;
-        for (int e = threadIdx.x; e < kBoysTermsF * kBoysPitch; e += blockDim.x)
-            dst[e] = __ldg(src + e);
+        for (int e = threadIdx.x; e < (N + kBoysTermsF) * kBoysPitch; e += blockDim.x)
+            dst[e] = __ldg(table + e);
     }
 
     // Boys function F_n(x), n = 0..N.  Reference method (src/lible/ints/boys_function.hpp:68-109):
@@ -300,38 +337,48 @@ namespace lible_b200
             F[k] = (x2 * F[k + 1] + ex) * (1.0 / (2 * k + 1));
     }
 
-    // The same function for quartets evaluated in FP32: the large-x asymptote and the downward
-    // recursion stay FP64, while the Taylor sum of F_N (10 float terms from the shared-memory FP32
-    // table) and e^{-x} (MUFU ex2) are single precision, so every F_k carries FP32 relative accuracy.
+    // The Boys function for quartets evaluated in FP32, F_0..F_N as floats.  The large-x asymptote
+    // stays FP64 (its inverse square root and upward products are formed in double and rounded
+    // once).  Below x = 30 every order n comes from its own Taylor sum about the nearest integer,
+    // sum_k F_{n+k}(x_i) (x_i - x)^k / k! with kBoysTermsF terms read from the staged FP32 table
+    // (rows F_0 .. F_{N+kBoysTermsF-1}), so no recursion is evaluated in single precision.
     template <int N>
-    __device__ __forceinline__ void boysF32(double x, const float *__restrict__ tabf, double *F)
+    __device__ __forceinline__ void boysF32(float x, const float *__restrict__ tabf, float *F)
     {
-        if (x > kBoysLargeX)
+        if (x > (float)kBoysLargeX)
         {
-            const double rs = rsqrt(x);
+            const double xd = x;
+            const double rs = rsqrt(xd);
             const double rx = rs * rs;
-            F[0] = 0.88622692545275801365 * rs;
+            double f = 0.88622692545275801365 * rs;
+            F[0] = (float)f;
 #pragma unroll
             for (int k = 1; k <= N; k++)
-                F[k] = F[k - 1] * ((k - 0.5) * rx);
+            {
+                f *= (k - 0.5) * rx;
+                F[k] = (float)f;
+            }
             return;
         }
-        const float xf = (float)x;
-        const int iv = __float2int_rn(xf);
-        const float m = (float)iv - xf;
-        const float *c = tabf + iv;
-        float s = ldsF(c + (kBoysTermsF - 1) * kBoysPitch);
+        constexpr int T = kBoysTermsF;
+        const int iv = __float2int_rn(x);
+        const float m = (float)iv - x;
+        float Fj[N + T];
 #pragma unroll
-        for (int k = kBoysTermsF - 2; k >= 0; k--)
-            s = fmaf(s, m, ldsF(c + k * kBoysPitch));
-        F[N] = (double)s;
-        if constexpr (N > 0)
+        for (int j = 0; j < N + T; j++)
+            Fj[j] = ldsF(tabf + j * kBoysPitch + iv);
+        float mk[T];
+#pragma unroll
+        for (int k = 1; k < T; k++)
+            mk[k] = m * (1.0f / k);
+#pragma unroll
+        for (int n = 0; n <= N; n++)
         {
-            const double ex = (double)__expf(-xf);
-            const double x2 = 2.0 * x;
+            float s = Fj[n + T - 1];
 #pragma unroll
-            for (int k = N - 1; k >= 0; k--)
-                F[k] = (x2 * F[k + 1] + ex) * (1.0 / (2 * k + 1));
+            for (int k = T - 1; k >= 1; k--)
+                s = fmaf(mk[k], s, Fj[n + k - 1]);
+            F[n] = s;
         }
     }
 

@@ -6,9 +6,11 @@
 
 #include <algorithm>
 #include <chrono>
+#include <climits>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <functional>
 #include <numeric>
 #include <stdexcept>
 
@@ -33,6 +35,7 @@ namespace lible_b200
         SphTables sph;
         double *pP, *ab, *E, *Et, *E1, *E1t;
         float *Ef, *Etf;
+        float *pPf;  // FP32 record [ppair][8]: p, 1/p, P (hi), P - hi (lo)
     };
 
     // Hermite E matrices of every primitive pair of one class, with the spherical transforms of both
@@ -79,6 +82,20 @@ namespace lible_b200
         a.pP[8 * ip + 5] = ea;
         a.pP[8 * ip + 6] = eb;
         a.pP[8 * ip + 7] = 0.0;
+        if (a.pPf)
+        {
+            // P split into float hi + lo parts: (P - Q) then keeps float relative accuracy even for
+            // nearby centres far from the origin
+            float *f = a.pPf + 8 * ip;
+            f[0] = (float)p;
+            f[1] = (float)(1.0 / p);
+            for (int k = 0; k < 3; k++)
+            {
+                const float hi = (float)P[k];
+                f[2 + k] = hi;
+                f[5 + k] = (float)(P[k] - (double)hi);
+            }
+        }
         a.ab[2 * ip + 0] = ea;
         a.ab[2 * ip + 1] = eb;
         const int nt = lab + 1;
@@ -259,9 +276,9 @@ namespace lible_b200
 
     // Builds the bra-side structure-of-arrays copies of one class in Schwarz order (layout in
     // DevPairClass): block-strided over positions, threads over (primitive, field).
-    __global__ void soaGatherKernel(const double *E, const float *Ef, const double *pP, const uint32_t *pofs,
-                                    const uint32_t *order, const uint4 *soa, long long n_pos, int sabhab, double *Es,
-                                    float *Efs, double *pPs)
+    __global__ void soaGatherKernel(const double *E, const float *Ef, const double *pP, const float *pPf,
+                                    const uint32_t *pofs, const uint32_t *order, const uint4 *soa, long long n_pos,
+                                    int sabhab, double *Es, float *Efs, double *pPs, float *pPfs)
     {
         for (long long j = blockIdx.x; j < n_pos; j += gridDim.x)
         {
@@ -280,6 +297,24 @@ namespace lible_b200
                 const int k = idx / 5, f = idx % 5;
                 pPs[sv.x + (size_t)idx * n] = pP[8 * ((size_t)p0 + k) + (f < 4 ? f : 4)];
             }
+            if (pPfs)
+                for (int idx = threadIdx.x; idx < (int)K * 8; idx += blockDim.x)
+                    pPfs[sv.w + (size_t)idx * n] = pPf[8 * (size_t)p0 + idx];
+        }
+    }
+
+    // D_ab blocks of every bra pair of a class in Schwarz order: Dab[mn * n_pos + position].
+    __global__ void dabGatherKernel(const double *D, const int4 *soa2, long long n_pos, int sa, int sb, double *Dab)
+    {
+        const long long total = n_pos * sa * sb;
+        for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+             idx += (long long)gridDim.x * blockDim.x)
+        {
+            const long long pos = idx % n_pos;
+            const int mn = (int)(idx / n_pos), m = mn / sb, nn = mn % sb;
+            const int4 si = soa2[pos];
+            const int n = si.w & 0xffff;
+            Dab[idx] = D[(size_t)(uint32_t)si.z + (size_t)(si.x + m) * n + si.y + nn];
         }
     }
 
@@ -408,6 +443,8 @@ namespace lible_b200
         clearStructure();
         for (void *p : persistent_)
             cudaFree(p);
+        for (double *p : staging_)
+            cudaFree(p);
         cudaFree(boys_);
         cudaFree(boys_f_);
         cudaFree(sph_rc_);
@@ -435,10 +472,13 @@ namespace lible_b200
             for (void *p : {(void *)d.pP, (void *)d.ab, (void *)d.pofs, (void *)d.info, (void *)d.coords,
                             (void *)d.E, (void *)d.Et, (void *)d.Ef, (void *)d.Etf, (void *)d.E1,
                             (void *)d.E1t, (void *)d.Q, (void *)d.pPs, (void *)d.Es, (void *)d.Efs,
-                            (void *)d.soa})
+                            (void *)d.soa, (void *)d.pPf, (void *)d.pPfs, (void *)d.soa2, (void *)d.Dab})
                 cudaFree(p);
         for (auto &o : cs.orders)
+        {
             cudaFree(o.d_order);
+            cudaFree(o.d_q);
+        }
         cs = ClassSet();
     }
 
@@ -589,6 +629,7 @@ namespace lible_b200
         {
             d.Ef = devAlloc<float>(np * sab * hab);
             d.Etf = devAlloc<float>(np * sab * hab);
+            d.pPf = devAlloc<float>(8 * np);
         }
         if (with_d1)
         {
@@ -622,6 +663,7 @@ namespace lible_b200
         ea.Et = d.Et;
         ea.Ef = d.Ef;
         ea.Etf = d.Etf;
+        ea.pPf = d.pPf;
         ea.E1 = d.E1;
         ea.E1t = d.E1t;
         const int bs = 64;
@@ -728,7 +770,7 @@ namespace lible_b200
 
     PairView Engine::view(const DevPairClass &d)
     {
-        return PairView{d.pP, d.ab, d.pofs, d.info, d.E, d.Et, d.Ef, d.Etf, d.E1, d.E1t};
+        return PairView{d.pP, d.ab, d.pofs, d.info, d.E, d.Et, d.Ef, d.Etf, d.E1, d.E1t, d.pPf};
     }
 
     // Runs one class pair over an explicit task list in store mode.  `bra` and `ket` are in the
@@ -1080,49 +1122,88 @@ namespace lible_b200
             const auto &mb = cs.host[c].mat_base;
             auto K = [&](uint32_t x) { return pofs[x + 1] - pofs[x]; };
             auto M = [&](uint32_t x) { return mb.empty() ? 0 : mb[x]; };
+            // Q buckets of a factor 4: pairs of one bucket survive or fail against most kets together
+            auto bucket = [&](uint32_t x) { return Q[x] > 0 ? (int)std::floor(0.5 * std::log2(Q[x])) : INT_MIN; };
+            const auto &hc0 = cs.host[c];
             ClassOrder &o = cs.orders[c];
             o.order.resize(Q.size());
             std::iota(o.order.begin(), o.order.end(), 0u);
+            // (molecule, K, bucket descending, AO of a, AO of b): inside a bucket, consecutive pairs
+            // share shells and neighbouring AOs, so a warp's digestion touches few rows of D, J, K
             std::stable_sort(o.order.begin(), o.order.end(), [&](uint32_t x, uint32_t y) {
                 if (M(x) != M(y))
                     return M(x) < M(y);
-                return K(x) != K(y) ? K(x) < K(y) : Q[x] > Q[y];
+                if (K(x) != K(y))
+                    return K(x) < K(y);
+                if (bucket(x) != bucket(y))
+                    return bucket(x) > bucket(y);
+                if (hc0.ao_a[x] != hc0.ao_a[y])
+                    return hc0.ao_a[x] < hc0.ao_a[y];
+                return hc0.ao_b[x] < hc0.ao_b[y];
             });
             o.q.resize(Q.size());
-            o.kpre.assign(Q.size() + 1, 0.0);
             for (size_t i = 0; i < Q.size(); i++)
             {
                 const uint32_t x = o.order[i];
                 o.q[i] = Q[x];
-                o.kpre[i + 1] = o.kpre[i] + K(x);
-                if (o.groups.empty() || o.groups.back().k != K(x) || o.groups.back().mol != M(x))
-                    o.groups.push_back({K(x), (uint32_t)i, (uint32_t)i, M(x)});
-                o.groups.back().end = (uint32_t)i + 1;
+                if (o.groups.empty() || o.groups.back().k != K(x) || o.groups.back().mol != M(x) ||
+                    o.groups.back().bucket != bucket(x))
+                    o.groups.push_back({K(x), (uint32_t)i, (uint32_t)i, M(x), bucket(x), Q[x], Q[x]});
+                auto &g = o.groups.back();
+                g.end = (uint32_t)i + 1;
+                g.qmax = std::max(g.qmax, Q[x]);
+                g.qmin = std::min(g.qmin, Q[x]);
             }
+            o.qs = o.q;
+            for (const auto &g : o.groups)
+                std::sort(o.qs.begin() + g.start, o.qs.begin() + g.end, std::greater<double>());
             o.d_order = devUpload(o.order, stream_);
+            o.d_q = devUpload(o.q, stream_);
             // bra-side structure-of-arrays copies in this order
             const int sabhab = nsph(d.la) * nsph(d.lb) * nherm(d.la + d.lb);
             std::vector<uint4> soa(Q.size());
-            size_t base_p = 0, base_e = 0;
+            size_t base_p = 0, base_e = 0, base_f = 0;
             for (const auto &g : o.groups)
             {
                 const uint32_t ng = g.end - g.start;
                 for (uint32_t i = 0; i < ng; i++)
-                    soa[g.start + i] = make_uint4((unsigned)(base_p + i), (unsigned)(base_e + i), ng, 0);
+                    soa[g.start + i] =
+                        make_uint4((unsigned)(base_p + i), (unsigned)(base_e + i), ng, (unsigned)(base_f + i));
                 base_p += (size_t)g.k * 5 * ng;
                 base_e += (size_t)g.k * sabhab * ng;
+                base_f += (size_t)g.k * 8 * ng;
             }
             if (base_e >= (1ULL << 32) || base_p >= (1ULL << 32))
                 throw EngineError(kStatusInvalid, "pair class too large for 32-bit structure-of-arrays offsets");
+            // per-position bra fields for the J/K digestion
+            std::vector<int4> soa2(Q.size());
+            const auto &hc = cs.host[c];
+            for (size_t j = 0; j < Q.size(); j++)
+            {
+                const uint32_t x = o.order[j];
+                const int mn = hc.mat_n.empty() ? (int)nao_ : hc.mat_n[x];
+                const int kk = (int)K(x);
+                if (mn >= (1 << 16) || kk >= (1 << 15))
+                    throw EngineError(kStatusInvalid, "molecule or contraction too large for the packed pair fields");
+                const bool same = hc.shell_a[x] == hc.shell_b[x];
+                soa2[j] = make_int4(hc.ao_a[x], hc.ao_b[x], hc.mat_base.empty() ? 0 : hc.mat_base[x],
+                                    (int)((unsigned)mn | ((unsigned)kk << 16) | (same ? 0x80000000u : 0u)));
+            }
             if (!soa.empty())
             {
                 d.soa = devUpload(soa, stream_);
+                d.soa2 = devUpload(soa2, stream_);
+                d.Dab = devAlloc<double>(soa.size() * nsph(d.la) * nsph(d.lb));
                 d.pPs = devAlloc<double>(std::max<size_t>(base_p, 1));
                 d.Es = devAlloc<double>(std::max<size_t>(base_e, 1));
                 if (d.Ef)
+                {
                     d.Efs = devAlloc<float>(std::max<size_t>(base_e, 1));
+                    d.pPfs = devAlloc<float>(std::max<size_t>(base_f, 1));
+                }
                 soaGatherKernel<<<(unsigned)std::min<size_t>(soa.size(), 65535), 128, 0, stream_>>>(
-                    d.E, d.Ef, d.pP, d.pofs, o.d_order, d.soa, (long long)soa.size(), sabhab, d.Es, d.Efs, d.pPs);
+                    d.E, d.Ef, d.pP, d.pPf, d.pofs, o.d_order, d.soa, (long long)soa.size(), sabhab, d.Es, d.Efs,
+                    d.pPs, d.pPfs);
                 cudaCheck(cudaGetLastError(), "soaGatherKernel");
             }
         }
@@ -1200,11 +1281,14 @@ namespace lible_b200
                                                double thr, double thr32, bool mixed)
     {
         const ClassOrder &ob = bs.orders[cb], &ok = ks.orders[ck];
-        // number of entries >= bound in the descending range q[b, e)
-        auto countAbove = [](const std::vector<double> &q, uint32_t b, uint32_t e, double bound) -> uint32_t {
-            return (uint32_t)(std::upper_bound(q.begin() + b, q.begin() + e, bound,
-                                               [](double x, double v) { return x > v; }) -
-                              (q.begin() + b));
+        // survivors of the predicate q_b * qj >= t in a group: a prefix of its Q values in decreasing
+        // order (the kernels evaluate the same product)
+        auto countGroup = [&](const ClassOrder::Group &g, double qj, double t) -> long long {
+            if (t <= 0)
+                return g.end - g.start;
+            return std::partition_point(ob.qs.begin() + g.start, ob.qs.begin() + g.end,
+                                        [&](double q) { return q * qj >= t; }) -
+                   (ob.qs.begin() + g.start);
         };
         JKClassPair cp;
         cp.cb = cb;
@@ -1214,6 +1298,7 @@ namespace lible_b200
         auto &run64 = cp.run64, &run32 = cp.run32;  // tasks per major entry
         auto &cost = cp.cost;                       // primitive quartets (+ overhead) per task
         double bra_prims64 = 0, bra_prims32 = 0;
+        const double lo64 = mixed ? thr32 : thr;
         // segments (bra group, ket group) of the same molecule, heaviest (largest K_b K_k) first
         std::vector<std::pair<uint32_t, uint32_t>> segs;
         for (uint32_t gb = 0; gb < (uint32_t)ob.groups.size(); gb++)
@@ -1224,44 +1309,92 @@ namespace lible_b200
             return (double)ob.groups[x.first].k * ok.groups[x.second].k >
                    (double)ob.groups[y.first].k * ok.groups[y.second].k;
         });
+        std::vector<int> fen;  // Fenwick tree over Q ranks (diagonal segments)
         for (const auto &sg : segs)
+        {
+            const size_t gb = sg.first, gc = sg.second;
+            const auto &B = ob.groups[gb], &C = ok.groups[gc];
+            const bool diag = triangle && gb == gc;
+            const uint32_t nb = B.end - B.start;
+            // diagonal segment: a ket at group offset r pairs with the bras at offsets >= r; the
+            // survivors among them are counted with a Fenwick tree over the ranks of their Q values,
+            // filled from the last offset down
+            std::vector<uint32_t> rank;
+            if (diag)
             {
-                const size_t gb = sg.first, gc = sg.second;
-                const auto &B = ob.groups[gb], &C = ok.groups[gc];
-                for (uint32_t j = C.start; j < C.end; j++)
-                {
-                    const double qj = ok.q[j];
-                    const uint32_t lo = (triangle && gb == gc) ? j - C.start : 0u;
-                    uint32_t nall = qj > 0 ? countAbove(ob.q, B.start, B.end, thr / qj) : 0;
-                    if (thr <= 0)
-                        nall = B.end - B.start;
-                    uint32_t n64 = nall;
-                    if (mixed)
-                        n64 = qj > 0 ? std::min(nall, countAbove(ob.q, B.start, B.end, thr32 / qj)) : 0;
-                    nall = std::max(nall, lo);
-                    n64 = std::max(n64, lo);
-                    if (nall == lo)
-                        continue;
-                    majors.push_back(ok.order[j]);
-                    b64.push_back(B.start + lo);
-                    b32.push_back(B.start + n64);
-                    p64.push_back(p64.back() + (n64 - lo));
-                    p32.push_back(p32.back() + (nall - n64));
-                    run64.push_back(n64 - lo);
-                    run32.push_back(nall - n64);
-                    cost.push_back((double)C.k * B.k + 4.0);
-                    const double kj = C.k;
-                    const double pr64 = ob.kpre[B.start + n64] - ob.kpre[B.start + lo];
-                    const double pr32 = ob.kpre[B.start + nall] - ob.kpre[B.start + n64];
-                    cp.prim64 += kj * pr64;
-                    cp.prim32 += kj * pr32;
-                    // bra-side work is counted per (bra primitive, ket pair)
-                    bra_prims64 += pr64;
-                    bra_prims32 += pr32;
-                }
+                fen.assign(nb + 1, 0);
+                std::vector<uint32_t> idx(nb);
+                std::iota(idx.begin(), idx.end(), 0u);
+                std::stable_sort(idx.begin(), idx.end(),
+                                 [&](uint32_t x, uint32_t y) { return ob.q[B.start + x] > ob.q[B.start + y]; });
+                rank.resize(nb);
+                for (uint32_t r = 0; r < nb; r++)
+                    rank[idx[r]] = r;
             }
-        cp.n64 = (long long)p64.back();
-        cp.n32 = (long long)p32.back();
+            auto fenAdd = [&](uint32_t r) {
+                for (uint32_t i = r + 1; i <= nb; i += i & (0u - i))
+                    fen[i]++;
+            };
+            auto fenSum = [&](uint32_t r) {  // entries with rank < r
+                long long v = 0;
+                for (uint32_t i = r; i > 0; i -= i & (0u - i))
+                    v += fen[i];
+                return v;
+            };
+            auto countDiag = [&](double qj, double t) -> long long {
+                if (t <= 0)
+                    return fenSum(nb);
+                const uint32_t r = (uint32_t)(std::partition_point(ob.qs.begin() + B.start, ob.qs.begin() + B.end,
+                                                                   [&](double q) { return q * qj >= t; }) -
+                                              (ob.qs.begin() + B.start));
+                return fenSum(r);
+            };
+            struct Entry
+            {
+                uint32_t major, lo;
+                long long c64, c32;
+            };
+            std::vector<Entry> entries;
+            for (uint32_t jr = C.end; jr-- > C.start;)
+            {
+                const uint32_t j = jr;
+                const double qj = ok.q[j];
+                const uint32_t lo = diag ? j - C.start : 0u;
+                if (diag)
+                    fenAdd(rank[lo]);
+                if (thr > 0 && B.qmax * qj < thr)
+                    continue;
+                const long long call = diag ? countDiag(qj, thr) : countGroup(B, qj, thr);
+                if (call == 0)
+                    continue;
+                const long long c64 = mixed ? (diag ? countDiag(qj, lo64) : countGroup(B, qj, lo64)) : call;
+                entries.push_back({j, lo, c64, call - c64});
+            }
+            // kets in increasing position (the diagonal walk above ran backwards)
+            for (size_t e = entries.size(); e-- > 0;)
+            {
+                const Entry &en = entries[e];
+                const uint32_t r = nb - en.lo;
+                majors.push_back(ok.order[en.major]);
+                b64.push_back(B.start + en.lo);
+                b32.push_back(B.start + en.lo);
+                const unsigned long long t64 = en.c64 > 0 ? r : 0, t32 = en.c32 > 0 ? r : 0;
+                p64.push_back(p64.back() + t64);
+                p32.push_back(p32.back() + t32);
+                run64.push_back(t64);
+                run32.push_back(t32);
+                cost.push_back((double)C.k * B.k + 4.0);
+                cp.n64 += en.c64;
+                cp.n32 += en.c32;
+                cp.prim64 += (double)en.c64 * B.k * C.k;
+                cp.prim32 += (double)en.c32 * B.k * C.k;
+                // bra-side work is counted per (bra primitive, ket pair)
+                bra_prims64 += (double)en.c64 * B.k;
+                bra_prims32 += (double)en.c32 * B.k;
+            }
+        }
+        cp.t64 = (long long)p64.back();
+        cp.t32 = (long long)p32.back();
         const auto &B = bs.host[cb], &K = ks.host[ck];
         cp.tb = pairType(B.la, B.lb);
         cp.tk = pairType(K.la, K.lb);
@@ -1290,7 +1423,7 @@ namespace lible_b200
     // `mult` work units.
     void Engine::rebuildChunks(JKClassPair &cp, bool fp32, int mult)
     {
-        const long long n = fp32 ? cp.n32 : cp.n64;
+        const long long n = fp32 ? cp.t32 : cp.t64;
         unsigned long long *&dev = fp32 ? cp.chunks32 : cp.chunks64;
         cudaFree(dev);
         dev = nullptr;
@@ -1343,6 +1476,7 @@ namespace lible_b200
         assignBranches(plan);
         cudaCheck(cudaStreamSynchronize(stream_), "plan");
         plan.thr = thr;
+        plan.thr32 = thr32;
         return plans_.emplace(key, std::move(plan)).first->second;
     }
 
@@ -1363,9 +1497,47 @@ namespace lible_b200
         }
     }
 
+    // D_ab of every pair of the main classes, in Schwarz order, for the coalesced J_cd digestion.
+    void Engine::gatherDab(const double *D)
+    {
+        for (const auto &d : mainSet(true).dev)
+            if (d.Dab && d.n_pairs)
+            {
+                const long long tot = (long long)d.n_pairs * nsph(d.la) * nsph(d.lb);
+                dabGatherKernel<<<(unsigned)std::min<long long>((tot + 255) / 256, num_sms_ * 8), 256, 0, stream_>>>(
+                    D, d.soa2, (long long)d.n_pairs, nsph(d.la), nsph(d.lb), d.Dab);
+            }
+        cudaCheck(cudaGetLastError(), "dabGatherKernel");
+    }
+
+    // Event pairs around each class launch of a profiled build.
+    struct Engine::LaunchTimer
+    {
+        std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev;
+        std::vector<LaunchTime> info;
+        void before(cudaStream_t s)
+        {
+            cudaEvent_t a, b;
+            cudaCheck(cudaEventCreate(&a), "event");
+            cudaCheck(cudaEventCreate(&b), "event");
+            ev.push_back({a, b});
+            cudaCheck(cudaEventRecord(a, s), "event");
+        }
+        void after(cudaStream_t s) { cudaCheck(cudaEventRecord(ev.back().second, s), "event"); }
+        ~LaunchTimer()
+        {
+            for (auto &e : ev)
+            {
+                cudaEventDestroy(e.first);
+                cudaEventDestroy(e.second);
+            }
+        }
+    };
+
     // Launches one J/K build of `plan` (memsets, class kernels over the stream branches, block
-    // symmetrisation) on stream_; usable inside a stream capture.
-    void Engine::enqueueJK(JKPlan &plan, const double *D, double *J, double *K, bool mixed)
+    // symmetrisation) on stream_; usable inside a stream capture.  With a timer every class launch
+    // goes to stream_ itself, bracketed by events.
+    void Engine::enqueueJK(JKPlan &plan, const double *D, double *J, double *K, bool mixed, LaunchTimer *timer)
     {
         ClassSet &cs = mainSet(true);
         const size_t n = (size_t)packed_;
@@ -1373,10 +1545,12 @@ namespace lible_b200
         cudaCheck(cudaMemsetAsync(K, 0, n * sizeof(double), stream_), "memset");
         cudaCheck(cudaMemsetAsync(plan.counters, 0, 2 * plan.pairs.size() * sizeof(unsigned long long), stream_),
                   "memset");
+        gatherDab(D);
         cudaCheck(cudaEventRecord(fork_, stream_), "fork");
         bool used[kBranches] = {};
-        for (const auto &cp : plan.pairs)
-            used[cp.branch] = true;
+        if (!timer)
+            for (const auto &cp : plan.pairs)
+                used[cp.branch] = true;
         for (int b = 0; b < kBranches; b++)
             if (used[b])
                 cudaCheck(cudaStreamWaitEvent(branch_[b], fork_, 0), "fork");
@@ -1384,7 +1558,8 @@ namespace lible_b200
         {
             const auto &cp = plan.pairs[ip];
             const auto &B = cs.dev[cp.cb], &Kc = cs.dev[cp.ck];
-            cudaStream_t st = branch_[cp.branch];
+            cudaStream_t st = timer ? stream_ : branch_[cp.branch];
+            const auto &Bh = cs.host[cp.cb], &Kh = cs.host[cp.ck];
             QuartetArgs a{};
             a.bra = view(B);
             a.ket = view(Kc);
@@ -1401,24 +1576,42 @@ namespace lible_b200
             a.J = J;
             a.K = K;
             a.nao = (int)nao_;
-            a.n_tasks = cp.n64;
+            a.n_tasks = cp.t64;
             a.prefix = cp.prefix64;
             a.minor_begin = cp.begin64;
             a.chunks = cp.chunks64;
             a.n_chunks = cp.n_chunks64;
             a.counter = plan.counters + 2 * ip;
             a.grid_div = cp.grid_div64;
+            a.bra_qpos = cs.orders[cp.cb].d_q;
+            a.bra_qpair = B.Q;
+            a.ket_qpair = Kc.Q;
+            a.q_lo = mixed ? plan.thr32 : plan.thr;
+            a.q_hi = HUGE_VAL;
             a.bra_soa = B.soa;
             a.bra_pPs = B.pPs;
             a.bra_Es = B.Es;
             a.bra_Efs = B.Efs;
+            a.bra_pPfs = B.pPfs;
+            a.bra_soa2 = B.soa2;
+            a.bra_Dab = B.Dab;
+            a.bra_npos = (int)B.n_pairs;
             LaunchFn f64 = lookupFwd64(cp.tb, cp.tk);
             if (!f64)
                 throw EngineError(kStatusUnsupported, "quartet class not instantiated");
-            cudaCheck(f64(a, st, num_sms_), "jk kernel");
-            if (mixed && cp.n32 > 0)
+            if (timer && cp.t64 > 0)
             {
-                a.n_tasks = cp.n32;
+                timer->before(st);
+                timer->info.push_back({{Bh.la, Bh.lb, Kh.la, Kh.lb}, 0, 0.0, cp.flops64, cp.n64});
+            }
+            cudaCheck(f64(a, st, num_sms_), "jk kernel");
+            if (timer && cp.t64 > 0)
+                timer->after(st);
+            if (mixed && cp.t32 > 0)
+            {
+                a.q_lo = plan.thr;
+                a.q_hi = plan.thr32;
+                a.n_tasks = cp.t32;
                 a.prefix = cp.prefix32;
                 a.minor_begin = cp.begin32;
                 a.chunks = cp.chunks32;
@@ -1428,7 +1621,14 @@ namespace lible_b200
                 LaunchFn f32 = lookupFwd32(cp.tb, cp.tk);
                 if (!f32)
                     throw EngineError(kStatusUnsupported, "FP32 quartet class not instantiated");
+                if (timer)
+                {
+                    timer->before(st);
+                    timer->info.push_back({{Bh.la, Bh.lb, Kh.la, Kh.lb}, 1, 0.0, cp.flops32, cp.n32});
+                }
                 cudaCheck(f32(a, st, num_sms_), "jk kernel fp32");
+                if (timer)
+                    timer->after(st);
             }
         }
         for (int b = 0; b < kBranches; b++)
@@ -1522,7 +1722,7 @@ namespace lible_b200
             stats->n_fp32 = plan.n_fp32;
             stats->n_launches = 2;
             for (const auto &cp : plan.pairs)
-                stats->n_launches += 1 + (cp.n32 > 0 ? 1 : 0);
+                stats->n_launches += 1 + (cp.t32 > 0 ? 1 : 0);
         }
     }
 
@@ -1566,7 +1766,7 @@ namespace lible_b200
         for (auto &cp : plan.pairs)
             for (int fp32 = 0; fp32 < 2; fp32++)
             {
-                const long long n = fp32 ? cp.n32 : cp.n64;
+                const long long n = fp32 ? cp.t32 : cp.t64;
                 if (n == 0)
                     continue;
                 const auto &B = cs.host[cp.cb], &K = cs.host[cp.ck];
@@ -1598,6 +1798,7 @@ namespace lible_b200
         cudaCheck(cudaEventCreate(&e0), "event");
         cudaCheck(cudaEventCreate(&e1), "event");
         std::string summary;
+        gatherDab(D);
         FILE *out = cache.empty() ? nullptr : fopen(cache.c_str(), "a");
         const int grid_divs[] = {1, 2};
         const int mults[] = {2, 8, 32};
@@ -1607,7 +1808,7 @@ namespace lible_b200
             const auto &B = cs.dev[cp.cb], &Kc = cs.dev[cp.ck];
             for (int fp32 = 0; fp32 < (mixed ? 2 : 1); fp32++)
             {
-                const long long n = fp32 ? cp.n32 : cp.n64;
+                const long long n = fp32 ? cp.t32 : cp.t64;
                 if (n == 0)
                     continue;
                 LaunchFn fn = fp32 ? lookupFwd32(cp.tb, cp.tk) : lookupFwd64(cp.tb, cp.tk);
@@ -1642,10 +1843,19 @@ namespace lible_b200
                         a.n_chunks = fp32 ? cp.n_chunks32 : cp.n_chunks64;
                         a.counter = plan.counters + 2 * ip + fp32;
                         a.grid_div = gd;
+                        a.bra_qpos = cs.orders[cp.cb].d_q;
+                        a.bra_qpair = B.Q;
+                        a.ket_qpair = Kc.Q;
+                        a.q_lo = fp32 ? plan.thr : (mixed ? plan.thr32 : plan.thr);
+                        a.q_hi = fp32 ? plan.thr32 : HUGE_VAL;
                         a.bra_soa = B.soa;
                         a.bra_pPs = B.pPs;
                         a.bra_Es = B.Es;
                         a.bra_Efs = B.Efs;
+                        a.bra_pPfs = B.pPfs;
+                        a.bra_soa2 = B.soa2;
+                        a.bra_Dab = B.Dab;
+                        a.bra_npos = (int)B.n_pairs;
                         float t_min = 1e30f;
                         for (int rep = 0; rep < 2; rep++)
                         {
@@ -1690,12 +1900,30 @@ namespace lible_b200
         return summary;
     }
 
+    std::vector<Engine::LaunchTime> Engine::jkProfile(const double *D, double *J, double *K, const JKOptions &opt)
+    {
+        const bool mixed = opt.precision == 1;
+        if (mixed && max_l_ > 2)
+            throw EngineError(kStatusUnsupported, "mixed precision is instantiated for l <= 2 bases only");
+        JKPlan &plan = jkPlan(opt.schwarz, opt.fp32_threshold, mixed);
+        LaunchTimer timer;
+        enqueueJK(plan, D, J, K, mixed, &timer);
+        cudaCheck(cudaStreamSynchronize(stream_), "profile");
+        for (size_t i = 0; i < timer.ev.size(); i++)
+        {
+            float ms = 0;
+            cudaCheck(cudaEventElapsedTime(&ms, timer.ev[i].first, timer.ev[i].second), "event");
+            timer.info[i].ms = ms;
+        }
+        return timer.info;
+    }
+
     long long Engine::jkLaunchCount(const JKOptions &opt)
     {
         JKPlan &plan = jkPlan(opt.schwarz, opt.fp32_threshold, opt.precision == 1);
         long long c = 2;
         for (const auto &cp : plan.pairs)
-            c += 1 + (cp.n32 > 0 ? 1 : 0);
+            c += 1 + (cp.t32 > 0 ? 1 : 0);
         return c;
     }
 
@@ -1752,7 +1980,11 @@ namespace lible_b200
             a.minor_begin = cp.begin64;
             a.prefix = cp.prefix64;
             a.n_major = cp.n_bra;
-            a.n_tasks = cp.n64;
+            a.n_tasks = cp.t64;
+            a.bra_qpair = B.Q;
+            a.ket_qpair = K.Q;
+            a.q_lo = plan.thr;
+            a.q_hi = HUGE_VAL;
             a.same_class = cp.cb == cp.ck;
             a.mode = kD1Grad;
             a.D = D_dev;
@@ -1799,7 +2031,12 @@ namespace lible_b200
             a.minor_begin = cp.begin64;
             a.prefix = cp.prefix64;
             a.n_major = cp.n_bra;
-            a.n_tasks = cp.n64;
+            a.n_tasks = cp.t64;
+            a.bra_qpos = bs.orders[cp.cb].d_q;
+            a.bra_qpair = B.Q;
+            a.ket_qpair = K.Q;
+            a.q_lo = plan.thr;
+            a.q_hi = HUGE_VAL;
             a.aux_side = cp.swap ? 1 : 0;
             a.D = D_dev;
             a.dcoef = dcoef_dev;
@@ -1811,6 +2048,7 @@ namespace lible_b200
             a.bra_pPs = B.pPs;
             a.bra_Es = B.Es;
             a.bra_Efs = B.Efs;
+            a.bra_pPfs = B.pPfs;
             a.chunks = cp.chunks64;
             a.n_chunks = cp.n_chunks64;
             if (gamma_dev)
@@ -1832,6 +2070,23 @@ namespace lible_b200
             cudaCheck(cudaGetLastError(), "symmetrize");
         }
         cudaCheck(cudaStreamSynchronize(stream_), "ri");
+    }
+
+    double *Engine::staging(int slot, size_t n)
+    {
+        if (slot < 0 || slot >= 4)
+            throw EngineError(kStatusInternal, "bad staging slot");
+        if (staging_n_[slot] < n)
+        {
+            releaseGraph();  // a captured graph may refer to the old buffer
+            cudaCheck(cudaStreamSynchronize(stream_), "staging");
+            cudaFree(staging_[slot]);
+            staging_[slot] = nullptr;
+            staging_n_[slot] = 0;
+            cudaCheck(cudaMalloc(&staging_[slot], n * sizeof(double)), "cudaMalloc");
+            staging_n_[slot] = n;
+        }
+        return staging_[slot];
     }
 
     void Engine::sync()

@@ -114,10 +114,15 @@ namespace lible_b200
         // Bra-side copies in Schwarz order, structure of arrays per (molecule, K) group g of n_g
         // pairs: element (prim k, field f) of the pair at group offset i sits at
         // base_g + (k * F + f) * n_g + i, so lanes holding consecutive Schwarz positions read
-        // consecutive words.  soa[position] = (pP base + i, E base + i, n_g, 0).
+        // consecutive words.  soa[position] = (pP base + i, E base + i, n_g, FP32 record base + i).
         double *pPs = nullptr;      // F = 5: p, Px, Py, Pz, 1/p
         double *Es = nullptr;       // F = S_ab H_ab
         float *Efs = nullptr;
+        float *pPfs = nullptr;      // F = 8: the FP32 record below, at soa.w
         uint4 *soa = nullptr;
+        float *pPf = nullptr;       // [n_ppairs][8] FP32 record: p, 1/p, P (float hi), P - hi (float lo)
+        int4 *soa2 = nullptr;       // per Schwarz position: ao_a, ao_b, packed-block base,
+                                    // N_m | K << 16 | (same shell) << 31
+        double *Dab = nullptr;      // per J/K call: D_ab of every pair, [mn][position]
     };
 }

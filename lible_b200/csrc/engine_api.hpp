@@ -134,6 +134,16 @@ namespace lible_b200
         // Direct J/K (device pointers).  J, K symmetric on return.  With opt.use_graph the launch
         // sequence is captured once per (plan, D, J, K) into a CUDA graph and replayed.
         void jk(const double *D_dev, double *J_dev, double *K_dev, const JKOptions &opt, JKStats *stats);
+        // One J/K build with every class launch serialised on the context stream and timed with CUDA
+        // events: (la, lb, lc, ld), FP32 flag, milliseconds, algorithmic FLOPs, tasks per launch.
+        struct LaunchTime
+        {
+            int l[4];
+            int fp32;
+            double ms, flops;
+            long long tasks;
+        };
+        std::vector<LaunchTime> jkProfile(const double *D_dev, double *J_dev, double *K_dev, const JKOptions &opt);
         // Times the candidate launch parameters of every class pair of the plan for `opt` on the
         // given buffers, keeps the fastest and appends them to `cache` (if non-empty).  Returns a
         // one-line summary per class pair.
@@ -155,6 +165,8 @@ namespace lible_b200
                         double schwarz);
 
         void sync();
+        // Cached device staging buffer `slot` (0..3) of at least n doubles (grow-only).
+        double *staging(int slot, size_t n);
 
     private:
         // Schwarz order of one class: pairs grouped by primitive-pair count K, decreasing Q inside
@@ -165,11 +177,15 @@ namespace lible_b200
             {
                 uint32_t k, start, end;
                 int32_t mol;  // packed-matrix base of the group's molecule (batches)
+                int bucket;   // floor(log4 Q) of its pairs
+                double qmax, qmin;
             };
             std::vector<uint32_t> order;
-            std::vector<double> q, kpre;
+            std::vector<double> q;   // Q per position
+            std::vector<double> qs;  // per group, its Q values in decreasing order (same index range)
             std::vector<Group> groups;
             uint32_t *d_order = nullptr;
+            double *d_q = nullptr;   // Q per position (device)
         };
         struct ClassSet
         {
@@ -185,7 +201,8 @@ namespace lible_b200
         {
             int cb = 0, ck = 0, n_bra = 0;
             bool swap = false;  // RI plans: bra is the auxiliary class
-            long long n64 = 0, n32 = 0;
+            long long n64 = 0, n32 = 0;  // surviving quartets
+            long long t64 = 0, t32 = 0;  // launched tasks (whole bra groups; the kernels test each)
             double prim64 = 0, prim32 = 0, flops64 = 0, flops32 = 0;
             unsigned long long *prefix64 = nullptr, *prefix32 = nullptr;
             uint32_t *begin64 = nullptr, *begin32 = nullptr, *majors = nullptr;
@@ -202,7 +219,7 @@ namespace lible_b200
         };
         struct JKPlan
         {
-            double thr = 0;
+            double thr = 0, thr32 = 0;
             long long n_quartets = 0, n_fp32 = 0;
             double n_prim = 0, flops64 = 0, flops32 = 0;
             std::vector<JKClassPair> pairs;
@@ -218,7 +235,9 @@ namespace lible_b200
 
         void rebuildChunks(JKClassPair &cp, bool fp32, int mult);
         void assignBranches(JKPlan &plan);
-        void enqueueJK(JKPlan &plan, const double *D, double *J, double *K, bool mixed);
+        struct LaunchTimer;
+        void enqueueJK(JKPlan &plan, const double *D, double *J, double *K, bool mixed, LaunchTimer *timer = nullptr);
+        void gatherDab(const double *D);
         void applyTuneCache(JKPlan &plan);
         void requireSingle() const;
         void releaseGraph();
@@ -247,6 +266,8 @@ namespace lible_b200
         std::vector<int> sph_ofs_;
         std::vector<void *> persistent_;
 
+        double *staging_[4] = {};
+        size_t staging_n_[4] = {};
         static constexpr int kBranches = 4;
         cudaStream_t branch_[kBranches] = {};
         cudaEvent_t fork_ = nullptr, join_[kBranches] = {};

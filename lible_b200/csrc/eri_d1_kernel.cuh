@@ -74,6 +74,8 @@ namespace lible_b200
         {
             uint32_t ib, ik;
             decodeTask(a, task, ib, ik);
+            if (!inWindow(a, ib, ik, 0, false))
+                continue;
             const int32_t *bi = a.bra.info + 8 * ib;
             const int32_t *ki = a.ket.info + 8 * ik;
             double acc[12];

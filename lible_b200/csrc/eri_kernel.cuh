@@ -83,7 +83,7 @@ namespace lible_b200
         // register path: the order-L Boys table, staged once per block
         static constexpr size_t off_boys = (reg_smem + 15) / 16 * 16;
         static constexpr size_t boys_bytes = sizeof(T) == 8 ? sizeof(double) * kBoysTerms * kBoysPitch
-                                                            : sizeof(float) * kBoysTermsF * kBoysPitch;
+                                                            : sizeof(float) * (C::L + kBoysTermsF) * kBoysPitch;
         static constexpr int IK = W == 0 ? 0 : (C::HAB * C::SCD + G - 1) / G;
         static constexpr int IB = W == 0 ? 0 : (C::SAB * C::SCD + G - 1) / G;
         // shared-memory carve-up (bytes) for the group shape
@@ -148,28 +148,46 @@ namespace lible_b200
         return (((size_t)b0 * db1 + b1) * dk0 + k0) * dk1 + k1;
     }
 
+    // The bra pair's fields the digestion needs: first AOs of its shells, its molecule's block of
+    // the packed D, J, K (first element, dimension; the ket shares it) and, optionally, the D_ab
+    // block gathered in Schwarz order (dab[mn * dab_stride]) for coalesced reads.
+    struct BraFields
+    {
+        int oa, ob, n;
+        uint32_t base;
+        const double *dab;
+        int dab_stride;
+    };
+
+    __device__ __forceinline__ BraFields braFields(const int32_t *bi)
+    {
+        return BraFields{bi[0], bi[1], bi[7], (uint32_t)bi[6], nullptr, 0};
+    }
+
     // Generic digestion of one batch V[SAB][SCD] (values read through `val(e)`), with the
     // thread subset [tid, tid + stride, ...] producing outputs.  Implements
     //   J_ab += 2 f V D_cd,  J_cd += 2 f V D_ab,
     //   K_ac += f V D_bd, K_ad += f V D_bc, K_bc += f V D_ad, K_bd += f V D_ac
-    // into the unsymmetrised accumulators (J = A + A^T, K = B + B^T afterwards).
+    // into the unsymmetrised accumulators (J = A + A^T, K = B + B^T afterwards).  The K blocks are
+    // written transposed (rows of the ket's AOs) and their D factors read through the symmetry of D,
+    // so a ket-uniform warp whose bras are sorted by AO touches neighbouring columns of one row.
     // `ket_uniform` (serial form only): every lane of the warp holds a quartet with the same ket
-    // pair, so the J_cd sums are reduced across the warp and added once.
+    // pair, so the J_cd sums are reduced across the warp and added once.  `active` = false (serial,
+    // ket-uniform form only): the lane holds no quartet; it joins that reduction with zeros and
+    // writes nothing else.
     template <int SA, int SB, int SC, int SD, bool SERIAL, typename F>
-    __device__ __forceinline__ void digestJK(const QuartetArgs &a, double f, const int32_t *bi,
+    __device__ __forceinline__ void digestJK(const QuartetArgs &a, double f, const BraFields &bf,
                                              const int32_t *ki, F val, int tid, int stride,
-                                             bool ket_uniform = false)
+                                             bool ket_uniform = false, bool active = true)
     {
         if constexpr (SERIAL)
         {
             tid = 0;
             stride = 1;
         }
-        // the quartet's molecule block of the packed D, J, K (bra and ket share it): first element
-        // and dimension from the bra pair's info record
-        const int n = bi[7];
-        const size_t base = (uint32_t)bi[6];
-        const int oa = bi[0], ob = bi[1], oc = ki[0], od = ki[1];
+        const int n = bf.n;
+        const size_t base = bf.base;
+        const int oa = bf.oa, ob = bf.ob, oc = ki[0], od = ki[1];
         const double *D = a.D + base;
         double *const Jm = a.J + base;
         double *const Km = a.K + base;
@@ -199,7 +217,9 @@ namespace lible_b200
                 for (int m = 0; m < SA; m++)
 #pragma unroll
                     for (int nn = 0; nn < SB; nn++)
-                        s += val(((m * SB + nn) * SC + k) * SD + t) * __ldg(D + (size_t)(oa + m) * n + ob + nn);
+                        s += val(((m * SB + nn) * SC + k) * SD + t) *
+                             (bf.dab ? __ldg(bf.dab + (size_t)(m * SB + nn) * bf.dab_stride)
+                                     : __ldg(D + (size_t)(oa + m) * n + ob + nn));
                 dst = Jm + (size_t)(oc + k) * n + od + t;
                 w = 2.0 * f;
             }
@@ -210,8 +230,8 @@ namespace lible_b200
                 for (int nn = 0; nn < SB; nn++)
 #pragma unroll
                     for (int t = 0; t < SD; t++)
-                        s += val(((m * SB + nn) * SC + k) * SD + t) * __ldg(D + (size_t)(ob + nn) * n + od + t);
-                dst = Km + (size_t)(oa + m) * n + oc + k;
+                        s += val(((m * SB + nn) * SC + k) * SD + t) * __ldg(D + (size_t)(od + t) * n + ob + nn);
+                dst = Km + (size_t)(oc + k) * n + oa + m;
                 w = f;
             }
             else if (o < n3)
@@ -221,8 +241,8 @@ namespace lible_b200
                 for (int nn = 0; nn < SB; nn++)
 #pragma unroll
                     for (int k = 0; k < SC; k++)
-                        s += val(((m * SB + nn) * SC + k) * SD + t) * __ldg(D + (size_t)(ob + nn) * n + oc + k);
-                dst = Km + (size_t)(oa + m) * n + od + t;
+                        s += val(((m * SB + nn) * SC + k) * SD + t) * __ldg(D + (size_t)(oc + k) * n + ob + nn);
+                dst = Km + (size_t)(od + t) * n + oa + m;
                 w = f;
             }
             else if (o < n4)
@@ -232,8 +252,8 @@ namespace lible_b200
                 for (int m = 0; m < SA; m++)
 #pragma unroll
                     for (int t = 0; t < SD; t++)
-                        s += val(((m * SB + nn) * SC + k) * SD + t) * __ldg(D + (size_t)(oa + m) * n + od + t);
-                dst = Km + (size_t)(ob + nn) * n + oc + k;
+                        s += val(((m * SB + nn) * SC + k) * SD + t) * __ldg(D + (size_t)(od + t) * n + oa + m);
+                dst = Km + (size_t)(oc + k) * n + ob + nn;
                 w = f;
             }
             else
@@ -243,11 +263,11 @@ namespace lible_b200
                 for (int m = 0; m < SA; m++)
 #pragma unroll
                     for (int k = 0; k < SC; k++)
-                        s += val(((m * SB + nn) * SC + k) * SD + t) * __ldg(D + (size_t)(oa + m) * n + oc + k);
-                dst = Km + (size_t)(ob + nn) * n + od + t;
+                        s += val(((m * SB + nn) * SC + k) * SD + t) * __ldg(D + (size_t)(oc + k) * n + oa + m);
+                dst = Km + (size_t)(od + t) * n + ob + nn;
                 w = f;
             }
-            double v = w * s;
+            double v = active ? w * s : 0.0;
             if constexpr (SERIAL)
             {
                 if (ket_uniform && o >= n0 && o < n1)
@@ -258,6 +278,8 @@ namespace lible_b200
                     if ((threadIdx.x & 31) != 0)
                         continue;
                 }
+                else if (!active)
+                    continue;
             }
             atomicAdd(dst, v);
         }
@@ -321,53 +343,99 @@ namespace lible_b200
     __device__ __forceinline__ const float *braEs<float>(const QuartetArgs &a) { return a.bra_Efs; }
 
     // `sv` is the bra's structure-of-arrays entry (sv.z = 0: read the per-pair records instead).
+    // `nk` >= 0 is the bra's primitive-pair count from the per-position fields (the bra records are
+    // then read from the structure-of-arrays copies only); -1 reads the pair's primitive range.
     template <int LA, int LB, int LC, int LD, typename T>
     __device__ __forceinline__ void quartetThread(const QuartetArgs &a, uint32_t ib, uint32_t ik, int c0, T *V,
-                                                  const T *btab, uint4 sv)
+                                                  const T *btab, uint4 sv, int nk)
     {
         using C = Cls<LA, LB, LC, LD>;
         constexpr int CW = Shape<LA, LB, LC, LD, T>::CW;
 #pragma unroll
         for (int x = 0; x < C::SAB * CW; x++)
             V[x] = T(0);
-        const uint32_t p0 = a.bra.pofs[ib], p1 = a.bra.pofs[ib + 1];
+        uint32_t p0 = 0, p1 = (uint32_t)nk;
+        if (nk < 0)
+        {
+            p0 = a.bra.pofs[ib];
+            p1 = a.bra.pofs[ib + 1];
+        }
         const uint32_t q0 = a.ket.pofs[ik], q1 = a.ket.pofs[ik + 1];
         const T *Eb = braE<T>(a.bra);
         const T *Ek = ketE<T>(a.ket) + c0;
         const size_t sn = sv.z;
         for (uint32_t p = p0; p < p1; p++)
         {
-            PQ4 P;
-            if (sn)
+            PQ4 P;          // FP64 record
+            float Pf[8];    // FP32 record: p, 1/p, P hi, P lo
+            if constexpr (sizeof(T) == 8)
             {
-                const double *pp = a.bra_pPs + sv.x + (size_t)(p - p0) * 5 * sn;
-                P = {__ldg(pp), __ldg(pp + sn), __ldg(pp + 2 * sn), __ldg(pp + 3 * sn), __ldg(pp + 4 * sn)};
+                if (sn)
+                {
+                    const double *pp = a.bra_pPs + sv.x + (size_t)(p - p0) * 5 * sn;
+                    P = {__ldg(pp), __ldg(pp + sn), __ldg(pp + 2 * sn), __ldg(pp + 3 * sn), __ldg(pp + 4 * sn)};
+                }
+                else
+                    P = loadPQ(a.bra.pP, p);
             }
             else
-                P = loadPQ(a.bra.pP, p);
+            {
+                if (sn)
+                {
+                    const float *pp = a.bra_pPfs + sv.w + (size_t)(p - p0) * 8 * sn;
+#pragma unroll
+                    for (int f = 0; f < 8; f++)
+                        Pf[f] = __ldg(pp + f * sn);
+                }
+                else
+                {
+                    const float4 u = __ldg(reinterpret_cast<const float4 *>(a.bra.pPf) + 2 * (size_t)p);
+                    const float4 w = __ldg(reinterpret_cast<const float4 *>(a.bra.pPf) + 2 * (size_t)p + 1);
+                    Pf[0] = u.x; Pf[1] = u.y; Pf[2] = u.z; Pf[3] = u.w;
+                    Pf[4] = w.x; Pf[5] = w.y; Pf[6] = w.z; Pf[7] = w.w;
+                }
+            }
             T RxE[C::HAB * CW];
 #pragma unroll
             for (int x = 0; x < C::HAB * CW; x++)
                 RxE[x] = T(0);
             for (uint32_t q = q0; q < q1; q++)
             {
-                const PQ4 Q = loadPQ(a.ket.pP, q);
-                // alpha = pq/(p+q) and the prefactor 2 pi^{5/2} / (p q sqrt(p+q)) from one rsqrt
-                const double rs = rsqrt(P.x + Q.x);
-                const double alpha = P.x * Q.x * (rs * rs);
-                const double X = P.y - Q.y, Y = P.z - Q.z, Z = P.w - Q.w;
-                const double fac = 34.986836655249725 * rs * P.ip * Q.ip;
-                double F[C::L + 1];
-                if constexpr (sizeof(T) == 8)
-                    boysF<C::L, true>(alpha * (X * X + Y * Y + Z * Z), reinterpret_cast<const double *>(btab), F);
-                else
-                    boysF32<C::L>(alpha * (X * X + Y * Y + Z * Z), reinterpret_cast<const float *>(btab), F);
-                T Ft[C::L + 1];
-#pragma unroll
-                for (int k = 0; k <= C::L; k++)
-                    Ft[k] = T(F[k] * fac);
                 T R[C::NR];
-                hermiteR<C::L, T>(T(-2.0 * alpha), Ft, T(X), T(Y), T(Z), R);
+                if constexpr (sizeof(T) == 8)
+                {
+                    const PQ4 Q = loadPQ(a.ket.pP, q);
+                    // alpha = pq/(p+q) and the prefactor 2 pi^{5/2} / (p q sqrt(p+q)) from one rsqrt
+                    const double rs = rsqrt(P.x + Q.x);
+                    const double alpha = P.x * Q.x * (rs * rs);
+                    const double X = P.y - Q.y, Y = P.z - Q.z, Z = P.w - Q.w;
+                    const double fac = 34.986836655249725 * rs * P.ip * Q.ip;
+                    double F[C::L + 1];
+                    boysF<C::L, true>(alpha * (X * X + Y * Y + Z * Z), reinterpret_cast<const double *>(btab), F);
+                    double Ft[C::L + 1];
+#pragma unroll
+                    for (int k = 0; k <= C::L; k++)
+                        Ft[k] = F[k] * fac;
+                    hermiteR<C::L, double>(-2.0 * alpha, Ft, X, Y, Z, reinterpret_cast<double *>(R));
+                }
+                else
+                {
+                    // FP32 geometry: P - Q from the hi/lo parts keeps float relative accuracy
+                    const float4 u = __ldg(reinterpret_cast<const float4 *>(a.ket.pPf) + 2 * (size_t)q);
+                    const float4 w = __ldg(reinterpret_cast<const float4 *>(a.ket.pPf) + 2 * (size_t)q + 1);
+                    const float rs = rsqrtf(Pf[0] + u.x);
+                    const float alpha = Pf[0] * u.x * (rs * rs);
+                    const float X = (Pf[2] - u.z) + (Pf[5] - w.y);
+                    const float Y = (Pf[3] - u.w) + (Pf[6] - w.z);
+                    const float Z = (Pf[4] - w.x) + (Pf[7] - w.w);
+                    const float fac = 34.986836655249725f * rs * Pf[1] * u.y;
+                    float F[C::L + 1];
+                    boysF32<C::L>(alpha * (X * X + Y * Y + Z * Z), reinterpret_cast<const float *>(btab), F);
+#pragma unroll
+                    for (int k = 0; k <= C::L; k++)
+                        F[k] *= fac;
+                    hermiteR<C::L, float>(-2.0f * alpha, F, X, Y, Z, reinterpret_cast<float *>(R));
+                }
                 const T *ec = Ek + (size_t)q * C::HCD * C::SCD;
 #pragma unroll
                 for (int hp = 0; hp < C::HCD; hp++)
@@ -824,13 +892,41 @@ namespace lible_b200
                 const bool valid = slot < QPW && t < end;
                 uint32_t ib = 0, ik = 0;
                 T V[C::SAB * CW];
+                BraFields bf{0, 0, 0, 0, nullptr, 0};
+                bool bsame = false;
+                bool active = false;  // a valid task inside the launch's Schwarz window
                 if (valid)
                 {
                     int my = cur;
                     uint32_t pos;
                     decodeCursor(a, t, my, ib, ik, pos);
+                    active = inWindow(a, ib, ik, pos, true);
                     const uint4 sv = a.bra_soa ? __ldg(a.bra_soa + pos) : make_uint4(0, 0, 0, 0);
-                    quartetThread<LA, LB, LC, LD, T>(a, ib, ik, member * CW, V, btab, sv);
+                    int nk = -1;
+                    if (a.bra_soa2)
+                    {
+                        // one coalesced 16-byte load instead of the pair's info record and
+                        // primitive range
+                        const int4 si = __ldg(a.bra_soa2 + pos);
+                        bf = BraFields{si.x, si.y, si.w & 0xffff, (uint32_t)si.z,
+                                       a.bra_Dab ? a.bra_Dab + pos : nullptr, a.bra_npos};
+                        nk = (si.w >> 16) & 0x7fff;
+                        bsame = si.w < 0;
+                    }
+                    else if (a.mode == kJK)
+                    {
+                        const int32_t *bi0 = a.bra.info + 8 * ib;
+                        bf = braFields(bi0);
+                        bsame = bi0[4] == bi0[5];
+                    }
+                    if (active)
+                        quartetThread<LA, LB, LC, LD, T>(a, ib, ik, member * CW, V, btab, sv, nk);
+                    else
+                    {
+#pragma unroll
+                        for (int x = 0; x < C::SAB * CW; x++)
+                            V[x] = T(0);
+                    }
                 }
                 if (!a.list)
                     cur = advanceMajor(a, base + QPW < end ? base + QPW : end - 1, cur);
@@ -838,7 +934,7 @@ namespace lible_b200
                 const int32_t *ki = a.ket.info + 8 * ik;
                 if (a.mode == kStore)
                 {
-                    if (valid)
+                    if (active)
                     {
 #pragma unroll
                         for (int m = 0; m < C::SAB; m++)
@@ -862,18 +958,19 @@ namespace lible_b200
                     if (a.mode == kJK)
                     {
                         if (uniform)
-                            digestJK<C::SA, C::SB, C::SC, C::SD, true>(a, quartetWeight(a, ib, ik), bi, ki, val, 0, 1,
-                                                                       true);
-                        else if (valid)
-                            digestJK<C::SA, C::SB, C::SC, C::SD, true>(a, quartetWeight(a, ib, ik), bi, ki, val, 0, 1);
+                            digestJK<C::SA, C::SB, C::SC, C::SD, true>(a, quartetWeight(a, bsame, ib, ik), bf, ki, val,
+                                                                       0, 1, true, active);
+                        else if (active)
+                            digestJK<C::SA, C::SB, C::SC, C::SD, true>(a, quartetWeight(a, bsame, ib, ik), bf, ki, val,
+                                                                       0, 1);
                     }
-                    else if (valid)
+                    else if (active)
                         digestRI<C::SA, C::SB, C::SC, C::SD, true>(a, bi, ki, val, 0, 1);
                 }
                 else
                 {
                     // gather the quartet's columns in shared memory, then digest with the group
-                    if (valid)
+                    if (active)
                     {
 #pragma unroll
                         for (int m = 0; m < C::SAB; m++)
@@ -882,12 +979,12 @@ namespace lible_b200
                                 vs[m * C::SCD + member * CW + c] = (double)V[m * CW + c];
                     }
                     __syncwarp();
-                    if (valid)
+                    if (active)
                     {
                         auto val = [&](int e) { return vs[e]; };
                         if (a.mode == kJK)
-                            digestJK<C::SA, C::SB, C::SC, C::SD, false>(a, quartetWeight(a, ib, ik), bi, ki, val,
-                                                                        member, GT);
+                            digestJK<C::SA, C::SB, C::SC, C::SD, false>(a, quartetWeight(a, bsame, ib, ik), bf, ki,
+                                                                        val, member, GT);
                         else
                             digestRI<C::SA, C::SB, C::SC, C::SD, false>(a, bi, ki, val, member, GT);
                     }
@@ -931,6 +1028,8 @@ namespace lible_b200
             {
                 uint32_t ib, ik;
                 decodeCursor(a, t, cur, ib, ik);
+                if (!inWindow(a, ib, ik, 0, false))
+                    continue;
                 double v[S::TPW2][2];
                 quartetGroupMMA<LA, LB, LC, LD>(a, ib, ik, smem, v);
                 // element (m, c) of the batch held by this thread: tile rows / columns
@@ -964,8 +1063,8 @@ namespace lible_b200
                     const int32_t *ki = a.ket.info + 8 * ik;
                     auto val = [&](int e) { return vs[e]; };
                     if (a.mode == kJK)
-                        digestJK<C::SA, C::SB, C::SC, C::SD, false>(a, quartetWeight(a, ib, ik), bi, ki, val,
-                                                                    threadIdx.x, S::G);
+                        digestJK<C::SA, C::SB, C::SC, C::SD, false>(a, quartetWeight(a, ib, ik), braFields(bi), ki,
+                                                                    val, threadIdx.x, S::G);
                     else
                         digestRI<C::SA, C::SB, C::SC, C::SD, false>(a, bi, ki, val, threadIdx.x, S::G);
                 }
@@ -1007,6 +1106,8 @@ namespace lible_b200
             {
                 uint32_t ib, ik;
                 decodeCursor(a, t, cur, ib, ik);
+                if (!inWindow(a, ib, ik, 0, false))
+                    continue;
                 T vals[S::IB];
                 quartetGroup<LA, LB, LC, LD, T>(a, ib, ik, smem, vals);
                 if (a.mode == kStore)
@@ -1038,8 +1139,8 @@ namespace lible_b200
                     const int32_t *ki = a.ket.info + 8 * ik;
                     auto val = [&](int e) { return (double)vs[e]; };
                     if (a.mode == kJK)
-                        digestJK<C::SA, C::SB, C::SC, C::SD, false>(a, quartetWeight(a, ib, ik), bi, ki, val,
-                                                                    threadIdx.x, S::G);
+                        digestJK<C::SA, C::SB, C::SC, C::SD, false>(a, quartetWeight(a, ib, ik), braFields(bi), ki,
+                                                                    val, threadIdx.x, S::G);
                     else
                         digestRI<C::SA, C::SB, C::SC, C::SD, false>(a, bi, ki, val, threadIdx.x, S::G);
                 }

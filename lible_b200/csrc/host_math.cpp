@@ -135,16 +135,25 @@ namespace lible_b200
         return g;
     }
 
-    // The FP32 tables: the first kBoysTermsF coefficients of every order, rounded to float.
+    // The FP32 table: F_j(x_i) for j = 0 .. kBoysMaxN + kBoysTermsF - 1 at the same integer points,
+    // unscaled and rounded to float, layout [j][kBoysPitch].  FP32 quartets evaluate every order
+    // n <= N from its own Taylor sum sum_k F_{n+k}(x_i) (x_i - x)^k / k!, so no recursion runs in FP32.
     std::vector<float> boysGridF()
     {
         const std::vector<double> g = boysGrid();
-        std::vector<float> f((size_t)(kBoysMaxN + 1) * kBoysTermsF * kBoysPitch);
-        for (int N = 0; N <= kBoysMaxN; N++)
-            for (int k = 0; k < kBoysTermsF; k++)
-                for (int i = 0; i < kBoysPitch; i++)
-                    f[((size_t)N * kBoysTermsF + k) * kBoysPitch + i] =
-                        (float)g[((size_t)N * kBoysTerms + k) * kBoysPitch + i];
+        const int nj = kBoysMaxN + kBoysTermsF;
+        std::vector<float> f((size_t)nj * kBoysPitch);
+        for (int j = 0; j < nj; j++)
+        {
+            // F_j(x_i) = c_N[k][i] k! with N + k = j, taken from the lowest available order N
+            const int N = std::max(0, j - (kBoysTerms - 1));
+            const int k = j - N;
+            double fact = 1.0;
+            for (int q = 2; q <= k; q++)
+                fact *= q;
+            for (int i = 0; i < kBoysPitch; i++)
+                f[(size_t)j * kBoysPitch + i] = (float)(g[((size_t)N * kBoysTerms + k) * kBoysPitch + i] * fact);
+        }
         return f;
     }
 }

@@ -32,7 +32,8 @@ namespace lible_b200
     // and the 31 possible rows of a warp's lookups fall on few distinct words (mostly broadcasts).
     // The reference grid is finer (step 0.01, 7 terms about the lower point,
     // src/lible/ints/boys_function.hpp:112-122); both are accurate to the last bits.
-    // The FP32 tables hold the first kBoysTermsF coefficients as floats (truncation 0.5^10/10! < 3e-10).
+    // The FP32 table holds F_j(x_i) unscaled, j < kBoysMaxN + kBoysTermsF; FP32 quartets sum
+    // kBoysTermsF Taylor terms per order (truncation 0.5^10/10! < 3e-10).
     constexpr int kBoysMaxN = 14;
     constexpr int kBoysTerms = 16;
     constexpr int kBoysTermsF = 10;

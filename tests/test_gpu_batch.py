@@ -109,3 +109,17 @@ def test_autotune_keeps_results_and_cache_round_trips(tmp_path):
     L.set_tune_cache(b2, cache)
     J2, K2, _ = L.jk(b2, Dp)
     assert np.abs(J2 - J).max() <= 1e-12 and np.abs(K2 - K).max() <= 1e-12
+
+
+def test_jk_profile_times_every_launch_and_returns_the_build():
+    Z, xyz, rng = water_cluster(3, 17)
+    s = L.Structure("cc-pvdz", Z, xyz, units="bohr")
+    D = random_density(s.nao, 15, rng)
+    J, K, _ = L.jk(s, D, 1e-12, "mixed")
+    Jp, Kp = np.empty_like(J), np.empty_like(K)
+    prof = L.jk_profile(s, D, 1e-12, "mixed", J=Jp, K=Kp)
+    assert np.abs(Jp - J).max() <= 1e-12 and np.abs(Kp - K).max() <= 1e-12
+    plan = L.jk_plan(s, 1e-12, "mixed")
+    assert sum(r["tasks"] for r in prof) == plan["n_quartets"]
+    assert any(r["fp32"] for r in prof) and all(r["ms"] > 0 for r in prof)
+    assert abs(sum(r["flops"] for r in prof) - plan["flops_fp64"] - plan["flops_fp32"]) <= 1e-6 * plan["flops_fp64"]
