@@ -29,7 +29,7 @@ N_WATERS, SEED, OCC = 32, 2024, 160
 SCHWARZ, FP32_THR = 1e-12, 1e-4
 # DRAM bytes (read + write) per launch of the dominant class kernels at this workload, from one ncu
 # capture each (dram__bytes_read.sum + dram__bytes_write.sum); the working set stays in L2
-DOMINANT_TRAFFIC = {(1, 0, 0, 0): None}
+DOMINANT_TRAFFIC = {(1, 0, 0, 0): 33.66e6}
 WORKLOAD = {"workload": "direct J+K build, (H2O)_32 water cluster, cc-pVDZ", "n_waters": N_WATERS, "nao": 768,
             "seed": SEED, "occupied": OCC, "schwarz": SCHWARZ, "fp32_threshold": FP32_THR,
             "geometry": "5.7 bohr cubic lattice, random rotations, +-0.6 bohr jitter",

@@ -79,7 +79,7 @@ def build(jobs=None, verbose=False):
     if errors:
         raise RuntimeError("nvcc failed:\n" + "\n".join(errors)[:20000])
     if not os.path.exists(LIB) or os.path.getmtime(LIB) < max(os.path.getmtime(o) for o in objs):
-        cmd = [nvcc()] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart", "-lcusolver"]
+        cmd = [nvcc()] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart", "-lcusolver", "-lcublas"]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError("link failed:\n" + r.stderr + r.stdout)

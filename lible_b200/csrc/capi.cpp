@@ -4,8 +4,10 @@
 #include "engine_api.hpp"
 
 #include <cuda_runtime.h>
+#include <cublas_v2.h>
 #include <cusolverDn.h>
 
+#include <algorithm>
 #include <cstring>
 #include <memory>
 #include <map>
@@ -23,6 +25,11 @@ struct lible_gpu_ctx
 {
     std::unique_ptr<Engine> eng;
     std::string err;
+    // last RI-J metric solve: 0 Cholesky, 1 eigendecomposition with cutoff; eigenvalue range (or
+    // the squared range of the Cholesky diagonal, a lower bound of the condition number); dropped
+    int rij_method = -1;
+    double rij_lo = 0, rij_hi = 0;
+    int rij_dropped = 0;
 };
 
 namespace
@@ -562,6 +569,7 @@ int lible_gpu_jk(lible_gpu_ctx *ctx, const double *D, double *J, double *K, cons
         e.jk(d.ptr, j.ptr, k.ptr, toOpts(opts), &st);
         j.copyOut();
         k.copyOut();
+        e.checkStatus();
         if (stats)
         {
             stats->n_quartets = st.n_quartets;
@@ -789,6 +797,21 @@ int lible_gpu_jk_energy_backward(lible_gpu_ctx *ctx, const double *D, const libl
     });
 }
 
+int lible_gpu_rij_last_solve(lible_gpu_ctx *ctx, int *method, double *lo, double *hi, int *dropped)
+{
+    if (!ctx)
+        return LIBLE_GPU_EINVAL;
+    if (method)
+        *method = ctx->rij_method;
+    if (lo)
+        *lo = ctx->rij_lo;
+    if (hi)
+        *hi = ctx->rij_hi;
+    if (dropped)
+        *dropped = ctx->rij_dropped;
+    return LIBLE_GPU_OK;
+}
+
 int lible_gpu_ri_contract(lible_gpu_ctx *ctx, const double *D, const double *dcoef, double schwarz_threshold,
                           double *gamma, double *J)
 {
@@ -837,6 +860,11 @@ int lible_gpu_rij(lible_gpu_ctx *ctx, const double *D, double schwarz_threshold,
         }
         e.eri2(metric);
         e.sync();
+        // keep a copy of the metric: a failed Cholesky overwrites it
+        double *metric2 = nullptr;
+        cudaCheck(cudaMalloc(&metric2, na * na * sizeof(double)), "cudaMalloc");
+        cudaCheck(cudaMemcpyAsync(metric2, metric, na * na * sizeof(double), cudaMemcpyDeviceToDevice, e.stream()),
+                  "copy");
         cusolverDnHandle_t h;
         if (cusolverDnCreate(&h) != CUSOLVER_STATUS_SUCCESS)
             throw EngineError(kStatusCuda, "cusolverDnCreate failed");
@@ -845,19 +873,99 @@ int lible_gpu_rij(lible_gpu_ctx *ctx, const double *D, double schwarz_threshold,
         cusolverDnDpotrf_bufferSize(h, CUBLAS_FILL_MODE_LOWER, (int)na, metric, (int)na, &lwork);
         cudaCheck(cudaMalloc(&work, std::max(lwork, 1) * sizeof(double)), "cudaMalloc");
         cusolverDnDpotrf(h, CUBLAS_FILL_MODE_LOWER, (int)na, metric, (int)na, work, lwork, info);
-        cusolverDnDpotrs(h, CUBLAS_FILL_MODE_LOWER, (int)na, 1, metric, (int)na, rhs, (int)na, info);
         int hinfo = 0;
         cudaCheck(cudaMemcpyAsync(&hinfo, info, sizeof(int), cudaMemcpyDeviceToHost, e.stream()), "info");
-        cudaCheck(cudaStreamSynchronize(e.stream()), "potrs");
+        cudaCheck(cudaStreamSynchronize(e.stream()), "potrf");
+        if (hinfo == 0)
+        {
+            cusolverDnDpotrs(h, CUBLAS_FILL_MODE_LOWER, (int)na, 1, metric, (int)na, rhs, (int)na, info);
+            // condition lower bound from the Cholesky diagonal
+            std::vector<double> dg(na);
+            cudaCheck(cudaMemcpy2DAsync(dg.data(), sizeof(double), metric, (na + 1) * sizeof(double), sizeof(double),
+                                        na, cudaMemcpyDeviceToHost, e.stream()),
+                      "diag");
+            cudaCheck(cudaStreamSynchronize(e.stream()), "potrs");
+            double lo = 1e300, hi = 0;
+            for (double v : dg)
+            {
+                lo = std::min(lo, v * v);
+                hi = std::max(hi, v * v);
+            }
+            ctx->rij_method = 0;
+            ctx->rij_lo = lo;
+            ctx->rij_hi = hi;
+            ctx->rij_dropped = 0;
+        }
+        else
+        {
+            // not numerically positive definite: d = V diag(1/w) V^T gamma over the eigenpairs with
+            // w > 1e-12 * max(w), the rest dropped
+            double *w = nullptr;
+            cudaCheck(cudaMalloc(&w, na * sizeof(double)), "cudaMalloc");
+            int lw2 = 0;
+            cusolverDnDsyevd_bufferSize(h, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, (int)na, metric2,
+                                        (int)na, w, &lw2);
+            cudaFree(work);
+            cudaCheck(cudaMalloc(&work, std::max(lw2, 1) * sizeof(double)), "cudaMalloc");
+            cusolverDnDsyevd(h, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, (int)na, metric2, (int)na, w, work,
+                             lw2, info);
+            std::vector<double> hw(na);
+            cudaCheck(cudaMemcpyAsync(&hinfo, info, sizeof(int), cudaMemcpyDeviceToHost, e.stream()), "info");
+            cudaCheck(cudaMemcpyAsync(hw.data(), w, na * 8, cudaMemcpyDeviceToHost, e.stream()), "w");
+            cudaCheck(cudaStreamSynchronize(e.stream()), "syevd");
+            cudaFree(w);
+            if (hinfo != 0)
+            {
+                cusolverDnDestroy(h);
+                cudaFree(work);
+                cudaFree(metric);
+                cudaFree(metric2);
+                cudaFree(info);
+                cudaFree(rhs);
+                throw EngineError(kStatusInternal, "eigendecomposition of the RI metric failed (info " +
+                                                       std::to_string(hinfo) + ")");
+            }
+            const double wmax = *std::max_element(hw.begin(), hw.end());
+            // eigenvectors are the columns of the column-major result; c = V^T gamma, c_k /= w_k
+            // (0 for dropped pairs), d = V c
+            std::vector<double> scale(na, 0.0);
+            int dropped = 0;
+            double lo = 1e300;
+            for (size_t k = 0; k < na; k++)
+                if (hw[k] > 1e-12 * wmax)
+                {
+                    scale[k] = 1.0 / hw[k];
+                    lo = std::min(lo, hw[k]);
+                }
+                else
+                    dropped++;
+            double *c = nullptr, *dscale = nullptr;
+            cudaCheck(cudaMalloc(&c, na * 8), "cudaMalloc");
+            cudaCheck(cudaMalloc(&dscale, na * 8), "cudaMalloc");
+            cudaCheck(cudaMemcpyAsync(dscale, scale.data(), na * 8, cudaMemcpyHostToDevice, e.stream()), "copy");
+            cublasHandle_t bh;
+            if (cublasCreate(&bh) != CUBLAS_STATUS_SUCCESS)
+                throw EngineError(kStatusCuda, "cublasCreate failed");
+            cublasSetStream(bh, e.stream());
+            const double one = 1.0, zero = 0.0;
+            cublasDgemv(bh, CUBLAS_OP_T, (int)na, (int)na, &one, metric2, (int)na, rhs, 1, &zero, c, 1);
+            // c_k *= scale_k as a diagonal matrix-vector product
+            cublasDdgmm(bh, CUBLAS_SIDE_LEFT, (int)na, 1, c, (int)na, dscale, 1, c, (int)na);
+            cublasDgemv(bh, CUBLAS_OP_N, (int)na, (int)na, &one, metric2, (int)na, c, 1, &zero, rhs, 1);
+            cudaCheck(cudaStreamSynchronize(e.stream()), "eigen solve");
+            cublasDestroy(bh);
+            cudaFree(c);
+            cudaFree(dscale);
+            ctx->rij_method = 1;
+            ctx->rij_lo = lo;
+            ctx->rij_hi = wmax;
+            ctx->rij_dropped = dropped;
+        }
         cusolverDnDestroy(h);
         cudaFree(work);
         cudaFree(metric);
+        cudaFree(metric2);
         cudaFree(info);
-        if (hinfo != 0)
-        {
-            cudaFree(rhs);
-            throw EngineError(kStatusInternal, "Cholesky of the RI metric failed (info " + std::to_string(hinfo) + ")");
-        }
         if (dcoef)
         {
             if (isDevice(dcoef))

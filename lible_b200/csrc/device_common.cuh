@@ -90,6 +90,8 @@ namespace lible_b200
         const double *bra_qpair;
         const double *ket_qpair;
         double q_lo, q_hi;
+        // ket E tiles zero-padded to the DMMA layout of this class (null: stage from Et)
+        const double *ket_EtP;
         // epilogue
         int mode;
         int flags;                        // kStore: bit0 swap bra shells, bit1 swap ket shells, bit2 swap bra/ket

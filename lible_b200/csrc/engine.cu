@@ -303,6 +303,20 @@ namespace lible_b200
         }
     }
 
+    // Ket E tiles zero-padded to the DMMA operand layout of their class: out[pp][rows][pitch] with
+    // the Et[pp][h'][c] entries for h' < hcd, c < scd and zeros elsewhere (bulk-copied whole).
+    __global__ void padEtKernel(const double *Et, long long n_pp, int hcd, int scd, int rows, int pitch, double *out)
+    {
+        const long long total = n_pp * rows * pitch;
+        for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+             idx += (long long)gridDim.x * blockDim.x)
+        {
+            const long long pp = idx / ((long long)rows * pitch);
+            const int r = (int)((idx / pitch) % rows), c = (int)(idx % pitch);
+            out[idx] = (r < hcd && c < scd) ? Et[((size_t)pp * hcd + r) * scd + c] : 0.0;
+        }
+    }
+
     // D_ab blocks of every bra pair of a class in Schwarz order: Dab[mn * n_pos + position].
     __global__ void dabGatherKernel(const double *D, const int4 *soa2, long long n_pos, int sa, int sb, double *Dab)
     {
@@ -416,6 +430,8 @@ namespace lible_b200
             cudaCheck(cudaEventCreateWithFlags(&join_[b], cudaEventDisableTiming), "cudaEventCreate");
         }
         cudaCheck(cudaEventCreateWithFlags(&fork_, cudaEventDisableTiming), "cudaEventCreate");
+        d_status_ = devAlloc<int>(1);
+        cudaCheck(cudaMemset(d_status_, 0, sizeof(int)), "memset");
         boys_ = devUpload(boysGrid(), stream_);
         boys_f_ = devUpload(boysGridF(), stream_);
         std::vector<int> rc;
@@ -445,6 +461,7 @@ namespace lible_b200
             cudaFree(p);
         for (double *p : staging_)
             cudaFree(p);
+        cudaFree(d_status_);
         cudaFree(boys_);
         cudaFree(boys_f_);
         cudaFree(sph_rc_);
@@ -472,7 +489,8 @@ namespace lible_b200
             for (void *p : {(void *)d.pP, (void *)d.ab, (void *)d.pofs, (void *)d.info, (void *)d.coords,
                             (void *)d.E, (void *)d.Et, (void *)d.Ef, (void *)d.Etf, (void *)d.E1,
                             (void *)d.E1t, (void *)d.Q, (void *)d.pPs, (void *)d.Es, (void *)d.Efs,
-                            (void *)d.soa, (void *)d.pPf, (void *)d.pPfs, (void *)d.soa2, (void *)d.Dab})
+                            (void *)d.soa, (void *)d.pPf, (void *)d.pPfs, (void *)d.soa2, (void *)d.Dab,
+                            (void *)d.EtP})
                 cudaFree(p);
         for (auto &o : cs.orders)
         {
@@ -669,6 +687,16 @@ namespace lible_b200
         const int bs = 64;
         ecoeffKernel<<<(unsigned)((pc.n_ppairs + bs - 1) / bs), bs, 0, stream_>>>(ea);
         cudaCheck(cudaGetLastError(), "ecoeffKernel");
+        {
+            // padded ket tiles for the bulk copies of the DMMA class kernels
+            const int hcd = nherm(pc.la + pc.lb), scd = nsph(pc.la) * nsph(pc.lb);
+            const int rows = (hcd + 3) / 4 * 4, pitch = kPitch(scd);
+            const long long tot = (long long)pc.n_ppairs * rows * pitch;
+            d.EtP = devAlloc<double>((size_t)std::max<long long>(tot, 1));
+            padEtKernel<<<(unsigned)std::min<long long>((tot + 255) / 256, 65535), 256, 0, stream_>>>(
+                d.Et, (long long)pc.n_ppairs, hcd, scd, rows, pitch, d.EtP);
+            cudaCheck(cudaGetLastError(), "padEtKernel");
+        }
         cudaCheck(cudaStreamSynchronize(stream_), "ecoeffKernel");
         cudaFree(exps);
         cudaFree(coeffs);
@@ -1546,6 +1574,7 @@ namespace lible_b200
         cudaCheck(cudaMemsetAsync(plan.counters, 0, 2 * plan.pairs.size() * sizeof(unsigned long long), stream_),
                   "memset");
         gatherDab(D);
+        cudaCheck(cudaMemsetAsync(d_status_, 0, sizeof(int), stream_), "memset");
         cudaCheck(cudaEventRecord(fork_, stream_), "fork");
         bool used[kBranches] = {};
         if (!timer)
@@ -1596,6 +1625,8 @@ namespace lible_b200
             a.bra_soa2 = B.soa2;
             a.bra_Dab = B.Dab;
             a.bra_npos = (int)B.n_pairs;
+            a.ket_EtP = Kc.EtP;
+            a.status = d_status_;
             LaunchFn f64 = lookupFwd64(cp.tb, cp.tk);
             if (!f64)
                 throw EngineError(kStatusUnsupported, "quartet class not instantiated");
@@ -1856,6 +1887,8 @@ namespace lible_b200
                         a.bra_soa2 = B.soa2;
                         a.bra_Dab = B.Dab;
                         a.bra_npos = (int)B.n_pairs;
+                        a.ket_EtP = Kc.EtP;
+                        a.status = d_status_;
                         float t_min = 1e30f;
                         for (int rep = 0; rep < 2; rep++)
                         {
@@ -2010,6 +2043,7 @@ namespace lible_b200
             cudaCheck(cudaMemsetAsync(gamma_dev, 0, naux_ * sizeof(double), stream_), "memset");
         if (J_dev)
             cudaCheck(cudaMemsetAsync(J_dev, 0, n * n * sizeof(double), stream_), "memset");
+        cudaCheck(cudaMemsetAsync(d_status_, 0, sizeof(int), stream_), "memset");
         cudaCheck(cudaMemsetAsync(plan.counters, 0, 2 * plan.pairs.size() * sizeof(unsigned long long), stream_),
                   "memset");
         for (size_t ip = 0; ip < plan.pairs.size(); ip++)
@@ -2035,6 +2069,8 @@ namespace lible_b200
             a.bra_qpos = bs.orders[cp.cb].d_q;
             a.bra_qpair = B.Q;
             a.ket_qpair = K.Q;
+            a.ket_EtP = K.EtP;
+            a.status = d_status_;
             a.q_lo = plan.thr;
             a.q_hi = HUGE_VAL;
             a.aux_side = cp.swap ? 1 : 0;
@@ -2070,6 +2106,17 @@ namespace lible_b200
             cudaCheck(cudaGetLastError(), "symmetrize");
         }
         cudaCheck(cudaStreamSynchronize(stream_), "ri");
+        checkStatus();
+    }
+
+    // Reads the device status word of the last calls (bounded waits that gave up set it).
+    void Engine::checkStatus()
+    {
+        int st = 0;
+        cudaCheck(cudaMemcpyAsync(&st, d_status_, sizeof(int), cudaMemcpyDeviceToHost, stream_), "status");
+        cudaCheck(cudaStreamSynchronize(stream_), "status");
+        if (st != 0)
+            throw EngineError(kStatusTimeout, "a bounded device wait gave up (bulk copy did not complete)");
     }
 
     double *Engine::staging(int slot, size_t n)

@@ -124,5 +124,6 @@ namespace lible_b200
         int4 *soa2 = nullptr;       // per Schwarz position: ao_a, ao_b, packed-block base,
                                     // N_m | K << 16 | (same shell) << 31
         double *Dab = nullptr;      // per J/K call: D_ab of every pair, [mn][position]
+        double *EtP = nullptr;      // Et zero-padded to the DMMA tile layout [ppair][rows][pitch]
     };
 }

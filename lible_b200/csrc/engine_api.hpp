@@ -165,6 +165,8 @@ namespace lible_b200
                         double schwarz);
 
         void sync();
+        // Throws kStatusTimeout when a kernel reported a bounded wait that gave up (synchronises).
+        void checkStatus();
         // Cached device staging buffer `slot` (0..3) of at least n doubles (grow-only).
         double *staging(int slot, size_t n);
 
@@ -266,6 +268,7 @@ namespace lible_b200
         std::vector<int> sph_ofs_;
         std::vector<void *> persistent_;
 
+        int *d_status_ = nullptr;
         double *staging_[4] = {};
         size_t staging_n_[4] = {};
         static constexpr int kBranches = 4;

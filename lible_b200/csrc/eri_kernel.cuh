@@ -62,14 +62,18 @@ namespace lible_b200
         static constexpr int WM = (TILES + 5) / 6 < 1 ? 1 : ((TILES + 5) / 6 > 8 ? 8 : (TILES + 5) / 6);
         static constexpr int TPW = (TILES + WM - 1) / WM, TPW2 = (TILES2 + WM - 1) / WM;
         static constexpr int P_RM = kPitch(C::HAB), P_EC = kPitch(C::SCD), P_EA = mPitch(C::HAB);
+        static constexpr size_t a16(size_t x) { return (x + 15) / 16 * 16; }
         static constexpr size_t m_off_rb = 0;                                            // 2 x NR
-        static constexpr size_t m_off_rm = m_off_rb + 8 * 2 * C::NR;                     // KT*4 x P_RM
-        static constexpr size_t m_off_ec = m_off_rm + 8 * (size_t)KT * 4 * P_RM;         // KT*4 x P_EC
-        static constexpr size_t m_off_ea = m_off_ec + 8 * (size_t)KT * 4 * P_EC;         // MT2*8 x P_EA
-        static constexpr size_t m_off_rx = m_off_ea + 8 * (size_t)MT2 * 8 * P_EA;        // MT*8 x P_EC
-        static constexpr size_t m_off_ix = m_off_rx + 8 * (size_t)MT * 8 * P_EC;         // HCD x HAB int16
-        static constexpr size_t m_off_ht = (m_off_ix + 2 * C::HCD * C::HAB + 15) / 16 * 16; // NR char4
-        static constexpr size_t m_smem = m_off_ht + 4 * C::NR;
+        static constexpr size_t m_off_rm = a16(m_off_rb + 8 * 2 * C::NR);                // KT*4 x P_RM
+        static constexpr size_t m_off_ec = a16(m_off_rm + 8 * (size_t)KT * 4 * P_RM);    // KT*4 x P_EC
+        static constexpr size_t m_off_ea = a16(m_off_ec + 8 * (size_t)KT * 4 * P_EC);    // MT2*8 x P_EA
+        static constexpr size_t m_off_rx = a16(m_off_ea + 8 * (size_t)MT2 * 8 * P_EA);   // MT*8 x P_EC
+        static constexpr size_t m_off_ix = a16(m_off_rx + 8 * (size_t)MT * 8 * P_EC);    // HCD x HAB int16
+        static constexpr size_t m_off_ht = a16(m_off_ix + 2 * C::HCD * C::HAB);          // NR char4
+        static constexpr size_t m_off_mb = a16(m_off_ht + 4 * C::NR);                    // mbarrier
+        static constexpr size_t m_smem = m_off_mb + 16;
+        // bytes of one padded ket E tile (KT*4 rows of P_EC doubles), the unit of the bulk copy
+        static constexpr unsigned ec_tile_bytes = 8u * KT * 4 * P_EC;
         static constexpr int W = GT ? 0
                                  : MMA ? WM
                                  : ((C::HAB * C::SCD + C::SAB * C::SCD) <= 64 * 32)     ? 1
@@ -97,6 +101,49 @@ namespace lible_b200
         static constexpr size_t smem = W == 0 ? off_boys + boys_bytes : MMA ? m_smem : off_ht + 4 * C::NR;
         static_assert(!MMA || m_smem <= 227 * 1024, "DMMA shared-memory layout exceeds 227 KB");
     };
+
+    // ---------------------------------------------------------------------------------------
+    // Bulk asynchronous copies (the TMA engine's 1-D form, cp.async.bulk) into shared memory,
+    // completed on an mbarrier.  Addresses and sizes are multiples of 16 bytes.
+    __device__ __forceinline__ void mbarInit(uint64_t *mbar)
+    {
+        const unsigned a = (unsigned)__cvta_generic_to_shared(mbar);
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(a) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+
+    // One thread: announce `bytes` on the barrier and start the copy global -> shared.
+    __device__ __forceinline__ void bulkLoad(void *dst_smem, const void *src_gmem, unsigned bytes, uint64_t *mbar)
+    {
+        const unsigned d = (unsigned)__cvta_generic_to_shared(dst_smem);
+        const unsigned m = (unsigned)__cvta_generic_to_shared(mbar);
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(m), "r"(bytes) : "memory");
+        asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(d),
+                     "l"(src_gmem), "r"(bytes), "r"(m)
+                     : "memory");
+    }
+
+    // Waits for the barrier phase with parity `phase`; gives up after a bounded number of polls,
+    // records kStatusTimeout-style failure in *status and returns false.
+    __device__ __forceinline__ bool mbarWait(uint64_t *mbar, unsigned phase, int *status)
+    {
+        const unsigned m = (unsigned)__cvta_generic_to_shared(mbar);
+        for (int it = 0; it < (1 << 20); it++)
+        {
+            unsigned done;
+            asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                         "selp.u32 %0, 1, 0, p;\n\t}"
+                         : "=r"(done)
+                         : "r"(m), "r"(phase)
+                         : "memory");
+            if (done)
+                return true;
+        }
+        if (status)
+            atomicExch(status, 6);
+        return false;
+    }
 
     // D += A B for one 8x8x4 FP64 tile (PTX mma.sync.aligned.m8n8k4.row.col.f64): lane l holds
     // A[l/4][l%4], B[l%4][l/4] and D[l/4][2(l%4) + {0,1}].
@@ -643,9 +690,12 @@ namespace lible_b200
     // primitives in registers (acc).  Per bra primitive the R.E tiles go to shared memory and the
     // warps accumulate their 8x8 tiles of E_bra . (R.E) into `v`.  Padded rows and columns of the
     // operand tiles are zeroed once per block and never written afterwards.
+    // `phase` is the parity of the block's mbarrier phase awaited next; it lives as long as the block
+    // (one completed phase per ket primitive of every quartet), so it is carried across calls.
     template <int LA, int LB, int LC, int LD>
     __device__ __forceinline__ void quartetGroupMMA(const QuartetArgs &a, uint32_t ib, uint32_t ik,
-                                                    unsigned char *smem, double (&v)[Shape<LA, LB, LC, LD, double>::TPW2][2])
+                                                    unsigned char *smem, double (&v)[Shape<LA, LB, LC, LD, double>::TPW2][2],
+                                                    unsigned &phase)
     {
         using C = Cls<LA, LB, LC, LD>;
         using S = Shape<LA, LB, LC, LD, double>;
@@ -658,6 +708,10 @@ namespace lible_b200
         double *rx = reinterpret_cast<double *>(smem + S::m_off_rx);
         const short *rix = reinterpret_cast<const short *>(smem + S::m_off_ix);
         const char4 *ht = reinterpret_cast<const char4 *>(smem + S::m_off_ht);
+        uint64_t *mbar = reinterpret_cast<uint64_t *>(smem + S::m_off_mb);
+        // the padded ket E tiles arrive by bulk copy (issued at the top of a ket-primitive iteration,
+        // overlapping the Boys function and the R recursion); without them the block stages the tile
+        const double *ket_tiles = a.ket_EtP;
 
 #pragma unroll
         for (int i = 0; i < S::TPW2; i++)
@@ -675,6 +729,8 @@ namespace lible_b200
                 acc[i][0] = acc[i][1] = 0.0;
             for (uint32_t q = q0; q < q1; q++)
             {
+                if (ket_tiles && tid == 0)
+                    bulkLoad(ec, ket_tiles + (size_t)q * (S::ec_tile_bytes / 8), S::ec_tile_bytes, mbar);
                 const PQ4 Q = loadPQ(a.ket.pP, q);
                 const double rs = rsqrt(P.x + Q.x);
                 const double alpha = P.x * Q.x * (rs * rs);
@@ -742,8 +798,14 @@ namespace lible_b200
                     const double r = cur[ix & 0x7fff];
                     rm[(e / C::HAB) * S::P_RM + e % C::HAB] = (ix & 0x8000) ? -r : r;
                 }
-                for (int e = tid; e < C::HCD * C::SCD; e += G)
-                    ec[(e / C::SCD) * S::P_EC + e % C::SCD] = __ldg(a.ket.Et + (size_t)q * C::HCD * C::SCD + e);
+                if (ket_tiles)
+                {
+                    mbarWait(mbar, phase, a.status);
+                    phase ^= 1u;
+                }
+                else
+                    for (int e = tid; e < C::HCD * C::SCD; e += G)
+                        ec[(e / C::SCD) * S::P_EC + e % C::SCD] = __ldg(a.ket.Et + (size_t)q * C::HCD * C::SCD + e);
                 groupSync(G);
                 // acc[tile] += R^T[h][h'] E_ket[h'][c] over h' (A = rm viewed transposed, row-major)
 #pragma unroll
@@ -824,6 +886,8 @@ namespace lible_b200
                 ix |= 0x8000;
             rix[e] = (short)ix;
         }
+        if (threadIdx.x == 0)
+            mbarInit(reinterpret_cast<uint64_t *>(smem + S::m_off_mb));
         __syncthreads();
     }
 
@@ -1021,6 +1085,7 @@ namespace lible_b200
             buildGroupTablesMMA<LA, LB, LC, LD>(smem);
             double *vs = reinterpret_cast<double *>(smem + S::m_off_rx);
             const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, r8 = lane >> 2, k4 = lane & 3;
+            unsigned phase = 0;  // parity of the block mbarrier's next phase
             // one quartet at a time for the whole block, tasks [start, end) of a chunk
             auto processRange = [&](long long start, long long end) {
             int cur = 0;
@@ -1031,7 +1096,7 @@ namespace lible_b200
                 if (!inWindow(a, ib, ik, 0, false))
                     continue;
                 double v[S::TPW2][2];
-                quartetGroupMMA<LA, LB, LC, LD>(a, ib, ik, smem, v);
+                quartetGroupMMA<LA, LB, LC, LD>(a, ib, ik, smem, v, phase);
                 // element (m, c) of the batch held by this thread: tile rows / columns
 #pragma unroll
                 for (int i = 0; i < S::TPW2; i++)

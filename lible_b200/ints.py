@@ -407,6 +407,14 @@ def rij(structure, D, schwarz=1e-12):
     return J, g, d
 
 
+def rij_last_solve(structure):
+    """How the last rij() solved the metric equations: {'method': 'cholesky'|'eigen', 'lo', 'hi', 'dropped'}."""
+    m, lo, hi, dr = ctypes.c_int(), ctypes.c_double(), ctypes.c_double(), ctypes.c_int()
+    _call(structure, "lible_gpu_rij_last_solve", ctypes.byref(m), ctypes.byref(lo), ctypes.byref(hi), ctypes.byref(dr))
+    return {"method": {0: "cholesky", 1: "eigen"}.get(m.value, None), "lo": lo.value, "hi": hi.value,
+            "dropped": dr.value}
+
+
 def ri_contract(structure, D=None, dcoef=None, schwarz=1e-12):
     """gamma_P = sum (mn|P) D_mn (if D is given) and J_mn = sum_P (mn|P) d_P (if dcoef is given)."""
     n, na = structure.nao, structure.naux
