@@ -188,6 +188,62 @@ def run_batch(steps, warmup, dev):
             "max_abs_dJ_vs_single": err}
 
 
+def run_rij(Z, xyz, D, J64, steps):
+    """RI-J of the (H2O)_32 workload with the even-tempered s-f auxiliary basis (0.1 * 2.5^k,
+    k = 0..11 per l and atom): wall time of one lible_gpu_rij call from host D to host J (both
+    three-centre contractions, the (P|Q) build and its solve), and the RI error against the direct
+    FP64 J of the same run."""
+    from lible_b200 import ints as L
+    from lible_b200.workloads import even_tempered_aux
+
+    t0 = time.perf_counter()
+    s = L.Structure("cc-pvdz", Z, xyz, even_tempered_aux(Z), units="bohr")
+    setup = time.perf_counter() - t0
+    Jri, _, _ = L.rij(s, D, SCHWARZ)  # warm-up: plans, Schwarz factors of the auxiliary classes
+    ts = []
+    for _ in range(max(1, steps)):
+        t = time.perf_counter()
+        Jri, _, _ = L.rij(s, D, SCHWARZ)
+        ts.append(time.perf_counter() - t)
+    return {"workload": "RI-J, (H2O)_32 cc-pVDZ, even-tempered s-f auxiliary basis, FP64", "naux": s.naux,
+            "setup_s": setup, "rij_s": float(np.mean(ts)), "solve": L.rij_last_solve(s),
+            "dEJ_Eh_vs_direct": float(0.5 * np.sum(D * (Jri - J64))),
+            "dJ_fro_vs_direct": float(np.linalg.norm(Jri - J64))}
+
+
+def run_gradient(steps, seed=2024):
+    """J/K energy gradient of (H2O)_8 cc-pVTZ (464 AOs, occupation 40): wall time of the backward
+    pass (derivative integrals contracted with the two-particle density on the device) and its
+    agreement with central finite differences (step 1e-4 bohr) of the forward energy on two
+    coordinates."""
+    from lible_b200 import ints as L
+    from lible_b200.workloads import random_density, water_cluster
+
+    Z, xyz, rng = water_cluster(8, seed)
+    s = L.Structure("cc-pvtz", Z, xyz, units="bohr")
+    D = random_density(s.nao, 40, rng)
+    g = L.jk_energy_backward(s, D, SCHWARZ)
+    ts = []
+    for _ in range(max(1, steps)):
+        t = time.perf_counter()
+        g = L.jk_energy_backward(s, D, SCHWARZ)
+        ts.append(time.perf_counter() - t)
+    t = time.perf_counter()
+    L.jk_energy_forward(s, D, SCHWARZ)
+    t_fwd = time.perf_counter() - t
+    h, worst = 1e-4, 0.0
+    for atom, x in [(0, 0), (13, 2)]:
+        e = []
+        for sgn in (1, -1):
+            c = xyz.copy()
+            c[atom, x] += sgn * h
+            e.append(L.jk_energy_forward(L.Structure("cc-pvtz", Z, c, units="bohr"), D, SCHWARZ))
+        worst = max(worst, abs((e[0] - e[1]) / (2 * h) - g[atom, x]))
+    return {"workload": "J/K energy gradient, (H2O)_8 cc-pVTZ, occupation 40, FP64", "nao": s.nao,
+            "backward_s": float(np.mean(ts)), "forward_energy_s": t_fwd,
+            "max_abs_fd_minus_analytic_Eh_per_bohr": worst, "fd_step_bohr": h}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -196,6 +252,7 @@ def main():
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the 64-molecule batched measurement")
+    ap.add_argument("--no-extras", action="store_true", help="skip the RI-J and gradient measurements")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
@@ -300,6 +357,10 @@ def main():
 
     # the batch is seconds per build: two timed steps after one warm-up keep the run short
     batch = None if args.no_batch else run_batch(min(args.steps, 2), 1, dev)
+    rij = gradient = None
+    if not args.no_extras and rank == 0:
+        rij = run_rij(Z, xyz, D, J64, min(args.steps, 2))
+        gradient = run_gradient(min(args.steps, 2))
 
     if rank != 0:
         if dist:
@@ -358,6 +419,8 @@ def main():
                 "h2d_bytes_per_step": int(D.nbytes), "d2h_bytes_per_step": int(2 * D.nbytes),
                 "path": "lible_b200.jk -> lible_gpu_jk with pinned host D/J/K"},
         "batch": batch,
+        "rij": rij,
+        "gradient": gradient,
         "gpu_launches": int(plan["n_launches"]) * args.steps,
         "clocks": clocks,
     }

@@ -213,10 +213,12 @@ int lible_gpu_jk_energy_backward(lible_gpu_ctx *ctx, const double *D, const libl
 int lible_gpu_rij(lible_gpu_ctx *ctx, const double *D, double schwarz_threshold, double *J, double *gamma,
                   double *dcoef);
 /* How the last lible_gpu_rij solved (P|Q) d = gamma: method 0 = Cholesky (lo, hi = smallest and
- * largest squared diagonal of the factor, a lower bound of the condition number hi/lo); method 1 =
- * eigendecomposition (used when the metric is not numerically positive definite: lo, hi = smallest
- * kept and largest eigenvalue, `dropped` eigenpairs below 1e-12 of the largest left out); -1 = none. */
-int lible_gpu_rij_last_solve(lible_gpu_ctx *ctx, int *method, double *lo, double *hi, int *dropped);
+ * largest squared diagonal of the factor, a lower bound of the condition number hi/lo); 2 = the
+ * metric was not numerically positive definite and Cholesky of (P|Q) + shift I succeeded (shift =
+ * 1e-11 of the largest diagonal element); 1 = eigendecomposition (when that also failed: lo, hi =
+ * smallest kept and largest eigenvalue, `dropped` eigenpairs below 1e-12 of the largest left out);
+ * -1 = none yet.  Any output may be NULL. */
+int lible_gpu_rij_last_solve(lible_gpu_ctx *ctx, int *method, double *lo, double *hi, int *dropped, double *shift);
 /* The two contractions separately (either output may be NULL). */
 int lible_gpu_ri_contract(lible_gpu_ctx *ctx, const double *D, const double *dcoef, double schwarz_threshold,
                           double *gamma, double *J);

@@ -70,7 +70,7 @@ SIGNATURES = {
     "lible_gpu_jk_plan_classes": [P, ctypes.POINTER(JKOpts), P, P, P, P, P, P],
     "lible_gpu_fp64_peak": [P, ctypes.POINTER(D), ctypes.POINTER(D)],
     "lible_gpu_ri_contract": [P, P, P, D, P, P],
-    "lible_gpu_rij_last_solve": [P, P, P, P, P],
+    "lible_gpu_rij_last_solve": [P, P, P, P, P, P],
     "lible_host_spherical_trafo": [I, P, P, P, P],
     "lible_host_shell_norms": [I, I, P, P, P],
     "lible_host_pair_classes": [S, S, I, P, P, I, I, P, P, P, P],

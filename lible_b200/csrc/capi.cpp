@@ -30,6 +30,7 @@ struct lible_gpu_ctx
     int rij_method = -1;
     double rij_lo = 0, rij_hi = 0;
     int rij_dropped = 0;
+    double rij_shift = 0;
 };
 
 namespace
@@ -125,6 +126,45 @@ namespace
             if (owned)
                 cudaFree(ptr);
         }
+    };
+
+    // Owning device buffer (freed on scope exit, also when a check throws).
+    template <class T>
+    struct DevBuf
+    {
+        T *p = nullptr;
+        explicit DevBuf(size_t n) { reset(n); }
+        void reset(size_t n)
+        {
+            cudaFree(p);
+            p = nullptr;
+            cudaCheck(cudaMalloc(&p, std::max<size_t>(n, 1) * sizeof(T)), "cudaMalloc");
+        }
+        ~DevBuf() { cudaFree(p); }
+        DevBuf(const DevBuf &) = delete;
+        DevBuf &operator=(const DevBuf &) = delete;
+    };
+
+    struct SolverHandle
+    {
+        cusolverDnHandle_t h = nullptr;
+        SolverHandle()
+        {
+            if (cusolverDnCreate(&h) != CUSOLVER_STATUS_SUCCESS)
+                throw EngineError(kStatusCuda, "cusolverDnCreate failed");
+        }
+        ~SolverHandle() { cusolverDnDestroy(h); }
+    };
+
+    struct BlasHandle
+    {
+        cublasHandle_t h = nullptr;
+        BlasHandle()
+        {
+            if (cublasCreate(&h) != CUBLAS_STATUS_SUCCESS)
+                throw EngineError(kStatusCuda, "cublasCreate failed");
+        }
+        ~BlasHandle() { cublasDestroy(h); }
     };
 
     std::vector<std::array<double, 3>> coords(int n_atoms, const double *xyz, int units)
@@ -756,15 +796,8 @@ int lible_gpu_jk_energy_forward(lible_gpu_ctx *ctx, const double *D, const lible
         DevArray d(D, nn, true, e.stream(), &e, 0);
         DevArray j(J, nn, false, e.stream(), &e, 1);
         DevArray k(K, nn, false, e.stream(), &e, 2);
-        double *jp = j.ptr, *kp = k.ptr, *tmp = nullptr;
-        if (!jp || !kp)
-        {
-            cudaCheck(cudaMalloc(&tmp, 2 * nn * sizeof(double)), "cudaMalloc");
-            if (!jp)
-                jp = tmp;
-            if (!kp)
-                kp = tmp + nn;
-        }
+        // without caller J / K the context's staging buffers of those slots hold them
+        double *jp = j.ptr ? j.ptr : e.staging(1, nn), *kp = k.ptr ? k.ptr : e.staging(2, nn);
         e.jk(d.ptr, jp, kp, toOpts(opts), nullptr);
         std::vector<double> hd(nn), hj(nn), hk(nn);
         cudaCheck(cudaMemcpyAsync(hd.data(), d.ptr, nn * 8, cudaMemcpyDeviceToHost, e.stream()), "D2H");
@@ -779,8 +812,7 @@ int lible_gpu_jk_energy_forward(lible_gpu_ctx *ctx, const double *D, const lible
             j.copyOut();
         if (K)
             k.copyOut();
-        if (tmp)
-            cudaFree(tmp);
+        e.checkStatus();
     });
 }
 
@@ -797,10 +829,12 @@ int lible_gpu_jk_energy_backward(lible_gpu_ctx *ctx, const double *D, const libl
     });
 }
 
-int lible_gpu_rij_last_solve(lible_gpu_ctx *ctx, int *method, double *lo, double *hi, int *dropped)
+int lible_gpu_rij_last_solve(lible_gpu_ctx *ctx, int *method, double *lo, double *hi, int *dropped, double *shift)
 {
     if (!ctx)
         return LIBLE_GPU_EINVAL;
+    if (shift)
+        *shift = ctx->rij_shift;
     if (method)
         *method = ctx->rij_method;
     if (lo)
@@ -844,11 +878,10 @@ int lible_gpu_rij(lible_gpu_ctx *ctx, const double *D, double schwarz_threshold,
         const size_t n = e.nao(), na = e.naux();
         DevArray d(D, n * n, true, e.stream());
         DevArray j(J, n * n, false, e.stream());
-        double *metric = nullptr, *rhs = nullptr, *work = nullptr;
-        int *info = nullptr;
-        cudaCheck(cudaMalloc(&metric, na * na * sizeof(double)), "cudaMalloc");
-        cudaCheck(cudaMalloc(&rhs, na * sizeof(double)), "cudaMalloc");
-        cudaCheck(cudaMalloc(&info, sizeof(int)), "cudaMalloc");
+        DevBuf<double> metric_b(na * na), rhs_b(na), work_b(1);
+        DevBuf<int> info_b(1);
+        double *metric = metric_b.p, *rhs = rhs_b.p;
+        int *info = info_b.p;
         e.riContract(d.ptr, nullptr, rhs, nullptr, schwarz_threshold);
         if (gamma)
         {
@@ -861,21 +894,43 @@ int lible_gpu_rij(lible_gpu_ctx *ctx, const double *D, double schwarz_threshold,
         e.eri2(metric);
         e.sync();
         // keep a copy of the metric: a failed Cholesky overwrites it
-        double *metric2 = nullptr;
-        cudaCheck(cudaMalloc(&metric2, na * na * sizeof(double)), "cudaMalloc");
+        DevBuf<double> metric2_b(na * na);
+        double *metric2 = metric2_b.p;
         cudaCheck(cudaMemcpyAsync(metric2, metric, na * na * sizeof(double), cudaMemcpyDeviceToDevice, e.stream()),
                   "copy");
-        cusolverDnHandle_t h;
-        if (cusolverDnCreate(&h) != CUSOLVER_STATUS_SUCCESS)
-            throw EngineError(kStatusCuda, "cusolverDnCreate failed");
+        SolverHandle sh;
+        cusolverDnHandle_t h = sh.h;
         cusolverDnSetStream(h, e.stream());
         int lwork = 0;
         cusolverDnDpotrf_bufferSize(h, CUBLAS_FILL_MODE_LOWER, (int)na, metric, (int)na, &lwork);
-        cudaCheck(cudaMalloc(&work, std::max(lwork, 1) * sizeof(double)), "cudaMalloc");
+        work_b.reset((size_t)std::max(lwork, 1));
+        double *work = work_b.p;
         cusolverDnDpotrf(h, CUBLAS_FILL_MODE_LOWER, (int)na, metric, (int)na, work, lwork, info);
         int hinfo = 0;
         cudaCheck(cudaMemcpyAsync(&hinfo, info, sizeof(int), cudaMemcpyDeviceToHost, e.stream()), "info");
         cudaCheck(cudaStreamSynchronize(e.stream()), "potrf");
+        double shift = 0.0;
+        if (hinfo != 0)
+        {
+            // not numerically positive definite: retry with the diagonal raised by 1e-11 of its largest
+            // element (Tikhonov regularisation), before resorting to an eigendecomposition
+            std::vector<double> dg(na);
+            cudaCheck(cudaMemcpy2DAsync(dg.data(), sizeof(double), metric2, (na + 1) * sizeof(double),
+                                        sizeof(double), na, cudaMemcpyDeviceToHost, e.stream()),
+                      "diag");
+            cudaCheck(cudaStreamSynchronize(e.stream()), "diag");
+            shift = 1e-11 * *std::max_element(dg.begin(), dg.end());
+            for (double &v : dg)
+                v += shift;
+            cudaCheck(cudaMemcpyAsync(metric, metric2, na * na * sizeof(double), cudaMemcpyDeviceToDevice, e.stream()),
+                      "copy");
+            cudaCheck(cudaMemcpy2DAsync(metric, (na + 1) * sizeof(double), dg.data(), sizeof(double), sizeof(double),
+                                        na, cudaMemcpyHostToDevice, e.stream()),
+                      "diag");
+            cusolverDnDpotrf(h, CUBLAS_FILL_MODE_LOWER, (int)na, metric, (int)na, work, lwork, info);
+            cudaCheck(cudaMemcpyAsync(&hinfo, info, sizeof(int), cudaMemcpyDeviceToHost, e.stream()), "info");
+            cudaCheck(cudaStreamSynchronize(e.stream()), "potrf");
+        }
         if (hinfo == 0)
         {
             cusolverDnDpotrs(h, CUBLAS_FILL_MODE_LOWER, (int)na, 1, metric, (int)na, rhs, (int)na, info);
@@ -891,37 +946,31 @@ int lible_gpu_rij(lible_gpu_ctx *ctx, const double *D, double schwarz_threshold,
                 lo = std::min(lo, v * v);
                 hi = std::max(hi, v * v);
             }
-            ctx->rij_method = 0;
+            ctx->rij_method = shift > 0 ? 2 : 0;
             ctx->rij_lo = lo;
             ctx->rij_hi = hi;
             ctx->rij_dropped = 0;
+            ctx->rij_shift = shift;
         }
         else
         {
             // not numerically positive definite: d = V diag(1/w) V^T gamma over the eigenpairs with
             // w > 1e-12 * max(w), the rest dropped
-            double *w = nullptr;
-            cudaCheck(cudaMalloc(&w, na * sizeof(double)), "cudaMalloc");
+            DevBuf<double> w_b(na);
+            double *w = w_b.p;
             int lw2 = 0;
             cusolverDnDsyevd_bufferSize(h, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, (int)na, metric2,
                                         (int)na, w, &lw2);
-            cudaFree(work);
-            cudaCheck(cudaMalloc(&work, std::max(lw2, 1) * sizeof(double)), "cudaMalloc");
+            work_b.reset((size_t)std::max(lw2, 1));
+            work = work_b.p;
             cusolverDnDsyevd(h, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, (int)na, metric2, (int)na, w, work,
                              lw2, info);
             std::vector<double> hw(na);
             cudaCheck(cudaMemcpyAsync(&hinfo, info, sizeof(int), cudaMemcpyDeviceToHost, e.stream()), "info");
             cudaCheck(cudaMemcpyAsync(hw.data(), w, na * 8, cudaMemcpyDeviceToHost, e.stream()), "w");
             cudaCheck(cudaStreamSynchronize(e.stream()), "syevd");
-            cudaFree(w);
             if (hinfo != 0)
             {
-                cusolverDnDestroy(h);
-                cudaFree(work);
-                cudaFree(metric);
-                cudaFree(metric2);
-                cudaFree(info);
-                cudaFree(rhs);
                 throw EngineError(kStatusInternal, "eigendecomposition of the RI metric failed (info " +
                                                        std::to_string(hinfo) + ")");
             }
@@ -939,13 +988,11 @@ int lible_gpu_rij(lible_gpu_ctx *ctx, const double *D, double schwarz_threshold,
                 }
                 else
                     dropped++;
-            double *c = nullptr, *dscale = nullptr;
-            cudaCheck(cudaMalloc(&c, na * 8), "cudaMalloc");
-            cudaCheck(cudaMalloc(&dscale, na * 8), "cudaMalloc");
+            DevBuf<double> c_b(na), dscale_b(na);
+            double *c = c_b.p, *dscale = dscale_b.p;
             cudaCheck(cudaMemcpyAsync(dscale, scale.data(), na * 8, cudaMemcpyHostToDevice, e.stream()), "copy");
-            cublasHandle_t bh;
-            if (cublasCreate(&bh) != CUBLAS_STATUS_SUCCESS)
-                throw EngineError(kStatusCuda, "cublasCreate failed");
+            BlasHandle bhh;
+            cublasHandle_t bh = bhh.h;
             cublasSetStream(bh, e.stream());
             const double one = 1.0, zero = 0.0;
             cublasDgemv(bh, CUBLAS_OP_T, (int)na, (int)na, &one, metric2, (int)na, rhs, 1, &zero, c, 1);
@@ -953,19 +1000,13 @@ int lible_gpu_rij(lible_gpu_ctx *ctx, const double *D, double schwarz_threshold,
             cublasDdgmm(bh, CUBLAS_SIDE_LEFT, (int)na, 1, c, (int)na, dscale, 1, c, (int)na);
             cublasDgemv(bh, CUBLAS_OP_N, (int)na, (int)na, &one, metric2, (int)na, c, 1, &zero, rhs, 1);
             cudaCheck(cudaStreamSynchronize(e.stream()), "eigen solve");
-            cublasDestroy(bh);
-            cudaFree(c);
-            cudaFree(dscale);
+
             ctx->rij_method = 1;
             ctx->rij_lo = lo;
             ctx->rij_hi = wmax;
             ctx->rij_dropped = dropped;
+            ctx->rij_shift = 0;
         }
-        cusolverDnDestroy(h);
-        cudaFree(work);
-        cudaFree(metric);
-        cudaFree(metric2);
-        cudaFree(info);
         if (dcoef)
         {
             if (isDevice(dcoef))
@@ -975,7 +1016,6 @@ int lible_gpu_rij(lible_gpu_ctx *ctx, const double *D, double schwarz_threshold,
         }
         e.riContract(nullptr, rhs, nullptr, j.ptr, schwarz_threshold);
         j.copyOut();
-        cudaFree(rhs);
     });
 }
 

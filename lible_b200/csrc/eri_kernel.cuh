@@ -240,6 +240,21 @@ namespace lible_b200
         double *const Km = a.K + base;
         constexpr int n0 = SA * SB, n1 = n0 + SC * SD, n2 = n1 + SA * SC, n3 = n2 + SA * SD,
                       n4 = n3 + SB * SC, n5 = n4 + SB * SD;
+        // ket-uniform warps over AO-sorted bras: neighbouring lanes with the same shell a form a run
+        // (a run starts where a differs from the left neighbour's) and write the same K_ac / K_ad
+        // elements; each run is summed with a shuffle tree and added once by its first lane
+        int run_last = 0;
+        bool run_head = true;
+        if constexpr (SERIAL)
+            if (ket_uniform)
+            {
+                const int lane = threadIdx.x & 31;
+                const int left = __shfl_up_sync(0xffffffffu, oa, 1);
+                run_head = lane == 0 || left != oa;
+                const unsigned heads = __ballot_sync(0xffffffffu, run_head);
+                const unsigned later = lane == 31 ? 0u : heads & (0xffffffffu << (lane + 1));
+                run_last = later ? __ffs(later) - 2 : 31;
+            }
 #pragma unroll
         for (int o = tid; o < n5; o += stride)
         {
@@ -323,6 +338,20 @@ namespace lible_b200
                     for (int sh = 16; sh > 0; sh >>= 1)
                         v += __shfl_xor_sync(0xffffffffu, v, sh);
                     if ((threadIdx.x & 31) != 0)
+                        continue;
+                }
+                else if (ket_uniform && o >= n1 && o < n3)
+                {
+                    // K_ac, K_ad: sum over the run of lanes with this lane's shell a
+                    const int lane = threadIdx.x & 31;
+#pragma unroll
+                    for (int off = 1; off < 32; off <<= 1)
+                    {
+                        const double u = __shfl_down_sync(0xffffffffu, v, off);
+                        if (lane + off <= run_last)
+                            v += u;
+                    }
+                    if (!run_head || v == 0.0)
                         continue;
                 }
                 else if (!active)

@@ -39,6 +39,37 @@ def _f64(x):
     return np.ascontiguousarray(np.asarray(x, dtype=np.float64))
 
 
+def basis_atoms(name, atomic_nrs, root=None):
+    """Per-atom shells [(l, exps, coeffs), ...] of a named basis, read from <root>/<family>/<name>.txt
+    in the reference's text format (element=Z, blocks "l=L n=K" of K exponent/coefficient lines,
+    end=Z; src/lible/ints/basis_sets.cpp:214-277)."""
+    root = root or BASIS_ROOT
+    path = None
+    for fam in sorted(os.listdir(root)):
+        cand = os.path.join(root, fam, name.lower() + ".txt")
+        if os.path.exists(cand):
+            path = cand
+    if path is None:
+        raise LibleGpuError(1, f"basis set {name} not found under {root}")
+    elements, cur, z = {}, None, None
+    lines = iter(open(path).read().split("\n"))
+    for line in lines:
+        line = line.strip()
+        if line.startswith("element="):
+            z, cur = int(line.split("=")[1]), []
+        elif line.startswith("end="):
+            elements[z] = cur
+        elif line.startswith("l="):
+            parts = dict(p.split("=") for p in line.split())
+            l, n = int(parts["l"]), int(parts["n"])
+            rows = [next(lines).split() for _ in range(n)]
+            cur.append((l, [float(r[0]) for r in rows], [float(r[1]) for r in rows]))
+    try:
+        return [list(elements[int(zz)]) for zz in atomic_nrs]
+    except KeyError as e:
+        raise LibleGpuError(1, f"element {e.args[0]} missing from basis set {name}") from None
+
+
 class Structure:
     """lible::ints::Structure (src/lible/ints/structure.hpp:18-62).
 
@@ -57,6 +88,8 @@ class Structure:
         if len(Z) != len(xyz):
             raise ValueError("number of atomic numbers does not match the number of coordinates")
         u = 0 if units == "angstrom" else 1
+        if isinstance(basis_set, str) and basis_set_aux is not None and not isinstance(basis_set_aux, str):
+            basis_set = basis_atoms(basis_set, Z, basis_root)
         if isinstance(basis_set, str):
             rc = self._lib.lible_gpu_set_structure_named(
                 ctx, (basis_root or BASIS_ROOT).encode(), basis_set.encode(),
@@ -408,11 +441,13 @@ def rij(structure, D, schwarz=1e-12):
 
 
 def rij_last_solve(structure):
-    """How the last rij() solved the metric equations: {'method': 'cholesky'|'eigen', 'lo', 'hi', 'dropped'}."""
-    m, lo, hi, dr = ctypes.c_int(), ctypes.c_double(), ctypes.c_double(), ctypes.c_int()
-    _call(structure, "lible_gpu_rij_last_solve", ctypes.byref(m), ctypes.byref(lo), ctypes.byref(hi), ctypes.byref(dr))
-    return {"method": {0: "cholesky", 1: "eigen"}.get(m.value, None), "lo": lo.value, "hi": hi.value,
-            "dropped": dr.value}
+    """How the last rij() solved the metric equations:
+    {'method': 'cholesky'|'cholesky+shift'|'eigen', 'lo', 'hi', 'dropped', 'shift'}."""
+    m, lo, hi, dr, sh = ctypes.c_int(), ctypes.c_double(), ctypes.c_double(), ctypes.c_int(), ctypes.c_double()
+    _call(structure, "lible_gpu_rij_last_solve", ctypes.byref(m), ctypes.byref(lo), ctypes.byref(hi), ctypes.byref(dr),
+          ctypes.byref(sh))
+    return {"method": {0: "cholesky", 1: "eigen", 2: "cholesky+shift"}.get(m.value, None), "lo": lo.value,
+            "hi": hi.value, "dropped": dr.value, "shift": sh.value}
 
 
 def ri_contract(structure, D=None, dcoef=None, schwarz=1e-12):

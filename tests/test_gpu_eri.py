@@ -236,3 +236,33 @@ def test_mixed_precision_jk_error_small():
     Em = np.sum(D * (0.5 * Jm - 0.25 * Km))
     assert abs(E - Em) <= 1e-8
     assert np.linalg.norm(Jm - J) <= 1e-6 and np.linalg.norm(Km - K) <= 1e-6
+
+
+def test_rij_even_tempered_aux_vs_reference():
+    # the s-f even-tempered auxiliary basis of the mixed-precision RI-J workload (0.1 * 2.5^k,
+    # k = 0..11 per l), on one water
+    from lible_b200.workloads import even_tempered_aux
+    from oracle import port
+
+    aux = even_tempered_aux(WATER_Z)
+    s = L.Structure("cc-pvdz", WATER_Z, WATER_BOHR, aux, units="bohr")
+    assert s.naux == 3 * 12 * (1 + 3 + 5 + 7)
+    r = R.RefStructure(port.read_basis("cc-pvdz", WATER_Z), WATER_Z, WATER_BOHR, aux=aux)
+    rng = np.random.default_rng(4)
+    D = random_density(s.nao, 5, rng)
+    J, gamma, dcoef = L.rij(s, D, schwarz=0.0)
+    gr = r.rij_gamma(D)
+    assert np.abs(gamma - gr).max() <= 1e-10 * max(1.0, np.abs(gr).max())
+    # the same solve in numpy on the reference metric
+    M = r.eri2()
+    info = L.rij_last_solve(s)
+    if info["method"] == "cholesky":
+        dref = np.linalg.solve(M, gr)
+    elif info["method"] == "cholesky+shift":
+        dref = np.linalg.solve(M + info["shift"] * np.eye(len(M)), gr)
+    else:
+        w, V = np.linalg.eigh(M)
+        keep = w > 1e-12 * w.max()
+        dref = V[:, keep] @ ((V[:, keep].T @ gr) / w[keep])
+    Jref = r.rij_j(dref)
+    assert np.abs(J - Jref).max() <= 1e-6 * max(1.0, np.abs(Jref).max())
