@@ -1243,7 +1243,7 @@ namespace lible_b200
     {
         for (auto &cp : p.pairs)
             for (void *x : {(void *)cp.prefix64, (void *)cp.prefix32, (void *)cp.begin64, (void *)cp.begin32,
-                            (void *)cp.majors, (void *)cp.chunks64, (void *)cp.chunks32})
+                            (void *)cp.majors, (void *)cp.chunks64, (void *)cp.chunks32, (void *)cp.chunksD1})
                 cudaFree(x);
         cudaFree(p.counters);
         p = JKPlan();
@@ -1998,9 +1998,19 @@ namespace lible_b200
         JKPlan &plan = jkPlan(schwarz, 0.0, false);
         const size_t n = nao_;
         cudaCheck(cudaMemsetAsync(grad_dev, 0, 3 * n_atoms_ * sizeof(double), stream_), "memset");
-        for (const auto &cp : plan.pairs)
+        cudaCheck(cudaMemsetAsync(plan.counters, 0, 2 * plan.pairs.size() * sizeof(unsigned long long), stream_),
+                  "memset");
+        for (size_t ip = 0; ip < plan.pairs.size(); ip++)
         {
+            auto &cp = plan.pairs[ip];
             const auto &B = cs.dev[cp.cb], &K = cs.dev[cp.ck];
+            if (!cp.chunksD1 && cp.t64 > 0)
+            {
+                // one quartet per block at a time: chunks of the heaviest quartet up to 8 tasks
+                auto ch = costChunks(cp.run64, cp.cost, 1, 8);
+                cp.n_chunksD1 = (long long)ch.size() - 1;
+                cp.chunksD1 = devUpload(ch, stream_);
+            }
             QuartetArgs a{};
             a.bra = view(B);
             a.ket = view(K);
@@ -2023,6 +2033,9 @@ namespace lible_b200
             a.D = D_dev;
             a.nao = (int)n;
             a.grad = grad_dev;
+            a.chunks = cp.chunksD1;
+            a.n_chunks = cp.n_chunksD1;
+            a.counter = plan.counters + 2 * ip;
             cudaCheck(lookupD1(pairType(B.la, B.lb), pairType(K.la, K.lb))(a, stream_, num_sms_), "grad kernel");
         }
         cudaCheck(cudaStreamSynchronize(stream_), "grad");

@@ -216,6 +216,8 @@ namespace lible_b200
             // launch parameters (autotuned): resident blocks per SM divided by grid_div, chunks of
             // at most chunk_mult work units
             int grid_div64 = 1, grid_div32 = 1, chunk_mult64 = 8, chunk_mult32 = 8;
+            unsigned long long *chunksD1 = nullptr;  // gradient launches: chunks of one-quartet units
+            long long n_chunksD1 = 0;
             int branch = 0;  // stream branch of the fork/join launch sequence
             int tb = 0, tk = 0;  // pair types of the launched (bra, ket) classes
         };

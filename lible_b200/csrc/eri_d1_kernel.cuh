@@ -5,9 +5,12 @@
 // where dR/dP_x is the R matrix shifted by one unit along x (Boys function to L+1) and E1 is the
 // derivative of the Hermite coefficients with respect to the pair separation.
 //
-// The work for one quartet is organised in four passes over the primitive quartets - one per
-// Cartesian direction for the shifted terms plus one for the E1_ab terms - so that only one R
-// matrix and two R.E accumulators are live at a time.  Two epilogues:
+// Per primitive quartet the R recursion runs once (to L+1); from it the block gathers the three
+// shifted R matrices and the plain one and forms the seven ket-side products
+//   dR/dP_x E_cd^T (x = 0..2),  R E_cd^T,  R E1_cd,x^T (x = 0..2)
+// into per-thread accumulators (four "passes": x, y, z and plain).  The bra-side contractions with
+// E_ab and E1_ab follow once per bra primitive.  The ket E and E1 tiles of a primitive are staged in
+// shared memory when the class's layout fits.  Two epilogues:
 //   kD1Store: the 12 blocks are accumulated straight into the caller's output (each element owned
 //             by exactly one thread, so no atomics);
 //   kD1Grad:  each block is contracted on the fly with the two-particle density of
@@ -24,7 +27,9 @@ namespace lible_b200
     {
         using C = Cls<LA, LB, LC, LD>;
         static constexpr int HS = C::HAB * C::SCD;
-        static constexpr int G = HS <= 24 * 32 ? 32 : HS <= 24 * 64 ? 64 : HS <= 24 * 128 ? 128 : 256;
+        // at most 4 accumulator slots per thread and pass, up to 256 threads
+        static constexpr int G0 = 32 * ((HS + 127) / 128);
+        static constexpr int G = G0 < 32 ? 32 : (G0 > 256 ? 256 : G0);
         static constexpr int IK = (HS + G - 1) / G;
         static constexpr size_t off_rb = 0;                                        // 2 x NR1 doubles
         static constexpr size_t off_rm = off_rb + 8 * 2 * C::NR1;                  // HCD x HAB
@@ -33,7 +38,10 @@ namespace lible_b200
         static constexpr size_t off_st = off_gm + 8 * C::SAB * C::SCD;             // HCD x HAB char4
         static constexpr size_t off_ht = off_st + 4 * C::HCD * C::HAB;             // NR1 char4
         static constexpr size_t off_rd = (off_ht + 4 * C::NR1 + 15) / 16 * 16;    // 9 x G/32 doubles
-        static constexpr size_t smem = off_rd + 8 * 9 * (G / 32);
+        static constexpr size_t off_ek = off_rd + 8 * 9 * (G / 32);                // 4 x HCD x SCD (staged)
+        static constexpr size_t smem_stage = off_ek + 8 * 4 * C::HCD * C::SCD;
+        static constexpr bool STAGE = smem_stage <= 200 * 1024;
+        static constexpr size_t smem = STAGE ? smem_stage : off_ek;
     };
 
     template <int LA, int LB, int LC, int LD>
@@ -70,12 +78,8 @@ namespace lible_b200
         }
         __syncthreads();
 
-        for (long long task = blockIdx.x; task < a.n_tasks; task += gridDim.x)
-        {
-            uint32_t ib, ik;
-            decodeTask(a, task, ib, ik);
-            if (!inWindow(a, ib, ik, 0, false))
-                continue;
+        // one quartet at a time for the whole block
+        auto processTask = [&](long long task, uint32_t ib, uint32_t ik) {
             const int32_t *bi = a.bra.info + 8 * ib;
             const int32_t *ki = a.ket.info + 8 * ik;
             double acc[12];
@@ -122,77 +126,103 @@ namespace lible_b200
                 const double2 AB = __ldg(reinterpret_cast<const double2 *>(a.bra.ab) + p);
                 const double *eab = a.bra.E + (size_t)p * C::SAB * C::HAB;
                 const double *e1ab = a.bra.E1 + (size_t)p * 3 * C::SAB * C::HAB;
-                for (int pass = 0; pass < 4; pass++)
+                // r1[x]: dR/dP_x E_cd^T (x < 3) and R E_cd^T (x = 3);
+                // r2[x]: -(c/q) dR/dP_x E_cd^T + R E1_cd,x^T.  Classes with at most 4 accumulator
+                // slots per thread keep all four passes live and sweep the ket primitives once; larger
+                // ones sweep once per pass (NPG = 1) to bound the live state.
+                constexpr int NPG = S::IK <= 4 ? 4 : 1;
+                for (int pg = 0; pg < 4; pg += NPG)
                 {
-                    double r1[S::IK], r2[S::IK];
+                double r1[NPG][S::IK], r2[NPG][S::IK];
 #pragma unroll
-                    for (int k = 0; k < S::IK; k++)
-                        r1[k] = r2[k] = 0.0;
-                    for (uint32_t q = q0; q < q1; q++)
+                for (int k = 0; k < S::IK; k++)
+#pragma unroll
+                    for (int x = 0; x < NPG; x++)
+                        r1[x][k] = r2[x][k] = 0.0;
+                for (uint32_t q = q0; q < q1; q++)
+                {
+                    const PQ4 Q = loadPQ(a.ket.pP, q);
+                    const double cexp = __ldg(a.ket.ab + 2 * q);
+                    const double rs = rsqrt(P.x + Q.x);
+                    const double alpha = P.x * Q.x * (rs * rs);
+                    const double X = P.y - Q.y, Y = P.z - Q.z, Z = P.w - Q.w;
+                    const double fac = 34.986836655249725 * rs * P.ip * Q.ip;
+                    double F[L1 + 1];
+                    boysF<L1, false>(alpha * (X * X + Y * Y + Z * Z), a.boys + L1 * kBoysTerms * kBoysPitch, F);
+                    const double m2a = -2.0 * alpha;
+                    double *cur = rb, *nxt = rb + C::NR1;
+                    if (tid == 0)
                     {
-                        const PQ4 Q = loadPQ(a.ket.pP, q);
-                        const double cexp = __ldg(a.ket.ab + 2 * q);
-                        const double rs = rsqrt(P.x + Q.x);
-                        const double alpha = P.x * Q.x * (rs * rs);
-                        const double X = P.y - Q.y, Y = P.z - Q.z, Z = P.w - Q.w;
-                        const double fac = 34.986836655249725 * rs * P.ip * Q.ip;
-                        double F[L1 + 1];
-                        boysF<L1, false>(alpha * (X * X + Y * Y + Z * Z), a.boys + L1 * kBoysTerms * kBoysPitch, F);
-                        const double m2a = -2.0 * alpha;
-                        double *cur = rb, *nxt = rb + C::NR1;
-                        if (tid == 0)
+                        double pw = 1.0;
+                        for (int k = 0; k < L1; k++)
+                            pw *= m2a;
+                        cur[0] = F[L1] * fac * pw;
+                    }
+                    // ket E and E1 tiles of this primitive (staged when the layout fits)
+                    const double *ecd = a.ket.Et + (size_t)q * C::HCD * C::SCD;
+                    const double *e1cd = a.ket.E1t + (size_t)q * 3 * C::HCD * C::SCD;
+                    if constexpr (S::STAGE)
+                    {
+                        double *ek = reinterpret_cast<double *>(smem + S::off_ek);
+                        for (int e = tid; e < C::HCD * C::SCD; e += G)
+                            ek[e] = __ldg(ecd + e);
+                        for (int e = tid; e < 3 * C::HCD * C::SCD; e += G)
+                            ek[C::HCD * C::SCD + e] = __ldg(e1cd + e);
+                        ecd = ek;
+                        e1cd = ek + C::HCD * C::SCD;
+                    }
+                    __syncthreads();
+#pragma unroll
+                    for (int n = L1 - 1; n >= 0; n--)
+                    {
+                        const int cnt = nherm(L1 - n);
+                        for (int e = tid; e < cnt; e += G)
                         {
-                            double pw = 1.0;
-                            for (int k = 0; k < L1; k++)
-                                pw *= m2a;
-                            cur[0] = F[L1] * fac * pw;
-                        }
-                        __syncthreads();
-                        for (int n = L1 - 1; n >= 0; n--)
-                        {
-                            const int cnt = nherm(L1 - n);
-                            for (int e = tid; e < cnt; e += G)
+                            double r;
+                            if (e == 0)
                             {
-                                double r;
-                                if (e == 0)
+                                double pn = 1.0;
+                                for (int k = 0; k < n; k++)
+                                    pn *= m2a;
+                                r = F[n] * fac * pn;
+                            }
+                            else
+                            {
+                                const char4 tv = ht[e];
+                                const int t = tv.x, u = tv.y, v = tv.z, m = tv.w;
+                                if (t > 0)
                                 {
-                                    double pn = 1.0;
-                                    for (int k = 0; k < n; k++)
-                                        pn *= m2a;
-                                    r = F[n] * fac * pn;
+                                    r = X * cur[nherm(m - 2) + cartIndex(u, v)];
+                                    if (t > 1)
+                                        r += (t - 1) * cur[nherm(m - 3) + cartIndex(u, v)];
+                                }
+                                else if (u > 0)
+                                {
+                                    r = Y * cur[nherm(m - 2) + cartIndex(u - 1, v)];
+                                    if (u > 1)
+                                        r += (u - 1) * cur[nherm(m - 3) + cartIndex(u - 2, v)];
                                 }
                                 else
                                 {
-                                    const char4 tv = ht[e];
-                                    const int t = tv.x, u = tv.y, v = tv.z, m = tv.w;
-                                    if (t > 0)
-                                    {
-                                        r = X * cur[nherm(m - 2) + cartIndex(u, v)];
-                                        if (t > 1)
-                                            r += (t - 1) * cur[nherm(m - 3) + cartIndex(u, v)];
-                                    }
-                                    else if (u > 0)
-                                    {
-                                        r = Y * cur[nherm(m - 2) + cartIndex(u - 1, v)];
-                                        if (u > 1)
-                                            r += (u - 1) * cur[nherm(m - 3) + cartIndex(u - 2, v)];
-                                    }
-                                    else
-                                    {
-                                        r = Z * cur[nherm(m - 2) + cartIndex(0, v - 1)];
-                                        if (v > 1)
-                                            r += (v - 1) * cur[nherm(m - 3) + cartIndex(0, v - 2)];
-                                    }
+                                    r = Z * cur[nherm(m - 2) + cartIndex(0, v - 1)];
+                                    if (v > 1)
+                                        r += (v - 1) * cur[nherm(m - 3) + cartIndex(0, v - 2)];
                                 }
-                                nxt[e] = r;
                             }
-                            __syncthreads();
-                            double *tmp = cur;
-                            cur = nxt;
-                            nxt = tmp;
+                            nxt[e] = r;
                         }
-                        const double *ecd = a.ket.Et + (size_t)q * C::HCD * C::SCD;
-                        // sub-step 1: shifted (pass < 3) or plain (pass 3) R matrix times E_cd
+                        __syncthreads();
+                        double *tmp = cur;
+                        cur = nxt;
+                        nxt = tmp;
+                    }
+                    const double cq = cexp / Q.x;
+                    // shifted R (passes x, y, z) and plain R (pass 3, and the E1_cd terms of the
+                    // x, y, z passes) from the one recursion
+#pragma unroll
+                    for (int j = 0; j < NPG; j++)
+                    {
+                        const int pass = pg + j;
                         const int dx = pass == 0, dy = pass == 1, dz = pass == 2;
                         for (int e = tid; e < C::HCD * C::HAB; e += G)
                         {
@@ -201,7 +231,6 @@ namespace lible_b200
                             rm[e] = s4.w ? -r : r;
                         }
                         __syncthreads();
-                        const double cq = cexp / Q.x;
 #pragma unroll
                         for (int k = 0; k < S::IK; k++)
                         {
@@ -209,50 +238,72 @@ namespace lible_b200
                             if (e < C::HAB * C::SCD)
                             {
                                 const int h = e / C::SCD, c = e % C::SCD;
-                                double s = 0.0;
+                                double sv = 0.0;
                                 for (int hp = 0; hp < C::HCD; hp++)
-                                    s += rm[hp * C::HAB + h] * ecd[hp * C::SCD + c];
-                                r1[k] += s;
+                                    sv += rm[hp * C::HAB + h] * ecd[hp * C::SCD + c];
+                                r1[j][k] += sv;
                                 if (pass < 3)
-                                    r2[k] -= cq * s;
+                                    r2[j][k] -= cq * sv;
+                                else if constexpr (NPG == 4)
+                                {
+#pragma unroll
+                                    for (int x = 0; x < 3; x++)
+                                    {
+                                        const double *e1 = e1cd + x * C::HCD * C::SCD;
+                                        double s1 = 0.0;
+                                        for (int hp = 0; hp < C::HCD; hp++)
+                                            s1 += rm[hp * C::HAB + h] * e1[hp * C::SCD + c];
+                                        r2[x][k] += s1;
+                                    }
+                                }
                             }
                         }
                         __syncthreads();
-                        if (pass < 3)
+                        if constexpr (NPG == 1)
                         {
-                            // sub-step 2: plain R matrix times E1_cd along this direction
-                            for (int e = tid; e < C::HCD * C::HAB; e += G)
+                            if (pass < 3)
                             {
-                                const char4 s4 = st[e];
-                                const double r = cur[hermIndex(s4.x, s4.y, s4.z)];
-                                rm[e] = s4.w ? -r : r;
-                            }
-                            __syncthreads();
-                            const double *e1cd = a.ket.E1t + ((size_t)q * 3 + pass) * C::HCD * C::SCD;
-#pragma unroll
-                            for (int k = 0; k < S::IK; k++)
-                            {
-                                const int e = tid + G * k;
-                                if (e < C::HAB * C::SCD)
+                                // this pass's E1_cd term needs the plain R matrix
+                                for (int e = tid; e < C::HCD * C::HAB; e += G)
                                 {
-                                    const int h = e / C::SCD, c = e % C::SCD;
-                                    double s = 0.0;
-                                    for (int hp = 0; hp < C::HCD; hp++)
-                                        s += rm[hp * C::HAB + h] * e1cd[hp * C::SCD + c];
-                                    r2[k] += s;
+                                    const char4 s4 = st[e];
+                                    const double r = cur[hermIndex(s4.x, s4.y, s4.z)];
+                                    rm[e] = s4.w ? -r : r;
                                 }
+                                __syncthreads();
+                                const double *e1 = e1cd + pass * C::HCD * C::SCD;
+#pragma unroll
+                                for (int k = 0; k < S::IK; k++)
+                                {
+                                    const int e = tid + G * k;
+                                    if (e < C::HAB * C::SCD)
+                                    {
+                                        const int h = e / C::SCD, c = e % C::SCD;
+                                        double s1 = 0.0;
+                                        for (int hp = 0; hp < C::HCD; hp++)
+                                            s1 += rm[hp * C::HAB + h] * e1[hp * C::SCD + c];
+                                        r2[j][k] += s1;
+                                    }
+                                }
+                                __syncthreads();
                             }
-                            __syncthreads();
                         }
                     }
+                }
+                // bra side of the passes of this group
+#pragma unroll
+                for (int j = 0; j < NPG; j++)
+                {
+                    const int pass = pg + j;
 #pragma unroll
                     for (int k = 0; k < S::IK; k++)
                     {
                         const int e = tid + G * k;
                         if (e < C::HAB * C::SCD)
                         {
-                            rx1[e] = r1[k];
-                            rx2[e] = r2[k];
+                            rx1[e] = r1[j][k];
+                            if (pass < 3)
+                                rx2[e] = NPG == 4 ? r2[pass][k] : r2[j][k];
                         }
                     }
                     __syncthreads();
@@ -276,15 +327,16 @@ namespace lible_b200
                         {
                             for (int x = 0; x < 3; x++)
                             {
-                                double s = 0.0;
+                                double sv = 0.0;
                                 for (int h = 0; h < C::HAB; h++)
-                                    s += e1ab[(x * C::SAB + m) * C::HAB + h] * rx1[h * C::SCD + c];
-                                emit(0, x, e, s);
-                                emit(1, x, e, -s);
+                                    sv += e1ab[(x * C::SAB + m) * C::HAB + h] * rx1[h * C::SCD + c];
+                                emit(0, x, e, sv);
+                                emit(1, x, e, -sv);
                             }
                         }
                     }
                     __syncthreads();
+                }
                 }
             }
 
@@ -322,6 +374,34 @@ namespace lible_b200
                 }
                 __syncthreads();
             }
+        };
+
+        auto runTask = [&](long long task) {
+            uint32_t ib, ik;
+            decodeTask(a, task, ib, ik);
+            if (inWindow(a, ib, ik, 0, false))
+                processTask(task, ib, ik);
+        };
+        if (a.chunks)
+        {
+            // work queue: the block claims chunks of consecutive tasks
+            __shared__ unsigned long long claimed;
+            for (;;)
+            {
+                if (tid == 0)
+                    claimed = atomicAdd(a.counter, 1ULL);
+                __syncthreads();
+                const unsigned long long c = claimed;
+                __syncthreads();
+                if (c >= (unsigned long long)a.n_chunks)
+                    break;
+                const long long t1 = (long long)__ldg(a.chunks + c + 1);
+                for (long long t = (long long)__ldg(a.chunks + c); t < t1; t++)
+                    runTask(t);
+            }
         }
+        else
+            for (long long task = blockIdx.x; task < a.n_tasks; task += gridDim.x)
+                runTask(task);
     }
 }

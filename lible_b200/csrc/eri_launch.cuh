@@ -103,7 +103,9 @@ namespace lible_b200
         cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, S::G, S::smem);
         if (e != cudaSuccess)
             return e;
-        long long grid = std::min<long long>(a.n_tasks, (long long)num_sms * std::max(occ, 1) * 4);
+        long long grid = a.chunks ? std::min<long long>(a.n_chunks, (long long)num_sms * std::max(occ, 1))
+                                  : std::min<long long>(a.n_tasks, (long long)num_sms * std::max(occ, 1) * 4);
+        grid = std::max<long long>(grid, 1);
         kern<<<(unsigned)grid, S::G, S::smem, s>>>(a);
         return cudaGetLastError();
     }
