@@ -40,6 +40,16 @@ def env_rank():
     return int(os.environ.get("RANK", 0)), int(os.environ.get("LOCAL_RANK", 0)), int(os.environ.get("WORLD_SIZE", 1))
 
 
+def max_over_ranks(x, dist=None, device="cpu"):
+    """The largest value of x over all ranks (timings of a multi-GPU job are its slowest rank's)."""
+    if dist is None:
+        return float(x)
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def emit(obj):
     print(json.dumps(obj), flush=True)
 
@@ -323,12 +333,7 @@ def main():
     clocks = clocks_stop(clk)
 
     def agg(ms):
-        t = float(np.mean(ms))
-        if dist:
-            tt = torch.tensor([t], device=dev)
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            t = float(tt.item())
-        return t
+        return max_over_ranks(float(np.mean(ms)), dist, dev)
 
     t64, tmx = agg(ms64), agg(msmx)
     head = "mixed" if mixed_ok else "fp64"
@@ -349,11 +354,7 @@ def main():
         a = time.perf_counter()
         L.jk(s, Dh, SCHWARZ, head, FP32_THR, J=Jh, K=Kh)
         e2e_s.append(time.perf_counter() - a)
-    e2e_t = float(np.mean(e2e_s))
-    if dist:
-        tt = torch.tensor([e2e_t], device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        e2e_t = float(tt.item())
+    e2e_t = max_over_ranks(float(np.mean(e2e_s)), dist, dev)
 
     # the batch is seconds per build: two timed steps after one warm-up keep the run short
     batch = None if args.no_batch else run_batch(min(args.steps, 2), 1, dev)

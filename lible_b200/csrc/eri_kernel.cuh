@@ -18,15 +18,25 @@
 namespace lible_b200
 {
     // Register-path group size: the smallest g dividing S_cd (g <= 32) for which one thread's share
-    // of the batch (S_ab x S_cd/g), of R.E (H_ab x S_cd/g) and the R vector fit the register
-    // budget; 0 when no split fits (the class then uses the shared-memory group path).
-    constexpr int kRegBudget = 104;
-    constexpr int pickRegGroup(int sab, int scd, int hab, int nr)
+    // of the batch (S_ab x S_cd/g), of R.E (H_ab x S_cd/g) and the R vector fit `budget` values; 0
+    // when none does.
+    constexpr int pickRegGroupWithin(int sab, int scd, int hab, int nr, int budget)
     {
         for (int g = 1; g <= 32; g++)
-            if (scd % g == 0 && sab * (scd / g) + hab * (scd / g) + nr <= kRegBudget)
+            if (scd % g == 0 && sab * (scd / g) + hab * (scd / g) + nr <= budget)
                 return g;
         return 0;
+    }
+    // Two tiers per arithmetic type: a share that fits the register file without spilling (104
+    // doubles / 200 floats) is preferred; failing that, a moderate overflow (144 / 288 values, a few
+    // hundred bytes of spills) still beats one quartet per warp on the group path; beyond that the
+    // class uses the group path (0).
+    template <typename T>
+    constexpr int pickRegGroup(int sab, int scd, int hab, int nr)
+    {
+        constexpr int tier1 = sizeof(T) == 8 ? 104 : 200, tier2 = sizeof(T) == 8 ? 144 : 288;
+        const int g = pickRegGroupWithin(sab, scd, hab, nr, tier1);
+        return g ? g : pickRegGroupWithin(sab, scd, hab, nr, tier2);
     }
 
     // Shared-memory pitches (in doubles) of the DMMA operand tiles.  Fragments read either 4 rows x 8
@@ -50,7 +60,7 @@ namespace lible_b200
     {
         using C = Cls<LA, LB, LC, LD>;
         // register path: GT threads per quartet, each owning CW consecutive ket columns
-        static constexpr int GT = pickRegGroup(C::SAB, C::SCD, C::HAB, C::NR);
+        static constexpr int GT = pickRegGroup<T>(C::SAB, C::SCD, C::HAB, C::NR);
         static constexpr int CW = GT ? C::SCD / GT : 0;
         static constexpr int QPW = GT ? 32 / GT : 0;           // quartets per warp
         // group path in FP64: both contractions on the DMMA pipe (mma.m8n8k4.f64) in 8x8 tiles of
