@@ -221,6 +221,46 @@ def run_rij(Z, xyz, D, J64, steps):
             "dJ_fro_vs_direct": float(np.linalg.norm(Jri - J64))}
 
 
+def run_rijk(Z, xyz, D, J64, K64, occ, steps):
+    """RI-JK of the (H2O)_32 workload with def2-universal-jkfit (3,616 auxiliary functions): wall
+    time of lible_gpu_rij (host D -> host J) and of lible_gpu_rik from the occupied factor C
+    (host C -> host K; D = C C^T, C from the eigenvectors of D), with the per-stage device times
+    and rates of the exchange build, and the RI errors against the direct FP64 J and K of the same
+    run.  The first call of each builds and factorises (P|Q), which later calls reuse."""
+    from lible_b200 import ints as L
+
+    w, V = np.linalg.eigh(D)
+    C = np.ascontiguousarray(V[:, -occ:] * np.sqrt(np.clip(w[-occ:], 0, None)))
+    t0 = time.perf_counter()
+    s = L.Structure("cc-pvdz", Z, xyz, "def2-universal-jkfit", units="bohr")
+    setup = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    Jri, _, _ = L.rij(s, D, SCHWARZ)
+    Kri = L.rik(s, C=C, schwarz=SCHWARZ)
+    first = time.perf_counter() - t0
+    tj, tk = [], []
+    for _ in range(max(1, steps)):
+        t = time.perf_counter()
+        Jri, _, _ = L.rij(s, D, SCHWARZ)
+        tj.append(time.perf_counter() - t)
+        t = time.perf_counter()
+        Kri, info = L.rik(s, C=C, schwarz=SCHWARZ, info=True)
+        tk.append(time.perf_counter() - t)
+    t = time.perf_counter()
+    Kd = L.rik(s, D=D, schwarz=SCHWARZ)
+    t_dpath = time.perf_counter() - t
+    rates = {k: info["flops_" + k] / max(info["t_" + k], 1e-12) / 1e12 for k in ("gemm", "solve", "syrk")}
+    return {"workload": "RI-JK, (H2O)_32 cc-pVDZ / def2-universal-jkfit, FP64, occupied factor C (160)",
+            "naux": s.naux, "setup_s": setup, "first_call_s": first, "rij_s": float(np.mean(tj)),
+            "rik_s": float(np.mean(tk)), "rik_from_D_s": t_dpath, "solve": L.rij_last_solve(s),
+            "rik_stages_s": {k: info["t_" + k] for k in ("ints", "gemm", "solve", "syrk")},
+            "rik_stage_tflops": rates, "rik_aux_blocks": info["n_blocks"],
+            "dEJ_Eh_vs_direct": float(0.5 * np.sum(D * (Jri - J64))),
+            "dEK_Eh_vs_direct": float(-0.25 * np.sum(D * (Kri - K64))),
+            "dK_fro_vs_direct": float(np.linalg.norm(Kri - K64)),
+            "dK_fro_C_vs_D_path": float(np.linalg.norm(Kri - Kd))}
+
+
 def run_gradient(steps, seed=2024):
     """J/K energy gradient of (H2O)_8 cc-pVTZ (464 AOs, occupation 40): wall time of the backward
     pass (derivative integrals contracted with the two-particle density on the device) and its
@@ -262,7 +302,7 @@ def main():
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the 64-molecule batched measurement")
-    ap.add_argument("--no-extras", action="store_true", help="skip the RI-J and gradient measurements")
+    ap.add_argument("--no-extras", action="store_true", help="skip the RI-J, RI-JK and gradient measurements")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
@@ -358,9 +398,10 @@ def main():
 
     # the batch is seconds per build: two timed steps after one warm-up keep the run short
     batch = None if args.no_batch else run_batch(min(args.steps, 2), 1, dev)
-    rij = gradient = None
+    rij = rijk = gradient = None
     if not args.no_extras and rank == 0:
         rij = run_rij(Z, xyz, D, J64, min(args.steps, 2))
+        rijk = run_rijk(Z, xyz, D, J64, K64, OCC, min(args.steps, 2))
         gradient = run_gradient(min(args.steps, 2))
 
     if rank != 0:
@@ -421,6 +462,7 @@ def main():
                 "path": "lible_b200.jk -> lible_gpu_jk with pinned host D/J/K"},
         "batch": batch,
         "rij": rij,
+        "rijk": rijk,
         "gradient": gradient,
         "gpu_launches": int(plan["n_launches"]) * args.steps,
         "clocks": clocks,

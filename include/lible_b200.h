@@ -223,6 +223,25 @@ int lible_gpu_rij_last_solve(lible_gpu_ctx *ctx, int *method, double *lo, double
 int lible_gpu_ri_contract(lible_gpu_ctx *ctx, const double *D, const double *dcoef, double schwarz_threshold,
                           double *gamma, double *J);
 
+/* ---- RI-K ------------------------------------------------------------------------------------
+ * K_mn = sum_{PQ} (ml|P) [(P|Q)^{-1}]_{PQ} (Q|ns) D_ls, the exchange half of RI-JK (no reference
+ * driver; built on the reference's ERI3Kernel / eri2 semantics, src/lible/ints/twoel/
+ * eri_kernels.cpp:1122-1162, and Schwarz-screened like lible_gpu_rij).  The density is given either
+ * as its factor C ([nao][n_occ] row-major, D = C C^T; D may then be NULL) or, with C NULL, as the
+ * symmetric D itself, which is factorised by its eigendecomposition (D = C+ C+^T - C- C-^T over the
+ * eigenpairs with |w| > 1e-12 max|w|).  (P|Q) is factorised as for lible_gpu_rij
+ * (lible_gpu_rij_last_solve reports it).  `info` (may be NULL) receives the factor ranks, the number
+ * of auxiliary blocks and per-stage device times and FLOP counts.  D, C, K: host or device. */
+typedef struct lible_gpu_rik_info
+{
+    long long n_pos, n_neg;  /* columns of C+ and C- (n_occ and 0 when C is given) */
+    int n_blocks;            /* blocks of auxiliary functions the three-centre integrals were built in */
+    double t_ints, t_gemm, t_solve, t_syrk;               /* seconds */
+    double flops_gemm, flops_solve, flops_syrk;           /* algorithmic FLOPs of the three stages */
+} lible_gpu_rik_info;
+int lible_gpu_rik(lible_gpu_ctx *ctx, const double *D, const double *C, long long n_occ, double schwarz_threshold,
+                  double *K, lible_gpu_rik_info *info);
+
 /* ---- host-only helpers (no GPU needed) --------------------------------------------------------
  * The host set-up the kernels consume, exposed for checking against the reference:
  *  - sphericalTrafo(l) (src/lible/ints/spherical_trafo.cpp:9-690): up to *n (row, cart, value) terms;

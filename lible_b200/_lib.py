@@ -30,6 +30,13 @@ class JKPlanInfo(ctypes.Structure):
                 ("flops_fp64", ctypes.c_double), ("flops_fp32", ctypes.c_double)]
 
 
+class RIKInfo(ctypes.Structure):
+    _fields_ = [("n_pos", ctypes.c_longlong), ("n_neg", ctypes.c_longlong), ("n_blocks", ctypes.c_int),
+                ("t_ints", ctypes.c_double), ("t_gemm", ctypes.c_double), ("t_solve", ctypes.c_double),
+                ("t_syrk", ctypes.c_double), ("flops_gemm", ctypes.c_double), ("flops_solve", ctypes.c_double),
+                ("flops_syrk", ctypes.c_double)]
+
+
 # name -> argument types; every function returns int (status) unless noted
 P = ctypes.c_void_p
 I = ctypes.c_int
@@ -71,6 +78,7 @@ SIGNATURES = {
     "lible_gpu_fp64_peak": [P, ctypes.POINTER(D), ctypes.POINTER(D)],
     "lible_gpu_ri_contract": [P, P, P, D, P, P],
     "lible_gpu_rij_last_solve": [P, P, P, P, P, P],
+    "lible_gpu_rik": [P, P, P, LL, D, P, ctypes.POINTER(RIKInfo)],
     "lible_host_spherical_trafo": [I, P, P, P, P],
     "lible_host_shell_norms": [I, I, P, P, P],
     "lible_host_pair_classes": [S, S, I, P, P, I, I, P, P, P, P],

@@ -2,6 +2,7 @@
 // stages host arrays through device memory.
 #include "../../include/lible_b200.h"
 #include "engine_api.hpp"
+#include "ri_solve.hpp"
 
 #include <cuda_runtime.h>
 #include <cublas_v2.h>
@@ -31,6 +32,33 @@ struct lible_gpu_ctx
     double rij_lo = 0, rij_hi = 0;
     int rij_dropped = 0;
     double rij_shift = 0;
+    // factorised RI metric of the current structure (built by the first RI-J / RI-K call) and the
+    // cuBLAS handle of the RI calls; both dropped when the structure changes
+    std::unique_ptr<MetricFactor> metric;
+    std::unique_ptr<BlasHandle> blas;
+
+    void structureChanged() { metric.reset(); }
+    const MetricFactor &metricFactor(Engine &e)
+    {
+        if (!metric)
+        {
+            auto m = std::make_unique<MetricFactor>();
+            factorMetric(e, *m);
+            metric = std::move(m);
+        }
+        rij_method = metric->method;
+        rij_lo = metric->lo;
+        rij_hi = metric->hi;
+        rij_dropped = metric->dropped;
+        rij_shift = metric->shift;
+        return *metric;
+    }
+    BlasHandle &blasHandle(Engine &e)
+    {
+        if (!blas)
+            blas = std::make_unique<BlasHandle>(e.stream());
+        return *blas;
+    }
 };
 
 namespace
@@ -126,45 +154,6 @@ namespace
             if (owned)
                 cudaFree(ptr);
         }
-    };
-
-    // Owning device buffer (freed on scope exit, also when a check throws).
-    template <class T>
-    struct DevBuf
-    {
-        T *p = nullptr;
-        explicit DevBuf(size_t n) { reset(n); }
-        void reset(size_t n)
-        {
-            cudaFree(p);
-            p = nullptr;
-            cudaCheck(cudaMalloc(&p, std::max<size_t>(n, 1) * sizeof(T)), "cudaMalloc");
-        }
-        ~DevBuf() { cudaFree(p); }
-        DevBuf(const DevBuf &) = delete;
-        DevBuf &operator=(const DevBuf &) = delete;
-    };
-
-    struct SolverHandle
-    {
-        cusolverDnHandle_t h = nullptr;
-        SolverHandle()
-        {
-            if (cusolverDnCreate(&h) != CUSOLVER_STATUS_SUCCESS)
-                throw EngineError(kStatusCuda, "cusolverDnCreate failed");
-        }
-        ~SolverHandle() { cusolverDnDestroy(h); }
-    };
-
-    struct BlasHandle
-    {
-        cublasHandle_t h = nullptr;
-        BlasHandle()
-        {
-            if (cublasCreate(&h) != CUBLAS_STATUS_SUCCESS)
-                throw EngineError(kStatusCuda, "cublasCreate failed");
-        }
-        ~BlasHandle() { cublasDestroy(h); }
     };
 
     std::vector<std::array<double, 3>> coords(int n_atoms, const double *xyz, int units)
@@ -347,6 +336,7 @@ int lible_gpu_set_structure_named(lible_gpu_ctx *ctx, const char *basis_root, co
             for (int a = 0; a < n_atoms; a++)
                 aux.push_back(readBasisAtom(apath, atomic_nrs[a]));
         }
+        ctx->structureChanged();
         e.setStructure(main, (aux_basis && aux_basis[0]) ? &aux : nullptr, coords(n_atoms, xyz, units));
     });
 }
@@ -365,6 +355,7 @@ int lible_gpu_set_structure(lible_gpu_ctx *ctx, int n_atoms, const int *atomic_n
         if (aux_shells_per_atom)
             aux = atomsFromArrays(n_atoms, atomic_nrs, aux_shells_per_atom, aux_shell_l, aux_shell_nprim, aux_exps,
                                   aux_coeffs);
+        ctx->structureChanged();
         e.setStructure(main, aux_shells_per_atom ? &aux : nullptr, coords(n_atoms, xyz, units));
     });
 }
@@ -643,6 +634,7 @@ int lible_gpu_set_batch(lible_gpu_ctx *ctx, int n_mol, const char *basis_root, c
             xyzs.push_back(coords(n_atoms[m], xyz + 3 * at, units));
             at += n_atoms[m];
         }
+        ctx->structureChanged();
         e.setBatch(mols, xyzs);
     });
 }
@@ -878,144 +870,76 @@ int lible_gpu_rij(lible_gpu_ctx *ctx, const double *D, double schwarz_threshold,
         const size_t n = e.nao(), na = e.naux();
         DevArray d(D, n * n, true, e.stream());
         DevArray j(J, n * n, false, e.stream());
-        DevBuf<double> metric_b(na * na), rhs_b(na), work_b(1);
-        DevBuf<int> info_b(1);
-        double *metric = metric_b.p, *rhs = rhs_b.p;
-        int *info = info_b.p;
+        DevBuf<double> rhs_b(na);
+        double *rhs = rhs_b.p;
         e.riContract(d.ptr, nullptr, rhs, nullptr, schwarz_threshold);
         if (gamma)
         {
             e.sync();
-            if (isDevice(gamma))
-                cudaCheck(cudaMemcpy(gamma, rhs, na * 8, cudaMemcpyDeviceToDevice), "copy");
-            else
-                cudaCheck(cudaMemcpy(gamma, rhs, na * 8, cudaMemcpyDeviceToHost), "copy");
-        }
-        e.eri2(metric);
-        e.sync();
-        // keep a copy of the metric: a failed Cholesky overwrites it
-        DevBuf<double> metric2_b(na * na);
-        double *metric2 = metric2_b.p;
-        cudaCheck(cudaMemcpyAsync(metric2, metric, na * na * sizeof(double), cudaMemcpyDeviceToDevice, e.stream()),
-                  "copy");
-        SolverHandle sh;
-        cusolverDnHandle_t h = sh.h;
-        cusolverDnSetStream(h, e.stream());
-        int lwork = 0;
-        cusolverDnDpotrf_bufferSize(h, CUBLAS_FILL_MODE_LOWER, (int)na, metric, (int)na, &lwork);
-        work_b.reset((size_t)std::max(lwork, 1));
-        double *work = work_b.p;
-        cusolverDnDpotrf(h, CUBLAS_FILL_MODE_LOWER, (int)na, metric, (int)na, work, lwork, info);
-        int hinfo = 0;
-        cudaCheck(cudaMemcpyAsync(&hinfo, info, sizeof(int), cudaMemcpyDeviceToHost, e.stream()), "info");
-        cudaCheck(cudaStreamSynchronize(e.stream()), "potrf");
-        double shift = 0.0;
-        if (hinfo != 0)
-        {
-            // not numerically positive definite: retry with the diagonal raised by 1e-11 of its largest
-            // element (Tikhonov regularisation), before resorting to an eigendecomposition
-            std::vector<double> dg(na);
-            cudaCheck(cudaMemcpy2DAsync(dg.data(), sizeof(double), metric2, (na + 1) * sizeof(double),
-                                        sizeof(double), na, cudaMemcpyDeviceToHost, e.stream()),
-                      "diag");
-            cudaCheck(cudaStreamSynchronize(e.stream()), "diag");
-            shift = 1e-11 * *std::max_element(dg.begin(), dg.end());
-            for (double &v : dg)
-                v += shift;
-            cudaCheck(cudaMemcpyAsync(metric, metric2, na * na * sizeof(double), cudaMemcpyDeviceToDevice, e.stream()),
+            cudaCheck(cudaMemcpy(gamma, rhs, na * 8, isDevice(gamma) ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost),
                       "copy");
-            cudaCheck(cudaMemcpy2DAsync(metric, (na + 1) * sizeof(double), dg.data(), sizeof(double), sizeof(double),
-                                        na, cudaMemcpyHostToDevice, e.stream()),
-                      "diag");
-            cusolverDnDpotrf(h, CUBLAS_FILL_MODE_LOWER, (int)na, metric, (int)na, work, lwork, info);
-            cudaCheck(cudaMemcpyAsync(&hinfo, info, sizeof(int), cudaMemcpyDeviceToHost, e.stream()), "info");
-            cudaCheck(cudaStreamSynchronize(e.stream()), "potrf");
         }
-        if (hinfo == 0)
+        solveMetric(e, ctx->metricFactor(e), rhs);
+        if (dcoef)
+            cudaCheck(cudaMemcpy(dcoef, rhs, na * 8, isDevice(dcoef) ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost),
+                      "copy");
+        e.riContract(nullptr, rhs, nullptr, j.ptr, schwarz_threshold);
+        j.copyOut();
+    });
+}
+
+int lible_gpu_rik(lible_gpu_ctx *ctx, const double *D, const double *C, long long n_occ, double schwarz_threshold,
+                  double *K, lible_gpu_rik_info *info)
+{
+    return guard(ctx, [&](Engine &e) {
+        if (!e.hasAux())
+            throw EngineError(kStatusNoAux, "RI approximation is not enabled");
+        if (!K || (!D && !C))
+            throw EngineError(kStatusInvalid, "null K, or neither D nor C given");
+        if (C && n_occ < 0)
+            throw EngineError(kStatusInvalid, "negative n_occ");
+        const size_t n = e.nao();
+        DevArray k(K, n * n, false, e.stream());
+        cudaCheck(cudaMemsetAsync(k.ptr, 0, n * n * sizeof(double), e.stream()), "memset");
+        const MetricFactor &mf = ctx->metricFactor(e);
+        BlasHandle &bh = ctx->blasHandle(e);
+        RIKStats st;
+        // one block of (mn|P): a quarter of the free device memory left after Z, 256 MiB .. 16 GiB
+        size_t free_b = 0, total_b = 0;
+        cudaCheck(cudaMemGetInfo(&free_b, &total_b), "meminfo");
+        const size_t z_bytes = e.naux() * n * (size_t)std::max<long long>(n_occ > 0 ? n_occ : (long long)n, 1) * 8;
+        const size_t avail = free_b > z_bytes ? free_b - z_bytes : 0;
+        const size_t block_bytes = std::min<size_t>(size_t(16) << 30, std::max<size_t>(size_t(256) << 20, avail / 4));
+        long long n_pos = n_occ, n_neg = 0;
+        if (C)
         {
-            cusolverDnDpotrs(h, CUBLAS_FILL_MODE_LOWER, (int)na, 1, metric, (int)na, rhs, (int)na, info);
-            // condition lower bound from the Cholesky diagonal
-            std::vector<double> dg(na);
-            cudaCheck(cudaMemcpy2DAsync(dg.data(), sizeof(double), metric, (na + 1) * sizeof(double), sizeof(double),
-                                        na, cudaMemcpyDeviceToHost, e.stream()),
-                      "diag");
-            cudaCheck(cudaStreamSynchronize(e.stream()), "potrs");
-            double lo = 1e300, hi = 0;
-            for (double v : dg)
-            {
-                lo = std::min(lo, v * v);
-                hi = std::max(hi, v * v);
-            }
-            ctx->rij_method = shift > 0 ? 2 : 0;
-            ctx->rij_lo = lo;
-            ctx->rij_hi = hi;
-            ctx->rij_dropped = 0;
-            ctx->rij_shift = shift;
+            DevArray c(C, n * (size_t)std::max<long long>(n_occ, 1), true, e.stream());
+            riExchange(e, bh, mf, c.ptr, n_occ, schwarz_threshold, 1.0, k.ptr, block_bytes, &st);
         }
         else
         {
-            // not numerically positive definite: d = V diag(1/w) V^T gamma over the eigenpairs with
-            // w > 1e-12 * max(w), the rest dropped
-            DevBuf<double> w_b(na);
-            double *w = w_b.p;
-            int lw2 = 0;
-            cusolverDnDsyevd_bufferSize(h, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, (int)na, metric2,
-                                        (int)na, w, &lw2);
-            work_b.reset((size_t)std::max(lw2, 1));
-            work = work_b.p;
-            cusolverDnDsyevd(h, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, (int)na, metric2, (int)na, w, work,
-                             lw2, info);
-            std::vector<double> hw(na);
-            cudaCheck(cudaMemcpyAsync(&hinfo, info, sizeof(int), cudaMemcpyDeviceToHost, e.stream()), "info");
-            cudaCheck(cudaMemcpyAsync(hw.data(), w, na * 8, cudaMemcpyDeviceToHost, e.stream()), "w");
-            cudaCheck(cudaStreamSynchronize(e.stream()), "syevd");
-            if (hinfo != 0)
-            {
-                throw EngineError(kStatusInternal, "eigendecomposition of the RI metric failed (info " +
-                                                       std::to_string(hinfo) + ")");
-            }
-            const double wmax = *std::max_element(hw.begin(), hw.end());
-            // eigenvectors are the columns of the column-major result; c = V^T gamma, c_k /= w_k
-            // (0 for dropped pairs), d = V c
-            std::vector<double> scale(na, 0.0);
-            int dropped = 0;
-            double lo = 1e300;
-            for (size_t k = 0; k < na; k++)
-                if (hw[k] > 1e-12 * wmax)
-                {
-                    scale[k] = 1.0 / hw[k];
-                    lo = std::min(lo, hw[k]);
-                }
-                else
-                    dropped++;
-            DevBuf<double> c_b(na), dscale_b(na);
-            double *c = c_b.p, *dscale = dscale_b.p;
-            cudaCheck(cudaMemcpyAsync(dscale, scale.data(), na * 8, cudaMemcpyHostToDevice, e.stream()), "copy");
-            BlasHandle bhh;
-            cublasHandle_t bh = bhh.h;
-            cublasSetStream(bh, e.stream());
-            const double one = 1.0, zero = 0.0;
-            cublasDgemv(bh, CUBLAS_OP_T, (int)na, (int)na, &one, metric2, (int)na, rhs, 1, &zero, c, 1);
-            // c_k *= scale_k as a diagonal matrix-vector product
-            cublasDdgmm(bh, CUBLAS_SIDE_LEFT, (int)na, 1, c, (int)na, dscale, 1, c, (int)na);
-            cublasDgemv(bh, CUBLAS_OP_N, (int)na, (int)na, &one, metric2, (int)na, c, 1, &zero, rhs, 1);
-            cudaCheck(cudaStreamSynchronize(e.stream()), "eigen solve");
-
-            ctx->rij_method = 1;
-            ctx->rij_lo = lo;
-            ctx->rij_hi = wmax;
-            ctx->rij_dropped = dropped;
-            ctx->rij_shift = 0;
+            DevArray d(D, n * n, true, e.stream());
+            DevBuf<double> cp, cm;
+            splitDensity(e, d.ptr, (long long)n, cp, n_pos, cm, n_neg);
+            riExchange(e, bh, mf, cp.p, n_pos, schwarz_threshold, 1.0, k.ptr, block_bytes, &st);
+            riExchange(e, bh, mf, cm.p, n_neg, schwarz_threshold, -1.0, k.ptr, block_bytes, &st);
         }
-        if (dcoef)
+        mirrorUpper(k.ptr, (long long)n, e.stream());
+        e.sync();
+        k.copyOut();
+        if (info)
         {
-            if (isDevice(dcoef))
-                cudaCheck(cudaMemcpy(dcoef, rhs, na * 8, cudaMemcpyDeviceToDevice), "copy");
-            else
-                cudaCheck(cudaMemcpy(dcoef, rhs, na * 8, cudaMemcpyDeviceToHost), "copy");
+            info->n_pos = n_pos;
+            info->n_neg = n_neg;
+            info->n_blocks = st.n_blocks;
+            info->t_ints = st.t_ints;
+            info->t_gemm = st.t_gemm;
+            info->t_solve = st.t_solve;
+            info->t_syrk = st.t_syrk;
+            info->flops_gemm = st.flops_gemm;
+            info->flops_solve = st.flops_solve;
+            info->flops_syrk = st.flops_syrk;
         }
-        e.riContract(nullptr, rhs, nullptr, j.ptr, schwarz_threshold);
-        j.copyOut();
     });
 }
 

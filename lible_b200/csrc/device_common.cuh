@@ -44,6 +44,7 @@ namespace lible_b200
         kRIJ = 3,        // J_mn += sum_P (mn|P) d_P
         kD1Store = 4,    // write the 12 derivative blocks
         kD1Grad = 5,     // contract the derivative blocks with the two-particle density
+        kRIStore = 6,    // out[P - ri_lo][m][n] = out[P - ri_lo][n][m] = (mn|P), P in [ri_lo, ri_hi)
     };
 
     struct QuartetArgs
@@ -96,6 +97,7 @@ namespace lible_b200
         int mode;
         int flags;                        // kStore: bit0 swap bra shells, bit1 swap ket shells, bit2 swap bra/ket
         int aux_side;                     // RI modes: 0 = ket is the auxiliary side, 1 = bra
+        int ri_lo, ri_hi;                 // kRIStore: the block of auxiliary functions written
         double *out;
         const double *D;
         double *J;
@@ -207,6 +209,13 @@ namespace lible_b200
     // Whether task (bra pair ib at Schwarz position pos, ket pair ik) lies in the launch's window.
     __device__ __forceinline__ bool inWindow(const QuartetArgs &a, uint32_t ib, uint32_t ik, uint32_t pos, bool by_pos)
     {
+        if (a.mode == kRIStore)
+        {
+            // only the auxiliary shells that start inside the block (blocks end at shell boundaries)
+            const int P = __ldg(a.aux_side == 0 ? a.ket.info + 8 * ik : a.bra.info + 8 * ib);
+            if (P < a.ri_lo || P >= a.ri_hi)
+                return false;
+        }
         if (!a.ket_qpair)
             return true;
         const double qb = (by_pos && a.bra_qpos) ? __ldg(a.bra_qpos + pos) : __ldg(a.bra_qpair + ib);

@@ -2044,12 +2044,60 @@ namespace lible_b200
     // ------------------------------------------------------------------------------------------
     // RI-J pieces: gamma_P = sum_mn (mn|P) D_mn and J_mn = sum_P (mn|P) d_P.
 
+    // Launch arguments of RI plan entry `ip` (epilogue fields left to the caller).
+    QuartetArgs Engine::riArgs(const JKPlan &plan, size_t ip)
+    {
+        ClassSet &ms = mainSet(true);
+        ClassSet &xs = auxSet();
+        const auto &cp = plan.pairs[ip];
+        // cp.cb / cp.ck index the bra / ket sets: (aux, main) when cp.swap, else (main, aux)
+        const ClassSet &bs = cp.swap ? xs : ms;
+        const auto &B = bs.dev[cp.cb];
+        const auto &K = (cp.swap ? ms : xs).dev[cp.ck];
+        QuartetArgs a{};
+        a.bra = view(B);
+        a.ket = view(K);
+        a.boys = boys_;
+        a.boys_f = boys_f_;
+        a.list = nullptr;
+        a.major_ket = 1;
+        a.major_order = cp.majors;
+        a.minor_order = bs.orders[cp.cb].d_order;
+        a.minor_begin = cp.begin64;
+        a.prefix = cp.prefix64;
+        a.n_major = cp.n_bra;
+        a.n_tasks = cp.t64;
+        a.bra_qpos = bs.orders[cp.cb].d_q;
+        a.bra_qpair = B.Q;
+        a.ket_qpair = K.Q;
+        a.ket_EtP = K.EtP;
+        a.status = d_status_;
+        a.q_lo = plan.thr;
+        a.q_hi = HUGE_VAL;
+        a.aux_side = cp.swap ? 1 : 0;
+        a.nao = (int)nao_;
+        a.bra_soa = B.soa;
+        a.bra_pPs = B.pPs;
+        a.bra_Es = B.Es;
+        a.bra_Efs = B.Efs;
+        a.bra_pPfs = B.pPfs;
+        a.chunks = cp.chunks64;
+        a.n_chunks = cp.n_chunks64;
+        return a;
+    }
+
+    LaunchFn Engine::riLaunchFn(const JKPlan &plan, size_t ip)
+    {
+        const auto &cp = plan.pairs[ip];
+        const auto &B = (cp.swap ? auxSet() : mainSet(true)).dev[cp.cb];
+        const auto &K = (cp.swap ? mainSet(true) : auxSet()).dev[cp.ck];
+        return lookupFwd64(pairType(B.la, B.lb), pairType(K.la, K.lb));
+    }
+
     void Engine::riContract(const double *D_dev, const double *dcoef_dev, double *gamma_dev, double *J_dev,
                             double schwarz)
     {
         requireSingle();
-        ClassSet &ms = mainSet(true);
-        ClassSet &xs = auxSet();
         JKPlan &plan = riPlan(schwarz);
         const size_t n = nao_;
         if (gamma_dev)
@@ -2061,45 +2109,12 @@ namespace lible_b200
                   "memset");
         for (size_t ip = 0; ip < plan.pairs.size(); ip++)
         {
-            const auto &cp = plan.pairs[ip];
-            // cp.cb / cp.ck index the bra / ket sets: (aux, main) when cp.swap, else (main, aux)
-            const ClassSet &bs = cp.swap ? xs : ms;
-            const auto &B = bs.dev[cp.cb];
-            const auto &K = (cp.swap ? ms : xs).dev[cp.ck];
-            QuartetArgs a{};
-            a.bra = view(B);
-            a.ket = view(K);
-            a.boys = boys_;
-            a.boys_f = boys_f_;
-            a.list = nullptr;
-            a.major_ket = 1;
-            a.major_order = cp.majors;
-            a.minor_order = bs.orders[cp.cb].d_order;
-            a.minor_begin = cp.begin64;
-            a.prefix = cp.prefix64;
-            a.n_major = cp.n_bra;
-            a.n_tasks = cp.t64;
-            a.bra_qpos = bs.orders[cp.cb].d_q;
-            a.bra_qpair = B.Q;
-            a.ket_qpair = K.Q;
-            a.ket_EtP = K.EtP;
-            a.status = d_status_;
-            a.q_lo = plan.thr;
-            a.q_hi = HUGE_VAL;
-            a.aux_side = cp.swap ? 1 : 0;
+            QuartetArgs a = riArgs(plan, ip);
             a.D = D_dev;
             a.dcoef = dcoef_dev;
             a.gamma = gamma_dev;
             a.J = J_dev;
-            a.nao = (int)n;
-            LaunchFn fn = lookupFwd64(pairType(B.la, B.lb), pairType(K.la, K.lb));
-            a.bra_soa = B.soa;
-            a.bra_pPs = B.pPs;
-            a.bra_Es = B.Es;
-            a.bra_Efs = B.Efs;
-            a.bra_pPfs = B.pPfs;
-            a.chunks = cp.chunks64;
-            a.n_chunks = cp.n_chunks64;
+            const LaunchFn fn = riLaunchFn(plan, ip);
             if (gamma_dev)
             {
                 a.counter = plan.counters + 2 * ip;
@@ -2120,6 +2135,40 @@ namespace lible_b200
         }
         cudaCheck(cudaStreamSynchronize(stream_), "ri");
         checkStatus();
+    }
+
+    std::vector<int> Engine::auxShellStarts()
+    {
+        requireStructure();
+        if (!has_aux_)
+            throw EngineError(kStatusNoAux, "RI approximation is not enabled");
+        std::vector<int> v;
+        for (const Shell &sh : aux_shells_)
+            v.push_back((int)sh.ofs_sph);
+        v.push_back((int)naux_);
+        std::sort(v.begin(), v.end());
+        v.erase(std::unique(v.begin(), v.end()), v.end());
+        return v;
+    }
+
+    void Engine::riStore(int P_lo, int P_hi, double *T_dev, double schwarz)
+    {
+        requireSingle();
+        JKPlan &plan = riPlan(schwarz);
+        const size_t n = nao_;
+        cudaCheck(cudaMemsetAsync(T_dev, 0, (size_t)(P_hi - P_lo) * n * n * sizeof(double), stream_), "memset");
+        cudaCheck(cudaMemsetAsync(plan.counters, 0, 2 * plan.pairs.size() * sizeof(unsigned long long), stream_),
+                  "memset");
+        for (size_t ip = 0; ip < plan.pairs.size(); ip++)
+        {
+            QuartetArgs a = riArgs(plan, ip);
+            a.out = T_dev;
+            a.ri_lo = P_lo;
+            a.ri_hi = P_hi;
+            a.counter = plan.counters + 2 * ip;
+            a.mode = kRIStore;
+            cudaCheck(riLaunchFn(plan, ip)(a, stream_, num_sms_), "ri store");
+        }
     }
 
     // Reads the device status word of the last calls (bounded waits that gave up set it).

@@ -12,6 +12,8 @@
 namespace lible_b200
 {
     struct PairView;
+    struct QuartetArgs;
+    using LaunchFn = cudaError_t (*)(const QuartetArgs &, cudaStream_t, int num_sms);
 
     // Status codes returned through the C ABI (mirrors include/lible_b200.h).
     enum Status : int
@@ -163,6 +165,12 @@ namespace lible_b200
         // RI-J contractions (either output may be null).
         void riContract(const double *D_dev, const double *dcoef_dev, double *gamma_dev, double *J_dev,
                         double schwarz);
+        // Dense block of three-centre integrals: T[P - P_lo][m][n] = (mn|P) for the auxiliary
+        // functions P in [P_lo, P_hi) (block ends on shell boundaries, see auxShellStarts), with the
+        // Schwarz test of the RI plan; enqueued on the context stream.
+        void riStore(int P_lo, int P_hi, double *T_dev, double schwarz);
+        // First auxiliary function of every auxiliary shell, ascending, followed by naux.
+        std::vector<int> auxShellStarts();
 
         void sync();
         // Throws kStatusTimeout when a kernel reported a bounded wait that gave up (synchronises).
@@ -236,6 +244,8 @@ namespace lible_b200
         JKClassPair buildClassPair(const ClassSet &bs, int cb, const ClassSet &ks, int ck, bool triangle,
                                    double thr, double thr32, bool mixed);
         JKPlan &riPlan(double thr);
+        QuartetArgs riArgs(const JKPlan &plan, size_t ip);
+        LaunchFn riLaunchFn(const JKPlan &plan, size_t ip);
 
         void rebuildChunks(JKClassPair &cp, bool fp32, int mult);
         void assignBranches(JKPlan &plan);

@@ -392,7 +392,20 @@ namespace lible_b200
         auto V = [&](int m, int nn, int x) {
             return auxket ? val((m * SB + nn) * SC * SD + x) : val(x * SC * SD + m * SD + nn);
         };
-        if (a.mode == kRIGamma)
+        if (a.mode == kRIStore)
+        {
+            // both orientations of the main pair; consecutive threads write consecutive n
+            const size_t nn2 = (size_t)n * n;
+            for (int o = tid; o < SX * S0 * S1; o += stride)
+            {
+                const int nn = o % S1, m = (o / S1) % S0, x = o / (S0 * S1);
+                const double v = V(m, nn, x);
+                double *blk = a.out + (size_t)(ox + x - a.ri_lo) * nn2;
+                blk[(size_t)(o0 + m) * n + o1 + nn] = v;
+                blk[(size_t)(o1 + nn) * n + o0 + m] = v;
+            }
+        }
+        else if (a.mode == kRIGamma)
         {
             for (int x = tid; x < SX; x += stride)
             {

@@ -1,0 +1,391 @@
+// RI metric factorisation (shared by RI-J and RI-K) and the RI exchange build
+//     K_mn = sum_{PQ} (m l|P) [(P|Q)^{-1}]_{PQ} (Q|n s) D_ls,   D = C C^T.
+// The reference exposes the three- and two-centre kernels this builds on (ERI3Kernel / eri2,
+// src/lible/ints/twoel/eri_kernels.cpp:1122-1162) but no RI exchange driver.
+//
+// Pipeline, all on the device:
+//   1. (P|Q) -> Cholesky factor L (or G = V w^{-1/2} from an eigendecomposition, see MetricFactor);
+//   2. per block of auxiliary functions: T[P][m][n] = (mn|P) by the class kernels (kRIStore), then
+//      Z[P][m][i] = sum_n T[P][m][n] C[n][i] as one DGEMM over the whole block;
+//   3. W = L^{-1} Z along P: one DTRSM with nao*occ right-hand sides (or W = Z G);
+//   4. K = sum_R W_R W_R^T: W is re-laid out as A[m][R][i] block by block and each block is one
+//      DSYRK with k = R_block * occ.
+// The three-centre tensor is never held in full: only Z (naux x nao x occ) and one block of T.
+#include "ri_solve.hpp"
+
+#include <cmath>
+#include <string>
+#include <vector>
+
+namespace lible_b200
+{
+    void blasCheck(cublasStatus_t s, const char *what)
+    {
+        if (s != CUBLAS_STATUS_SUCCESS)
+            throw EngineError(kStatusCuda, std::string("cuBLAS ") + what + " failed (status " + std::to_string((int)s) +
+                                               ")");
+    }
+
+    namespace
+    {
+        // A[(m * rb + r) * occ + i] = W[((r0 + r) * n + m) * occ + i] for r < rb.
+        __global__ void relayoutKernel(const double *__restrict__ W, long long n, long long occ, long long r0,
+                                       long long rb, double *__restrict__ A)
+        {
+            const long long total = n * rb * occ;
+            for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; g < total;
+                 g += (long long)gridDim.x * blockDim.x)
+            {
+                const long long i = g % occ, mr = g / occ;
+                const long long r = mr % rb, m = mr / rb;
+                A[g] = W[((r0 + r) * n + m) * occ + i];
+            }
+        }
+
+        __global__ void mirrorUpperKernel(double *K, long long n)
+        {
+            for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; g < n * n;
+                 g += (long long)gridDim.x * blockDim.x)
+            {
+                const long long r = g / n, c = g % n;
+                if (r > c)
+                    K[r * n + c] = K[c * n + r];
+            }
+        }
+
+        // C[m * k + j] = U[m + idx[j] * n] * scale[j]  (U column-major n x n, C row-major n x k).
+        __global__ void factorColumnsKernel(const double *__restrict__ U, long long n, const int *__restrict__ idx,
+                                            const double *__restrict__ scale, long long k, double *__restrict__ C)
+        {
+            for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; g < n * k;
+                 g += (long long)gridDim.x * blockDim.x)
+            {
+                const long long m = g / k, j = g % k;
+                C[g] = U[m + (long long)idx[j] * n] * scale[j];
+            }
+        }
+
+        struct EventPair
+        {
+            cudaEvent_t a = nullptr, b = nullptr;
+            EventPair()
+            {
+                cudaCheck(cudaEventCreate(&a), "event");
+                cudaCheck(cudaEventCreate(&b), "event");
+            }
+            ~EventPair()
+            {
+                cudaEventDestroy(a);
+                cudaEventDestroy(b);
+            }
+            double seconds() const
+            {
+                float ms = 0;
+                cudaCheck(cudaEventElapsedTime(&ms, a, b), "event");
+                return 1e-3 * ms;
+            }
+        };
+
+        int gridFor(long long total)
+        {
+            return (int)std::max<long long>(1, std::min<long long>((total + 255) / 256, 148LL * 16));
+        }
+    }
+
+    void mirrorUpper(double *K_dev, long long n, cudaStream_t s)
+    {
+        mirrorUpperKernel<<<gridFor(n * n), 256, 0, s>>>(K_dev, n);
+        cudaCheck(cudaGetLastError(), "mirror");
+    }
+
+    void factorMetric(Engine &e, MetricFactor &mf)
+    {
+        const size_t na = e.naux();
+        const cudaStream_t s = e.stream();
+        mf.method = -1;
+        mf.lo = mf.hi = mf.shift = 0;
+        mf.dropped = 0;
+        mf.naux = na;
+        mf.fac.reset(na * na);
+        double *metric = mf.fac.p;
+        e.eri2(metric);
+        e.sync();
+        // keep a copy: a failed Cholesky overwrites the matrix
+        DevBuf<double> copy(na * na), work;
+        DevBuf<int> info(1);
+        cudaCheck(cudaMemcpyAsync(copy.p, metric, na * na * sizeof(double), cudaMemcpyDeviceToDevice, s), "copy");
+        SolverHandle sh(s);
+        int lwork = 0;
+        cusolverDnDpotrf_bufferSize(sh.h, CUBLAS_FILL_MODE_LOWER, (int)na, metric, (int)na, &lwork);
+        work.reset((size_t)std::max(lwork, 1));
+        cusolverDnDpotrf(sh.h, CUBLAS_FILL_MODE_LOWER, (int)na, metric, (int)na, work.p, lwork, info.p);
+        int hinfo = 0;
+        cudaCheck(cudaMemcpyAsync(&hinfo, info.p, sizeof(int), cudaMemcpyDeviceToHost, s), "info");
+        cudaCheck(cudaStreamSynchronize(s), "potrf");
+        double shift = 0.0;
+        if (hinfo != 0)
+        {
+            // not numerically positive definite: retry with the diagonal raised by 1e-11 of its largest
+            // element (Tikhonov regularisation) before resorting to an eigendecomposition
+            std::vector<double> dg(na);
+            cudaCheck(cudaMemcpy2DAsync(dg.data(), sizeof(double), copy.p, (na + 1) * sizeof(double), sizeof(double),
+                                        na, cudaMemcpyDeviceToHost, s),
+                      "diag");
+            cudaCheck(cudaStreamSynchronize(s), "diag");
+            shift = 1e-11 * *std::max_element(dg.begin(), dg.end());
+            for (double &v : dg)
+                v += shift;
+            cudaCheck(cudaMemcpyAsync(metric, copy.p, na * na * sizeof(double), cudaMemcpyDeviceToDevice, s), "copy");
+            cudaCheck(cudaMemcpy2DAsync(metric, (na + 1) * sizeof(double), dg.data(), sizeof(double), sizeof(double),
+                                        na, cudaMemcpyHostToDevice, s),
+                      "diag");
+            cusolverDnDpotrf(sh.h, CUBLAS_FILL_MODE_LOWER, (int)na, metric, (int)na, work.p, lwork, info.p);
+            cudaCheck(cudaMemcpyAsync(&hinfo, info.p, sizeof(int), cudaMemcpyDeviceToHost, s), "info");
+            cudaCheck(cudaStreamSynchronize(s), "potrf");
+        }
+        if (hinfo == 0)
+        {
+            std::vector<double> dg(na);
+            cudaCheck(cudaMemcpy2DAsync(dg.data(), sizeof(double), metric, (na + 1) * sizeof(double), sizeof(double),
+                                        na, cudaMemcpyDeviceToHost, s),
+                      "diag");
+            cudaCheck(cudaStreamSynchronize(s), "diag");
+            double lo = 1e300, hi = 0;
+            for (double v : dg)
+            {
+                lo = std::min(lo, v * v);
+                hi = std::max(hi, v * v);
+            }
+            mf.method = shift > 0 ? 2 : 0;
+            mf.lo = lo;
+            mf.hi = hi;
+            mf.shift = shift;
+            return;
+        }
+        // eigendecomposition of the unmodified metric (in `copy`; eigenvectors overwrite it)
+        DevBuf<double> w(na);
+        int lw2 = 0;
+        cusolverDnDsyevd_bufferSize(sh.h, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, (int)na, copy.p, (int)na,
+                                    w.p, &lw2);
+        work.reset((size_t)std::max(lw2, 1));
+        cusolverDnDsyevd(sh.h, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, (int)na, copy.p, (int)na, w.p, work.p,
+                         lw2, info.p);
+        std::vector<double> hw(na);
+        cudaCheck(cudaMemcpyAsync(&hinfo, info.p, sizeof(int), cudaMemcpyDeviceToHost, s), "info");
+        cudaCheck(cudaMemcpyAsync(hw.data(), w.p, na * sizeof(double), cudaMemcpyDeviceToHost, s), "w");
+        cudaCheck(cudaStreamSynchronize(s), "syevd");
+        if (hinfo != 0)
+            throw EngineError(kStatusInternal,
+                              "eigendecomposition of the RI metric failed (info " + std::to_string(hinfo) + ")");
+        const double wmax = *std::max_element(hw.begin(), hw.end());
+        std::vector<double> scale(na, 0.0);
+        int dropped = 0;
+        double lo = 1e300;
+        for (size_t k = 0; k < na; k++)
+            if (hw[k] > 1e-12 * wmax)
+            {
+                scale[k] = 1.0 / std::sqrt(hw[k]);
+                lo = std::min(lo, hw[k]);
+            }
+            else
+                dropped++;
+        DevBuf<double> dscale(na);
+        cudaCheck(cudaMemcpyAsync(dscale.p, scale.data(), na * sizeof(double), cudaMemcpyHostToDevice, s), "copy");
+        BlasHandle bh(s);
+        // G = V diag(scale): column k of the column-major eigenvector matrix times scale_k
+        blasCheck(cublasDdgmm(bh.h, CUBLAS_SIDE_RIGHT, (int)na, (int)na, copy.p, (int)na, dscale.p, 1, mf.fac.p,
+                              (int)na),
+                  "dgmm");
+        cudaCheck(cudaStreamSynchronize(s), "metric factor");
+        mf.method = 1;
+        mf.lo = lo;
+        mf.hi = wmax;
+        mf.dropped = dropped;
+    }
+
+    void solveMetric(Engine &e, const MetricFactor &mf, double *rhs)
+    {
+        const int na = (int)mf.naux;
+        const cudaStream_t s = e.stream();
+        if (mf.method == 0 || mf.method == 2)
+        {
+            SolverHandle sh(s);
+            DevBuf<int> info(1);
+            cusolverDnDpotrs(sh.h, CUBLAS_FILL_MODE_LOWER, na, 1, mf.fac.p, na, rhs, na, info.p);
+            cudaCheck(cudaStreamSynchronize(s), "potrs");
+            return;
+        }
+        // d = G (G^T gamma)
+        BlasHandle bh(s);
+        DevBuf<double> c(mf.naux);
+        const double one = 1.0, zero = 0.0;
+        blasCheck(cublasDgemv(bh.h, CUBLAS_OP_T, na, na, &one, mf.fac.p, na, rhs, 1, &zero, c.p, 1), "gemv");
+        blasCheck(cublasDgemv(bh.h, CUBLAS_OP_N, na, na, &one, mf.fac.p, na, c.p, 1, &zero, rhs, 1), "gemv");
+        cudaCheck(cudaStreamSynchronize(s), "eigen solve");
+    }
+
+    void riExchange(Engine &e, BlasHandle &bh, const MetricFactor &mf, const double *C_dev, long long occ,
+                    double schwarz, double sign, double *K_dev, size_t block_bytes, RIKStats *stats)
+    {
+        if (occ <= 0)
+            return;
+        const long long n = (long long)e.nao(), na = (long long)e.naux();
+        const cudaStream_t s = e.stream();
+        const long long m = n * occ;  // rows of the column-major view of Z: (m, i) fused
+        if (m > INT32_MAX || na > INT32_MAX)
+            throw EngineError(kStatusUnsupported, "RI-K: nao * occ exceeds the 32-bit cuBLAS dimension range");
+
+        // auxiliary blocks: whole shells, at most block_bytes of T (one shell at least)
+        const std::vector<int> starts = e.auxShellStarts();
+        const long long per_fn = n * n * (long long)sizeof(double);
+        const long long cap = std::max<long long>(1, (long long)block_bytes / per_fn);
+        std::vector<std::pair<int, int>> blocks;
+        for (size_t i = 0; i + 1 < starts.size();)
+        {
+            size_t j = i + 1;
+            while (j + 1 < starts.size() && starts[j + 1] - starts[i] <= cap)
+                j++;
+            blocks.push_back({starts[i], starts[j]});
+            i = j;
+        }
+        long long pb_max = 0;
+        for (auto &b : blocks)
+            pb_max = std::max<long long>(pb_max, b.second - b.first);
+
+        // T also serves as the scratch of the eigen-path product (na per row) and of the re-laid-out
+        // W blocks (m per auxiliary function)
+        DevBuf<double> Z((size_t)(na * m)), T((size_t)std::max({pb_max * n * n, na, m}));
+        EventPair ev_int, ev_gemm, ev_solve, ev_syrk;
+        double t_int = 0, t_gemm = 0;
+        const double one = 1.0, zero = 0.0;
+        for (auto &b : blocks)
+        {
+            const long long pb = b.second - b.first;
+            cudaCheck(cudaEventRecord(ev_int.a, s), "event");
+            e.riStore(b.first, b.second, T.p, schwarz);
+            cudaCheck(cudaEventRecord(ev_int.b, s), "event");
+            // Z_cm (occ x pb*n) = C_cm (occ x n) . T_cm (n x pb*n): row-major Z[P][m][i] = T[P][m][:] . C
+            cudaCheck(cudaEventRecord(ev_gemm.a, s), "event");
+            blasCheck(cublasDgemm(bh.h, CUBLAS_OP_N, CUBLAS_OP_N, (int)occ, (int)(pb * n), (int)n, &one, C_dev,
+                                  (int)occ, T.p, (int)n, &zero, Z.p + (size_t)b.first * m, (int)occ),
+                      "dgemm");
+            cudaCheck(cudaEventRecord(ev_gemm.b, s), "event");
+            cudaCheck(cudaEventSynchronize(ev_gemm.b), "ri block");
+            t_int += ev_int.seconds();
+            t_gemm += ev_gemm.seconds();
+        }
+        e.checkStatus();
+
+        // W = L^{-1} Z along P.  Column-major view: Z_cm (m x na), W_cm L^T = Z_cm.
+        cudaCheck(cudaEventRecord(ev_solve.a, s), "event");
+        if (mf.method == 0 || mf.method == 2)
+        {
+            blasCheck(cublasDtrsm(bh.h, CUBLAS_SIDE_RIGHT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_T, CUBLAS_DIAG_NON_UNIT,
+                                  (int)m, (int)na, &one, mf.fac.p, (int)na, Z.p, (int)m),
+                      "dtrsm");
+        }
+        else
+        {
+            // W_cm = Z_cm G, by row blocks of Z_cm through a scratch of at most T's size
+            const long long mb = std::max<long long>(1, std::min<long long>(m, (long long)T.n / na));
+            for (long long r0 = 0; r0 < m; r0 += mb)
+            {
+                const long long rows = std::min(mb, m - r0);
+                blasCheck(cublasDgemm(bh.h, CUBLAS_OP_N, CUBLAS_OP_N, (int)rows, (int)na, (int)na, &one, Z.p + r0,
+                                      (int)m, mf.fac.p, (int)na, &zero, T.p, (int)rows),
+                          "dgemm");
+                cudaCheck(cudaMemcpy2DAsync(Z.p + r0, (size_t)m * sizeof(double), T.p, (size_t)rows * sizeof(double),
+                                            (size_t)rows * sizeof(double), (size_t)na, cudaMemcpyDeviceToDevice, s),
+                          "copy");
+            }
+        }
+        cudaCheck(cudaEventRecord(ev_solve.b, s), "event");
+
+        // K += sign * sum_R W_R W_R^T, R in blocks laid out as A[m][R][i] (T reused as A)
+        cudaCheck(cudaEventRecord(ev_syrk.a, s), "event");
+        const long long rb = std::max<long long>(1, std::min<long long>(na, (long long)T.n / m));
+        for (long long r0 = 0; r0 < na; r0 += rb)
+        {
+            const long long rows = std::min(rb, na - r0);
+            relayoutKernel<<<gridFor(n * rows * occ), 256, 0, s>>>(Z.p, n, occ, r0, rows, T.p);
+            cudaCheck(cudaGetLastError(), "relayout");
+            blasCheck(cublasDsyrk(bh.h, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_T, (int)n, (int)(rows * occ), &sign, T.p,
+                                  (int)(rows * occ), &one, K_dev, (int)n),
+                      "dsyrk");
+        }
+        cudaCheck(cudaEventRecord(ev_syrk.b, s), "event");
+        cudaCheck(cudaEventSynchronize(ev_syrk.b), "ri exchange");
+        if (stats)
+        {
+            stats->t_ints += t_int;
+            stats->t_gemm += t_gemm;
+            stats->t_solve += ev_solve.seconds();
+            stats->t_syrk += ev_syrk.seconds();
+            stats->n_blocks += (int)blocks.size();
+            stats->flops_gemm += 2.0 * (double)na * (double)n * (double)n * (double)occ;
+            stats->flops_solve += (mf.method == 1 ? 2.0 : 1.0) * (double)na * (double)na * (double)m;
+            stats->flops_syrk += (double)n * (double)(n + 1) * (double)na * (double)occ;
+        }
+    }
+
+    void splitDensity(Engine &e, const double *D_dev, long long n, DevBuf<double> &Cp, long long &n_pos,
+                      DevBuf<double> &Cm, long long &n_neg)
+    {
+        const cudaStream_t s = e.stream();
+        // D is symmetric, so its row-major layout is also its column-major one
+        DevBuf<double> U((size_t)(n * n)), w((size_t)n), work;
+        DevBuf<int> info(1);
+        cudaCheck(cudaMemcpyAsync(U.p, D_dev, (size_t)(n * n) * sizeof(double), cudaMemcpyDeviceToDevice, s), "copy");
+        SolverHandle sh(s);
+        int lw = 0;
+        cusolverDnDsyevd_bufferSize(sh.h, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, (int)n, U.p, (int)n, w.p,
+                                    &lw);
+        work.reset((size_t)std::max(lw, 1));
+        cusolverDnDsyevd(sh.h, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, (int)n, U.p, (int)n, w.p, work.p, lw,
+                         info.p);
+        int hinfo = 0;
+        std::vector<double> hw((size_t)n);
+        cudaCheck(cudaMemcpyAsync(&hinfo, info.p, sizeof(int), cudaMemcpyDeviceToHost, s), "info");
+        cudaCheck(cudaMemcpyAsync(hw.data(), w.p, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, s), "w");
+        cudaCheck(cudaStreamSynchronize(s), "syevd");
+        if (hinfo != 0)
+            throw EngineError(kStatusInternal, "eigendecomposition of D failed (info " + std::to_string(hinfo) + ")");
+        double wmax = 0;
+        for (double v : hw)
+            wmax = std::max(wmax, std::fabs(v));
+        std::vector<int> ip, im;
+        std::vector<double> sp, sm;
+        for (long long k = 0; k < n; k++)
+        {
+            if (!(std::fabs(hw[k]) > 1e-12 * wmax))
+                continue;
+            if (hw[k] > 0)
+            {
+                ip.push_back((int)k);
+                sp.push_back(std::sqrt(hw[k]));
+            }
+            else
+            {
+                im.push_back((int)k);
+                sm.push_back(std::sqrt(-hw[k]));
+            }
+        }
+        auto build = [&](const std::vector<int> &idx, const std::vector<double> &sc, DevBuf<double> &C) {
+            const long long k = (long long)idx.size();
+            C.reset((size_t)std::max<long long>(n * k, 1));
+            if (k == 0)
+                return;
+            DevBuf<int> didx(idx.size());
+            DevBuf<double> dsc(sc.size());
+            cudaCheck(cudaMemcpyAsync(didx.p, idx.data(), idx.size() * sizeof(int), cudaMemcpyHostToDevice, s), "copy");
+            cudaCheck(cudaMemcpyAsync(dsc.p, sc.data(), sc.size() * sizeof(double), cudaMemcpyHostToDevice, s), "copy");
+            factorColumnsKernel<<<gridFor(n * k), 256, 0, s>>>(U.p, n, didx.p, dsc.p, k, C.p);
+            cudaCheck(cudaGetLastError(), "factor");
+            cudaCheck(cudaStreamSynchronize(s), "factor");
+        };
+        build(ip, sp, Cp);
+        build(im, sm, Cm);
+        n_pos = (long long)ip.size();
+        n_neg = (long long)im.size();
+    }
+}

@@ -16,7 +16,7 @@ import os
 
 import numpy as np
 
-from ._lib import JKOpts, JKPlanInfo, JKStats, LibleGpuError, check, load
+from ._lib import JKOpts, JKPlanInfo, JKStats, LibleGpuError, RIKInfo, check, load
 
 BASIS_ROOT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "basis", "main")
 AUX_BASIS_ROOT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "basis", "aux")
@@ -448,6 +448,29 @@ def rij_last_solve(structure):
           ctypes.byref(sh))
     return {"method": {0: "cholesky", 1: "eigen", 2: "cholesky+shift"}.get(m.value, None), "lo": lo.value,
             "hi": hi.value, "dropped": dr.value, "shift": sh.value}
+
+
+def rik(structure, D=None, C=None, schwarz=1e-12, info=False):
+    """RI-K: K_mn = sum_PQ (ml|P) [(P|Q)^-1]_PQ (Q|ns) D_ls.  Give the density factor C ([nao][occ],
+    D = C C^T) or the symmetric D itself (factorised on the device by its eigendecomposition).
+    With info=True also returns the stage times / FLOPs of the build."""
+    n = structure.nao
+    if C is None and D is None:
+        raise ValueError("rik needs D or C")
+    K = np.empty((n, n))
+    st = RIKInfo()
+    if C is not None:
+        C = C if hasattr(C, "data_ptr") else _f64(C)
+        if len(C.shape) != 2 or C.shape[0] != n:
+            raise ValueError(f"C must be [{n}][occ]")
+        _call(structure, "lible_gpu_rik", None, _ptr(C), int(C.shape[1]), float(schwarz), _ptr(K),
+              ctypes.byref(st))
+    else:
+        D = D if hasattr(D, "data_ptr") else _f64(D)
+        _call(structure, "lible_gpu_rik", _ptr(D), None, 0, float(schwarz), _ptr(K), ctypes.byref(st))
+    if info:
+        return K, {k: getattr(st, k) for k, _ in RIKInfo._fields_}
+    return K
 
 
 def ri_contract(structure, D=None, dcoef=None, schwarz=1e-12):

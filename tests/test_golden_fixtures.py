@@ -10,7 +10,8 @@ import numpy as np
 import pytest
 
 from lible_b200.workloads import WATER_BOHR, WATER_Z
-from oracle import port
+from oracle import port, ri
+from oracle import ref as R
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 H2O_ANG = [[0.0, 0.0, 0.0], [0.757, 0.586, 0.0], [-0.757, 0.586, 0.0]]
@@ -42,6 +43,23 @@ def test_port_jk_and_gradient_match_golden():
     assert nq == int(g["n_quartets"])
     assert np.abs(J - g["J"]).max() <= 1e-11 and np.abs(K - g["K"]).max() <= 1e-11
     assert np.abs(m.jk_grad(g["D"]) - g["grad"]).max() <= 1e-11
+
+
+@pytest.mark.skipif(not R.available(), reason="reference library not built")
+def test_ri_restatement_matches_golden():
+    """oracle/ri.py on the reference's eri3 / eri2 reproduces the committed RI-K / RI-J fixture, and
+    its RI-J agrees with the reference's own (mn|P) D_mn digestion."""
+    g = load("dimer_rik.npz")
+    r = R.RefStructure("cc-pvdz", list(g["Z"]), g["xyz"], aux="def2-universal-jkfit")
+    B3, M = r.eri3(), r.eri2()
+    D = g["C"] @ g["C"].T
+    assert np.abs(ri.ri_exchange(B3, M, D) - g["K"]).max() <= 1e-12
+    assert np.abs(ri.ri_exchange(B3, M, g["D2"]) - g["K2"]).max() <= 1e-12
+    J = ri.ri_coulomb(B3, M, D)
+    assert np.abs(J - g["J"]).max() <= 1e-12
+    F, method = ri.metric_factor(M)
+    assert method == 0
+    assert np.abs(J - r.rij_j(F.T @ (F @ r.rij_gamma(D)))).max() <= 1e-11
 
 
 # ---- CUDA path (GPU) --------------------------------------------------------------------------
@@ -92,3 +110,25 @@ def test_gpu_d1_and_ri_batches_match_golden():
     got = L.ERI3Kernel(a, x).batch(idx).reshape(r["eri3"].shape)
     assert np.abs(got - r["eri3"]).max() <= 1e-12
     assert np.abs(L.eri2(s) - r["eri2"]).max() <= 1e-12
+
+
+@pytest.mark.gpu
+def test_gpu_rik_matches_golden():
+    """RI-K through the C ABI from the density factor and from D itself (an indefinite D exercises
+    the C+ / C- split).  Tolerance 1e-10: the metric's condition number is ~4e7."""
+    from lible_b200 import ints as L
+
+    g = load("dimer_rik.npz")
+    s = L.Structure("cc-pvdz", list(g["Z"]), g["xyz"], "def2-universal-jkfit", units="bohr")
+    K, info = L.rik(s, C=g["C"], schwarz=0.0, info=True)
+    assert np.abs(K - g["K"]).max() <= 1e-10
+    assert np.abs(K - K.T).max() == 0.0
+    assert info["n_pos"] == 10 and info["n_neg"] == 0 and info["n_blocks"] >= 1
+    Kd = L.rik(s, D=g["C"] @ g["C"].T, schwarz=0.0)
+    assert np.abs(Kd - g["K"]).max() <= 1e-10
+    K2, info2 = L.rik(s, D=g["D2"], schwarz=0.0, info=True)
+    assert info2["n_pos"] == 6 and info2["n_neg"] == 3
+    assert np.abs(K2 - g["K2"]).max() <= 1e-10
+    J, _, _ = L.rij(s, g["C"] @ g["C"].T, schwarz=0.0)
+    assert np.abs(J - g["J"]).max() <= 1e-10
+    assert L.rij_last_solve(s)["method"] == "cholesky"

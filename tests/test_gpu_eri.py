@@ -266,3 +266,29 @@ def test_rij_even_tempered_aux_vs_reference():
         dref = V[:, keep] @ ((V[:, keep].T @ gr) / w[keep])
     Jref = r.rij_j(dref)
     assert np.abs(J - Jref).max() <= 1e-6 * max(1.0, np.abs(Jref).max())
+
+
+def test_rik_blocks_and_ill_conditioned_metric_vs_reference():
+    """RI-K of a water trimer with the even-tempered s-f auxiliary basis, whose metric is not
+    numerically positive definite (shifted Cholesky or eigendecomposition): against the numpy
+    restatement on the reference's own eri3 / eri2 with the same metric policy, and with the Schwarz
+    test on (its effect stays far below the tolerance)."""
+    from oracle import ri
+
+    from lible_b200.workloads import even_tempered_aux
+    from oracle import port
+
+    Z, xyz, rng = water_cluster(3, 11)
+    aux = even_tempered_aux(Z)
+    s = L.Structure("cc-pvdz", Z, xyz, aux, units="bohr")
+    r = R.RefStructure(port.read_basis("cc-pvdz", Z), Z, xyz, aux=aux)
+    B3, M = r.eri3(), r.eri2()
+    C = np.linalg.qr(rng.standard_normal((s.nao, 15)))[0]
+    K = L.rik(s, C=C, schwarz=0.0)
+    F, method = ri.metric_factor(M)
+    solve = L.rij_last_solve(s)
+    assert {0: "cholesky", 1: "eigen", 2: "cholesky+shift"}[method] == solve["method"]
+    Kref = ri.ri_exchange(B3, M, C @ C.T)
+    assert np.abs(K - Kref).max() <= 1e-6 * max(1.0, np.abs(Kref).max())
+    Ks = L.rik(s, C=C, schwarz=1e-12)
+    assert np.abs(Ks - K).max() <= 1e-6 * max(1.0, np.abs(Kref).max())
