@@ -261,6 +261,33 @@ def run_rijk(Z, xyz, D, J64, K64, occ, steps):
             "dK_fro_C_vs_D_path": float(np.linalg.norm(Kri - Kd))}
 
 
+def run_one_electron(Z, xyz, steps, cpu=True):
+    """Overlap, kinetic energy and nuclear attraction of the (H2O)_32 cc-pVDZ workload in one pass
+    (lible_gpu_one_electron, host outputs), beside the reference's own overlap / kineticEnergy /
+    nuclearAttraction on every host core (oracle/_ref), with the largest element difference."""
+    from lible_b200 import ints as L
+
+    s = L.Structure("cc-pvdz", Z, xyz, units="bohr")
+    S, T, V = L.one_electron(s)
+    ts = []
+    for _ in range(max(1, steps)):
+        t = time.perf_counter()
+        S, T, V = L.one_electron(s)
+        ts.append(time.perf_counter() - t)
+    out = {"workload": "overlap + kinetic + nuclear attraction, (H2O)_32 cc-pVDZ, FP64", "nao": s.nao,
+           "gpu_s": float(np.mean(ts))}
+    from oracle import ref as R
+    if cpu and R.available():
+        R.set_threads(os.cpu_count() or 1)
+        r = R.RefStructure("cc-pvdz", Z, xyz)
+        t = time.perf_counter()
+        ref = [r.one_electron(k) for k in range(3)]
+        out["reference_cpu_s"] = time.perf_counter() - t
+        out["reference_cores"] = os.cpu_count() or 1
+        out["max_abs_diff"] = float(max(np.abs(a - b).max() for a, b in zip((S, T, V), ref)))
+    return out
+
+
 def run_gradient(steps, seed=2024):
     """J/K energy gradient of (H2O)_8 cc-pVTZ (464 AOs, occupation 40): wall time of the backward
     pass (derivative integrals contracted with the two-particle density on the device) and its
@@ -302,7 +329,7 @@ def main():
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the 64-molecule batched measurement")
-    ap.add_argument("--no-extras", action="store_true", help="skip the RI-J, RI-JK and gradient measurements")
+    ap.add_argument("--no-extras", action="store_true", help="skip the RI-J, RI-JK, one-electron and gradient measurements")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
@@ -398,10 +425,11 @@ def main():
 
     # the batch is seconds per build: two timed steps after one warm-up keep the run short
     batch = None if args.no_batch else run_batch(min(args.steps, 2), 1, dev)
-    rij = rijk = gradient = None
+    rij = rijk = one_el = gradient = None
     if not args.no_extras and rank == 0:
         rij = run_rij(Z, xyz, D, J64, min(args.steps, 2))
         rijk = run_rijk(Z, xyz, D, J64, K64, OCC, min(args.steps, 2))
+        one_el = run_one_electron(Z, xyz, min(args.steps, 2), cpu=not args.no_cpu_baseline)
         gradient = run_gradient(min(args.steps, 2))
 
     if rank != 0:
@@ -463,6 +491,7 @@ def main():
         "batch": batch,
         "rij": rij,
         "rijk": rijk,
+        "one_electron": one_el,
         "gradient": gradient,
         "gpu_launches": int(plan["n_launches"]) * args.steps,
         "clocks": clocks,

@@ -223,6 +223,21 @@ int lible_gpu_rij_last_solve(lible_gpu_ctx *ctx, int *method, double *lo, double
 int lible_gpu_ri_contract(lible_gpu_ctx *ctx, const double *D, const double *dcoef, double schwarz_threshold,
                           double *gamma, double *J);
 
+/* ---- one-electron integrals ------------------------------------------------------------------
+ * lible::ints::overlap, kineticEnergy, nuclearAttraction and externalCharges
+ * (src/lible/ints/ints.hpp:29-61, oneelints.cpp:169-197, 348-376, 1087-1120, 1703-1744): full
+ * nao x nao matrices, AO order as eri4.  Point charges are [n_charges][4] = x, y, z (bohr), q; the
+ * potential is that of the charges acting on an electron (negative for positive q), as in the
+ * reference.  lible_gpu_one_electron computes any subset in one pass (NULL outputs are skipped;
+ * charges NULL = the nuclei).  Main-basis shells up to l = 3; charges in host memory, outputs host
+ * or device. */
+int lible_gpu_overlap(lible_gpu_ctx *ctx, double *out);
+int lible_gpu_kinetic_energy(lible_gpu_ctx *ctx, double *out);
+int lible_gpu_nuclear_attraction(lible_gpu_ctx *ctx, double *out);
+int lible_gpu_external_charges(lible_gpu_ctx *ctx, const double *charges, int n_charges, double *out);
+int lible_gpu_one_electron(lible_gpu_ctx *ctx, const double *charges, int n_charges, double *S, double *T,
+                           double *V);
+
 /* ---- RI-K ------------------------------------------------------------------------------------
  * K_mn = sum_{PQ} (ml|P) [(P|Q)^{-1}]_{PQ} (Q|ns) D_ls, the exchange half of RI-JK (no reference
  * driver; built on the reference's ERI3Kernel / eri2 semantics, src/lible/ints/twoel/

@@ -79,6 +79,11 @@ SIGNATURES = {
     "lible_gpu_ri_contract": [P, P, P, D, P, P],
     "lible_gpu_rij_last_solve": [P, P, P, P, P, P],
     "lible_gpu_rik": [P, P, P, LL, D, P, ctypes.POINTER(RIKInfo)],
+    "lible_gpu_overlap": [P, P],
+    "lible_gpu_kinetic_energy": [P, P],
+    "lible_gpu_nuclear_attraction": [P, P],
+    "lible_gpu_external_charges": [P, P, I, P],
+    "lible_gpu_one_electron": [P, P, I, P, P, P],
     "lible_host_spherical_trafo": [I, P, P, P, P],
     "lible_host_shell_norms": [I, I, P, P, P],
     "lible_host_pair_classes": [S, S, I, P, P, I, I, P, P, P, P],

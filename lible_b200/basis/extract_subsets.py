@@ -5,7 +5,7 @@ The engine reads basis sets in the reference's plain-text format
 src/lible/ints/basis_sets.cpp:214-277 of the reference) and in its directory layout
 (``<root>/<family>/<name>.txt``, src/lible/ints/basis_sets.cpp:318-360).  Only the elements and
 basis sets the tests and benchmarks use are kept: H, C and O, in the main sets
-cc-pVDZ, cc-pVTZ, def2-SVP, def2-TZVP and the auxiliary sets def2-QZVP-RIFIT,
+cc-pVDZ, cc-pVTZ, def2-SVP, def2-TZVP, 6-31+G and the auxiliary sets def2-QZVP-RIFIT,
 def2-universal-JKFIT and cc-pVDZ-RIFIT.  The numbers are the published basis-set data, copied
 verbatim so that integrals agree with the reference to the last bit.
 
@@ -16,7 +16,7 @@ import os
 import sys
 
 ELEMENTS = (1, 6, 8)
-MAIN = {"dunning": ("cc-pvdz", "cc-pvtz"), "ahlrichs": ("def2-svp", "def2-tzvp")}
+MAIN = {"dunning": ("cc-pvdz", "cc-pvtz"), "ahlrichs": ("def2-svp", "def2-tzvp"), "pople": ("6-31+g",)}
 AUX = {"ahlrichs": ("def2-qzvp-rifit", "def2-universal-jkfit"), "dunning": ("cc-pvdz-rifit",)}
 
 

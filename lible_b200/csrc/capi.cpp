@@ -888,6 +888,47 @@ int lible_gpu_rij(lible_gpu_ctx *ctx, const double *D, double schwarz_threshold,
     });
 }
 
+int lible_gpu_one_electron(lible_gpu_ctx *ctx, const double *charges, int n_charges, double *S, double *T,
+                           double *V)
+{
+    return guard(ctx, [&](Engine &e) {
+        if (!S && !T && !V)
+            throw EngineError(kStatusInvalid, "no output requested");
+        if (charges && n_charges < 0)
+            throw EngineError(kStatusInvalid, "negative n_charges");
+        const size_t n = e.nao();
+        DevArray s(S, n * n, false, e.stream()), t(T, n * n, false, e.stream()), v(V, n * n, false, e.stream());
+        e.oneElectron(charges, charges ? n_charges : 0, charges == nullptr, s.ptr, t.ptr, v.ptr);
+        e.sync();
+        s.copyOut();
+        t.copyOut();
+        v.copyOut();
+    });
+}
+
+int lible_gpu_overlap(lible_gpu_ctx *ctx, double *out)
+{
+    return lible_gpu_one_electron(ctx, nullptr, 0, out, nullptr, nullptr);
+}
+
+int lible_gpu_kinetic_energy(lible_gpu_ctx *ctx, double *out)
+{
+    return lible_gpu_one_electron(ctx, nullptr, 0, nullptr, out, nullptr);
+}
+
+int lible_gpu_nuclear_attraction(lible_gpu_ctx *ctx, double *out)
+{
+    return lible_gpu_one_electron(ctx, nullptr, 0, nullptr, nullptr, out);
+}
+
+int lible_gpu_external_charges(lible_gpu_ctx *ctx, const double *charges, int n_charges, double *out)
+{
+    if (!charges && n_charges > 0)
+        return fail(ctx, LIBLE_GPU_EINVAL, "null charges");
+    static const double none[4] = {0, 0, 0, 0};
+    return lible_gpu_one_electron(ctx, charges ? charges : none, charges ? n_charges : 0, nullptr, nullptr, out);
+}
+
 int lible_gpu_rik(lible_gpu_ctx *ctx, const double *D, const double *C, long long n_occ, double schwarz_threshold,
                   double *K, lible_gpu_rik_info *info)
 {

@@ -171,6 +171,10 @@ namespace lible_b200
         void riStore(int P_lo, int P_hi, double *T_dev, double schwarz);
         // First auxiliary function of every auxiliary shell, ascending, followed by naux.
         std::vector<int> auxShellStarts();
+        // One-electron integrals (device outputs, any may be null): overlap, kinetic energy and the
+        // attraction of point charges ([n][4] x, y, z in bohr, q; with `nuclei` the atoms' nuclei).
+        void oneElectron(const double *charges_host, int n_charges, bool nuclei, double *S_dev, double *T_dev,
+                         double *V_dev);
 
         void sync();
         // Throws kStatusTimeout when a kernel reported a bounded wait that gave up (synchronises).

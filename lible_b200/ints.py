@@ -450,6 +450,46 @@ def rij_last_solve(structure):
             "hi": hi.value, "dropped": dr.value, "shift": sh.value}
 
 
+def _square(structure, fn, *args):
+    n = structure.nao
+    out = np.empty((n, n))
+    _call(structure, fn, *args, _ptr(out))
+    return out
+
+
+def overlap(structure):
+    """lible::ints::overlap (src/lible/ints/ints.hpp:30): the nao x nao overlap matrix."""
+    return _square(structure, "lible_gpu_overlap")
+
+
+def kineticEnergy(structure):
+    """lible::ints::kineticEnergy (ints.hpp:39)."""
+    return _square(structure, "lible_gpu_kinetic_energy")
+
+
+def nuclearAttraction(structure):
+    """lible::ints::nuclearAttraction (ints.hpp:48): the nuclei's attraction on an electron."""
+    return _square(structure, "lible_gpu_nuclear_attraction")
+
+
+def externalCharges(point_charges, structure):
+    """lible::ints::externalCharges (ints.hpp:55): point charges [[x, y, z, q], ...] in bohr."""
+    q = _f64(point_charges).reshape(-1, 4)
+    return _square(structure, "lible_gpu_external_charges", _ptr(q), int(len(q)))
+
+
+def one_electron(structure, point_charges=None):
+    """(S, T, V) in one pass; V from the nuclei, or from `point_charges` ([n][4], bohr) if given."""
+    n = structure.nao
+    S, T, V = np.empty((n, n)), np.empty((n, n)), np.empty((n, n))
+    if point_charges is None:
+        _call(structure, "lible_gpu_one_electron", None, 0, _ptr(S), _ptr(T), _ptr(V))
+    else:
+        q = _f64(point_charges).reshape(-1, 4)
+        _call(structure, "lible_gpu_one_electron", _ptr(q), int(len(q)), _ptr(S), _ptr(T), _ptr(V))
+    return S, T, V
+
+
 def rik(structure, D=None, C=None, schwarz=1e-12, info=False):
     """RI-K: K_mn = sum_PQ (ml|P) [(P|Q)^-1]_PQ (Q|ns) D_ls.  Give the density factor C ([nao][occ],
     D = C C^T) or the symmetric D itself (factorised on the device by its eigendecomposition).

@@ -49,6 +49,7 @@ def lib():
         L.ref_jk_grad.argtypes = [P, P, P]
         L.ref_rij_gamma.argtypes = [P, P, P]
         L.ref_rij_j.argtypes = [P, P, P]
+        L.ref_one_electron.argtypes = [P, ctypes.c_int, P, ctypes.c_int, P]
         _lib = L
     return _lib
 
@@ -109,6 +110,14 @@ class RefStructure:
     def eri2(self):
         out = np.empty((self.naux, self.naux))
         self._chk(lib().ref_eri2(self.h, _p(out)))
+        return out
+
+    def one_electron(self, which, charges=None):
+        """The reference's overlap / kineticEnergy / nuclearAttraction / externalCharges
+        (which = 0..3; charges [n][4] = x, y, z in bohr, q)."""
+        out = np.empty((self.nao, self.nao))
+        q = np.ascontiguousarray(charges if charges is not None else np.zeros((0, 4)), dtype=np.float64)
+        self._chk(lib().ref_one_electron(self.h, which, _p(q), len(q), _p(out)))
         return out
 
     def eri2_diagonal(self):

@@ -231,6 +231,31 @@ int ref_eri2(void *h, double *out)
     });
 }
 
+// One-electron integrals of the reference (src/lible/ints/oneelints.cpp): 0 overlap, 1 kinetic
+// energy, 2 nuclear attraction, 3 external point charges (charges [n][4] x, y, z (bohr), q).
+int ref_one_electron(void *h, int which, const double *charges, int n_charges, double *out)
+{
+    return guarded([&]
+    {
+        const lints::Structure &st = *static_cast<RefStructure *>(h)->s;
+        lible::vec2d v;
+        if (which == 0)
+            v = lints::overlap(st);
+        else if (which == 1)
+            v = lints::kineticEnergy(st);
+        else if (which == 2)
+            v = lints::nuclearAttraction(st);
+        else
+        {
+            std::vector<std::array<double, 4>> q(n_charges);
+            for (int i = 0; i < n_charges; i++)
+                q[i] = {charges[4 * i], charges[4 * i + 1], charges[4 * i + 2], charges[4 * i + 3]};
+            v = lints::externalCharges(q, st);
+        }
+        std::memcpy(out, v.memptr(), v.size() * sizeof(double));
+    });
+}
+
 int ref_eri2_diagonal(void *h, double *out)
 {
     return guarded([&]

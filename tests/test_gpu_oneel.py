@@ -1,0 +1,68 @@
+"""One-electron integrals through the C ABI against the reference's own overlap / kineticEnergy /
+nuclearAttraction / externalCharges (oracle/_ref) and its golden sums
+(test/tests_ints.cpp:167-358: C2H4 cc-pVDZ overlap and kinetic energy, CO2 6-31+G nuclear
+attraction and external charges).  Tolerances: 1e-12 absolute per element (the reference's test
+tolerance, test/tests_ints.cpp:15); golden sums to 1e-13 relative."""
+import numpy as np
+import pytest
+
+from lible_b200 import ints as L
+from lible_b200.workloads import water_cluster
+from oracle import ref as R
+
+pytestmark = pytest.mark.gpu
+
+C2H4_Z = [6, 6, 1, 1, 1, 1]
+C2H4_ANG = [[3.402, 0.773, -9.252], [4.697, 0.791, -8.909], [2.933, -0.150, -9.521],
+            [2.837, 1.682, -9.258], [5.262, -0.118, -8.904], [5.167, 1.714, -8.641]]
+CO2_Z = [6, 8, 8]
+CO2_ANG = [[0.0, 0.0, 0.32942], [0.0, 1.15362, -0.12353], [0.0, -1.15362, -0.12353]]
+
+
+def seqsum(x):
+    return float(np.cumsum(np.abs(np.asarray(x)).ravel())[-1])
+
+
+def golden(value, expected):
+    return abs(value - expected) <= 1e-13 * abs(expected)
+
+
+def test_overlap_and_kinetic_golden_c2h4():
+    s = L.Structure("cc-pvdz", C2H4_Z, C2H4_ANG)
+    r = R.RefStructure("cc-pvdz", C2H4_Z, C2H4_ANG, units="angstrom")
+    S, T = L.overlap(s), L.kineticEnergy(s)
+    assert golden(seqsum(S), 226.099184393591)
+    assert golden(seqsum(T), 252.755644635021)
+    assert np.abs(S - r.one_electron(0)).max() <= 1e-12
+    assert np.abs(T - r.one_electron(1)).max() <= 1e-12
+
+
+def test_nuclear_attraction_and_external_charges_golden_co2():
+    s = L.Structure("6-31+g", CO2_Z, CO2_ANG)
+    r = R.RefStructure("6-31+g", CO2_Z, CO2_ANG, units="angstrom")
+    V = L.nuclearAttraction(s)
+    assert golden(seqsum(V), 2141.927982294058)
+    assert np.abs(V - r.one_electron(2)).max() <= 1e-12
+    # the nuclei as explicit charges (structure.getZs() in the reference test)
+    q = np.array([[x / 0.5291772083 for x in c] + [z] for c, z in zip(CO2_ANG, CO2_Z)])
+    Vq = L.externalCharges(q, s)
+    assert golden(seqsum(Vq), 2141.927982294058)
+    assert np.abs(Vq - V).max() <= 1e-12
+
+
+def test_one_electron_f_shells_and_random_charges_vs_reference():
+    # cc-pVTZ water dimer: f shells on O (the l <= 3 limit), 200 random point charges
+    Z, xyz, rng = water_cluster(2, 5)
+    s = L.Structure("cc-pvtz", Z, xyz, units="bohr")
+    r = R.RefStructure("cc-pvtz", Z, xyz)
+    q = np.concatenate([rng.uniform(-8, 8, (200, 3)), rng.uniform(-1, 1, (200, 1))], axis=1)
+    S, T, V = L.one_electron(s)
+    assert np.abs(S - r.one_electron(0)).max() <= 1e-12
+    assert np.abs(T - r.one_electron(1)).max() <= 1e-12
+    assert np.abs(V - r.one_electron(2)).max() <= 1e-11 * max(1.0, np.abs(V).max())
+    Vq = L.externalCharges(q, s)
+    assert np.abs(Vq - r.one_electron(3, q)).max() <= 1e-12 * max(1.0, np.abs(Vq).max())
+    assert np.abs(L.externalCharges(np.zeros((0, 4)), s)).max() == 0.0
+    # symmetric (diagonal shell blocks are written from both orientations, as in the reference, so
+    # to the last bit only), and the same matrices as the single-operator calls
+    assert np.abs(S - S.T).max() <= 1e-15 and np.abs(L.overlap(s) - S).max() == 0.0

@@ -147,3 +147,20 @@ def test_water_cluster_generator_is_seeded():
     # rigid waters: O-H distances preserved
     d = np.linalg.norm(x1[1::3] - x1[0::3], axis=1)
     assert np.allclose(d, np.linalg.norm([1.4305, 1.1093, 0.0]))
+
+
+@needs_ref
+def test_reference_one_electron_golden():
+    # the compiled reference reproduces its own one-electron golden sums
+    # (test/tests_ints.cpp:167-182, 236-251, 303-318); these pin the one-electron oracle
+    c2h4 = [[3.402, 0.773, -9.252], [4.697, 0.791, -8.909], [2.933, -0.150, -9.521],
+            [2.837, 1.682, -9.258], [5.262, -0.118, -8.904], [5.167, 1.714, -8.641]]
+    r = ref.RefStructure("cc-pvdz", [6, 6, 1, 1, 1, 1], c2h4, units="angstrom")
+    assert abs(seqsum(r.one_electron(0)) - 226.099184393591) <= 1e-13 * 226.1
+    assert abs(seqsum(r.one_electron(1)) - 252.755644635021) <= 1e-13 * 252.8
+    co2 = [[0.0, 0.0, 0.32942], [0.0, 1.15362, -0.12353], [0.0, -1.15362, -0.12353]]
+    r2 = ref.RefStructure("6-31+g", [6, 8, 8], co2, units="angstrom")
+    V = r2.one_electron(2)
+    assert abs(seqsum(V) - 2141.927982294058) <= 1e-13 * 2141.9
+    q = np.array([[x / 0.5291772083 for x in c] + [z] for c, z in zip(co2, [6, 8, 8])])
+    assert np.abs(r2.one_electron(3, q) - V).max() <= 1e-13
