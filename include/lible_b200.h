@@ -237,6 +237,18 @@ int lible_gpu_nuclear_attraction(lible_gpu_ctx *ctx, double *out);
 int lible_gpu_external_charges(lible_gpu_ctx *ctx, const double *charges, int n_charges, double *out);
 int lible_gpu_one_electron(lible_gpu_ctx *ctx, const double *charges, int n_charges, double *S, double *T,
                            double *V);
+/* The per-pair kernels of the reference: overlapKernel, kineticEnergyKernel, externalChargesKernel
+ * (op 0, 1, 2; blocks [S_a][S_b]) and overlapD1Kernel, kineticEnergyD1Kernel,
+ * externalChargesD1Kernel (op 3, 4, 5; [6][S_a][S_b] = d/dA x, y, z, d/dB x, y, z; for op 5 the
+ * orbital part, as the reference) for `n` pair indices of class `class_ab` of
+ * lible_gpu_pair_classes(use_symm) (src/lible/ints/ints.hpp:33-93, oneelints.cpp:57-164, 199-346,
+ * 508-789).  charges as above (NULL = the nuclei); out: n consecutive blocks, host or device. */
+int lible_gpu_one_electron_batch(lible_gpu_ctx *ctx, int use_symm, int class_ab, int op, long long n,
+                                 const unsigned *pairs, const double *charges, int n_charges, double *out);
+/* Nuclear gradient of the one-electron energy terms, grad[atom][xyz] = d/dR (sum D (T + V) -
+ * sum W S), V the nuclear attraction (orbital and operator parts).  D and W symmetric nao x nao,
+ * either may be NULL (the term is skipped). */
+int lible_gpu_one_electron_grad(lible_gpu_ctx *ctx, const double *D, const double *W, double *grad);
 
 /* ---- RI-K ------------------------------------------------------------------------------------
  * K_mn = sum_{PQ} (ml|P) [(P|Q)^{-1}]_{PQ} (Q|ns) D_ls, the exchange half of RI-JK (no reference

@@ -84,6 +84,8 @@ SIGNATURES = {
     "lible_gpu_nuclear_attraction": [P, P],
     "lible_gpu_external_charges": [P, P, I, P],
     "lible_gpu_one_electron": [P, P, I, P, P, P],
+    "lible_gpu_one_electron_batch": [P, I, I, I, LL, P, P, I, P],
+    "lible_gpu_one_electron_grad": [P, P, P, P],
     "lible_host_spherical_trafo": [I, P, P, P, P],
     "lible_host_shell_norms": [I, I, P, P, P],
     "lible_host_pair_classes": [S, S, I, P, P, I, I, P, P, P, P],

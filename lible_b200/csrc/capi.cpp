@@ -906,6 +906,36 @@ int lible_gpu_one_electron(lible_gpu_ctx *ctx, const double *charges, int n_char
     });
 }
 
+int lible_gpu_one_electron_batch(lible_gpu_ctx *ctx, int use_symm, int class_ab, int op, long long n,
+                                 const unsigned *pairs, const double *charges, int n_charges, double *out)
+{
+    return guard(ctx, [&](Engine &e) {
+        if (n < 0 || (n > 0 && (!pairs || !out)) || (charges && n_charges < 0))
+            throw EngineError(kStatusInvalid, "bad one-electron batch arguments");
+        const auto cls = e.pairClasses(use_symm != 0);
+        if (class_ab < 0 || class_ab >= (int)cls.size())
+            throw EngineError(kStatusInvalid, "bad class index");
+        const size_t blk = (size_t)(2 * cls[class_ab].la + 1) * (2 * cls[class_ab].lb + 1) * (op >= 3 ? 6 : 1);
+        DevArray o(out, (size_t)n * blk, false, e.stream());
+        e.oneElectronBatch(use_symm != 0, class_ab, op, n, pairs, charges, charges ? n_charges : 0, o.ptr);
+        o.copyOut();
+    });
+}
+
+int lible_gpu_one_electron_grad(lible_gpu_ctx *ctx, const double *D, const double *W, double *grad)
+{
+    return guard(ctx, [&](Engine &e) {
+        if (!grad)
+            throw EngineError(kStatusInvalid, "null grad");
+        const size_t n = e.nao();
+        DevArray d(D, n * n, true, e.stream()), w(W, n * n, true, e.stream());
+        DevArray g(grad, (size_t)e.nAtoms() * 3, false, e.stream());
+        e.oneElectronGrad(d.ptr, w.ptr, g.ptr);
+        e.sync();
+        g.copyOut();
+    });
+}
+
 int lible_gpu_overlap(lible_gpu_ctx *ctx, double *out)
 {
     return lible_gpu_one_electron(ctx, nullptr, 0, out, nullptr, nullptr);

@@ -175,6 +175,15 @@ namespace lible_b200
         // attraction of point charges ([n][4] x, y, z in bohr, q; with `nuclei` the atoms' nuclei).
         void oneElectron(const double *charges_host, int n_charges, bool nuclei, double *S_dev, double *T_dev,
                          double *V_dev);
+        // Per-pair one-electron blocks of class `cls` of shellPairData(use_symm) for the listed pairs:
+        // op 0..2 = S, T, V ([S_a][S_b] each), 3..5 = their first derivatives ([6][S_a][S_b]: A_xyz,
+        // B_xyz; V orbital part).  Charges as above, null = the nuclei.  out_dev: device memory.
+        void oneElectronBatch(bool use_symm, int cls, int op, long long n_tasks, const uint32_t *pairs_host,
+                              const double *charges_host, int n_charges, double *out_dev);
+        // grad[atom][xyz] = d/dR ( sum_mn D_mn (T + V)_mn - sum_mn W_mn S_mn ), the nuclei as the
+        // charges of V (orbital and operator parts); D, W symmetric device matrices, either may be null.
+        void oneElectronGrad(const double *D_dev, const double *W_dev, double *grad_dev);
+        std::vector<double> nucleiCharges() const;
 
         void sync();
         // Throws kStatusTimeout when a kernel reported a bounded wait that gave up (synchronises).

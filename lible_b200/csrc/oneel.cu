@@ -220,6 +220,413 @@ namespace lible_b200
             }
         }
 
+        // ---- per-pair blocks (the reference's kernel API) and the gradient contraction --------------
+        // Operators of the per-pair form: forward S, T, V ([S_a][S_b] per pair) and their first
+        // derivatives ([6][S_a][S_b]: A_x, A_y, A_z, B_x, B_y, B_z), V being the orbital part
+        // (src/lible/ints/oneelints.cpp: overlapD1Kernel :103-164, kineticEnergyD1Kernel :278-346,
+        // externalChargesD1Kernel :682-789).  The derivatives use dE/d(A - B) (hermiteE1) and, for
+        // V, the charge-summed Hermite integrals of one order higher:
+        //   d/dA = -((a/p) dP + dR),  d/dB = -((b/p) dP - dR),
+        //   dP_x = f sum E_t E_u E_v R_{t+1,u,v},  dR_x = f sum E1_t E_u E_v R_{tuv}.
+        enum OneOp : int
+        {
+            kOpS = 0,
+            kOpT = 1,
+            kOpV = 2,
+            kOpSD1 = 3,
+            kOpTD1 = 4,
+            kOpVD1 = 5,
+        };
+
+        struct OnePairArgs
+        {
+            int op;                  // OneOp (store mode)
+            long long n_tasks;
+            const uint32_t *list;    // pair index of each task (store mode), null = every pair
+            int n_pairs, nao;
+            const double *exps, *coeffs, *coords, *norms_a, *norms_b;
+            const uint32_t *pofs;
+            const int32_t *ao;       // [n_pairs][2]
+            const int32_t *atoms;    // [n_pairs][2] (gradient mode)
+            const int32_t *same;     // [n_pairs]: 1 when a and b are the same shell (gradient mode)
+            const double *charges;   // [n][4]
+            int n_charges;
+            const double *boys;
+            const int *sph_rc;
+            const double *sph_val;
+            int sph_ofs_a0, sph_ofs_a1, sph_ofs_b0, sph_ofs_b1;
+            double *out;             // store mode: [task][blocks][S_a][S_b]
+            const double *D, *W;     // gradient mode: full nao x nao (either may be null)
+            double *grad;            // [n_atoms][3]
+        };
+
+        template <int LA, int LB>
+        struct PairShape
+        {
+            static constexpr int L = LA + LB, L1 = L + 1;
+            static constexpr int NCA = (LA + 1) * (LA + 2) / 2, NCB = (LB + 1) * (LB + 2) / 2;
+            static constexpr int NC = NCA * NCB;
+            static constexpr int PER_LANE = (NC + 31) / 32;
+            static constexpr int NT = LA + LB + 3;
+            static constexpr int EAX = (LA + 1) * (LB + 3) * NT;
+            static constexpr int NR = (L + 1) * (L + 2) * (L + 3) / 6;
+            static constexpr int NR1 = (L1 + 1) * (L1 + 2) * (L1 + 3) / 6;
+            static constexpr int SA = 2 * LA + 1, SB = 2 * LB + 1;
+            // E and E1 tables, the charge-summed R (order L + 1), the density-weighted Hermite
+            // vector, then 6 Cartesian blocks (store) or the Cartesian D and W blocks (gradient)
+            static constexpr int WARP_DOUBLES = 6 * EAX + NR1 + NR + 6 * NC;
+        };
+
+        template <int LA, int LB, bool GRAD>
+        __global__ void __launch_bounds__(128) onePairKernel(OnePairArgs a)
+        {
+            using S = PairShape<LA, LB>;
+            constexpr int L = S::L, L1 = S::L1, NT = S::NT, NB = LB + 3;
+            extern __shared__ __align__(16) double smem2[];
+            const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+            double *E = smem2 + (size_t)warp * S::WARP_DOUBLES;  // [axis][i][j][t]
+            double *E1 = E + 3 * S::EAX;
+            double *Rs = E1 + 3 * S::EAX;                         // order L + 1
+            double *dt = Rs + S::NR1;                             // density-weighted Hermite vector
+            double *blk = dt + S::NR;                             // 6 x NC
+            const long long task = (long long)blockIdx.x * (blockDim.x >> 5) + warp;
+            if (task >= a.n_tasks)
+                return;
+            const int ipair = a.list ? (int)a.list[task] : (int)task;
+            auto ex = [&](int axis, int i, int j, int t) { return E[axis * S::EAX + (i * NB + j) * NT + t]; };
+            auto ex1 = [&](int axis, int i, int j, int t) { return E1[axis * S::EAX + (i * NB + j) * NT + t]; };
+            const int op = GRAD ? -1 : a.op;
+            const bool wantV = GRAD ? a.D != nullptr : (op == kOpV || op == kOpVD1);
+            const bool d1 = GRAD || op >= kOpSD1;
+            const int oa = a.ao[2 * ipair], ob = a.ao[2 * ipair + 1];
+            const size_t n = (size_t)a.nao;
+            const double *nA = a.norms_a + (size_t)ipair * S::SA, *nB = a.norms_b + (size_t)ipair * S::SB;
+            if constexpr (GRAD)
+            {
+                // Cartesian D and W blocks of the pair, with the AO norms and the pair's multiplicity
+                // in sum_{mn} (both orientations of an off-diagonal pair)
+                const double mult = a.same[ipair] ? 1.0 : 2.0;
+                for (int e = lane; e < S::NC; e += 32)
+                {
+                    const int ca = e / S::NCB, cb = e % S::NCB;
+                    double sd = 0.0, sw = 0.0;
+                    for (int ta = a.sph_ofs_a0; ta < a.sph_ofs_a1; ta++)
+                    {
+                        if (a.sph_rc[2 * ta + 1] != ca)
+                            continue;
+                        const int m = a.sph_rc[2 * ta];
+                        const double va = a.sph_val[ta] * nA[m];
+                        for (int tb = a.sph_ofs_b0; tb < a.sph_ofs_b1; tb++)
+                        {
+                            if (a.sph_rc[2 * tb + 1] != cb)
+                                continue;
+                            const int nn = a.sph_rc[2 * tb];
+                            const double f = va * a.sph_val[tb] * nB[nn];
+                            const size_t idx = (oa + m) * n + ob + nn;
+                            if (a.D)
+                                sd += f * a.D[idx];
+                            if (a.W)
+                                sw += f * a.W[idx];
+                        }
+                    }
+                    blk[e] = mult * sd;
+                    blk[S::NC + e] = mult * sw;
+                }
+                __syncwarp();
+            }
+            double acc[6][S::PER_LANE];
+#pragma unroll
+            for (int d = 0; d < 6; d++)
+#pragma unroll
+                for (int w = 0; w < S::PER_LANE; w++)
+                    acc[d][w] = 0.0;
+            double gA[3] = {0, 0, 0}, gB[3] = {0, 0, 0};
+            const double *A = a.coords + 6 * (size_t)ipair, *B = A + 3;
+            for (uint32_t pp = a.pofs[ipair]; pp < a.pofs[ipair + 1]; pp++)
+            {
+                const double ea = a.exps[2 * pp], eb = a.exps[2 * pp + 1];
+                const double dadb = a.coeffs[2 * pp] * a.coeffs[2 * pp + 1];
+                const double p = ea + eb, mu = ea * eb / p;
+                double P[3];
+#pragma unroll
+                for (int k = 0; k < 3; k++)
+                    P[k] = (ea * A[k] + eb * B[k]) / p;
+                if (lane < 3)
+                {
+                    const double d = A[lane] - B[lane];
+                    hermiteE(LA, LB + 2, 0.5 / p, P[lane] - A[lane], P[lane] - B[lane], exp(-mu * d * d),
+                             E + lane * S::EAX);
+                    if (d1)
+                        hermiteE1(LA, LB + 2, ea, eb, d, E + lane * S::EAX, E1 + lane * S::EAX);
+                }
+                if (wantV)
+                {
+                    double r[S::NR1];
+#pragma unroll
+                    for (int h = 0; h < S::NR1; h++)
+                        r[h] = 0.0;
+                    for (int c = lane; c < a.n_charges; c += 32)
+                    {
+                        const double *q = a.charges + 4 * (size_t)c;
+                        const double X = P[0] - q[0], Y = P[1] - q[1], Z = P[2] - q[2];
+                        double F[L1 + 1], R[S::NR1];
+                        boysF<L1, false>(p * (X * X + Y * Y + Z * Z), a.boys + (size_t)L1 * kBoysTerms * kBoysPitch, F);
+#pragma unroll
+                        for (int k = 0; k <= L1; k++)
+                            F[k] *= q[3];
+                        hermiteR<L1, double>(-2.0 * p, F, X, Y, Z, R);
+#pragma unroll
+                        for (int h = 0; h < S::NR1; h++)
+                            r[h] += R[h];
+                    }
+#pragma unroll
+                    for (int h = 0; h < S::NR1; h++)
+                    {
+                        double v = r[h];
+#pragma unroll
+                        for (int o = 16; o > 0; o >>= 1)
+                            v += __shfl_xor_sync(0xffffffffu, v, o);
+                        if (lane == 0)
+                            Rs[h] = v;
+                    }
+                }
+                __syncwarp();
+                const double fs = dadb * pow(3.14159265358979323846 / p, 1.5);
+                const double fv = 2.0 * 3.14159265358979323846 / p * dadb;
+                const double b2 = eb * eb;
+#pragma unroll
+                for (int w = 0; w < S::PER_LANE; w++)
+                {
+                    const int e = lane + 32 * w;
+                    if (e >= S::NC)
+                        break;
+                    int ijk[3], ijk_[3];
+                    cartExps(LA, e / S::NCB, ijk[0], ijk[1], ijk[2]);
+                    cartExps(LB, e % S::NCB, ijk_[0], ijk_[1], ijk_[2]);
+                    double s0[3], s1[3];
+#pragma unroll
+                    for (int x = 0; x < 3; x++)
+                    {
+                        s0[x] = ex(x, ijk[x], ijk_[x], 0);
+                        s1[x] = d1 ? ex1(x, ijk[x], ijk_[x], 0) : 0.0;
+                    }
+                    // kinetic factor of one axis from table E (tab 0) or E1 (tab 1)
+                    auto kin = [&](int tab, int x) {
+                        const int m = ijk[x], m_ = ijk_[x];
+                        auto g = [&](int jj) { return tab ? ex1(x, m, jj, 0) : ex(x, m, jj, 0); };
+                        double t = -2.0 * b2 * g(m_ + 2) + eb * (2 * m_ + 1) * g(m_);
+                        if (m_ >= 2)
+                            t -= 0.5 * m_ * (m_ - 1) * g(m_ - 2);
+                        return t;
+                    };
+                    // V pieces: sum over t <= i + i', u, v of the E products times R (optionally shifted)
+                    auto vsum = [&](int dx, int use1) {
+                        double v = 0.0;
+                        for (int t = 0; t <= ijk[0] + ijk_[0]; t++)
+                            for (int u = 0; u <= ijk[1] + ijk_[1]; u++)
+                                for (int s = 0; s <= ijk[2] + ijk_[2]; s++)
+                                {
+                                    const double e0 = (use1 == 0 ? ex1(0, ijk[0], ijk_[0], t) : ex(0, ijk[0], ijk_[0], t)) *
+                                                      (use1 == 1 ? ex1(1, ijk[1], ijk_[1], u) : ex(1, ijk[1], ijk_[1], u)) *
+                                                      (use1 == 2 ? ex1(2, ijk[2], ijk_[2], s) : ex(2, ijk[2], ijk_[2], s));
+                                    v += e0 * Rs[hermIndex(t + (dx == 0), u + (dx == 1), s + (dx == 2))];
+                                }
+                        return v;
+                    };
+                    if (!GRAD)
+                    {
+                        if (op == kOpS)
+                            acc[0][w] += fs * s0[0] * s0[1] * s0[2];
+                        else if (op == kOpT)
+                            acc[0][w] += fs * (kin(0, 0) * s0[1] * s0[2] + s0[0] * kin(0, 1) * s0[2] +
+                                               s0[0] * s0[1] * kin(0, 2));
+                        else if (op == kOpV)
+                            acc[0][w] -= fv * vsum(-1, -1);
+                        else
+                        {
+#pragma unroll
+                            for (int x = 0; x < 3; x++)
+                            {
+                                double dA, dB;
+                                if (op == kOpSD1)
+                                {
+                                    const double v = fs * (x == 0 ? s1[0] : s0[0]) * (x == 1 ? s1[1] : s0[1]) *
+                                                     (x == 2 ? s1[2] : s0[2]);
+                                    dA = v;
+                                    dB = -v;
+                                }
+                                else if (op == kOpTD1)
+                                {
+                                    // the x-axis table replaced by E1 in every term
+                                    const double sx = x == 0 ? s1[0] : s0[0], sy = x == 1 ? s1[1] : s0[1],
+                                                 sz = x == 2 ? s1[2] : s0[2];
+                                    const double v = fs * (kin(x == 0, 0) * sy * sz + sx * kin(x == 1, 1) * sz +
+                                                           sx * sy * kin(x == 2, 2));
+                                    dA = v;
+                                    dB = -v;
+                                }
+                                else
+                                {
+                                    const double dp = fv * vsum(x, -1), dr = fv * vsum(-1, x);
+                                    dA = -((ea / p) * dp + dr);
+                                    dB = -((eb / p) * dp - dr);
+                                }
+                                acc[x][w] += dA;
+                                acc[3 + x][w] += dB;
+                            }
+                        }
+                    }
+                    else
+                    {
+                        const double dd = blk[e], ww = blk[S::NC + e];
+#pragma unroll
+                        for (int x = 0; x < 3; x++)
+                        {
+                            const double sx = x == 0 ? s1[0] : s0[0], sy = x == 1 ? s1[1] : s0[1],
+                                         sz = x == 2 ? s1[2] : s0[2];
+                            // overlap (with W) and kinetic (with D): d/dB = -d/dA
+                            double g = -ww * fs * sx * sy * sz;
+                            if (a.D)
+                                g += dd * fs * (kin(x == 0, 0) * sy * sz + sx * kin(x == 1, 1) * sz + sx * sy * kin(x == 2, 2));
+                            gA[x] += g;
+                            gB[x] -= g;
+                            if (a.D)
+                            {
+                                const double dp = fv * vsum(x, -1), dr = fv * vsum(-1, x);
+                                gA[x] -= dd * ((ea / p) * dp + dr);
+                                gB[x] -= dd * ((eb / p) * dp - dr);
+                            }
+                        }
+                    }
+                }
+                if (GRAD && a.D)
+                {
+                    // operator part: d/dC_x of -f q_C sum D E R(P - C) = f q_C sum D E R_{t+1}
+                    __syncwarp();
+                    for (int h = lane; h < S::NR; h += 32)
+                    {
+                        int t0 = 0, u0 = 0, v0 = 0;
+                        for (int nn = 0, idx = 0; nn <= L; nn++)
+                            for (int t = nn; t >= 0; t--)
+                                for (int u = nn - t; u >= 0; u--, idx++)
+                                    if (idx == h)
+                                    {
+                                        t0 = t;
+                                        u0 = u;
+                                        v0 = nn - t - u;
+                                    }
+                        double v = 0.0;
+                        for (int e = 0; e < S::NC; e++)
+                        {
+                            int i, j, k, i_, j_, k_;
+                            cartExps(LA, e / S::NCB, i, j, k);
+                            cartExps(LB, e % S::NCB, i_, j_, k_);
+                            if (t0 > i + i_ || u0 > j + j_ || v0 > k + k_)
+                                continue;
+                            v += blk[e] * ex(0, i, i_, t0) * ex(1, j, j_, u0) * ex(2, k, k_, v0);
+                        }
+                        dt[h] = fv * v;
+                    }
+                    __syncwarp();
+                    for (int c = lane; c < a.n_charges; c += 32)
+                    {
+                        const double *q = a.charges + 4 * (size_t)c;
+                        const double X = P[0] - q[0], Y = P[1] - q[1], Z = P[2] - q[2];
+                        double F[L1 + 1], R[S::NR1];
+                        boysF<L1, false>(p * (X * X + Y * Y + Z * Z), a.boys + (size_t)L1 * kBoysTerms * kBoysPitch, F);
+                        hermiteR<L1, double>(-2.0 * p, F, X, Y, Z, R);
+                        double g[3] = {0, 0, 0};
+                        for (int nn = 0, h = 0; nn <= L; nn++)
+                            for (int t = nn; t >= 0; t--)
+                                for (int u = nn - t; u >= 0; u--, h++)
+                                {
+                                    const int v = nn - t - u;
+                                    g[0] += dt[h] * R[hermIndex(t + 1, u, v)];
+                                    g[1] += dt[h] * R[hermIndex(t, u + 1, v)];
+                                    g[2] += dt[h] * R[hermIndex(t, u, v + 1)];
+                                }
+                        // charge c is atom c (the nuclei in atom order)
+                        for (int x = 0; x < 3; x++)
+                            atomicAdd(a.grad + 3 * (size_t)c + x, q[3] * g[x]);
+                    }
+                }
+                __syncwarp();
+            }
+            if constexpr (GRAD)
+            {
+#pragma unroll
+                for (int x = 0; x < 3; x++)
+                {
+                    double u = gA[x], v = gB[x];
+#pragma unroll
+                    for (int o = 16; o > 0; o >>= 1)
+                    {
+                        u += __shfl_xor_sync(0xffffffffu, u, o);
+                        v += __shfl_xor_sync(0xffffffffu, v, o);
+                    }
+                    if (lane == 0)
+                    {
+                        atomicAdd(a.grad + 3 * (size_t)a.atoms[2 * ipair] + x, u);
+                        atomicAdd(a.grad + 3 * (size_t)a.atoms[2 * ipair + 1] + x, v);
+                    }
+                }
+            }
+            else
+            {
+                // spherical transform and norms of each stored block
+                const int nblk = d1 ? 6 : 1;
+                for (int d = 0; d < nblk; d++)
+#pragma unroll
+                    for (int w = 0; w < S::PER_LANE; w++)
+                    {
+                        const int e = lane + 32 * w;
+                        if (e < S::NC)
+                            blk[d * S::NC + e] = acc[d][w];
+                    }
+                __syncwarp();
+                double *out = a.out + (size_t)task * nblk * S::SA * S::SB;
+                for (int o = lane; o < nblk * S::SA * S::SB; o += 32)
+                {
+                    const int d = o / (S::SA * S::SB), m = (o / S::SB) % S::SA, nn = o % S::SB;
+                    double sum = 0.0;
+                    for (int ta = a.sph_ofs_a0; ta < a.sph_ofs_a1; ta++)
+                    {
+                        if (a.sph_rc[2 * ta] != m)
+                            continue;
+                        const int ca = a.sph_rc[2 * ta + 1];
+                        for (int tb = a.sph_ofs_b0; tb < a.sph_ofs_b1; tb++)
+                            if (a.sph_rc[2 * tb] == nn)
+                                sum += a.sph_val[ta] * a.sph_val[tb] * blk[d * S::NC + ca * S::NCB + a.sph_rc[2 * tb + 1]];
+                    }
+                    out[o] = nA[m] * nB[nn] * sum;
+                }
+            }
+        }
+
+        using PairFn = void (*)(const OnePairArgs &, cudaStream_t, bool);
+        template <int LA, int LB>
+        void launchPair(const OnePairArgs &a, cudaStream_t s, bool grad)
+        {
+            constexpr int warps = 4;
+            const size_t smem = sizeof(double) * warps * PairShape<LA, LB>::WARP_DOUBLES;
+            auto k = grad ? onePairKernel<LA, LB, true> : onePairKernel<LA, LB, false>;
+            if (smem > 48 * 1024)
+                cudaCheck(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "attr");
+            k<<<(unsigned)((a.n_tasks + warps - 1) / warps), 32 * warps, smem, s>>>(a);
+            cudaCheck(cudaGetLastError(), "one-electron pair kernel");
+        }
+
+        PairFn lookupPair(int la, int lb)
+        {
+            static const PairFn table[4][4] = {
+                {&launchPair<0, 0>, &launchPair<0, 1>, &launchPair<0, 2>, &launchPair<0, 3>},
+                {&launchPair<1, 0>, &launchPair<1, 1>, &launchPair<1, 2>, &launchPair<1, 3>},
+                {&launchPair<2, 0>, &launchPair<2, 1>, &launchPair<2, 2>, &launchPair<2, 3>},
+                {&launchPair<3, 0>, &launchPair<3, 1>, &launchPair<3, 2>, &launchPair<3, 3>},
+            };
+            return (la < 4 && lb < 4) ? table[la][lb] : nullptr;
+        }
+
         using OneFn = void (*)(const OneArgs &, cudaStream_t, int);
         template <int LA, int LB>
         void launchOne(const OneArgs &a, cudaStream_t s, int)
@@ -253,6 +660,158 @@ namespace lible_b200
         }
     }
 
+    namespace
+    {
+        // Device copies of the host fields of one pair class that the one-electron kernels read.
+        struct OneClassData
+        {
+            DevBuf<double> ex, co, xy, na, nb;
+            DevBuf<uint32_t> po;
+            DevBuf<int32_t> ao, atoms, same;
+            OneClassData(const PairClass &pc, cudaStream_t s)
+            {
+                std::vector<int32_t> ao_h(2 * pc.n_pairs), at_h(2 * pc.n_pairs), same_h(pc.n_pairs);
+                for (size_t i = 0; i < pc.n_pairs; i++)
+                {
+                    ao_h[2 * i] = pc.ao_a[i];
+                    ao_h[2 * i + 1] = pc.ao_b[i];
+                    at_h[2 * i] = pc.atom_a[i];
+                    at_h[2 * i + 1] = pc.atom_b[i];
+                    same_h[i] = pc.shell_a[i] == pc.shell_b[i];
+                }
+                upload(ex, pc.exps, s);
+                upload(co, pc.coeffs, s);
+                upload(xy, pc.coords, s);
+                upload(na, pc.norms_a, s);
+                upload(nb, pc.norms_b, s);
+                upload(po, pc.pofs, s);
+                upload(ao, ao_h, s);
+                upload(atoms, at_h, s);
+                upload(same, same_h, s);
+            }
+        };
+    }
+
+    // The nuclei as point charges, one per atom in atom order: x, y, z (bohr), Z.
+    std::vector<double> Engine::nucleiCharges() const
+    {
+        std::vector<double> q;
+        int next = 0;
+        for (const Shell &sh : shells_)
+            if ((int)sh.atom == next)
+            {
+                q.insert(q.end(), {sh.xyz[0], sh.xyz[1], sh.xyz[2], (double)sh.z});
+                next++;
+            }
+        if (next != n_atoms_)
+            throw EngineError(kStatusInternal, "atoms without basis shells");
+        return q;
+    }
+
+    void Engine::oneElectronBatch(bool use_symm, int cls, int op, long long n_tasks, const uint32_t *pairs_host,
+                                  const double *charges_host, int n_charges, double *out_dev)
+    {
+        requireSingle();
+        ClassSet &cs = mainSet(use_symm);
+        if (cls < 0 || cls >= (int)cs.host.size())
+            throw EngineError(kStatusInvalid, "bad class index");
+        if (op < 0 || op > 5)
+            throw EngineError(kStatusInvalid, "bad one-electron operator");
+        const PairClass &pc = cs.host[cls];
+        const PairFn fn = lookupPair(pc.la, pc.lb);
+        if (!fn)
+            throw EngineError(kStatusUnsupported, "one-electron kernels are instantiated for l <= 3");
+        if (n_tasks <= 0)
+            return;
+        std::vector<uint32_t> list(pairs_host, pairs_host + n_tasks);
+        for (uint32_t i : list)
+            if (i >= pc.n_pairs)
+                throw EngineError(kStatusInvalid, "pair index out of range");
+        std::vector<double> q = charges_host ? std::vector<double>(charges_host, charges_host + 4 * (size_t)n_charges)
+                                             : nucleiCharges();
+        OneClassData d(pc, stream_);
+        DevBuf<uint32_t> dl;
+        DevBuf<double> dq;
+        upload(dl, list, stream_);
+        upload(dq, q, stream_);
+        OnePairArgs a{};
+        a.op = op;
+        a.n_tasks = n_tasks;
+        a.list = dl.p;
+        a.n_pairs = (int)pc.n_pairs;
+        a.nao = (int)nao_;
+        a.exps = d.ex.p;
+        a.coeffs = d.co.p;
+        a.coords = d.xy.p;
+        a.norms_a = d.na.p;
+        a.norms_b = d.nb.p;
+        a.pofs = d.po.p;
+        a.ao = d.ao.p;
+        a.atoms = d.atoms.p;
+        a.same = d.same.p;
+        a.charges = dq.p;
+        a.n_charges = (int)(q.size() / 4);
+        a.boys = boys_;
+        a.sph_rc = sph_rc_;
+        a.sph_val = sph_val_;
+        a.sph_ofs_a0 = sph_ofs_[pc.la];
+        a.sph_ofs_a1 = sph_ofs_[pc.la + 1];
+        a.sph_ofs_b0 = sph_ofs_[pc.lb];
+        a.sph_ofs_b1 = sph_ofs_[pc.lb + 1];
+        a.out = out_dev;
+        fn(a, stream_, false);
+        cudaCheck(cudaStreamSynchronize(stream_), "one-electron batch");
+    }
+
+    void Engine::oneElectronGrad(const double *D_dev, const double *W_dev, double *grad_dev)
+    {
+        requireSingle();
+        if (max_l_ > 3)
+            throw EngineError(kStatusUnsupported, "one-electron kernels are instantiated for l <= 3");
+        cudaCheck(cudaMemsetAsync(grad_dev, 0, (size_t)n_atoms_ * 3 * sizeof(double), stream_), "memset");
+        if (!D_dev && !W_dev)
+            return;
+        const std::vector<double> q = nucleiCharges();
+        DevBuf<double> dq;
+        upload(dq, q, stream_);
+        ClassSet &cs = mainSet(true);
+        for (size_t c = 0; c < cs.host.size(); c++)
+        {
+            const PairClass &pc = cs.host[c];
+            if (pc.n_pairs == 0)
+                continue;
+            OneClassData d(pc, stream_);
+            OnePairArgs a{};
+            a.n_tasks = (long long)pc.n_pairs;
+            a.list = nullptr;
+            a.n_pairs = (int)pc.n_pairs;
+            a.nao = (int)nao_;
+            a.exps = d.ex.p;
+            a.coeffs = d.co.p;
+            a.coords = d.xy.p;
+            a.norms_a = d.na.p;
+            a.norms_b = d.nb.p;
+            a.pofs = d.po.p;
+            a.ao = d.ao.p;
+            a.atoms = d.atoms.p;
+            a.same = d.same.p;
+            a.charges = dq.p;
+            a.n_charges = (int)(q.size() / 4);
+            a.boys = boys_;
+            a.sph_rc = sph_rc_;
+            a.sph_val = sph_val_;
+            a.sph_ofs_a0 = sph_ofs_[pc.la];
+            a.sph_ofs_a1 = sph_ofs_[pc.la + 1];
+            a.sph_ofs_b0 = sph_ofs_[pc.lb];
+            a.sph_ofs_b1 = sph_ofs_[pc.lb + 1];
+            a.D = D_dev;
+            a.W = W_dev;
+            a.grad = grad_dev;
+            lookupPair(pc.la, pc.lb)(a, stream_, true);
+            cudaCheck(cudaStreamSynchronize(stream_), "one-electron gradient");
+        }
+    }
+
     void Engine::oneElectron(const double *charges_host, int n_charges, bool nuclei, double *S_dev, double *T_dev,
                              double *V_dev)
     {
@@ -263,16 +822,7 @@ namespace lible_b200
         // the point charges: the nuclei (one per atom, in atom order) or the caller's list
         std::vector<double> q;
         if (nuclei)
-        {
-            std::vector<int> seen;
-            for (const Shell &sh : shells_)
-            {
-                if (std::find(seen.begin(), seen.end(), (int)sh.atom) != seen.end())
-                    continue;
-                seen.push_back((int)sh.atom);
-                q.insert(q.end(), {sh.xyz[0], sh.xyz[1], sh.xyz[2], (double)sh.z});
-            }
-        }
+            q = nucleiCharges();
         else if (n_charges > 0)
             q.assign(charges_host, charges_host + 4 * (size_t)n_charges);
         DevBuf<double> dq;

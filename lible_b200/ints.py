@@ -490,6 +490,65 @@ def one_electron(structure, point_charges=None):
     return S, T, V
 
 
+def _one_batch(op, ipair, sp, charges=None):
+    """Per-pair one-electron blocks through lible_gpu_one_electron_batch; `ipair` an index (returns
+    the block, or the list of 6 derivative blocks) or a sequence of indices (returns an array)."""
+    single = np.ndim(ipair) == 0
+    idx = np.ascontiguousarray(np.atleast_1d(np.asarray(ipair, dtype=np.uint32)))
+    nb = 6 if op >= 3 else 1
+    out = np.empty((len(idx), nb, _nsph(sp.la_), _nsph(sp.lb_)))
+    if charges is None:
+        q, nq = None, 0
+    else:
+        q = _f64(charges).reshape(-1, 4)
+        nq = len(q)
+    _call(sp.structure, "lible_gpu_one_electron_batch", int(sp.uses_symm), int(sp.index), int(op), int(len(idx)),
+          _ptr(idx), _ptr(q), nq, _ptr(out))
+    if nb == 1:
+        out = out[:, 0]
+    if single:
+        return list(out[0]) if nb > 1 else out[0]
+    return out
+
+
+def overlapKernel(ipair, sp_data):
+    """lible::ints::overlapKernel (ints.hpp:33)."""
+    return _one_batch(0, ipair, sp_data)
+
+
+def kineticEnergyKernel(ipair, sp_data):
+    """lible::ints::kineticEnergyKernel (ints.hpp:42)."""
+    return _one_batch(1, ipair, sp_data)
+
+
+def externalChargesKernel(ipair, charges, sp_data):
+    """lible::ints::externalChargesKernel (ints.hpp:66); the Boys grid argument is not needed."""
+    return _one_batch(2, ipair, sp_data, charges)
+
+
+def overlapD1Kernel(ipair, sp_data):
+    """lible::ints::overlapD1Kernel (ints.hpp:36): [d/dA x, y, z, d/dB x, y, z]."""
+    return _one_batch(3, ipair, sp_data)
+
+
+def kineticEnergyD1Kernel(ipair, sp_data):
+    """lible::ints::kineticEnergyD1Kernel (ints.hpp:45)."""
+    return _one_batch(4, ipair, sp_data)
+
+
+def externalChargesD1Kernel(ipair, charges, sp_data):
+    """lible::ints::externalChargesD1Kernel (ints.hpp:79): the orbital part."""
+    return _one_batch(5, ipair, sp_data, charges)
+
+
+def one_electron_grad(structure, D=None, W=None):
+    """[n_atoms][3] gradient of sum D (T + V) - sum W S with respect to the nuclear coordinates."""
+    g = np.empty((structure.n_atoms, 3))
+    _call(structure, "lible_gpu_one_electron_grad", _ptr(_f64(D)) if D is not None else None,
+          _ptr(_f64(W)) if W is not None else None, _ptr(g))
+    return g
+
+
 def rik(structure, D=None, C=None, schwarz=1e-12, info=False):
     """RI-K: K_mn = sum_PQ (ml|P) [(P|Q)^-1]_PQ (Q|ns) D_ls.  Give the density factor C ([nao][occ],
     D = C C^T) or the symmetric D itself (factorised on the device by its eigendecomposition).

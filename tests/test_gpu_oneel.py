@@ -66,3 +66,58 @@ def test_one_electron_f_shells_and_random_charges_vs_reference():
     # symmetric (diagonal shell blocks are written from both orientations, as in the reference, so
     # to the last bit only), and the same matrices as the single-operator calls
     assert np.abs(S - S.T).max() <= 1e-15 and np.abs(L.overlap(s) - S).max() == 0.0
+
+
+def _kernel_blocks(structure, use_symm, fn, *args):
+    parts = []
+    for sp in L.shellPairData(use_symm, structure):
+        if sp.n_pairs_:
+            parts.append(np.asarray(fn(list(range(sp.n_pairs_)), *args, sp)).ravel())
+    return np.concatenate(parts)
+
+
+def test_per_pair_kernels_golden():
+    # the reference's kernel-API golden sums (test/tests_ints.cpp:185-300, 381-480): blocks summed
+    # in class / pair / [derivative] / element order, as the reference's loops do
+    c2h4 = L.Structure("cc-pvdz", C2H4_Z, C2H4_ANG)
+    assert golden(seqsum(_kernel_blocks(c2h4, True, L.overlapKernel)), 137.049592196795)
+    assert golden(seqsum(_kernel_blocks(c2h4, False, L.overlapD1Kernel)), 712.697494155785)
+    assert golden(seqsum(_kernel_blocks(c2h4, False, L.kineticEnergyKernel)), 252.755644635020)
+    assert golden(seqsum(_kernel_blocks(c2h4, False, L.kineticEnergyD1Kernel)), 1153.592041307799)
+    co2 = L.Structure("6-31+g", CO2_Z, CO2_ANG)
+    q = np.array([[x / 0.5291772083 for x in c] + [z] for c, z in zip(CO2_ANG, CO2_Z)])
+    assert golden(seqsum(_kernel_blocks(co2, True, L.externalChargesKernel, q)), 1338.606063918550)
+    assert golden(seqsum(_kernel_blocks(co2, True, L.externalChargesD1Kernel, q)), 3274.419345348923)
+    # a single pair returns the block, or the list of six derivative blocks
+    sp = L.shellPairData(True, c2h4)[0]
+    assert np.abs(L.overlapKernel(0, sp) - L.overlapKernel([0], sp)[0]).max() == 0.0
+    assert len(L.overlapD1Kernel(0, sp)) == 6
+
+
+def test_one_electron_gradient_vs_finite_differences():
+    """d/dR (sum D (T + V) - sum W S) against central differences (step 1e-4 bohr) of the forward
+    integrals, cc-pVDZ and cc-pVTZ (f shells); translational invariance of the total."""
+    for basis, nw, seed in (("cc-pvdz", 2, 3), ("cc-pvtz", 1, 8)):
+        Z, xyz, rng = water_cluster(nw, seed)
+        s = L.Structure(basis, Z, xyz, units="bohr")
+        n = s.nao
+        C = np.linalg.qr(rng.standard_normal((n, 5 * nw)))[0]
+        D = C @ C.T
+        X = rng.standard_normal((n, n)) * 0.1
+        W = X + X.T
+        g = L.one_electron_grad(s, D, W)
+        assert np.abs(g.sum(axis=0)).max() <= 1e-9 * max(1.0, np.abs(g).max())
+
+        def energy(c):
+            S, T, V = L.one_electron(L.Structure(basis, Z, c, units="bohr"))
+            return float(np.sum(D * (T + V)) - np.sum(W * S))
+
+        h = 1e-4
+        for atom, x in ((0, 0), (1, 1), (len(Z) - 1, 2)):
+            cp, cm = xyz.copy(), xyz.copy()
+            cp[atom, x] += h
+            cm[atom, x] -= h
+            fd = (energy(cp) - energy(cm)) / (2 * h)
+            assert abs(fd - g[atom, x]) <= 1e-6 * max(1.0, abs(fd)), (basis, atom, x, fd, g[atom, x])
+        # the D and W terms separately add up to the whole
+        assert np.abs(L.one_electron_grad(s, D, None) + L.one_electron_grad(s, None, W) - g).max() <= 1e-10
