@@ -223,7 +223,8 @@ def run_rij(Z, xyz, D, J64, steps):
 
 def run_rijk(Z, xyz, D, J64, K64, occ, steps):
     """RI-JK of the (H2O)_32 workload with def2-universal-jkfit (3,616 auxiliary functions): wall
-    time of lible_gpu_rij (host D -> host J) and of lible_gpu_rik from the occupied factor C
+    time of lible_gpu_rij (host D -> host J), of the RI-J nuclear gradient, and of lible_gpu_rik from
+    the occupied factor C
     (host C -> host K; D = C C^T, C from the eigenvectors of D), with the per-stage device times
     and rates of the exchange build, and the RI errors against the direct FP64 J and K of the same
     run.  The first call of each builds and factorises (P|Q), which later calls reuse."""
@@ -249,10 +250,16 @@ def run_rijk(Z, xyz, D, J64, K64, occ, steps):
     t = time.perf_counter()
     Kd = L.rik(s, D=D, schwarz=SCHWARZ)
     t_dpath = time.perf_counter() - t
+    L.rij_grad(s, D, SCHWARZ)
+    t = time.perf_counter()
+    gJ, _ = L.rij_grad(s, D, SCHWARZ)
+    t_grad = time.perf_counter() - t
     rates = {k: info["flops_" + k] / max(info["t_" + k], 1e-12) / 1e12 for k in ("gemm", "solve", "syrk")}
     return {"workload": "RI-JK, (H2O)_32 cc-pVDZ / def2-universal-jkfit, FP64, occupied factor C (160)",
             "naux": s.naux, "setup_s": setup, "first_call_s": first, "rij_s": float(np.mean(tj)),
-            "rik_s": float(np.mean(tk)), "rik_from_D_s": t_dpath, "solve": L.rij_last_solve(s),
+            "rik_s": float(np.mean(tk)), "rik_from_D_s": t_dpath, "rij_gradient_s": t_grad,
+            "rij_gradient_translational_residual": float(np.abs(gJ.sum(axis=0)).max()),
+            "solve": L.rij_last_solve(s),
             "rik_stages_s": {k: info["t_" + k] for k in ("ints", "gemm", "solve", "syrk")},
             "rik_stage_tflops": rates, "rik_aux_blocks": info["n_blocks"],
             "dEJ_Eh_vs_direct": float(0.5 * np.sum(D * (Jri - J64))),

@@ -219,6 +219,12 @@ int lible_gpu_rij(lible_gpu_ctx *ctx, const double *D, double schwarz_threshold,
  * smallest kept and largest eigenvalue, `dropped` eigenpairs below 1e-12 of the largest left out);
  * -1 = none yet.  Any output may be NULL. */
 int lible_gpu_rij_last_solve(lible_gpu_ctx *ctx, int *method, double *lo, double *hi, int *dropped, double *shift);
+/* Gradient of the RI-J energy E = 1/2 gamma^T (P|Q)^{-1} gamma (= 1/2 Tr(D J_RI)) with respect to
+ * the nuclear coordinates, grad[n_atoms][3]:
+ *   sum_P d_P sum_mn D_mn d(mn|P)/dR - 1/2 sum_PQ d_P d_Q d(P|Q)/dR,   d = (P|Q)^{-1} gamma,
+ * the derivative integrals (ERI3D1 / ERI2D1 semantics, src/lible/ints/twoel/eri_kernels.hpp:134-169)
+ * contracted inside the class kernels.  D symmetric; `energy` (may be NULL) receives E. */
+int lible_gpu_rij_grad(lible_gpu_ctx *ctx, const double *D, double schwarz_threshold, double *grad, double *energy);
 /* The two contractions separately (either output may be NULL). */
 int lible_gpu_ri_contract(lible_gpu_ctx *ctx, const double *D, const double *dcoef, double schwarz_threshold,
                           double *gamma, double *J);

@@ -79,6 +79,7 @@ SIGNATURES = {
     "lible_gpu_ri_contract": [P, P, P, D, P, P],
     "lible_gpu_rij_last_solve": [P, P, P, P, P, P],
     "lible_gpu_rik": [P, P, P, LL, D, P, ctypes.POINTER(RIKInfo)],
+    "lible_gpu_rij_grad": [P, P, D, P, ctypes.POINTER(D)],
     "lible_gpu_overlap": [P, P],
     "lible_gpu_kinetic_energy": [P, P],
     "lible_gpu_nuclear_attraction": [P, P],

@@ -959,6 +959,34 @@ int lible_gpu_external_charges(lible_gpu_ctx *ctx, const double *charges, int n_
     return lible_gpu_one_electron(ctx, charges ? charges : none, charges ? n_charges : 0, nullptr, nullptr, out);
 }
 
+int lible_gpu_rij_grad(lible_gpu_ctx *ctx, const double *D, double schwarz_threshold, double *grad, double *energy)
+{
+    return guard(ctx, [&](Engine &e) {
+        if (!e.hasAux())
+            throw EngineError(kStatusNoAux, "RI approximation is not enabled");
+        if (!D || !grad)
+            throw EngineError(kStatusInvalid, "null D/grad");
+        const size_t n = e.nao(), na = e.naux();
+        DevArray d(D, n * n, true, e.stream());
+        DevArray g(grad, (size_t)e.nAtoms() * 3, false, e.stream());
+        DevBuf<double> rhs(na);
+        e.riContract(d.ptr, nullptr, rhs.p, nullptr, schwarz_threshold);
+        std::vector<double> gamma(na), dc(na);
+        cudaCheck(cudaMemcpy(gamma.data(), rhs.p, na * 8, cudaMemcpyDeviceToHost), "copy");
+        solveMetric(e, ctx->metricFactor(e), rhs.p);
+        e.riGradient(d.ptr, rhs.p, g.ptr, schwarz_threshold);
+        g.copyOut();
+        if (energy)
+        {
+            cudaCheck(cudaMemcpy(dc.data(), rhs.p, na * 8, cudaMemcpyDeviceToHost), "copy");
+            double s = 0.0;
+            for (size_t i = 0; i < na; i++)
+                s += gamma[i] * dc[i];
+            *energy = 0.5 * s;
+        }
+    });
+}
+
 int lible_gpu_rik(lible_gpu_ctx *ctx, const double *D, const double *C, long long n_occ, double schwarz_threshold,
                   double *K, lible_gpu_rik_info *info)
 {

@@ -45,6 +45,7 @@ namespace lible_b200
         kD1Store = 4,    // write the 12 derivative blocks
         kD1Grad = 5,     // contract the derivative blocks with the two-particle density
         kRIStore = 6,    // out[P - ri_lo][m][n] = out[P - ri_lo][n][m] = (mn|P), P in [ri_lo, ri_hi)
+        kD1GradRI = 7,   // RI-J gradient: derivative blocks contracted with D_mn d_P (3c) or d_P d_Q (2c)
     };
 
     struct QuartetArgs
@@ -96,7 +97,7 @@ namespace lible_b200
         // epilogue
         int mode;
         int flags;                        // kStore: bit0 swap bra shells, bit1 swap ket shells, bit2 swap bra/ket
-        int aux_side;                     // RI modes: 0 = ket is the auxiliary side, 1 = bra
+        int aux_side;                     // RI modes: 0 = ket is the auxiliary side, 1 = bra, 2 = both
         int ri_lo, ri_hi;                 // kRIStore: the block of auxiliary functions written
         double *out;
         const double *D;

@@ -2137,6 +2137,97 @@ namespace lible_b200
         checkStatus();
     }
 
+    // Unique auxiliary shell pairs (P|Q) with the RI plan's Schwarz test, for the two-centre part of
+    // the RI-J gradient.
+    Engine::JKPlan &Engine::ri2Plan(double thr)
+    {
+        ClassSet &xs = auxSet();
+        ensureSchwarz(xs);
+        char key[64];
+        snprintf(key, sizeof(key), "2c %.6e", thr);
+        auto it = ri_plans_.find(key);
+        if (it != ri_plans_.end())
+            return it->second;
+        JKPlan plan;
+        for (size_t ca = 0; ca < xs.dev.size(); ca++)
+            for (size_t cb = 0; cb <= ca; cb++)
+            {
+                // the larger pair type in the bra, as the class kernels are instantiated
+                const bool swap = pairType(xs.dev[ca].la, 0) < pairType(xs.dev[cb].la, 0);
+                const int b = swap ? (int)cb : (int)ca, k = swap ? (int)ca : (int)cb;
+                JKClassPair cp = buildClassPair(xs, b, xs, k, ca == cb, thr, 0.0, false);
+                if (cp.n64 == 0)
+                    continue;
+                plan.n_quartets += cp.n64;
+                plan.pairs.push_back(cp);
+            }
+        plan.counters = devAlloc<unsigned long long>(2 * std::max<size_t>(plan.pairs.size(), 1));
+        cudaCheck(cudaStreamSynchronize(stream_), "plan");
+        plan.thr = thr;
+        return ri_plans_.emplace(key, std::move(plan)).first->second;
+    }
+
+    void Engine::riGradient(const double *D_dev, const double *dcoef_dev, double *grad_dev, double schwarz)
+    {
+        requireSingle();
+        ClassSet &ms = mainSet(true);
+        ClassSet &xs = auxSet();
+        JKPlan &p3 = riPlan(schwarz);
+        JKPlan &p2 = ri2Plan(schwarz);
+        cudaCheck(cudaMemsetAsync(grad_dev, 0, 3 * n_atoms_ * sizeof(double), stream_), "memset");
+        cudaCheck(cudaMemsetAsync(d_status_, 0, sizeof(int), stream_), "memset");
+        for (JKPlan *plan : {&p3, &p2})
+        {
+            const bool two = plan == &p2;
+            cudaCheck(cudaMemsetAsync(plan->counters, 0, 2 * plan->pairs.size() * sizeof(unsigned long long), stream_),
+                      "memset");
+            for (size_t ip = 0; ip < plan->pairs.size(); ip++)
+            {
+                auto &cp = plan->pairs[ip];
+                const ClassSet &bs = two ? xs : (cp.swap ? xs : ms);
+                const ClassSet &ks = two ? xs : (cp.swap ? ms : xs);
+                const auto &B = bs.dev[cp.cb], &K = ks.dev[cp.ck];
+                if (!cp.chunksD1 && cp.t64 > 0)
+                {
+                    auto ch = costChunks(cp.run64, cp.cost, 1, 8);
+                    cp.n_chunksD1 = (long long)ch.size() - 1;
+                    cp.chunksD1 = devUpload(ch, stream_);
+                }
+                QuartetArgs a{};
+                a.bra = view(B);
+                a.ket = view(K);
+                a.boys = boys_;
+                a.boys_f = boys_f_;
+                a.list = nullptr;
+                a.major_ket = 1;
+                a.major_order = cp.majors;
+                a.minor_order = bs.orders[cp.cb].d_order;
+                a.minor_begin = cp.begin64;
+                a.prefix = cp.prefix64;
+                a.n_major = cp.n_bra;
+                a.n_tasks = cp.t64;
+                a.bra_qpair = B.Q;
+                a.ket_qpair = K.Q;
+                a.q_lo = plan->thr;
+                a.q_hi = HUGE_VAL;
+                a.same_class = two && cp.cb == cp.ck;
+                a.aux_side = two ? 2 : (cp.swap ? 1 : 0);
+                a.mode = kD1GradRI;
+                a.D = D_dev;
+                a.dcoef = dcoef_dev;
+                a.nao = (int)nao_;
+                a.grad = grad_dev;
+                a.status = d_status_;
+                a.chunks = cp.chunksD1;
+                a.n_chunks = cp.n_chunksD1;
+                a.counter = plan->counters + 2 * ip;
+                cudaCheck(lookupD1(pairType(B.la, B.lb), pairType(K.la, K.lb))(a, stream_, num_sms_), "ri grad");
+            }
+        }
+        cudaCheck(cudaStreamSynchronize(stream_), "ri grad");
+        checkStatus();
+    }
+
     std::vector<int> Engine::auxShellStarts()
     {
         requireStructure();

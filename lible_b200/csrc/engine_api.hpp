@@ -169,6 +169,9 @@ namespace lible_b200
         // functions P in [P_lo, P_hi) (block ends on shell boundaries, see auxShellStarts), with the
         // Schwarz test of the RI plan; enqueued on the context stream.
         void riStore(int P_lo, int P_hi, double *T_dev, double schwarz);
+        // Gradient of the RI-J energy 1/2 gamma^T (P|Q)^{-1} gamma given d = (P|Q)^{-1} gamma (device
+        // vector): sum_P d_P sum_mn D_mn d(mn|P)/dR - 1/2 sum_PQ d_P d_Q d(P|Q)/dR, [n_atoms][3].
+        void riGradient(const double *D_dev, const double *dcoef_dev, double *grad_dev, double schwarz);
         // First auxiliary function of every auxiliary shell, ascending, followed by naux.
         std::vector<int> auxShellStarts();
         // One-electron integrals (device outputs, any may be null): overlap, kinetic energy and the
@@ -257,6 +260,7 @@ namespace lible_b200
         JKClassPair buildClassPair(const ClassSet &bs, int cb, const ClassSet &ks, int ck, bool triangle,
                                    double thr, double thr32, bool mixed);
         JKPlan &riPlan(double thr);
+        JKPlan &ri2Plan(double thr);
         QuartetArgs riArgs(const JKPlan &plan, size_t ip);
         LaunchFn riLaunchFn(const JKPlan &plan, size_t ip);
 

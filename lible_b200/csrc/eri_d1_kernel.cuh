@@ -15,7 +15,11 @@
 //             by exactly one thread, so no atomics);
 //   kD1Grad:  each block is contracted on the fly with the two-particle density of
 //             E = 1/2 Tr(DJ) - 1/4 Tr(DK),  Gamma = f (4 D_ab D_cd - D_ac D_bd - D_ad D_bc),
-//             and the per-atom sums are added to the gradient (the adjoint of the J/K build).
+//             and the per-atom sums are added to the gradient (the adjoint of the J/K build);
+//   kD1GradRI: the same for the RI-J energy E = 1/2 gamma^T (P|Q)^{-1} gamma, whose gradient is
+//             sum_P d_P sum_mn D_mn d(mn|P) - 1/2 sum_PQ d_P d_Q d(P|Q) with d = (P|Q)^{-1} gamma:
+//             Gamma = w D_mn d_P for three-centre blocks and -w/2 d_P d_Q for two-centre ones, w the
+//             multiplicity of the unique pair (2, or 1 for a shell with itself).
 #pragma once
 
 #include "device_common.cuh"
@@ -92,6 +96,42 @@ namespace lible_b200
                 outq = a.out + (size_t)task * 12 * blk;
                 for (int e = tid; e < 12 * blk; e += G)
                     outq[e] = 0.0;
+            }
+            else if (a.mode == kD1GradRI)
+            {
+                const int n = a.nao;
+                if (a.aux_side == 2)
+                {
+                    const double w = (a.same_class && ib == ik) ? 0.5 : 1.0;  // -w/2 with w = 1 or 2
+                    for (int e = tid; e < blk; e += G)
+                    {
+                        const int P = bi[0] + e / C::SCD, Q = ki[0] + e % C::SCD;
+                        gm[e] = -w * a.dcoef[P] * a.dcoef[Q];
+                    }
+                }
+                else
+                {
+                    const int32_t *mi = a.aux_side == 0 ? bi : ki;
+                    const double w = mi[4] == mi[5] ? 1.0 : 2.0;
+                    for (int e = tid; e < blk; e += G)
+                    {
+                        const int mn = e / C::SCD, kt = e % C::SCD;
+                        int mu, nu, P;
+                        if (a.aux_side == 0)
+                        {
+                            mu = bi[0] + mn / C::SB;
+                            nu = bi[1] + mn % C::SB;
+                            P = ki[0] + kt;
+                        }
+                        else
+                        {
+                            P = bi[0] + mn;
+                            mu = ki[0] + kt / C::SD;
+                            nu = ki[1] + kt % C::SD;
+                        }
+                        gm[e] = w * a.D[(size_t)mu * n + nu] * a.dcoef[P];
+                    }
+                }
             }
             else
             {

@@ -440,6 +440,14 @@ def rij(structure, D, schwarz=1e-12):
     return J, g, d
 
 
+def rij_grad(structure, D, schwarz=1e-12):
+    """Gradient [n_atoms][3] of the RI-J energy 1/2 gamma^T (P|Q)^-1 gamma, and that energy."""
+    g = np.empty((structure.n_atoms, 3))
+    e = ctypes.c_double()
+    _call(structure, "lible_gpu_rij_grad", _ptr(_f64(D)), float(schwarz), _ptr(g), ctypes.byref(e))
+    return g, e.value
+
+
 def rij_last_solve(structure):
     """How the last rij() solved the metric equations:
     {'method': 'cholesky'|'cholesky+shift'|'eigen', 'lo', 'hi', 'dropped', 'shift'}."""
