@@ -114,6 +114,16 @@ int lible_gpu_eri2_batch(lible_gpu_ctx *ctx, int aux_class_a, int aux_class_b, l
                          const unsigned *idx, double *out);
 int lible_gpu_eri2d1_batch(lible_gpu_ctx *ctx, int aux_class_a, int aux_class_b, long long n,
                            const unsigned *idx, double *out);
+/* ERI4SOCKernel / ERI3SOCKernel (twoel/eri_kernels.hpp:187-223): the three Cartesian components of the
+ * two-electron spin-orbit integrals, out[i] = [3][Sa][Sb][Sc][Sd] (resp. [3][Sa][Sb][Sc]).
+ * ERI2D2Kernel (eri_kernels.hpp:171-185): second derivatives of (P|Q), out[i] = [6][6][Sa][Sb]
+ * (A_xyz, B_xyz twice).  Pairs as for the batches above. */
+int lible_gpu_eri4soc_batch(lible_gpu_ctx *ctx, int use_symm, int class_ab, int class_cd, long long n,
+                            const unsigned *pairs, double *out);
+int lible_gpu_eri3soc_batch(lible_gpu_ctx *ctx, int use_symm, int class_ab, int aux_class, long long n,
+                            const unsigned *pairs, double *out);
+int lible_gpu_eri2d2_batch(lible_gpu_ctx *ctx, int aux_class_a, int aux_class_b, long long n, const unsigned *pairs,
+                           double *out);
 
 /* ---- direct Coulomb / exchange (no reference counterpart; built on the eri4 kernels) ----------
  * J_mn = sum_ls (mn|ls) D_ls,  K_mn = sum_ls (ml|ns) D_ls over Schwarz-surviving unique quartets

@@ -63,6 +63,9 @@ SIGNATURES = {
     "lible_gpu_eri3d1_batch": [P, I, I, I, LL, P, P],
     "lible_gpu_eri2_batch": [P, I, I, LL, P, P],
     "lible_gpu_eri2d1_batch": [P, I, I, LL, P, P],
+    "lible_gpu_eri4soc_batch": [P, I, I, I, LL, P, P],
+    "lible_gpu_eri3soc_batch": [P, I, I, I, LL, P, P],
+    "lible_gpu_eri2d2_batch": [P, I, I, LL, P, P],
     "lible_gpu_jk": [P, P, P, P, ctypes.POINTER(JKOpts), ctypes.POINTER(JKStats)],
     "lible_gpu_jk_energy_forward": [P, P, ctypes.POINTER(JKOpts), P, P, P],
     "lible_gpu_jk_energy_backward": [P, P, ctypes.POINTER(JKOpts), P],

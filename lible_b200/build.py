@@ -34,7 +34,7 @@ def sources():
     import gen_instances  # noqa: E402
     gen_instances.main()
     srcs = [os.path.join(CSRC, f) for f in ("host_math.cpp", "host_basis.cpp", "engine.cu", "peak.cu", "noalloc.cu",
-                                            "ri_k.cu", "oneel.cu", "capi.cpp")]
+                                            "ri_k.cu", "oneel.cu", "eri_special.cu", "capi.cpp")]
     srcs += sorted(glob.glob(os.path.join(CSRC, "gen", "*.cu")))
     return srcs
 

@@ -573,6 +573,46 @@ int lible_gpu_eri2d1_batch(lible_gpu_ctx *ctx, int a, int b, long long n, const 
     return batch2(ctx, a, b, n, idx, out, true);
 }
 
+static int specialBatch(lible_gpu_ctx *ctx, int kind, int use_symm, int a, int b, long long n, const unsigned *pairs,
+                        double *out)
+{
+    return guard(ctx, [&](Engine &e) {
+        if (n < 0 || (n > 0 && (!pairs || !out)))
+            throw EngineError(kStatusInvalid, "bad batch arguments");
+        if (kind != 0 && !e.hasAux())
+            throw EngineError(kStatusNoAux, "RI approximation is not enabled");
+        const auto main = e.pairClasses(use_symm != 0);
+        const auto aux = kind == 0 ? std::vector<Engine::ClassInfo>{} : e.auxClasses();
+        const auto &ca = kind == 2 ? aux : main;
+        const auto &cb = kind == 0 ? main : aux;
+        if (a < 0 || a >= (int)ca.size() || b < 0 || b >= (int)cb.size())
+            throw EngineError(kStatusInvalid, "class index out of range");
+        const size_t blk = (size_t)(2 * ca[a].la + 1) * (2 * ca[a].lb + 1) * (2 * cb[b].la + 1) * (2 * cb[b].lb + 1) *
+                           (kind == 2 ? 36 : 3);
+        DevArray o(out, (size_t)n * blk, false, e.stream());
+        e.specialBatch(kind, use_symm != 0, a, b, n, pairs, o.ptr);
+        o.copyOut();
+    });
+}
+
+int lible_gpu_eri4soc_batch(lible_gpu_ctx *ctx, int use_symm, int class_ab, int class_cd, long long n,
+                            const unsigned *pairs, double *out)
+{
+    return specialBatch(ctx, 0, use_symm, class_ab, class_cd, n, pairs, out);
+}
+
+int lible_gpu_eri3soc_batch(lible_gpu_ctx *ctx, int use_symm, int class_ab, int aux_class, long long n,
+                            const unsigned *pairs, double *out)
+{
+    return specialBatch(ctx, 1, use_symm, class_ab, aux_class, n, pairs, out);
+}
+
+int lible_gpu_eri2d2_batch(lible_gpu_ctx *ctx, int aux_class_a, int aux_class_b, long long n, const unsigned *pairs,
+                           double *out)
+{
+    return specialBatch(ctx, 2, 0, aux_class_a, aux_class_b, n, pairs, out);
+}
+
 static JKOptions toOpts(const lible_gpu_jk_opts *o)
 {
     JKOptions j;

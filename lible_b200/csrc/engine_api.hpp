@@ -115,6 +115,10 @@ namespace lible_b200
                        bool d1);
         void eri3Batch(bool use_symm, int cab, int cx, long long n, const uint32_t *idx_host, double *out_dev, bool d1);
         void eri2Batch(int ca, int cb, long long n, const uint32_t *idx_host, double *out_dev, bool d1);
+        // ERI4SOCKernel (kind 0, main x main), ERI3SOCKernel (1, main x aux), ERI2D2Kernel (2, aux x
+        // aux) batches: out [n][3][block] (SOC) or [n][6][6][Sa][Sb] (D2), device memory.
+        void specialBatch(int kind, bool use_symm, int c_ab, int c_cd, long long n, const uint32_t *pairs_host,
+                          double *out_dev);
         // eri4Batch without any device allocation: the pair list is staged in `scratch` (device
         // memory the caller owns, room for 2 * max_pairs indices); `out_dev` must be device memory.
         // The class set must already exist on the device (built by an earlier pairClasses call).

@@ -241,6 +241,8 @@ namespace lible_b200
         struct OnePairArgs
         {
             int op;                  // OneOp (store mode)
+            int swap;                // store mode: the class is stored with a and b exchanged; write the
+                                     // caller's orientation (blocks transposed, d/dA and d/dB exchanged)
             long long n_tasks;
             const uint32_t *list;    // pair index of each task (store mode), null = every pair
             int n_pairs, nao;
@@ -588,6 +590,7 @@ namespace lible_b200
                 for (int o = lane; o < nblk * S::SA * S::SB; o += 32)
                 {
                     const int d = o / (S::SA * S::SB), m = (o / S::SB) % S::SA, nn = o % S::SB;
+                    const int dst = a.swap ? ((nblk == 6 ? (d + 3) % 6 : d) * S::SA * S::SB + nn * S::SA + m) : o;
                     double sum = 0.0;
                     for (int ta = a.sph_ofs_a0; ta < a.sph_ofs_a1; ta++)
                     {
@@ -598,7 +601,7 @@ namespace lible_b200
                             if (a.sph_rc[2 * tb] == nn)
                                 sum += a.sph_val[ta] * a.sph_val[tb] * blk[d * S::NC + ca * S::NCB + a.sph_rc[2 * tb + 1]];
                     }
-                    out[o] = nA[m] * nB[nn] * sum;
+                    out[dst] = nA[m] * nB[nn] * sum;
                 }
             }
         }
@@ -736,6 +739,7 @@ namespace lible_b200
         upload(dq, q, stream_);
         OnePairArgs a{};
         a.op = op;
+        a.swap = cs.swapped[cls] ? 1 : 0;
         a.n_tasks = n_tasks;
         a.list = dl.p;
         a.n_pairs = (int)pc.n_pairs;

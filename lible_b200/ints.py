@@ -305,6 +305,27 @@ class ERI2D1Kernel(ERI2Kernel):
     _fn, _nblk = "lible_gpu_eri2d1_batch", 6
 
 
+class ERI2D2Kernel(ERI2Kernel):
+    """lible::ints::ERI2D2Kernel (eri_kernels.hpp:171-185): 6 x 6 blocks [A, B] x [x, y, z]."""
+    _fn, _nblk = "lible_gpu_eri2d2_batch", 36
+
+    def batch(self, idx):
+        return super().batch(idx).reshape(-1, 6, 6, *self._dims())
+
+    def __call__(self, i, j, *_):
+        return self.batch([[i, j]])[0]
+
+
+class ERI4SOCKernel(ERI4Kernel):
+    """lible::ints::ERI4SOCKernel (eri_kernels.hpp:187-203): the three spin-orbit components."""
+    _fn, _nblk = "lible_gpu_eri4soc_batch", 3
+
+
+class ERI3SOCKernel(ERI3Kernel):
+    """lible::ints::ERI3SOCKernel (eri_kernels.hpp:205-221)."""
+    _fn, _nblk = "lible_gpu_eri3soc_batch", 3
+
+
 class Batch:
     """A batch of molecules whose J/K are built together (no reference counterpart).
 

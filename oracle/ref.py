@@ -50,6 +50,10 @@ def lib():
         L.ref_rij_gamma.argtypes = [P, P, P]
         L.ref_rij_j.argtypes = [P, P, P]
         L.ref_one_electron.argtypes = [P, ctypes.c_int, P, ctypes.c_int, P]
+        L.ref_eri4soc_class.argtypes = [P, ctypes.c_int, ctypes.c_int, ctypes.c_int, P]
+        L.ref_eri3soc_class.argtypes = [P, ctypes.c_int, ctypes.c_int, ctypes.c_int, P]
+        L.ref_eri2d2_class.argtypes = [P, ctypes.c_int, ctypes.c_int, P]
+        L.ref_one_electron_class.argtypes = [P, ctypes.c_int, ctypes.c_int, ctypes.c_int, P, ctypes.c_int, P]
         _lib = L
     return _lib
 
@@ -119,6 +123,34 @@ class RefStructure:
         q = np.ascontiguousarray(charges if charges is not None else np.zeros((0, 4)), dtype=np.float64)
         self._chk(lib().ref_one_electron(self.h, which, _p(q), len(q), _p(out)))
         return out
+
+    def eri4soc_class(self, use_symm, iab, icd):
+        cls = self.pair_classes(use_symm)
+        (la, lb, na, _), (lc, ld, nc, _) = cls[iab], cls[icd]
+        out = np.empty((na, nc, 3, 2 * la + 1, 2 * lb + 1, 2 * lc + 1, 2 * ld + 1))
+        self._chk(lib().ref_eri4soc_class(self.h, int(use_symm), iab, icd, _p(out)))
+        return out
+
+    def eri3soc_class(self, use_symm, iab, ic):
+        (la, lb, na, _), (lc, nc) = self.pair_classes(use_symm)[iab], self.aux_classes()[ic]
+        out = np.empty((na, nc, 3, 2 * la + 1, 2 * lb + 1, 2 * lc + 1))
+        self._chk(lib().ref_eri3soc_class(self.h, int(use_symm), iab, ic, _p(out)))
+        return out
+
+    def eri2d2_class(self, ia, ib):
+        acls = self.aux_classes()
+        (la, na), (lb, nb) = acls[ia], acls[ib]
+        out = np.empty((na, nb, 6, 6, 2 * la + 1, 2 * lb + 1))
+        self._chk(lib().ref_eri2d2_class(self.h, ia, ib, _p(out)))
+        return out
+
+    def one_electron_class(self, use_symm, iab, op, charges=None):
+        la, lb, na, _ = self.pair_classes(use_symm)[iab]
+        nb = 6 if op >= 3 else 1
+        out = np.empty((na, nb, 2 * la + 1, 2 * lb + 1))
+        q = np.ascontiguousarray(charges if charges is not None else np.zeros((0, 4)), dtype=np.float64)
+        self._chk(lib().ref_one_electron_class(self.h, int(use_symm), iab, op, _p(q), len(q), _p(out)))
+        return out if nb > 1 else out[:, 0]
 
     def eri2_diagonal(self):
         out = np.empty(self.naux)

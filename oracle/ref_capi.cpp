@@ -231,6 +231,113 @@ int ref_eri2(void *h, double *out)
     });
 }
 
+// All ERI4SOCKernel / ERI3SOCKernel batches of one class pair, [n_ab][n_cd][3][block]
+// (src/lible/ints/twoel/eri_kernels.hpp:187-223).
+int ref_eri4soc_class(void *h, int use_symm, int iab, int icd, double *out)
+{
+    return guarded([&]
+    {
+        auto sp = lints::shellPairData(use_symm != 0, *static_cast<RefStructure *>(h)->s);
+        const auto &ab = sp.at(iab);
+        const auto &cd = sp.at(icd);
+        lints::ERI4SOCKernel k(ab, cd);
+        size_t blk = lints::numSphericals(ab.la_) * lints::numSphericals(ab.lb_) *
+                     lints::numSphericals(cd.la_) * lints::numSphericals(cd.lb_);
+#pragma omp parallel for schedule(dynamic)
+        for (size_t i = 0; i < ab.n_pairs_; i++)
+            for (size_t j = 0; j < cd.n_pairs_; j++)
+            {
+                auto b = k(i, j, ab, cd);
+                for (int x = 0; x < 3; x++)
+                    std::memcpy(out + ((i * cd.n_pairs_ + j) * 3 + x) * blk, b[x].memptr(), blk * sizeof(double));
+            }
+    });
+}
+
+int ref_eri3soc_class(void *h, int use_symm, int iab, int ic, double *out)
+{
+    return guarded([&]
+    {
+        auto &S = *static_cast<RefStructure *>(h)->s;
+        auto sp = lints::shellPairData(use_symm != 0, S);
+        auto sh = lints::shellDataAux(S);
+        const auto &ab = sp.at(iab);
+        const auto &c = sh.at(ic);
+        lints::ERI3SOCKernel k(ab, c);
+        size_t blk = lints::numSphericals(ab.la_) * lints::numSphericals(ab.lb_) * lints::numSphericals(c.l_);
+#pragma omp parallel for schedule(dynamic)
+        for (size_t i = 0; i < ab.n_pairs_; i++)
+            for (size_t j = 0; j < c.n_shells_; j++)
+            {
+                auto b = k(i, j, ab, c);
+                for (int x = 0; x < 3; x++)
+                    std::memcpy(out + ((i * c.n_shells_ + j) * 3 + x) * blk, b[x].memptr(), blk * sizeof(double));
+            }
+    });
+}
+
+// All ERI2D2Kernel batches of one auxiliary class pair, [n_a][n_b][6][6][Sa Sb]
+// (eri_kernels.hpp:171-185).
+int ref_eri2d2_class(void *h, int ia, int ib, double *out)
+{
+    return guarded([&]
+    {
+        auto sh = lints::shellDataAux(*static_cast<RefStructure *>(h)->s);
+        const auto &a = sh.at(ia);
+        const auto &b = sh.at(ib);
+        lints::ERI2D2Kernel k(a, b);
+        size_t blk = lints::numSphericals(a.l_) * lints::numSphericals(b.l_);
+#pragma omp parallel for schedule(dynamic)
+        for (size_t i = 0; i < a.n_shells_; i++)
+            for (size_t j = 0; j < b.n_shells_; j++)
+            {
+                auto r = k(i, j, a, b);
+                for (int x = 0; x < 6; x++)
+                    for (int y = 0; y < 6; y++)
+                        std::memcpy(out + (((i * b.n_shells_ + j) * 6 + x) * 6 + y) * blk, r[x][y].memptr(),
+                                    blk * sizeof(double));
+            }
+    });
+}
+
+// The reference's per-pair one-electron kernels for every pair of one class, [n_pairs][blocks][Sa Sb]:
+// op 0 overlapKernel, 1 kineticEnergyKernel, 2 externalChargesKernel, 3 overlapD1Kernel,
+// 4 kineticEnergyD1Kernel, 5 externalChargesD1Kernel (oneelints.cpp:57-789).
+int ref_one_electron_class(void *h, int use_symm, int iab, int op, const double *charges, int n_charges, double *out)
+{
+    return guarded([&]
+    {
+        auto sp = lints::shellPairData(use_symm != 0, *static_cast<RefStructure *>(h)->s);
+        const auto &ab = sp.at(iab);
+        std::vector<std::array<double, 4>> q(n_charges);
+        for (int i = 0; i < n_charges; i++)
+            q[i] = {charges[4 * i], charges[4 * i + 1], charges[4 * i + 2], charges[4 * i + 3]};
+        const int lab = ab.la_ + ab.lb_;
+        lints::BoysGrid grid(op == 5 ? lab + 1 : lab);
+        size_t blk = lints::numSphericals(ab.la_) * lints::numSphericals(ab.lb_);
+        const int nb = op >= 3 ? 6 : 1;
+        for (size_t i = 0; i < ab.n_pairs_; i++)
+        {
+            double *o = out + i * nb * blk;
+            if (op < 3)
+            {
+                lible::vec2d v = op == 0 ? lints::overlapKernel(i, ab)
+                                 : op == 1 ? lints::kineticEnergyKernel(i, ab)
+                                           : lints::externalChargesKernel(i, q, grid, ab);
+                std::memcpy(o, v.memptr(), blk * sizeof(double));
+            }
+            else
+            {
+                std::array<lible::vec2d, 6> v = op == 3 ? lints::overlapD1Kernel(i, ab)
+                                                : op == 4 ? lints::kineticEnergyD1Kernel(i, ab)
+                                                          : lints::externalChargesD1Kernel(i, q, grid, ab);
+                for (int d = 0; d < 6; d++)
+                    std::memcpy(o + d * blk, v[d].memptr(), blk * sizeof(double));
+            }
+        }
+    });
+}
+
 // One-electron integrals of the reference (src/lible/ints/oneelints.cpp): 0 overlap, 1 kinetic
 // energy, 2 nuclear attraction, 3 external point charges (charges [n][4] x, y, z (bohr), q).
 int ref_one_electron(void *h, int which, const double *charges, int n_charges, double *out)

@@ -321,3 +321,37 @@ def test_rij_gradient_vs_finite_differences():
     # the Schwarz-screened gradient stays within the screening error
     gs, _ = L.rij_grad(s, D, schwarz=1e-12)
     assert np.abs(gs - g).max() <= 1e-8
+
+
+def test_soc_and_eri2d2_kernels_vs_reference():
+    """ERI4SOCKernel, ERI3SOCKernel and ERI2D2Kernel batches of every class pair (shellPairData
+    without symmetry, so classes with la < lb are included) element-wise against the reference's
+    own kernels, and the reference's golden sums (test/tests_ints.cpp:1055-1150)."""
+    s = L.Structure("def2-svp", [8, 8, 8], O3_ANG, "def2-universal-jkfit")
+    r = R.RefStructure("def2-svp", [8, 8, 8], O3_ANG, aux="def2-universal-jkfit", units="angstrom")
+    sp = L.shellPairData(False, s)
+    aux = L.shellDataAux(s)
+    parts4, parts3, parts2 = [], [], []
+    for i, a in enumerate(sp):
+        for j, c in enumerate(sp):
+            idx = [(p, q) for p in range(a.n_pairs_) for q in range(c.n_pairs_)]
+            got = L.ERI4SOCKernel(a, c).batch(idx)
+            want = r.eri4soc_class(False, i, j).reshape(got.shape)
+            assert np.abs(got - want).max() <= 1e-12, (i, j)
+            parts4.append(got.ravel())
+        for j, x in enumerate(aux):
+            idx = [(p, q) for p in range(a.n_pairs_) for q in range(x.n_shells_)]
+            got = L.ERI3SOCKernel(a, x).batch(idx)
+            want = r.eri3soc_class(False, i, j).reshape(got.shape)
+            assert np.abs(got - want).max() <= 1e-12, (i, j)
+            parts3.append(got.ravel())
+    for i, x in enumerate(aux):
+        for j, y in enumerate(aux):
+            idx = [(p, q) for p in range(x.n_shells_) for q in range(y.n_shells_)]
+            got = L.ERI2D2Kernel(x, y).batch(idx)
+            want = r.eri2d2_class(i, j).reshape(got.shape)
+            assert np.abs(got - want).max() <= 1e-11 * max(1.0, np.abs(want).max()), (i, j)
+            parts2.append(got.ravel())
+    assert golden(seqsum(np.concatenate(parts4)), 12940.953099658431)
+    assert golden(seqsum(np.concatenate(parts3)), 18124.713152990007)
+    assert golden(seqsum(np.concatenate(parts2)), 175567.635699242965)

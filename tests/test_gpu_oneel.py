@@ -121,3 +121,21 @@ def test_one_electron_gradient_vs_finite_differences():
             assert abs(fd - g[atom, x]) <= 1e-6 * max(1.0, abs(fd)), (basis, atom, x, fd, g[atom, x])
         # the D and W terms separately add up to the whole
         assert np.abs(L.one_electron_grad(s, D, None) + L.one_electron_grad(s, None, W) - g).max() <= 1e-10
+
+
+def test_per_pair_kernels_vs_reference_elementwise():
+    # every class of shellPairData with and without symmetry (la < lb classes included), all six
+    # operators, against the reference's own per-pair kernels
+    s = L.Structure("cc-pvdz", C2H4_Z, C2H4_ANG)
+    r = R.RefStructure("cc-pvdz", C2H4_Z, C2H4_ANG, units="angstrom")
+    q = np.array([[1.0, -2.0, 0.5, 0.7], [-3.0, 1.0, -16.0, -1.2], [6.0, 2.0, -17.0, 2.0]])
+    fns = [L.overlapKernel, L.kineticEnergyKernel, L.externalChargesKernel, L.overlapD1Kernel,
+           L.kineticEnergyD1Kernel, L.externalChargesD1Kernel]
+    for use_symm in (True, False):
+        for i, sp in enumerate(L.shellPairData(use_symm, s)):
+            idx = list(range(sp.n_pairs_))
+            for op, fn in enumerate(fns):
+                got = fn(idx, q, sp) if op in (2, 5) else fn(idx, sp)
+                want = r.one_electron_class(use_symm, i, op, q if op in (2, 5) else None)
+                assert np.abs(got - want.reshape(got.shape)).max() <= 1e-12 * max(1.0, np.abs(want).max()), \
+                    (use_symm, i, op)

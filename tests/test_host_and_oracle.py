@@ -164,3 +164,22 @@ def test_reference_one_electron_golden():
     assert abs(seqsum(V) - 2141.927982294058) <= 1e-13 * 2141.9
     q = np.array([[x / 0.5291772083 for x in c] + [z] for c, z in zip(co2, [6, 8, 8])])
     assert np.abs(r2.one_electron(3, q) - V).max() <= 1e-13
+
+
+@needs_ref
+def test_reference_soc_and_d2_golden():
+    # the compiled reference reproduces its ERI4SOC / ERI3SOC / ERI2D2 kernel golden sums
+    # (test/tests_ints.cpp:1055-1150) through the oracle's per-class wrappers
+    o3 = [[0, 0, 0], [0, 1, 1], [0, 0, 2]]
+    r = ref.RefStructure("def2-svp", [8, 8, 8], o3, aux="def2-universal-jkfit", units="angstrom")
+    nc, na = len(r.pair_classes(False)), len(r.aux_classes())
+
+    def total(blocks):
+        return seqsum(np.concatenate([np.ravel(b) for b in blocks]))
+
+    assert abs(total(r.eri4soc_class(False, i, j) for i in range(nc) for j in range(nc)) -
+               12940.953099658431) <= 1e-13 * 12940.95
+    assert abs(total(r.eri3soc_class(False, i, j) for i in range(nc) for j in range(na)) -
+               18124.713152990007) <= 1e-13 * 18124.71
+    assert abs(total(r.eri2d2_class(i, j) for i in range(na) for j in range(na)) -
+               175567.635699242965) <= 1e-13 * 175567.6
