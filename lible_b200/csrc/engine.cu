@@ -813,6 +813,7 @@ namespace lible_b200
         QuartetArgs a{};
         a.bra = view(swap ? ket : bra);
         a.ket = view(swap ? bra : ket);
+        a.ket_EtP = (swap ? bra : ket).EtP;
         a.boys = boys_;
         a.boys_f = boys_f_;
         a.n_tasks = n;

@@ -972,10 +972,26 @@ namespace lible_b200
         __syncthreads();
     }
 
-    // Forward kernel: every mode except the derivative ones.
+    // Resident blocks per SM the compiler must allow for (register cap 65536 / (block * n)).  Three
+    // instead of the default two for the register-path classes where the higher occupancy outweighs
+    // the few spills it costs, as measured on the (H2O)_32 cc-pVDZ J/K build: (dp|ps), (ds|ps),
+    // (dp|ss) in FP64 and (dp|ps), (ds|pp) in FP32; every other class loses more to spills.
     template <int LA, int LB, int LC, int LD, typename T>
-    __global__ void __launch_bounds__(Shape<LA, LB, LC, LD, T>::block)
-    eriKernel(QuartetArgs a)
+    constexpr int minBlocksPerSM()
+    {
+        if (Shape<LA, LB, LC, LD, T>::W != 0)
+            return 1;
+        constexpr bool d = sizeof(T) == 8;
+        constexpr bool dp_ps = LA == 2 && LB == 1 && LC == 1 && LD == 0;
+        constexpr bool ds_ps = LA == 2 && LB == 0 && LC == 1 && LD == 0;
+        constexpr bool dp_ss = LA == 2 && LB == 1 && LC == 0 && LD == 0;
+        constexpr bool ds_pp = LA == 2 && LB == 0 && LC == 1 && LD == 1;
+        return (dp_ps || (d && (ds_ps || dp_ss)) || (!d && ds_pp)) ? 3 : 1;
+    }
+
+    // Forward kernel body: every mode except the derivative ones.
+    template <int LA, int LB, int LC, int LD, typename T>
+    __device__ __forceinline__ void eriKernelBody(const QuartetArgs &a)
     {
         using C = Cls<LA, LB, LC, LD>;
         using S = Shape<LA, LB, LC, LD, T>;
@@ -1288,5 +1304,26 @@ namespace lible_b200
                     processRange(chunk * CHB, (chunk + 1) * CHB < a.n_tasks ? (chunk + 1) * CHB : a.n_tasks);
             }
         }
+    }
+
+    // The class kernels: the default register bound, or (minBlocksPerSM == 3) one that lets three
+    // blocks reside per SM.  Only the selected one is instantiated per class (eriKernelFor).
+    template <int LA, int LB, int LC, int LD, typename T>
+    __global__ void __launch_bounds__(Shape<LA, LB, LC, LD, T>::block) eriKernel(QuartetArgs a)
+    {
+        eriKernelBody<LA, LB, LC, LD, T>(a);
+    }
+    template <int LA, int LB, int LC, int LD, typename T>
+    __global__ void __launch_bounds__(Shape<LA, LB, LC, LD, T>::block, 3) eriKernelOcc3(QuartetArgs a)
+    {
+        eriKernelBody<LA, LB, LC, LD, T>(a);
+    }
+    template <int LA, int LB, int LC, int LD, typename T>
+    constexpr auto eriKernelFor()
+    {
+        if constexpr (minBlocksPerSM<LA, LB, LC, LD, T>() == 3)
+            return &eriKernelOcc3<LA, LB, LC, LD, T>;
+        else
+            return &eriKernel<LA, LB, LC, LD, T>;
     }
 }

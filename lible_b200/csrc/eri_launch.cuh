@@ -36,7 +36,7 @@ namespace lible_b200
         using S = Shape<LA, LB, LC, LD, T>;
         if (a.n_tasks <= 0)
             return cudaSuccess;
-        auto kern = eriKernel<LA, LB, LC, LD, T>;
+        auto kern = eriKernelFor<LA, LB, LC, LD, T>();
         long long grid;
         if (a.chunks)
         {
