@@ -30,11 +30,11 @@ SCHWARZ, FP32_THR = 1e-12, 1e-4
 # DRAM bytes (read + write) per launch of the dominant class kernels at this workload, from one ncu
 # capture each (dram__bytes_read.sum + dram__bytes_write.sum); the working set stays in L2
 DOMINANT_TRAFFIC = {(1, 0, 0, 0): 33.66e6, (2, 1, 1, 0): 24.16e6}
-# classes compiled with the three-blocks-per-SM register bound (eriKernelOcc3, minBlocksPerSM in
+# classes compiled with a raised occupancy bound (eriKernelOcc, minBlocksPerSM in
 # lible_b200/csrc/eri_kernel.cuh): (class, fp32) -> kernel name
-OCC3_KERNELS = {((2, 1, 1, 0), False): "eriKernelOcc3", ((2, 0, 1, 0), False): "eriKernelOcc3",
-                ((2, 1, 0, 0), False): "eriKernelOcc3", ((2, 1, 1, 0), True): "eriKernelOcc3",
-                ((2, 0, 1, 1), True): "eriKernelOcc3"}
+OCC_KERNELS = {(c, f): "eriKernelOcc" for c, f in [((2, 1, 1, 0), False), ((2, 0, 1, 0), False), ((2, 1, 0, 0), False),
+                                                  ((1, 0, 0, 0), False), ((2, 1, 1, 0), True), ((2, 0, 1, 1), True),
+                                                  ((1, 1, 1, 0), True), ((1, 0, 1, 0), True), ((2, 0, 0, 0), True)]}
 WORKLOAD = {"workload": "direct J+K build, (H2O)_32 water cluster, cc-pVDZ", "n_waters": N_WATERS, "nao": 768,
             "seed": SEED, "occupied": OCC, "schwarz": SCHWARZ, "fp32_threshold": FP32_THR,
             "geometry": "5.7 bohr cubic lattice, random rotations, +-0.6 bohr jitter",
@@ -495,7 +495,7 @@ def main():
         "roofline": {"bound": "tensor", "achieved": dom_tflops, "peak": fp64_peak, "unit": "TFLOP/s",
                      "frac": dom_tflops / fp64_peak if fp64_peak else None,
                      "traffic": DOMINANT_TRAFFIC.get(dom_key[0]),
-                     "kernel": "%s<%d,%d,%d,%d,%s>" % ((OCC3_KERNELS.get((dom_key[0], dom_key[1]), "eriKernel"),) +
+                     "kernel": "%s<%d,%d,%d,%d,%s>" % ((OCC_KERNELS.get((dom_key[0], dom_key[1]), "eriKernel"),) +
                                                       dom_key[0] + ("float" if dom_key[1] else "double",)),
                      "kernel_ms": dom_ms, "kernel_quartets": dom["tasks"],
                      "scope": "dominant class kernel of the FP64 build: algorithmic FLOPs per launch / CUDA-event "

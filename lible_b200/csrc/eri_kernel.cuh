@@ -972,21 +972,20 @@ namespace lible_b200
         __syncthreads();
     }
 
-    // Resident blocks per SM the compiler must allow for (register cap 65536 / (block * n)).  Three
-    // instead of the default two for the register-path classes where the higher occupancy outweighs
-    // the few spills it costs, as measured on the (H2O)_32 cc-pVDZ J/K build: (dp|ps), (ds|ps),
-    // (dp|ss) in FP64 and (dp|ps), (ds|pp) in FP32; every other class loses more to spills.
+    // Resident blocks per SM the compiler must allow for (register cap 65536 / (block * n)), for the
+    // register-path classes where a higher occupancy measured faster on the (H2O)_32 cc-pVDZ J/K build
+    // than the default bound (which lets the compiler use more registers): FP64 (dp|ps), (ds|ps),
+    // (dp|ss) at 3 blocks and (ps|ss) at 6; FP32 (dp|ps), (ds|pp) at 3, (pp|ps) at 4, (ps|ps) at 6,
+    // (ds|ss) at 8.  1 = the default bound.
     template <int LA, int LB, int LC, int LD, typename T>
     constexpr int minBlocksPerSM()
     {
         if (Shape<LA, LB, LC, LD, T>::W != 0)
             return 1;
-        constexpr bool d = sizeof(T) == 8;
-        constexpr bool dp_ps = LA == 2 && LB == 1 && LC == 1 && LD == 0;
-        constexpr bool ds_ps = LA == 2 && LB == 0 && LC == 1 && LD == 0;
-        constexpr bool dp_ss = LA == 2 && LB == 1 && LC == 0 && LD == 0;
-        constexpr bool ds_pp = LA == 2 && LB == 0 && LC == 1 && LD == 1;
-        return (dp_ps || (d && (ds_ps || dp_ss)) || (!d && ds_pp)) ? 3 : 1;
+        constexpr int c = LA * 1000 + LB * 100 + LC * 10 + LD;
+        if (sizeof(T) == 8)
+            return (c == 2110 || c == 2010 || c == 2100) ? 3 : c == 1000 ? 6 : 1;
+        return (c == 2110 || c == 2011) ? 3 : c == 1110 ? 4 : c == 1010 ? 6 : c == 2000 ? 8 : 1;
     }
 
     // Forward kernel body: every mode except the derivative ones.
@@ -1314,15 +1313,16 @@ namespace lible_b200
         eriKernelBody<LA, LB, LC, LD, T>(a);
     }
     template <int LA, int LB, int LC, int LD, typename T>
-    __global__ void __launch_bounds__(Shape<LA, LB, LC, LD, T>::block, 3) eriKernelOcc3(QuartetArgs a)
+    __global__ void __launch_bounds__(Shape<LA, LB, LC, LD, T>::block, minBlocksPerSM<LA, LB, LC, LD, T>())
+    eriKernelOcc(QuartetArgs a)
     {
         eriKernelBody<LA, LB, LC, LD, T>(a);
     }
     template <int LA, int LB, int LC, int LD, typename T>
     constexpr auto eriKernelFor()
     {
-        if constexpr (minBlocksPerSM<LA, LB, LC, LD, T>() == 3)
-            return &eriKernelOcc3<LA, LB, LC, LD, T>;
+        if constexpr (minBlocksPerSM<LA, LB, LC, LD, T>() > 1)
+            return &eriKernelOcc<LA, LB, LC, LD, T>;
         else
             return &eriKernel<LA, LB, LC, LD, T>;
     }
