@@ -107,6 +107,7 @@ namespace lible_b200
         double *gamma;
         const double *dcoef;
         double *grad;                     // [n_atoms][3]
+        int n_atoms;                      // gradient launches: rows of grad
         int *status;                      // error word (non-zero = failure)
     };
 

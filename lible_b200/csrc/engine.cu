@@ -2007,8 +2007,10 @@ namespace lible_b200
             const auto &B = cs.dev[cp.cb], &K = cs.dev[cp.ck];
             if (!cp.chunksD1 && cp.t64 > 0)
             {
-                // one quartet per block at a time: chunks of the heaviest quartet up to 8 tasks
-                auto ch = costChunks(cp.run64, cp.cost, 1, 8);
+                // one quartet per block at a time: chunks of the heaviest quartet up to 8 tasks; the
+                // register classes take 32 quartets per warp step
+                const int unit = d1RegisterClass(B.la, B.lb, K.la, K.lb) ? 32 : 1;
+                auto ch = costChunks(cp.run64, cp.cost, unit, 8 * unit);
                 cp.n_chunksD1 = (long long)ch.size() - 1;
                 cp.chunksD1 = devUpload(ch, stream_);
             }
@@ -2034,6 +2036,7 @@ namespace lible_b200
             a.D = D_dev;
             a.nao = (int)n;
             a.grad = grad_dev;
+            a.n_atoms = n_atoms_;
             a.chunks = cp.chunksD1;
             a.n_chunks = cp.n_chunksD1;
             a.counter = plan.counters + 2 * ip;

@@ -444,4 +444,238 @@ namespace lible_b200
             for (long long task = blockIdx.x; task < a.n_tasks; task += gridDim.x)
                 runTask(task);
     }
+
+    // ---------------------------------------------------------------------------------------
+    // Register form of the J/K-gradient contraction for the smallest classes (d1RegisterClass): one
+    // thread per quartet.  With Gamma the two-particle density block of the quartet (as in kD1Grad)
+    // and, per bra primitive, GE = Gamma^T E_ab and GE1_x = Gamma^T E1_ab,x (H_ab x S_cd each), the
+    // gradient terms of the formulas above become per primitive quartet
+    //   t1_x  = sum GE  . (dR/dP_x E_cd^T),   t13_x = sum GE1_x . (R E_cd^T),
+    //   tc_x  = sum GE  . (-(c/q) dR/dP_x E_cd^T + R E1_cd,x^T),
+    // and A_x += (a/p) t1_x + t13_x, B_x += (b/p) t1_x - t13_x, C_x += tc_x (D by invariance).
+    template <int LA, int LB, int LC, int LD>
+    __device__ __forceinline__ void quartetD1Reg(const QuartetArgs &a, uint32_t ib, uint32_t ik, double *g)
+    {
+        using C = Cls<LA, LB, LC, LD>;
+        constexpr int L1 = C::L + 1;
+        const int32_t *bi = a.bra.info + 8 * ib;
+        const int32_t *ki = a.ket.info + 8 * ik;
+        const double f = quartetWeight(a, ib, ik);
+        const size_t n = (size_t)a.nao;
+        const double *D = a.D;
+        double gam[C::SAB * C::SCD];
+#pragma unroll
+        for (int m = 0; m < C::SAB; m++)
+#pragma unroll
+            for (int c = 0; c < C::SCD; c++)
+            {
+                const size_t mu = bi[0] + m / C::SB, nu = bi[1] + m % C::SB;
+                const size_t ka = ki[0] + c / C::SD, ta = ki[1] + c % C::SD;
+                gam[m * C::SCD + c] = f * (4.0 * __ldg(D + mu * n + nu) * __ldg(D + ka * n + ta) -
+                                           __ldg(D + mu * n + ka) * __ldg(D + nu * n + ta) -
+                                           __ldg(D + mu * n + ta) * __ldg(D + nu * n + ka));
+            }
+#pragma unroll
+        for (int x = 0; x < 9; x++)
+            g[x] = 0.0;
+        const uint32_t p0 = a.bra.pofs[ib], p1 = a.bra.pofs[ib + 1];
+        const uint32_t q0 = a.ket.pofs[ik], q1 = a.ket.pofs[ik + 1];
+        for (uint32_t p = p0; p < p1; p++)
+        {
+            const PQ4 P = loadPQ(a.bra.pP, p);
+            const double2 AB = __ldg(reinterpret_cast<const double2 *>(a.bra.ab) + p);
+            const double *eab = a.bra.E + (size_t)p * C::SAB * C::HAB;
+            const double *e1ab = a.bra.E1 + (size_t)p * 3 * C::SAB * C::HAB;
+            double ge[C::HAB * C::SCD], ge1[3 * C::HAB * C::SCD];
+#pragma unroll
+            for (int h = 0; h < C::HAB; h++)
+#pragma unroll
+                for (int c = 0; c < C::SCD; c++)
+                {
+                    double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+#pragma unroll
+                    for (int m = 0; m < C::SAB; m++)
+                    {
+                        const double gm = gam[m * C::SCD + c];
+                        s0 += gm * __ldg(eab + m * C::HAB + h);
+                        s1 += gm * __ldg(e1ab + (0 * C::SAB + m) * C::HAB + h);
+                        s2 += gm * __ldg(e1ab + (1 * C::SAB + m) * C::HAB + h);
+                        s3 += gm * __ldg(e1ab + (2 * C::SAB + m) * C::HAB + h);
+                    }
+                    ge[h * C::SCD + c] = s0;
+                    ge1[(0 * C::HAB + h) * C::SCD + c] = s1;
+                    ge1[(1 * C::HAB + h) * C::SCD + c] = s2;
+                    ge1[(2 * C::HAB + h) * C::SCD + c] = s3;
+                }
+            double t1[3] = {0, 0, 0}, t13[3] = {0, 0, 0}, tc[3] = {0, 0, 0};
+            for (uint32_t q = q0; q < q1; q++)
+            {
+                const PQ4 Q = loadPQ(a.ket.pP, q);
+                const double cq = __ldg(a.ket.ab + 2 * q) / Q.x;
+                const double rs = rsqrt(P.x + Q.x);
+                const double alpha = P.x * Q.x * (rs * rs);
+                const double X = P.y - Q.y, Y = P.z - Q.z, Z = P.w - Q.w;
+                const double fac = 34.986836655249725 * rs * P.ip * Q.ip;
+                double F[L1 + 1];
+                boysF<L1, false>(alpha * (X * X + Y * Y + Z * Z), a.boys + L1 * kBoysTerms * kBoysPitch, F);
+#pragma unroll
+                for (int k = 0; k <= L1; k++)
+                    F[k] *= fac;
+                double R[nherm(L1)];
+                hermiteR<L1, double>(-2.0 * alpha, F, X, Y, Z, R);
+                const double *ecd = a.ket.Et + (size_t)q * C::HCD * C::SCD;
+                const double *e1cd = a.ket.E1t + (size_t)q * 3 * C::HCD * C::SCD;
+#pragma unroll
+                for (int h = 0, nh = 0; nh <= C::LAB; nh++)
+#pragma unroll
+                    for (int th = nh; th >= 0; th--)
+#pragma unroll
+                        for (int uh = nh - th; uh >= 0; uh--, h++)
+                        {
+                            const int vh = nh - th - uh;
+#pragma unroll
+                            for (int c = 0; c < C::SCD; c++)
+                            {
+                                double u0 = 0.0, ux = 0.0, uy = 0.0, uz = 0.0, vx = 0.0, vy = 0.0, vz = 0.0;
+#pragma unroll
+                                for (int hp = 0, np = 0; np <= C::LCD; np++)
+#pragma unroll
+                                    for (int tp = np; tp >= 0; tp--)
+#pragma unroll
+                                        for (int up = np - tp; up >= 0; up--, hp++)
+                                        {
+                                            const int vp = np - tp - up;
+                                            const double sgn = (np & 1) ? -1.0 : 1.0;
+                                            const double e0 = sgn * __ldg(ecd + hp * C::SCD + c);
+                                            const int t = th + tp, u = uh + up, v = vh + vp;
+                                            const double r0 = R[hermIndex(t, u, v)];
+                                            u0 += r0 * e0;
+                                            ux += R[hermIndex(t + 1, u, v)] * e0;
+                                            uy += R[hermIndex(t, u + 1, v)] * e0;
+                                            uz += R[hermIndex(t, u, v + 1)] * e0;
+                                            const double rs0 = sgn * r0;
+                                            vx += rs0 * __ldg(e1cd + (0 * C::HCD + hp) * C::SCD + c);
+                                            vy += rs0 * __ldg(e1cd + (1 * C::HCD + hp) * C::SCD + c);
+                                            vz += rs0 * __ldg(e1cd + (2 * C::HCD + hp) * C::SCD + c);
+                                        }
+                                const double gev = ge[h * C::SCD + c];
+                                t1[0] += gev * ux;
+                                t1[1] += gev * uy;
+                                t1[2] += gev * uz;
+                                t13[0] += ge1[(0 * C::HAB + h) * C::SCD + c] * u0;
+                                t13[1] += ge1[(1 * C::HAB + h) * C::SCD + c] * u0;
+                                t13[2] += ge1[(2 * C::HAB + h) * C::SCD + c] * u0;
+                                tc[0] += gev * (vx - cq * ux);
+                                tc[1] += gev * (vy - cq * uy);
+                                tc[2] += gev * (vz - cq * uz);
+                            }
+                        }
+            }
+            const double ap = AB.x * P.ip, bp = AB.y * P.ip;
+#pragma unroll
+            for (int x = 0; x < 3; x++)
+            {
+                g[x] += ap * t1[x] + t13[x];
+                g[3 + x] += bp * t1[x] - t13[x];
+                g[6 + x] += tc[x];
+            }
+        }
+    }
+
+    // J/K-gradient kernel of the register classes: warps take 32 consecutive tasks of a work-queue
+    // chunk (one per lane); each block sums its gradient in shared memory ([n_atoms][3], shared
+    // atomics; the ket-centre terms of a warp whose lanes share the ket pair are summed by shuffles
+    // first) and adds it to the output once.
+    template <int LA, int LB, int LC, int LD>
+    __global__ void __launch_bounds__(128) eriD1RegKernel(QuartetArgs a)
+    {
+        extern __shared__ __align__(16) double sg[];
+        for (int e = threadIdx.x; e < 3 * a.n_atoms; e += blockDim.x)
+            sg[e] = 0.0;
+        __syncthreads();
+        const int lane = threadIdx.x & 31;
+        auto processRange = [&](long long start, long long end) {
+            int cur = a.list ? 0 : advanceMajor(a, start, 0);
+            for (long long base = start; base < end; base += 32)
+            {
+                const long long t = base + lane;
+                uint32_t ib = 0, ik = 0;
+                bool active = false;
+                double g[9];
+#pragma unroll
+                for (int x = 0; x < 9; x++)
+                    g[x] = 0.0;
+                if (t < end)
+                {
+                    int my = cur;
+                    decodeCursor(a, t, my, ib, ik);
+                    active = inWindow(a, ib, ik, 0, false);
+                    if (active)
+                        quartetD1Reg<LA, LB, LC, LD>(a, ib, ik, g);
+                }
+                if (!a.list)
+                    cur = advanceMajor(a, base + 32 < end ? base + 32 : end - 1, cur);
+                const int32_t *bi = a.bra.info + 8 * ib;
+                const int32_t *ki = a.ket.info + 8 * ik;
+                const unsigned vmask = __ballot_sync(0xffffffffu, active);
+                const uint32_t ik0 = __shfl_sync(0xffffffffu, ik, 0);
+                const bool uniform = vmask == 0xffffffffu && __all_sync(0xffffffffu, ik == ik0);
+#pragma unroll
+                for (int x = 0; x < 3; x++)
+                {
+                    double gc = g[6 + x], gd = -(g[x] + g[3 + x] + g[6 + x]);
+                    if (uniform)
+                    {
+#pragma unroll
+                        for (int o = 16; o > 0; o >>= 1)
+                        {
+                            gc += __shfl_xor_sync(0xffffffffu, gc, o);
+                            gd += __shfl_xor_sync(0xffffffffu, gd, o);
+                        }
+                        if (lane == 0)
+                        {
+                            atomicAdd(sg + 3 * ki[2] + x, gc);
+                            atomicAdd(sg + 3 * ki[3] + x, gd);
+                        }
+                    }
+                    else if (active)
+                    {
+                        atomicAdd(sg + 3 * ki[2] + x, gc);
+                        atomicAdd(sg + 3 * ki[3] + x, gd);
+                    }
+                    if (active)
+                    {
+                        atomicAdd(sg + 3 * bi[2] + x, g[x]);
+                        atomicAdd(sg + 3 * bi[3] + x, g[3 + x]);
+                    }
+                }
+            }
+        };
+        if (a.chunks)
+        {
+            for (;;)
+            {
+                unsigned long long c = 0;
+                if (lane == 0)
+                    c = atomicAdd(a.counter, 1ULL);
+                c = __shfl_sync(0xffffffffu, c, 0);
+                if (c >= (unsigned long long)a.n_chunks)
+                    break;
+                processRange((long long)__ldg(a.chunks + c), (long long)__ldg(a.chunks + c + 1));
+            }
+        }
+        else
+        {
+            const long long warps = (long long)gridDim.x * (blockDim.x >> 5);
+            const long long gw = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+            constexpr long long CH = 8 * 32;
+            const long long n_chunks = (a.n_tasks + CH - 1) / CH;
+            for (long long chunk = gw; chunk < n_chunks; chunk += warps)
+                processRange(chunk * CH, (chunk + 1) * CH < a.n_tasks ? (chunk + 1) * CH : a.n_tasks);
+        }
+        __syncthreads();
+        for (int e = threadIdx.x; e < 3 * a.n_atoms; e += blockDim.x)
+            if (sg[e] != 0.0)
+                atomicAdd(a.grad + e, sg[e]);
+    }
 }

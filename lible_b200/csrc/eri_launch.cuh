@@ -92,6 +92,24 @@ namespace lible_b200
         using S = ShapeD1<LA, LB, LC, LD>;
         if (a.n_tasks <= 0)
             return cudaSuccess;
+        if constexpr (d1RegisterClass(LA, LB, LC, LD))
+        {
+            // J/K gradient of the smallest classes: one quartet per thread, the block's gradient in
+            // shared memory (up to 2,048 atoms)
+            const size_t sg = sizeof(double) * 3 * (size_t)std::max(a.n_atoms, 1);
+            if (a.mode == kD1Grad && a.n_atoms > 0 && sg <= 48 * 1024)
+            {
+                auto rk = eriD1RegKernel<LA, LB, LC, LD>;
+                int occ = 0;
+                cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, rk, 128, sg);
+                if (e != cudaSuccess)
+                    return e;
+                long long grid = a.chunks ? (a.n_chunks + 3) / 4 : (a.n_tasks + 8LL * 128 - 1) / (8LL * 128);
+                grid = std::max<long long>(1, std::min<long long>(grid, (long long)num_sms * std::max(occ, 1)));
+                rk<<<(unsigned)grid, 128, sg, s>>>(a);
+                return cudaGetLastError();
+            }
+        }
         auto kern = eriD1Kernel<LA, LB, LC, LD>;
         if (S::smem > 48 * 1024)
         {

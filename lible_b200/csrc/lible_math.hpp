@@ -56,6 +56,14 @@ namespace lible_b200
         return nherm(t + u + v - 1) + cartIndex(u, v);
     }
 
+    // Derivative classes whose J/K-gradient contraction runs one quartet per thread with its state
+    // in registers (eriD1RegKernel): the Gamma-weighted bra coefficients (4 x H_ab x S_cd values) and
+    // the R vector to order L + 1 must fit about 80 doubles.
+    LB_HD constexpr bool d1RegisterClass(int la, int lb, int lc, int ld)
+    {
+        return 4 * nherm(la + lb) * nsph(lc) * nsph(ld) + nherm(la + lb + lc + ld + 1) <= 80;
+    }
+
     // Hermite expansion coefficients of a primitive pair along one axis, McMurchie-Davidson
     // recurrences (Helgaker, Jorgensen, Olsen, Molecular Electronic-Structure Theory, 9.5.6-9.5.7).
     // E[i][j][t] is stored at E[(i * (lb + 1) + j) * (la + lb + 1) + t].  `one_o_2p` = 1/(2p),
