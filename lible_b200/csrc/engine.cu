@@ -2009,7 +2009,8 @@ namespace lible_b200
             {
                 // one quartet per block at a time: chunks of the heaviest quartet up to 8 tasks; the
                 // register classes take 32 quartets per warp step
-                const int unit = d1RegisterClass(B.la, B.lb, K.la, K.lb) ? 32 : 1;
+                const int gt = d1RegisterGroup(B.la, B.lb, K.la, K.lb);
+                const int unit = gt ? 32 / gt : 1;
                 auto ch = costChunks(cp.run64, cp.cost, unit, 8 * unit);
                 cp.n_chunksD1 = (long long)ch.size() - 1;
                 cp.chunksD1 = devUpload(ch, stream_);

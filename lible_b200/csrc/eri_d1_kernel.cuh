@@ -454,24 +454,27 @@ namespace lible_b200
     //   tc_x  = sum GE  . (-(c/q) dR/dP_x E_cd^T + R E1_cd,x^T),
     // and A_x += (a/p) t1_x + t13_x, B_x += (b/p) t1_x - t13_x, C_x += tc_x (D by invariance).
     template <int LA, int LB, int LC, int LD>
-    __device__ __forceinline__ void quartetD1Reg(const QuartetArgs &a, uint32_t ib, uint32_t ik, double *g)
+    __device__ __forceinline__ void quartetD1Reg(const QuartetArgs &a, uint32_t ib, uint32_t ik, int c0, double *g)
     {
         using C = Cls<LA, LB, LC, LD>;
         constexpr int L1 = C::L + 1;
+        // this thread's ket columns [c0, c0 + CW)
+        constexpr int CW = C::SCD / d1RegisterGroup(LA, LB, LC, LD);
         const int32_t *bi = a.bra.info + 8 * ib;
         const int32_t *ki = a.ket.info + 8 * ik;
         const double f = quartetWeight(a, ib, ik);
         const size_t n = (size_t)a.nao;
         const double *D = a.D;
-        double gam[C::SAB * C::SCD];
+        double gam[C::SAB * CW];
 #pragma unroll
         for (int m = 0; m < C::SAB; m++)
 #pragma unroll
-            for (int c = 0; c < C::SCD; c++)
+            for (int cw = 0; cw < CW; cw++)
             {
+                const int c = c0 + cw;
                 const size_t mu = bi[0] + m / C::SB, nu = bi[1] + m % C::SB;
                 const size_t ka = ki[0] + c / C::SD, ta = ki[1] + c % C::SD;
-                gam[m * C::SCD + c] = f * (4.0 * __ldg(D + mu * n + nu) * __ldg(D + ka * n + ta) -
+                gam[m * CW + cw] = f * (4.0 * __ldg(D + mu * n + nu) * __ldg(D + ka * n + ta) -
                                            __ldg(D + mu * n + ka) * __ldg(D + nu * n + ta) -
                                            __ldg(D + mu * n + ta) * __ldg(D + nu * n + ka));
             }
@@ -486,26 +489,26 @@ namespace lible_b200
             const double2 AB = __ldg(reinterpret_cast<const double2 *>(a.bra.ab) + p);
             const double *eab = a.bra.E + (size_t)p * C::SAB * C::HAB;
             const double *e1ab = a.bra.E1 + (size_t)p * 3 * C::SAB * C::HAB;
-            double ge[C::HAB * C::SCD], ge1[3 * C::HAB * C::SCD];
+            double ge[C::HAB * CW], ge1[3 * C::HAB * CW];
 #pragma unroll
             for (int h = 0; h < C::HAB; h++)
 #pragma unroll
-                for (int c = 0; c < C::SCD; c++)
+                for (int cw = 0; cw < CW; cw++)
                 {
                     double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
 #pragma unroll
                     for (int m = 0; m < C::SAB; m++)
                     {
-                        const double gm = gam[m * C::SCD + c];
+                        const double gm = gam[m * CW + cw];
                         s0 += gm * __ldg(eab + m * C::HAB + h);
                         s1 += gm * __ldg(e1ab + (0 * C::SAB + m) * C::HAB + h);
                         s2 += gm * __ldg(e1ab + (1 * C::SAB + m) * C::HAB + h);
                         s3 += gm * __ldg(e1ab + (2 * C::SAB + m) * C::HAB + h);
                     }
-                    ge[h * C::SCD + c] = s0;
-                    ge1[(0 * C::HAB + h) * C::SCD + c] = s1;
-                    ge1[(1 * C::HAB + h) * C::SCD + c] = s2;
-                    ge1[(2 * C::HAB + h) * C::SCD + c] = s3;
+                    ge[h * CW + cw] = s0;
+                    ge1[(0 * C::HAB + h) * CW + cw] = s1;
+                    ge1[(1 * C::HAB + h) * CW + cw] = s2;
+                    ge1[(2 * C::HAB + h) * CW + cw] = s3;
                 }
             double t1[3] = {0, 0, 0}, t13[3] = {0, 0, 0}, tc[3] = {0, 0, 0};
             for (uint32_t q = q0; q < q1; q++)
@@ -534,8 +537,9 @@ namespace lible_b200
                         {
                             const int vh = nh - th - uh;
 #pragma unroll
-                            for (int c = 0; c < C::SCD; c++)
+                            for (int cw = 0; cw < CW; cw++)
                             {
+                                const int c = c0 + cw;
                                 double u0 = 0.0, ux = 0.0, uy = 0.0, uz = 0.0, vx = 0.0, vy = 0.0, vz = 0.0;
 #pragma unroll
                                 for (int hp = 0, np = 0; np <= C::LCD; np++)
@@ -558,13 +562,13 @@ namespace lible_b200
                                             vy += rs0 * __ldg(e1cd + (1 * C::HCD + hp) * C::SCD + c);
                                             vz += rs0 * __ldg(e1cd + (2 * C::HCD + hp) * C::SCD + c);
                                         }
-                                const double gev = ge[h * C::SCD + c];
+                                const double gev = ge[h * CW + cw];
                                 t1[0] += gev * ux;
                                 t1[1] += gev * uy;
                                 t1[2] += gev * uz;
-                                t13[0] += ge1[(0 * C::HAB + h) * C::SCD + c] * u0;
-                                t13[1] += ge1[(1 * C::HAB + h) * C::SCD + c] * u0;
-                                t13[2] += ge1[(2 * C::HAB + h) * C::SCD + c] * u0;
+                                t13[0] += ge1[(0 * C::HAB + h) * CW + cw] * u0;
+                                t13[1] += ge1[(1 * C::HAB + h) * CW + cw] * u0;
+                                t13[2] += ge1[(2 * C::HAB + h) * CW + cw] * u0;
                                 tc[0] += gev * (vx - cq * ux);
                                 tc[1] += gev * (vy - cq * uy);
                                 tc[2] += gev * (vz - cq * uz);
@@ -594,32 +598,39 @@ namespace lible_b200
             sg[e] = 0.0;
         __syncthreads();
         const int lane = threadIdx.x & 31;
+        // GT threads per quartet (each owning S_cd / GT ket columns), QPW quartets per warp step
+        constexpr int GT = d1RegisterGroup(LA, LB, LC, LD), QPW = 32 / GT;
+        constexpr int CW = Cls<LA, LB, LC, LD>::SCD / GT;
+        constexpr unsigned used = QPW * GT == 32 ? 0xffffffffu : ((1u << (QPW * GT)) - 1u);
+        const int slot = lane / GT, member = lane % GT;
         auto processRange = [&](long long start, long long end) {
             int cur = a.list ? 0 : advanceMajor(a, start, 0);
-            for (long long base = start; base < end; base += 32)
+            for (long long base = start; base < end; base += QPW)
             {
-                const long long t = base + lane;
+                const long long t = base + slot;
                 uint32_t ib = 0, ik = 0;
                 bool active = false;
                 double g[9];
 #pragma unroll
                 for (int x = 0; x < 9; x++)
                     g[x] = 0.0;
-                if (t < end)
+                if (slot < QPW && t < end)
                 {
                     int my = cur;
                     decodeCursor(a, t, my, ib, ik);
                     active = inWindow(a, ib, ik, 0, false);
                     if (active)
-                        quartetD1Reg<LA, LB, LC, LD>(a, ib, ik, g);
+                        quartetD1Reg<LA, LB, LC, LD>(a, ib, ik, member * CW, g);
                 }
                 if (!a.list)
-                    cur = advanceMajor(a, base + 32 < end ? base + 32 : end - 1, cur);
+                    cur = advanceMajor(a, base + QPW < end ? base + QPW : end - 1, cur);
                 const int32_t *bi = a.bra.info + 8 * ib;
                 const int32_t *ki = a.ket.info + 8 * ik;
+                // every used lane holds a quartet of one ket pair: the ket-centre terms are summed
+                // across the warp (the group members' partial sums included)
                 const unsigned vmask = __ballot_sync(0xffffffffu, active);
                 const uint32_t ik0 = __shfl_sync(0xffffffffu, ik, 0);
-                const bool uniform = vmask == 0xffffffffu && __all_sync(0xffffffffu, ik == ik0);
+                const bool uniform = vmask == used && __all_sync(0xffffffffu, !((used >> lane) & 1u) || ik == ik0);
 #pragma unroll
                 for (int x = 0; x < 3; x++)
                 {

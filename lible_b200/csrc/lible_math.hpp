@@ -56,12 +56,21 @@ namespace lible_b200
         return nherm(t + u + v - 1) + cartIndex(u, v);
     }
 
-    // Derivative classes whose J/K-gradient contraction runs one quartet per thread with its state
-    // in registers (eriD1RegKernel): the Gamma-weighted bra coefficients (4 x H_ab x S_cd values) and
-    // the R vector to order L + 1 must fit about 80 doubles.
+    // Derivative classes whose J/K-gradient contraction runs in registers (eriD1RegKernel): a group
+    // of g threads per quartet, each owning S_cd / g ket columns, with its Gamma-weighted bra
+    // coefficients (4 x H_ab x S_cd / g values) and the R vector to order L + 1 within about 120
+    // doubles.  Returns the smallest such g (a divisor of S_cd), 0 when none fits.
+    LB_HD constexpr int d1RegisterGroup(int la, int lb, int lc, int ld)
+    {
+        const int scd = nsph(lc) * nsph(ld);
+        for (int g = 1; g <= 32 && g <= scd; g++)
+            if (scd % g == 0 && 4 * nherm(la + lb) * (scd / g) + nherm(la + lb + lc + ld + 1) <= 120)
+                return g;
+        return 0;
+    }
     LB_HD constexpr bool d1RegisterClass(int la, int lb, int lc, int ld)
     {
-        return 4 * nherm(la + lb) * nsph(lc) * nsph(ld) + nherm(la + lb + lc + ld + 1) <= 80;
+        return d1RegisterGroup(la, lb, lc, ld) > 0;
     }
 
     // Hermite expansion coefficients of a primitive pair along one axis, McMurchie-Davidson
