@@ -58,13 +58,15 @@ namespace lible_b200
 
     // Derivative classes whose J/K-gradient contraction runs in registers (eriD1RegKernel): a group
     // of g threads per quartet, each owning S_cd / g ket columns, with its Gamma-weighted bra
-    // coefficients (4 x H_ab x S_cd / g values) and the R vector to order L + 1 within about 120
-    // doubles.  Returns the smallest such g (a divisor of S_cd), 0 when none fits.
+    // coefficients (4 x H_ab x S_cd / g values) and the R vector to order L + 1 within 170 doubles
+    // (the steady-state (H2O)_8 cc-pVTZ gradient measured 0.85 s at 120, 0.73 s at 170, 0.82 s at 230:
+    // beyond 170 the spills outweigh the block kernel's synchronisation).  Returns the smallest such
+    // g (a divisor of S_cd), 0 when none fits.
     LB_HD constexpr int d1RegisterGroup(int la, int lb, int lc, int ld)
     {
         const int scd = nsph(lc) * nsph(ld);
         for (int g = 1; g <= 32 && g <= scd; g++)
-            if (scd % g == 0 && 4 * nherm(la + lb) * (scd / g) + nherm(la + lb + lc + ld + 1) <= 120)
+            if (scd % g == 0 && 4 * nherm(la + lb) * (scd / g) + nherm(la + lb + lc + ld + 1) <= 170)
                 return g;
         return 0;
     }
