@@ -2194,7 +2194,9 @@ namespace lible_b200
                 const auto &B = bs.dev[cp.cb], &K = ks.dev[cp.ck];
                 if (!cp.chunksD1 && cp.t64 > 0)
                 {
-                    auto ch = costChunks(cp.run64, cp.cost, 1, 8);
+                    const int gt = d1RegisterGroup(B.la, B.lb, K.la, K.lb);
+                    const int unit = gt ? 32 / gt : 1;
+                    auto ch = costChunks(cp.run64, cp.cost, unit, 8 * unit);
                     cp.n_chunksD1 = (long long)ch.size() - 1;
                     cp.chunksD1 = devUpload(ch, stream_);
                 }
@@ -2222,6 +2224,7 @@ namespace lible_b200
                 a.dcoef = dcoef_dev;
                 a.nao = (int)nao_;
                 a.grad = grad_dev;
+                a.n_atoms = n_atoms_;
                 a.status = d_status_;
                 a.chunks = cp.chunksD1;
                 a.n_chunks = cp.n_chunksD1;

@@ -446,10 +446,11 @@ namespace lible_b200
     }
 
     // ---------------------------------------------------------------------------------------
-    // Register form of the J/K-gradient contraction for the smallest classes (d1RegisterClass): one
-    // thread per quartet.  With Gamma the two-particle density block of the quartet (as in kD1Grad)
-    // and, per bra primitive, GE = Gamma^T E_ab and GE1_x = Gamma^T E1_ab,x (H_ab x S_cd each), the
-    // gradient terms of the formulas above become per primitive quartet
+    // Register form of the gradient contraction (J/K, kD1Grad, and RI-J, kD1GradRI) for the classes
+    // of d1RegisterClass: GT threads per quartet, each owning S_cd / GT ket columns.  With Gamma the
+    // density block of the quartet (as in the block kernel's epilogues) and, per bra primitive,
+    // GE = Gamma^T E_ab and GE1_x = Gamma^T E1_ab,x, the gradient terms of the formulas above become
+    // per primitive quartet
     //   t1_x  = sum GE  . (dR/dP_x E_cd^T),   t13_x = sum GE1_x . (R E_cd^T),
     //   tc_x  = sum GE  . (-(c/q) dR/dP_x E_cd^T + R E1_cd,x^T),
     // and A_x += (a/p) t1_x + t13_x, B_x += (b/p) t1_x - t13_x, C_x += tc_x (D by invariance).
@@ -462,22 +463,47 @@ namespace lible_b200
         constexpr int CW = C::SCD / d1RegisterGroup(LA, LB, LC, LD);
         const int32_t *bi = a.bra.info + 8 * ib;
         const int32_t *ki = a.ket.info + 8 * ik;
-        const double f = quartetWeight(a, ib, ik);
         const size_t n = (size_t)a.nao;
         const double *D = a.D;
         double gam[C::SAB * CW];
+        if (a.mode == kD1GradRI)
+        {
+            // RI-J: w D_mn d_P (three-centre, the auxiliary shell on either side) or -w/2 d_P d_Q
+            // (two-centre), w the multiplicity of the unique pair, as in the block kernel
+            const int32_t *mi = a.aux_side == 0 ? bi : ki;
+            const double w = a.aux_side == 2 ? -((a.same_class && ib == ik) ? 0.5 : 1.0) : (mi[4] == mi[5] ? 1.0 : 2.0);
 #pragma unroll
-        for (int m = 0; m < C::SAB; m++)
+            for (int m = 0; m < C::SAB; m++)
 #pragma unroll
-            for (int cw = 0; cw < CW; cw++)
-            {
-                const int c = c0 + cw;
-                const size_t mu = bi[0] + m / C::SB, nu = bi[1] + m % C::SB;
-                const size_t ka = ki[0] + c / C::SD, ta = ki[1] + c % C::SD;
-                gam[m * CW + cw] = f * (4.0 * __ldg(D + mu * n + nu) * __ldg(D + ka * n + ta) -
-                                           __ldg(D + mu * n + ka) * __ldg(D + nu * n + ta) -
-                                           __ldg(D + mu * n + ta) * __ldg(D + nu * n + ka));
-            }
+                for (int cw = 0; cw < CW; cw++)
+                {
+                    const int c = c0 + cw;
+                    double v;
+                    if (a.aux_side == 2)
+                        v = __ldg(a.dcoef + bi[0] + m) * __ldg(a.dcoef + ki[0] + c);
+                    else if (a.aux_side == 0)
+                        v = __ldg(D + (size_t)(bi[0] + m / C::SB) * n + bi[1] + m % C::SB) * __ldg(a.dcoef + ki[0] + c);
+                    else
+                        v = __ldg(D + (size_t)(ki[0] + c / C::SD) * n + ki[1] + c % C::SD) * __ldg(a.dcoef + bi[0] + m);
+                    gam[m * CW + cw] = w * v;
+                }
+        }
+        else
+        {
+            const double f = quartetWeight(a, ib, ik);
+#pragma unroll
+            for (int m = 0; m < C::SAB; m++)
+#pragma unroll
+                for (int cw = 0; cw < CW; cw++)
+                {
+                    const int c = c0 + cw;
+                    const size_t mu = bi[0] + m / C::SB, nu = bi[1] + m % C::SB;
+                    const size_t ka = ki[0] + c / C::SD, ta = ki[1] + c % C::SD;
+                    gam[m * CW + cw] = f * (4.0 * __ldg(D + mu * n + nu) * __ldg(D + ka * n + ta) -
+                                               __ldg(D + mu * n + ka) * __ldg(D + nu * n + ta) -
+                                               __ldg(D + mu * n + ta) * __ldg(D + nu * n + ka));
+                }
+        }
 #pragma unroll
         for (int x = 0; x < 9; x++)
             g[x] = 0.0;

@@ -97,7 +97,7 @@ namespace lible_b200
             // J/K gradient of the smallest classes: one quartet per thread, the block's gradient in
             // shared memory (up to 2,048 atoms)
             const size_t sg = sizeof(double) * 3 * (size_t)std::max(a.n_atoms, 1);
-            if (a.mode == kD1Grad && a.n_atoms > 0 && sg <= 48 * 1024)
+            if ((a.mode == kD1Grad || a.mode == kD1GradRI) && a.n_atoms > 0 && sg <= 48 * 1024)
             {
                 auto rk = eriD1RegKernel<LA, LB, LC, LD>;
                 int occ = 0;
