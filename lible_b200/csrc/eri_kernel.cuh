@@ -228,14 +228,16 @@ namespace lible_b200
     // into the unsymmetrised accumulators (J = A + A^T, K = B + B^T afterwards).  The K blocks are
     // written transposed (rows of the ket's AOs) and their D factors read through the symmetry of D,
     // so a ket-uniform warp whose bras are sorted by AO touches neighbouring columns of one row.
-    // `ket_uniform` (serial form only): every lane of the warp holds a quartet with the same ket
-    // pair, so the J_cd sums are reduced across the warp and added once.  `active` = false (serial,
-    // ket-uniform form only): the lane holds no quartet; it joins that reduction with zeros and
-    // writes nothing else.
+    // `collective` (serial form only): all 32 lanes of the warp call together, lane i holding the
+    // quartet of ket pair `ket` (consecutive lanes hold consecutive tasks, so equal kets form runs).
+    // The J_cd sums of each run of lanes with one ket pair, and the K_ac / K_ad sums of each run
+    // with one ket pair and one shell a, are reduced by shuffles and added once by the run's first
+    // lane.  `active` = false (collective form only): the lane holds no quartet; it forms a run of
+    // its own with zeros and writes nothing.
     template <int SA, int SB, int SC, int SD, bool SERIAL, typename F>
     __device__ __forceinline__ void digestJK(const QuartetArgs &a, double f, const BraFields &bf,
                                              const int32_t *ki, F val, int tid, int stride,
-                                             bool ket_uniform = false, bool active = true)
+                                             bool collective = false, bool active = true, uint32_t ket = 0)
     {
         if constexpr (SERIAL)
         {
@@ -250,20 +252,25 @@ namespace lible_b200
         double *const Km = a.K + base;
         constexpr int n0 = SA * SB, n1 = n0 + SC * SD, n2 = n1 + SA * SC, n3 = n2 + SA * SD,
                       n4 = n3 + SB * SC, n5 = n4 + SB * SD;
-        // ket-uniform warps over AO-sorted bras: neighbouring lanes with the same shell a form a run
-        // (a run starts where a differs from the left neighbour's) and write the same K_ac / K_ad
-        // elements; each run is summed with a shuffle tree and added once by its first lane
-        int run_last = 0;
-        bool run_head = true;
+        // runs of neighbouring lanes (a run starts where the key differs from the left neighbour's):
+        // one ket pair for J_cd; one ket pair and one shell a for K_ac / K_ad (AO-sorted bras put
+        // equal a next to each other).  Each run is summed with a shuffle tree and added once by its
+        // first lane.
+        int run_last_j = 0, run_last_k = 0;
+        bool head_j = true, head_k = true;
         if constexpr (SERIAL)
-            if (ket_uniform)
+            if (collective)
             {
                 const int lane = threadIdx.x & 31;
-                const int left = __shfl_up_sync(0xffffffffu, oa, 1);
-                run_head = lane == 0 || left != oa;
-                const unsigned heads = __ballot_sync(0xffffffffu, run_head);
-                const unsigned later = lane == 31 ? 0u : heads & (0xffffffffu << (lane + 1));
-                run_last = later ? __ffs(later) - 2 : 31;
+                const long long kj = active ? (long long)ket : -1 - lane;
+                const long long kleft = __shfl_up_sync(0xffffffffu, kj, 1);
+                const int oleft = __shfl_up_sync(0xffffffffu, oa, 1);
+                head_j = lane == 0 || kleft != kj;
+                head_k = head_j || oleft != oa;
+                const unsigned hj = __ballot_sync(0xffffffffu, head_j), hk = __ballot_sync(0xffffffffu, head_k);
+                const unsigned above = lane == 31 ? 0u : (0xffffffffu << (lane + 1));
+                run_last_j = (hj & above) ? __ffs(hj & above) - 2 : 31;
+                run_last_k = (hk & above) ? __ffs(hk & above) - 2 : 31;
             }
 #pragma unroll
         for (int o = tid; o < n5; o += stride)
@@ -342,26 +349,20 @@ namespace lible_b200
             double v = active ? w * s : 0.0;
             if constexpr (SERIAL)
             {
-                if (ket_uniform && o >= n0 && o < n1)
+                if (collective && o >= n0 && o < n3)
                 {
-#pragma unroll
-                    for (int sh = 16; sh > 0; sh >>= 1)
-                        v += __shfl_xor_sync(0xffffffffu, v, sh);
-                    if ((threadIdx.x & 31) != 0)
-                        continue;
-                }
-                else if (ket_uniform && o >= n1 && o < n3)
-                {
-                    // K_ac, K_ad: sum over the run of lanes with this lane's shell a
+                    // J_cd over the run of lanes with this lane's ket pair; K_ac, K_ad over the run
+                    // with this lane's ket pair and shell a
                     const int lane = threadIdx.x & 31;
+                    const int last = o < n1 ? run_last_j : run_last_k;
 #pragma unroll
                     for (int off = 1; off < 32; off <<= 1)
                     {
                         const double u = __shfl_down_sync(0xffffffffu, v, off);
-                        if (lane + off <= run_last)
+                        if (lane + off <= last)
                             v += u;
                     }
-                    if (!run_head || v == 0.0)
+                    if (!(o < n1 ? head_j : head_k) || v == 0.0)
                         continue;
                 }
                 else if (!active)
@@ -1082,19 +1083,11 @@ namespace lible_b200
                 else if constexpr (GT == 1)
                 {
                     auto val = [&](int e) { return (double)V[e]; };
-                    // ket-major enumeration: usually the whole warp shares one ket pair
-                    const unsigned vmask = __ballot_sync(0xffffffffu, valid);
-                    const uint32_t ik0 = __shfl_sync(0xffffffffu, ik, 0);
-                    const bool uniform = vmask == 0xffffffffu && __all_sync(0xffffffffu, ik == ik0);
+                    // ket-major enumeration: consecutive lanes mostly share the ket pair, and the
+                    // whole warp digests together (runs of equal ket pairs reduced)
                     if (a.mode == kJK)
-                    {
-                        if (uniform)
-                            digestJK<C::SA, C::SB, C::SC, C::SD, true>(a, quartetWeight(a, bsame, ib, ik), bf, ki, val,
-                                                                       0, 1, true, active);
-                        else if (active)
-                            digestJK<C::SA, C::SB, C::SC, C::SD, true>(a, quartetWeight(a, bsame, ib, ik), bf, ki, val,
-                                                                       0, 1);
-                    }
+                        digestJK<C::SA, C::SB, C::SC, C::SD, true>(a, quartetWeight(a, bsame, ib, ik), bf, ki, val, 0,
+                                                                   1, true, active, ik);
                     else if (active)
                         digestRI<C::SA, C::SB, C::SC, C::SD, true>(a, bi, ki, val, 0, 1);
                 }
