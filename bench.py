@@ -16,6 +16,7 @@ import json
 import math
 import os
 import subprocess
+import tempfile
 import sys
 import time
 
@@ -60,8 +61,8 @@ def emit(obj):
 
 
 def clocks_start(gpu_index):
-    os.makedirs(os.path.join(ROOT, "gpurun_out"), exist_ok=True)
-    path = os.path.join(ROOT, "gpurun_out", f"clocks_{gpu_index}.csv")
+    # nvidia-smi samples of the timed region, in the temporary directory (summarised into the JSON line)
+    path = os.path.join(tempfile.gettempdir(), f"lible_b200_clocks_{os.getpid()}_{gpu_index}.csv")
     q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
          "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
          "clocks_event_reasons.sw_power_cap")
