@@ -36,7 +36,9 @@ namespace lible_b200
     {
         constexpr int tier1 = sizeof(T) == 8 ? 104 : 200, tier2 = sizeof(T) == 8 ? 144 : 288;
         const int g = pickRegGroupWithin(sab, scd, hab, nr, tier1);
-        return g ? g : pickRegGroupWithin(sab, scd, hab, nr, tier2);
+        const int g2 = g ? g : pickRegGroupWithin(sab, scd, hab, nr, tier2);
+        // third budget, whole quartets per thread only (e.g. (fd|ss)): still ahead of the DMMA group path
+        return g2 ? g2 : (sab * scd + hab * scd + nr <= (sizeof(T) == 8 ? 170 : 340) ? 1 : 0);
     }
 
     // Shared-memory pitches (in doubles) of the DMMA operand tiles.  Fragments read either 4 rows x 8
