@@ -29,15 +29,15 @@ namespace lible_b200
     }
     // Two tiers per arithmetic type: a share that fits the register file without spilling (104
     // doubles / 200 floats) is preferred; failing that, a moderate overflow (144 / 288 values, a few
-    // hundred bytes of spills) still beats one quartet per warp on the group path; beyond that the
-    // class uses the group path (0).
+    // hundred bytes of spills) still beats one quartet per warp on the group path; a third budget
+    // (170 / 340) is open to whole quartets per thread only; beyond that the class uses the group
+    // path (0).
     template <typename T>
     constexpr int pickRegGroup(int sab, int scd, int hab, int nr)
     {
         constexpr int tier1 = sizeof(T) == 8 ? 104 : 200, tier2 = sizeof(T) == 8 ? 144 : 288;
         const int g = pickRegGroupWithin(sab, scd, hab, nr, tier1);
         const int g2 = g ? g : pickRegGroupWithin(sab, scd, hab, nr, tier2);
-        // third budget, whole quartets per thread only (e.g. (fd|ss)): still ahead of the DMMA group path
         return g2 ? g2 : (sab * scd + hab * scd + nr <= (sizeof(T) == 8 ? 170 : 340) ? 1 : 0);
     }
 
