@@ -1300,7 +1300,7 @@ namespace lible_b200
         }
     }
 
-    // The class kernels: the default register bound, or (minBlocksPerSM == 3) one that lets three
+    // The class kernels: the default register bound, or (minBlocksPerSM > 1) one that lets that many
     // blocks reside per SM.  Only the selected one is instantiated per class (eriKernelFor).
     template <int LA, int LB, int LC, int LD, typename T>
     __global__ void __launch_bounds__(Shape<LA, LB, LC, LD, T>::block) eriKernel(QuartetArgs a)
