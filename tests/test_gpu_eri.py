@@ -121,6 +121,23 @@ def test_eri4_class_batches_elementwise():
                 assert np.abs(got - want).max() <= 1e-12, (a.getLPair(), c.getLPair())
 
 
+def test_eri4_class_batches_elementwise_f_shells():
+    # def2-TZVP water has f functions on O: every class pair up to (ff|ff), among them the
+    # one-thread-per-quartet classes with the largest register budget ((fd|ss)) and the classes
+    # evaluated by whole warps on the tensor-core path ((fd|ps), (ff|dd), ...)
+    s = L.Structure("def2-tzvp", [8, 1, 1], H2O_ANG)
+    r = R.RefStructure("def2-tzvp", [8, 1, 1], H2O_ANG, units="angstrom")
+    sp = L.shellPairData(True, s)
+    assert [(x.la_, x.lb_, x.n_pairs_, x.n_ppairs_) for x in sp] == r.pair_classes(True)
+    assert max(x.la_ for x in sp) == 3
+    for a in sp:
+        for c in sp:
+            idx = [(i, j) for i in range(a.n_pairs_) for j in range(c.n_pairs_)]
+            got = L.ERI4Kernel(a, c).batch(idx).reshape(a.n_pairs_, c.n_pairs_, -1)
+            want = r.eri4_class(True, a.index, c.index).reshape(a.n_pairs_, c.n_pairs_, -1)
+            assert np.abs(got - want).max() <= 1e-12, (a.getLPair(), c.getLPair())
+
+
 def test_eri4d1_class_batches_elementwise():
     s = L.Structure("def2-svp", [8, 1, 1], H2O_ANG)
     r = R.RefStructure("def2-svp", [8, 1, 1], H2O_ANG, units="angstrom")
@@ -165,6 +182,23 @@ def test_jk_water_dimer_vs_reference_kernels():
     assert np.abs(J - Jr).max() <= 1e-11
     assert np.abs(K - Kr).max() <= 1e-11
     J2, K2, st2 = L.jk(s, D, schwarz=1e-12)
+    assert np.abs(J2 - Jr).max() <= 1e-9
+    assert np.abs(K2 - Kr).max() <= 1e-9
+
+
+def test_jk_water_dimer_ccpvtz_vs_reference_kernels():
+    # the J/K digestion epilogues of the f- and d-shell classes of cc-pVTZ (d on H, f on O)
+    Z, xyz, rng = water_cluster(2, seed=11)
+    s = L.Structure("cc-pvtz", Z, xyz, units="bohr")
+    assert s.nao == 116
+    D = random_density(s.nao, 10, rng)
+    r = R.RefStructure("cc-pvtz", Z, xyz)
+    J, K, st = L.jk(s, D, schwarz=0.0)
+    Jr, Kr, nq, _ = r.jk(D, schwarz=0.0)
+    assert st["n_quartets"] == nq
+    assert np.abs(J - Jr).max() <= 1e-11
+    assert np.abs(K - Kr).max() <= 1e-11
+    J2, K2, _ = L.jk(s, D, schwarz=1e-12)
     assert np.abs(J2 - Jr).max() <= 1e-9
     assert np.abs(K2 - Kr).max() <= 1e-9
 
