@@ -150,6 +150,18 @@ def test_eri4d1_class_batches_elementwise():
             assert np.abs(got - want).max() <= 1e-11, (a.getLPair(), c.getLPair())
 
 
+def test_eri4d1_class_batches_elementwise_f_shells():
+    s = L.Structure("def2-tzvp", [8, 1, 1], H2O_ANG)
+    r = R.RefStructure("def2-tzvp", [8, 1, 1], H2O_ANG, units="angstrom")
+    sp = L.shellPairData(True, s)
+    for a in sp:
+        for c in sp:
+            idx = [(i, j) for i in range(a.n_pairs_) for j in range(c.n_pairs_)]
+            got = L.ERI4D1Kernel(a, c).batch(idx).reshape(a.n_pairs_, c.n_pairs_, 12, -1)
+            want = r.eri4_class(True, a.index, c.index, d1=True).reshape(a.n_pairs_, c.n_pairs_, 12, -1)
+            assert np.abs(got - want).max() <= 1e-11, (a.getLPair(), c.getLPair())
+
+
 def test_deploy_eri3_eri2_golden():
     s = L.Structure("def2-svp", [8, 8, 8], O3_ANG, "def2-universal-jkfit")
     sp = L.shellPairData(False, s)
@@ -220,6 +232,16 @@ def test_jk_gradient_vs_reference_and_fd():
             e.append(L.jk_energy_forward(L.Structure("cc-pvdz", Z, c, units="bohr"), D, schwarz=0.0))
         fd = (e[0] - e[1]) / (2 * h)
         assert abs(fd - g[atom, x]) <= 1e-6
+
+
+def test_jk_gradient_ccpvtz_vs_reference():
+    # f and d classes through the register form of the derivative contraction
+    Z, xyz, rng = water_cluster(2, seed=5)
+    s = L.Structure("cc-pvtz", Z, xyz, units="bohr")
+    D = random_density(s.nao, 10, rng)
+    g = L.jk_energy_backward(s, D, schwarz=0.0)
+    gr = R.RefStructure("cc-pvtz", Z, xyz).jk_grad(D)
+    assert np.abs(g - gr).max() <= 1e-10
 
 
 def test_jk_gradient_screened_matches_screened_energy():
