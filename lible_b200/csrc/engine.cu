@@ -11,6 +11,7 @@
 #include <cstdio>
 #include <cstring>
 #include <functional>
+#include <memory>
 #include <numeric>
 #include <stdexcept>
 
@@ -416,6 +417,15 @@ namespace lible_b200
         return p;
     }
 
+    // Device allocation released on scope exit, also when a check throws (cudaFree synchronises,
+    // so a kernel still reading the buffer finishes first).
+    struct CudaFreeDeleter
+    {
+        void operator()(void *p) const { cudaFree(p); }
+    };
+    template <class T>
+    using DevPtr = std::unique_ptr<T, CudaFreeDeleter>;
+
     Engine::Engine(int device) : device_(device)
     {
         cudaCheck(cudaSetDevice(device), "cudaSetDevice");
@@ -656,20 +666,18 @@ namespace lible_b200
         }
         if (pc.n_ppairs == 0)
             return;
-        double *exps = devUpload(pc.exps, stream_);
-        double *coeffs = devUpload(pc.coeffs, stream_);
-        double *na = devUpload(pc.norms_a, stream_);
-        double *nb = devUpload(pc.norms_b, stream_);
+        DevPtr<double> exps(devUpload(pc.exps, stream_)), coeffs(devUpload(pc.coeffs, stream_)),
+            na(devUpload(pc.norms_a, stream_)), nb(devUpload(pc.norms_b, stream_));
         EArgs ea{};
         ea.la = pc.la;
         ea.lb = pc.lb;
         ea.n_pairs = pc.n_pairs;
         ea.n_ppairs = pc.n_ppairs;
-        ea.exps = exps;
-        ea.coeffs = coeffs;
+        ea.exps = exps.get();
+        ea.coeffs = coeffs.get();
         ea.coords = d.coords;
-        ea.norms_a = na;
-        ea.norms_b = nb;
+        ea.norms_a = na.get();
+        ea.norms_b = nb.get();
         ea.pofs = d.pofs;
         ea.sph.rc = sph_rc_;
         ea.sph.val = sph_val_;
@@ -698,10 +706,6 @@ namespace lible_b200
             cudaCheck(cudaGetLastError(), "padEtKernel");
         }
         cudaCheck(cudaStreamSynchronize(stream_), "ecoeffKernel");
-        cudaFree(exps);
-        cudaFree(coeffs);
-        cudaFree(na);
-        cudaFree(nb);
     }
 
     // Reference class order: la = 0..lmax, lb = 0..la (symmetric) or lb = 0..lmax (no symmetry)
@@ -917,16 +921,14 @@ namespace lible_b200
                 const long long nt = (long long)list.size() / 2;
                 if (nt == 0)
                     continue;
-                uint32_t *dl = devUpload(list, stream_);
+                DevPtr<uint32_t> dl(devUpload(list, stream_));
                 const int sa = nsph(B.la), sb = nsph(B.lb), sc = nsph(K.la), sd = nsph(K.lb);
-                double *tmp = devAlloc<double>((size_t)nt * sa * sb * sc * sd);
-                runStore(B, false, K, false, dl, nt, false, tmp, cb == ck);
-                scatter4Kernel<<<num_sms_ * 8, 256, 0, stream_>>>(tmp, dl, nt, B.info, K.info, sa, sb, sc, sd, n,
-                                                                   out_dev);
+                DevPtr<double> tmp(devAlloc<double>((size_t)nt * sa * sb * sc * sd));
+                runStore(B, false, K, false, dl.get(), nt, false, tmp.get(), cb == ck);
+                scatter4Kernel<<<num_sms_ * 8, 256, 0, stream_>>>(tmp.get(), dl.get(), nt, B.info, K.info, sa, sb, sc,
+                                                                   sd, n, out_dev);
                 cudaCheck(cudaGetLastError(), "scatter4");
                 cudaCheck(cudaStreamSynchronize(stream_), "eri4");
-                cudaFree(tmp);
-                cudaFree(dl);
             }
     }
 
@@ -945,16 +947,14 @@ namespace lible_b200
                 list.push_back(i);
                 list.push_back(i);
             }
-            uint32_t *dl = devUpload(list, stream_);
+            DevPtr<uint32_t> dl(devUpload(list, stream_));
             const size_t sab = (size_t)nsph(B.la) * nsph(B.lb);
-            double *tmp = devAlloc<double>(B.n_pairs * sab * sab);
-            runStore(B, false, B, false, dl, (long long)B.n_pairs, false, tmp, true);
+            DevPtr<double> tmp(devAlloc<double>(B.n_pairs * sab * sab));
+            runStore(B, false, B, false, dl.get(), (long long)B.n_pairs, false, tmp.get(), true);
             out[c].resize(B.n_pairs * sab * sab);
-            cudaCheck(cudaMemcpyAsync(out[c].data(), tmp, out[c].size() * sizeof(double), cudaMemcpyDeviceToHost,
-                                      stream_), "diag");
+            cudaCheck(cudaMemcpyAsync(out[c].data(), tmp.get(), out[c].size() * sizeof(double),
+                                      cudaMemcpyDeviceToHost, stream_), "diag");
             cudaCheck(cudaStreamSynchronize(stream_), "diag");
-            cudaFree(tmp);
-            cudaFree(dl);
         }
         return out;
     }
@@ -1004,16 +1004,14 @@ namespace lible_b200
                 const long long nt = (long long)list.size() / 2;
                 if (nt == 0)
                     continue;
-                uint32_t *dl = devUpload(list, stream_);
+                DevPtr<uint32_t> dl(devUpload(list, stream_));
                 const int sa = nsph(B.la), sb = nsph(B.lb), sc = nsph(X.la);
-                double *tmp = devAlloc<double>((size_t)nt * sa * sb * sc);
-                runStore(B, false, X, false, dl, nt, false, tmp, false);
-                scatter3Kernel<<<num_sms_ * 8, 256, 0, stream_>>>(tmp, dl, nt, B.info, X.info, 0, sa, sb, sc, n, na,
-                                                                   out_dev);
+                DevPtr<double> tmp(devAlloc<double>((size_t)nt * sa * sb * sc));
+                runStore(B, false, X, false, dl.get(), nt, false, tmp.get(), false);
+                scatter3Kernel<<<num_sms_ * 8, 256, 0, stream_>>>(tmp.get(), dl.get(), nt, B.info, X.info, 0, sa, sb,
+                                                                   sc, n, na, out_dev);
                 cudaCheck(cudaGetLastError(), "scatter3");
                 cudaCheck(cudaStreamSynchronize(stream_), "eri3");
-                cudaFree(tmp);
-                cudaFree(dl);
             }
     }
 
@@ -1037,15 +1035,14 @@ namespace lible_b200
                 const long long nt = (long long)list.size() / 2;
                 if (nt == 0)
                     continue;
-                uint32_t *dl = devUpload(list, stream_);
+                DevPtr<uint32_t> dl(devUpload(list, stream_));
                 const int sa = nsph(A.la), sb = nsph(B.la);
-                double *tmp = devAlloc<double>((size_t)nt * sa * sb);
-                runStore(A, false, B, false, dl, nt, false, tmp, ca == cb);
-                scatter2Kernel<<<num_sms_ * 8, 256, 0, stream_>>>(tmp, dl, nt, A.info, B.info, 0, sa, sb, na, out_dev);
+                DevPtr<double> tmp(devAlloc<double>((size_t)nt * sa * sb));
+                runStore(A, false, B, false, dl.get(), nt, false, tmp.get(), ca == cb);
+                scatter2Kernel<<<num_sms_ * 8, 256, 0, stream_>>>(tmp.get(), dl.get(), nt, A.info, B.info, 0, sa, sb, na,
+                                                                   out_dev);
                 cudaCheck(cudaGetLastError(), "scatter2");
                 cudaCheck(cudaStreamSynchronize(stream_), "eri2");
-                cudaFree(tmp);
-                cudaFree(dl);
             }
     }
 
@@ -1080,10 +1077,9 @@ namespace lible_b200
             if (pairs_host[2 * i] >= B.n_pairs || pairs_host[2 * i + 1] >= K.n_pairs)
                 throw EngineError(kStatusInvalid, "pair index out of range");
         std::vector<uint32_t> list(pairs_host, pairs_host + 2 * n);
-        uint32_t *dl = devUpload(list, stream_);
-        runStore(B, cs.swapped[cab], K, cs.swapped[ccd], dl, n, d1, out_dev, use_symm && cab == ccd);
+        DevPtr<uint32_t> dl(devUpload(list, stream_));
+        runStore(B, cs.swapped[cab], K, cs.swapped[ccd], dl.get(), n, d1, out_dev, use_symm && cab == ccd);
         cudaCheck(cudaStreamSynchronize(stream_), "batch");
-        cudaFree(dl);
     }
 
     void Engine::eri3Batch(bool use_symm, int cab, int cx, long long n, const uint32_t *idx_host, double *out_dev,
@@ -1099,10 +1095,9 @@ namespace lible_b200
             if (idx_host[2 * i] >= B.n_pairs || idx_host[2 * i + 1] >= X.n_pairs)
                 throw EngineError(kStatusInvalid, "index out of range");
         std::vector<uint32_t> list(idx_host, idx_host + 2 * n);
-        uint32_t *dl = devUpload(list, stream_);
-        runStore(B, cs.swapped[cab], X, false, dl, n, d1, out_dev, false);
+        DevPtr<uint32_t> dl(devUpload(list, stream_));
+        runStore(B, cs.swapped[cab], X, false, dl.get(), n, d1, out_dev, false);
         cudaCheck(cudaStreamSynchronize(stream_), "batch");
-        cudaFree(dl);
     }
 
     void Engine::eri2Batch(int ca, int cb, long long n, const uint32_t *idx_host, double *out_dev, bool d1)
@@ -1116,10 +1111,9 @@ namespace lible_b200
             if (idx_host[2 * i] >= A.n_pairs || idx_host[2 * i + 1] >= B.n_pairs)
                 throw EngineError(kStatusInvalid, "index out of range");
         std::vector<uint32_t> list(idx_host, idx_host + 2 * n);
-        uint32_t *dl = devUpload(list, stream_);
-        runStore(A, false, B, false, dl, n, d1, out_dev, false);
+        DevPtr<uint32_t> dl(devUpload(list, stream_));
+        runStore(A, false, B, false, dl.get(), n, d1, out_dev, false);
         cudaCheck(cudaStreamSynchronize(stream_), "batch");
-        cudaFree(dl);
     }
 
     // ------------------------------------------------------------------------------------------

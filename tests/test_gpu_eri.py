@@ -162,6 +162,31 @@ def test_eri4d1_class_batches_elementwise_f_shells():
             assert np.abs(got - want).max() <= 1e-11, (a.getLPair(), c.getLPair())
 
 
+def test_kernel_batches_empty_and_out_of_range():
+    # an empty batch returns an empty block; pair and shell indices are checked on the host before
+    # anything reaches the device, and the context stays usable after the error
+    s = L.Structure("def2-svp", [8, 1, 1], H2O_ANG, "def2-universal-jkfit")
+    r = R.RefStructure("def2-svp", [8, 1, 1], H2O_ANG, units="angstrom")
+    sp = L.shellPairData(True, s)
+    aux = L.shellDataAux(s)
+    a, c, x = sp[1], sp[-1], aux[0]
+    assert L.ERI4Kernel(a, c).batch(np.zeros((0, 2))).shape == (0, 3, 1, 5, 5)
+    assert L.ERI4D1Kernel(a, c).batch(np.zeros((0, 2))).shape == (0, 12, 3, 1, 5, 5)
+    assert L.ERI3Kernel(a, x).batch(np.zeros((0, 2))).shape == (0, 3, 1, 1)
+    bad = [(L.ERI4Kernel(a, c), [[a.n_pairs_, 0]]), (L.ERI4Kernel(a, c), [[0, c.n_pairs_]]),
+           (L.ERI4D1Kernel(a, c), [[0, c.n_pairs_]]), (L.ERI3Kernel(a, x), [[0, x.n_shells_]]),
+           (L.ERI3D1Kernel(a, x), [[a.n_pairs_, 0]]), (L.ERI2Kernel(x, x), [[x.n_shells_, 0]]),
+           (L.ERI2D1Kernel(x, x), [[0, x.n_shells_]])]
+    for k, idx in bad:
+        with pytest.raises(L.LibleGpuError) as e:
+            k.batch(idx)
+        assert e.value.code == 1, type(k).__name__
+    idx = [(i, j) for i in range(a.n_pairs_) for j in range(c.n_pairs_)]
+    got = L.ERI4Kernel(a, c).batch(idx).reshape(a.n_pairs_, c.n_pairs_, -1)
+    want = r.eri4_class(True, a.index, c.index).reshape(a.n_pairs_, c.n_pairs_, -1)
+    assert np.abs(got - want).max() <= 1e-12
+
+
 def test_deploy_eri3_eri2_golden():
     s = L.Structure("def2-svp", [8, 8, 8], O3_ANG, "def2-universal-jkfit")
     sp = L.shellPairData(False, s)
