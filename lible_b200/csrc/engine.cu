@@ -826,6 +826,7 @@ namespace lible_b200
         if (swap)
             a.flags = (ket_swapped ? 1 : 0) | (bra_swapped ? 2 : 0) | 4;
         uint32_t *list = const_cast<uint32_t *>(d_list);
+        DevPtr<uint32_t> swapped_list;
         if (swap)
         {
             // swap the (bra, ket) columns of the task list
@@ -834,7 +835,8 @@ namespace lible_b200
             cudaCheck(cudaStreamSynchronize(stream_), "list");
             for (long long i = 0; i < n; i++)
                 std::swap(h[2 * i], h[2 * i + 1]);
-            list = devUpload(h, stream_);
+            swapped_list.reset(devUpload(h, stream_));
+            list = swapped_list.get();
         }
         a.list = list;
         if (!d1)
@@ -849,9 +851,9 @@ namespace lible_b200
         else
         {
             const long long blk = (long long)nsph(bra.la) * nsph(bra.lb) * nsph(ket.la) * nsph(ket.lb);
-            double *tmp = devAlloc<double>(n * 12 * blk);
+            DevPtr<double> tmp(devAlloc<double>(n * 12 * blk));
             a.mode = kD1Store;
-            a.out = tmp;
+            a.out = tmp.get();
             const int flags = a.flags;
             a.flags = 0;
             LaunchFn fn = lookupD1(swap ? tk : tb, swap ? tb : tk);
@@ -886,16 +888,12 @@ namespace lible_b200
             const auto &sb = swap ? ket : bra;
             const auto &sk = swap ? bra : ket;
             reorderD1Kernel<<<std::max(1, num_sms_ * 8), 256, 0, stream_>>>(
-                tmp, n, nsph(sb.la), nsph(sb.lb), nsph(sk.la), nsph(sk.lb), flags, slot, nb, d_out);
+                tmp.get(), n, nsph(sb.la), nsph(sb.lb), nsph(sk.la), nsph(sk.lb), flags, slot, nb, d_out);
             cudaCheck(cudaGetLastError(), "reorder");
             cudaCheck(cudaStreamSynchronize(stream_), "reorder");
-            cudaFree(tmp);
         }
         if (swap)
-        {
             cudaCheck(cudaStreamSynchronize(stream_), "store");
-            cudaFree(list);
-        }
     }
 
     // ------------------------------------------------------------------------------------------
