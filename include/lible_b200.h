@@ -15,8 +15,11 @@
  * caller passes Angstrom, converted with 1/0.5291772083 (src/lible/ints/defs.hpp:9-12); AO order is
  * atom -> shell (basis-file order) -> m = 0, +1, -1, +2, -2, ...
  *
- * Threading: a context owns one CUDA stream; calls on one context must be serialised by the caller.
- * Different contexts may be used from different threads.
+ * Threading: a context owns one CUDA stream.  Calls on one context may come from several threads
+ * (the reference calls its kernel functors concurrently from OpenMP threads, src/lible/ints/twoel/
+ * eri4.cpp:55-63): each call holds the context's lock, so they run one after another.  Different
+ * contexts run independently.  lible_gpu_last_error reports the calling thread's last failure on
+ * the context.
  */
 #ifndef LIBLE_B200_H
 #define LIBLE_B200_H

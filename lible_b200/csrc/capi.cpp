@@ -12,6 +12,7 @@
 #include <cstring>
 #include <memory>
 #include <map>
+#include <mutex>
 #include <string>
 
 using namespace lible_b200;
@@ -25,7 +26,8 @@ namespace lible_b200
 struct lible_gpu_ctx
 {
     std::unique_ptr<Engine> eng;
-    std::string err;
+    // serialises the calls on this context (every entry point that touches it holds the lock)
+    std::recursive_mutex mu;
     // last RI-J metric solve: 0 Cholesky, 1 eigendecomposition with cutoff; eigenvalue range (or
     // the squared range of the Cholesky diagonal, a lower bound of the condition number); dropped
     int rij_method = -1;
@@ -63,10 +65,14 @@ struct lible_gpu_ctx
 
 namespace
 {
+    // The calling thread's last error message per context: a call that succeeds on another thread
+    // in the meantime does not clear it.
+    thread_local std::map<const lible_gpu_ctx *, std::string> t_errors;
+
     int fail(lible_gpu_ctx *ctx, int code, const std::string &msg)
     {
         if (ctx)
-            ctx->err = msg;
+            t_errors[ctx] = msg;
         return code;
     }
 
@@ -75,11 +81,12 @@ namespace
     {
         if (!ctx || !ctx->eng)
             return LIBLE_GPU_EINVAL;
+        std::lock_guard<std::recursive_mutex> lock(ctx->mu);
         try
         {
             cudaSetDevice(ctx->eng->device());
             f(*ctx->eng);
-            ctx->err.clear();
+            t_errors.erase(ctx);
             return LIBLE_GPU_OK;
         }
         catch (const EngineError &e)
@@ -309,13 +316,17 @@ int lible_gpu_create(int device, lible_gpu_ctx **ctx)
 
 int lible_gpu_destroy(lible_gpu_ctx *ctx)
 {
+    t_errors.erase(ctx);
     delete ctx;
     return LIBLE_GPU_OK;
 }
 
 const char *lible_gpu_last_error(const lible_gpu_ctx *ctx)
 {
-    return ctx ? ctx->err.c_str() : "null context";
+    if (!ctx)
+        return "null context";
+    const auto it = t_errors.find(ctx);
+    return it == t_errors.end() ? "" : it->second.c_str();
 }
 
 int lible_gpu_set_structure_named(lible_gpu_ctx *ctx, const char *basis_root, const char *basis,
@@ -865,6 +876,7 @@ int lible_gpu_rij_last_solve(lible_gpu_ctx *ctx, int *method, double *lo, double
 {
     if (!ctx)
         return LIBLE_GPU_EINVAL;
+    std::lock_guard<std::recursive_mutex> lock(ctx->mu);
     if (shift)
         *shift = ctx->rij_shift;
     if (method)

@@ -187,6 +187,45 @@ def test_kernel_batches_empty_and_out_of_range():
     assert np.abs(got - want).max() <= 1e-12
 
 
+def test_concurrent_calls_on_one_context():
+    # the reference's drivers call one kernel functor from many OpenMP threads; here four threads
+    # share one context, one of them also making failing calls whose messages must stay its own
+    import threading
+
+    s = L.Structure("def2-svp", [8, 1, 1], H2O_ANG)
+    sp = L.shellPairData(True, s)
+    jobs = [(a, c) for a in sp for c in sp]
+
+    def run(a, c):
+        idx = [(i, j) for i in range(a.n_pairs_) for j in range(c.n_pairs_)]
+        return L.ERI4Kernel(a, c).batch(idx)
+
+    serial = {(a.index, c.index): run(a, c) for a, c in jobs}
+    got, errors, messages = {}, [], []
+
+    def work(part, failing):
+        try:
+            for _ in range(3):
+                for a, c in part:
+                    got[(a.index, c.index)] = run(a, c)
+                    if failing:
+                        with pytest.raises(L.LibleGpuError) as e:
+                            L.ERI4Kernel(a, c).batch([[a.n_pairs_, 0]])
+                        messages.append(str(e.value))
+        except Exception as e:  # reported below
+            errors.append(e)
+
+    threads = [threading.Thread(target=work, args=(jobs[i::4], i == 0)) for i in range(4)]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    assert not errors, errors
+    assert messages and all("out of range" in m for m in messages)
+    for k, v in serial.items():
+        assert np.array_equal(got[k], v), k
+
+
 def test_deploy_eri3_eri2_golden():
     s = L.Structure("def2-svp", [8, 8, 8], O3_ANG, "def2-universal-jkfit")
     sp = L.shellPairData(False, s)
