@@ -208,6 +208,12 @@ int lible_gpu_stream(lible_gpu_ctx *ctx, void **stream);
  * (mma.sync m8n8k4 f64) loop; the roofline denominators of the engine's kernels. */
 int lible_gpu_fp64_peak(lible_gpu_ctx *ctx, double *dfma_tflops, double *dmma_tflops);
 
+/* Diagnostic of the failure path of the kernels' bounded waits: one wait on a barrier that nothing
+ * completes gives up after `polls` polls (1 .. 2^20) and the call returns LIBLE_GPU_ETIMEOUT, the
+ * status a stalled bulk copy produces.  No copy is in flight and the context stays usable.  It has
+ * no counterpart in the reference, whose CPU code has no device waits. */
+int lible_gpu_check_bounded_wait(lible_gpu_ctx *ctx, int polls);
+
 /* ---- J/K energy and its nuclear gradient (forward / backward pair) ----------------------------
  * forward:  E = 1/2 Tr(D J) - 1/4 Tr(D K)  (J, K from lible_gpu_jk with opts; J/K may be NULL).
  * backward: grad[3*atom + x] = dE/dR_{atom,x}, contracting the first-derivative integrals

@@ -829,6 +829,11 @@ int lible_gpu_fp64_peak(lible_gpu_ctx *ctx, double *dfma, double *dmma)
     });
 }
 
+int lible_gpu_check_bounded_wait(lible_gpu_ctx *ctx, int polls)
+{
+    return guard(ctx, [&](Engine &e) { e.checkBoundedWait(polls); });
+}
+
 int lible_gpu_jk_energy_forward(lible_gpu_ctx *ctx, const double *D, const lible_gpu_jk_opts *opts, double *energy,
                                 double *J, double *K)
 {

@@ -2269,7 +2269,34 @@ namespace lible_b200
         cudaCheck(cudaMemcpyAsync(&st, d_status_, sizeof(int), cudaMemcpyDeviceToHost, stream_), "status");
         cudaCheck(cudaStreamSynchronize(stream_), "status");
         if (st != 0)
+        {
+            cudaCheck(cudaMemsetAsync(d_status_, 0, sizeof(int), stream_), "memset");
+            cudaCheck(cudaStreamSynchronize(stream_), "status");
             throw EngineError(kStatusTimeout, "a bounded device wait gave up (bulk copy did not complete)");
+        }
+    }
+
+    // One thread waits on a freshly initialised shared-memory barrier that expects one arrival
+    // and gets none: the wait runs out after `polls` polls and records the timeout status, exactly
+    // as a stalled bulk copy would.  Nothing is in flight when the block exits.
+    __global__ void boundedWaitKernel(int *status, int polls)
+    {
+        __shared__ __align__(8) uint64_t mbar;
+        if (threadIdx.x == 0)
+        {
+            mbarInit(&mbar);
+            mbarWait(&mbar, 0, status, polls);
+        }
+    }
+
+    void Engine::checkBoundedWait(int polls)
+    {
+        if (polls < 1 || polls > (1 << 20))
+            throw EngineError(kStatusInvalid, "polls must be in [1, 2^20]");
+        cudaCheck(cudaMemsetAsync(d_status_, 0, sizeof(int), stream_), "memset");
+        boundedWaitKernel<<<1, 32, 0, stream_>>>(d_status_, polls);
+        cudaCheck(cudaGetLastError(), "boundedWaitKernel");
+        checkStatus();
     }
 
     double *Engine::staging(int slot, size_t n)

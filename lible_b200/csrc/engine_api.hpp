@@ -193,8 +193,12 @@ namespace lible_b200
         std::vector<double> nucleiCharges() const;
 
         void sync();
-        // Throws kStatusTimeout when a kernel reported a bounded wait that gave up (synchronises).
+        // Throws kStatusTimeout when a kernel reported a bounded wait that gave up (synchronises);
+        // the status word is cleared first, so the context stays usable.
         void checkStatus();
+        // Runs one bounded wait that cannot complete (a barrier that nothing arrives on, no copy in
+        // flight) with `polls` polls, then checkStatus(): exercises the give-up path end to end.
+        void checkBoundedWait(int polls);
         // Cached device staging buffer `slot` (0..3) of at least n doubles (grow-only).
         double *staging(int slot, size_t n);
 

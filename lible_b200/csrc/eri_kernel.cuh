@@ -136,12 +136,12 @@ namespace lible_b200
                      : "memory");
     }
 
-    // Waits for the barrier phase with parity `phase`; gives up after a bounded number of polls,
-    // records kStatusTimeout-style failure in *status and returns false.
-    __device__ __forceinline__ bool mbarWait(uint64_t *mbar, unsigned phase, int *status)
+    // Waits for the barrier phase with parity `phase`; gives up after `polls` polls, records
+    // kStatusTimeout-style failure in *status and returns false.
+    __device__ __forceinline__ bool mbarWait(uint64_t *mbar, unsigned phase, int *status, int polls = 1 << 20)
     {
         const unsigned m = (unsigned)__cvta_generic_to_shared(mbar);
-        for (int it = 0; it < (1 << 20); it++)
+        for (int it = 0; it < polls; it++)
         {
             unsigned done;
             asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"

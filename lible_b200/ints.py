@@ -633,6 +633,12 @@ def fp64_peak(structure):
     return a.value, b.value
 
 
+def check_bounded_wait(structure, polls=4096):
+    """Runs one device wait that cannot complete and lets it give up after `polls` polls: raises
+    LibleGpuError with code 6 (ETIMEOUT), the error a stalled bulk copy produces."""
+    _call(structure, "lible_gpu_check_bounded_wait", int(polls))
+
+
 def jk_plan_classes(structure, schwarz=1e-12, precision="fp64", fp32_threshold=1e-4):
     """Per class pair of the J/K plan (launch order): (la, lb, lc, ld), n_fp64, n_fp32, primitive
     quartets, algorithmic FLOPs."""

@@ -226,6 +226,25 @@ def test_concurrent_calls_on_one_context():
         assert np.array_equal(got[k], v), k
 
 
+def test_bounded_wait_gives_up_and_context_survives():
+    # a wait that nothing completes runs out of polls: ETIMEOUT on the host, and the same context
+    # still builds the same J/K afterwards
+    Z, xyz, rng = water_cluster(2, seed=7)
+    s = L.Structure("cc-pvdz", Z, xyz, units="bohr")
+    D = random_density(s.nao, 10, rng)
+    J0, K0, _ = L.jk(s, D, schwarz=0.0)
+    for polls in (1, 4096):
+        with pytest.raises(L.LibleGpuError) as e:
+            L.check_bounded_wait(s, polls)
+        assert e.value.code == 6
+    with pytest.raises(L.LibleGpuError) as e:
+        L.check_bounded_wait(s, 0)
+    assert e.value.code == 1
+    J1, K1, _ = L.jk(s, D, schwarz=0.0)
+    assert np.abs(J1 - J0).max() <= 1e-12
+    assert np.abs(K1 - K0).max() <= 1e-12
+
+
 def test_deploy_eri3_eri2_golden():
     s = L.Structure("def2-svp", [8, 8, 8], O3_ANG, "def2-universal-jkfit")
     sp = L.shellPairData(False, s)
