@@ -1,11 +1,13 @@
 """Runs direct J/K builds of a seeded water cluster and prints the screening plan and timings.
 
     python -m lible_b200.jk_run --waters 8 --basis cc-pvdz --precision fp64 --repeat 2
+    python -m lible_b200.jk_run --waters 2 --basis cc-pvtz --gradient --repeat 2
 
 The cluster and density follow lible_b200.workloads (5.7 bohr lattice, random rotations, +-0.6 bohr
 jitter, D = C C^T with occupation 5 per water unless --occ is given).  Every build is a separate
 lible_gpu_jk call on the structure's stream; the first one also builds the Schwarz factors and the
-screening plan.  Small cases of this command are what kernel profiles are taken on.
+screening plan.  --gradient runs the J/K energy gradient (lible_gpu_jk_energy_backward) instead.
+Small cases of this command are what kernel profiles are taken on.
 """
 import argparse
 import json
@@ -23,6 +25,7 @@ def main(argv=None):
     ap.add_argument("--occ", type=int, default=None)
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--repeat", type=int, default=2)
+    ap.add_argument("--gradient", action="store_true")
     args = ap.parse_args(argv)
 
     import torch
@@ -39,12 +42,15 @@ def main(argv=None):
     for _ in range(args.repeat):
         torch.cuda.synchronize()
         t = time.perf_counter()
-        L.jk(s, Dd, args.schwarz, args.precision, args.fp32_threshold, J=J, K=K)
+        if args.gradient:
+            L.jk_energy_backward(s, D, args.schwarz)
+        else:
+            L.jk(s, Dd, args.schwarz, args.precision, args.fp32_threshold, J=J, K=K)
         torch.cuda.synchronize()
         times.append(time.perf_counter() - t)
     plan = L.jk_plan(s, args.schwarz, args.precision, args.fp32_threshold)
     print(json.dumps({"waters": args.waters, "basis": args.basis, "nao": s.nao, "precision": args.precision,
-                      "plan": plan, "wall_s": times}))
+                      "gradient": args.gradient, "plan": plan, "wall_s": times}))
     return 0
 
 
