@@ -109,7 +109,13 @@ namespace lible_b200
         double *grad;                     // [n_atoms][3]
         int n_atoms;                      // gradient launches: rows of grad
         int *status;                      // error word (non-zero = failure)
+        // failure-path check of the bulk-copy waits: > 0 = issue no copy and give up after this many
+        // polls (the wait then fails exactly as a stalled copy's would); 0 = normal operation
+        int wait_inject;
     };
+
+    // Poll limit of the kernels' barrier waits on bulk copies.
+    constexpr int kWaitPolls = 1 << 20;
 
     // Primitive-pair record as stored in DevPairClass::pP: [p, Px, Py, Pz, 1/p, a, b, 0].
     // x = p, (y, z, w) = P, ip = 1/p.

@@ -810,6 +810,8 @@ namespace lible_b200
     void Engine::runStore(const DevPairClass &bra, bool bra_swapped, const DevPairClass &ket, bool ket_swapped,
                           const uint32_t *d_list, long long n, bool d1, double *d_out, bool same_class)
     {
+        const int inject = wait_inject_;
+        wait_inject_ = 0;
         if (n == 0)
             return;
         const int tb = pairType(bra.la, bra.lb), tk = pairType(ket.la, ket.lb);
@@ -820,6 +822,9 @@ namespace lible_b200
         a.ket_EtP = (swap ? bra : ket).EtP;
         a.boys = boys_;
         a.boys_f = boys_f_;
+        a.status = d_status_;
+        a.wait_inject = inject;
+        cudaCheck(cudaMemsetAsync(d_status_, 0, sizeof(int), stream_), "memset");
         a.n_tasks = n;
         a.same_class = same_class ? 1 : 0;
         a.flags = (bra_swapped ? 1 : 0) | (ket_swapped ? 2 : 0) | (swap ? 4 : 0);
@@ -892,8 +897,9 @@ namespace lible_b200
             cudaCheck(cudaGetLastError(), "reorder");
             cudaCheck(cudaStreamSynchronize(stream_), "reorder");
         }
-        if (swap)
-            cudaCheck(cudaStreamSynchronize(stream_), "store");
+        // a bounded wait that gave up makes the call fail (synchronises, so the swapped list stays
+        // alive until the kernel is done)
+        checkStatus();
     }
 
     // ------------------------------------------------------------------------------------------
@@ -2287,6 +2293,13 @@ namespace lible_b200
             mbarInit(&mbar);
             mbarWait(&mbar, 0, status, polls);
         }
+    }
+
+    void Engine::injectWaitTimeout(int polls)
+    {
+        if (polls < 0 || polls > kWaitPolls)
+            throw EngineError(kStatusInvalid, "polls must be in [0, 2^20]");
+        wait_inject_ = polls;
     }
 
     void Engine::checkBoundedWait(int polls)

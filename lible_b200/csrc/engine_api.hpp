@@ -199,6 +199,13 @@ namespace lible_b200
         // Runs one bounded wait that cannot complete (a barrier that nothing arrives on, no copy in
         // flight) with `polls` polls, then checkStatus(): exercises the give-up path end to end.
         void checkBoundedWait(int polls);
+        // The next kernel-API store call (eri4/eri3/eri2 batches, their no-allocation form) runs its
+        // bulk-copy classes without issuing the copies, so their waits give up after `polls` polls
+        // (1 .. 2^20) and the call returns kStatusTimeout; one call only, 0 cancels.
+        void injectWaitTimeout(int polls);
+        // Evaluates the device special functions for tests: which 0 = e^{-x} (out[i]), 1 = FP64 Boys
+        // F_0..F_order (out[i * (order + 1) + k]), 2 = the FP32 Boys form; x in [0, 700] resp. x >= 0.
+        void evalSpecial(int which, int order, long long n, const double *x_dev, double *out_dev);
         // Cached device staging buffer `slot` (0..3) of at least n doubles (grow-only).
         double *staging(int slot, size_t n);
 
@@ -306,6 +313,7 @@ namespace lible_b200
         std::vector<void *> persistent_;
 
         int *d_status_ = nullptr;
+        int wait_inject_ = 0;  // see injectWaitTimeout
         double *staging_[4] = {};
         size_t staging_n_[4] = {};
         static constexpr int kBranches = 4;

@@ -138,7 +138,7 @@ namespace lible_b200
 
     // Waits for the barrier phase with parity `phase`; gives up after `polls` polls, records
     // kStatusTimeout-style failure in *status and returns false.
-    __device__ __forceinline__ bool mbarWait(uint64_t *mbar, unsigned phase, int *status, int polls = 1 << 20)
+    __device__ __forceinline__ bool mbarWait(uint64_t *mbar, unsigned phase, int *status, int polls = kWaitPolls)
     {
         const unsigned m = (unsigned)__cvta_generic_to_shared(mbar);
         for (int it = 0; it < polls; it++)
@@ -747,8 +747,10 @@ namespace lible_b200
     // operand tiles are zeroed once per block and never written afterwards.
     // `phase` is the parity of the block's mbarrier phase awaited next; it lives as long as the block
     // (one completed phase per ket primitive of every quartet), so it is carried across calls.
+    // Returns false when a bounded wait on a ket tile gave up (status word set): the block has then
+    // let any copy still in flight land (again bounded) and must stop without using the batch.
     template <int LA, int LB, int LC, int LD>
-    __device__ __forceinline__ void quartetGroupMMA(const QuartetArgs &a, uint32_t ib, uint32_t ik,
+    __device__ __forceinline__ bool quartetGroupMMA(const QuartetArgs &a, uint32_t ib, uint32_t ik,
                                                     unsigned char *smem, double (&v)[Shape<LA, LB, LC, LD, double>::TPW2][2],
                                                     unsigned &phase)
     {
@@ -784,7 +786,7 @@ namespace lible_b200
                 acc[i][0] = acc[i][1] = 0.0;
             for (uint32_t q = q0; q < q1; q++)
             {
-                if (ket_tiles && tid == 0)
+                if (ket_tiles && tid == 0 && !a.wait_inject)
                     bulkLoad(ec, ket_tiles + (size_t)q * (S::ec_tile_bytes / 8), S::ec_tile_bytes, mbar);
                 const PQ4 Q = loadPQ(a.ket.pP, q);
                 const double rs = rsqrt(P.x + Q.x);
@@ -855,8 +857,16 @@ namespace lible_b200
                 }
                 if (ket_tiles)
                 {
-                    mbarWait(mbar, phase, a.status);
+                    const unsigned ph = phase;
+                    const bool ok = mbarWait(mbar, ph, a.status, a.wait_inject ? a.wait_inject : kWaitPolls);
                     phase ^= 1u;
+                    // the block agrees on the outcome; after a give-up no thread reads the tile
+                    if (__syncthreads_or(!ok))
+                    {
+                        if (tid == 0 && !a.wait_inject)
+                            mbarWait(mbar, ph, nullptr);  // a late copy lands before the block exits
+                        return false;
+                    }
                 }
                 else
                     for (int e = tid; e < C::HCD * C::SCD; e += G)
@@ -910,6 +920,7 @@ namespace lible_b200
             }
             groupSync(G);
         }
+        return true;
     }
 
     // Tables and zero padding of the DMMA layout (once per block).
@@ -1148,8 +1159,9 @@ namespace lible_b200
             double *vs = reinterpret_cast<double *>(smem + S::m_off_rx);
             const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, r8 = lane >> 2, k4 = lane & 3;
             unsigned phase = 0;  // parity of the block mbarrier's next phase
-            // one quartet at a time for the whole block, tasks [start, end) of a chunk
-            auto processRange = [&](long long start, long long end) {
+            // one quartet at a time for the whole block, tasks [start, end) of a chunk; false = a
+            // bounded wait gave up and the block stops
+            auto processRange = [&](long long start, long long end) -> bool {
             int cur = 0;
             for (long long t = start; t < end; t++)
             {
@@ -1158,7 +1170,8 @@ namespace lible_b200
                 if (!inWindow(a, ib, ik, 0, false))
                     continue;
                 double v[S::TPW2][2];
-                quartetGroupMMA<LA, LB, LC, LD>(a, ib, ik, smem, v, phase);
+                if (!quartetGroupMMA<LA, LB, LC, LD>(a, ib, ik, smem, v, phase))
+                    return false;
                 // element (m, c) of the batch held by this thread: tile rows / columns
 #pragma unroll
                 for (int i = 0; i < S::TPW2; i++)
@@ -1197,6 +1210,7 @@ namespace lible_b200
                 }
                 __syncthreads();
             }
+            return true;
             };
             if (a.chunks)
             {
@@ -1210,7 +1224,8 @@ namespace lible_b200
                     __syncthreads();
                     if (c >= (unsigned long long)a.n_chunks)
                         break;
-                    processRange((long long)__ldg(a.chunks + c), (long long)__ldg(a.chunks + c + 1));
+                    if (!processRange((long long)__ldg(a.chunks + c), (long long)__ldg(a.chunks + c + 1)))
+                        break;
                 }
             }
             else
@@ -1218,7 +1233,8 @@ namespace lible_b200
                 constexpr long long CHB = 8;
                 const long long n_chunks = (a.n_tasks + CHB - 1) / CHB;
                 for (long long chunk = blockIdx.x; chunk < n_chunks; chunk += gridDim.x)
-                    processRange(chunk * CHB, (chunk + 1) * CHB < a.n_tasks ? (chunk + 1) * CHB : a.n_tasks);
+                    if (!processRange(chunk * CHB, (chunk + 1) * CHB < a.n_tasks ? (chunk + 1) * CHB : a.n_tasks))
+                        break;
             }
         }
         else

@@ -15,7 +15,7 @@
 #include "engine_api.hpp"
 #include "eri_launch.cuh"
 
-#include <mutex>
+#include <vector>
 
 namespace lible_b200
 {
@@ -25,29 +25,24 @@ namespace lible_b200
     // comes from cudaGetSymbolAddress below.
     static __device__ __align__(256) uint32_t g_pair_list_scratch[2 * kNoAllocMaxPairs];
 
-    // Device address of the buffer on `device` (which must be current), looked up once per device.
-    static uint32_t *scratchAddress(int device)
+    // Device address of the buffer on the current device.  It is looked up on every call (a cheap
+    // host call) rather than cached, so a new primary context, which may load the module at another
+    // address, is always seen.
+    static uint32_t *scratchAddress()
     {
-        static std::mutex mu;
-        static uint32_t *addr[256] = {};
-        if (device < 0 || device >= 256)
-            throw EngineError(kStatusInvalid, "device ordinal out of range");
-        std::lock_guard<std::mutex> lock(mu);
-        if (!addr[device])
-        {
-            void *p = nullptr;
-            const cudaError_t e = cudaGetSymbolAddress(&p, g_pair_list_scratch);
-            if (e != cudaSuccess)
-                throw EngineError(kStatusCuda, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
-            addr[device] = static_cast<uint32_t *>(p);
-        }
-        return addr[device];
+        void *p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_pair_list_scratch);
+        if (e != cudaSuccess)
+            throw EngineError(kStatusCuda, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+        return static_cast<uint32_t *>(p);
     }
 
     void Engine::eri4BatchNoAlloc(bool use_symm, int cab, int ccd, long long n, const uint32_t *pairs_host,
                                   double *out_dev, uint32_t *scratch, long long max_pairs)
     {
-        requireStructure();
+        const int inject = wait_inject_;
+        wait_inject_ = 0;
+        requireSingle();
         if (n < 0 || n > max_pairs)
             throw EngineError(kStatusInvalid, "eri4 batch without allocation: n = " + std::to_string(n) +
                                                   " exceeds the maximum of " + std::to_string(max_pairs) + " pairs");
@@ -67,15 +62,23 @@ namespace lible_b200
         // while staging when the caller's orientation is the other one
         const int tb = pairType(bra.la, bra.lb), tk = pairType(ket.la, ket.lb);
         const bool swap = tb < tk;
-        const size_t w = sizeof(uint32_t), pitch = 2 * sizeof(uint32_t);
         if (!swap)
-            cudaCheck(cudaMemcpyAsync(scratch, pairs_host, (size_t)n * pitch, cudaMemcpyHostToDevice, stream_), "stage");
+            cudaCheck(cudaMemcpyAsync(scratch, pairs_host, (size_t)n * 2 * sizeof(uint32_t), cudaMemcpyHostToDevice,
+                                      stream_),
+                      "stage");
         else
         {
-            cudaCheck(cudaMemcpy2DAsync(scratch, pitch, pairs_host + 1, pitch, w, (size_t)n, cudaMemcpyHostToDevice,
-                                        stream_), "stage");
-            cudaCheck(cudaMemcpy2DAsync(scratch + 1, pitch, pairs_host, pitch, w, (size_t)n, cudaMemcpyHostToDevice,
-                                        stream_), "stage");
+            // swapped columns in host memory (the no-allocation rule is about device memory), staged
+            // with one contiguous copy
+            std::vector<uint32_t> h(2 * (size_t)n);
+            for (long long i = 0; i < n; i++)
+            {
+                h[2 * i] = pairs_host[2 * i + 1];
+                h[2 * i + 1] = pairs_host[2 * i];
+            }
+            cudaCheck(cudaMemcpyAsync(scratch, h.data(), h.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, stream_),
+                      "stage");
+            cudaCheck(cudaStreamSynchronize(stream_), "stage");
         }
         const bool bs = cs.swapped[cab], ks = cs.swapped[ccd];
         QuartetArgs a{};
@@ -84,6 +87,9 @@ namespace lible_b200
         a.ket_EtP = (swap ? bra : ket).EtP;
         a.boys = boys_;
         a.boys_f = boys_f_;
+        a.status = d_status_;  // allocated with the context: a bounded wait that gives up is reported
+        a.wait_inject = inject;
+        cudaCheck(cudaMemsetAsync(d_status_, 0, sizeof(int), stream_), "memset");
         a.list = scratch;
         a.n_tasks = n;
         a.same_class = (use_symm && cab == ccd) ? 1 : 0;
@@ -94,12 +100,12 @@ namespace lible_b200
         if (!fn)
             throw EngineError(kStatusUnsupported, "quartet class not instantiated");
         cudaCheck(fn(a, stream_, num_sms_), "eri kernel");
-        cudaCheck(cudaStreamSynchronize(stream_), "batch");
+        checkStatus();  // synchronises
     }
 
-    uint32_t *noAllocScratch(int device, long long *max_pairs)
+    uint32_t *noAllocScratch(long long *max_pairs)
     {
         *max_pairs = kNoAllocMaxPairs;
-        return scratchAddress(device);
+        return scratchAddress();
     }
 }
