@@ -100,10 +100,13 @@ int lible_gpu_eri4d1_batch(lible_gpu_ctx *ctx, int use_symm, int class_ab, int c
  * The pair list is staged in a fixed 8 MiB buffer inside the library's device image (held on every
  * GPU that loads the library until the process exits), so n may be at most 1048576 pairs; larger n
  * returns LIBLE_GPU_EINVAL.  pairs must be host memory, out device memory of the context's GPU.
- * The shell-pair classes must already be on the device: call lible_gpu_pair_classes(ctx, use_symm,
- * ...) once first.  The first call on a device also looks up the buffer's device address
- * (cudaGetSymbolAddress); make that first call before any stream capture.  All calls share the
- * buffer: calls whose GPU work overlaps (other streams or contexts on the same device) race. */
+ * The context must hold a single structure (a batch context returns LIBLE_GPU_EUNSUPPORTED), and
+ * its shell-pair classes must already be on the device: call lible_gpu_pair_classes(ctx, use_symm,
+ * ...) once first.  Every call looks up the buffer's device address (cudaGetSymbolAddress); the
+ * first call on a device may load the module, so make it before any stream capture.  A bounded
+ * device wait that gives up returns LIBLE_GPU_ETIMEOUT, as for lible_gpu_eri4_batch.  All calls
+ * share the buffer: calls whose GPU work overlaps (other streams or contexts on the same device)
+ * race. */
 int lible_gpu_eri4_batch_noalloc(lible_gpu_ctx *ctx, int use_symm, int class_ab, int class_cd, long long n,
                                  const unsigned *pairs, double *out);
 /* ERI3Kernel (eri_kernels.hpp:78-94): idx[2*i] = ipair_ab, idx[2*i+1] = ishell_c; out[i] = [Sa][Sb][Sc]. */
@@ -207,12 +210,28 @@ int lible_gpu_stream(lible_gpu_ctx *ctx, void **stream);
 /* Measured FP64 throughput of this GPU (TFLOP/s): a register-resident DFMA loop and a DMMA
  * (mma.sync m8n8k4 f64) loop; the roofline denominators of the engine's kernels. */
 int lible_gpu_fp64_peak(lible_gpu_ctx *ctx, double *dfma_tflops, double *dmma_tflops);
+/* Measured FP32 throughput (TFLOP/s): a scalar FFMA loop and a packed fma.rn.f32x2 loop; the
+ * roofline denominators of the FP32 quartet kernels. */
+int lible_gpu_fp32_peak(lible_gpu_ctx *ctx, double *ffma_tflops, double *ffma2_tflops);
 
 /* Diagnostic of the failure path of the kernels' bounded waits: one wait on a barrier that nothing
  * completes gives up after `polls` polls (1 .. 2^20) and the call returns LIBLE_GPU_ETIMEOUT, the
  * status a stalled bulk copy produces.  No copy is in flight and the context stays usable.  It has
  * no counterpart in the reference, whose CPU code has no device waits. */
 int lible_gpu_check_bounded_wait(lible_gpu_ctx *ctx, int polls);
+
+/* The same failure path in the real class kernels: the next kernel-API store launch on the context
+ * (lible_gpu_eri4_batch, lible_gpu_eri4_batch_noalloc, ...) runs its bulk-copy (DMMA) classes
+ * without issuing the ket-tile copies, so their first wait gives up after `polls` polls (1 .. 2^20);
+ * the block stops without using the tile and the call returns LIBLE_GPU_ETIMEOUT.  Applies to one
+ * launch; 0 cancels.  No copy is in flight and the context stays usable.  No reference counterpart. */
+int lible_gpu_inject_wait_timeout(lible_gpu_ctx *ctx, int polls);
+
+/* The device special functions of the class kernels, evaluated directly (for their tests; no
+ * reference counterpart as a call, the reference's are BoysF2 / calcBoysF, boys_function.hpp:68-109):
+ * which = 0: out[i] = e^{-x[i]}, x in [0, 700]; which = 1: FP64 Boys F_0..F_order(x[i]) into
+ * out[i*(order+1) + k], order <= 14; which = 2: the FP32 Boys form used by FP32 quartets. */
+int lible_gpu_eval_special(lible_gpu_ctx *ctx, int which, int order, long long n, const double *x, double *out);
 
 /* ---- J/K energy and its nuclear gradient (forward / backward pair) ----------------------------
  * forward:  E = 1/2 Tr(D J) - 1/4 Tr(D K)  (J, K from lible_gpu_jk with opts; J/K may be NULL).

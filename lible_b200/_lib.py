@@ -79,7 +79,10 @@ SIGNATURES = {
     "lible_gpu_stream": [P, ctypes.POINTER(P)],
     "lible_gpu_jk_plan_classes": [P, ctypes.POINTER(JKOpts), P, P, P, P, P, P],
     "lible_gpu_fp64_peak": [P, ctypes.POINTER(D), ctypes.POINTER(D)],
+    "lible_gpu_fp32_peak": [P, ctypes.POINTER(D), ctypes.POINTER(D)],
     "lible_gpu_check_bounded_wait": [P, ctypes.c_int],
+    "lible_gpu_inject_wait_timeout": [P, ctypes.c_int],
+    "lible_gpu_eval_special": [P, ctypes.c_int, ctypes.c_int, LL, P, P],
     "lible_gpu_ri_contract": [P, P, P, D, P, P],
     "lible_gpu_rij_last_solve": [P, P, P, P, P, P],
     "lible_gpu_rik": [P, P, P, LL, D, P, ctypes.POINTER(RIKInfo)],

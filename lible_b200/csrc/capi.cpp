@@ -19,8 +19,10 @@ using namespace lible_b200;
 
 namespace lible_b200
 {
-    // noalloc.cu: device address of the allocation-free call's staging buffer on `device`.
-    uint32_t *noAllocScratch(int device, long long *max_pairs);
+    // noalloc.cu: device address of the allocation-free call's staging buffer on the current device.
+    uint32_t *noAllocScratch(long long *max_pairs);
+    // peak.cu: measured FP32 throughput {FFMA, packed FFMA2} in TFLOP/s.
+    std::pair<double, double> measureFp32Peak(int device, cudaStream_t s);
 }
 
 struct lible_gpu_ctx
@@ -518,7 +520,7 @@ int lible_gpu_eri4_batch_noalloc(lible_gpu_ctx *ctx, int use_symm, int class_ab,
         if (n < 0 || (n > 0 && (!pairs || !out)))
             throw EngineError(kStatusInvalid, "invalid batch arguments");
         long long max_pairs = 0;
-        uint32_t *scratch = noAllocScratch(e.device(), &max_pairs);
+        uint32_t *scratch = noAllocScratch(&max_pairs);
         if (n > max_pairs)
             throw EngineError(kStatusInvalid, "eri4 batch without allocation: n = " + std::to_string(n) +
                                                   " exceeds the maximum of " + std::to_string(max_pairs) + " pairs");
@@ -829,9 +831,38 @@ int lible_gpu_fp64_peak(lible_gpu_ctx *ctx, double *dfma, double *dmma)
     });
 }
 
+int lible_gpu_fp32_peak(lible_gpu_ctx *ctx, double *ffma, double *ffma2)
+{
+    return guard(ctx, [&](Engine &e) {
+        auto p = measureFp32Peak(e.device(), e.stream());
+        if (ffma)
+            *ffma = p.first;
+        if (ffma2)
+            *ffma2 = p.second;
+    });
+}
+
 int lible_gpu_check_bounded_wait(lible_gpu_ctx *ctx, int polls)
 {
     return guard(ctx, [&](Engine &e) { e.checkBoundedWait(polls); });
+}
+
+int lible_gpu_inject_wait_timeout(lible_gpu_ctx *ctx, int polls)
+{
+    return guard(ctx, [&](Engine &e) { e.injectWaitTimeout(polls); });
+}
+
+int lible_gpu_eval_special(lible_gpu_ctx *ctx, int which, int order, long long n, const double *x, double *out)
+{
+    return guard(ctx, [&](Engine &e) {
+        if (n < 0 || (n > 0 && (!x || !out)) || which < 0 || which > 2)
+            throw EngineError(kStatusInvalid, "invalid special-function arguments");
+        const size_t per = which == 0 ? 1 : (size_t)std::max(order, 0) + 1;
+        DevArray xi(const_cast<double *>(x), (size_t)n, true, e.stream());
+        DevArray o(out, (size_t)n * per, false, e.stream());
+        e.evalSpecial(which, order, n, xi.ptr, o.ptr);
+        o.copyOut();
+    });
 }
 
 int lible_gpu_jk_energy_forward(lible_gpu_ctx *ctx, const double *D, const lible_gpu_jk_opts *opts, double *energy,

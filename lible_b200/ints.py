@@ -633,10 +633,34 @@ def fp64_peak(structure):
     return a.value, b.value
 
 
+def fp32_peak(structure):
+    """Measured (scalar FFMA, packed FFMA2) FP32 TFLOP/s of the structure's GPU."""
+    a, b = ctypes.c_double(), ctypes.c_double()
+    _call(structure, "lible_gpu_fp32_peak", ctypes.byref(a), ctypes.byref(b))
+    return a.value, b.value
+
+
 def check_bounded_wait(structure, polls=4096):
     """Runs one device wait that cannot complete and lets it give up after `polls` polls: raises
     LibleGpuError with code 6 (ETIMEOUT), the error a stalled bulk copy produces."""
     _call(structure, "lible_gpu_check_bounded_wait", int(polls))
+
+
+def eval_special(structure, which, x, order=0):
+    """Device special functions for tests: which "exp" -> e^{-x}; "boys" / "boys32" -> F_0..F_order(x)
+    in FP64 / in the FP32 form of FP32 quartets (rows per x)."""
+    w = {"exp": 0, "boys": 1, "boys32": 2}[which]
+    x = _f64(x).ravel()
+    out = np.empty(len(x) if w == 0 else (len(x), order + 1))
+    _call(structure, "lible_gpu_eval_special", w, int(order), len(x), _ptr(x), _ptr(out))
+    return out
+
+
+def inject_wait_timeout(structure, polls=4096):
+    """Makes the next kernel-API store launch on the structure's context run its bulk-copy classes
+    without issuing the copies, so their waits give up after `polls` polls and that call raises
+    LibleGpuError with code 6 (ETIMEOUT); nothing is in flight and the context stays usable."""
+    _call(structure, "lible_gpu_inject_wait_timeout", int(polls))
 
 
 def jk_plan_classes(structure, schwarz=1e-12, precision="fp64", fp32_threshold=1e-4):

@@ -47,6 +47,7 @@ def lib():
         L.ref_pair_classes.argtypes = [P, ctypes.c_int, P, P, P, P]
         L.ref_aux_classes.argtypes = [P, P, P, P]
         L.ref_jk_grad.argtypes = [P, P, P]
+        L.ref_jk_grad_sample.argtypes = [P, P, P, ctypes.c_double, ctypes.c_int, P, P]
         L.ref_rij_gamma.argtypes = [P, P, P]
         L.ref_rij_j.argtypes = [P, P, P]
         L.ref_one_electron.argtypes = [P, ctypes.c_int, P, ctypes.c_int, P]
@@ -214,6 +215,16 @@ class RefStructure:
         g = np.empty((self.n_atoms, 3))
         self._chk(lib().ref_jk_grad(self.h, _p(D), _p(g)))
         return g
+
+    def jk_grad_sample(self, D, schwarz=1e-12, bra_stride=1):
+        """The gradient over the Schwarz-surviving quartets of every bra_stride-th bra pair (a timing
+        sample); returns (grad, quartets processed, seconds)."""
+        D = np.ascontiguousarray(D, dtype=np.float64)
+        g = np.empty((self.n_atoms, 3))
+        nq, sec = ctypes.c_longlong(), ctypes.c_double()
+        self._chk(lib().ref_jk_grad_sample(self.h, _p(D), _p(g), schwarz, bra_stride, ctypes.byref(nq),
+                                           ctypes.byref(sec)))
+        return g, nq.value, sec.value
 
     def rij_gamma(self, D):
         D = np.ascontiguousarray(D, dtype=np.float64)

@@ -723,65 +723,91 @@ int ref_jk(void *h, const double *D, double *J, double *K, double schwarz, int b
 // Gradient of E = 1/2 Tr(DJ) - 1/4 Tr(DK) with respect to the nuclear coordinates, from the
 // reference's ERI4D1Kernel batches over the unique quartets (no Schwarz screening, which keeps the
 // result exact for finite-difference checks).  grad is [n_atoms][3].
-int ref_jk_grad(void *h, const double *D, double *grad)
+// `schwarz` > 0 keeps a quartet iff Q_ab Q_cd >= schwarz (the screened backward pass of the
+// product keeps the same ones); `bra_stride` > 1 processes every bra_stride-th bra pair only, a
+// bounded sample for timing.  Returns the quartets processed and the wall time.
+static void jkGradImpl(void *h, const double *D, double *grad, double schwarz, int bra_stride, long long *n_quartets,
+                       double *seconds)
 {
-    return guarded([&]
-    {
-        auto &S = *static_cast<RefStructure *>(h)->s;
-        auto sp = lints::shellPairData(true, S);
-        const size_t n = S.getDimAO();
-        const size_t na_t = S.getNAtoms();
-        int nt = omp_get_max_threads();
-        std::vector<std::vector<double>> Gt(nt, std::vector<double>(3 * na_t, 0.0));
-        for (size_t cab = 0; cab < sp.size(); cab++)
-            for (size_t ccd = 0; ccd <= cab; ccd++)
+    auto &S = *static_cast<RefStructure *>(h)->s;
+    auto t0 = std::chrono::steady_clock::now();
+    auto sp = lints::shellPairData(true, S);
+    const size_t n = S.getDimAO();
+    const size_t na_t = S.getNAtoms();
+    std::vector<std::vector<double>> Q(sp.size());
+    if (schwarz > 0)
+        for (size_t c = 0; c < sp.size(); c++)
+            Q[c] = schwarzFactors(sp[c]);
+    const int stride = bra_stride > 0 ? bra_stride : 1;
+    int nt = omp_get_max_threads();
+    std::vector<std::vector<double>> Gt(nt, std::vector<double>(3 * na_t, 0.0));
+    long long nq = 0;
+    for (size_t cab = 0; cab < sp.size(); cab++)
+        for (size_t ccd = 0; ccd <= cab; ccd++)
+        {
+            const auto &ab = sp[cab];
+            const auto &cd = sp[ccd];
+            lints::ERI4D1Kernel kern(ab, cd);
+            const int na = lints::numSphericals(ab.la_), nb = lints::numSphericals(ab.lb_);
+            const int nc = lints::numSphericals(cd.la_), nd = lints::numSphericals(cd.lb_);
+            const bool same = cab == ccd;
+#pragma omp parallel for schedule(dynamic) reduction(+ : nq)
+            for (size_t i = 0; i < ab.n_pairs_; i += stride)
             {
-                const auto &ab = sp[cab];
-                const auto &cd = sp[ccd];
-                lints::ERI4D1Kernel kern(ab, cd);
-                const int na = lints::numSphericals(ab.la_), nb = lints::numSphericals(ab.lb_);
-                const int nc = lints::numSphericals(cd.la_), nd = lints::numSphericals(cd.lb_);
-                const bool same = cab == ccd;
-#pragma omp parallel for schedule(dynamic)
-                for (size_t i = 0; i < ab.n_pairs_; i++)
+                double *G = Gt[omp_get_thread_num()].data();
+                size_t bound = same ? i + 1 : cd.n_pairs_;
+                for (size_t j = 0; j < bound; j++)
                 {
-                    double *G = Gt[omp_get_thread_num()].data();
-                    size_t bound = same ? i + 1 : cd.n_pairs_;
-                    for (size_t j = 0; j < bound; j++)
-                    {
-                        auto blocks = kern(i, j, ab, cd);
-                        double f = quartetWeight(ab, i, cd, j, same);
-                        size_t oa = ab.offsets_sph_[2 * i], ob = ab.offsets_sph_[2 * i + 1];
-                        size_t oc = cd.offsets_sph_[2 * j], od = cd.offsets_sph_[2 * j + 1];
-                        size_t atoms[4] = {ab.atomic_idxs_[2 * i], ab.atomic_idxs_[2 * i + 1],
-                                           cd.atomic_idxs_[2 * j], cd.atomic_idxs_[2 * j + 1]};
-                        double acc[12] = {};
-                        for (int x = 0; x < na; x++)
-                            for (int y = 0; y < nb; y++)
-                                for (int z = 0; z < nc; z++)
-                                    for (int w = 0; w < nd; w++)
-                                    {
-                                        size_t m = oa + x, nu = ob + y, k = oc + z, t = od + w;
-                                        double gam = f * (4 * D[m * n + nu] * D[k * n + t] -
-                                                          D[m * n + k] * D[nu * n + t] -
-                                                          D[m * n + t] * D[nu * n + k]);
-                                        size_t e = ((x * nb + y) * nc + z) * nd + w;
-                                        for (int c = 0; c < 12; c++)
-                                            acc[c] += gam * blocks[c].memptr()[e];
-                                    }
-                        for (int c = 0; c < 12; c++)
-                            G[3 * atoms[c / 3] + c % 3] += acc[c];
-                    }
+                    if (schwarz > 0 && Q[cab][i] * Q[ccd][j] < schwarz)
+                        continue;
+                    nq++;
+                    auto blocks = kern(i, j, ab, cd);
+                    double f = quartetWeight(ab, i, cd, j, same);
+                    size_t oa = ab.offsets_sph_[2 * i], ob = ab.offsets_sph_[2 * i + 1];
+                    size_t oc = cd.offsets_sph_[2 * j], od = cd.offsets_sph_[2 * j + 1];
+                    size_t atoms[4] = {ab.atomic_idxs_[2 * i], ab.atomic_idxs_[2 * i + 1],
+                                       cd.atomic_idxs_[2 * j], cd.atomic_idxs_[2 * j + 1]};
+                    double acc[12] = {};
+                    for (int x = 0; x < na; x++)
+                        for (int y = 0; y < nb; y++)
+                            for (int z = 0; z < nc; z++)
+                                for (int w = 0; w < nd; w++)
+                                {
+                                    size_t m = oa + x, nu = ob + y, k = oc + z, t = od + w;
+                                    double gam = f * (4 * D[m * n + nu] * D[k * n + t] -
+                                                      D[m * n + k] * D[nu * n + t] -
+                                                      D[m * n + t] * D[nu * n + k]);
+                                    size_t e = ((x * nb + y) * nc + z) * nd + w;
+                                    for (int c = 0; c < 12; c++)
+                                        acc[c] += gam * blocks[c].memptr()[e];
+                                }
+                    for (int c = 0; c < 12; c++)
+                        G[3 * atoms[c / 3] + c % 3] += acc[c];
                 }
             }
-        for (size_t x = 0; x < 3 * na_t; x++)
-        {
-            double s = 0;
-            for (int t = 0; t < nt; t++)
-                s += Gt[t][x];
-            grad[x] = s;
         }
-    });
+    for (size_t x = 0; x < 3 * na_t; x++)
+    {
+        double s = 0;
+        for (int t = 0; t < nt; t++)
+            s += Gt[t][x];
+        grad[x] = s;
+    }
+    if (n_quartets)
+        *n_quartets = nq;
+    if (seconds)
+        *seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+}
+
+int ref_jk_grad(void *h, const double *D, double *grad)
+{
+    return guarded([&] { jkGradImpl(h, D, grad, 0.0, 1, nullptr, nullptr); });
+}
+
+int ref_jk_grad_sample(void *h, const double *D, double *grad, double schwarz, int bra_stride, long long *n_quartets,
+                       double *seconds)
+{
+    return guarded([&] { jkGradImpl(h, D, grad, schwarz, bra_stride, n_quartets, seconds); });
 }
 
 // RI-J pieces from the reference kernels: gamma_P = sum_mn (mn|P) D_mn over all pairs (ERI3Kernel

@@ -245,6 +245,47 @@ def test_bounded_wait_gives_up_and_context_survives():
     assert np.abs(K1 - K0).max() <= 1e-12
 
 
+def _dd_dd_class(sp):
+    return next(c for c in sp if (c.la_, c.lb_) == (2, 2))
+
+
+def test_store_mode_wait_gives_up_and_context_survives():
+    # the (dd|dd) class runs on the DMMA path, whose ket tiles arrive by bulk copy; with the copies
+    # withheld its first wait runs out of polls, the store call reports ETIMEOUT (allocating and
+    # allocation-free forms), and the next calls on the same context match the reference
+    import ctypes
+
+    import torch
+
+    from lible_b200 import _lib
+
+    s = L.Structure("def2-svp", [8, 8, 8], O3_ANG)
+    sp = L.shellPairData(True, s)
+    dd = _dd_dd_class(sp)
+    idx = np.array([(i, j) for i in range(dd.n_pairs_) for j in range(dd.n_pairs_)], dtype=np.uint32)
+    ref = R.RefStructure("def2-svp", [8, 8, 8], O3_ANG, units="angstrom").eri4_class(True, dd.index, dd.index)
+    for polls in (1, 4096):
+        L.inject_wait_timeout(s, polls)
+        with pytest.raises(L.LibleGpuError) as e:
+            L.ERI4Kernel(dd, dd).batch(idx)
+        assert e.value.code == 6
+        got = L.ERI4Kernel(dd, dd).batch(idx)
+        assert np.abs(got.reshape(ref.shape) - ref).max() <= 1e-12
+    lib = _lib.load()
+    out = torch.zeros(ref.size, dtype=torch.float64, device="cuda")
+    L.inject_wait_timeout(s, 64)
+    rc = lib.lible_gpu_eri4_batch_noalloc(s.ctx, 1, dd.index, dd.index, len(idx), ctypes.c_void_p(idx.ctypes.data),
+                                          ctypes.c_void_p(out.data_ptr()))
+    assert rc == 6, lib.lible_gpu_last_error(s.ctx)
+    rc = lib.lible_gpu_eri4_batch_noalloc(s.ctx, 1, dd.index, dd.index, len(idx), ctypes.c_void_p(idx.ctypes.data),
+                                          ctypes.c_void_p(out.data_ptr()))
+    assert rc == 0, lib.lible_gpu_last_error(s.ctx)
+    assert np.abs(out.cpu().numpy().reshape(ref.shape) - ref).max() <= 1e-12
+    with pytest.raises(L.LibleGpuError) as e:
+        L.inject_wait_timeout(s, -1)
+    assert e.value.code == 1
+
+
 def test_deploy_eri3_eri2_golden():
     s = L.Structure("def2-svp", [8, 8, 8], O3_ANG, "def2-universal-jkfit")
     sp = L.shellPairData(False, s)
@@ -296,6 +337,39 @@ def test_jk_water_dimer_ccpvtz_vs_reference_kernels():
     J2, K2, _ = L.jk(s, D, schwarz=1e-12)
     assert np.abs(J2 - Jr).max() <= 1e-9
     assert np.abs(K2 - Kr).max() <= 1e-9
+
+
+def test_jk_config_h2o16_ccpvdz_vs_reference():
+    # the direct J/K configuration: (H2O)_16 cc-pVDZ (384 AOs), occupation 40, Schwarz 1e-12, FP64,
+    # against the reference's ERI4Kernel batches digested on the host cores (unsampled)
+    Z, xyz, rng = water_cluster(16, seed=2016)
+    s = L.Structure("cc-pvdz", Z, xyz, units="bohr")
+    assert s.nao == 384
+    D = random_density(s.nao, 40, rng)
+    J, K, st = L.jk(s, D, schwarz=1e-12)
+    R.set_threads(R.max_threads())
+    Jr, Kr, nq, _ = R.RefStructure("cc-pvdz", Z, xyz).jk(D, 1e-12, bra_stride=1)
+    assert st["n_quartets"] == nq
+    dJ, dK = np.abs(J - Jr).max(), np.abs(K - Kr).max()
+    assert dJ <= 1e-11 and dK <= 1e-11, (dJ, dK, np.linalg.norm(J - Jr), np.linalg.norm(K - Kr))
+    # the mixed-precision build of the same configuration stays within the energy bound
+    Jm, Km, stm = L.jk(s, D, schwarz=1e-12, precision="mixed", fp32_threshold=1e-4)
+    E = lambda J_, K_: float(np.sum(D * (0.5 * J_ - 0.25 * K_)))
+    assert stm["n_fp32"] > 0
+    assert abs(E(Jm, Km) - E(Jr, Kr)) <= 1e-8
+
+
+def test_jk_gradient_h2o4_ccpvtz_vs_reference():
+    # the gradient configuration's basis and density rule on (H2O)_4 cc-pVTZ (232 AOs, occupation
+    # 20): the backward pass against the reference's ERI4D1Kernel batches contracted on the host
+    Z, xyz, rng = water_cluster(4, seed=2008)
+    s = L.Structure("cc-pvtz", Z, xyz, units="bohr")
+    assert s.nao == 232
+    D = random_density(s.nao, 20, rng)
+    g = L.jk_energy_backward(s, D, schwarz=0.0)
+    R.set_threads(R.max_threads())
+    gr = R.RefStructure("cc-pvtz", Z, xyz).jk_grad(D)
+    assert np.abs(g - gr).max() <= 1e-10, float(np.abs(g - gr).max())
 
 
 def test_jk_gradient_vs_reference_and_fd():
