@@ -1,4 +1,4 @@
-"""Regenerate the basis-set text files shipped in this directory.
+"""Maintenance recipe: regenerates the basis-set text files shipped in lible_b200/basis/.
 
 The engine reads basis sets in the reference's plain-text format
 (``element=Z`` / ``l=L n=K`` / ``exponent coefficient`` lines / ``end=Z``; parser at
@@ -9,8 +9,8 @@ cc-pVDZ, cc-pVTZ, def2-SVP, def2-TZVP, 6-31+G and the auxiliary sets def2-QZVP-R
 def2-universal-JKFIT and cc-pVDZ-RIFIT.  The numbers are the published basis-set data, copied
 verbatim so that integrals agree with the reference to the last bit.
 
-Usage (needs a checkout of the reference project):
-    python lible_b200/basis/extract_subsets.py /path/to/Lible
+Usage (needs a checkout of the reference project, given explicitly):
+    python oracle/extract_basis.py <reference checkout>
 """
 import os
 import sys
@@ -37,7 +37,7 @@ def extract(src_path, dst_path):
 
 
 def main(ref_root):
-    here = os.path.dirname(os.path.abspath(__file__))
+    here = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "lible_b200", "basis")
     src = os.path.join(ref_root, "src", "lible", "ints")
     for kind, table, sub in (("main", MAIN, "lible_basis"), ("aux", AUX, "lible_aux_basis")):
         for family, names in table.items():
@@ -47,4 +47,6 @@ def main(ref_root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: python oracle/extract_basis.py <reference checkout>")
+    main(sys.argv[1])
