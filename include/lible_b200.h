@@ -301,17 +301,27 @@ int lible_gpu_one_electron_grad(lible_gpu_ctx *ctx, const double *D, const doubl
  * as its factor C ([nao][n_occ] row-major, D = C C^T; D may then be NULL) or, with C NULL, as the
  * symmetric D itself, which is factorised by its eigendecomposition (D = C+ C+^T - C- C-^T over the
  * eigenpairs with |w| > 1e-12 max|w|).  (P|Q) is factorised as for lible_gpu_rij
- * (lible_gpu_rij_last_solve reports it).  `info` (may be NULL) receives the factor ranks, the number
- * of auxiliary blocks and per-stage device times and FLOP counts.  D, C, K: host or device. */
+ * (lible_gpu_rij_last_solve reports it).  The first call on a structure (and Schwarz threshold)
+ * builds the fitted three-centre tensor B_R = sum_P F_PR (mn|P) with the metric's factor F
+ * (naux * nao^2 doubles) and keeps it on the context when it takes at most 60% of the free device
+ * memory; later calls are then one batched DGEMM and one DSYRK.  Without the room every call
+ * streams blocks of integrals and solves with the factor.  `info` (may be NULL) receives the
+ * factor ranks, the number of auxiliary blocks, per-stage device times (t_ints includes the
+ * tensor build on the call that made it) and FLOP counts, and whether the tensor was used.
+ * D, C, K: host or device. */
 typedef struct lible_gpu_rik_info
 {
     long long n_pos, n_neg;  /* columns of C+ and C- (n_occ and 0 when C is given) */
     int n_blocks;            /* blocks of auxiliary functions the three-centre integrals were built in */
     double t_ints, t_gemm, t_solve, t_syrk;               /* seconds */
     double flops_gemm, flops_solve, flops_syrk;           /* algorithmic FLOPs of the three stages */
+    int fitted;              /* 1: the cached fitted tensor served the call */
 } lible_gpu_rik_info;
 int lible_gpu_rik(lible_gpu_ctx *ctx, const double *D, const double *C, long long n_occ, double schwarz_threshold,
                   double *K, lible_gpu_rik_info *info);
+/* mode 1 (default): RI-K keeps the fitted tensor when it fits; 0: never build it (frees a cached one)
+ * and stream the integrals on every call. */
+int lible_gpu_rik_set_fitted(lible_gpu_ctx *ctx, int mode);
 
 /* ---- host-only helpers (no GPU needed) --------------------------------------------------------
  * The host set-up the kernels consume, exposed for checking against the reference:

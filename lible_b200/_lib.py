@@ -34,7 +34,7 @@ class RIKInfo(ctypes.Structure):
     _fields_ = [("n_pos", ctypes.c_longlong), ("n_neg", ctypes.c_longlong), ("n_blocks", ctypes.c_int),
                 ("t_ints", ctypes.c_double), ("t_gemm", ctypes.c_double), ("t_solve", ctypes.c_double),
                 ("t_syrk", ctypes.c_double), ("flops_gemm", ctypes.c_double), ("flops_solve", ctypes.c_double),
-                ("flops_syrk", ctypes.c_double)]
+                ("flops_syrk", ctypes.c_double), ("fitted", ctypes.c_int)]
 
 
 # name -> argument types; every function returns int (status) unless noted
@@ -86,6 +86,7 @@ SIGNATURES = {
     "lible_gpu_ri_contract": [P, P, P, D, P, P],
     "lible_gpu_rij_last_solve": [P, P, P, P, P, P],
     "lible_gpu_rik": [P, P, P, LL, D, P, ctypes.POINTER(RIKInfo)],
+    "lible_gpu_rik_set_fitted": [P, I],
     "lible_gpu_rij_grad": [P, P, D, P, ctypes.POINTER(D)],
     "lible_gpu_overlap": [P, P],
     "lible_gpu_kinetic_energy": [P, P],

@@ -40,8 +40,16 @@ struct lible_gpu_ctx
     // cuBLAS handle of the RI calls; both dropped when the structure changes
     std::unique_ptr<MetricFactor> metric;
     std::unique_ptr<BlasHandle> blas;
+    // fitted three-centre tensor of the RI-K calls (built by the first call that has the room);
+    // rik_fitted_mode 0 = never build it (stream the integrals on every call), 1 = when it fits
+    std::unique_ptr<FittedTensor> fitted;
+    int rik_fitted_mode = 1;
 
-    void structureChanged() { metric.reset(); }
+    void structureChanged()
+    {
+        metric.reset();
+        fitted.reset();
+    }
     const MetricFactor &metricFactor(Engine &e)
     {
         if (!metric)
@@ -1098,18 +1106,40 @@ int lible_gpu_rik(lible_gpu_ctx *ctx, const double *D, const double *C, long lon
         const size_t avail = free_b > z_bytes ? free_b - z_bytes : 0;
         const size_t block_bytes = std::min<size_t>(size_t(16) << 30, std::max<size_t>(size_t(256) << 20, avail / 4));
         long long n_pos = n_occ, n_neg = 0;
+        // the fitted tensor (naux * nao^2 doubles) is built once and kept when it takes at most
+        // 60% of the free memory after Z; otherwise every call streams blocks of integrals
+        const size_t fit_bytes = e.naux() * n * n * sizeof(double);
+        if (ctx->fitted && ctx->fitted->schwarz != schwarz_threshold)
+            ctx->fitted.reset();
+        if (ctx->rik_fitted_mode == 0)
+            ctx->fitted.reset();
+        if (!ctx->fitted && ctx->rik_fitted_mode == 1 && fit_bytes <= (size_t)(0.6 * (double)avail))
+        {
+            auto ft = std::make_unique<FittedTensor>();
+            buildFitted(e, bh, mf, schwarz_threshold, *ft);
+            st.t_ints += ft->t_build;
+            st.n_blocks += 1;
+            ctx->fitted = std::move(ft);
+        }
+        const FittedTensor *ft = ctx->fitted.get();
+        auto exchange = [&](const double *c, long long occ, double sign) {
+            if (ft)
+                riExchangeFitted(e, bh, *ft, c, occ, sign, k.ptr, &st);
+            else
+                riExchange(e, bh, mf, c, occ, schwarz_threshold, sign, k.ptr, block_bytes, &st);
+        };
         if (C)
         {
             DevArray c(C, n * (size_t)std::max<long long>(n_occ, 1), true, e.stream());
-            riExchange(e, bh, mf, c.ptr, n_occ, schwarz_threshold, 1.0, k.ptr, block_bytes, &st);
+            exchange(c.ptr, n_occ, 1.0);
         }
         else
         {
             DevArray d(D, n * n, true, e.stream());
             DevBuf<double> cp, cm;
             splitDensity(e, d.ptr, (long long)n, cp, n_pos, cm, n_neg);
-            riExchange(e, bh, mf, cp.p, n_pos, schwarz_threshold, 1.0, k.ptr, block_bytes, &st);
-            riExchange(e, bh, mf, cm.p, n_neg, schwarz_threshold, -1.0, k.ptr, block_bytes, &st);
+            exchange(cp.p, n_pos, 1.0);
+            exchange(cm.p, n_neg, -1.0);
         }
         mirrorUpper(k.ptr, (long long)n, e.stream());
         e.sync();
@@ -1126,7 +1156,19 @@ int lible_gpu_rik(lible_gpu_ctx *ctx, const double *D, const double *C, long lon
             info->flops_gemm = st.flops_gemm;
             info->flops_solve = st.flops_solve;
             info->flops_syrk = st.flops_syrk;
+            info->fitted = ft ? 1 : 0;
         }
+    });
+}
+
+int lible_gpu_rik_set_fitted(lible_gpu_ctx *ctx, int mode)
+{
+    return guard(ctx, [&](Engine &) {
+        if (mode != 0 && mode != 1)
+            throw EngineError(kStatusInvalid, "mode must be 0 (stream) or 1 (cache when it fits)");
+        ctx->rik_fitted_mode = mode;
+        if (mode == 0)
+            ctx->fitted.reset();
     });
 }
 

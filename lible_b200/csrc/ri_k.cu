@@ -11,6 +11,9 @@
 //   4. K = sum_R W_R W_R^T: W is re-laid out as A[m][R][i] block by block and each block is one
 //      DSYRK with k = R_block * occ.
 // The three-centre tensor is never held in full: only Z (naux x nao x occ) and one block of T.
+// When the fitted tensor B = L^{-1} (mn|P) fits in device memory it is instead built once per
+// structure (buildFitted) and every call is one strided-batched DGEMM and one DSYRK
+// (riExchangeFitted): no integrals and no triangular solve per call.
 #include "ri_solve.hpp"
 
 #include <cmath>
@@ -324,6 +327,89 @@ namespace lible_b200
             stats->n_blocks += (int)blocks.size();
             stats->flops_gemm += 2.0 * (double)na * (double)n * (double)n * (double)occ;
             stats->flops_solve += (mf.method == 1 ? 2.0 : 1.0) * (double)na * (double)na * (double)m;
+            stats->flops_syrk += (double)n * (double)(n + 1) * (double)na * (double)occ;
+        }
+    }
+
+    void buildFitted(Engine &e, BlasHandle &bh, const MetricFactor &mf, double schwarz, FittedTensor &ft)
+    {
+        const long long n = (long long)e.nao(), na = (long long)e.naux();
+        const cudaStream_t s = e.stream();
+        const long long rows = n * n;  // column-major view of T[P][m][n]: rows (m, n), columns P
+        if (rows > INT32_MAX || na > INT32_MAX)
+            throw EngineError(kStatusUnsupported, "RI-K: nao^2 exceeds the 32-bit cuBLAS dimension range");
+        ft.B.reset((size_t)(na * rows));
+        EventPair ev;
+        cudaCheck(cudaEventRecord(ev.a, s), "event");
+        // all auxiliary functions in one store launch sequence: T[P][m][n] = (mn|P)
+        e.riStore(0, (int)na, ft.B.p, schwarz);
+        e.checkStatus();
+        const double one = 1.0, zero = 0.0;
+        if (mf.method == 0 || mf.method == 2)
+        {
+            // B_cm L^T = T_cm  (B_cm = T_cm L^{-T}: column R of B is sum_P T_P (L^{-T})_PR)
+            blasCheck(cublasDtrsm(bh.h, CUBLAS_SIDE_RIGHT, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_T, CUBLAS_DIAG_NON_UNIT,
+                                  (int)rows, (int)na, &one, mf.fac.p, (int)na, ft.B.p, (int)rows),
+                      "dtrsm");
+        }
+        else
+        {
+            // B_cm = T_cm G by row blocks through a scratch of at most 1 GiB
+            const long long mb = std::max<long long>(1, std::min<long long>(rows, (1LL << 27) / std::max(na, 1LL)));
+            DevBuf<double> tmp((size_t)(mb * na));
+            for (long long r0 = 0; r0 < rows; r0 += mb)
+            {
+                const long long rr = std::min(mb, rows - r0);
+                blasCheck(cublasDgemm(bh.h, CUBLAS_OP_N, CUBLAS_OP_N, (int)rr, (int)na, (int)na, &one, ft.B.p + r0,
+                                      (int)rows, mf.fac.p, (int)na, &zero, tmp.p, (int)rr),
+                          "dgemm");
+                cudaCheck(cudaMemcpy2DAsync(ft.B.p + r0, (size_t)rows * sizeof(double), tmp.p,
+                                            (size_t)rr * sizeof(double), (size_t)rr * sizeof(double), (size_t)na,
+                                            cudaMemcpyDeviceToDevice, s),
+                          "copy");
+            }
+        }
+        cudaCheck(cudaEventRecord(ev.b, s), "event");
+        cudaCheck(cudaEventSynchronize(ev.b), "fitted tensor");
+        ft.schwarz = schwarz;
+        ft.naux = (size_t)na;
+        ft.nao = (size_t)n;
+        ft.t_build = ev.seconds();
+    }
+
+    void riExchangeFitted(Engine &e, BlasHandle &bh, const FittedTensor &ft, const double *C_dev, long long occ,
+                          double sign, double *K_dev, RIKStats *stats)
+    {
+        if (occ <= 0)
+            return;
+        const long long n = (long long)ft.nao, na = (long long)ft.naux;
+        const cudaStream_t s = e.stream();
+        const long long k = na * occ;
+        if (k > INT32_MAX)
+            throw EngineError(kStatusUnsupported, "RI-K: naux * occ exceeds the 32-bit cuBLAS dimension range");
+        // Z[m][R][i] = sum_n B[R][m][n] C[n][i], written straight in the layout of the final product:
+        // per R one GEMM, in column-major terms Z_R,cm (occ x n, ld = naux*occ) = C_cm (occ x n) B_R,cm
+        // (B_R symmetric in (m, n)); all R as one strided batch
+        DevBuf<double> Z((size_t)(n * k));
+        EventPair ev_gemm, ev_syrk;
+        const double one = 1.0, zero = 0.0;
+        cudaCheck(cudaEventRecord(ev_gemm.a, s), "event");
+        blasCheck(cublasDgemmStridedBatched(bh.h, CUBLAS_OP_N, CUBLAS_OP_N, (int)occ, (int)n, (int)n, &one, C_dev,
+                                            (int)occ, 0, ft.B.p, (int)n, n * n, &zero, Z.p, (int)k, occ, (int)na),
+                  "dgemm batched");
+        cudaCheck(cudaEventRecord(ev_gemm.b, s), "event");
+        // K += sign Z Z^T over (R, i): column-major Z_cm is (k x n), K_cm += sign Z_cm^T Z_cm
+        cudaCheck(cudaEventRecord(ev_syrk.a, s), "event");
+        blasCheck(cublasDsyrk(bh.h, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_T, (int)n, (int)k, &sign, Z.p, (int)k, &one,
+                              K_dev, (int)n),
+                  "dsyrk");
+        cudaCheck(cudaEventRecord(ev_syrk.b, s), "event");
+        cudaCheck(cudaEventSynchronize(ev_syrk.b), "ri exchange");
+        if (stats)
+        {
+            stats->t_gemm += ev_gemm.seconds();
+            stats->t_syrk += ev_syrk.seconds();
+            stats->flops_gemm += 2.0 * (double)na * (double)n * (double)n * (double)occ;
             stats->flops_syrk += (double)n * (double)(n + 1) * (double)na * (double)occ;
         }
     }

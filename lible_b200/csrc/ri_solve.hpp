@@ -99,6 +99,22 @@ namespace lible_b200
     void riExchange(Engine &e, BlasHandle &bh, const MetricFactor &mf, const double *C_dev, long long occ,
                     double schwarz, double sign, double *K_dev, size_t block_bytes, RIKStats *stats);
 
+    // The fitted three-centre tensor B[R][m][n] = sum_P F_PR (mn|P), F = L^{-T} (Cholesky) or G
+    // (eigendecomposition), so that sum_R B_R,mn B_R,ls = sum_PQ (mn|P) M^{-1}_PQ (Q|ls).  Built once
+    // per structure and Schwarz threshold (naux * nao^2 doubles) and kept in HBM; every later
+    // exchange build is then one strided-batched DGEMM and one DSYRK.
+    struct FittedTensor
+    {
+        DevBuf<double> B;
+        double schwarz = -1;
+        size_t naux = 0, nao = 0;
+        double t_build = 0;  // seconds of the build (integrals + fit)
+    };
+    void buildFitted(Engine &e, BlasHandle &bh, const MetricFactor &mf, double schwarz, FittedTensor &ft);
+    // K += sign * sum_R (B_R C)(B_R C)^T with the cached tensor (same contract as riExchange).
+    void riExchangeFitted(Engine &e, BlasHandle &bh, const FittedTensor &ft, const double *C_dev, long long occ,
+                          double sign, double *K_dev, RIKStats *stats);
+
     // Mirrors the row-major upper triangle of the n x n matrix into the lower one.
     void mirrorUpper(double *K_dev, long long n, cudaStream_t s);
 

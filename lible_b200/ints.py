@@ -601,6 +601,12 @@ def rik(structure, D=None, C=None, schwarz=1e-12, info=False):
     return K
 
 
+def rik_set_fitted(structure, mode):
+    """1 (default): RI-K keeps the fitted three-centre tensor on the context when it fits; 0: stream
+    the integrals on every call (and drop a cached tensor)."""
+    _call(structure, "lible_gpu_rik_set_fitted", int(mode))
+
+
 def ri_contract(structure, D=None, dcoef=None, schwarz=1e-12):
     """gamma_P = sum (mn|P) D_mn (if D is given) and J_mn = sum_P (mn|P) d_P (if dcoef is given)."""
     n, na = structure.nao, structure.naux

@@ -132,3 +132,10 @@ def test_gpu_rik_matches_golden():
     J, _, _ = L.rij(s, g["C"] @ g["C"].T, schwarz=0.0)
     assert np.abs(J - g["J"]).max() <= 1e-10
     assert L.rij_last_solve(s)["method"] == "cholesky"
+    # the first call built the fitted three-centre tensor; the streaming path gives the same K
+    assert info["fitted"] == 1 and info2["fitted"] == 1
+    L.rik_set_fitted(s, 0)
+    Ks, infos = L.rik(s, C=g["C"], schwarz=0.0, info=True)
+    assert infos["fitted"] == 0 and infos["n_blocks"] >= 1
+    assert np.abs(Ks - g["K"]).max() <= 1e-10
+    L.rik_set_fitted(s, 1)
