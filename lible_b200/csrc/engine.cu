@@ -762,7 +762,7 @@ namespace lible_b200
             }
         cs.dev.resize(cs.host.size());
         for (size_t c = 0; c < cs.host.size(); c++)
-            uploadClass(cs.host[c], true, use_symm && max_l_ <= 2, cs.dev[c]);
+            uploadClass(cs.host[c], true, use_symm, cs.dev[c]);
         cs.built = true;
         return cs;
     }
@@ -1712,8 +1712,6 @@ namespace lible_b200
     void Engine::jk(const double *D_dev, double *J_dev, double *K_dev, const JKOptions &opt, JKStats *stats)
     {
         const bool mixed = opt.precision == 1;
-        if (mixed && max_l_ > 2)
-            throw EngineError(kStatusUnsupported, "mixed precision is instantiated for l <= 2 bases only");
         JKPlan &plan = jkPlan(opt.schwarz, opt.fp32_threshold, mixed);
         if (opt.use_graph)
         {
@@ -1817,8 +1815,6 @@ namespace lible_b200
                                    const std::string &cache)
     {
         const bool mixed = opt.precision == 1;
-        if (mixed && max_l_ > 2)
-            throw EngineError(kStatusUnsupported, "mixed precision is instantiated for l <= 2 bases only");
         if (!cache.empty())
             tune_cache_ = cache;
         JKPlan &plan = jkPlan(opt.schwarz, opt.fp32_threshold, mixed);
@@ -1935,8 +1931,6 @@ namespace lible_b200
     std::vector<Engine::LaunchTime> Engine::jkProfile(const double *D, double *J, double *K, const JKOptions &opt)
     {
         const bool mixed = opt.precision == 1;
-        if (mixed && max_l_ > 2)
-            throw EngineError(kStatusUnsupported, "mixed precision is instantiated for l <= 2 bases only");
         JKPlan &plan = jkPlan(opt.schwarz, opt.fp32_threshold, mixed);
         LaunchTimer timer;
         enqueueJK(plan, D, J, K, mixed, &timer);

@@ -7,7 +7,7 @@ host swaps bra and ket (and transposes the output) for the other orientation.
 import os
 
 PAIR_TYPES = [(0, 0), (1, 0), (1, 1), (2, 0), (2, 1), (2, 2), (3, 0), (3, 1), (3, 2), (3, 3), (4, 0), (5, 0)]
-FP32_MAX_TYPE = 5  # mixed precision is instantiated for the l <= 2 classes
+FP32_MAX_TYPE = 9  # mixed precision is instantiated for the l <= 3 classes (cc-pVTZ)
 
 
 def kinds():

@@ -451,6 +451,24 @@ def test_mixed_precision_jk_error_small():
     assert np.linalg.norm(Jm - J) <= 1e-6 and np.linalg.norm(Km - K) <= 1e-6
 
 
+def test_mixed_precision_jk_ccpvtz():
+    # FP32 quartets of the f- and d-shell classes of cc-pVTZ (register and shared-memory shapes)
+    Z, xyz, rng = water_cluster(3, seed=13)
+    s = L.Structure("cc-pvtz", Z, xyz, units="bohr")
+    D = random_density(s.nao, 15, rng)
+    J, K, st = L.jk(s, D, 1e-12, "fp64")
+    Jm, Km, stm = L.jk(s, D, 1e-12, "mixed", 1e-4)
+    assert stm["n_fp32"] > 0 and stm["n_quartets"] == st["n_quartets"]
+    E = np.sum(D * (0.5 * J - 0.25 * K))
+    Em = np.sum(D * (0.5 * Jm - 0.25 * Km))
+    assert abs(E - Em) <= 1e-8
+    assert np.linalg.norm(Jm - J) <= 1e-6 and np.linalg.norm(Km - K) <= 1e-6
+    # every class pair takes part in both precisions at a loose threshold
+    Jm2, Km2, stm2 = L.jk(s, D, 1e-12, "mixed", 1e-1)
+    assert stm2["n_fp32"] > stm["n_fp32"]
+    assert np.linalg.norm(Jm2 - J) <= 1e-4 and np.linalg.norm(Km2 - K) <= 1e-4
+
+
 def test_rij_even_tempered_aux_vs_reference():
     # the s-f even-tempered auxiliary basis of the mixed-precision RI-J workload (0.1 * 2.5^k,
     # k = 0..11 per l), on one water
