@@ -30,7 +30,10 @@ N_WATERS, SEED, OCC = 32, 2024, 160
 SCHWARZ, FP32_THR = 1e-12, 1e-4
 # DRAM bytes (read + write) per launch of the dominant class kernels at this workload, from one ncu
 # capture each (dram__bytes_read.sum + dram__bytes_write.sum); the working set stays in L2
-DOMINANT_TRAFFIC = {(1, 0, 0, 0): 34.29e6, (2, 1, 1, 0): 24.16e6}
+DOMINANT_TRAFFIC = {((1, 0, 0, 0), False): 34.29e6, ((2, 1, 1, 0), False): 24.16e6}
+# L2 atomic (RED) bytes per launch of the dominant FP64 kernel, lts__t_sectors_op_red.sum x 32 from one
+# ncu capture of this workload (profiles/)
+L2_ATOMIC_BYTES = {}
 # classes compiled with a raised occupancy bound (eriKernelOcc, minBlocksPerSM in
 # lible_b200/csrc/eri_kernel.cuh): (class, fp32) -> kernel name
 OCC_KERNELS = {(c, f): "eriKernelOcc" for c, f in [((2, 1, 1, 0), False), ((2, 0, 1, 0), False), ((2, 1, 0, 0), False),
@@ -58,6 +61,28 @@ def max_over_ranks(x, dist=None, device="cpu"):
 
 def emit(obj):
     print(json.dumps(obj), flush=True)
+
+
+def cpu_model():
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return None
+
+
+def digestion_bytes(classes):
+    """Algorithmic bytes of the J/K digestion of one build: per unique quartet (ab|cd), 8 bytes per
+    D-block element read and 16 per J/K-block element read-modify-written, over the six blocks
+    (ab), (cd), (ac), (ad), (bc), (bd) of spherical sizes n_x n_y."""
+    total = 0.0
+    for (la, lb, lc, ld), n64, n32, _, _ in classes:
+        na, nb, nc, nd = (2 * l + 1 for l in (la, lb, lc, ld))
+        blocks = na * nb + nc * nd + na * nc + na * nd + nb * nc + nb * nd
+        total += (n64 + n32) * 24.0 * blocks
+    return total
 
 
 def clocks_start(gpu_index):
@@ -109,12 +134,24 @@ def cpu_reference(steps, warmup, Z, xyz, D, target_s=12.0):
     r = R.RefStructure("cc-pvdz", Z, xyz)
     _, _, nq, sec = r.jk(D, SCHWARZ, 256)
     stride = max(1, int(math.ceil(256 * sec / target_s)))
-    best = None
+    for _ in range(max(0, warmup)):
+        r.jk(D, SCHWARZ, stride)
+    rates = []
     for _ in range(max(1, steps)):
         _, _, nq, sec = r.jk(D, SCHWARZ, stride)
-        qps = nq / sec
-        best = qps if best is None else max(best, qps)
-    return best, cores, stride, nq, sec
+        rates.append(nq / sec)
+    return float(np.mean(rates)), cores, stride, nq, sec
+
+
+def oracle_jk_full(Z, xyz, D):
+    """The reference's ERI4Kernel batches digested into J/K on every host core, unsampled: the CPU
+    baseline of the whole workload and the oracle the GPU builds are checked against."""
+    from oracle import ref as R
+    cores = os.cpu_count() or 1
+    R.set_threads(cores)
+    r = R.RefStructure("cc-pvdz", Z, xyz)
+    J, K, nq, sec = r.jk(D, SCHWARZ, 1)
+    return J, K, nq, sec, cores
 
 
 def run_reference(args):
@@ -134,7 +171,8 @@ def run_reference(args):
           "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sec, "higher_is_better": True,
           "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
           "config": WORKLOAD,
-          "cpu_baseline": {"value": qps, "unit": "quartets/s", "cores": cores, "kind": "reference", "sample": sample},
+          "cpu_baseline": {"value": qps, "unit": "quartets/s", "cores": cores, "kind": "reference", "sample": sample,
+                           "cpu_model": cpu_model()},
           "e2e": {"value": qps, "unit": "quartets/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}})
 
 
@@ -301,7 +339,7 @@ def run_one_electron(Z, xyz, steps, cpu=True):
     return out
 
 
-def run_gradient(steps, seed=2024):
+def run_gradient(steps, seed=2024, cpu=True):
     """J/K energy gradient of (H2O)_8 cc-pVTZ (464 AOs, occupation 40): wall time of the backward
     pass (derivative integrals contracted with the two-particle density on the device) and its
     agreement with central finite differences (step 1e-4 bohr) of the forward energy on two
@@ -329,9 +367,26 @@ def run_gradient(steps, seed=2024):
             c[atom, x] += sgn * h
             e.append(L.jk_energy_forward(L.Structure("cc-pvtz", Z, c, units="bohr"), D, SCHWARZ))
         worst = max(worst, abs((e[0] - e[1]) / (2 * h) - g[atom, x]))
-    return {"workload": "J/K energy gradient, (H2O)_8 cc-pVTZ, occupation 40, FP64", "nao": s.nao,
-            "backward_s": float(np.mean(ts)), "forward_energy_s": t_fwd,
-            "max_abs_fd_minus_analytic_Eh_per_bohr": worst, "fd_step_bohr": h}
+    out = {"workload": "J/K energy gradient, (H2O)_8 cc-pVTZ, occupation 40, FP64", "nao": s.nao,
+           "backward_s": float(np.mean(ts)), "forward_energy_s": t_fwd,
+           "max_abs_fd_minus_analytic_Eh_per_bohr": worst, "fd_step_bohr": h}
+    from oracle import ref as R
+    if cpu and R.available():
+        # the reference's ERI4D1Kernel batches contracted with the same two-particle density on every
+        # host core, over the same Schwarz-surviving quartets of every stride-th bra pair (~10 s)
+        cores = os.cpu_count() or 1
+        R.set_threads(cores)
+        r = R.RefStructure("cc-pvtz", Z, xyz)
+        _, nq, sec = r.jk_grad_sample(D, SCHWARZ, 512)
+        stride = max(1, int(math.ceil(512 * sec / 10.0)))
+        _, nq, sec = r.jk_grad_sample(D, SCHWARZ, stride)
+        n_full = L.jk_plan(s, SCHWARZ, "fp64")["n_quartets"]
+        est = sec * n_full / max(nq, 1)
+        out["reference_cpu"] = {"cores": cores, "cpu_model": cpu_model(), "quartets": nq, "seconds": sec,
+                                "quartets_per_s": nq / sec, "estimated_full_s": est,
+                                "gpu_speedup_estimate": est / out["backward_s"],
+                                "sample": f"every {stride}-th bra shell pair, Schwarz 1e-12 ({nq} of {n_full} quartets)"}
+    return out
 
 
 def main():
@@ -450,72 +505,113 @@ def main():
         rij = run_rij(Z, xyz, D, J64, min(args.steps, 2))
         rijk = run_rijk(Z, xyz, D, J64, K64, OCC, min(args.steps, 2))
         one_el = run_one_electron(Z, xyz, min(args.steps, 2), cpu=not args.no_cpu_baseline)
-        gradient = run_gradient(min(args.steps, 2))
+        gradient = run_gradient(min(args.steps, 2), cpu=not args.no_cpu_baseline)
 
     if rank != 0:
         if dist:
             dist.destroy_process_group()
         return
 
-    cpu = None
+    # CPU leg (rank 0, one GPU): the reference's ERI4Kernel batches digested into J/K on every host
+    # core, unsampled -- the CPU baseline of the whole workload and the oracle of both GPU builds
+    cpu = oracle = None
     if world == 1 and not args.no_cpu_baseline:
         from oracle import ref as R
         if R.available():
-            qps, cores, stride, nq, sec = cpu_reference(1, 0, Z, xyz, D)
-            cpu = {"value": qps, "unit": "quartets/s", "cores": cores, "kind": "reference",
-                   "sample": f"reference ERI4Kernel + J/K digestion, every {stride}-th bra shell pair of every "
-                             f"class pair: {nq} quartets in {sec:.2f} s"}
+            Jr, Kr, nq_ref, sec_ref, cores = oracle_jk_full(Z, xyz, D)
+            Er = float(np.sum(D * (0.5 * Jr - 0.25 * Kr)))
+            cpu = {"value": nq_ref / sec_ref, "unit": "quartets/s", "cores": cores, "kind": "reference",
+                   "cpu_model": cpu_model(),
+                   "sample": f"whole workload, unsampled: reference ERI4Kernel batches + J/K digestion (OpenMP), "
+                             f"{nq_ref} quartets in {sec_ref:.2f} s"}
+            oracle = {"n_quartets_match": int(nq_ref) == int(plan64["n_quartets"]),
+                      "fp64_max_abs_dJ": float(np.abs(J64 - Jr).max()), "fp64_max_abs_dK": float(np.abs(K64 - Kr).max()),
+                      "fp64_abs_dE_Eh": abs(E64 - Er),
+                      "mixed_max_abs_dJ": float(np.abs(Jmx - Jr).max()), "mixed_max_abs_dK": float(np.abs(Kmx - Kr).max()),
+                      "mixed_abs_dE_Eh": abs(Emx - Er),
+                      "mixed_dJ_fro": float(np.linalg.norm(Jmx - Jr)), "mixed_dK_fro": float(np.linalg.norm(Kmx - Kr))}
 
     flops64 = plan64["flops_fp64"]
     achieved64 = flops64 / (t64 * 1e-3) / 1e12
-    # dominant kernel of the FP64 build: every class launch timed by CUDA events (launches
-    # serialised on the structure's stream), mean of three profiled builds after the timed region
-    prof = {}
-    for _ in range(3):
-        for r in L.jk_profile(s, Dd, SCHWARZ, "fp64", J=J, K=K):
-            key = (r["classes"], r["fp32"])
-            e = prof.setdefault(key, {"ms": [], "flops": r["flops"], "tasks": r["tasks"]})
-            e["ms"].append(r["ms"])
-    dom_key, dom = max(prof.items(), key=lambda kv: np.mean(kv[1]["ms"]))
-    dom_ms = float(np.mean(dom["ms"]))
-    dom_tflops = dom["flops"] / (dom_ms * 1e-3) / 1e12
-    fp64_peak = max(dfma, dmma)
+    ffma, ffma2 = L.fp32_peak(s)
+    fp64_peak, fp32_peak = max(dfma, dmma), max(ffma, ffma2)
+
+    # every class launch timed by CUDA events (launches serialised on the structure's stream), mean
+    # of three profiled builds after the timed region; the dominant launch of a build is its roofline
+    def dominant(precision):
+        prof = {}
+        for _ in range(3):
+            for r in L.jk_profile(s, Dd, SCHWARZ, precision, FP32_THR, J=J, K=K):
+                key = (r["classes"], r["fp32"])
+                e = prof.setdefault(key, {"ms": [], "flops": r["flops"], "tasks": r["tasks"]})
+                e["ms"].append(r["ms"])
+        key, d = max(prof.items(), key=lambda kv: np.mean(kv[1]["ms"]))
+        ms = float(np.mean(d["ms"]))
+        tf = d["flops"] / (ms * 1e-3) / 1e12
+        fp32 = bool(key[1])
+        peak = fp32_peak if fp32 else fp64_peak
+        name = "%s<%d,%d,%d,%d,%s>" % ((OCC_KERNELS.get((key[0], key[1]), "eriKernel"),) + tuple(key[0]) +
+                                       ("float" if fp32 else "double",))
+        return {"bound": "fp32" if fp32 else "fp64", "achieved": tf, "peak": peak, "unit": "TFLOP/s",
+                "frac": tf / peak if peak else None, "traffic": DOMINANT_TRAFFIC.get((tuple(key[0]), fp32)),
+                "kernel": name, "kernel_ms": ms, "kernel_quartets": d["tasks"],
+                "scope": f"dominant class kernel of the {precision} build: algorithmic FLOPs per launch / CUDA-event "
+                         "launch time (serialised profile builds after the timed region); the limiter ncu shows is "
+                         "issue / L1 latency, not the HBM (the working set stays in L2)",
+                "peak_source": ("FP32 peak measured in this run (lible_gpu_fp32_peak: scalar FFMA and packed "
+                                "fma.rn.f32x2 loops, the larger)" if fp32 else
+                                "FP64 peak measured in this run (lible_gpu_fp64_peak: DFMA and DMMA m8n8k4 loops, the "
+                                "larger)") + "; the measured-peaks file has no FP64 or FP32 entry"}
+
+    roof_head = dominant(head)
+    roof64 = roof_head if head == "fp64" else dominant("fp64")
+    roof64 = dict(roof64, build_fp64_tflops=achieved64, dfma_peak=dfma, dmma_peak=dmma)
+    roof_head = dict(roof_head, ffma_peak=ffma, ffma2_peak=ffma2) if head == "mixed" else roof64
+
+    # J/K digestion: algorithmic bytes of one build over the build time, against the measured HBM copy
+    # bandwidth (the accumulators stay in L2, so this is an L2-side rate)
+    hbm, hbm_src = 6650.0, "fallback"
+    try:
+        hbm, hbm_src = float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"]), "measured"
+    except (OSError, ValueError, KeyError):
+        pass
+    dig_b = digestion_bytes(L.jk_plan_classes(s, SCHWARZ, "fp64", FP32_THR))
+    digestion = {"bytes_per_build": dig_b, "fp64_gbs": dig_b / (t64 * 1e-3) / 1e9,
+                 "mixed_gbs": dig_b / (tmx * 1e-3) / 1e9, "hbm_gbs": hbm, "hbm_source": hbm_src,
+                 "fp64_frac_of_hbm": dig_b / (t64 * 1e-3) / 1e9 / hbm,
+                 "l2_atomic_bytes_fp64_dominant_launch": L2_ATOMIC_BYTES.get(roof64["kernel"]),
+                 "definition": "per unique quartet 8 B per D-block element read + 16 B per J/K-block element updated, "
+                               "blocks ab, cd, ac, ad, bc, bd"}
     out = {
         "metric": METRIC, "value": value, "unit": "quartets/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": th, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64+f32 (mixed)" if mixed_ok else "f64", "data": "synthetic",
-        "config": dict(WORKLOAD, parallelism=f"replicas x{world}", path=head),
-        "jk_build_s": th * 1e-3,
-        "fp64": {"jk_build_s": t64 * 1e-3, "quartets_per_s": world * plan64["n_quartets"] / (t64 * 1e-3),
-                 "n_quartets": plan64["n_quartets"], "n_prim_quartets": plan64["n_prim_quartets"]},
-        "mixed": {"jk_build_s": tmx * 1e-3, "quartets_per_s": world * planmx["n_quartets"] / (tmx * 1e-3),
-                  "n_fp32_quartets": planmx["n_fp32"], "speedup_vs_fp64": t64 / tmx, "abs_dE_Eh": dE,
-                  "dJ_fro": float(np.linalg.norm(Jmx - J64)), "dK_fro": float(np.linalg.norm(Kmx - K64)),
-                  "meets_1e-8": mixed_ok},
-        "setup_s": setup_s, "plan_setup_s": plan_s, "autotuned": not args.no_autotune,
-        "roofline": {"bound": "tensor", "achieved": dom_tflops, "peak": fp64_peak, "unit": "TFLOP/s",
-                     "frac": dom_tflops / fp64_peak if fp64_peak else None,
-                     "traffic": DOMINANT_TRAFFIC.get(dom_key[0]),
-                     "kernel": "%s<%d,%d,%d,%d,%s>" % ((OCC_KERNELS.get((dom_key[0], dom_key[1]), "eriKernel"),) +
-                                                      dom_key[0] + ("float" if dom_key[1] else "double",)),
-                     "kernel_ms": dom_ms, "kernel_quartets": dom["tasks"],
-                     "scope": "dominant class kernel of the FP64 build: algorithmic FLOPs per launch / CUDA-event "
-                              "launch time (serialised profile builds after the timed region)",
-                     "peak_source": "FP64 peak measured in this run (lible_gpu_fp64_peak: register-resident DFMA "
-                                    "and DMMA m8n8k4 loops, the larger); the measured-peaks file has no FP64 entry",
-                     "dfma_peak": dfma, "dmma_peak": dmma,
-                     "build_fp64_tflops": achieved64},
-        "cpu_baseline": cpu,
-        "e2e": {"value": world * plan["n_quartets"] / e2e_t, "unit": "quartets/s",
-                "h2d_bytes_per_step": int(D.nbytes), "d2h_bytes_per_step": int(2 * D.nbytes),
-                "path": "lible_b200.jk -> lible_gpu_jk with pinned host D/J/K"},
+        "config": WORKLOAD,
         "batch": batch,
         "rij": rij,
         "rijk": rijk,
         "one_electron": one_el,
         "gradient": gradient,
-        "gpu_launches": int(plan["n_launches"]) * args.steps,
+        "setup_s": setup_s, "plan_setup_s": plan_s, "autotuned": not args.no_autotune,
+        "parallelism": f"replicas x{world}",
+        "roofline_fp64": roof64,
+        "cpu_baseline": cpu,
+        "e2e": {"value": world * plan["n_quartets"] / e2e_t, "unit": "quartets/s",
+                "h2d_bytes_per_step": int(D.nbytes), "d2h_bytes_per_step": int(2 * D.nbytes),
+                "path": "lible_b200.jk -> lible_gpu_jk with pinned host D/J/K"},
         "clocks": clocks,
+        "gpu_launches": int(plan["n_launches"]) * args.steps,
+        "roofline": roof_head,
+        "digestion": digestion,
+        "oracle_check": oracle,
+        "fp64": {"jk_build_s": t64 * 1e-3, "quartets_per_s": world * plan64["n_quartets"] / (t64 * 1e-3),
+                 "n_quartets": plan64["n_quartets"], "n_prim_quartets": plan64["n_prim_quartets"]},
+        "mixed": {"jk_build_s": tmx * 1e-3, "quartets_per_s": world * planmx["n_quartets"] / (tmx * 1e-3),
+                  "n_fp32_quartets": planmx["n_fp32"], "abs_dE_Eh_vs_fp64": dE,
+                  "dJ_fro": float(np.linalg.norm(Jmx - J64)), "dK_fro": float(np.linalg.norm(Kmx - K64)),
+                  "meets_1e-8": mixed_ok, "speedup_vs_fp64": t64 / tmx},
+        "path": head,
+        "jk_build_s": th * 1e-3,
     }
     emit(out)
     if dist:

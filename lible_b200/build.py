@@ -1,7 +1,8 @@
 """Builds lible_b200/liblible_b200.so (sm_100a) in-tree with nvcc.
 
-Objects go to lible_b200/_build/; each translation unit is rebuilt when it or any header under
-csrc/ is newer than its object.  Instantiation files are regenerated first.
+Objects go to lible_b200/_build/; each translation unit is rebuilt when it or any header it
+includes (transitively, #include "...") is newer than its object.  Instantiation files are
+regenerated first.
 
     python -m lible_b200.build [-j N]
 """
@@ -9,6 +10,7 @@ import argparse
 import concurrent.futures as cf
 import glob
 import os
+import re
 import shutil
 import subprocess
 import sys
@@ -39,10 +41,24 @@ def sources():
     return srcs
 
 
-def newest_header():
-    hdrs = glob.glob(os.path.join(CSRC, "*.hpp")) + glob.glob(os.path.join(CSRC, "*.cuh"))
-    hdrs.append(os.path.join(os.path.dirname(HERE), "include", "lible_b200.h"))
-    return max(os.path.getmtime(h) for h in hdrs if os.path.exists(h))
+_INCLUDE = re.compile(r'^\s*#\s*include\s+"([^"]+)"', re.M)
+
+
+def local_deps(path, seen=None):
+    """The source file and every header it includes with #include "..." (transitively)."""
+    seen = set() if seen is None else seen
+    path = os.path.normpath(path)
+    if path in seen or not os.path.exists(path):
+        return seen
+    seen.add(path)
+    with open(path) as fh:
+        for inc in _INCLUDE.findall(fh.read()):
+            local_deps(os.path.join(os.path.dirname(path), inc), seen)
+    return seen
+
+
+def newest_dep(src):
+    return max(os.path.getmtime(d) for d in local_deps(src))
 
 
 def obj_path(src):
@@ -50,9 +66,9 @@ def obj_path(src):
     return os.path.join(OUT_DIR, rel + ".o")
 
 
-def compile_one(src, hdr_time, verbose=False):
+def compile_one(src, verbose=False):
     obj = obj_path(src)
-    if os.path.exists(obj) and os.path.getmtime(obj) >= max(os.path.getmtime(src), hdr_time):
+    if os.path.exists(obj) and os.path.getmtime(obj) >= newest_dep(src):
         return obj, None
     cmd = [nvcc()] + NVCC_FLAGS + ["-c", src, "-o", obj]
     if src.endswith(".cpp"):
@@ -68,11 +84,10 @@ def compile_one(src, hdr_time, verbose=False):
 def build(jobs=None, verbose=False):
     os.makedirs(OUT_DIR, exist_ok=True)
     srcs = sources()
-    hdr = newest_header()
     jobs = jobs or os.cpu_count() or 4
     objs, errors = [], []
     with cf.ThreadPoolExecutor(max_workers=jobs) as ex:
-        for obj, err in ex.map(lambda s: compile_one(s, hdr, verbose), srcs):
+        for obj, err in ex.map(lambda s: compile_one(s, verbose), srcs):
             objs.append(obj)
             if err:
                 errors.append(err)
