@@ -2,6 +2,7 @@
 // E-coefficient kernel, Schwarz screening, the drivers (eri4 / eri4Diagonal / eri3 / eri2 /
 // eri2Diagonal, kernel-API batches, direct J/K, RI-J, J/K gradient) and their support kernels.
 #include "engine_api.hpp"
+#include "eri_kernel.cuh"  // operand pitches and the bounded barrier wait
 #include "eri_launch.cuh"
 
 #include <algorithm>

@@ -23,6 +23,7 @@
 #pragma once
 
 #include "device_common.cuh"
+#include "eri_kernel.cuh"  // DMMA fragment helpers and operand pitches
 
 namespace lible_b200
 {
@@ -714,5 +715,375 @@ namespace lible_b200
         for (int e = threadIdx.x; e < 3 * a.n_atoms; e += blockDim.x)
             if (sg[e] != 0.0)
                 atomicAdd(a.grad + e, sg[e]);
+    }
+
+    // ---------------------------------------------------------------------------------------
+    // Tensor-pipe form of the gradient contraction (kD1Grad, kD1GradRI) for the classes that are
+    // not register classes.  With GE = Gamma^T E_ab and GE1_x = Gamma^T E1_ab,x formed once per bra
+    // primitive, the seven ket-side products of a primitive quartet become traces
+    //   W0 = GE E_cd^T,  W1_x = GE1_x E_cd^T,  W2_x = GE E1_cd,x^T   ([H_ab x H_cd], K = S_cd)
+    //   t1_x  += sum_{h h'} W0[h][h'] s(h') R[h + h' + e_x],   t13_x += sum W1_x[h][h'] s(h') R[h + h'],
+    //   tc_x  += sum W2_x[h][h'] s(h') R[h + h'] - (c/q) sum W0[h][h'] s(h') R[h + h' + e_x]
+    // (s(h') = (-1)^{|h'|}, the terms of the register form above), so both the GE products
+    // (H_ab x S_cd, K = S_ab) and the W products run as mma.m8n8k4.f64 tiles on the DMMA pipe.  The
+    // accumulators of a W tile are consumed in registers: every lane gathers the R entries of its
+    // own two elements.  One block (WD warps) per quartet; R by the shared recursion to L + 1.
+    template <int LA, int LB, int LC, int LD>
+    struct ShapeD1M
+    {
+        using C = Cls<LA, LB, LC, LD>;
+        static constexpr int MT = (C::HAB + 7) / 8;                          // rows h of GE and W
+        static constexpr int NT1 = (C::SCD + 7) / 8, KT1 = (C::SAB + 3) / 4;  // GE: N = c, K = m
+        static constexpr int NT2 = (C::HCD + 7) / 8, KT2 = (C::SCD + 3) / 4;  // W: N = h', K = c
+        static constexpr int TILES1 = MT * NT1, TILES2 = MT * NT2;
+        static constexpr int WD0 = (TILES2 + 3) / 4;
+        static constexpr int WD = WD0 < 2 ? 2 : (WD0 > 8 ? 8 : WD0);
+        static constexpr int G = 32 * WD;
+        // operand tiles: E_ab staged [m][h] (A^T of the GE product, k-major), Gamma [m][c] (k-major
+        // B), GE [h][c] and E_cd [h'][c] (m-major A and B of the W product)
+        static constexpr int P_EA = kPitch(MT * 8), P_G = kPitch(NT1 * 8);
+        static constexpr int P_GE = mPitch(NT1 * 8 > KT2 * 4 ? NT1 * 8 : KT2 * 4), P_EC = mPitch(KT2 * 4);
+        static constexpr size_t a16(size_t x) { return (x + 15) / 16 * 16; }
+        static constexpr size_t off_rb = 0;                                               // 2 x NR1
+        static constexpr size_t off_ea = a16(off_rb + 8 * 2 * C::NR1);                    // KT1*4 x P_EA
+        static constexpr size_t off_g = a16(off_ea + 8 * (size_t)KT1 * 4 * P_EA);        // KT1*4 x P_G
+        static constexpr size_t off_ge = a16(off_g + 8 * (size_t)KT1 * 4 * P_G);         // 4 x MT*8 x P_GE
+        static constexpr size_t off_ec = a16(off_ge + 8 * 4 * (size_t)MT * 8 * P_GE);     // 4 x NT2*8 x P_EC
+        static constexpr size_t off_rd = a16(off_ec + 8 * 4 * (size_t)NT2 * 8 * P_EC);    // 9 x WD
+        static constexpr size_t off_ht = a16(off_rd + 8 * 9 * WD);                        // NR1 char4
+        static constexpr size_t off_hab = a16(off_ht + 4 * C::NR1);                       // HAB char4
+        static constexpr size_t off_hcd = a16(off_hab + 4 * C::HAB);                      // HCD char4
+        static constexpr size_t smem = a16(off_hcd + 4 * C::HCD);
+        // the classes this form serves, as measured on the (H2O)_8 cc-pVTZ gradient: not a register
+        // class, a ket of at least S_cd = 5 spherical and H_cd = 10 Hermite functions (with smaller
+        // kets the W products are too thin to pay for the GE products and the staging; (dd|ss), (fp|ss)
+        // and (dd|ps) ran up to 2.3x slower than in the block form), and a layout that fits one block
+        // per SM
+        static constexpr bool USE = !d1RegisterClass(LA, LB, LC, LD) && C::SCD >= 5 && C::HCD >= 10 &&
+                                    smem <= 200 * 1024;
+    };
+
+    template <int LA, int LB, int LC, int LD>
+    __global__ void __launch_bounds__(ShapeD1M<LA, LB, LC, LD>::G) eriD1MmaKernel(QuartetArgs a)
+    {
+        using C = Cls<LA, LB, LC, LD>;
+        using S = ShapeD1M<LA, LB, LC, LD>;
+        constexpr int G = S::G, WD = S::WD;
+        constexpr int L1 = C::L + 1;
+        extern __shared__ __align__(16) unsigned char smem[];
+        double *rb = reinterpret_cast<double *>(smem + S::off_rb);
+        double *ea = reinterpret_cast<double *>(smem + S::off_ea);
+        double *gs = reinterpret_cast<double *>(smem + S::off_g);
+        double *ge = reinterpret_cast<double *>(smem + S::off_ge);
+        double *ec = reinterpret_cast<double *>(smem + S::off_ec);
+        double *red = reinterpret_cast<double *>(smem + S::off_rd);
+        char4 *ht = reinterpret_cast<char4 *>(smem + S::off_ht);
+        char4 *hab = reinterpret_cast<char4 *>(smem + S::off_hab);
+        char4 *hcd = reinterpret_cast<char4 *>(smem + S::off_hcd);
+        const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, r8 = lane >> 2, k4 = lane & 3;
+        constexpr size_t GE_SZ = (size_t)S::MT * 8 * S::P_GE, EC_SZ = (size_t)S::NT2 * 8 * S::P_EC;
+
+        // once per block: zero every operand tile (padding rows and columns are never written
+        // afterwards, so they stay zero) and the Hermite (t, u, v, order) tables
+        {
+            const int nz = (int)((S::off_rd - S::off_ea) / 8);
+            for (int e = tid; e < nz; e += G)
+                ea[e] = 0.0;
+            for (int e = tid; e < C::NR1; e += G)
+            {
+                int t, u, v;
+                hermTuv(e, t, u, v);
+                ht[e] = make_char4((char)t, (char)u, (char)v, (char)(t + u + v));
+            }
+            for (int e = tid; e < C::HAB; e += G)
+            {
+                int t, u, v;
+                hermTuv(e, t, u, v);
+                hab[e] = make_char4((char)t, (char)u, (char)v, 0);
+            }
+            for (int e = tid; e < C::HCD; e += G)
+            {
+                int t, u, v;
+                hermTuv(e, t, u, v);
+                hcd[e] = make_char4((char)t, (char)u, (char)v, (char)((t + u + v) & 1));
+            }
+        }
+        __syncthreads();
+
+        auto processTask = [&](uint32_t ib, uint32_t ik) {
+            const int32_t *bi = a.bra.info + 8 * ib;
+            const int32_t *ki = a.ket.info + 8 * ik;
+            // Gamma[m][c] of the quartet (as in the block kernel's epilogues)
+            {
+                const int n = a.nao;
+                const double *D = a.D;
+                double w = 0.0;
+                if (a.mode == kD1GradRI)
+                {
+                    const int32_t *mi = a.aux_side == 0 ? bi : ki;
+                    w = a.aux_side == 2 ? -((a.same_class && ib == ik) ? 0.5 : 1.0) : (mi[4] == mi[5] ? 1.0 : 2.0);
+                }
+                else
+                    w = quartetWeight(a, ib, ik);
+                for (int e = tid; e < C::SAB * C::SCD; e += G)
+                {
+                    const int m = e / C::SCD, c = e % C::SCD;
+                    double v;
+                    if (a.mode == kD1GradRI)
+                    {
+                        if (a.aux_side == 2)
+                            v = __ldg(a.dcoef + bi[0] + m) * __ldg(a.dcoef + ki[0] + c);
+                        else if (a.aux_side == 0)
+                            v = __ldg(D + (size_t)(bi[0] + m / C::SB) * n + bi[1] + m % C::SB) * __ldg(a.dcoef + ki[0] + c);
+                        else
+                            v = __ldg(D + (size_t)(ki[0] + c / C::SD) * n + ki[1] + c % C::SD) * __ldg(a.dcoef + bi[0] + m);
+                    }
+                    else
+                    {
+                        const size_t mu = bi[0] + m / C::SB, nu = bi[1] + m % C::SB;
+                        const size_t ka = ki[0] + c / C::SD, ta = ki[1] + c % C::SD;
+                        v = 4.0 * __ldg(D + mu * n + nu) * __ldg(D + ka * n + ta) - __ldg(D + mu * n + ka) * __ldg(D + nu * n + ta) -
+                            __ldg(D + mu * n + ta) * __ldg(D + nu * n + ka);
+                    }
+                    gs[m * S::P_G + c] = w * v;
+                }
+            }
+            double g[9];
+#pragma unroll
+            for (int x = 0; x < 9; x++)
+                g[x] = 0.0;
+            const uint32_t p0 = a.bra.pofs[ib], p1 = a.bra.pofs[ib + 1];
+            const uint32_t q0 = a.ket.pofs[ik], q1 = a.ket.pofs[ik + 1];
+            for (uint32_t p = p0; p < p1; p++)
+            {
+                const PQ4 P = loadPQ(a.bra.pP, p);
+                const double2 AB = __ldg(reinterpret_cast<const double2 *>(a.bra.ab) + p);
+                // GE (x4 = 0) and GE1_x (x4 = 1..3) = E^T Gamma, one staged E matrix at a time
+                for (int x4 = 0; x4 < 4; x4++)
+                {
+                    const double *src = x4 == 0 ? a.bra.E + (size_t)p * C::SAB * C::HAB
+                                                : a.bra.E1 + ((size_t)p * 3 + (x4 - 1)) * C::SAB * C::HAB;
+                    __syncthreads();  // the previous product has read ea (and, first time, gs is written)
+                    for (int e = tid; e < C::SAB * C::HAB; e += G)
+                        ea[(e / C::HAB) * S::P_EA + e % C::HAB] = __ldg(src + e);
+                    __syncthreads();
+                    double *out = ge + x4 * GE_SZ;
+                    for (int t = warp; t < S::TILES1; t += WD)
+                    {
+                        const int mt = t / S::NT1, nt = t % S::NT1;
+                        double d0 = 0.0, d1 = 0.0;
+                        const double *A = ea + k4 * S::P_EA + mt * 8 + r8;
+                        const double *B = gs + k4 * S::P_G + nt * 8 + r8;
+#pragma unroll 4
+                        for (int ks = 0; ks < S::KT1; ks++)
+                            dmma8x8x4(d0, d1, A[ks * 4 * S::P_EA], B[ks * 4 * S::P_G]);
+                        double *o = out + (mt * 8 + r8) * S::P_GE + nt * 8 + 2 * k4;
+                        o[0] = d0;
+                        o[1] = d1;
+                    }
+                }
+                double t1[3] = {0, 0, 0}, t13[3] = {0, 0, 0}, tc[3] = {0, 0, 0};
+                for (uint32_t q = q0; q < q1; q++)
+                {
+                    const PQ4 Q = loadPQ(a.ket.pP, q);
+                    const double cq = __ldg(a.ket.ab + 2 * q) / Q.x;
+                    const double rs = rsqrt(P.x + Q.x);
+                    const double alpha = P.x * Q.x * (rs * rs);
+                    const double X = P.y - Q.y, Y = P.z - Q.z, Z = P.w - Q.w;
+                    const double fac = 34.986836655249725 * rs * P.ip * Q.ip;
+                    double F[L1 + 1];
+                    boysF<L1, false>(alpha * (X * X + Y * Y + Z * Z), a.boys + L1 * kBoysTerms * kBoysPitch, F);
+                    const double m2a = -2.0 * alpha;
+                    __syncthreads();  // the previous primitive's R and E tiles are no longer read
+                    // ket E and E1 tiles [h'][c]
+                    {
+                        const double *ecd = a.ket.Et + (size_t)q * C::HCD * C::SCD;
+                        const double *e1cd = a.ket.E1t + (size_t)q * 3 * C::HCD * C::SCD;
+                        for (int e = tid; e < C::HCD * C::SCD; e += G)
+                        {
+                            const int o = (e / C::SCD) * S::P_EC + e % C::SCD;
+                            ec[o] = __ldg(ecd + e);
+                            ec[EC_SZ + o] = __ldg(e1cd + e);
+                            ec[2 * EC_SZ + o] = __ldg(e1cd + C::HCD * C::SCD + e);
+                            ec[3 * EC_SZ + o] = __ldg(e1cd + 2 * C::HCD * C::SCD + e);
+                        }
+                    }
+                    // R to order L + 1 (levels split over the block)
+                    double *cur = rb, *nxt = rb + C::NR1;
+                    if (tid == 0)
+                    {
+                        double pw = 1.0;
+                        for (int k = 0; k < L1; k++)
+                            pw *= m2a;
+                        cur[0] = F[L1] * fac * pw;
+                    }
+                    __syncthreads();
+#pragma unroll
+                    for (int nl = L1 - 1; nl >= 0; nl--)
+                    {
+                        const int cnt = nherm(L1 - nl);
+                        for (int e = tid; e < cnt; e += G)
+                        {
+                            double r;
+                            if (e == 0)
+                            {
+                                double pn = 1.0;
+                                for (int k = 0; k < nl; k++)
+                                    pn *= m2a;
+                                r = F[nl] * fac * pn;
+                            }
+                            else
+                            {
+                                const char4 tv = ht[e];
+                                const int t = tv.x, u = tv.y, v = tv.z, m = tv.w;
+                                if (t > 0)
+                                {
+                                    r = X * cur[nherm(m - 2) + cartIndex(u, v)];
+                                    if (t > 1)
+                                        r += (t - 1) * cur[nherm(m - 3) + cartIndex(u, v)];
+                                }
+                                else if (u > 0)
+                                {
+                                    r = Y * cur[nherm(m - 2) + cartIndex(u - 1, v)];
+                                    if (u > 1)
+                                        r += (u - 1) * cur[nherm(m - 3) + cartIndex(u - 2, v)];
+                                }
+                                else
+                                {
+                                    r = Z * cur[nherm(m - 2) + cartIndex(0, v - 1)];
+                                    if (v > 1)
+                                        r += (v - 1) * cur[nherm(m - 3) + cartIndex(0, v - 2)];
+                                }
+                            }
+                            nxt[e] = r;
+                        }
+                        __syncthreads();
+                        double *tmp = cur;
+                        cur = nxt;
+                        nxt = tmp;
+                    }
+                    // the seven W products per tile, consumed in registers
+                    double ax = 0, ay = 0, az = 0, c2x = 0, c2y = 0, c2z = 0;
+                    for (int t = warp; t < S::TILES2; t += WD)
+                    {
+                        const int mt = t / S::NT2, nt = t % S::NT2;
+                        double w[7][2];
+#pragma unroll
+                        for (int k = 0; k < 7; k++)
+                            w[k][0] = w[k][1] = 0.0;
+                        const double *A = ge + (mt * 8 + r8) * S::P_GE + k4;
+                        const double *B = ec + (nt * 8 + r8) * S::P_EC + k4;
+#pragma unroll 2
+                        for (int ks = 0; ks < S::KT2; ks++)
+                        {
+                            const double a0 = A[ks * 4], a1 = A[GE_SZ + ks * 4], a2 = A[2 * GE_SZ + ks * 4],
+                                         a3 = A[3 * GE_SZ + ks * 4];
+                            const double b0 = B[ks * 4], b1 = B[EC_SZ + ks * 4], b2 = B[2 * EC_SZ + ks * 4],
+                                         b3 = B[3 * EC_SZ + ks * 4];
+                            dmma8x8x4(w[0][0], w[0][1], a0, b0);
+                            dmma8x8x4(w[1][0], w[1][1], a1, b0);
+                            dmma8x8x4(w[2][0], w[2][1], a2, b0);
+                            dmma8x8x4(w[3][0], w[3][1], a3, b0);
+                            dmma8x8x4(w[4][0], w[4][1], a0, b1);
+                            dmma8x8x4(w[5][0], w[5][1], a0, b2);
+                            dmma8x8x4(w[6][0], w[6][1], a0, b3);
+                        }
+                        const int h = mt * 8 + r8;
+                        if (h < C::HAB)
+                        {
+                            const char4 th = hab[h];
+#pragma unroll
+                            for (int j = 0; j < 2; j++)
+                            {
+                                const int hp = nt * 8 + 2 * k4 + j;
+                                if (hp < C::HCD)
+                                {
+                                    const char4 tp = hcd[hp];
+                                    const int tt = th.x + tp.x, uu = th.y + tp.y, vv = th.z + tp.z;
+                                    const double sg = tp.w ? -1.0 : 1.0;
+                                    const double r0 = sg * cur[hermIndex(tt, uu, vv)];
+                                    const double rx = sg * cur[hermIndex(tt + 1, uu, vv)];
+                                    const double ry = sg * cur[hermIndex(tt, uu + 1, vv)];
+                                    const double rz = sg * cur[hermIndex(tt, uu, vv + 1)];
+                                    ax += w[0][j] * rx;
+                                    ay += w[0][j] * ry;
+                                    az += w[0][j] * rz;
+                                    t13[0] += w[1][j] * r0;
+                                    t13[1] += w[2][j] * r0;
+                                    t13[2] += w[3][j] * r0;
+                                    c2x += w[4][j] * r0;
+                                    c2y += w[5][j] * r0;
+                                    c2z += w[6][j] * r0;
+                                }
+                            }
+                        }
+                    }
+                    t1[0] += ax;
+                    t1[1] += ay;
+                    t1[2] += az;
+                    tc[0] += c2x - cq * ax;
+                    tc[1] += c2y - cq * ay;
+                    tc[2] += c2z - cq * az;
+                }
+                const double ap = AB.x * P.ip, bp = AB.y * P.ip;
+#pragma unroll
+                for (int x = 0; x < 3; x++)
+                {
+                    g[x] += ap * t1[x] + t13[x];
+                    g[3 + x] += bp * t1[x] - t13[x];
+                    g[6 + x] += tc[x];
+                }
+            }
+            // the 9 sums over the block, then per atom (D by translational invariance)
+#pragma unroll
+            for (int x = 0; x < 9; x++)
+            {
+                double v = g[x];
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1)
+                    v += __shfl_down_sync(0xffffffffu, v, o);
+                if (lane == 0)
+                    red[warp * 9 + x] = v;
+            }
+            __syncthreads();
+            if (tid < 9)
+            {
+                double v = 0.0;
+                for (int w = 0; w < WD; w++)
+                    v += red[w * 9 + tid];
+                const int centre = tid / 3, x = tid % 3;
+                const int atom = centre == 0 ? bi[2] : centre == 1 ? bi[3] : ki[2];
+                atomicAdd(a.grad + 3 * atom + x, v);
+                atomicAdd(a.grad + 3 * ki[3] + x, -v);
+            }
+            __syncthreads();
+        };
+
+        auto runTask = [&](long long task) {
+            uint32_t ib, ik;
+            decodeTask(a, task, ib, ik);
+            if (inWindow(a, ib, ik, 0, false))
+                processTask(ib, ik);
+        };
+        if (a.chunks)
+        {
+            __shared__ unsigned long long claimed;
+            for (;;)
+            {
+                if (tid == 0)
+                    claimed = atomicAdd(a.counter, 1ULL);
+                __syncthreads();
+                const unsigned long long c = claimed;
+                __syncthreads();
+                if (c >= (unsigned long long)a.n_chunks)
+                    break;
+                const long long t1 = (long long)__ldg(a.chunks + c + 1);
+                for (long long t = (long long)__ldg(a.chunks + c); t < t1; t++)
+                    runTask(t);
+            }
+        }
+        else
+            for (long long task = blockIdx.x; task < a.n_tasks; task += gridDim.x)
+                runTask(task);
     }
 }

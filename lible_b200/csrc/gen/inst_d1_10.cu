@@ -1,5 +1,5 @@
 // Generated by gen_instances.py: class kernels with bra pair type (4,0).
-#include "../eri_launch.cuh"
+#include "../eri_launch_d1.cuh"
 
 namespace lible_b200
 {

@@ -1,0 +1,24 @@
+// Generated by gen_instances.py: class kernels with bra pair type (3,0).
+#include "../eri_launch_fwd.cuh"
+
+namespace lible_b200
+{
+    extern const LaunchFn k_fwd32_06[7] = {
+        &launchFwd<3,0,0,0,float>,
+        &launchFwd<3,0,1,0,float>,
+        &launchFwd<3,0,1,1,float>,
+        &launchFwd<3,0,2,0,float>,
+        &launchFwd<3,0,2,1,float>,
+        &launchFwd<3,0,2,2,float>,
+        &launchFwd<3,0,3,0,float>,
+    };
+    extern const int u_fwd32_06[7] = {
+        workUnit<3,0,0,0,float>(),
+        workUnit<3,0,1,0,float>(),
+        workUnit<3,0,1,1,float>(),
+        workUnit<3,0,2,0,float>(),
+        workUnit<3,0,2,1,float>(),
+        workUnit<3,0,2,2,float>(),
+        workUnit<3,0,3,0,float>(),
+    };
+}

@@ -1,5 +1,5 @@
 // Generated by gen_instances.py: class kernels with bra pair type (3,2).
-#include "../eri_launch.cuh"
+#include "../eri_launch_fwd.cuh"
 
 namespace lible_b200
 {

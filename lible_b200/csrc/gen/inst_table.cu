@@ -41,8 +41,16 @@ namespace lible_b200
     extern const int u_fwd32_04[5];
     extern const LaunchFn k_fwd32_05[6];
     extern const int u_fwd32_05[6];
-    static const int *const u_fwd32[6] = {u_fwd32_00, u_fwd32_01, u_fwd32_02, u_fwd32_03, u_fwd32_04, u_fwd32_05};
-    static const LaunchFn *const k_fwd32[6] = {k_fwd32_00, k_fwd32_01, k_fwd32_02, k_fwd32_03, k_fwd32_04, k_fwd32_05};
+    extern const LaunchFn k_fwd32_06[7];
+    extern const int u_fwd32_06[7];
+    extern const LaunchFn k_fwd32_07[8];
+    extern const int u_fwd32_07[8];
+    extern const LaunchFn k_fwd32_08[9];
+    extern const int u_fwd32_08[9];
+    extern const LaunchFn k_fwd32_09[10];
+    extern const int u_fwd32_09[10];
+    static const int *const u_fwd32[10] = {u_fwd32_00, u_fwd32_01, u_fwd32_02, u_fwd32_03, u_fwd32_04, u_fwd32_05, u_fwd32_06, u_fwd32_07, u_fwd32_08, u_fwd32_09};
+    static const LaunchFn *const k_fwd32[10] = {k_fwd32_00, k_fwd32_01, k_fwd32_02, k_fwd32_03, k_fwd32_04, k_fwd32_05, k_fwd32_06, k_fwd32_07, k_fwd32_08, k_fwd32_09};
     extern const LaunchFn k_d1_00[1];
     extern const LaunchFn k_d1_01[2];
     extern const LaunchFn k_d1_02[3];
@@ -64,7 +72,7 @@ namespace lible_b200
     }
     LaunchFn lookupFwd32(int bt, int kt)
     {
-        if (bt < 0 || bt >= 6 || kt < 0 || kt > bt)
+        if (bt < 0 || bt >= 10 || kt < 0 || kt > bt)
             return nullptr;
         return k_fwd32[bt][kt];
     }
@@ -76,7 +84,7 @@ namespace lible_b200
     }
     int unitFwd(int bt, int kt, bool fp32)
     {
-        if (bt < 0 || kt < 0 || kt > bt || bt >= (fp32 ? 6 : 12))
+        if (bt < 0 || kt < 0 || kt > bt || bt >= (fp32 ? 10 : 12))
             return 0;
         return fp32 ? u_fwd32[bt][kt] : u_fwd64[bt][kt];
     }

@@ -32,7 +32,8 @@ def main():
                 entries.append("&" + tmpl.format(la=la, lb=lb, lc=lc, ld=ld))
             name = f"inst_{kind}_{bt:02d}.cu"
             body = ['// Generated by gen_instances.py: class kernels with bra pair type '
-                    f'({la},{lb}).', '#include "../eri_launch.cuh"', '', 'namespace lible_b200', '{',
+                    f'({la},{lb}).', '#include "../%s"' % ("eri_launch_d1.cuh" if kind == "d1" else "eri_launch_fwd.cuh"),
+                    '', 'namespace lible_b200', '{',
                     f'    extern const LaunchFn k_{kind}_{bt:02d}[{bt + 1}] = {{']
             body += [f'        {e},' for e in entries]
             body += ['    };']
