@@ -20,7 +20,7 @@ CSRC = os.path.join(HERE, "csrc")
 OUT_DIR = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "liblible_b200.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-NVCC_FLAGS = ARCH + ["-lineinfo", "-O3", "-std=c++17", "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC",
+NVCC_FLAGS = ARCH + ["-lineinfo", "-O3", "-std=c++20", "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC",
                      "-Xcompiler", "-O3", "-I" + CSRC]
 
 
@@ -83,6 +83,14 @@ def compile_one(src, verbose=False):
 
 def build(jobs=None, verbose=False):
     os.makedirs(OUT_DIR, exist_ok=True)
+    # objects built with other flags are stale
+    stamp = os.path.join(OUT_DIR, "flags.txt")
+    flags = " ".join(NVCC_FLAGS)
+    if not os.path.exists(stamp) or open(stamp).read() != flags:
+        for o in glob.glob(os.path.join(OUT_DIR, "*.o")):
+            os.remove(o)
+        with open(stamp, "w") as fh:
+            fh.write(flags)
     srcs = sources()
     jobs = jobs or os.cpu_count() or 4
     objs, errors = [], []
