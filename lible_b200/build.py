@@ -101,6 +101,9 @@ def build(jobs=None, verbose=False):
                 errors.append(err)
     if errors:
         raise RuntimeError("nvcc failed:\n" + "\n".join(errors)[:20000])
+    for o in glob.glob(os.path.join(OUT_DIR, "*.o")):
+        if o not in objs:
+            os.remove(o)  # object of a source that no longer exists
     if not os.path.exists(LIB) or os.path.getmtime(LIB) < max(os.path.getmtime(o) for o in objs):
         cmd = [nvcc()] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart", "-lcusolver", "-lcublas"]
         r = subprocess.run(cmd, capture_output=True, text=True)

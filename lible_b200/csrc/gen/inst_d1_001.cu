@@ -1,0 +1,18 @@
+// Generated by gen_instances.py: class kernels (1,1|0,0), (1,1|1,0), (1,1|1,1).
+#include "../eri_launch_d1.cuh"
+
+namespace lible_b200
+{
+    cudaError_t launch_d1_02_00(const QuartetArgs &a, cudaStream_t s, int n)
+    {
+        return launchD1<1,1,0,0>(a, s, n);
+    }
+    cudaError_t launch_d1_02_01(const QuartetArgs &a, cudaStream_t s, int n)
+    {
+        return launchD1<1,1,1,0>(a, s, n);
+    }
+    cudaError_t launch_d1_02_02(const QuartetArgs &a, cudaStream_t s, int n)
+    {
+        return launchD1<1,1,1,1>(a, s, n);
+    }
+}

@@ -1,0 +1,18 @@
+// Generated by gen_instances.py: class kernels (2,0|2,0), (2,1|0,0), (2,1|1,0).
+#include "../eri_launch_d1.cuh"
+
+namespace lible_b200
+{
+    cudaError_t launch_d1_03_03(const QuartetArgs &a, cudaStream_t s, int n)
+    {
+        return launchD1<2,0,2,0>(a, s, n);
+    }
+    cudaError_t launch_d1_04_00(const QuartetArgs &a, cudaStream_t s, int n)
+    {
+        return launchD1<2,1,0,0>(a, s, n);
+    }
+    cudaError_t launch_d1_04_01(const QuartetArgs &a, cudaStream_t s, int n)
+    {
+        return launchD1<2,1,1,0>(a, s, n);
+    }
+}

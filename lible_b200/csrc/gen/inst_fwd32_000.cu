@@ -1,0 +1,14 @@
+// Generated by gen_instances.py: class kernels (0,0|0,0), (1,0|0,0).
+#include "../eri_launch_fwd.cuh"
+
+namespace lible_b200
+{
+    cudaError_t launch_fwd32_00_00(const QuartetArgs &a, cudaStream_t s, int n)
+    {
+        return launchFwd<0,0,0,0,float>(a, s, n);
+    }
+    cudaError_t launch_fwd32_01_00(const QuartetArgs &a, cudaStream_t s, int n)
+    {
+        return launchFwd<1,0,0,0,float>(a, s, n);
+    }
+}

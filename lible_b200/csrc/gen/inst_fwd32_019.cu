@@ -1,0 +1,14 @@
+// Generated by gen_instances.py: class kernels (3,2|1,1), (3,2|2,0).
+#include "../eri_launch_fwd.cuh"
+
+namespace lible_b200
+{
+    cudaError_t launch_fwd32_08_02(const QuartetArgs &a, cudaStream_t s, int n)
+    {
+        return launchFwd<3,2,1,1,float>(a, s, n);
+    }
+    cudaError_t launch_fwd32_08_03(const QuartetArgs &a, cudaStream_t s, int n)
+    {
+        return launchFwd<3,2,2,0,float>(a, s, n);
+    }
+}

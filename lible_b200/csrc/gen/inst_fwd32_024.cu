@@ -1,0 +1,14 @@
+// Generated by gen_instances.py: class kernels (3,3|2,0), (3,3|2,1).
+#include "../eri_launch_fwd.cuh"
+
+namespace lible_b200
+{
+    cudaError_t launch_fwd32_09_03(const QuartetArgs &a, cudaStream_t s, int n)
+    {
+        return launchFwd<3,3,2,0,float>(a, s, n);
+    }
+    cudaError_t launch_fwd32_09_04(const QuartetArgs &a, cudaStream_t s, int n)
+    {
+        return launchFwd<3,3,2,1,float>(a, s, n);
+    }
+}

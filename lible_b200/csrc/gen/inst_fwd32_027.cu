@@ -1,0 +1,10 @@
+// Generated by gen_instances.py: class kernels (3,3|3,3).
+#include "../eri_launch_fwd.cuh"
+
+namespace lible_b200
+{
+    cudaError_t launch_fwd32_09_09(const QuartetArgs &a, cudaStream_t s, int n)
+    {
+        return launchFwd<3,3,3,3,float>(a, s, n);
+    }
+}

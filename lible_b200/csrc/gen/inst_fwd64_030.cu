@@ -1,0 +1,14 @@
+// Generated by gen_instances.py: class kernels (4,0|2,2), (4,0|3,0).
+#include "../eri_launch_fwd.cuh"
+
+namespace lible_b200
+{
+    cudaError_t launch_fwd64_10_05(const QuartetArgs &a, cudaStream_t s, int n)
+    {
+        return launchFwd<4,0,2,2,double>(a, s, n);
+    }
+    cudaError_t launch_fwd64_10_06(const QuartetArgs &a, cudaStream_t s, int n)
+    {
+        return launchFwd<4,0,3,0,double>(a, s, n);
+    }
+}

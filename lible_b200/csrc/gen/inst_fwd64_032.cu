@@ -1,0 +1,14 @@
+// Generated by gen_instances.py: class kernels (4,0|3,3), (4,0|4,0).
+#include "../eri_launch_fwd.cuh"
+
+namespace lible_b200
+{
+    cudaError_t launch_fwd64_10_09(const QuartetArgs &a, cudaStream_t s, int n)
+    {
+        return launchFwd<4,0,3,3,double>(a, s, n);
+    }
+    cudaError_t launch_fwd64_10_10(const QuartetArgs &a, cudaStream_t s, int n)
+    {
+        return launchFwd<4,0,4,0,double>(a, s, n);
+    }
+}

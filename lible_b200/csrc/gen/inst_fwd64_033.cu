@@ -1,0 +1,14 @@
+// Generated by gen_instances.py: class kernels (5,0|0,0), (5,0|1,0).
+#include "../eri_launch_fwd.cuh"
+
+namespace lible_b200
+{
+    cudaError_t launch_fwd64_11_00(const QuartetArgs &a, cudaStream_t s, int n)
+    {
+        return launchFwd<5,0,0,0,double>(a, s, n);
+    }
+    cudaError_t launch_fwd64_11_01(const QuartetArgs &a, cudaStream_t s, int n)
+    {
+        return launchFwd<5,0,1,0,double>(a, s, n);
+    }
+}

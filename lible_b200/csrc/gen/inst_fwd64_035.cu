@@ -1,0 +1,14 @@
+// Generated by gen_instances.py: class kernels (5,0|2,1), (5,0|2,2).
+#include "../eri_launch_fwd.cuh"
+
+namespace lible_b200
+{
+    cudaError_t launch_fwd64_11_04(const QuartetArgs &a, cudaStream_t s, int n)
+    {
+        return launchFwd<5,0,2,1,double>(a, s, n);
+    }
+    cudaError_t launch_fwd64_11_05(const QuartetArgs &a, cudaStream_t s, int n)
+    {
+        return launchFwd<5,0,2,2,double>(a, s, n);
+    }
+}

@@ -1,8 +1,9 @@
 """Writes the per-class kernel instantiation files under lible_b200/csrc/gen/.
 
-One file per (kernel kind, bra pair type) keeps each nvcc invocation small so the build can run
-in parallel.  A quartet class is always instantiated with the larger pair type in the bra; the
-host swaps bra and ket (and transposes the output) for the other orientation.
+Each file holds a small group of classes of one kernel kind, so the build runs in parallel;
+inst_table.cu maps (bra pair type, ket pair type) to the launch wrappers.  A quartet class is
+always instantiated with the larger pair type in the bra; the host swaps bra and ket (and
+transposes the output) for the other orientation.
 """
 import os
 
@@ -16,44 +17,51 @@ def kinds():
     yield "d1", "launchD1<{la},{lb},{lc},{ld}>", len(PAIR_TYPES)
 
 
+# classes per generated file: small groups keep every nvcc invocation short, so a rebuild spreads
+# over all cores instead of waiting on the files of the largest bra types
+GROUP = {"fwd64": 2, "fwd32": 2, "d1": 3}
+
+
 def main():
     here = os.path.dirname(os.path.abspath(__file__))
     out = os.path.join(here, "gen")
     os.makedirs(out, exist_ok=True)
     written = []
     table = ['// Generated by gen_instances.py: lookup of class kernels.',
-             '#include "../eri_launch.cuh"', '', 'namespace lible_b200', '{']
+             '#include "../eri_launch_fwd.cuh"', '', 'namespace lible_b200', '{']
     for kind, tmpl, ntypes in kinds():
-        for bt in range(ntypes):
-            la, lb = PAIR_TYPES[bt]
-            entries = []
-            for kt in range(bt + 1):
+        launcher = "launchD1" if kind == "d1" else "launchFwd"
+        T = {"fwd64": ",double", "fwd32": ",float", "d1": ""}[kind]
+        classes = [(bt, kt) for bt in range(ntypes) for kt in range(bt + 1)]
+        name_of = lambda bt, kt: f"launch_{kind}_{bt:02d}_{kt:02d}"
+        for g in range(0, len(classes), GROUP[kind]):
+            part = classes[g:g + GROUP[kind]]
+            body = ['// Generated by gen_instances.py: class kernels ' +
+                    ", ".join("(%d,%d|%d,%d)" % (PAIR_TYPES[bt] + PAIR_TYPES[kt]) for bt, kt in part) + '.',
+                    '#include "../%s"' % ("eri_launch_d1.cuh" if kind == "d1" else "eri_launch_fwd.cuh"),
+                    '', 'namespace lible_b200', '{']
+            for bt, kt in part:
+                la, lb = PAIR_TYPES[bt]
                 lc, ld = PAIR_TYPES[kt]
-                entries.append("&" + tmpl.format(la=la, lb=lb, lc=lc, ld=ld))
-            name = f"inst_{kind}_{bt:02d}.cu"
-            body = ['// Generated by gen_instances.py: class kernels with bra pair type '
-                    f'({la},{lb}).', '#include "../%s"' % ("eri_launch_d1.cuh" if kind == "d1" else "eri_launch_fwd.cuh"),
-                    '', 'namespace lible_b200', '{',
-                    f'    extern const LaunchFn k_{kind}_{bt:02d}[{bt + 1}] = {{']
-            body += [f'        {e},' for e in entries]
-            body += ['    };']
-            if kind.startswith("fwd"):
-                T = "double" if kind == "fwd64" else "float"
-                body += [f'    extern const int u_{kind}_{bt:02d}[{bt + 1}] = {{']
-                for kt in range(bt + 1):
-                    lc, ld = PAIR_TYPES[kt]
-                    body.append(f'        workUnit<{la},{lb},{lc},{ld},{T}>(),')
-                body += ['    };']
+                body += [f'    cudaError_t {name_of(bt, kt)}(const QuartetArgs &a, cudaStream_t s, int n)',
+                         '    {', f'        return {launcher}<{la},{lb},{lc},{ld}{T}>(a, s, n);', '    }']
             body += ['}', '']
+            name = f"inst_{kind}_{g // GROUP[kind]:03d}.cu"
             path = os.path.join(out, name)
             text = "\n".join(body)
             if not os.path.exists(path) or open(path).read() != text:
                 with open(path, "w") as fh:
                     fh.write(text)
             written.append(name)
-            table.append(f'    extern const LaunchFn k_{kind}_{bt:02d}[{bt + 1}];')
+        table += [f'    cudaError_t {name_of(bt, kt)}(const QuartetArgs &, cudaStream_t, int);' for bt, kt in classes]
+        for bt in range(ntypes):
+            la, lb = PAIR_TYPES[bt]
+            table.append(f'    static const LaunchFn k_{kind}_{bt:02d}[{bt + 1}] = {{' +
+                         ", ".join(f"&{name_of(bt, kt)}" for kt in range(bt + 1)) + '};')
             if kind.startswith("fwd"):
-                table.append(f'    extern const int u_{kind}_{bt:02d}[{bt + 1}];')
+                table.append(f'    static const int u_{kind}_{bt:02d}[{bt + 1}] = {{' +
+                             ", ".join(f"workUnit<{la},{lb},{PAIR_TYPES[kt][0]},{PAIR_TYPES[kt][1]}{T}>()"
+                                       for kt in range(bt + 1)) + '};')
         if kind.startswith("fwd"):
             table.append(f'    static const int *const u_{kind}[{ntypes}] = {{' +
                          ", ".join(f"u_{kind}_{bt:02d}" for bt in range(ntypes)) + '};')
@@ -74,6 +82,10 @@ def main():
         with open(path, "w") as fh:
             fh.write(text)
     written.append("inst_table.cu")
+    # drop files of an earlier grouping
+    for f in os.listdir(out):
+        if f.endswith(".cu") and f not in written:
+            os.remove(os.path.join(out, f))
     return [os.path.join(out, w) for w in written]
 
 
