@@ -31,9 +31,9 @@ SCHWARZ, FP32_THR = 1e-12, 1e-4
 # DRAM bytes (read + write) per launch of the dominant class kernels at this workload, from one ncu
 # capture each (dram__bytes_read.sum + dram__bytes_write.sum); the working set stays in L2
 DOMINANT_TRAFFIC = {((1, 0, 0, 0), False): 34.29e6, ((2, 1, 1, 0), False): 24.16e6}
-# L2 atomic (RED) bytes per launch of the dominant FP64 kernel, lts__t_sectors_op_red.sum x 32 from one
-# ncu capture of this workload (profiles/)
-L2_ATOMIC_BYTES = {}
+# L2 atomic (RED) bytes per launch of the dominant kernels, lts__t_sectors_op_red.sum x 32 from one
+# ncu capture each of this workload (profiles/)
+L2_ATOMIC_BYTES = {"eriKernelOcc<1,0,0,0,double>": 1222249650 * 32, "eriKernel<1,0,0,0,float>": 1107513230 * 32}
 # classes compiled with a raised occupancy bound (eriKernelOcc, minBlocksPerSM in
 # lible_b200/csrc/eri_kernel.cuh): (class, fp32) -> kernel name
 OCC_KERNELS = {(c, f): "eriKernelOcc" for c, f in [((2, 1, 1, 0), False), ((2, 0, 1, 0), False), ((2, 1, 0, 0), False),
@@ -580,6 +580,9 @@ def main():
                  "mixed_gbs": dig_b / (tmx * 1e-3) / 1e9, "hbm_gbs": hbm, "hbm_source": hbm_src,
                  "fp64_frac_of_hbm": dig_b / (t64 * 1e-3) / 1e9 / hbm,
                  "l2_atomic_bytes_fp64_dominant_launch": L2_ATOMIC_BYTES.get(roof64["kernel"]),
+                 "l2_atomic_bytes_headline_dominant_launch": L2_ATOMIC_BYTES.get(roof_head["kernel"]),
+                 "l2_atomic_source": "ncu lts__t_sectors_op_red.sum x 32 B, one launch "
+                                     "(profiles/jk_digestion_atomics_h2o32_dz.md)",
                  "definition": "per unique quartet 8 B per D-block element read + 16 B per J/K-block element updated, "
                                "blocks ab, cd, ac, ad, bc, bd"}
     out = {
