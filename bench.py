@@ -30,13 +30,13 @@ N_WATERS, SEED, OCC = 32, 2024, 160
 SCHWARZ, FP32_THR = 1e-12, 1e-4
 # DRAM bytes (read + write) per launch of the dominant class kernels at this workload, from one ncu
 # capture each (dram__bytes_read.sum + dram__bytes_write.sum); the working set stays in L2
-DOMINANT_TRAFFIC = {((1, 0, 0, 0), False): 34.29e6, ((2, 1, 1, 0), False): 24.16e6}
+DOMINANT_TRAFFIC = {((1, 0, 0, 0), False): 34.29e6, ((2, 1, 1, 0), False): 24.16e6, ((1, 0, 0, 0), True): 28.35e6}
 # L2 atomic (RED) bytes per launch of the dominant kernels, lts__t_sectors_op_red.sum x 32 from one
 # ncu capture each of this workload (profiles/)
-L2_ATOMIC_BYTES = {"eriKernelOcc<1,0,0,0,double>": 1222249650 * 32, "eriKernel<1,0,0,0,float>": 1107513230 * 32}
-# classes compiled with a raised occupancy bound (eriKernelOcc, minBlocksPerSM in
-# lible_b200/csrc/eri_kernel.cuh): (class, fp32) -> kernel name
-OCC_KERNELS = {(c, f): "eriKernelOcc" for c, f in [((2, 1, 1, 0), False), ((2, 0, 1, 0), False), ((2, 1, 0, 0), False),
+L2_ATOMIC_BYTES = {"eriKernelOcc<1,0,0,0,double,0>": 1222249650 * 32, "eriKernel<1,0,0,0,float,0>": 1107513230 * 32}
+# classes whose default tile shape is compiled with a raised occupancy bound (eriKernelOcc,
+# minBlocksPerSM in lible_b200/csrc/eri_kernel.cuh): (class, fp32)
+OCC_KERNELS = {(c, f) for c, f in [((2, 1, 1, 0), False), ((2, 0, 1, 0), False), ((2, 1, 0, 0), False),
                                                   ((1, 0, 0, 0), False), ((2, 1, 1, 0), True), ((2, 0, 1, 1), True),
                                                   ((1, 1, 1, 0), True), ((1, 0, 1, 0), True), ((2, 0, 0, 0), True)]}
 WORKLOAD = {"workload": "direct J+K build, (H2O)_32 water cluster, cc-pVDZ", "n_waters": N_WATERS, "nao": 768,
@@ -543,15 +543,16 @@ def main():
         for _ in range(3):
             for r in L.jk_profile(s, Dd, SCHWARZ, precision, FP32_THR, J=J, K=K):
                 key = (r["classes"], r["fp32"])
-                e = prof.setdefault(key, {"ms": [], "flops": r["flops"], "tasks": r["tasks"]})
+                e = prof.setdefault(key, {"ms": [], "flops": r["flops"], "tasks": r["tasks"], "shape": r["shape"]})
                 e["ms"].append(r["ms"])
         key, d = max(prof.items(), key=lambda kv: np.mean(kv[1]["ms"]))
         ms = float(np.mean(d["ms"]))
         tf = d["flops"] / (ms * 1e-3) / 1e12
         fp32 = bool(key[1])
         peak = fp32_peak if fp32 else fp64_peak
-        name = "%s<%d,%d,%d,%d,%s>" % ((OCC_KERNELS.get((key[0], key[1]), "eriKernel"),) + tuple(key[0]) +
-                                       ("float" if fp32 else "double",))
+        occ = d["shape"] == 0 and (tuple(key[0]), fp32) in OCC_KERNELS
+        name = "%s<%d,%d,%d,%d,%s,%d>" % (("eriKernelOcc" if occ else "eriKernel",) + tuple(key[0]) +
+                                          ("float" if fp32 else "double", d["shape"]))
         return {"bound": "fp32" if fp32 else "fp64", "achieved": tf, "peak": peak, "unit": "TFLOP/s",
                 "frac": tf / peak if peak else None, "traffic": DOMINANT_TRAFFIC.get((tuple(key[0]), fp32)),
                 "kernel": name, "kernel_ms": ms, "kernel_quartets": d["tasks"],

@@ -1461,7 +1461,7 @@ namespace lible_b200
             return;
         // bra / ket classes of the launch: the bra set is the auxiliary one for swapped RI pairs
         const int tb = cp.tb, tk = cp.tk;
-        const int unit = unitFwd(tb, tk, fp32);
+        const int unit = unitFwd(tb, tk, fp32, fp32 ? cp.shape32 : cp.shape64);
         if (unit == 0)
             return;
         auto ch = costChunks(fp32 ? cp.run32 : cp.run64, cp.cost, unit, mult * unit);
@@ -1627,13 +1627,13 @@ namespace lible_b200
             a.bra_npos = (int)B.n_pairs;
             a.ket_EtP = Kc.EtP;
             a.status = d_status_;
-            LaunchFn f64 = lookupFwd64(cp.tb, cp.tk);
+            LaunchFn f64 = lookupFwd64(cp.tb, cp.tk, cp.shape64);
             if (!f64)
                 throw EngineError(kStatusUnsupported, "quartet class not instantiated");
             if (timer && cp.t64 > 0)
             {
                 timer->before(st);
-                timer->info.push_back({{Bh.la, Bh.lb, Kh.la, Kh.lb}, 0, 0.0, cp.flops64, cp.n64});
+                timer->info.push_back({{Bh.la, Bh.lb, Kh.la, Kh.lb}, 2 * cp.shape64, 0.0, cp.flops64, cp.n64});
             }
             cudaCheck(f64(a, st, num_sms_), "jk kernel");
             if (timer && cp.t64 > 0)
@@ -1649,13 +1649,13 @@ namespace lible_b200
                 a.n_chunks = cp.n_chunks32;
                 a.counter = plan.counters + 2 * ip + 1;
                 a.grid_div = cp.grid_div32;
-                LaunchFn f32 = lookupFwd32(cp.tb, cp.tk);
+                LaunchFn f32 = lookupFwd32(cp.tb, cp.tk, cp.shape32);
                 if (!f32)
                     throw EngineError(kStatusUnsupported, "FP32 quartet class not instantiated");
                 if (timer)
                 {
                     timer->before(st);
-                    timer->info.push_back({{Bh.la, Bh.lb, Kh.la, Kh.lb}, 1, 0.0, cp.flops32, cp.n32});
+                    timer->info.push_back({{Bh.la, Bh.lb, Kh.la, Kh.lb}, 1 + 2 * cp.shape32, 0.0, cp.flops32, cp.n32});
                 }
                 cudaCheck(f32(a, st, num_sms_), "jk kernel fp32");
                 if (timer)
@@ -1778,7 +1778,11 @@ namespace lible_b200
         FILE *f = fopen(tune_cache_.c_str(), "r");
         if (!f)
             return;
-        std::map<std::string, std::pair<int, int>> entries;
+        struct Choice
+        {
+            int gd, cm, shape;
+        };
+        std::map<std::string, Choice> entries;
         char line[512];
         while (fgets(line, sizeof(line), f))
         {
@@ -1786,9 +1790,10 @@ namespace lible_b200
             const size_t bar = l.rfind('|');
             if (bar == std::string::npos)
                 continue;
-            int gd = 0, cm = 0;
-            if (sscanf(l.c_str() + bar + 1, "%d %d", &gd, &cm) == 2 && gd > 0 && cm > 0)
-                entries[l.substr(0, bar)] = {gd, cm};
+            int gd = 0, cm = 0, shape = 0;  // lines without the shape field are the default shape
+            const int got = sscanf(l.c_str() + bar + 1, "%d %d %d", &gd, &cm, &shape);
+            if (got >= 2 && gd > 0 && cm > 0 && (shape == 0 || shape == 1))
+                entries[l.substr(0, bar)] = {gd, cm, got == 3 ? shape : 0};
         }
         fclose(f);
         ClassSet &cs = mainSet(true);
@@ -1805,9 +1810,11 @@ namespace lible_b200
                 auto it = entries.find(key);
                 if (it == entries.end())
                     continue;
-                (fp32 ? cp.grid_div32 : cp.grid_div64) = it->second.first;
-                if (it->second.second != (fp32 ? cp.chunk_mult32 : cp.chunk_mult64))
-                    rebuildChunks(cp, fp32 == 1, it->second.second);
+                const Choice &ch = it->second;
+                const int shape = (ch.shape == 1 && hasFwdVariant(cp.tb, cp.tk, fp32 == 1)) ? 1 : 0;
+                (fp32 ? cp.grid_div32 : cp.grid_div64) = ch.gd;
+                (fp32 ? cp.shape32 : cp.shape64) = shape;
+                rebuildChunks(cp, fp32 == 1, ch.cm);
                 plan.tuned = true;
             }
     }
@@ -1838,14 +1845,17 @@ namespace lible_b200
                 const long long n = fp32 ? cp.t32 : cp.t64;
                 if (n == 0)
                     continue;
-                LaunchFn fn = fp32 ? lookupFwd32(cp.tb, cp.tk) : lookupFwd64(cp.tb, cp.tk);
-                if (!fn)
-                    throw EngineError(kStatusUnsupported, "quartet class not instantiated");
+                const int n_shapes = hasFwdVariant(cp.tb, cp.tk, fp32 == 1) ? 2 : 1;
                 float best = 1e30f;
-                int best_gd = 1, best_cm = 8;
+                int best_gd = 1, best_cm = 8, best_shape = 0;
+                for (int shape = 0; shape < n_shapes; shape++)
                 for (int cm : mults)
                 {
-                    rebuildChunks(cp, fp32 == 1, cm);
+                    LaunchFn fn = fp32 ? lookupFwd32(cp.tb, cp.tk, shape) : lookupFwd64(cp.tb, cp.tk, shape);
+                    if (!fn)
+                        throw EngineError(kStatusUnsupported, "quartet class not instantiated");
+                    (fp32 ? cp.shape32 : cp.shape64) = shape;
+                    rebuildChunks(cp, fp32 == 1, cm);  // the work unit depends on the shape
                     for (int gd : grid_divs)
                     {
                         QuartetArgs a{};
@@ -1902,21 +1912,22 @@ namespace lible_b200
                             best = t_min;
                             best_gd = gd;
                             best_cm = cm;
+                            best_shape = shape;
                         }
                     }
                 }
-                if (best_cm != (fp32 ? cp.chunk_mult32 : cp.chunk_mult64))
-                    rebuildChunks(cp, fp32 == 1, best_cm);
+                (fp32 ? cp.shape32 : cp.shape64) = best_shape;
+                rebuildChunks(cp, fp32 == 1, best_cm);
                 (fp32 ? cp.grid_div32 : cp.grid_div64) = best_gd;
                 const auto &Bh = cs.host[cp.cb], &Kh = cs.host[cp.ck];
                 char line[320];
-                snprintf(line, sizeof(line), "%s|%d %d %d %d|%d|%d|%d %d\n", gpu_name_.c_str(), Bh.la, Bh.lb, Kh.la,
-                         Kh.lb, fp32, sizeBucket(n), best_gd, best_cm);
+                snprintf(line, sizeof(line), "%s|%d %d %d %d|%d|%d|%d %d %d\n", gpu_name_.c_str(), Bh.la, Bh.lb, Kh.la,
+                         Kh.lb, fp32, sizeBucket(n), best_gd, best_cm, best_shape);
                 if (out)
                     fputs(line, out);
-                char info[160];
-                snprintf(info, sizeof(info), "(%d%d|%d%d) %s tasks=%lld grid_div=%d chunk_mult=%d %.3f ms\n", Bh.la,
-                         Bh.lb, Kh.la, Kh.lb, fp32 ? "fp32" : "fp64", n, best_gd, best_cm, best);
+                char info[200];
+                snprintf(info, sizeof(info), "(%d%d|%d%d) %s tasks=%lld shape=%d grid_div=%d chunk_mult=%d %.3f ms\n",
+                         Bh.la, Bh.lb, Kh.la, Kh.lb, fp32 ? "fp32" : "fp64", n, best_shape, best_gd, best_cm, best);
                 summary += info;
             }
         }

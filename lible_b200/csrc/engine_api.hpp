@@ -255,6 +255,8 @@ namespace lible_b200
             // launch parameters (autotuned): resident blocks per SM divided by grid_div, chunks of
             // at most chunk_mult work units
             int grid_div64 = 1, grid_div32 = 1, chunk_mult64 = 8, chunk_mult32 = 8;
+            // tile-shape variant of the class kernel (0 default, 1 the alternative), autotuned
+            int shape64 = 0, shape32 = 0;
             unsigned long long *chunksD1 = nullptr;  // gradient launches: chunks of one-quartet units
             long long n_chunksD1 = 0;
             int branch = 0;  // stream branch of the fork/join launch sequence

@@ -57,12 +57,29 @@ namespace lible_b200
         return p;
     }
 
-    template <int LA, int LB, int LC, int LD, typename T>
+    // The alternative register-path group of shape variant 1: the next divisor of S_cd above g0 (more
+    // threads per quartet, fewer values per thread); g0 itself when there is none.
+    constexpr int altRegGroup(int scd, int g0)
+    {
+        if (g0 == 0)
+            return 0;
+        for (int g = g0 + 1; g <= 32 && g <= scd; g++)
+            if (scd % g == 0)
+                return g;
+        return g0;
+    }
+
+    // Tile shape of a class kernel.  Shape variant SV = 0 is the default; SV = 1 is the alternative
+    // the launch autotuner times against it: twice the warps per quartet on the group paths (each
+    // warp owning fewer output tiles), the next larger thread group on the register path, and the
+    // default register bound for the classes compiled with a raised occupancy bound.
+    template <int LA, int LB, int LC, int LD, typename T, int SV = 0>
     struct Shape
     {
         using C = Cls<LA, LB, LC, LD>;
         // register path: GT threads per quartet, each owning CW consecutive ket columns
-        static constexpr int GT = pickRegGroup<T>(C::SAB, C::SCD, C::HAB, C::NR);
+        static constexpr int GT0 = pickRegGroup<T>(C::SAB, C::SCD, C::HAB, C::NR);
+        static constexpr int GT = SV == 0 ? GT0 : altRegGroup(C::SCD, GT0);
         static constexpr int CW = GT ? C::SCD / GT : 0;
         static constexpr int QPW = GT ? 32 / GT : 0;           // quartets per warp
         // group path in FP64: both contractions on the DMMA pipe (mma.m8n8k4.f64) in 8x8 tiles of
@@ -71,7 +88,9 @@ namespace lible_b200
         static constexpr int MT = (C::HAB + 7) / 8, NT = (C::SCD + 7) / 8, KT = (C::HCD + 3) / 4;
         static constexpr int MT2 = (C::SAB + 7) / 8, KT2 = (C::HAB + 3) / 4;
         static constexpr int TILES = MT * NT, TILES2 = MT2 * NT;
-        static constexpr int WM = (TILES + 5) / 6 < 1 ? 1 : ((TILES + 5) / 6 > 8 ? 8 : (TILES + 5) / 6);
+        static constexpr int WM0 = (TILES + 5) / 6 < 1 ? 1 : ((TILES + 5) / 6 > 8 ? 8 : (TILES + 5) / 6);
+        static constexpr int WM1 = 2 * WM0 > 8 ? 8 : (2 * WM0 > TILES ? (TILES > WM0 ? TILES : WM0) : 2 * WM0);
+        static constexpr int WM = SV == 0 ? WM0 : WM1;
         static constexpr int TPW = (TILES + WM - 1) / WM, TPW2 = (TILES2 + WM - 1) / WM;
         static constexpr int P_RM = kPitch(C::HAB), P_EC = kPitch(C::SCD), P_EA = mPitch(C::HAB);
         static constexpr size_t a16(size_t x) { return (x + 15) / 16 * 16; }
@@ -86,12 +105,11 @@ namespace lible_b200
         static constexpr size_t m_smem = m_off_mb + 16;
         // bytes of one padded ket E tile (KT*4 rows of P_EC doubles), the unit of the bulk copy
         static constexpr unsigned ec_tile_bytes = 8u * KT * 4 * P_EC;
-        static constexpr int W = GT ? 0
-                                 : MMA ? WM
-                                 : ((C::HAB * C::SCD + C::SAB * C::SCD) <= 64 * 32)     ? 1
-                                 : ((C::HAB * C::SCD + C::SAB * C::SCD) <= 64 * 64)     ? 2
-                                 : ((C::HAB * C::SCD + C::SAB * C::SCD) <= 64 * 128)    ? 4
-                                                                                          : 8;
+        static constexpr int W0 = ((C::HAB * C::SCD + C::SAB * C::SCD) <= 64 * 32)    ? 1
+                                  : ((C::HAB * C::SCD + C::SAB * C::SCD) <= 64 * 64)  ? 2
+                                  : ((C::HAB * C::SCD + C::SAB * C::SCD) <= 64 * 128) ? 4
+                                                                                       : 8;
+        static constexpr int W = GT ? 0 : MMA ? WM : (SV == 0 ? W0 : (2 * W0 > 8 ? 8 : 2 * W0));
         static constexpr int G = W == 0 ? 1 : 32 * W;
         static constexpr int block = W == 0 ? 128 : G;
         // register path: per-warp staging of finished batches for the digestion epilogue
@@ -447,12 +465,12 @@ namespace lible_b200
     // `sv` is the bra's structure-of-arrays entry (sv.z = 0: read the per-pair records instead).
     // `nk` >= 0 is the bra's primitive-pair count from the per-position fields (the bra records are
     // then read from the structure-of-arrays copies only); -1 reads the pair's primitive range.
-    template <int LA, int LB, int LC, int LD, typename T>
+    template <int LA, int LB, int LC, int LD, typename T, int SV = 0>
     __device__ __forceinline__ void quartetThread(const QuartetArgs &a, uint32_t ib, uint32_t ik, int c0, T *V,
                                                   const T *btab, uint4 sv, int nk)
     {
         using C = Cls<LA, LB, LC, LD>;
-        constexpr int CW = Shape<LA, LB, LC, LD, T>::CW;
+        constexpr int CW = Shape<LA, LB, LC, LD, T, SV>::CW;
 #pragma unroll
         for (int x = 0; x < C::SAB * CW; x++)
             V[x] = T(0);
@@ -593,12 +611,12 @@ namespace lible_b200
 
     // ---------------------------------------------------------------------------------------
     // G = 32 W: one thread group (the whole block) per contracted quartet.
-    template <int LA, int LB, int LC, int LD, typename T>
+    template <int LA, int LB, int LC, int LD, typename T, int SV = 0>
     __device__ __forceinline__ void quartetGroup(const QuartetArgs &a, uint32_t ib, uint32_t ik,
                                                  unsigned char *smem, T *vals)
     {
         using C = Cls<LA, LB, LC, LD>;
-        using S = Shape<LA, LB, LC, LD, T>;
+        using S = Shape<LA, LB, LC, LD, T, SV>;
         constexpr int G = S::G;
         const int tid = threadIdx.x;
         T *rb = reinterpret_cast<T *>(smem + S::off_rb);
@@ -749,13 +767,13 @@ namespace lible_b200
     // (one completed phase per ket primitive of every quartet), so it is carried across calls.
     // Returns false when a bounded wait on a ket tile gave up (status word set): the block has then
     // let any copy still in flight land (again bounded) and must stop without using the batch.
-    template <int LA, int LB, int LC, int LD>
+    template <int LA, int LB, int LC, int LD, int SV = 0>
     __device__ __forceinline__ bool quartetGroupMMA(const QuartetArgs &a, uint32_t ib, uint32_t ik,
-                                                    unsigned char *smem, double (&v)[Shape<LA, LB, LC, LD, double>::TPW2][2],
+                                                    unsigned char *smem, double (&v)[Shape<LA, LB, LC, LD, double, SV>::TPW2][2],
                                                     unsigned &phase)
     {
         using C = Cls<LA, LB, LC, LD>;
-        using S = Shape<LA, LB, LC, LD, double>;
+        using S = Shape<LA, LB, LC, LD, double, SV>;
         constexpr int G = S::G;
         const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, r8 = lane >> 2, k4 = lane & 3;
         double *rb = reinterpret_cast<double *>(smem + S::m_off_rb);
@@ -924,11 +942,11 @@ namespace lible_b200
     }
 
     // Tables and zero padding of the DMMA layout (once per block).
-    template <int LA, int LB, int LC, int LD>
+    template <int LA, int LB, int LC, int LD, int SV = 0>
     __device__ __forceinline__ void buildGroupTablesMMA(unsigned char *smem)
     {
         using C = Cls<LA, LB, LC, LD>;
-        using S = Shape<LA, LB, LC, LD, double>;
+        using S = Shape<LA, LB, LC, LD, double, SV>;
         double *z = reinterpret_cast<double *>(smem + S::m_off_rm);
         const int nz = (int)((S::m_off_ix - S::m_off_rm) / 8);
         for (int e = threadIdx.x; e < nz; e += blockDim.x)
@@ -959,11 +977,11 @@ namespace lible_b200
 
     // Builds the per-block tables of the group shape: Hermite (t,u,v,order) list and the signed
     // combined index of (h + h') for the R matrix.
-    template <int LA, int LB, int LC, int LD, typename T>
+    template <int LA, int LB, int LC, int LD, typename T, int SV = 0>
     __device__ __forceinline__ void buildGroupTables(unsigned char *smem)
     {
         using C = Cls<LA, LB, LC, LD>;
-        using S = Shape<LA, LB, LC, LD, T>;
+        using S = Shape<LA, LB, LC, LD, T, SV>;
         short *rix = reinterpret_cast<short *>(smem + S::off_ix);
         char4 *ht = reinterpret_cast<char4 *>(smem + S::off_ht);
         for (int e = threadIdx.x; e < C::NR; e += blockDim.x)
@@ -991,10 +1009,10 @@ namespace lible_b200
     // than the default bound (which lets the compiler use more registers): FP64 (dp|ps), (ds|ps),
     // (dp|ss) at 3 blocks and (ps|ss) at 6; FP32 (dp|ps), (ds|pp) at 3, (pp|ps) at 4, (ps|ps) at 6,
     // (ds|ss) at 8.  1 = the default bound.
-    template <int LA, int LB, int LC, int LD, typename T>
+    template <int LA, int LB, int LC, int LD, typename T, int SV = 0>
     constexpr int minBlocksPerSM()
     {
-        if (Shape<LA, LB, LC, LD, T>::W != 0)
+        if (SV != 0 || Shape<LA, LB, LC, LD, T, SV>::W != 0)
             return 1;
         constexpr int c = LA * 1000 + LB * 100 + LC * 10 + LD;
         if (sizeof(T) == 8)
@@ -1003,11 +1021,11 @@ namespace lible_b200
     }
 
     // Forward kernel body: every mode except the derivative ones.
-    template <int LA, int LB, int LC, int LD, typename T>
+    template <int LA, int LB, int LC, int LD, typename T, int SV = 0>
     __device__ __forceinline__ void eriKernelBody(const QuartetArgs &a)
     {
         using C = Cls<LA, LB, LC, LD>;
-        using S = Shape<LA, LB, LC, LD, T>;
+        using S = Shape<LA, LB, LC, LD, T, SV>;
         constexpr int blk = C::SAB * C::SCD;
         if constexpr (S::W == 0)
         {
@@ -1065,7 +1083,7 @@ namespace lible_b200
                         bsame = bi0[4] == bi0[5];
                     }
                     if (active)
-                        quartetThread<LA, LB, LC, LD, T>(a, ib, ik, member * CW, V, btab, sv, nk);
+                        quartetThread<LA, LB, LC, LD, T, SV>(a, ib, ik, member * CW, V, btab, sv, nk);
                     else
                     {
 #pragma unroll
@@ -1155,7 +1173,7 @@ namespace lible_b200
         else if constexpr (S::MMA)
         {
             extern __shared__ __align__(16) unsigned char smem[];
-            buildGroupTablesMMA<LA, LB, LC, LD>(smem);
+            buildGroupTablesMMA<LA, LB, LC, LD, SV>(smem);
             double *vs = reinterpret_cast<double *>(smem + S::m_off_rx);
             const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, r8 = lane >> 2, k4 = lane & 3;
             unsigned phase = 0;  // parity of the block mbarrier's next phase
@@ -1170,7 +1188,7 @@ namespace lible_b200
                 if (!inWindow(a, ib, ik, 0, false))
                     continue;
                 double v[S::TPW2][2];
-                if (!quartetGroupMMA<LA, LB, LC, LD>(a, ib, ik, smem, v, phase))
+                if (!quartetGroupMMA<LA, LB, LC, LD, SV>(a, ib, ik, smem, v, phase))
                     return false;
                 // element (m, c) of the batch held by this thread: tile rows / columns
 #pragma unroll
@@ -1240,7 +1258,7 @@ namespace lible_b200
         else
         {
             extern __shared__ __align__(16) unsigned char smem[];
-            buildGroupTables<LA, LB, LC, LD, T>(smem);
+            buildGroupTables<LA, LB, LC, LD, T, SV>(smem);
             T *vs = reinterpret_cast<T *>(smem + S::off_rx);
             // one quartet at a time for the whole block, tasks [start, end) of a chunk
             auto processRange = [&](long long start, long long end) {
@@ -1252,7 +1270,7 @@ namespace lible_b200
                 if (!inWindow(a, ib, ik, 0, false))
                     continue;
                 T vals[S::IB];
-                quartetGroup<LA, LB, LC, LD, T>(a, ib, ik, smem, vals);
+                quartetGroup<LA, LB, LC, LD, T, SV>(a, ib, ik, smem, vals);
                 if (a.mode == kStore)
                 {
 #pragma unroll
@@ -1318,23 +1336,32 @@ namespace lible_b200
 
     // The class kernels: the default register bound, or (minBlocksPerSM > 1) one that lets that many
     // blocks reside per SM.  Only the selected one is instantiated per class (eriKernelFor).
-    template <int LA, int LB, int LC, int LD, typename T>
-    __global__ void __launch_bounds__(Shape<LA, LB, LC, LD, T>::block) eriKernel(QuartetArgs a)
+    template <int LA, int LB, int LC, int LD, typename T, int SV = 0>
+    __global__ void __launch_bounds__(Shape<LA, LB, LC, LD, T, SV>::block) eriKernel(QuartetArgs a)
     {
-        eriKernelBody<LA, LB, LC, LD, T>(a);
+        eriKernelBody<LA, LB, LC, LD, T, SV>(a);
     }
-    template <int LA, int LB, int LC, int LD, typename T>
-    __global__ void __launch_bounds__(Shape<LA, LB, LC, LD, T>::block, minBlocksPerSM<LA, LB, LC, LD, T>())
+    template <int LA, int LB, int LC, int LD, typename T, int SV = 0>
+    __global__ void __launch_bounds__(Shape<LA, LB, LC, LD, T, SV>::block, minBlocksPerSM<LA, LB, LC, LD, T, SV>())
     eriKernelOcc(QuartetArgs a)
     {
-        eriKernelBody<LA, LB, LC, LD, T>(a);
+        eriKernelBody<LA, LB, LC, LD, T, SV>(a);
     }
+    // Whether shape variant 1 differs from the default (otherwise only variant 0 is instantiated).
     template <int LA, int LB, int LC, int LD, typename T>
+    constexpr bool hasShapeVariant()
+    {
+        using S0 = Shape<LA, LB, LC, LD, T, 0>;
+        using S1 = Shape<LA, LB, LC, LD, T, 1>;
+        return S0::GT != S1::GT || S0::W != S1::W || minBlocksPerSM<LA, LB, LC, LD, T, 0>() > 1;
+    }
+
+    template <int LA, int LB, int LC, int LD, typename T, int SV = 0>
     constexpr auto eriKernelFor()
     {
-        if constexpr (minBlocksPerSM<LA, LB, LC, LD, T>() > 1)
-            return &eriKernelOcc<LA, LB, LC, LD, T>;
+        if constexpr (minBlocksPerSM<LA, LB, LC, LD, T, SV>() > 1)
+            return &eriKernelOcc<LA, LB, LC, LD, T, SV>;
         else
-            return &eriKernel<LA, LB, LC, LD, T>;
+            return &eriKernel<LA, LB, LC, LD, T, SV>;
     }
 }

@@ -19,8 +19,11 @@ namespace lible_b200
     }
 
     // Implemented by the generated instantiation files.
-    LaunchFn lookupFwd64(int bra_type, int ket_type);
-    LaunchFn lookupFwd32(int bra_type, int ket_type);
+    // `shape` selects the tile-shape variant of the forward class kernels (0 default, 1 the
+    // alternative of Shape<..., 1>); variant 1 is null where it equals the default.
+    LaunchFn lookupFwd64(int bra_type, int ket_type, int shape = 0);
+    LaunchFn lookupFwd32(int bra_type, int ket_type, int shape = 0);
     LaunchFn lookupD1(int bra_type, int ket_type);
-    int unitFwd(int bra_type, int ket_type, bool fp32);
+    int unitFwd(int bra_type, int ket_type, bool fp32, int shape = 0);
+    bool hasFwdVariant(int bra_type, int ket_type, bool fp32);
 }

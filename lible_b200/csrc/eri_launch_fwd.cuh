@@ -11,20 +11,20 @@ namespace lible_b200
     // Quartets a worker processes side by side: QPW per warp on the register path, one per block on
     // the group path.  Work-queue chunks are cut so that each holds at least one unit of the most
     // expensive quartets.
-    template <int LA, int LB, int LC, int LD, typename T>
+    template <int LA, int LB, int LC, int LD, typename T, int SV = 0>
     constexpr int workUnit()
     {
-        using S = Shape<LA, LB, LC, LD, T>;
+        using S = Shape<LA, LB, LC, LD, T, SV>;
         return S::W == 0 ? S::QPW : 1;
     }
 
-    template <int LA, int LB, int LC, int LD, typename T>
+    template <int LA, int LB, int LC, int LD, typename T, int SV = 0>
     cudaError_t launchFwd(const QuartetArgs &a, cudaStream_t s, int num_sms)
     {
-        using S = Shape<LA, LB, LC, LD, T>;
+        using S = Shape<LA, LB, LC, LD, T, SV>;
         if (a.n_tasks <= 0)
             return cudaSuccess;
-        auto kern = eriKernelFor<LA, LB, LC, LD, T>();
+        auto kern = eriKernelFor<LA, LB, LC, LD, T, SV>();
         long long grid;
         if (a.chunks)
         {

@@ -7,8 +7,22 @@ namespace lible_b200
     {
         return launchFwd<0,0,0,0,float>(a, s, n);
     }
+    cudaError_t launch_fwd32_00_00_v1(const QuartetArgs &a, cudaStream_t s, int n)
+    {
+        if constexpr (hasShapeVariant<0,0,0,0,float>())
+            return launchFwd<0,0,0,0,float,1>(a, s, n);
+        else
+            return cudaErrorNotSupported;
+    }
     cudaError_t launch_fwd32_01_00(const QuartetArgs &a, cudaStream_t s, int n)
     {
         return launchFwd<1,0,0,0,float>(a, s, n);
+    }
+    cudaError_t launch_fwd32_01_00_v1(const QuartetArgs &a, cudaStream_t s, int n)
+    {
+        if constexpr (hasShapeVariant<1,0,0,0,float>())
+            return launchFwd<1,0,0,0,float,1>(a, s, n);
+        else
+            return cudaErrorNotSupported;
     }
 }

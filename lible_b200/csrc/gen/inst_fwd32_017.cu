@@ -7,8 +7,22 @@ namespace lible_b200
     {
         return launchFwd<3,1,3,0,float>(a, s, n);
     }
+    cudaError_t launch_fwd32_07_06_v1(const QuartetArgs &a, cudaStream_t s, int n)
+    {
+        if constexpr (hasShapeVariant<3,1,3,0,float>())
+            return launchFwd<3,1,3,0,float,1>(a, s, n);
+        else
+            return cudaErrorNotSupported;
+    }
     cudaError_t launch_fwd32_07_07(const QuartetArgs &a, cudaStream_t s, int n)
     {
         return launchFwd<3,1,3,1,float>(a, s, n);
+    }
+    cudaError_t launch_fwd32_07_07_v1(const QuartetArgs &a, cudaStream_t s, int n)
+    {
+        if constexpr (hasShapeVariant<3,1,3,1,float>())
+            return launchFwd<3,1,3,1,float,1>(a, s, n);
+        else
+            return cudaErrorNotSupported;
     }
 }

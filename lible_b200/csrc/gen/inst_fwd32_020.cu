@@ -7,8 +7,22 @@ namespace lible_b200
     {
         return launchFwd<3,2,2,1,float>(a, s, n);
     }
+    cudaError_t launch_fwd32_08_04_v1(const QuartetArgs &a, cudaStream_t s, int n)
+    {
+        if constexpr (hasShapeVariant<3,2,2,1,float>())
+            return launchFwd<3,2,2,1,float,1>(a, s, n);
+        else
+            return cudaErrorNotSupported;
+    }
     cudaError_t launch_fwd32_08_05(const QuartetArgs &a, cudaStream_t s, int n)
     {
         return launchFwd<3,2,2,2,float>(a, s, n);
+    }
+    cudaError_t launch_fwd32_08_05_v1(const QuartetArgs &a, cudaStream_t s, int n)
+    {
+        if constexpr (hasShapeVariant<3,2,2,2,float>())
+            return launchFwd<3,2,2,2,float,1>(a, s, n);
+        else
+            return cudaErrorNotSupported;
     }
 }

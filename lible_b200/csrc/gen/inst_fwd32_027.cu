@@ -7,4 +7,11 @@ namespace lible_b200
     {
         return launchFwd<3,3,3,3,float>(a, s, n);
     }
+    cudaError_t launch_fwd32_09_09_v1(const QuartetArgs &a, cudaStream_t s, int n)
+    {
+        if constexpr (hasShapeVariant<3,3,3,3,float>())
+            return launchFwd<3,3,3,3,float,1>(a, s, n);
+        else
+            return cudaErrorNotSupported;
+    }
 }

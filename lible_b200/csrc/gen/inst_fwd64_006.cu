@@ -7,8 +7,22 @@ namespace lible_b200
     {
         return launchFwd<2,1,1,1,double>(a, s, n);
     }
+    cudaError_t launch_fwd64_04_02_v1(const QuartetArgs &a, cudaStream_t s, int n)
+    {
+        if constexpr (hasShapeVariant<2,1,1,1,double>())
+            return launchFwd<2,1,1,1,double,1>(a, s, n);
+        else
+            return cudaErrorNotSupported;
+    }
     cudaError_t launch_fwd64_04_03(const QuartetArgs &a, cudaStream_t s, int n)
     {
         return launchFwd<2,1,2,0,double>(a, s, n);
+    }
+    cudaError_t launch_fwd64_04_03_v1(const QuartetArgs &a, cudaStream_t s, int n)
+    {
+        if constexpr (hasShapeVariant<2,1,2,0,double>())
+            return launchFwd<2,1,2,0,double,1>(a, s, n);
+        else
+            return cudaErrorNotSupported;
     }
 }

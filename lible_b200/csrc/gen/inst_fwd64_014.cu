@@ -7,8 +7,22 @@ namespace lible_b200
     {
         return launchFwd<3,1,0,0,double>(a, s, n);
     }
+    cudaError_t launch_fwd64_07_00_v1(const QuartetArgs &a, cudaStream_t s, int n)
+    {
+        if constexpr (hasShapeVariant<3,1,0,0,double>())
+            return launchFwd<3,1,0,0,double,1>(a, s, n);
+        else
+            return cudaErrorNotSupported;
+    }
     cudaError_t launch_fwd64_07_01(const QuartetArgs &a, cudaStream_t s, int n)
     {
         return launchFwd<3,1,1,0,double>(a, s, n);
+    }
+    cudaError_t launch_fwd64_07_01_v1(const QuartetArgs &a, cudaStream_t s, int n)
+    {
+        if constexpr (hasShapeVariant<3,1,1,0,double>())
+            return launchFwd<3,1,1,0,double,1>(a, s, n);
+        else
+            return cudaErrorNotSupported;
     }
 }

@@ -7,8 +7,22 @@ namespace lible_b200
     {
         return launchFwd<3,3,2,2,double>(a, s, n);
     }
+    cudaError_t launch_fwd64_09_05_v1(const QuartetArgs &a, cudaStream_t s, int n)
+    {
+        if constexpr (hasShapeVariant<3,3,2,2,double>())
+            return launchFwd<3,3,2,2,double,1>(a, s, n);
+        else
+            return cudaErrorNotSupported;
+    }
     cudaError_t launch_fwd64_09_06(const QuartetArgs &a, cudaStream_t s, int n)
     {
         return launchFwd<3,3,3,0,double>(a, s, n);
+    }
+    cudaError_t launch_fwd64_09_06_v1(const QuartetArgs &a, cudaStream_t s, int n)
+    {
+        if constexpr (hasShapeVariant<3,3,3,0,double>())
+            return launchFwd<3,3,3,0,double,1>(a, s, n);
+        else
+            return cudaErrorNotSupported;
     }
 }

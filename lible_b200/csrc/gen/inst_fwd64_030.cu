@@ -7,8 +7,22 @@ namespace lible_b200
     {
         return launchFwd<4,0,2,2,double>(a, s, n);
     }
+    cudaError_t launch_fwd64_10_05_v1(const QuartetArgs &a, cudaStream_t s, int n)
+    {
+        if constexpr (hasShapeVariant<4,0,2,2,double>())
+            return launchFwd<4,0,2,2,double,1>(a, s, n);
+        else
+            return cudaErrorNotSupported;
+    }
     cudaError_t launch_fwd64_10_06(const QuartetArgs &a, cudaStream_t s, int n)
     {
         return launchFwd<4,0,3,0,double>(a, s, n);
+    }
+    cudaError_t launch_fwd64_10_06_v1(const QuartetArgs &a, cudaStream_t s, int n)
+    {
+        if constexpr (hasShapeVariant<4,0,3,0,double>())
+            return launchFwd<4,0,3,0,double,1>(a, s, n);
+        else
+            return cudaErrorNotSupported;
     }
 }

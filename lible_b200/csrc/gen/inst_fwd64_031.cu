@@ -7,8 +7,22 @@ namespace lible_b200
     {
         return launchFwd<4,0,3,1,double>(a, s, n);
     }
+    cudaError_t launch_fwd64_10_07_v1(const QuartetArgs &a, cudaStream_t s, int n)
+    {
+        if constexpr (hasShapeVariant<4,0,3,1,double>())
+            return launchFwd<4,0,3,1,double,1>(a, s, n);
+        else
+            return cudaErrorNotSupported;
+    }
     cudaError_t launch_fwd64_10_08(const QuartetArgs &a, cudaStream_t s, int n)
     {
         return launchFwd<4,0,3,2,double>(a, s, n);
+    }
+    cudaError_t launch_fwd64_10_08_v1(const QuartetArgs &a, cudaStream_t s, int n)
+    {
+        if constexpr (hasShapeVariant<4,0,3,2,double>())
+            return launchFwd<4,0,3,2,double,1>(a, s, n);
+        else
+            return cudaErrorNotSupported;
     }
 }

@@ -7,8 +7,22 @@ namespace lible_b200
     {
         return launchFwd<4,0,3,3,double>(a, s, n);
     }
+    cudaError_t launch_fwd64_10_09_v1(const QuartetArgs &a, cudaStream_t s, int n)
+    {
+        if constexpr (hasShapeVariant<4,0,3,3,double>())
+            return launchFwd<4,0,3,3,double,1>(a, s, n);
+        else
+            return cudaErrorNotSupported;
+    }
     cudaError_t launch_fwd64_10_10(const QuartetArgs &a, cudaStream_t s, int n)
     {
         return launchFwd<4,0,4,0,double>(a, s, n);
+    }
+    cudaError_t launch_fwd64_10_10_v1(const QuartetArgs &a, cudaStream_t s, int n)
+    {
+        if constexpr (hasShapeVariant<4,0,4,0,double>())
+            return launchFwd<4,0,4,0,double,1>(a, s, n);
+        else
+            return cudaErrorNotSupported;
     }
 }

@@ -7,8 +7,22 @@ namespace lible_b200
     {
         return launchFwd<5,0,3,2,double>(a, s, n);
     }
+    cudaError_t launch_fwd64_11_08_v1(const QuartetArgs &a, cudaStream_t s, int n)
+    {
+        if constexpr (hasShapeVariant<5,0,3,2,double>())
+            return launchFwd<5,0,3,2,double,1>(a, s, n);
+        else
+            return cudaErrorNotSupported;
+    }
     cudaError_t launch_fwd64_11_09(const QuartetArgs &a, cudaStream_t s, int n)
     {
         return launchFwd<5,0,3,3,double>(a, s, n);
+    }
+    cudaError_t launch_fwd64_11_09_v1(const QuartetArgs &a, cudaStream_t s, int n)
+    {
+        if constexpr (hasShapeVariant<5,0,3,3,double>())
+            return launchFwd<5,0,3,3,double,1>(a, s, n);
+        else
+            return cudaErrorNotSupported;
     }
 }

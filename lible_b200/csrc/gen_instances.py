@@ -45,6 +45,12 @@ def main():
                 lc, ld = PAIR_TYPES[kt]
                 body += [f'    cudaError_t {name_of(bt, kt)}(const QuartetArgs &a, cudaStream_t s, int n)',
                          '    {', f'        return {launcher}<{la},{lb},{lc},{ld}{T}>(a, s, n);', '    }']
+                if kind.startswith("fwd"):
+                    # shape variant 1, instantiated only where it differs from the default
+                    body += [f'    cudaError_t {name_of(bt, kt)}_v1(const QuartetArgs &a, cudaStream_t s, int n)',
+                             '    {', f'        if constexpr (hasShapeVariant<{la},{lb},{lc},{ld}{T}>())',
+                             f'            return {launcher}<{la},{lb},{lc},{ld}{T},1>(a, s, n);',
+                             '        else', '            return cudaErrorNotSupported;', '    }']
             body += ['}', '']
             name = f"inst_{kind}_{g // GROUP[kind]:03d}.cu"
             path = os.path.join(out, name)
@@ -54,27 +60,46 @@ def main():
                     fh.write(text)
             written.append(name)
         table += [f'    cudaError_t {name_of(bt, kt)}(const QuartetArgs &, cudaStream_t, int);' for bt, kt in classes]
+        if kind.startswith("fwd"):
+            table += [f'    cudaError_t {name_of(bt, kt)}_v1(const QuartetArgs &, cudaStream_t, int);'
+                      for bt, kt in classes]
+        cls = lambda bt, kt: "%d,%d,%d,%d%s" % (PAIR_TYPES[bt] + PAIR_TYPES[kt] + (T,))
         for bt in range(ntypes):
-            la, lb = PAIR_TYPES[bt]
             table.append(f'    static const LaunchFn k_{kind}_{bt:02d}[{bt + 1}] = {{' +
                          ", ".join(f"&{name_of(bt, kt)}" for kt in range(bt + 1)) + '};')
             if kind.startswith("fwd"):
-                table.append(f'    static const int u_{kind}_{bt:02d}[{bt + 1}] = {{' +
-                             ", ".join(f"workUnit<{la},{lb},{PAIR_TYPES[kt][0]},{PAIR_TYPES[kt][1]}{T}>()"
+                table.append(f'    static const LaunchFn k_{kind}v_{bt:02d}[{bt + 1}] = {{' +
+                             ", ".join(f"hasShapeVariant<{cls(bt, kt)}>() ? &{name_of(bt, kt)}_v1 : nullptr"
                                        for kt in range(bt + 1)) + '};')
+                for v in (0, 1):
+                    table.append(f'    static const int u_{kind}_{v}_{bt:02d}[{bt + 1}] = {{' +
+                                 ", ".join(f"workUnit<{cls(bt, kt)},{v}>()" for kt in range(bt + 1)) + '};')
         if kind.startswith("fwd"):
-            table.append(f'    static const int *const u_{kind}[{ntypes}] = {{' +
-                         ", ".join(f"u_{kind}_{bt:02d}" for bt in range(ntypes)) + '};')
+            for v in (0, 1):
+                table.append(f'    static const int *const u_{kind}_{v}[{ntypes}] = {{' +
+                             ", ".join(f"u_{kind}_{v}_{bt:02d}" for bt in range(ntypes)) + '};')
+            table.append(f'    static const LaunchFn *const k_{kind}v[{ntypes}] = {{' +
+                         ", ".join(f"k_{kind}v_{bt:02d}" for bt in range(ntypes)) + '};')
         table.append(f'    static const LaunchFn *const k_{kind}[{ntypes}] = {{' +
                      ", ".join(f"k_{kind}_{bt:02d}" for bt in range(ntypes)) + '};')
     for kind, _, ntypes in kinds():
         fn = {"fwd64": "lookupFwd64", "fwd32": "lookupFwd32", "d1": "lookupD1"}[kind]
-        table += [f'    LaunchFn {fn}(int bt, int kt)', '    {',
-                  f'        if (bt < 0 || bt >= {ntypes} || kt < 0 || kt > bt)',
-                  '            return nullptr;', f'        return k_{kind}[bt][kt];', '    }']
-    table += ['    int unitFwd(int bt, int kt, bool fp32)', '    {',
+        if kind == "d1":
+            table += [f'    LaunchFn {fn}(int bt, int kt)', '    {',
+                      f'        if (bt < 0 || bt >= {ntypes} || kt < 0 || kt > bt)',
+                      '            return nullptr;', f'        return k_{kind}[bt][kt];', '    }']
+        else:
+            table += [f'    LaunchFn {fn}(int bt, int kt, int shape)', '    {',
+                      f'        if (bt < 0 || bt >= {ntypes} || kt < 0 || kt > bt)',
+                      '            return nullptr;', f'        return shape ? k_{kind}v[bt][kt] : k_{kind}[bt][kt];', '    }']
+    table += ['    int unitFwd(int bt, int kt, bool fp32, int shape)', '    {',
               '        if (bt < 0 || kt < 0 || kt > bt || bt >= (fp32 ? %d : %d))' % (FP32_MAX_TYPE + 1, len(PAIR_TYPES)),
-              '            return 0;', '        return fp32 ? u_fwd32[bt][kt] : u_fwd64[bt][kt];', '    }']
+              '            return 0;',
+              '        if (shape)',
+              '            return fp32 ? u_fwd32_1[bt][kt] : u_fwd64_1[bt][kt];',
+              '        return fp32 ? u_fwd32_0[bt][kt] : u_fwd64_0[bt][kt];', '    }',
+              '    bool hasFwdVariant(int bt, int kt, bool fp32)', '    {',
+              '        return (fp32 ? lookupFwd32(bt, kt, 1) : lookupFwd64(bt, kt, 1)) != nullptr;', '    }']
     table += ['}', '']
     path = os.path.join(out, "inst_table.cu")
     text = "\n".join(table)

@@ -415,7 +415,7 @@ def jk_autotune(structure, D, schwarz=1e-12, precision="fp64", fp32_threshold=1e
 
 def jk_profile(structure, D, schwarz=1e-12, precision="fp64", fp32_threshold=1e-4, J=None, K=None):
     """One J/K build with every class launch serialised and timed by CUDA events.  Returns a list of
-    dicts (classes, fp32, ms, flops, tasks) in launch order."""
+    dicts (classes, fp32, shape = the launch's tile-shape variant, ms, flops, tasks) in launch order."""
     Dh = D if hasattr(D, "data_ptr") else _f64(D)
     J = np.empty(_jk_shape(structure)) if J is None else J
     K = np.empty(_jk_shape(structure)) if K is None else K
@@ -426,8 +426,9 @@ def jk_profile(structure, D, schwarz=1e-12, precision="fp64", fp32_threshold=1e-
     opts = _opts(schwarz, precision, fp32_threshold)
     _call(structure, "lible_gpu_jk_profile", _ptr(Dh), _ptr(J), _ptr(K), ctypes.byref(opts), ctypes.byref(n),
           _ptr(ls), _ptr(f32), _ptr(ms), _ptr(fl), _ptr(tk))
-    return [{"classes": tuple(int(x) for x in ls[4 * i:4 * i + 4]), "fp32": bool(f32[i]), "ms": float(ms[i]),
-             "flops": float(fl[i]), "tasks": int(tk[i])} for i in range(min(n.value, cap))]
+    return [{"classes": tuple(int(x) for x in ls[4 * i:4 * i + 4]), "fp32": bool(f32[i] & 1),
+             "shape": int(f32[i] >> 1), "ms": float(ms[i]), "flops": float(fl[i]), "tasks": int(tk[i])}
+            for i in range(min(n.value, cap))]
 
 
 def set_tune_cache(structure, path):
