@@ -179,8 +179,9 @@ def run_reference(args):
 def run_batch(steps, warmup, dev):
     """The heterogeneous batch: 64 water clusters (1..12 waters, half cc-pVDZ, half cc-pVTZ), FP64,
     Schwarz 1e-12.  Times the batched build (one work-queue launch per quartet class for all
-    molecules, replayed from a CUDA graph) against the same molecules built one after another
-    through the single-structure path."""
+    molecules, replayed from a CUDA graph, class launches autotuned once in the set-up) against the
+    same molecules built one after another through the single-structure path, and the mixed
+    precision batch with its largest per-molecule energy error against FP64."""
     import torch
 
     from lible_b200 import ints as L
@@ -194,22 +195,36 @@ def run_batch(steps, warmup, dev):
     J, K = torch.empty_like(Dp), torch.empty_like(Dp)
     plan = L.jk_plan(b, SCHWARZ, "fp64")
     setup_s = time.perf_counter() - t0
+    # one-time autotuning of the batch's class launches (tile shapes, occupancy, queue granularity)
+    t0 = time.perf_counter()
+    L.jk_autotune(b, Dp, SCHWARZ, "fp64", J=J, K=K)
+    L.jk_autotune(b, Dp, SCHWARZ, "mixed", FP32_THR, J=J, K=K)
+    tune_s = time.perf_counter() - t0
     stream = torch.cuda.ExternalStream(L.stream_handle(b), device=dev)
 
-    def time_batch(use_graph):
+    def time_batch(use_graph, precision="fp64"):
         for _ in range(warmup):
-            L.jk(b, Dp, SCHWARZ, "fp64", J=J, K=K, use_graph=use_graph)
+            L.jk(b, Dp, SCHWARZ, precision, FP32_THR, J=J, K=K, use_graph=use_graph)
         torch.cuda.synchronize()
         ms = []
         for _ in range(steps):
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(stream)
-            L.jk(b, Dp, SCHWARZ, "fp64", J=J, K=K, use_graph=use_graph)
+            L.jk(b, Dp, SCHWARZ, precision, FP32_THR, J=J, K=K, use_graph=use_graph)
             e1.record(stream)
             e1.synchronize()
             ms.append(e0.elapsed_time(e1))
         return float(np.mean(ms))
 
+    # the mixed-precision batch (FP32 for every class up to (ff|ff)): time and largest per-molecule
+    # energy error against the FP64 batch
+    t_mixed = time_batch(True, "mixed")
+    Jx, Kx = J.cpu().numpy(), K.cpu().numpy()
+    L.jk(b, Dp, SCHWARZ, "fp64", J=J, K=K)
+    J64, K64 = J.cpu().numpy(), K.cpu().numpy()
+    Dh = Dp.cpu().numpy()
+    dE_mixed = max(abs(float(np.sum(d * (0.5 * (jx - j) - 0.25 * (kx - k)))))
+                   for d, j, k, jx, kx in zip(b.unpack(Dh), b.unpack(J64), b.unpack(K64), b.unpack(Jx), b.unpack(Kx)))
     t_direct = time_batch(False)
     t_graph = time_batch(True)
     flops = plan["flops_fp64"]
@@ -235,8 +250,9 @@ def run_batch(steps, warmup, dev):
     nq = plan["n_quartets"]
     return {"workload": "64 water clusters, 1..12 waters, half cc-pVDZ / half cc-pVTZ, FP64, Schwarz 1e-12",
             "n_molecules": len(specs), "n_quartets": nq, "n_prim_quartets": plan["n_prim_quartets"],
-            "packed_elements": int(b.packed), "setup_s": setup_s,
+            "packed_elements": int(b.packed), "setup_s": setup_s, "autotune_s": tune_s,
             "batched_graph_ms": t_graph, "batched_direct_ms": t_direct, "sequential_single_ms": t_seq,
+            "mixed_batched_graph_ms": t_mixed, "mixed_max_abs_dE_Eh_per_molecule": dE_mixed,
             "quartets_per_s": nq / (t_graph * 1e-3), "speedup_vs_sequential": t_seq / t_graph,
             "algorithmic_fp64_tflops": flops / (t_graph * 1e-3) / 1e12,
             "max_abs_dJ_vs_single": err}
@@ -245,22 +261,31 @@ def run_batch(steps, warmup, dev):
 def run_rij(Z, xyz, D, J64, steps):
     """RI-J of the (H2O)_32 workload with the even-tempered s-f auxiliary basis (0.1 * 2.5^k,
     k = 0..11 per l and atom): wall time of one lible_gpu_rij call from host D to host J (both
-    three-centre contractions, the (P|Q) build and its solve), and the RI error against the direct
-    FP64 J of the same run."""
+    contractions over the kept three-centre tensor, and the solve with the cached metric factor;
+    the first call, which builds both, is timed separately), the rate at which a call reads the
+    tensor (two passes, whole-call time), and the RI error against the direct FP64 J of the same run."""
     from lible_b200 import ints as L
     from lible_b200.workloads import even_tempered_aux
 
     t0 = time.perf_counter()
     s = L.Structure("cc-pvdz", Z, xyz, even_tempered_aux(Z), units="bohr")
     setup = time.perf_counter() - t0
-    Jri, _, _ = L.rij(s, D, SCHWARZ)  # warm-up: plans, Schwarz factors of the auxiliary classes
+    # first call: plans, Schwarz factors of the auxiliary classes, the metric factor and the kept
+    # three-centre tensor
+    t0 = time.perf_counter()
+    Jri, _, _ = L.rij(s, D, SCHWARZ)
+    first = time.perf_counter() - t0
     ts = []
     for _ in range(max(1, steps)):
         t = time.perf_counter()
         Jri, _, _ = L.rij(s, D, SCHWARZ)
         ts.append(time.perf_counter() - t)
+    tensor_bytes = 8.0 * s.naux * s.nao * s.nao
     return {"workload": "RI-J, (H2O)_32 cc-pVDZ, even-tempered s-f auxiliary basis, FP64", "naux": s.naux,
-            "setup_s": setup, "rij_s": float(np.mean(ts)), "solve": L.rij_last_solve(s),
+            "setup_s": setup, "first_call_s": first, "rij_s": float(np.mean(ts)),
+            "tensor_bytes": tensor_bytes,
+            "tensor_read_gbs": 2 * tensor_bytes / float(np.mean(ts)) / 1e9,
+            "solve": L.rij_last_solve(s),
             "dEJ_Eh_vs_direct": float(0.5 * np.sum(D * (Jri - J64))),
             "dJ_fro_vs_direct": float(np.linalg.norm(Jri - J64))}
 

@@ -87,6 +87,7 @@ SIGNATURES = {
     "lible_gpu_rij_last_solve": [P, P, P, P, P, P],
     "lible_gpu_rik": [P, P, P, LL, D, P, ctypes.POINTER(RIKInfo)],
     "lible_gpu_rik_set_fitted": [P, I],
+    "lible_gpu_rij_set_cached": [P, I],
     "lible_gpu_rij_grad": [P, P, D, P, ctypes.POINTER(D)],
     "lible_gpu_overlap": [P, P],
     "lible_gpu_kinetic_energy": [P, P],

@@ -44,11 +44,16 @@ struct lible_gpu_ctx
     // rik_fitted_mode 0 = never build it (stream the integrals on every call), 1 = when it fits
     std::unique_ptr<FittedTensor> fitted;
     int rik_fitted_mode = 1;
+    // three-centre tensor (mn|P) of the RI-J calls, kept when it fits (rij_cached_mode 1) so that
+    // every later RI-J is two streaming passes over it instead of two integral evaluations
+    std::unique_ptr<CachedT3> t3;
+    int rij_cached_mode = 1;
 
     void structureChanged()
     {
         metric.reset();
         fitted.reset();
+        t3.reset();
     }
     const MetricFactor &metricFactor(Engine &e)
     {
@@ -968,7 +973,28 @@ int lible_gpu_rij(lible_gpu_ctx *ctx, const double *D, double schwarz_threshold,
         DevArray j(J, n * n, false, e.stream());
         DevBuf<double> rhs_b(na);
         double *rhs = rhs_b.p;
-        e.riContract(d.ptr, nullptr, rhs, nullptr, schwarz_threshold);
+        // the tensor (naux * nao^2 doubles) is built by the first call when it takes at most 60% of
+        // the free memory and kept until the structure, the threshold or the mode changes
+        if (ctx->t3 && (ctx->t3->schwarz != schwarz_threshold || ctx->rij_cached_mode == 0))
+            ctx->t3.reset();
+        if (!ctx->t3 && ctx->rij_cached_mode == 1)
+        {
+            size_t free_b = 0, total_b = 0;
+            cudaCheck(cudaMemGetInfo(&free_b, &total_b), "meminfo");
+            if (na * n * n * sizeof(double) <= (size_t)(0.6 * (double)free_b))
+            {
+                auto t = std::make_unique<CachedT3>();
+                buildT3(e, schwarz_threshold, *t);
+                ctx->t3 = std::move(t);
+            }
+        }
+        if (ctx->t3)
+        {
+            t3Gamma(e, *ctx->t3, d.ptr, rhs);
+            e.sync();
+        }
+        else
+            e.riContract(d.ptr, nullptr, rhs, nullptr, schwarz_threshold);
         if (gamma)
         {
             e.sync();
@@ -979,8 +1005,25 @@ int lible_gpu_rij(lible_gpu_ctx *ctx, const double *D, double schwarz_threshold,
         if (dcoef)
             cudaCheck(cudaMemcpy(dcoef, rhs, na * 8, isDevice(dcoef) ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost),
                       "copy");
-        e.riContract(nullptr, rhs, nullptr, j.ptr, schwarz_threshold);
+        if (ctx->t3)
+        {
+            t3Coulomb(e, *ctx->t3, rhs, j.ptr);
+            e.sync();
+        }
+        else
+            e.riContract(nullptr, rhs, nullptr, j.ptr, schwarz_threshold);
         j.copyOut();
+    });
+}
+
+int lible_gpu_rij_set_cached(lible_gpu_ctx *ctx, int mode)
+{
+    return guard(ctx, [&](Engine &) {
+        if (mode != 0 && mode != 1)
+            throw EngineError(kStatusInvalid, "mode must be 0 (evaluate on every call) or 1 (cache when it fits)");
+        ctx->rij_cached_mode = mode;
+        if (mode == 0)
+            ctx->t3.reset();
     });
 }
 

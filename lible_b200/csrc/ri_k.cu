@@ -1,4 +1,5 @@
-// RI metric factorisation (shared by RI-J and RI-K) and the RI exchange build
+// RI metric factorisation (shared by RI-J and RI-K), the cached three-centre tensor of RI-J and the
+// RI exchange build
 //     K_mn = sum_{PQ} (m l|P) [(P|Q)^{-1}]_{PQ} (Q|n s) D_ls,   D = C C^T.
 // The reference exposes the three- and two-centre kernels this builds on (ERI3Kernel / eri2,
 // src/lible/ints/twoel/eri_kernels.cpp:1122-1162) but no RI exchange driver.
@@ -210,12 +211,62 @@ namespace lible_b200
     {
         const int na = (int)mf.naux;
         const cudaStream_t s = e.stream();
-        if (mf.method == 0 || mf.method == 2)
+        if (!mf.solver)
+            mf.solver = std::make_unique<SolverHandle>(s);
+        if (mf.method == 2)
         {
-            SolverHandle sh(s);
             DevBuf<int> info(1);
-            cusolverDnDpotrs(sh.h, CUBLAS_FILL_MODE_LOWER, na, 1, mf.fac.p, na, rhs, na, info.p);
+            cusolverDnDpotrs(mf.solver->h, CUBLAS_FILL_MODE_LOWER, na, 1, mf.fac.p, na, rhs, na, info.p);
             cudaCheck(cudaStreamSynchronize(s), "potrs");
+            return;
+        }
+        if (mf.method == 0)
+        {
+            // M^{-1} from the factor once (potri), then per solve one DSYMV and one step of iterative
+            // refinement against the factor (two DTRMV and a second DSYMV) instead of two
+            // triangular solves with a single right-hand side: matrix-vector products stream the
+            // triangle at HBM rate, and the refinement brings the explicit inverse's error (~cond(M)
+            // eps, cond up to 1e10 for even-tempered fitting sets) back to the level of the
+            // triangular solves
+            if (!mf.inv.p)
+            {
+                mf.inv.reset((size_t)na * na);
+                cudaCheck(cudaMemcpyAsync(mf.inv.p, mf.fac.p, (size_t)na * na * sizeof(double),
+                                          cudaMemcpyDeviceToDevice, s),
+                          "copy");
+                DevBuf<int> info(1);
+                DevBuf<double> work;
+                int lwork = 0;
+                cusolverDnDpotri_bufferSize(mf.solver->h, CUBLAS_FILL_MODE_LOWER, na, mf.inv.p, na, &lwork);
+                work.reset((size_t)std::max(lwork, 1));
+                cusolverDnDpotri(mf.solver->h, CUBLAS_FILL_MODE_LOWER, na, mf.inv.p, na, work.p, lwork, info.p);
+                int hinfo = 0;
+                cudaCheck(cudaMemcpyAsync(&hinfo, info.p, sizeof(int), cudaMemcpyDeviceToHost, s), "info");
+                cudaCheck(cudaStreamSynchronize(s), "potri");
+                if (hinfo != 0)
+                {
+                    mf.inv.clear();
+                    throw EngineError(kStatusInternal, "inverse of the RI metric failed (info " +
+                                                           std::to_string(hinfo) + ")");
+                }
+            }
+            if (!mf.blas)
+                mf.blas = std::make_unique<BlasHandle>(s);
+            const cublasHandle_t h = mf.blas->h;
+            DevBuf<double> x(mf.naux), t(mf.naux);
+            const double one = 1.0, zero = 0.0, mone = -1.0;
+            // x0 = M^{-1} b
+            blasCheck(cublasDsymv(h, CUBLAS_FILL_MODE_LOWER, na, &one, mf.inv.p, na, rhs, 1, &zero, x.p, 1), "symv");
+            // r = b - L L^T x0 (in place of b), then x = x0 + M^{-1} r
+            cudaCheck(cudaMemcpyAsync(t.p, x.p, mf.naux * sizeof(double), cudaMemcpyDeviceToDevice, s), "copy");
+            blasCheck(cublasDtrmv(h, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_T, CUBLAS_DIAG_NON_UNIT, na, mf.fac.p, na, t.p, 1),
+                      "trmv");
+            blasCheck(cublasDtrmv(h, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT, na, mf.fac.p, na, t.p, 1),
+                      "trmv");
+            blasCheck(cublasDaxpy(h, na, &mone, t.p, 1, rhs, 1), "axpy");
+            blasCheck(cublasDsymv(h, CUBLAS_FILL_MODE_LOWER, na, &one, mf.inv.p, na, rhs, 1, &one, x.p, 1), "symv");
+            cudaCheck(cudaMemcpyAsync(rhs, x.p, mf.naux * sizeof(double), cudaMemcpyDeviceToDevice, s), "copy");
+            cudaCheck(cudaStreamSynchronize(s), "symv");
             return;
         }
         // d = G (G^T gamma)
@@ -412,6 +463,145 @@ namespace lible_b200
             stats->flops_gemm += 2.0 * (double)na * (double)n * (double)n * (double)occ;
             stats->flops_syrk += (double)n * (double)(n + 1) * (double)na * (double)occ;
         }
+    }
+
+    namespace
+    {
+        // gamma[P] = sum_e T[P][e] D[e], e over the n^2 elements: one block per row P (rows of n^2
+        // doubles streamed once from HBM, D read from L2), a block reduction of 256 partial sums.
+        // Rows are read as double2 when n^2 is even (every row then starts on 16 bytes).
+        template <bool VEC>
+        __global__ void __launch_bounds__(256) t3GammaKernel(const double *__restrict__ T, const double *__restrict__ D,
+                                                             long long n2, long long naux, double *__restrict__ gamma)
+        {
+            __shared__ double red[8];
+            for (long long P = blockIdx.x; P < naux; P += gridDim.x)
+            {
+                double s0 = 0.0, s1 = 0.0;
+                if constexpr (VEC)
+                {
+                    const double2 *row = reinterpret_cast<const double2 *>(T + P * n2);
+                    const double2 *d2 = reinterpret_cast<const double2 *>(D);
+                    for (long long e = threadIdx.x; e < n2 / 2; e += 256)
+                    {
+                        const double2 t = __ldcs(row + e);  // streamed once: no reuse in L2
+                        const double2 d = __ldg(d2 + e);
+                        s0 = fma(t.x, d.x, s0);
+                        s1 = fma(t.y, d.y, s1);
+                    }
+                }
+                else
+                {
+                    for (long long e = threadIdx.x; e < n2; e += 256)
+                        s0 = fma(__ldcs(T + P * n2 + e), __ldg(D + e), s0);
+                }
+                double v = s0 + s1;
+                for (int o = 16; o > 0; o >>= 1)
+                    v += __shfl_down_sync(0xffffffffu, v, o);
+                if ((threadIdx.x & 31) == 0)
+                    red[threadIdx.x >> 5] = v;
+                __syncthreads();
+                if (threadIdx.x == 0)
+                {
+                    double t = 0.0;
+                    for (int w = 0; w < 8; w++)
+                        t += red[w];
+                    gamma[P] = t;
+                }
+                __syncthreads();
+            }
+        }
+
+        // J[e] += sum_{P in the block's range} d[P] T[P][e]: blocks tile the n^2 elements (a double2
+        // per thread when n^2 is even, else one double) and split the auxiliary range in slices of
+        // `per`; each element of T is read once, two rows in flight per step.
+        template <bool VEC>
+        __global__ void __launch_bounds__(256) t3CoulombKernel(const double *__restrict__ T, const double *__restrict__ dcoef,
+                                                               long long n2, long long naux, long long per,
+                                                               double *__restrict__ J)
+        {
+            const long long e = (long long)blockIdx.x * 256 + threadIdx.x;
+            const long long P0 = (long long)blockIdx.y * per, P1 = P0 + per < naux ? P0 + per : naux;
+            if constexpr (VEC)
+            {
+                if (2 * e >= n2)
+                    return;
+                double a0 = 0.0, a1 = 0.0, b0 = 0.0, b1 = 0.0;
+                long long P = P0;
+                for (; P + 1 < P1; P += 2)
+                {
+                    const double2 t0 = __ldcs(reinterpret_cast<const double2 *>(T + P * n2) + e);
+                    const double2 t1 = __ldcs(reinterpret_cast<const double2 *>(T + (P + 1) * n2) + e);
+                    const double d0 = __ldg(dcoef + P), d1 = __ldg(dcoef + P + 1);
+                    a0 = fma(t0.x, d0, a0);
+                    a1 = fma(t0.y, d0, a1);
+                    b0 = fma(t1.x, d1, b0);
+                    b1 = fma(t1.y, d1, b1);
+                }
+                if (P < P1)
+                {
+                    const double2 t0 = __ldcs(reinterpret_cast<const double2 *>(T + P * n2) + e);
+                    const double d0 = __ldg(dcoef + P);
+                    a0 = fma(t0.x, d0, a0);
+                    a1 = fma(t0.y, d0, a1);
+                }
+                atomicAdd(J + 2 * e, a0 + b0);
+                atomicAdd(J + 2 * e + 1, a1 + b1);
+            }
+            else
+            {
+                if (e >= n2)
+                    return;
+                double a0 = 0.0;
+                for (long long P = P0; P < P1; P++)
+                    a0 = fma(__ldcs(T + P * n2 + e), __ldg(dcoef + P), a0);
+                atomicAdd(J + e, a0);
+            }
+        }
+    }
+
+    void buildT3(Engine &e, double schwarz, CachedT3 &t3)
+    {
+        const size_t n = e.nao(), na = e.naux();
+        t3.T.reset(na * n * n);
+        EventPair ev;
+        cudaCheck(cudaEventRecord(ev.a, e.stream()), "event");
+        e.riStore(0, (int)na, t3.T.p, schwarz);
+        e.checkStatus();
+        cudaCheck(cudaEventRecord(ev.b, e.stream()), "event");
+        cudaCheck(cudaEventSynchronize(ev.b), "three-centre tensor");
+        t3.schwarz = schwarz;
+        t3.naux = na;
+        t3.nao = n;
+        t3.t_build = ev.seconds();
+    }
+
+    void t3Gamma(Engine &e, const CachedT3 &t3, const double *D_dev, double *gamma_dev)
+    {
+        const long long n2 = (long long)(t3.nao * t3.nao), na = (long long)t3.naux;
+        const int grid = (int)std::min<long long>(na, 148LL * 8);
+        if (n2 % 2 == 0)
+            t3GammaKernel<true><<<grid, 256, 0, e.stream()>>>(t3.T.p, D_dev, n2, na, gamma_dev);
+        else
+            t3GammaKernel<false><<<grid, 256, 0, e.stream()>>>(t3.T.p, D_dev, n2, na, gamma_dev);
+        cudaCheck(cudaGetLastError(), "t3 gamma");
+    }
+
+    void t3Coulomb(Engine &e, const CachedT3 &t3, const double *d_dev, double *J_dev)
+    {
+        const long long n2 = (long long)(t3.nao * t3.nao), na = (long long)t3.naux;
+        cudaCheck(cudaMemsetAsync(J_dev, 0, (size_t)n2 * sizeof(double), e.stream()), "memset");
+        const bool vec = n2 % 2 == 0;
+        const long long blocks = ((vec ? n2 / 2 : n2) + 255) / 256;
+        // enough auxiliary slices to give every SM several blocks
+        const long long ps = std::max<long long>(1, std::min<long long>(na, (148LL * 16 + blocks - 1) / blocks));
+        const long long per = (na + ps - 1) / ps;
+        const dim3 grid((unsigned)blocks, (unsigned)((na + per - 1) / per));
+        if (vec)
+            t3CoulombKernel<true><<<grid, 256, 0, e.stream()>>>(t3.T.p, d_dev, n2, na, per, J_dev);
+        else
+            t3CoulombKernel<false><<<grid, 256, 0, e.stream()>>>(t3.T.p, d_dev, n2, na, per, J_dev);
+        cudaCheck(cudaGetLastError(), "t3 coulomb");
     }
 
     void splitDensity(Engine &e, const double *D_dev, long long n, DevBuf<double> &Cp, long long &n_pos,

@@ -9,6 +9,7 @@
 #include <cusolverDn.h>
 
 #include <algorithm>
+#include <memory>
 
 namespace lible_b200
 {
@@ -27,6 +28,12 @@ namespace lible_b200
             n = 0;
             cudaCheck(cudaMalloc(&p, std::max<size_t>(count, 1) * sizeof(T)), "cudaMalloc");
             n = count;
+        }
+        void clear()
+        {
+            cudaFree(p);
+            p = nullptr;
+            n = 0;
         }
         ~DevBuf() { cudaFree(p); }
         DevBuf(const DevBuf &) = delete;
@@ -79,6 +86,13 @@ namespace lible_b200
         int dropped = 0;
         size_t naux = 0;
         DevBuf<double> fac;
+        // M^{-1} (lower triangle, column-major), formed from the Cholesky factor by the first solve
+        // of method 0 (a positive definite metric), so that every solve is one symmetric
+        // matrix-vector product; the shifted and eigen methods keep their solves
+        mutable DevBuf<double> inv;
+        // solver and cuBLAS handles of the solves, created once
+        mutable std::unique_ptr<SolverHandle> solver;
+        mutable std::unique_ptr<BlasHandle> blas;
     };
     void factorMetric(Engine &e, MetricFactor &mf);
 
@@ -114,6 +128,21 @@ namespace lible_b200
     // K += sign * sum_R (B_R C)(B_R C)^T with the cached tensor (same contract as riExchange).
     void riExchangeFitted(Engine &e, BlasHandle &bh, const FittedTensor &ft, const double *C_dev, long long occ,
                           double sign, double *K_dev, RIKStats *stats);
+
+    // The raw three-centre tensor T[P][m][n] = (mn|P) (both orientations of each pair, Schwarz
+    // screened), kept in HBM by the RI-J calls when it fits; each RI-J is then two passes over it.
+    struct CachedT3
+    {
+        DevBuf<double> T;
+        double schwarz = -1;
+        size_t naux = 0, nao = 0;
+        double t_build = 0;  // seconds of the build
+    };
+    void buildT3(Engine &e, double schwarz, CachedT3 &t3);
+    // gamma_P = sum_mn T[P][mn] D_mn (full sum over both triangles).
+    void t3Gamma(Engine &e, const CachedT3 &t3, const double *D_dev, double *gamma_dev);
+    // J_mn = sum_P T[P][mn] d_P (symmetric by construction).
+    void t3Coulomb(Engine &e, const CachedT3 &t3, const double *d_dev, double *J_dev);
 
     // Mirrors the row-major upper triangle of the n x n matrix into the lower one.
     void mirrorUpper(double *K_dev, long long n, cudaStream_t s);

@@ -608,6 +608,12 @@ def rik_set_fitted(structure, mode):
     _call(structure, "lible_gpu_rik_set_fitted", int(mode))
 
 
+def rij_set_cached(structure, mode):
+    """1 (default): rij() keeps the three-centre tensor (mn|P) on the context when it fits; 0:
+    evaluate the integrals on every call (and drop a cached tensor)."""
+    _call(structure, "lible_gpu_rij_set_cached", int(mode))
+
+
 def ri_contract(structure, D=None, dcoef=None, schwarz=1e-12):
     """gamma_P = sum (mn|P) D_mn (if D is given) and J_mn = sum_P (mn|P) d_P (if dcoef is given)."""
     n, na = structure.nao, structure.naux

@@ -129,9 +129,20 @@ def test_gpu_rik_matches_golden():
     K2, info2 = L.rik(s, D=g["D2"], schwarz=0.0, info=True)
     assert info2["n_pos"] == 6 and info2["n_neg"] == 3
     assert np.abs(K2 - g["K2"]).max() <= 1e-10
-    J, _, _ = L.rij(s, g["C"] @ g["C"].T, schwarz=0.0)
+    J, gam, dco = L.rij(s, g["C"] @ g["C"].T, schwarz=0.0)
     assert np.abs(J - g["J"]).max() <= 1e-10
     assert L.rij_last_solve(s)["method"] == "cholesky"
+    # that call contracted the cached three-centre tensor; evaluating the integrals on every call
+    # gives the same J, gamma and fitting coefficients (summation order differs only)
+    L.rij_set_cached(s, 0)
+    Jn, gn, dn = L.rij(s, g["C"] @ g["C"].T, schwarz=0.0)
+    assert np.abs(Jn - g["J"]).max() <= 1e-10
+    assert np.abs(Jn - J).max() <= 1e-12
+    assert np.abs(gn - gam).max() <= 1e-12 * max(1.0, np.abs(gn).max())
+    assert np.abs(dn - dco).max() <= 1e-10 * max(1.0, np.abs(dn).max())
+    L.rij_set_cached(s, 1)
+    Jc, gc, dc = L.rij(s, g["C"] @ g["C"].T, schwarz=0.0)
+    assert np.abs(Jc - J).max() <= 1e-12 and np.abs(gc - gam).max() <= 1e-12 * max(1.0, np.abs(gc).max())
     # the first call built the fitted three-centre tensor; the streaming path gives the same K
     assert info["fitted"] == 1 and info2["fitted"] == 1
     L.rik_set_fitted(s, 0)
