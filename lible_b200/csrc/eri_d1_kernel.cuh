@@ -192,7 +192,7 @@ namespace lible_b200
                     boysF<L1, false>(alpha * (X * X + Y * Y + Z * Z), a.boys + L1 * kBoysTerms * kBoysPitch, F);
                     const double m2a = -2.0 * alpha;
                     double *cur = rb, *nxt = rb + C::NR1;
-                    if (tid == 0)
+                    if (!closedFormR<L1>() && tid == 0)
                     {
                         double pw = 1.0;
                         for (int k = 0; k < L1; k++)
@@ -212,6 +212,12 @@ namespace lible_b200
                         ecd = ek;
                         e1cd = ek + C::HCD * C::SCD;
                     }
+                    if constexpr (closedFormR<L1>())
+                    {
+                        groupHermiteR<L1, double>(F, fac, m2a, X, Y, Z, nxt, cur, ht, tid, G);
+                    }
+                    else
+                    {
                     __syncthreads();
 #pragma unroll
                     for (int n = L1 - 1; n >= 0; n--)
@@ -256,6 +262,7 @@ namespace lible_b200
                         double *tmp = cur;
                         cur = nxt;
                         nxt = tmp;
+                    }
                     }
                     const double cq = cexp / Q.x;
                     // shifted R (passes x, y, z) and plain R (pass 3, and the E1_cd terms of the
@@ -908,8 +915,14 @@ namespace lible_b200
                             ec[3 * EC_SZ + o] = __ldg(e1cd + 2 * C::HCD * C::SCD + e);
                         }
                     }
-                    // R to order L + 1 (levels split over the block)
+                    // R to order L + 1 (closed form, or levels split over the block)
                     double *cur = rb, *nxt = rb + C::NR1;
+                    if constexpr (closedFormR<L1>())
+                    {
+                        groupHermiteR<L1, double>(F, fac, m2a, X, Y, Z, nxt, cur, ht, tid, G);
+                    }
+                    else
+                    {
                     if (tid == 0)
                     {
                         double pw = 1.0;
@@ -961,6 +974,7 @@ namespace lible_b200
                         double *tmp = cur;
                         cur = nxt;
                         nxt = tmp;
+                    }
                     }
                     // the seven W products per tile, consumed in registers
                     double ax = 0, ay = 0, az = 0, c2x = 0, c2y = 0, c2z = 0;

@@ -192,6 +192,86 @@ namespace lible_b200
             __syncthreads();
     }
 
+    static __device__ HermAxisTable kHermAxis = makeHermAxisTable();
+
+    // Group paths of total angular momentum L build R from its closed form (groupHermiteR) when the
+    // staging fits the second R buffer and the expansion's extra terms stay few (it sums about 1.5x
+    // the recursion's terms at L = 8 and 2x at L = 12, but needs two group barriers instead of L + 1).
+    template <int L>
+    constexpr bool closedFormR()
+    {
+        return L >= 4 && L <= 10 && 3 * hermAxisOffset(L + 1) + L + 1 <= nherm(L);
+    }
+
+    // R_tuv (t + u + v <= L) of one primitive quartet into out[0 .. nherm(L)) by the G threads of a
+    // group, without the level-by-level recursion.  With g_n = fac (-2 alpha)^n F_n,
+    //   R_tuv = sum_{a <= t/2} sum_{b <= u/2} sum_{c <= v/2} A_x[t][a] A_y[u][b] A_z[v][c] g_{t+u+v-a-b-c},
+    //   A_x[t][a] = h(t, a) X^{t-2a}   (and A_y, A_z from Y, Z; h in HermAxisTable),
+    // which is the McMurchie-Davidson recursion R^{(n)}_{t+1,u,v} = t R^{(n+1)}_{t-1,u,v} +
+    // X R^{(n+1)}_{tuv} (Helgaker, Jorgensen, Olsen 9.9.18-9.9.20; src/lible/ints/rints.hpp:112-175)
+    // unrolled to its closed form.  Step 1 writes the three axis tables and g (3 NH + L + 1 values)
+    // to `stage`; step 2 sums every entry's terms.  Every thread of the group holds the same F, fac,
+    // alpha and X, Y, Z; `ht` is the block's (t, u, v, t + u + v) table of the entries.
+    template <int L, typename T>
+    __device__ __forceinline__ void groupHermiteR(const double (&F)[L + 1], double fac, double m2a, double X, double Y,
+                                                  double Z, T *stage, T *out, const char4 *ht, int tid, int G)
+    {
+        constexpr int NH = hermAxisOffset(L + 1);
+        constexpr int NS = 3 * NH + L + 1;
+        for (int j = tid; j < NS; j += G)
+        {
+            double base, pw;
+            int p;
+            if (j < 3 * NH)
+            {
+                const int axis = j >= 2 * NH ? 2 : (j >= NH ? 1 : 0);
+                const int idx = j - axis * NH;
+                base = axis == 0 ? X : (axis == 1 ? Y : Z);
+                pw = __ldg(&kHermAxis.c[idx]);
+                p = __ldg(&kHermAxis.p[idx]);
+            }
+            else
+            {
+                p = j - 3 * NH;
+                double fn = F[0];
+#pragma unroll
+                for (int k = 1; k <= L; k++)
+                    if (p == k)
+                        fn = F[k];
+                base = m2a;
+                pw = fn * fac;
+            }
+            while (p)
+            {
+                if (p & 1)
+                    pw *= base;
+                base *= base;
+                p >>= 1;
+            }
+            stage[j] = T(pw);
+        }
+        groupSync(G);
+        const T *Ax = stage, *Ay = stage + NH, *Az = stage + 2 * NH, *g = stage + 3 * NH;
+        for (int e = tid; e < nherm(L); e += G)
+        {
+            const char4 tv = ht[e];
+            const int t = tv.x, u = tv.y, v = tv.z;
+            const T *ax = Ax + hermAxisOffset(t), *ay = Ay + hermAxisOffset(u), *az = Az + hermAxisOffset(v);
+            const T *gt = g + tv.w;
+            T r = T(0);
+            for (int a = 0; 2 * a <= t; a++)
+                for (int b = 0; 2 * b <= u; b++)
+                {
+                    const T xy = ax[a] * ay[b];
+                    const T *gn = gt - a - b;
+                    for (int c = 0; 2 * c <= v; c++)
+                        r += xy * az[c] * gn[-c];
+                }
+            out[e] = r;
+        }
+        groupSync(G);
+    }
+
     template <typename T>
     __device__ __forceinline__ const T *braE(const PairView &v);
     template <>
@@ -653,8 +733,14 @@ namespace lible_b200
                 double F[C::L + 1];
                 boysF<C::L, false>(alpha * (X * X + Y * Y + Z * Z), a.boys + C::L * kBoysTerms * kBoysPitch, F);
                 const double m2a = -2.0 * alpha;
-                // level L
                 T *cur = rb, *nxt = rb + C::NR;
+                if constexpr (closedFormR<C::L>())
+                {
+                    groupHermiteR<C::L, T>(F, fac, m2a, X, Y, Z, nxt, cur, ht, tid, G);
+                }
+                else
+                {
+                // level L
                 double pw = 1.0;
                 for (int k = 0; k < C::L; k++)
                     pw *= m2a;
@@ -703,6 +789,7 @@ namespace lible_b200
                     T *tmp = cur;
                     cur = nxt;
                     nxt = tmp;
+                }
                 }
                 // signed R matrix [h'][h] and the staged ket E[q] [h'][cd]
                 for (int e = tid; e < C::HCD * C::HAB; e += G)
@@ -815,6 +902,12 @@ namespace lible_b200
                 boysF<C::L, false>(alpha * (X * X + Y * Y + Z * Z), a.boys + C::L * kBoysTerms * kBoysPitch, F);
                 const double m2a = -2.0 * alpha;
                 double *cur = rb, *nxt = rb + C::NR;
+                if constexpr (closedFormR<C::L>())
+                {
+                    groupHermiteR<C::L, double>(F, fac, m2a, X, Y, Z, nxt, cur, ht, tid, G);
+                }
+                else
+                {
                 double pw = 1.0;
                 for (int k = 0; k < C::L; k++)
                     pw *= m2a;
@@ -865,6 +958,7 @@ namespace lible_b200
                     double *tmp = cur;
                     cur = nxt;
                     nxt = tmp;
+                }
                 }
                 // signed R matrix rm[h'][h] and the staged ket E[q] ec[h'][c]
                 for (int e = tid; e < C::HCD * C::HAB; e += G)

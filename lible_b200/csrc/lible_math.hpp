@@ -56,6 +56,32 @@ namespace lible_b200
         return nherm(t + u + v - 1) + cartIndex(u, v);
     }
 
+    // One-dimensional Hermite expansion behind the closed form of R_tuv: with g_n = (-2 alpha)^n F_n
+    // and d/dX g_n = X g_{n+1}, d^t/dX^t g_0 = sum_{a <= t/2} h(t, a) X^{t-2a} g_{t-a} with
+    // h(t, a) = t! / (a! (t - 2a)! 2^a).  Entry hermAxisOffset(t) + a of the table holds h(t, a)
+    // and the power t - 2a, for t = 0..kMaxLTotal.
+    LB_HD constexpr int hermAxisOffset(int t) { return (t / 2) * (t / 2 + 1) + ((t & 1) ? t / 2 + 1 : 0); }
+    constexpr int kHermAxisEntries = hermAxisOffset(kMaxLTotal + 1);
+    struct HermAxisTable
+    {
+        double c[kHermAxisEntries];
+        int p[kHermAxisEntries];
+    };
+    constexpr HermAxisTable makeHermAxisTable()
+    {
+        HermAxisTable tab{};
+        for (int t = 0; t <= kMaxLTotal; t++)
+            for (int a = 0; 2 * a <= t; a++)
+            {
+                double h = 1.0;  // h(t, i + 1) = h(t, i) (t - 2i) (t - 2i - 1) / (2 (i + 1)), exact integers
+                for (int i = 0; i < a; i++)
+                    h = h * (t - 2 * i) * (t - 2 * i - 1) / (2.0 * (i + 1));
+                tab.c[hermAxisOffset(t) + a] = h;
+                tab.p[hermAxisOffset(t) + a] = t - 2 * a;
+            }
+        return tab;
+    }
+
     // Derivative classes whose J/K-gradient contraction runs in registers (eriD1RegKernel): a group
     // of g threads per quartet, each owning S_cd / g ket columns, with its Gamma-weighted bra
     // coefficients (4 x H_ab x S_cd / g values) and the R vector to order L + 1 within 170 doubles
