@@ -131,6 +131,17 @@ namespace lible_b200
         return {a.x, a.y, b.x, b.y, c.x};
     }
 
+    // One task of the block-per-quartet (group) paths, decoded ahead of its evaluation: pair
+    // indices, primitive ranges, whether it lies in the launch's window, and the first bra / ket
+    // primitive records.
+    struct GroupTask
+    {
+        uint32_t ib, ik, p0, p1, q0, q1;
+        int ok, pad;
+        PQ4 P, Q;
+    };
+    constexpr int kGroupTaskBatch = 32;  // tasks a block decodes at once, one per thread
+
     // Largest major position i >= lo with prefix[i] <= t, given prefix[lo] <= t: gallops forward
     // from the caller's cursor, so walking consecutive tasks costs a load or two, not a full search.
     __device__ __forceinline__ int advanceMajor(const QuartetArgs &a, long long t, int lo)
@@ -229,6 +240,30 @@ namespace lible_b200
         const double qb = (by_pos && a.bra_qpos) ? __ldg(a.bra_qpos + pos) : __ldg(a.bra_qpair + ib);
         const double qq = qb * __ldg(a.ket_qpair + ik);
         return qq >= a.q_lo && qq < a.q_hi;
+    }
+
+    // Decodes task t into g (the thread's cursor `cur` moves forward, as in decodeCursor).
+    __device__ __forceinline__ void loadGroupTask(const QuartetArgs &a, long long t, int &cur, GroupTask &g)
+    {
+        uint32_t ib, ik;
+        decodeCursor(a, t, cur, ib, ik);
+        const bool ok = inWindow(a, ib, ik, 0, false);
+        g.ib = ib;
+        g.ik = ik;
+        g.ok = ok;
+        if (ok)
+        {
+            const uint32_t p0 = __ldg(a.bra.pofs + ib), p1 = __ldg(a.bra.pofs + ib + 1);
+            const uint32_t q0 = __ldg(a.ket.pofs + ik), q1 = __ldg(a.ket.pofs + ik + 1);
+            g.p0 = p0;
+            g.p1 = p1;
+            g.q0 = q0;
+            g.q1 = q1;
+            if (p0 < p1)
+                g.P = loadPQ(a.bra.pP, p0);
+            if (q0 < q1)
+                g.Q = loadPQ(a.ket.pP, q0);
+        }
     }
 
     // Degeneracy weight of a unique quartet: 1/2 for each coinciding shell pair / pair pair.

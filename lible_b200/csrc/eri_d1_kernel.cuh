@@ -424,9 +424,12 @@ namespace lible_b200
             }
         };
 
+        // the block's tasks come in increasing order, so one forward-moving cursor decodes them
+        // (a load or two per task instead of a binary search)
+        int cur = 0;
         auto runTask = [&](long long task) {
             uint32_t ib, ik;
-            decodeTask(a, task, ib, ik);
+            decodeCursor(a, task, cur, ib, ik);
             if (inWindow(a, ib, ik, 0, false))
                 processTask(task, ib, ik);
         };
@@ -637,8 +640,11 @@ namespace lible_b200
         constexpr int CW = Cls<LA, LB, LC, LD>::SCD / GT;
         constexpr unsigned used = QPW * GT == 32 ? 0xffffffffu : ((1u << (QPW * GT)) - 1u);
         const int slot = lane / GT, member = lane % GT;
+        // the task cursor carries over between the warp's chunks (increasing task order)
+        int cur = 0;
         auto processRange = [&](long long start, long long end) {
-            int cur = a.list ? 0 : advanceMajor(a, start, 0);
+            if (!a.list)
+                cur = advanceMajor(a, start, cur);
             for (long long base = start; base < end; base += QPW)
             {
                 const long long t = base + slot;
@@ -1073,9 +1079,11 @@ namespace lible_b200
             __syncthreads();
         };
 
+        // the block's tasks come in increasing order, so one forward-moving cursor decodes them
+        int cur = 0;
         auto runTask = [&](long long task) {
             uint32_t ib, ik;
-            decodeTask(a, task, ib, ik);
+            decodeCursor(a, task, cur, ib, ik);
             if (inWindow(a, ib, ik, 0, false))
                 processTask(ib, ik);
         };

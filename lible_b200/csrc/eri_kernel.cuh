@@ -102,7 +102,8 @@ namespace lible_b200
         static constexpr size_t m_off_ix = a16(m_off_rx + 8 * (size_t)MT * 8 * P_EC);    // HCD x HAB int16
         static constexpr size_t m_off_ht = a16(m_off_ix + 2 * C::HCD * C::HAB);          // NR char4
         static constexpr size_t m_off_mb = a16(m_off_ht + 4 * C::NR);                    // mbarrier
-        static constexpr size_t m_smem = m_off_mb + 16;
+        static constexpr size_t m_off_tb = m_off_mb + 16;                                // decoded tasks
+        static constexpr size_t m_smem = m_off_tb + sizeof(GroupTask) * kGroupTaskBatch;
         // bytes of one padded ket E tile (KT*4 rows of P_EC doubles), the unit of the bulk copy
         static constexpr unsigned ec_tile_bytes = 8u * KT * 4 * P_EC;
         static constexpr int W0 = ((C::HAB * C::SCD + C::SAB * C::SCD) <= 64 * 32)    ? 1
@@ -855,7 +856,7 @@ namespace lible_b200
     // Returns false when a bounded wait on a ket tile gave up (status word set): the block has then
     // let any copy still in flight land (again bounded) and must stop without using the batch.
     template <int LA, int LB, int LC, int LD, int SV = 0>
-    __device__ __forceinline__ bool quartetGroupMMA(const QuartetArgs &a, uint32_t ib, uint32_t ik,
+    __device__ __forceinline__ bool quartetGroupMMA(const QuartetArgs &a, const GroupTask &g,
                                                     unsigned char *smem, double (&v)[Shape<LA, LB, LC, LD, double, SV>::TPW2][2],
                                                     unsigned &phase)
     {
@@ -878,11 +879,11 @@ namespace lible_b200
 #pragma unroll
         for (int i = 0; i < S::TPW2; i++)
             v[i][0] = v[i][1] = 0.0;
-        const uint32_t p0 = a.bra.pofs[ib], p1 = a.bra.pofs[ib + 1];
-        const uint32_t q0 = a.ket.pofs[ik], q1 = a.ket.pofs[ik + 1];
+        const uint32_t p0 = g.p0, p1 = g.p1;
+        const uint32_t q0 = g.q0, q1 = g.q1;
         for (uint32_t p = p0; p < p1; p++)
         {
-            const PQ4 P = loadPQ(a.bra.pP, p);
+            const PQ4 P = p == p0 ? g.P : loadPQ(a.bra.pP, p);
             for (int e = tid; e < C::SAB * C::HAB; e += G)
                 ea[(e / C::HAB) * S::P_EA + e % C::HAB] = __ldg(a.bra.E + (size_t)p * C::SAB * C::HAB + e);
             double acc[S::TPW][2];
@@ -893,7 +894,7 @@ namespace lible_b200
             {
                 if (ket_tiles && tid == 0 && !a.wait_inject)
                     bulkLoad(ec, ket_tiles + (size_t)q * (S::ec_tile_bytes / 8), S::ec_tile_bytes, mbar);
-                const PQ4 Q = loadPQ(a.ket.pP, q);
+                const PQ4 Q = q == q0 ? g.Q : loadPQ(a.ket.pP, q);
                 const double rs = rsqrt(P.x + Q.x);
                 const double alpha = P.x * Q.x * (rs * rs);
                 const double X = P.y - Q.y, Y = P.z - Q.z, Z = P.w - Q.w;
@@ -1137,12 +1138,13 @@ namespace lible_b200
                 stageBoys(a.boys_f, C::L, reinterpret_cast<float *>(btab));
             __syncthreads();
             // each warp walks chunks of consecutive tasks (QPW per iteration); consecutive tasks
-            // share the major pair, so the task cursor rarely moves
+            // share the major pair, so the task cursor rarely moves.  A warp's chunks come in
+            // increasing task order, so the cursor carries over from one chunk to the next.
+            int cur = 0;
             // tasks [start, end) of one chunk, QPW quartets per warp step
             auto processRange = [&](long long start, long long end) {
-            int cur = 0;
             if (!a.list)
-                cur = advanceMajor(a, start, 0);
+                cur = advanceMajor(a, start, cur);
             for (long long base = start; base < end; base += QPW)
             {
                 const long long t = base + slot;
@@ -1269,20 +1271,32 @@ namespace lible_b200
             extern __shared__ __align__(16) unsigned char smem[];
             buildGroupTablesMMA<LA, LB, LC, LD, SV>(smem);
             double *vs = reinterpret_cast<double *>(smem + S::m_off_rx);
+            GroupTask *tasks = reinterpret_cast<GroupTask *>(smem + S::m_off_tb);
             const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, r8 = lane >> 2, k4 = lane & 3;
             unsigned phase = 0;  // parity of the block mbarrier's next phase
-            // one quartet at a time for the whole block, tasks [start, end) of a chunk; false = a
-            // bounded wait gave up and the block stops
-            auto processRange = [&](long long start, long long end) -> bool {
+            // each thread's task cursor: a block's chunks, and a thread's tasks in them, come in
+            // increasing task order, so the cursor only moves forward
             int cur = 0;
-            for (long long t = start; t < end; t++)
+            // one quartet at a time for the whole block, tasks [start, end) of a chunk; false = a
+            // bounded wait gave up and the block stops.  The tasks are decoded kGroupTaskBatch at a
+            // time, one per thread, with their primitive ranges and first primitive records, so each
+            // quartet starts from shared memory rather than a chain of dependent global loads.
+            auto processRange = [&](long long start, long long end) -> bool {
+            for (long long t0 = start; t0 < end; t0 += kGroupTaskBatch)
             {
-                uint32_t ib, ik;
-                decodeCursor(a, t, cur, ib, ik);
-                if (!inWindow(a, ib, ik, 0, false))
+            const int nb = (int)(end - t0 < kGroupTaskBatch ? end - t0 : kGroupTaskBatch);
+            if ((int)threadIdx.x < nb)
+                loadGroupTask(a, t0 + threadIdx.x, cur, tasks[threadIdx.x]);
+            __syncthreads();
+            for (int j = 0; j < nb; j++)
+            {
+                const GroupTask &gt = tasks[j];
+                if (!gt.ok)
                     continue;
+                const long long t = t0 + j;
+                const uint32_t ib = gt.ib, ik = gt.ik;
                 double v[S::TPW2][2];
-                if (!quartetGroupMMA<LA, LB, LC, LD, SV>(a, ib, ik, smem, v, phase))
+                if (!quartetGroupMMA<LA, LB, LC, LD, SV>(a, gt, smem, v, phase))
                     return false;
                 // element (m, c) of the batch held by this thread: tile rows / columns
 #pragma unroll
@@ -1322,6 +1336,8 @@ namespace lible_b200
                 }
                 __syncthreads();
             }
+            __syncthreads();  // every thread is done with the batch's task records
+            }
             return true;
             };
             if (a.chunks)
@@ -1354,9 +1370,10 @@ namespace lible_b200
             extern __shared__ __align__(16) unsigned char smem[];
             buildGroupTables<LA, LB, LC, LD, T, SV>(smem);
             T *vs = reinterpret_cast<T *>(smem + S::off_rx);
+            // the task cursor carries over between the block's chunks (increasing task order)
+            int cur = 0;
             // one quartet at a time for the whole block, tasks [start, end) of a chunk
             auto processRange = [&](long long start, long long end) {
-            int cur = 0;
             for (long long t = start; t < end; t++)
             {
                 uint32_t ib, ik;
