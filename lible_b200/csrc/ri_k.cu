@@ -94,6 +94,158 @@ namespace lible_b200
         {
             return (int)std::max<long long>(1, std::min<long long>((total + 255) / 256, 148LL * 16));
         }
+
+        // ---- symmetric rank-k update on the DMMA pipe -------------------------------------------
+        // K[r][c] += sign * sum_j Z[r][j] Z[c][j] for c >= r (the row-major upper triangle; callers
+        // mirror it), Z row-major n x k with an even row pitch ldz, so every row starts on 16 bytes.
+        // A block owns one 128 x 128 output tile on or above the diagonal and one slice of k; its 16
+        // warps own 32 x 32 sub-tiles as 4 x 4 mma.m8n8k4.f64 tiles.  The two 128-row operand panels
+        // stream through a 4-stage cp.async pipeline in 16-column steps (row pitch 20 doubles, so the
+        // fragment reads of a warp spread over all banks), and each partial sum reaches K by one FP64
+        // atomic per element and slice.  Algorithmic FLOPs: n (n + 1) k.
+        constexpr int kSyrkBM = 128, kSyrkKB = 16, kSyrkP = 20, kSyrkStages = 4, kSyrkThreads = 512;
+        constexpr int kSyrkStageDoubles = 2 * kSyrkBM * kSyrkP;
+        constexpr size_t kSyrkSmem = (size_t)kSyrkStages * kSyrkStageDoubles * sizeof(double);
+
+        __device__ __forceinline__ void cpAsync16(double *dst, const double *src, int bytes)
+        {
+            const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(d), "l"(src), "r"(bytes) : "memory");
+        }
+        __device__ __forceinline__ void cpAsyncCommit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+        template <int N>
+        __device__ __forceinline__ void cpAsyncWait()
+        {
+            asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+        }
+        __device__ __forceinline__ void dmmaF64(double &d0, double &d1, double a, double b)
+        {
+            asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+                         : "+d"(d0), "+d"(d1)
+                         : "d"(a), "d"(b));
+        }
+
+        __global__ void __launch_bounds__(kSyrkThreads, 1)
+            syrkUpperKernel(const double *__restrict__ Z, long long n, long long k, long long ldz, long long kslice,
+                            int tiles_per_side, double sign, double *__restrict__ K)
+        {
+            extern __shared__ __align__(16) double sm[];
+            // tile (bi, bj), bj >= bi, numbered row by row
+            int t = (int)blockIdx.x, bi = 0;
+            while (t >= tiles_per_side - bi)
+            {
+                t -= tiles_per_side - bi;
+                bi++;
+            }
+            const int bj = bi + t;
+            const long long r0 = (long long)bi * kSyrkBM, c0 = (long long)bj * kSyrkBM;
+            const long long kb = (long long)blockIdx.y * kslice;
+            const long long ke = kb + kslice < k ? kb + kslice : k;
+            if (kb >= ke)
+                return;
+            const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, r8 = lane >> 2, k4 = lane & 3;
+            const int wm = warp >> 2, wn = warp & 3;
+            const long long nsteps = (ke - kb + kSyrkKB - 1) / kSyrkKB;
+
+            // one step: 2 panels x 128 rows x 16 doubles = 2048 chunks of 16 bytes, 4 per thread;
+            // rows past n and columns past the slice are zero-filled
+            auto load = [&](long long step, int buf) {
+                double *base = sm + (size_t)buf * kSyrkStageDoubles;
+                const long long k0 = kb + step * kSyrkKB;
+#pragma unroll
+                for (int i = 0; i < 4; i++)
+                {
+                    const int ch = tid + i * kSyrkThreads;
+                    const int which = ch >> 10, row = (ch >> 3) & (kSyrkBM - 1), col = (ch & 7) * 2;
+                    const long long grow = (which ? c0 : r0) + row, gcol = k0 + col;
+                    int bytes = 0;
+                    if (grow < n && gcol < ke)
+                        bytes = gcol + 1 < ke ? 16 : 8;
+                    const double *src = bytes ? Z + grow * ldz + gcol : Z;
+                    cpAsync16(base + which * kSyrkBM * kSyrkP + row * kSyrkP + col, src, bytes);
+                }
+            };
+
+            double acc[4][4][2];
+#pragma unroll
+            for (int i = 0; i < 4; i++)
+#pragma unroll
+                for (int j = 0; j < 4; j++)
+                    acc[i][j][0] = acc[i][j][1] = 0.0;
+#pragma unroll
+            for (int s = 0; s < kSyrkStages - 1; s++)
+            {
+                if (s < nsteps)
+                    load(s, s);
+                cpAsyncCommit();
+            }
+            for (long long step = 0; step < nsteps; step++)
+            {
+                // step's copies have landed, and every warp is done with the buffer refilled next
+                cpAsyncWait<kSyrkStages - 2>();
+                __syncthreads();
+                const long long nx = step + kSyrkStages - 1;
+                if (nx < nsteps)
+                    load(nx, (int)(nx % kSyrkStages));
+                cpAsyncCommit();
+                const double *As = sm + (size_t)(step % kSyrkStages) * kSyrkStageDoubles;
+                const double *Bs = As + kSyrkBM * kSyrkP;
+#pragma unroll
+                for (int kk = 0; kk < kSyrkKB; kk += 4)
+                {
+                    double af[4], bf[4];
+#pragma unroll
+                    for (int i = 0; i < 4; i++)
+                    {
+                        af[i] = As[(wm * 32 + i * 8 + r8) * kSyrkP + kk + k4];
+                        bf[i] = Bs[(wn * 32 + i * 8 + r8) * kSyrkP + kk + k4];
+                    }
+#pragma unroll
+                    for (int i = 0; i < 4; i++)
+#pragma unroll
+                        for (int j = 0; j < 4; j++)
+                            dmmaF64(acc[i][j][0], acc[i][j][1], af[i], bf[j]);
+                }
+            }
+            cpAsyncWait<0>();
+#pragma unroll
+            for (int i = 0; i < 4; i++)
+#pragma unroll
+                for (int j = 0; j < 4; j++)
+#pragma unroll
+                    for (int h = 0; h < 2; h++)
+                    {
+                        const long long r = r0 + wm * 32 + i * 8 + r8;
+                        const long long c = c0 + wn * 32 + j * 8 + 2 * k4 + h;
+                        if (r < n && c < n && c >= r)
+                            atomicAdd(K + r * n + c, sign * acc[i][j][h]);
+                    }
+        }
+    }
+
+    void syrkUpper(const double *Z, long long n, long long k, long long ldz, double sign, double *K, cudaStream_t s)
+    {
+        if (n <= 0 || k <= 0)
+            return;
+        if ((ldz & 1) || (reinterpret_cast<uintptr_t>(Z) & 15))
+            throw EngineError(kStatusInternal, "syrkUpper: operand rows must start on 16 bytes");
+        cudaCheck(cudaFuncSetAttribute(syrkUpperKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSyrkSmem),
+                  "syrk attribute");
+        int dev = 0, sms = 148;
+        cudaCheck(cudaGetDevice(&dev), "device");
+        cudaCheck(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "sm count");
+        const long long T = (n + kSyrkBM - 1) / kSyrkBM;
+        const long long tiles = T * (T + 1) / 2;
+        // one block per SM: split k so that tiles x slices fills the SMs once
+        long long slices = std::max<long long>(1, sms / tiles);
+        long long kslice = (k + slices - 1) / slices;
+        kslice = (kslice + kSyrkKB - 1) / kSyrkKB * kSyrkKB;
+        slices = (k + kslice - 1) / kslice;
+        if (tiles > INT32_MAX || slices > 65535)
+            throw EngineError(kStatusUnsupported, "syrkUpper: problem too large for one launch");
+        syrkUpperKernel<<<dim3((unsigned)tiles, (unsigned)slices), kSyrkThreads, kSyrkSmem, s>>>(Z, n, k, ldz, kslice,
+                                                                                               (int)T, sign, K);
+        cudaCheck(cudaGetLastError(), "syrk");
     }
 
     void mirrorUpper(double *K_dev, long long n, cudaStream_t s)
@@ -363,9 +515,13 @@ namespace lible_b200
             const long long rows = std::min(rb, na - r0);
             relayoutKernel<<<gridFor(n * rows * occ), 256, 0, s>>>(Z.p, n, occ, r0, rows, T.p);
             cudaCheck(cudaGetLastError(), "relayout");
-            blasCheck(cublasDsyrk(bh.h, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_T, (int)n, (int)(rows * occ), &sign, T.p,
-                                  (int)(rows * occ), &one, K_dev, (int)n),
-                      "dsyrk");
+            // the DMMA SYRK on even row lengths (rows start on 16 bytes), else cuBLAS
+            if ((rows * occ) % 2 == 0)
+                syrkUpper(T.p, n, rows * occ, rows * occ, sign, K_dev, s);
+            else
+                blasCheck(cublasDsyrk(bh.h, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_T, (int)n, (int)(rows * occ), &sign,
+                                      T.p, (int)(rows * occ), &one, K_dev, (int)n),
+                          "dsyrk");
         }
         cudaCheck(cudaEventRecord(ev_syrk.b, s), "event");
         cudaCheck(cudaEventSynchronize(ev_syrk.b), "ri exchange");
@@ -441,19 +597,21 @@ namespace lible_b200
         // Z[m][R][i] = sum_n B[R][m][n] C[n][i], written straight in the layout of the final product:
         // per R one GEMM, in column-major terms Z_R,cm (occ x n, ld = naux*occ) = C_cm (occ x n) B_R,cm
         // (B_R symmetric in (m, n)); all R as one strided batch
-        DevBuf<double> Z((size_t)(n * k));
+        // rows of Z padded to an even length, so each starts on 16 bytes for the SYRK's copies
+        const long long ldz = k + (k & 1);
+        if (ldz > INT32_MAX)
+            throw EngineError(kStatusUnsupported, "RI-K: naux * occ exceeds the 32-bit cuBLAS dimension range");
+        DevBuf<double> Z((size_t)(n * ldz));
         EventPair ev_gemm, ev_syrk;
         const double one = 1.0, zero = 0.0;
         cudaCheck(cudaEventRecord(ev_gemm.a, s), "event");
         blasCheck(cublasDgemmStridedBatched(bh.h, CUBLAS_OP_N, CUBLAS_OP_N, (int)occ, (int)n, (int)n, &one, C_dev,
-                                            (int)occ, 0, ft.B.p, (int)n, n * n, &zero, Z.p, (int)k, occ, (int)na),
+                                            (int)occ, 0, ft.B.p, (int)n, n * n, &zero, Z.p, (int)ldz, occ, (int)na),
                   "dgemm batched");
         cudaCheck(cudaEventRecord(ev_gemm.b, s), "event");
-        // K += sign Z Z^T over (R, i): column-major Z_cm is (k x n), K_cm += sign Z_cm^T Z_cm
+        // K += sign Z Z^T over (R, i), the upper triangle by the DMMA kernel
         cudaCheck(cudaEventRecord(ev_syrk.a, s), "event");
-        blasCheck(cublasDsyrk(bh.h, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_T, (int)n, (int)k, &sign, Z.p, (int)k, &one,
-                              K_dev, (int)n),
-                  "dsyrk");
+        syrkUpper(Z.p, n, k, ldz, sign, K_dev, s);
         cudaCheck(cudaEventRecord(ev_syrk.b, s), "event");
         cudaCheck(cudaEventSynchronize(ev_syrk.b), "ri exchange");
         if (stats)
