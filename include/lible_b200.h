@@ -299,6 +299,27 @@ int lible_gpu_one_electron(lible_gpu_ctx *ctx, const double *charges, int n_char
  * 508-789).  charges as above (NULL = the nuclei); out: n consecutive blocks, host or device. */
 int lible_gpu_one_electron_batch(lible_gpu_ctx *ctx, int use_symm, int class_ab, int op, long long n,
                                  const unsigned *pairs, const double *charges, int n_charges, double *out);
+/* The same with the remaining per-pair kernels: op 6 dipoleMomentKernel, 7 momentumKernel, 8
+ * angularMomentumKernel ([3][S_a][S_b] = x, y, z; `origin` [3] for 6 and 8, bohr) and op 9
+ * externalChargesErfKernel ([S_a][S_b]; `omegas` one range parameter per charge, NULL charges = the
+ * nuclei with one omega per atom) (ints.hpp:71-75, 123-148; oneelints.cpp:379-473, 587-680,
+ * 1513-1577, 1617-1701).  Unused pointers may be NULL. */
+int lible_gpu_one_electron_batch_ex(lible_gpu_ctx *ctx, int use_symm, int class_ab, int op, long long n,
+                                    const unsigned *pairs, const double *charges, const double *omegas, int n_charges,
+                                    const double *origin, double *out);
+/* Whole-matrix forms, out [3][nao][nao] (x, y, z) or [nao][nao], host or device:
+ *   dipoleMoment (ints.hpp:123-125): <m| r - origin |n>, symmetric;
+ *   momentum (ints.hpp:139): -<m| d/dr |n>, antisymmetric, every element filled (the reference's
+ *     driver, oneelints.cpp:1477-1511, writes only the (a, b) blocks of its unique pairs, negated);
+ *   angularMomentum (ints.hpp:146-147): -<m| (r - origin) x d/dr |n>, antisymmetric;
+ *   nuclearAttractionErf (ints.hpp:52): the nuclei's erf(w r)/r attraction, `omegas` one per atom;
+ *   externalChargesErf (ints.hpp:60-62): the same for point charges [n][4], one omega each. */
+int lible_gpu_dipole_moment(lible_gpu_ctx *ctx, const double *origin, double *out);
+int lible_gpu_momentum(lible_gpu_ctx *ctx, double *out);
+int lible_gpu_angular_momentum(lible_gpu_ctx *ctx, const double *origin, double *out);
+int lible_gpu_nuclear_attraction_erf(lible_gpu_ctx *ctx, const double *omegas, double *out);
+int lible_gpu_external_charges_erf(lible_gpu_ctx *ctx, const double *charges, const double *omegas, int n_charges,
+                                   double *out);
 /* Nuclear gradient of the one-electron energy terms, grad[atom][xyz] = d/dR (sum D (T + V) -
  * sum W S), V the nuclear attraction (orbital and operator parts).  D and W symmetric nao x nao,
  * either may be NULL (the term is skipped). */

@@ -15,6 +15,8 @@
  *   eri4, eri4Diagonal, eri3, eri2, eri2Diagonal            src/lible/ints/ints.hpp:165-179
  *   ERI4Kernel, ERI3Kernel, ERI2Kernel, ERI4D1Kernel,
  *   ERI3D1Kernel, ERI2D1Kernel (operator())                 src/lible/ints/twoel/eri_kernels.hpp:60-169
+ *   overlap, kineticEnergy, nuclearAttraction, nuclearAttractionErf, externalCharges,
+ *   externalChargesErf, dipoleMoment, momentum, angularMomentum  src/lible/ints/ints.hpp:29-151
  * Failures throw std::runtime_error with the library's message, as the reference throws
  * std::runtime_error for its own error cases.  jk(), jkEnergy() and jkEnergyGradient() have no
  * reference counterpart.
@@ -28,6 +30,7 @@
 
 #include "lible_b200.h"
 
+#include <algorithm>
 #include <array>
 #include <cstddef>
 #include <stdexcept>
@@ -206,6 +209,144 @@ namespace lible::ints::gpu
     {
         Context c(structure, device);
         return eri2Diagonal(c);
+    }
+
+    // ---- one-electron drivers (ints.hpp:29-151) ---------------------------------------------------
+    // Point charges are {x, y, z, q} with coordinates in bohr, as the reference's.
+
+    namespace detail
+    {
+        inline std::vector<double> flatCharges(const std::vector<std::array<double, 4>> &q)
+        {
+            std::vector<double> f;
+            f.reserve(4 * q.size());
+            for (const auto &c : q)
+                f.insert(f.end(), c.begin(), c.end());
+            return f;
+        }
+        inline std::array<vec2d, 3> three(Context &c, const std::vector<double> &flat)
+        {
+            const std::size_t n = c.dimAO();
+            std::array<vec2d, 3> out{vec2d(n, n), vec2d(n, n), vec2d(n, n)};
+            for (int d = 0; d < 3; d++)
+                std::copy(flat.begin() + (std::ptrdiff_t)(d * n * n), flat.begin() + (std::ptrdiff_t)((d + 1) * n * n),
+                          out[d].memptr());
+            return out;
+        }
+    }
+
+    inline vec2d overlap(Context &c)
+    {
+        vec2d out(c.dimAO(), c.dimAO());
+        c.check(lible_gpu_overlap(c.get(), out.memptr()));
+        return out;
+    }
+    inline vec2d overlap(const Structure &structure, int device = 0)
+    {
+        Context c(structure, device);
+        return overlap(c);
+    }
+    inline vec2d kineticEnergy(Context &c)
+    {
+        vec2d out(c.dimAO(), c.dimAO());
+        c.check(lible_gpu_kinetic_energy(c.get(), out.memptr()));
+        return out;
+    }
+    inline vec2d kineticEnergy(const Structure &structure, int device = 0)
+    {
+        Context c(structure, device);
+        return kineticEnergy(c);
+    }
+    inline vec2d nuclearAttraction(Context &c)
+    {
+        vec2d out(c.dimAO(), c.dimAO());
+        c.check(lible_gpu_nuclear_attraction(c.get(), out.memptr()));
+        return out;
+    }
+    inline vec2d nuclearAttraction(const Structure &structure, int device = 0)
+    {
+        Context c(structure, device);
+        return nuclearAttraction(c);
+    }
+    inline vec2d nuclearAttractionErf(Context &c, const std::vector<double> &omegas)
+    {
+        if (omegas.size() != (std::size_t)c.nAtoms())
+            throw std::runtime_error("nuclearAttractionErf(): number of omega values must match number of atoms");
+        vec2d out(c.dimAO(), c.dimAO());
+        c.check(lible_gpu_nuclear_attraction_erf(c.get(), omegas.data(), out.memptr()));
+        return out;
+    }
+    inline vec2d nuclearAttractionErf(const Structure &structure, const std::vector<double> &omegas, int device = 0)
+    {
+        Context c(structure, device);
+        return nuclearAttractionErf(c, omegas);
+    }
+    inline vec2d externalCharges(const std::vector<std::array<double, 4>> &point_charges, Context &c)
+    {
+        const std::vector<double> q = detail::flatCharges(point_charges);
+        vec2d out(c.dimAO(), c.dimAO());
+        c.check(lible_gpu_external_charges(c.get(), q.data(), (int)point_charges.size(), out.memptr()));
+        return out;
+    }
+    inline vec2d externalCharges(const std::vector<std::array<double, 4>> &point_charges, const Structure &structure,
+                                 int device = 0)
+    {
+        Context c(structure, device);
+        return externalCharges(point_charges, c);
+    }
+    inline vec2d externalChargesErf(const std::vector<std::array<double, 4>> &point_charges,
+                                    const std::vector<double> &omegas, Context &c)
+    {
+        if (omegas.size() != point_charges.size())
+            throw std::runtime_error("externalChargesErf(): number of omega values must match number of charges");
+        const std::vector<double> q = detail::flatCharges(point_charges);
+        vec2d out(c.dimAO(), c.dimAO());
+        c.check(lible_gpu_external_charges_erf(c.get(), q.data(), omegas.data(), (int)point_charges.size(),
+                                               out.memptr()));
+        return out;
+    }
+    inline vec2d externalChargesErf(const std::vector<std::array<double, 4>> &point_charges,
+                                    const std::vector<double> &omegas, const Structure &structure, int device = 0)
+    {
+        Context c(structure, device);
+        return externalChargesErf(point_charges, omegas, c);
+    }
+    inline std::array<vec2d, 3> dipoleMoment(const std::array<double, 3> &origin, Context &c)
+    {
+        std::vector<double> flat(3 * c.dimAO() * c.dimAO());
+        c.check(lible_gpu_dipole_moment(c.get(), origin.data(), flat.data()));
+        return detail::three(c, flat);
+    }
+    inline std::array<vec2d, 3> dipoleMoment(const std::array<double, 3> &origin, const Structure &structure,
+                                             int device = 0)
+    {
+        Context c(structure, device);
+        return dipoleMoment(origin, c);
+    }
+    // The full antisymmetric matrices of -<m| d/dr |n> (the reference's driver writes only one
+    // orientation of each pair of different shells, negated).
+    inline std::array<vec2d, 3> momentum(Context &c)
+    {
+        std::vector<double> flat(3 * c.dimAO() * c.dimAO());
+        c.check(lible_gpu_momentum(c.get(), flat.data()));
+        return detail::three(c, flat);
+    }
+    inline std::array<vec2d, 3> momentum(const Structure &structure, int device = 0)
+    {
+        Context c(structure, device);
+        return momentum(c);
+    }
+    inline std::array<vec2d, 3> angularMomentum(const std::array<double, 3> &origin, Context &c)
+    {
+        std::vector<double> flat(3 * c.dimAO() * c.dimAO());
+        c.check(lible_gpu_angular_momentum(c.get(), origin.data(), flat.data()));
+        return detail::three(c, flat);
+    }
+    inline std::array<vec2d, 3> angularMomentum(const std::array<double, 3> &origin, const Structure &structure,
+                                                int device = 0)
+    {
+        Context c(structure, device);
+        return angularMomentum(origin, c);
     }
 
     // ---- kernel functors (eri_kernels.hpp:60-169) -------------------------------------------------

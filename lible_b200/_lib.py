@@ -95,6 +95,12 @@ SIGNATURES = {
     "lible_gpu_external_charges": [P, P, I, P],
     "lible_gpu_one_electron": [P, P, I, P, P, P],
     "lible_gpu_one_electron_batch": [P, I, I, I, LL, P, P, I, P],
+    "lible_gpu_one_electron_batch_ex": [P, I, I, I, LL, P, P, P, I, P, P],
+    "lible_gpu_dipole_moment": [P, P, P],
+    "lible_gpu_momentum": [P, P],
+    "lible_gpu_angular_momentum": [P, P, P],
+    "lible_gpu_nuclear_attraction_erf": [P, P, P],
+    "lible_gpu_external_charges_erf": [P, P, P, I, P],
     "lible_gpu_one_electron_grad": [P, P, P, P],
     "lible_host_spherical_trafo": [I, P, P, P, P],
     "lible_host_shell_norms": [I, I, P, P, P],

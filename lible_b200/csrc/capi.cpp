@@ -1045,20 +1045,79 @@ int lible_gpu_one_electron(lible_gpu_ctx *ctx, const double *charges, int n_char
     });
 }
 
-int lible_gpu_one_electron_batch(lible_gpu_ctx *ctx, int use_symm, int class_ab, int op, long long n,
-                                 const unsigned *pairs, const double *charges, int n_charges, double *out)
+int lible_gpu_one_electron_batch_ex(lible_gpu_ctx *ctx, int use_symm, int class_ab, int op, long long n,
+                                    const unsigned *pairs, const double *charges, const double *omegas, int n_charges,
+                                    const double *origin, double *out)
 {
     return guard(ctx, [&](Engine &e) {
         if (n < 0 || (n > 0 && (!pairs || !out)) || (charges && n_charges < 0))
             throw EngineError(kStatusInvalid, "bad one-electron batch arguments");
+        if (op < 0 || op > 9)
+            throw EngineError(kStatusInvalid, "bad one-electron operator");
         const auto cls = e.pairClasses(use_symm != 0);
         if (class_ab < 0 || class_ab >= (int)cls.size())
             throw EngineError(kStatusInvalid, "bad class index");
-        const size_t blk = (size_t)(2 * cls[class_ab].la + 1) * (2 * cls[class_ab].lb + 1) * (op >= 3 ? 6 : 1);
+        const int nblk = (op >= 3 && op <= 5) ? 6 : (op >= 6 && op <= 8) ? 3 : 1;
+        const size_t blk = (size_t)(2 * cls[class_ab].la + 1) * (2 * cls[class_ab].lb + 1) * nblk;
         DevArray o(out, (size_t)n * blk, false, e.stream());
-        e.oneElectronBatch(use_symm != 0, class_ab, op, n, pairs, charges, charges ? n_charges : 0, o.ptr);
+        e.oneElectronBatch(use_symm != 0, class_ab, op, n, pairs, charges, charges ? n_charges : 0, o.ptr, omegas,
+                           origin);
         o.copyOut();
     });
+}
+
+int lible_gpu_one_electron_batch(lible_gpu_ctx *ctx, int use_symm, int class_ab, int op, long long n,
+                                 const unsigned *pairs, const double *charges, int n_charges, double *out)
+{
+    if (op > 5)
+        return fail(ctx, LIBLE_GPU_EINVAL, "ops 6..9 take lible_gpu_one_electron_batch_ex");
+    return lible_gpu_one_electron_batch_ex(ctx, use_symm, class_ab, op, n, pairs, charges, nullptr, n_charges,
+                                           nullptr, out);
+}
+
+namespace
+{
+    int oneElectronOperator(lible_gpu_ctx *ctx, int op, const double *charges, const double *omegas, int n_charges,
+                            const double *origin, double *out)
+    {
+        return guard(ctx, [&](Engine &e) {
+            if (!out || (charges && n_charges < 0))
+                throw EngineError(kStatusInvalid, "bad one-electron operator arguments");
+            const size_t n = e.nao();
+            const int nblk = op == 9 ? 1 : 3;
+            DevArray o(out, (size_t)nblk * n * n, false, e.stream());
+            e.oneElectronOperator(op, charges, charges ? n_charges : 0, omegas, origin, o.ptr);
+            o.copyOut();
+        });
+    }
+}
+
+int lible_gpu_dipole_moment(lible_gpu_ctx *ctx, const double *origin, double *out)
+{
+    return oneElectronOperator(ctx, 6, nullptr, nullptr, 0, origin, out);
+}
+
+int lible_gpu_momentum(lible_gpu_ctx *ctx, double *out)
+{
+    return oneElectronOperator(ctx, 7, nullptr, nullptr, 0, nullptr, out);
+}
+
+int lible_gpu_angular_momentum(lible_gpu_ctx *ctx, const double *origin, double *out)
+{
+    return oneElectronOperator(ctx, 8, nullptr, nullptr, 0, origin, out);
+}
+
+int lible_gpu_nuclear_attraction_erf(lible_gpu_ctx *ctx, const double *omegas, double *out)
+{
+    return oneElectronOperator(ctx, 9, nullptr, omegas, 0, nullptr, out);
+}
+
+int lible_gpu_external_charges_erf(lible_gpu_ctx *ctx, const double *charges, const double *omegas, int n_charges,
+                                   double *out)
+{
+    if (!charges || n_charges < 0)
+        return fail(ctx, LIBLE_GPU_EINVAL, "null charges");
+    return oneElectronOperator(ctx, 9, charges, omegas, n_charges, nullptr, out);
 }
 
 int lible_gpu_one_electron_grad(lible_gpu_ctx *ctx, const double *D, const double *W, double *grad)

@@ -184,9 +184,16 @@ namespace lible_b200
                          double *V_dev);
         // Per-pair one-electron blocks of class `cls` of shellPairData(use_symm) for the listed pairs:
         // op 0..2 = S, T, V ([S_a][S_b] each), 3..5 = their first derivatives ([6][S_a][S_b]: A_xyz,
-        // B_xyz; V orbital part).  Charges as above, null = the nuclei.  out_dev: device memory.
+        // B_xyz; V orbital part), 6 = dipole, 7 = momentum, 8 = angular momentum ([3][S_a][S_b],
+        // x, y, z; `origin` for 6 and 8), 9 = erf-attenuated V (`omegas`, one per charge).  Charges as
+        // above, null = the nuclei.  out_dev: device memory.
         void oneElectronBatch(bool use_symm, int cls, int op, long long n_tasks, const uint32_t *pairs_host,
-                              const double *charges_host, int n_charges, double *out_dev);
+                              const double *charges_host, int n_charges, double *out_dev,
+                              const double *omegas_host = nullptr, const double *origin = nullptr);
+        // Whole-matrix form of ops 6..9 over every shell pair: out_dev [blocks][nao][nao], the lower
+        // triangle mirrored (negated for the antisymmetric momentum and angular momentum).
+        void oneElectronOperator(int op, const double *charges_host, int n_charges, const double *omegas_host,
+                                 const double *origin, double *out_dev);
         // grad[atom][xyz] = d/dR ( sum_mn D_mn (T + V)_mn - sum_mn W_mn S_mn ), the nuclei as the
         // charges of V (orbital and operator parts); D, W symmetric device matrices, either may be null.
         void oneElectronGrad(const double *D_dev, const double *W_dev, double *grad_dev);

@@ -18,6 +18,7 @@
 #include "engine_api.hpp"
 #include "ri_solve.hpp"
 
+#include <algorithm>
 #include <vector>
 
 namespace lible_b200
@@ -228,6 +229,15 @@ namespace lible_b200
         // V, the charge-summed Hermite integrals of one order higher:
         //   d/dA = -((a/p) dP + dR),  d/dB = -((b/p) dP - dR),
         //   dP_x = f sum E_t E_u E_v R_{t+1,u,v},  dR_x = f sum E1_t E_u E_v R_{tuv}.
+        // Multipole-type operators of one pair, three blocks each (x, y, z), with O the caller's origin
+        // (src/lible/ints/oneelints.cpp: dipoleMomentKernel :379-473, momentumKernel :1513-1577,
+        // angularMomentumKernel :1617-1701), from the same Hermite tables:
+        //   dipole:   fs (E^x_{ii'1} + PO_x E^x_{ii'0}) E^y E^z             (and y, z)
+        //   momentum: -fs D^x E^y E^z,  D^x = -2b E^x_{i,i'+1,0} + i' E^x_{i,i'-1,0}
+        //   angular:  -fs E^x (S^y D^z - S^z D^y),  S^y = E^y_{jj'1} + PO_y E^y_{jj'0}   (cyclic)
+        // and the erf-attenuated Coulomb attraction of point charges with a range parameter w_C each
+        // (externalChargesErfKernel :587-680): the charge's R_tuv taken with the exponent
+        // p w^2 / (p + w^2) and scaled by q_C w / sqrt(w^2 + p).
         enum OneOp : int
         {
             kOpS = 0,
@@ -236,7 +246,15 @@ namespace lible_b200
             kOpSD1 = 3,
             kOpTD1 = 4,
             kOpVD1 = 5,
+            kOpDipole = 6,
+            kOpMomentum = 7,
+            kOpAngular = 8,
+            kOpVErf = 9,
         };
+        __host__ __device__ constexpr int oneOpBlocks(int op)
+        {
+            return (op >= kOpSD1 && op <= kOpVD1) ? 6 : (op >= kOpDipole && op <= kOpAngular) ? 3 : 1;
+        }
 
         struct OnePairArgs
         {
@@ -252,7 +270,9 @@ namespace lible_b200
             const int32_t *atoms;    // [n_pairs][2] (gradient mode)
             const int32_t *same;     // [n_pairs]: 1 when a and b are the same shell (gradient mode)
             const double *charges;   // [n][4]
+            const double *omegas;    // [n] range parameters (kOpVErf), else null
             int n_charges;
+            double origin[3];        // multipole origin (kOpDipole, kOpAngular)
             const double *boys;
             const int *sph_rc;
             const double *sph_val;
@@ -298,8 +318,8 @@ namespace lible_b200
             auto ex = [&](int axis, int i, int j, int t) { return E[axis * S::EAX + (i * NB + j) * NT + t]; };
             auto ex1 = [&](int axis, int i, int j, int t) { return E1[axis * S::EAX + (i * NB + j) * NT + t]; };
             const int op = GRAD ? -1 : a.op;
-            const bool wantV = GRAD ? a.D != nullptr : (op == kOpV || op == kOpVD1);
-            const bool d1 = GRAD || op >= kOpSD1;
+            const bool wantV = GRAD ? a.D != nullptr : (op == kOpV || op == kOpVD1 || op == kOpVErf);
+            const bool d1 = GRAD || oneOpBlocks(op) == 6;
             const int oa = a.ao[2 * ipair], ob = a.ao[2 * ipair + 1];
             const size_t n = (size_t)a.nao;
             const double *nA = a.norms_a + (size_t)ipair * S::SA, *nB = a.norms_b + (size_t)ipair * S::SB;
@@ -372,11 +392,19 @@ namespace lible_b200
                         const double *q = a.charges + 4 * (size_t)c;
                         const double X = P[0] - q[0], Y = P[1] - q[1], Z = P[2] - q[2];
                         double F[L1 + 1], R[S::NR1];
-                        boysF<L1, false>(p * (X * X + Y * Y + Z * Z), a.boys + (size_t)L1 * kBoysTerms * kBoysPitch, F);
+                        // erf attenuation: exponent p w^2 / (p + w^2), scale w / sqrt(w^2 + p)
+                        double pe = p, qs = q[3];
+                        if (a.omegas)
+                        {
+                            const double w = a.omegas[c], w2 = w * w;
+                            pe = p * w2 / (p + w2);
+                            qs *= w / sqrt(w2 + p);
+                        }
+                        boysF<L1, false>(pe * (X * X + Y * Y + Z * Z), a.boys + (size_t)L1 * kBoysTerms * kBoysPitch, F);
 #pragma unroll
                         for (int k = 0; k <= L1; k++)
-                            F[k] *= q[3];
-                        hermiteR<L1, double>(-2.0 * p, F, X, Y, Z, R);
+                            F[k] *= qs;
+                        hermiteR<L1, double>(-2.0 * pe, F, X, Y, Z, R);
 #pragma unroll
                         for (int h = 0; h < S::NR1; h++)
                             r[h] += R[h];
@@ -442,8 +470,38 @@ namespace lible_b200
                         else if (op == kOpT)
                             acc[0][w] += fs * (kin(0, 0) * s0[1] * s0[2] + s0[0] * kin(0, 1) * s0[2] +
                                                s0[0] * s0[1] * kin(0, 2));
-                        else if (op == kOpV)
+                        else if (op == kOpV || op == kOpVErf)
                             acc[0][w] -= fv * vsum(-1, -1);
+                        else if (op >= kOpDipole)
+                        {
+                            // first moments about the origin and first derivatives on b, per axis
+                            double m1[3], dd[3];
+#pragma unroll
+                            for (int x = 0; x < 3; x++)
+                            {
+                                const int i = ijk[x], i_ = ijk_[x];
+                                m1[x] = ex(x, i, i_, 1) + (P[x] - a.origin[x]) * s0[x];
+                                dd[x] = -2.0 * eb * ex(x, i, i_ + 1, 0) + (i_ > 0 ? i_ * ex(x, i, i_ - 1, 0) : 0.0);
+                            }
+                            if (op == kOpDipole)
+                            {
+                                acc[0][w] += fs * m1[0] * s0[1] * s0[2];
+                                acc[1][w] += fs * s0[0] * m1[1] * s0[2];
+                                acc[2][w] += fs * s0[0] * s0[1] * m1[2];
+                            }
+                            else if (op == kOpMomentum)
+                            {
+                                acc[0][w] -= fs * dd[0] * s0[1] * s0[2];
+                                acc[1][w] -= fs * s0[0] * dd[1] * s0[2];
+                                acc[2][w] -= fs * s0[0] * s0[1] * dd[2];
+                            }
+                            else
+                            {
+                                acc[0][w] -= fs * s0[0] * (m1[1] * dd[2] - m1[2] * dd[1]);
+                                acc[1][w] -= fs * s0[1] * (m1[2] * dd[0] - m1[0] * dd[2]);
+                                acc[2][w] -= fs * s0[2] * (m1[0] * dd[1] - m1[1] * dd[0]);
+                            }
+                        }
                         else
                         {
 #pragma unroll
@@ -575,8 +633,11 @@ namespace lible_b200
             }
             else
             {
-                // spherical transform and norms of each stored block
-                const int nblk = d1 ? 6 : 1;
+                // spherical transform and norms of each stored block; a swapped class is written in the
+                // caller's orientation: blocks transposed, d/dA and d/dB exchanged, and the
+                // antisymmetric operators (momentum, angular momentum) negated
+                const int nblk = oneOpBlocks(op);
+                const double sgn = (a.swap && (op == kOpMomentum || op == kOpAngular)) ? -1.0 : 1.0;
                 for (int d = 0; d < nblk; d++)
 #pragma unroll
                     for (int w = 0; w < S::PER_LANE; w++)
@@ -601,7 +662,7 @@ namespace lible_b200
                             if (a.sph_rc[2 * tb] == nn)
                                 sum += a.sph_val[ta] * a.sph_val[tb] * blk[d * S::NC + ca * S::NCB + a.sph_rc[2 * tb + 1]];
                     }
-                    out[dst] = nA[m] * nB[nn] * sum;
+                    out[dst] = sgn * nA[m] * nB[nn] * sum;
                 }
             }
         }
@@ -711,15 +772,148 @@ namespace lible_b200
         return q;
     }
 
+    namespace
+    {
+        // M[d][a][b] = blk, M[d][b][a] = sign * blk for every stored pair block [pair][d][S_a][S_b].
+        __global__ void scatterPairBlocks(const double *__restrict__ blocks, long long n_pairs, int nblk, int sa,
+                                          int sb, const int32_t *__restrict__ ao, long long nao, double sign,
+                                          double *__restrict__ M)
+        {
+            const long long per = (long long)nblk * sa * sb, total = n_pairs * per;
+            for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; g < total;
+                 g += (long long)gridDim.x * blockDim.x)
+            {
+                const long long ip = g / per;
+                const int o = (int)(g % per), d = o / (sa * sb), m = (o / sb) % sa, nn = o % sb;
+                const long long r = ao[2 * ip] + m, c = ao[2 * ip + 1] + nn;
+                const double v = blocks[g];
+                M[((size_t)d * nao + r) * nao + c] = v;
+                M[((size_t)d * nao + c) * nao + r] = sign * v;
+            }
+        }
+
+        // M[d] = (M[d] + sign M[d]^T) / 2, so the matrices are exactly symmetric (sign 1) or
+        // antisymmetric with a zero diagonal (sign -1): the diagonal shell blocks are written from both
+        // orientations of their element pairs, which agree only to rounding.
+        __global__ void symmetrizeBlocks(double *M, long long nao, int nblk, double sign)
+        {
+            const long long total = (long long)nblk * nao * nao;
+            for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; g < total;
+                 g += (long long)gridDim.x * blockDim.x)
+            {
+                const long long d = g / (nao * nao), r = (g / nao) % nao, c = g % nao;
+                if (c < r)
+                    continue;
+                double *a = M + (d * nao + r) * nao + c, *b = M + (d * nao + c) * nao + r;
+                if (c == r)
+                {
+                    if (sign < 0)
+                        *a = 0.0;
+                    continue;
+                }
+                const double m = 0.5 * (*a + sign * *b);
+                *a = m;
+                *b = sign * m;
+            }
+        }
+
+        void checkOneOp(int op, const double *omegas_host, const double *origin)
+        {
+            if (op < 0 || op > kOpVErf)
+                throw EngineError(kStatusInvalid, "bad one-electron operator");
+            if (op == kOpVErf && !omegas_host)
+                throw EngineError(kStatusInvalid, "the erf-attenuated operator needs one omega per charge");
+            if ((op == kOpDipole || op == kOpAngular) && !origin)
+                throw EngineError(kStatusInvalid, "the operator needs an origin");
+        }
+    }
+
+    void Engine::oneElectronOperator(int op, const double *charges_host, int n_charges, const double *omegas_host,
+                                     const double *origin, double *out_dev)
+    {
+        requireSingle();
+        if (op < kOpDipole)
+            throw EngineError(kStatusInvalid, "the whole-matrix operator form covers ops 6..9");
+        checkOneOp(op, omegas_host, origin);
+        if (max_l_ > 3)
+            throw EngineError(kStatusUnsupported, "one-electron kernels are instantiated for l <= 3");
+        const std::vector<double> q = charges_host
+                                          ? std::vector<double>(charges_host, charges_host + 4 * (size_t)n_charges)
+                                          : nucleiCharges();
+        const int nq = (int)(q.size() / 4);
+        DevBuf<double> dq, dw;
+        upload(dq, q, stream_);
+        if (op == kOpVErf)
+            upload(dw, std::vector<double>(omegas_host, omegas_host + nq), stream_);
+        const int nblk = oneOpBlocks(op);
+        const size_t n = nao_;
+        cudaCheck(cudaMemsetAsync(out_dev, 0, (size_t)nblk * n * n * sizeof(double), stream_), "memset");
+        const double sign = (op == kOpMomentum || op == kOpAngular) ? -1.0 : 1.0;
+        ClassSet &cs = mainSet(true);
+        for (size_t c = 0; c < cs.host.size(); c++)
+        {
+            const PairClass &pc = cs.host[c];
+            if (pc.n_pairs == 0)
+                continue;
+            const PairFn fn = lookupPair(pc.la, pc.lb);
+            if (!fn)
+                throw EngineError(kStatusUnsupported, "one-electron kernels are instantiated for l <= 3");
+            OneClassData d(pc, stream_);
+            const int sa = 2 * pc.la + 1, sb = 2 * pc.lb + 1;
+            DevBuf<double> blocks((size_t)pc.n_pairs * nblk * sa * sb);
+            OnePairArgs a{};
+            a.op = op;
+            a.swap = 0;  // blocks in the stored orientation, scattered both ways below
+            a.n_tasks = (long long)pc.n_pairs;
+            a.list = nullptr;
+            a.n_pairs = (int)pc.n_pairs;
+            a.nao = (int)n;
+            a.exps = d.ex.p;
+            a.coeffs = d.co.p;
+            a.coords = d.xy.p;
+            a.norms_a = d.na.p;
+            a.norms_b = d.nb.p;
+            a.pofs = d.po.p;
+            a.ao = d.ao.p;
+            a.atoms = d.atoms.p;
+            a.same = d.same.p;
+            a.charges = dq.p;
+            a.omegas = op == kOpVErf ? dw.p : nullptr;
+            a.n_charges = nq;
+            if (origin)
+                for (int x = 0; x < 3; x++)
+                    a.origin[x] = origin[x];
+            a.boys = boys_;
+            a.sph_rc = sph_rc_;
+            a.sph_val = sph_val_;
+            a.sph_ofs_a0 = sph_ofs_[pc.la];
+            a.sph_ofs_a1 = sph_ofs_[pc.la + 1];
+            a.sph_ofs_b0 = sph_ofs_[pc.lb];
+            a.sph_ofs_b1 = sph_ofs_[pc.lb + 1];
+            a.out = blocks.p;
+            fn(a, stream_, false);
+            const long long total = (long long)pc.n_pairs * nblk * sa * sb;
+            scatterPairBlocks<<<(unsigned)std::min<long long>((total + 255) / 256, 148LL * 16), 256, 0, stream_>>>(
+                blocks.p, (long long)pc.n_pairs, nblk, sa, sb, d.ao.p, (long long)n, sign, out_dev);
+            cudaCheck(cudaGetLastError(), "scatter");
+            cudaCheck(cudaStreamSynchronize(stream_), "one-electron operator");
+        }
+        const long long total = (long long)nblk * (long long)n * (long long)n;
+        symmetrizeBlocks<<<(unsigned)std::min<long long>((total + 255) / 256, 148LL * 16), 256, 0, stream_>>>(
+            out_dev, (long long)n, nblk, sign);
+        cudaCheck(cudaGetLastError(), "symmetrize");
+        cudaCheck(cudaStreamSynchronize(stream_), "one-electron operator");
+    }
+
     void Engine::oneElectronBatch(bool use_symm, int cls, int op, long long n_tasks, const uint32_t *pairs_host,
-                                  const double *charges_host, int n_charges, double *out_dev)
+                                  const double *charges_host, int n_charges, double *out_dev,
+                                  const double *omegas_host, const double *origin)
     {
         requireSingle();
         ClassSet &cs = mainSet(use_symm);
         if (cls < 0 || cls >= (int)cs.host.size())
             throw EngineError(kStatusInvalid, "bad class index");
-        if (op < 0 || op > 5)
-            throw EngineError(kStatusInvalid, "bad one-electron operator");
+        checkOneOp(op, omegas_host, origin);
         const PairClass &pc = cs.host[cls];
         const PairFn fn = lookupPair(pc.la, pc.lb);
         if (!fn)
@@ -734,11 +928,17 @@ namespace lible_b200
                                              : nucleiCharges();
         OneClassData d(pc, stream_);
         DevBuf<uint32_t> dl;
-        DevBuf<double> dq;
+        DevBuf<double> dq, dw;
         upload(dl, list, stream_);
         upload(dq, q, stream_);
+        if (op == kOpVErf)
+            upload(dw, std::vector<double>(omegas_host, omegas_host + q.size() / 4), stream_);
         OnePairArgs a{};
         a.op = op;
+        a.omegas = op == kOpVErf ? dw.p : nullptr;
+        if (origin)
+            for (int x = 0; x < 3; x++)
+                a.origin[x] = origin[x];
         a.swap = cs.swapped[cls] ? 1 : 0;
         a.n_tasks = n_tasks;
         a.list = dl.p;

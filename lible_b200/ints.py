@@ -520,20 +520,23 @@ def one_electron(structure, point_charges=None):
     return S, T, V
 
 
-def _one_batch(op, ipair, sp, charges=None):
-    """Per-pair one-electron blocks through lible_gpu_one_electron_batch; `ipair` an index (returns
-    the block, or the list of 6 derivative blocks) or a sequence of indices (returns an array)."""
+def _one_batch(op, ipair, sp, charges=None, omegas=None, origin=None):
+    """Per-pair one-electron blocks through lible_gpu_one_electron_batch_ex; `ipair` an index (returns
+    the block, or the list of 6 derivative / 3 Cartesian blocks) or a sequence of indices (returns an
+    array)."""
     single = np.ndim(ipair) == 0
     idx = np.ascontiguousarray(np.atleast_1d(np.asarray(ipair, dtype=np.uint32)))
-    nb = 6 if op >= 3 else 1
+    nb = 6 if 3 <= op <= 5 else 3 if 6 <= op <= 8 else 1
     out = np.empty((len(idx), nb, _nsph(sp.la_), _nsph(sp.lb_)))
     if charges is None:
         q, nq = None, 0
     else:
         q = _f64(charges).reshape(-1, 4)
         nq = len(q)
-    _call(sp.structure, "lible_gpu_one_electron_batch", int(sp.uses_symm), int(sp.index), int(op), int(len(idx)),
-          _ptr(idx), _ptr(q), nq, _ptr(out))
+    w = None if omegas is None else _f64(omegas)
+    o = None if origin is None else _f64(origin)
+    _call(sp.structure, "lible_gpu_one_electron_batch_ex", int(sp.uses_symm), int(sp.index), int(op), int(len(idx)),
+          _ptr(idx), _ptr(q), _ptr(w), nq, _ptr(o), _ptr(out))
     if nb == 1:
         out = out[:, 0]
     if single:
@@ -569,6 +572,70 @@ def kineticEnergyD1Kernel(ipair, sp_data):
 def externalChargesD1Kernel(ipair, charges, sp_data):
     """lible::ints::externalChargesD1Kernel (ints.hpp:79): the orbital part."""
     return _one_batch(5, ipair, sp_data, charges)
+
+
+def dipoleMomentKernel(ipair, origin, sp_data):
+    """lible::ints::dipoleMomentKernel (ints.hpp:127-129): [x, y, z] blocks of <a| r - origin |b>."""
+    return _one_batch(6, ipair, sp_data, origin=origin)
+
+
+def momentumKernel(ipair, sp_data):
+    """lible::ints::momentumKernel (ints.hpp:141): [x, y, z] blocks of -<a| d/dr |b>."""
+    return _one_batch(7, ipair, sp_data)
+
+
+def angularMomentumKernel(ipair, origin, sp_data):
+    """lible::ints::angularMomentumKernel (ints.hpp:149-151): [x, y, z] blocks of
+    -<a| (r - origin) x d/dr |b>."""
+    return _one_batch(8, ipair, sp_data, origin=origin)
+
+
+def externalChargesErfKernel(ipair, charges, omegas, sp_data):
+    """lible::ints::externalChargesErfKernel (ints.hpp:71-75): erf(w r)/r attraction of the charges
+    [x, y, z, q], one omega per charge; the Boys grid argument is not needed."""
+    return _one_batch(9, ipair, sp_data, charges, omegas=omegas)
+
+
+def _one_operator(structure, fn, nblk, *args):
+    n = structure.nao
+    out = np.empty((nblk, n, n) if nblk > 1 else (n, n))
+    _call(structure, fn, *args, _ptr(out))
+    return out
+
+
+def dipoleMoment(origin, structure):
+    """lible::ints::dipoleMoment (ints.hpp:123-125): [3][nao][nao], symmetric."""
+    return _one_operator(structure, "lible_gpu_dipole_moment", 3, _ptr(_f64(origin)))
+
+
+def momentum(structure):
+    """lible::ints::momentum (ints.hpp:139): [3][nao][nao] of -<m| d/dr |n>, the full antisymmetric
+    matrices (the reference's driver leaves the lower blocks of its unique pairs unwritten and negates
+    the upper ones)."""
+    return _one_operator(structure, "lible_gpu_momentum", 3)
+
+
+def angularMomentum(origin, structure):
+    """lible::ints::angularMomentum (ints.hpp:146-147): [3][nao][nao], antisymmetric."""
+    return _one_operator(structure, "lible_gpu_angular_momentum", 3, _ptr(_f64(origin)))
+
+
+def nuclearAttractionErf(structure, omegas):
+    """lible::ints::nuclearAttractionErf (ints.hpp:52): one omega per atom."""
+    w = _f64(omegas)
+    if w.size != structure.n_atoms:
+        raise ValueError("one omega per atom")
+    return _one_operator(structure, "lible_gpu_nuclear_attraction_erf", 1, _ptr(w))
+
+
+def externalChargesErf(point_charges, omegas, structure):
+    """lible::ints::externalChargesErf (ints.hpp:60-62): charges [n][4] (x, y, z bohr, q), one omega
+    per charge."""
+    q = _f64(point_charges).reshape(-1, 4)
+    w = _f64(omegas)
+    if w.size != len(q):
+        raise ValueError("one omega per charge")
+    return _one_operator(structure, "lible_gpu_external_charges_erf", 1, _ptr(q), _ptr(w), len(q))
 
 
 def one_electron_grad(structure, D=None, W=None):

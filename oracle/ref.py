@@ -55,6 +55,8 @@ def lib():
         L.ref_eri3soc_class.argtypes = [P, ctypes.c_int, ctypes.c_int, ctypes.c_int, P]
         L.ref_eri2d2_class.argtypes = [P, ctypes.c_int, ctypes.c_int, P]
         L.ref_one_electron_class.argtypes = [P, ctypes.c_int, ctypes.c_int, ctypes.c_int, P, ctypes.c_int, P]
+        L.ref_one_electron_class_ex.argtypes = [P, ctypes.c_int, ctypes.c_int, ctypes.c_int, P, P, ctypes.c_int, P, P]
+        L.ref_one_electron_ex.argtypes = [P, ctypes.c_int, P, P, ctypes.c_int, P, P]
         _lib = L
     return _lib
 
@@ -125,6 +127,17 @@ class RefStructure:
         self._chk(lib().ref_one_electron(self.h, which, _p(q), len(q), _p(out)))
         return out
 
+    def one_electron_ex(self, which, charges=None, omegas=None, origin=None):
+        """The reference's dipoleMoment / momentum / angularMomentum ([3][nao][nao], which = 4, 5, 6)
+        and nuclearAttractionErf / externalChargesErf (which = 7, 8)."""
+        out = np.empty((3, self.nao, self.nao) if which <= 6 else (self.nao, self.nao))
+        q = np.ascontiguousarray(charges if charges is not None else np.zeros((0, 4)), dtype=np.float64)
+        w = None if omegas is None else np.ascontiguousarray(omegas, dtype=np.float64)
+        o = None if origin is None else np.ascontiguousarray(origin, dtype=np.float64)
+        self._chk(lib().ref_one_electron_ex(self.h, which, _p(q), _p(w) if w is not None else None, len(q),
+                                            _p(o) if o is not None else None, _p(out)))
+        return out
+
     def eri4soc_class(self, use_symm, iab, icd):
         cls = self.pair_classes(use_symm)
         (la, lb, na, _), (lc, ld, nc, _) = cls[iab], cls[icd]
@@ -151,6 +164,20 @@ class RefStructure:
         out = np.empty((na, nb, 2 * la + 1, 2 * lb + 1))
         q = np.ascontiguousarray(charges if charges is not None else np.zeros((0, 4)), dtype=np.float64)
         self._chk(lib().ref_one_electron_class(self.h, int(use_symm), iab, op, _p(q), len(q), _p(out)))
+        return out if nb > 1 else out[:, 0]
+
+    def one_electron_class_ex(self, use_symm, iab, op, charges=None, omegas=None, origin=None):
+        """op 6 dipoleMomentKernel, 7 momentumKernel, 8 angularMomentumKernel ([n][3][Sa][Sb]),
+        9 externalChargesErfKernel ([n][Sa][Sb]) for every pair of one class."""
+        la, lb, na, _ = self.pair_classes(use_symm)[iab]
+        nb = 1 if op == 9 else 3
+        out = np.empty((na, nb, 2 * la + 1, 2 * lb + 1))
+        q = np.ascontiguousarray(charges if charges is not None else np.zeros((0, 4)), dtype=np.float64)
+        w = None if omegas is None else np.ascontiguousarray(omegas, dtype=np.float64)
+        o = None if origin is None else np.ascontiguousarray(origin, dtype=np.float64)
+        self._chk(lib().ref_one_electron_class_ex(self.h, int(use_symm), iab, op, _p(q),
+                                                  _p(w) if w is not None else None, len(q),
+                                                  _p(o) if o is not None else None, _p(out)))
         return out if nb > 1 else out[:, 0]
 
     def eri2_diagonal(self):

@@ -363,6 +363,79 @@ int ref_one_electron(void *h, int which, const double *charges, int n_charges, d
     });
 }
 
+// The reference's remaining per-pair one-electron kernels for every pair of one class:
+// op 6 dipoleMomentKernel, 7 momentumKernel, 8 angularMomentumKernel ([n_pairs][3][Sa Sb]; origin
+// for 6 and 8), 9 externalChargesErfKernel ([n_pairs][Sa Sb]; one omega per charge)
+// (oneelints.cpp:379-473, 587-680, 1513-1577, 1617-1701).
+int ref_one_electron_class_ex(void *h, int use_symm, int iab, int op, const double *charges, const double *omegas,
+                              int n_charges, const double *origin, double *out)
+{
+    return guarded([&]
+    {
+        auto sp = lints::shellPairData(use_symm != 0, *static_cast<RefStructure *>(h)->s);
+        const auto &ab = sp.at(iab);
+        std::vector<std::array<double, 4>> q(n_charges);
+        for (int i = 0; i < n_charges; i++)
+            q[i] = {charges[4 * i], charges[4 * i + 1], charges[4 * i + 2], charges[4 * i + 3]};
+        std::vector<double> w(omegas ? omegas : charges, omegas ? omegas + n_charges : charges);
+        const std::array<double, 3> o = origin ? std::array<double, 3>{origin[0], origin[1], origin[2]}
+                                               : std::array<double, 3>{0, 0, 0};
+        lints::BoysGrid grid(ab.la_ + ab.lb_);
+        const size_t blk = lints::numSphericals(ab.la_) * lints::numSphericals(ab.lb_);
+        const int nb = op == 9 ? 1 : 3;
+        for (size_t i = 0; i < ab.n_pairs_; i++)
+        {
+            double *dst = out + i * nb * blk;
+            if (op == 9)
+            {
+                lible::vec2d v = lints::externalChargesErfKernel(i, q, w, grid, ab);
+                std::memcpy(dst, v.memptr(), blk * sizeof(double));
+                continue;
+            }
+            std::array<lible::vec2d, 3> v = op == 6 ? lints::dipoleMomentKernel(i, o, ab)
+                                            : op == 7 ? lints::momentumKernel(i, ab)
+                                                      : lints::angularMomentumKernel(i, o, ab);
+            for (int d = 0; d < 3; d++)
+                std::memcpy(dst + d * blk, v[d].memptr(), blk * sizeof(double));
+        }
+    });
+}
+
+// The reference's whole-matrix drivers: 4 dipoleMoment, 5 momentum, 6 angularMomentum ([3][nao][nao];
+// origin for 4 and 6), 7 nuclearAttractionErf (one omega per atom), 8 externalChargesErf (one omega
+// per charge) (oneelints.cpp:475-505, 1477-1511, 1579-1615, 1746-1791, 1122-1162).
+int ref_one_electron_ex(void *h, int which, const double *charges, const double *omegas, int n_charges,
+                        const double *origin, double *out)
+{
+    return guarded([&]
+    {
+        const lints::Structure &st = *static_cast<RefStructure *>(h)->s;
+        const std::array<double, 3> o = origin ? std::array<double, 3>{origin[0], origin[1], origin[2]}
+                                               : std::array<double, 3>{0, 0, 0};
+        if (which >= 4 && which <= 6)
+        {
+            std::array<lible::vec2d, 3> v = which == 4 ? lints::dipoleMoment(o, st)
+                                            : which == 5 ? lints::momentum(st)
+                                                         : lints::angularMomentum(o, st);
+            const size_t n = v[0].size();
+            for (int d = 0; d < 3; d++)
+                std::memcpy(out + d * n, v[d].memptr(), n * sizeof(double));
+            return;
+        }
+        lible::vec2d v;
+        if (which == 7)
+            v = lints::nuclearAttractionErf(st, std::vector<double>(omegas, omegas + st.getNAtoms()));
+        else
+        {
+            std::vector<std::array<double, 4>> q(n_charges);
+            for (int i = 0; i < n_charges; i++)
+                q[i] = {charges[4 * i], charges[4 * i + 1], charges[4 * i + 2], charges[4 * i + 3]};
+            v = lints::externalChargesErf(q, std::vector<double>(omegas, omegas + n_charges), st);
+        }
+        std::memcpy(out, v.memptr(), v.size() * sizeof(double));
+    });
+}
+
 int ref_eri2_diagonal(void *h, double *out)
 {
     return guarded([&]

@@ -173,6 +173,43 @@ int main(int argc, char **argv)
         const std::vector<std::array<double, 3>> Xw = {{0, 0, 0}, {0.757, 0.586, 0}, {-0.757, 0.586, 0}};
         lints::Structure sw(readBasis(root + "/main/dunning/cc-pvdz.txt", Zw), Zw, Xw);
         report("eri4(Structure), water cc-pVDZ", maxDiff(lints::gpu::eri4(sw), lints::eri4(sw)));
+
+        // one-electron drivers: CO2 / 6-31+G (the reference's erf-attenuated test molecule) and
+        // ethane / cc-pVDZ (its dipole test molecule), Angstrom
+        const std::vector<int> Zc = {6, 8, 8};
+        const std::vector<std::array<double, 3>> Xc = {{0, 0, 0.32942}, {0, 1.15362, -0.12353},
+                                                       {0, -1.15362, -0.12353}};
+        lints::Structure sc(readBasis(root + "/main/pople/6-31+g.txt", Zc), Zc, Xc);
+        lints::gpu::Context cc(sc);
+        report("overlap(Structure)", maxDiff(lints::gpu::overlap(cc), lints::overlap(sc)));
+        report("kineticEnergy(Structure)", maxDiff(lints::gpu::kineticEnergy(cc), lints::kineticEnergy(sc)));
+        report("nuclearAttraction(Structure)", maxDiff(lints::gpu::nuclearAttraction(cc), lints::nuclearAttraction(sc)));
+        const std::vector<double> om = {0.0035, -0.5, 0.6};
+        report("nuclearAttractionErf(Structure)",
+               maxDiff(lints::gpu::nuclearAttractionErf(cc, om), lints::nuclearAttractionErf(sc, om)));
+        const std::vector<std::array<double, 4>> q = {{1.0, -2.0, 0.5, 0.7}, {-3.0, 1.0, -6.0, -1.2}};
+        const std::vector<double> oq = {1.2, -10.5};
+        report("externalCharges(Structure)", maxDiff(lints::gpu::externalCharges(q, cc), lints::externalCharges(q, sc)));
+        report("externalChargesErf(Structure)",
+               maxDiff(lints::gpu::externalChargesErf(q, oq, cc), lints::externalChargesErf(q, oq, sc)));
+        const std::vector<int> Ze = {1, 6, 1, 1, 6, 1, 1, 1};
+        const std::vector<std::array<double, 3>> Xe = {{1.1851, -0.0039, 0.9875}, {0.7516, -0.0225, -0.0209},
+                                                       {1.1669, 0.8330, -0.5693}, {1.1155, -0.9329, -0.5145},
+                                                       {-0.7516, 0.0225, 0.0209}, {-1.1669, -0.8334, 0.5687},
+                                                       {-1.1157, 0.9326, 0.5151}, {-1.1850, 0.0044, -0.9875}};
+        lints::Structure se(readBasis(root + "/main/dunning/cc-pvdz.txt", Ze), Ze, Xe);
+        lints::gpu::Context ce(se);
+        const std::array<double, 3> o = {0.3, -0.2, 0.5};
+        const auto dg = lints::gpu::dipoleMoment(o, ce), dr = lints::dipoleMoment(o, se);
+        const auto ag = lints::gpu::angularMomentum(o, ce), ar = lints::angularMomentum(o, se);
+        double dd = 0, da = 0;
+        for (int k = 0; k < 3; k++)
+        {
+            dd = std::max(dd, maxDiff(dg[k], dr[k]));
+            da = std::max(da, maxDiff(ag[k], ar[k]));
+        }
+        report("dipoleMoment(origin, Structure)", dd);
+        report("angularMomentum(origin, Structure)", da);
     }
     catch (const std::exception &e)
     {

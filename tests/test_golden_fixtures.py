@@ -133,13 +133,14 @@ def test_gpu_rik_matches_golden():
     assert np.abs(J - g["J"]).max() <= 1e-10
     assert L.rij_last_solve(s)["method"] == "cholesky"
     # that call contracted the cached three-centre tensor; evaluating the integrals on every call
-    # gives the same J, gamma and fitting coefficients (summation order differs only)
+    # gives the same J, gamma and fitting coefficients (summation order differs only; d = M^-1 gamma
+    # carries the metric's condition number, ~4e7, so its bound is 1e-8 relative)
     L.rij_set_cached(s, 0)
     Jn, gn, dn = L.rij(s, g["C"] @ g["C"].T, schwarz=0.0)
     assert np.abs(Jn - g["J"]).max() <= 1e-10
     assert np.abs(Jn - J).max() <= 1e-12
     assert np.abs(gn - gam).max() <= 1e-12 * max(1.0, np.abs(gn).max())
-    assert np.abs(dn - dco).max() <= 1e-10 * max(1.0, np.abs(dn).max())
+    assert np.abs(dn - dco).max() <= 1e-8 * max(1.0, np.abs(dn).max())
     L.rij_set_cached(s, 1)
     Jc, gc, dc = L.rij(s, g["C"] @ g["C"].T, schwarz=0.0)
     assert np.abs(Jc - J).max() <= 1e-12 and np.abs(gc - gam).max() <= 1e-12 * max(1.0, np.abs(gc).max())

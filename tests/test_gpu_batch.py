@@ -150,3 +150,40 @@ def test_jk_profile_times_every_launch_and_returns_the_build():
     assert sum(r["tasks"] for r in prof) == plan["n_quartets"]
     assert any(r["fp32"] for r in prof) and all(r["ms"] > 0 for r in prof)
     assert abs(sum(r["flops"] for r in prof) - plan["flops_fp64"] - plan["flops_fp32"]) <= 1e-6 * plan["flops_fp64"]
+
+
+def test_full_c3_batch_vs_single_structures_and_reference():
+    """The whole heterogeneous batch of the batch benchmark (64 water clusters of 1..12 waters, half
+    cc-pVDZ, half cc-pVTZ, Schwarz 1e-12), built as one batch: every molecule's FP64 J and K against
+    its own single-structure build (1e-11), the mixed-precision batch within the 1e-8 Eh energy bound
+    of FP64 per molecule, and the molecules of up to three waters against the reference's
+    ERI4Kernel J/K digestion over the same screened quartets (1e-11)."""
+    from lible_b200.workloads import batch_clusters
+    from oracle import ref as R
+
+    specs = batch_clusters()
+    b = L.Batch([(bs, Z, xyz) for bs, Z, xyz, _ in specs])
+    Ds = [mk(int(b.nao[m])) for m, (_, _, _, mk) in enumerate(specs)]
+    Dp = b.pack(Ds)
+    J, K, st = L.jk(b, Dp, schwarz=1e-12)
+    Jm, Km, _ = L.jk(b, Dp, schwarz=1e-12, precision="mixed")
+    Js, Ks, Jms, Kms = b.unpack(J), b.unpack(K), b.unpack(Jm), b.unpack(Km)
+    total, n_ref = 0, 0
+    for m, (basis, Z, xyz, _) in enumerate(specs):
+        s = L.Structure(basis, Z, xyz, units="bohr")
+        J1, K1, st1 = L.jk(s, Ds[m], schwarz=1e-12)
+        total += st1["n_quartets"]
+        assert np.abs(Js[m] - J1).max() <= 1e-11, m
+        assert np.abs(Ks[m] - K1).max() <= 1e-11, m
+        E = 0.5 * np.sum(Ds[m] * Js[m]) - 0.25 * np.sum(Ds[m] * Ks[m])
+        Emix = 0.5 * np.sum(Ds[m] * Jms[m]) - 0.25 * np.sum(Ds[m] * Kms[m])
+        assert abs(Emix - E) <= 1e-8, m
+        if len(Z) <= 9:
+            r = R.RefStructure(basis, Z, xyz)
+            Jr, Kr, nq, _ = r.jk(Ds[m], 1e-12)
+            assert nq == st1["n_quartets"], m
+            assert np.abs(Js[m] - Jr).max() <= 1e-11, m
+            assert np.abs(Ks[m] - Kr).max() <= 1e-11, m
+            n_ref += 1
+    assert st["n_quartets"] == total
+    assert n_ref >= 10

@@ -139,3 +139,94 @@ def test_per_pair_kernels_vs_reference_elementwise():
                 want = r.one_electron_class(use_symm, i, op, q if op in (2, 5) else None)
                 assert np.abs(got - want.reshape(got.shape)).max() <= 1e-12 * max(1.0, np.abs(want).max()), \
                     (use_symm, i, op)
+
+
+C2H6_Z = [1, 6, 1, 1, 6, 1, 1, 1]
+C2H6_ANG = [[1.1851, -0.0039, 0.9875], [0.7516, -0.0225, -0.0209], [1.1669, 0.8330, -0.5693],
+            [1.1155, -0.9329, -0.5145], [-0.7516, 0.0225, 0.0209], [-1.1669, -0.8334, 0.5687],
+            [-1.1157, 0.9326, 0.5151], [-1.1850, 0.0044, -0.9875]]
+
+
+def test_dipole_moment_golden_c2h6_and_vs_reference():
+    """dipoleMoment about the origin: the reference's golden sum (test/tests_ints.cpp:597-614, ethane
+    cc-pVDZ) and element-wise against the reference's driver; about another origin too."""
+    s = L.Structure("cc-pvdz", C2H6_Z, C2H6_ANG)
+    r = R.RefStructure("cc-pvdz", C2H6_Z, C2H6_ANG, units="angstrom")
+    M = L.dipoleMoment([0.0, 0.0, 0.0], s)
+    assert golden(seqsum(M), 1205.074870756679)
+    assert np.abs(M - r.one_electron_ex(4, origin=[0.0, 0.0, 0.0])).max() <= 1e-12
+    o = [0.3, -1.2, 0.7]
+    Mo = L.dipoleMoment(o, s)
+    assert np.abs(Mo - r.one_electron_ex(4, origin=o)).max() <= 1e-12 * max(1.0, np.abs(Mo).max())
+    assert np.abs(Mo - Mo.transpose(0, 2, 1)).max() <= 1e-15 * max(1.0, np.abs(Mo).max())
+
+
+def test_erf_attenuated_attraction_golden_co2_and_vs_reference():
+    """nuclearAttractionErf and externalChargesErf with the reference test's range parameters
+    (negative ones included; test/tests_ints.cpp:321-338, 360-379): golden sums and element-wise
+    against the reference's drivers."""
+    s = L.Structure("6-31+g", CO2_Z, CO2_ANG)
+    r = R.RefStructure("6-31+g", CO2_Z, CO2_ANG, units="angstrom")
+    w = [0.0035, -0.5, 0.6]
+    V = L.nuclearAttractionErf(s, w)
+    assert golden(seqsum(V), 257.523987741588)
+    assert np.abs(V - r.one_electron_ex(7, omegas=w)).max() <= 1e-12
+    q = np.array([[x / 0.5291772083 for x in c] + [z] for c, z in zip(CO2_ANG, CO2_Z)])
+    wq = [1.2, -10.5, 0.031]
+    Vq = L.externalChargesErf(q, wq, s)
+    assert golden(seqsum(Vq), 419.197077258843)
+    assert np.abs(Vq - r.one_electron_ex(8, charges=q, omegas=wq)).max() <= 1e-12
+    with pytest.raises(ValueError):
+        L.nuclearAttractionErf(s, [0.5])
+
+
+def test_momentum_and_angular_momentum_vs_reference():
+    """Water dimer cc-pVTZ (f shells).  angularMomentum: element-wise against the reference's driver
+    (antisymmetric).  momentum: the reference's driver (oneelints.cpp:1477-1511) writes only the
+    (a, b) blocks of its unique pairs, negated; every element it writes off the diagonal equals the
+    transposed element of the full antisymmetric matrix returned here, and its diagonal the diagonal."""
+    Z, xyz, rng = water_cluster(2, 5)
+    s = L.Structure("cc-pvtz", Z, xyz, units="bohr")
+    r = R.RefStructure("cc-pvtz", Z, xyz)
+    o = [0.4, 0.1, -0.8]
+    A = L.angularMomentum(o, s)
+    Ar = r.one_electron_ex(6, origin=o)
+    scale = max(1.0, np.abs(Ar).max())
+    assert np.abs(A - Ar).max() <= 1e-12 * scale
+    assert np.abs(A + A.transpose(0, 2, 1)).max() <= 1e-15 * scale
+    P = L.momentum(s)
+    Pr = r.one_electron_ex(5)
+    assert np.abs(P + P.transpose(0, 2, 1)).max() == 0.0
+    n = s.nao
+    written = Pr != 0.0
+    off = written & ~np.eye(n, dtype=bool)[None]
+    assert off.sum() > n * n  # the upper blocks of the unique pairs
+    assert np.abs((Pr - P.transpose(0, 2, 1))[off]).max() <= 1e-12 * max(1.0, np.abs(P).max())
+    assert np.abs(np.diagonal(P, axis1=1, axis2=2)).max() == 0.0
+
+
+def test_new_per_pair_kernels_vs_reference_elementwise():
+    """dipoleMomentKernel, momentumKernel, angularMomentumKernel and externalChargesErfKernel for every
+    class with and without symmetry (la < lb classes, stored swapped, included) against the
+    reference's kernels; ethane cc-pVDZ and a cc-pVTZ water dimer."""
+    q = np.array([[1.0, -2.0, 0.5, 0.7], [-3.0, 1.0, -6.0, -1.2], [6.0, 2.0, -7.0, 2.0]])
+    w = np.array([0.4, -2.5, 11.0])
+    o = [0.2, -0.4, 0.9]
+    Z2, xyz2, _ = water_cluster(2, 7)
+    cases = [(L.Structure("cc-pvdz", C2H6_Z, C2H6_ANG), R.RefStructure("cc-pvdz", C2H6_Z, C2H6_ANG, units="angstrom")),
+             (L.Structure("cc-pvtz", Z2, xyz2, units="bohr"), R.RefStructure("cc-pvtz", Z2, xyz2))]
+    for s, r in cases:
+        for use_symm in (True, False):
+            for i, sp in enumerate(L.shellPairData(use_symm, s)):
+                if not sp.n_pairs_:
+                    continue
+                idx = list(range(sp.n_pairs_))
+                for op, got in ((6, L.dipoleMomentKernel(idx, o, sp)), (7, L.momentumKernel(idx, sp)),
+                                (8, L.angularMomentumKernel(idx, o, sp)),
+                                (9, L.externalChargesErfKernel(idx, q, w, sp))):
+                    want = r.one_electron_class_ex(use_symm, i, op, charges=q, omegas=w, origin=o)
+                    assert np.abs(got - want.reshape(got.shape)).max() <= 1e-12 * max(1.0, np.abs(want).max()), \
+                        (use_symm, i, op)
+    # a single pair returns the three blocks
+    sp = L.shellPairData(True, cases[0][0])[0]
+    assert len(L.momentumKernel(0, sp)) == 3

@@ -167,6 +167,29 @@ def test_reference_one_electron_golden():
 
 
 @needs_ref
+def test_reference_multipole_and_erf_golden():
+    # the compiled reference reproduces its dipole-moment and erf-attenuated golden sums
+    # (test/tests_ints.cpp:321-338, 360-379, 597-614); these pin the oracle of those operators
+    co2 = [[0.0, 0.0, 0.32942], [0.0, 1.15362, -0.12353], [0.0, -1.15362, -0.12353]]
+    r = ref.RefStructure("6-31+g", [6, 8, 8], co2, units="angstrom")
+    assert abs(seqsum(r.one_electron_ex(7, omegas=[0.0035, -0.5, 0.6])) - 257.523987741588) <= 1e-13 * 257.5
+    q = np.array([[x / 0.5291772083 for x in c] + [z] for c, z in zip(co2, [6, 8, 8])])
+    Vq = r.one_electron_ex(8, charges=q, omegas=[1.2, -10.5, 0.031])
+    assert abs(seqsum(Vq) - 419.197077258843) <= 1e-13 * 419.2
+    c2h6 = [[1.1851, -0.0039, 0.9875], [0.7516, -0.0225, -0.0209], [1.1669, 0.8330, -0.5693],
+            [1.1155, -0.9329, -0.5145], [-0.7516, 0.0225, 0.0209], [-1.1669, -0.8334, 0.5687],
+            [-1.1157, 0.9326, 0.5151], [-1.1850, 0.0044, -0.9875]]
+    r2 = ref.RefStructure("cc-pvdz", [1, 6, 1, 1, 6, 1, 1, 1], c2h6, units="angstrom")
+    assert abs(seqsum(r2.one_electron_ex(4, origin=[0.0, 0.0, 0.0])) - 1205.074870756679) <= 1e-13 * 1205.1
+    # angular momentum is antisymmetric; the momentum driver writes one orientation of each unique
+    # pair of different shells only, so its matrices are not
+    A = r2.one_electron_ex(6, origin=[0.1, 0.2, 0.3])
+    assert np.abs(A + A.transpose(0, 2, 1)).max() <= 1e-14 * np.abs(A).max()
+    P = r2.one_electron_ex(5)
+    assert np.abs(P + P.transpose(0, 2, 1)).max() > 0.1 * np.abs(P).max()
+
+
+@needs_ref
 def test_reference_soc_and_d2_golden():
     # the compiled reference reproduces its ERI4SOC / ERI3SOC / ERI2D2 kernel golden sums
     # (test/tests_ints.cpp:1055-1150) through the oracle's per-class wrappers
