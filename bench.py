@@ -282,7 +282,7 @@ def run_rij(Z, xyz, D, J64, steps):
         ts.append(time.perf_counter() - t)
     tensor_bytes = 8.0 * s.naux * s.nao * s.nao
     return {"workload": "RI-J, (H2O)_32 cc-pVDZ, even-tempered s-f auxiliary basis, FP64", "naux": s.naux,
-            "setup_s": setup, "first_call_s": first, "rij_s": float(np.mean(ts)),
+            "setup_s": setup, "first_call_s": first, "rij_s": float(np.mean(ts)), "rij_samples_s": ts,
             "tensor_bytes": tensor_bytes,
             "tensor_read_gbs": 2 * tensor_bytes / float(np.mean(ts)) / 1e9,
             "solve": L.rij_last_solve(s),
@@ -326,7 +326,8 @@ def run_rijk(Z, xyz, D, J64, K64, occ, steps):
     rates = {k: info["flops_" + k] / max(info["t_" + k], 1e-12) / 1e12 for k in ("gemm", "solve", "syrk")}
     return {"workload": "RI-JK, (H2O)_32 cc-pVDZ / def2-universal-jkfit, FP64, occupied factor C (160)",
             "naux": s.naux, "setup_s": setup, "first_call_s": first, "rij_s": float(np.mean(tj)),
-            "rik_s": float(np.mean(tk)), "rik_from_D_s": t_dpath, "rij_gradient_s": t_grad,
+            "rik_s": float(np.mean(tk)), "rij_samples_s": tj, "rik_samples_s": tk, "rik_from_D_s": t_dpath,
+            "rij_gradient_s": t_grad,
             "rij_gradient_translational_residual": float(np.abs(gJ.sum(axis=0)).max()),
             "solve": L.rij_last_solve(s),
             "rik_stages_s": {k: info["t_" + k] for k in ("ints", "gemm", "solve", "syrk")},

@@ -300,10 +300,16 @@ int lible_gpu_one_electron(lible_gpu_ctx *ctx, const double *charges, int n_char
 int lible_gpu_one_electron_batch(lible_gpu_ctx *ctx, int use_symm, int class_ab, int op, long long n,
                                  const unsigned *pairs, const double *charges, int n_charges, double *out);
 /* The same with the remaining per-pair kernels: op 6 dipoleMomentKernel, 7 momentumKernel, 8
- * angularMomentumKernel ([3][S_a][S_b] = x, y, z; `origin` [3] for 6 and 8, bohr) and op 9
- * externalChargesErfKernel ([S_a][S_b]; `omegas` one range parameter per charge, NULL charges = the
- * nuclei with one omega per atom) (ints.hpp:71-75, 123-148; oneelints.cpp:379-473, 587-680,
- * 1513-1577, 1617-1701).  Unused pointers may be NULL. */
+ * angularMomentumKernel ([3][S_a][S_b] = x, y, z; `origin` [3] for 6 and 8, bohr), op 9
+ * externalChargesErfKernel ([S_a][S_b]), op 10 externalChargesErfD1Kernel ([6][S_a][S_b], orbital
+ * part), op 11 / 12 the operator part d/dC_xyz of externalChargesKernel / externalChargesErfKernel
+ * summed over the given charges ([3][S_a][S_b]; one charge per call gives the reference's
+ * externalChargesOperator(Erf)D1Kernel entry for that charge), op 13 spinOrbitCoupling1ElKernel
+ * ([3][S_a][S_b], the given charges; ints.hpp:135-137, oneelints.cpp:1209-1316).  `omegas`: one range parameter per
+ * charge for 9, 10, 12 (NULL charges = the nuclei, one omega per atom; 9 scales a charge by
+ * w / sqrt(w^2 + p), 10 and 12 by sqrt(w^2 / (w^2 + p)), as the reference's kernels do) (ints.hpp:66-148;
+ * oneelints.cpp:379-473, 587-680, 791-889, 1513-1577, 1617-1701, 1844-2060).  Unused pointers may be
+ * NULL. */
 int lible_gpu_one_electron_batch_ex(lible_gpu_ctx *ctx, int use_symm, int class_ab, int op, long long n,
                                     const unsigned *pairs, const double *charges, const double *omegas, int n_charges,
                                     const double *origin, double *out);
@@ -313,10 +319,12 @@ int lible_gpu_one_electron_batch_ex(lible_gpu_ctx *ctx, int use_symm, int class_
  *     driver, oneelints.cpp:1477-1511, writes only the (a, b) blocks of its unique pairs, negated);
  *   angularMomentum (ints.hpp:146-147): -<m| (r - origin) x d/dr |n>, antisymmetric;
  *   nuclearAttractionErf (ints.hpp:52): the nuclei's erf(w r)/r attraction, `omegas` one per atom;
- *   externalChargesErf (ints.hpp:60-62): the same for point charges [n][4], one omega each. */
+ *   externalChargesErf (ints.hpp:60-62): the same for point charges [n][4], one omega each;
+ *   spinOrbitCoupling1El (ints.hpp:131): the one-electron SOC integrals of the nuclei, antisymmetric. */
 int lible_gpu_dipole_moment(lible_gpu_ctx *ctx, const double *origin, double *out);
 int lible_gpu_momentum(lible_gpu_ctx *ctx, double *out);
 int lible_gpu_angular_momentum(lible_gpu_ctx *ctx, const double *origin, double *out);
+int lible_gpu_spin_orbit_coupling_1el(lible_gpu_ctx *ctx, double *out);
 int lible_gpu_nuclear_attraction_erf(lible_gpu_ctx *ctx, const double *omegas, double *out);
 int lible_gpu_external_charges_erf(lible_gpu_ctx *ctx, const double *charges, const double *omegas, int n_charges,
                                    double *out);

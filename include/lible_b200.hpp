@@ -16,7 +16,8 @@
  *   ERI4Kernel, ERI3Kernel, ERI2Kernel, ERI4D1Kernel,
  *   ERI3D1Kernel, ERI2D1Kernel (operator())                 src/lible/ints/twoel/eri_kernels.hpp:60-169
  *   overlap, kineticEnergy, nuclearAttraction, nuclearAttractionErf, externalCharges,
- *   externalChargesErf, dipoleMoment, momentum, angularMomentum  src/lible/ints/ints.hpp:29-151
+ *   externalChargesErf, dipoleMoment, momentum, angularMomentum,
+ *   spinOrbitCoupling1El                                     src/lible/ints/ints.hpp:29-151
  * Failures throw std::runtime_error with the library's message, as the reference throws
  * std::runtime_error for its own error cases.  jk(), jkEnergy() and jkEnergyGradient() have no
  * reference counterpart.
@@ -347,6 +348,17 @@ namespace lible::ints::gpu
     {
         Context c(structure, device);
         return angularMomentum(origin, c);
+    }
+    inline std::array<vec2d, 3> spinOrbitCoupling1El(Context &c)
+    {
+        std::vector<double> flat(3 * c.dimAO() * c.dimAO());
+        c.check(lible_gpu_spin_orbit_coupling_1el(c.get(), flat.data()));
+        return detail::three(c, flat);
+    }
+    inline std::array<vec2d, 3> spinOrbitCoupling1El(const Structure &structure, int device = 0)
+    {
+        Context c(structure, device);
+        return spinOrbitCoupling1El(c);
     }
 
     // ---- kernel functors (eri_kernels.hpp:60-169) -------------------------------------------------

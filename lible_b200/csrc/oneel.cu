@@ -250,10 +250,24 @@ namespace lible_b200
             kOpMomentum = 7,
             kOpAngular = 8,
             kOpVErf = 9,
+            kOpVErfD1 = 10,   // externalChargesErfD1Kernel: orbital part, [6] blocks
+            kOpVOpD1 = 11,    // externalChargesOperatorD1Kernel for the charges summed: d/dC_xyz, [3]
+            kOpVErfOpD1 = 12, // the same, erf-attenuated
+            kOpSOC = 13,      // spinOrbitCoupling1ElKernel, [3]
         };
         __host__ __device__ constexpr int oneOpBlocks(int op)
         {
-            return (op >= kOpSD1 && op <= kOpVD1) ? 6 : (op >= kOpDipole && op <= kOpAngular) ? 3 : 1;
+            return ((op >= kOpSD1 && op <= kOpVD1) || op == kOpVErfD1)                   ? 6
+                   : ((op >= kOpDipole && op <= kOpAngular) || op >= kOpVOpD1) ? 3
+                                                                                          : 1;
+        }
+        __host__ __device__ constexpr bool oneOpUsesCharges(int op)
+        {
+            return op == kOpV || op == kOpVD1 || op >= kOpVErf;
+        }
+        __host__ __device__ constexpr bool oneOpUsesOmegas(int op)
+        {
+            return op == kOpVErf || op == kOpVErfD1 || op == kOpVErfOpD1;
         }
 
         struct OnePairArgs
@@ -318,8 +332,8 @@ namespace lible_b200
             auto ex = [&](int axis, int i, int j, int t) { return E[axis * S::EAX + (i * NB + j) * NT + t]; };
             auto ex1 = [&](int axis, int i, int j, int t) { return E1[axis * S::EAX + (i * NB + j) * NT + t]; };
             const int op = GRAD ? -1 : a.op;
-            const bool wantV = GRAD ? a.D != nullptr : (op == kOpV || op == kOpVD1 || op == kOpVErf);
-            const bool d1 = GRAD || oneOpBlocks(op) == 6;
+            const bool wantV = GRAD ? a.D != nullptr : oneOpUsesCharges(op);
+            const bool d1 = GRAD || oneOpBlocks(op) == 6 || op == kOpSOC;
             const int oa = a.ao[2 * ipair], ob = a.ao[2 * ipair + 1];
             const size_t n = (size_t)a.nao;
             const double *nA = a.norms_a + (size_t)ipair * S::SA, *nB = a.norms_b + (size_t)ipair * S::SB;
@@ -392,13 +406,15 @@ namespace lible_b200
                         const double *q = a.charges + 4 * (size_t)c;
                         const double X = P[0] - q[0], Y = P[1] - q[1], Z = P[2] - q[2];
                         double F[L1 + 1], R[S::NR1];
-                        // erf attenuation: exponent p w^2 / (p + w^2), scale w / sqrt(w^2 + p)
+                        // erf attenuation: exponent p w^2 / (p + w^2), scale w / sqrt(w^2 + p); the
+                        // reference's derivative kernels scale by sqrt(w^2 / (w^2 + p)) instead
+                        // (oneelints.cpp:1907-1909, 2028-2030 against :628), which differs for w < 0
                         double pe = p, qs = q[3];
                         if (a.omegas)
                         {
                             const double w = a.omegas[c], w2 = w * w;
                             pe = p * w2 / (p + w2);
-                            qs *= w / sqrt(w2 + p);
+                            qs *= (op == kOpVErfD1 || op == kOpVErfOpD1 ? fabs(w) : w) / sqrt(w2 + p);
                         }
                         boysF<L1, false>(pe * (X * X + Y * Y + Z * Z), a.boys + (size_t)L1 * kBoysTerms * kBoysPitch, F);
 #pragma unroll
@@ -472,7 +488,23 @@ namespace lible_b200
                                                s0[0] * s0[1] * kin(0, 2));
                         else if (op == kOpV || op == kOpVErf)
                             acc[0][w] -= fv * vsum(-1, -1);
-                        else if (op >= kOpDipole)
+                        else if (op == kOpSOC)
+                        {
+                            // the reference's SOC form (oneelints.cpp:1209-1316): with
+                            // [d, e] = sum E(E1 on axis e) R_{+1 on axis d},
+                            // x: -f ([z, y] - [y, z]), y: -f ([x, z] - [z, x]), z: -f ([y, x] - [x, y])
+                            acc[0][w] -= fv * (vsum(2, 1) - vsum(1, 2));
+                            acc[1][w] -= fv * (vsum(0, 2) - vsum(2, 0));
+                            acc[2][w] -= fv * (vsum(1, 0) - vsum(0, 1));
+                        }
+                        else if (op == kOpVOpD1 || op == kOpVErfOpD1)
+                        {
+                            // d/dC of -f q sum E R(P - C): +f q sum E R_{t+1} (and u, v)
+#pragma unroll
+                            for (int x = 0; x < 3; x++)
+                                acc[x][w] += fv * vsum(x, -1);
+                        }
+                        else if (op >= kOpDipole && op <= kOpAngular)
                         {
                             // first moments about the origin and first derivatives on b, per axis
                             double m1[3], dd[3];
@@ -637,7 +669,7 @@ namespace lible_b200
                 // caller's orientation: blocks transposed, d/dA and d/dB exchanged, and the
                 // antisymmetric operators (momentum, angular momentum) negated
                 const int nblk = oneOpBlocks(op);
-                const double sgn = (a.swap && (op == kOpMomentum || op == kOpAngular)) ? -1.0 : 1.0;
+                const double sgn = (a.swap && (op == kOpMomentum || op == kOpAngular || op == kOpSOC)) ? -1.0 : 1.0;
                 for (int d = 0; d < nblk; d++)
 #pragma unroll
                     for (int w = 0; w < S::PER_LANE; w++)
@@ -819,9 +851,9 @@ namespace lible_b200
 
         void checkOneOp(int op, const double *omegas_host, const double *origin)
         {
-            if (op < 0 || op > kOpVErf)
+            if (op < 0 || op > kOpSOC)
                 throw EngineError(kStatusInvalid, "bad one-electron operator");
-            if (op == kOpVErf && !omegas_host)
+            if (oneOpUsesOmegas(op) && !omegas_host)
                 throw EngineError(kStatusInvalid, "the erf-attenuated operator needs one omega per charge");
             if ((op == kOpDipole || op == kOpAngular) && !origin)
                 throw EngineError(kStatusInvalid, "the operator needs an origin");
@@ -832,8 +864,8 @@ namespace lible_b200
                                      const double *origin, double *out_dev)
     {
         requireSingle();
-        if (op < kOpDipole)
-            throw EngineError(kStatusInvalid, "the whole-matrix operator form covers ops 6..9");
+        if (op < kOpDipole || (op > kOpVErf && op != kOpSOC))
+            throw EngineError(kStatusInvalid, "the whole-matrix operator form covers ops 6..9 and 13");
         checkOneOp(op, omegas_host, origin);
         if (max_l_ > 3)
             throw EngineError(kStatusUnsupported, "one-electron kernels are instantiated for l <= 3");
@@ -848,7 +880,7 @@ namespace lible_b200
         const int nblk = oneOpBlocks(op);
         const size_t n = nao_;
         cudaCheck(cudaMemsetAsync(out_dev, 0, (size_t)nblk * n * n * sizeof(double), stream_), "memset");
-        const double sign = (op == kOpMomentum || op == kOpAngular) ? -1.0 : 1.0;
+        const double sign = (op == kOpMomentum || op == kOpAngular || op == kOpSOC) ? -1.0 : 1.0;
         ClassSet &cs = mainSet(true);
         for (size_t c = 0; c < cs.host.size(); c++)
         {
@@ -931,11 +963,11 @@ namespace lible_b200
         DevBuf<double> dq, dw;
         upload(dl, list, stream_);
         upload(dq, q, stream_);
-        if (op == kOpVErf)
+        if (oneOpUsesOmegas(op))
             upload(dw, std::vector<double>(omegas_host, omegas_host + q.size() / 4), stream_);
         OnePairArgs a{};
         a.op = op;
-        a.omegas = op == kOpVErf ? dw.p : nullptr;
+        a.omegas = oneOpUsesOmegas(op) ? dw.p : nullptr;
         if (origin)
             for (int x = 0; x < 3; x++)
                 a.origin[x] = origin[x];

@@ -526,7 +526,7 @@ def _one_batch(op, ipair, sp, charges=None, omegas=None, origin=None):
     array)."""
     single = np.ndim(ipair) == 0
     idx = np.ascontiguousarray(np.atleast_1d(np.asarray(ipair, dtype=np.uint32)))
-    nb = 6 if 3 <= op <= 5 else 3 if 6 <= op <= 8 else 1
+    nb = 6 if (3 <= op <= 5 or op == 10) else 3 if (6 <= op <= 8 or op >= 11) else 1
     out = np.empty((len(idx), nb, _nsph(sp.la_), _nsph(sp.lb_)))
     if charges is None:
         q, nq = None, 0
@@ -596,6 +596,50 @@ def externalChargesErfKernel(ipair, charges, omegas, sp_data):
     return _one_batch(9, ipair, sp_data, charges, omegas=omegas)
 
 
+def externalChargesErfD1Kernel(ipair, charges, omegas, sp_data):
+    """lible::ints::externalChargesErfD1Kernel (ints.hpp:86-89): the orbital part, six blocks."""
+    return _one_batch(10, ipair, sp_data, charges, omegas=omegas)
+
+
+def _per_charge(op, ipair, charges, sp_data, omegas=None):
+    q = _f64(charges).reshape(-1, 4)
+    w = None if omegas is None else _f64(omegas).ravel()
+    if w is not None and w.size != len(q):
+        raise ValueError("one omega per charge")
+    parts = [np.asarray(_one_batch(op, ipair, sp_data, q[c:c + 1], omegas=None if w is None else w[c:c + 1]))
+             for c in range(len(q))]
+    if np.ndim(ipair) == 0:
+        return [list(p) if op >= 11 else p for p in parts]
+    return np.stack(parts, axis=1)
+
+
+def externalChargesOperatorD1Kernel(ipair, charges, sp_data):
+    """lible::ints::externalChargesOperatorD1Kernel (ints.hpp:93-96): per charge, the derivatives
+    with respect to its position [x, y, z]."""
+    return _per_charge(11, ipair, charges, sp_data)
+
+
+def externalChargesOperatorErfD1Kernel(ipair, charges, omegas, sp_data):
+    """lible::ints::externalChargesOperatorErfD1Kernel (ints.hpp:101-105)."""
+    return _per_charge(12, ipair, charges, sp_data, omegas)
+
+
+def potentialAtExternalChargesKernel(ipair, charges, sp_data):
+    """lible::ints::potentialAtExternalChargesKernel (ints.hpp:109-112): one block per charge."""
+    return _per_charge(2, ipair, charges, sp_data)
+
+
+def potentialAtExternalChargesErfKernel(ipair, charges, omegas, sp_data):
+    """lible::ints::potentialAtExternalChargesErfKernel (ints.hpp:116-120)."""
+    return _per_charge(9, ipair, charges, sp_data, omegas)
+
+
+def spinOrbitCoupling1ElKernel(ipair, charges, sp_data):
+    """lible::ints::spinOrbitCoupling1ElKernel (ints.hpp:135-137): [x, y, z] blocks for the point
+    charges [x, y, z, q]; the Boys grid argument is not needed."""
+    return _one_batch(13, ipair, sp_data, charges)
+
+
 def _one_operator(structure, fn, nblk, *args):
     n = structure.nao
     out = np.empty((nblk, n, n) if nblk > 1 else (n, n))
@@ -618,6 +662,11 @@ def momentum(structure):
 def angularMomentum(origin, structure):
     """lible::ints::angularMomentum (ints.hpp:146-147): [3][nao][nao], antisymmetric."""
     return _one_operator(structure, "lible_gpu_angular_momentum", 3, _ptr(_f64(origin)))
+
+
+def spinOrbitCoupling1El(structure):
+    """lible::ints::spinOrbitCoupling1El (ints.hpp:131): [3][nao][nao] for the nuclei, antisymmetric."""
+    return _one_operator(structure, "lible_gpu_spin_orbit_coupling_1el", 3)
 
 
 def nuclearAttractionErf(structure, omegas):

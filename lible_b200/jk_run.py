@@ -2,11 +2,14 @@
 
     python -m lible_b200.jk_run --waters 8 --basis cc-pvdz --precision fp64 --repeat 2
     python -m lible_b200.jk_run --waters 2 --basis cc-pvtz --gradient --repeat 2
+    python -m lible_b200.jk_run --waters 8 --rik def2-universal-jkfit --occ 40 --repeat 2
 
 The cluster and density follow lible_b200.workloads (5.7 bohr lattice, random rotations, +-0.6 bohr
 jitter, D = C C^T with occupation 5 per water unless --occ is given).  Every build is a separate
 lible_gpu_jk call on the structure's stream; the first one also builds the Schwarz factors and the
-screening plan.  --gradient runs the J/K energy gradient (lible_gpu_jk_energy_backward) instead.
+screening plan.  --gradient runs the J/K energy gradient (lible_gpu_jk_energy_backward) instead;
+--rik AUX runs RI-K with that auxiliary basis from an orthonormal occupied factor C (the first call
+builds and keeps the fitted three-centre tensor).
 Small cases of this command are what kernel profiles are taken on.
 """
 import argparse
@@ -26,6 +29,7 @@ def main(argv=None):
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--repeat", type=int, default=2)
     ap.add_argument("--gradient", action="store_true")
+    ap.add_argument("--rik", default=None, metavar="AUX")
     args = ap.parse_args(argv)
 
     import torch
@@ -34,6 +38,19 @@ def main(argv=None):
     from .workloads import random_density, water_cluster
 
     Z, xyz, rng = water_cluster(args.waters, args.seed)
+    if args.rik:
+        import numpy as np
+
+        s = L.Structure(args.basis, Z, xyz, args.rik, units="bohr")
+        C = np.linalg.qr(rng.standard_normal((s.nao, args.occ or 5 * args.waters)))[0]
+        times, info = [], None
+        for _ in range(args.repeat):
+            t = time.perf_counter()
+            _, info = L.rik(s, C=C, schwarz=args.schwarz, info=True)
+            times.append(time.perf_counter() - t)
+        print(json.dumps({"waters": args.waters, "basis": args.basis, "aux": args.rik, "nao": s.nao,
+                          "naux": s.naux, "rik": info, "wall_s": times}))
+        return 0
     s = L.Structure(args.basis, Z, xyz, units="bohr")
     D = random_density(s.nao, args.occ or 5 * args.waters, rng)
     Dd = torch.tensor(D, device="cuda")

@@ -130,7 +130,7 @@ class RefStructure:
     def one_electron_ex(self, which, charges=None, omegas=None, origin=None):
         """The reference's dipoleMoment / momentum / angularMomentum ([3][nao][nao], which = 4, 5, 6)
         and nuclearAttractionErf / externalChargesErf (which = 7, 8)."""
-        out = np.empty((3, self.nao, self.nao) if which <= 6 else (self.nao, self.nao))
+        out = np.empty((3, self.nao, self.nao) if (which <= 6 or which == 9) else (self.nao, self.nao))
         q = np.ascontiguousarray(charges if charges is not None else np.zeros((0, 4)), dtype=np.float64)
         w = None if omegas is None else np.ascontiguousarray(omegas, dtype=np.float64)
         o = None if origin is None else np.ascontiguousarray(origin, dtype=np.float64)
@@ -168,11 +168,14 @@ class RefStructure:
 
     def one_electron_class_ex(self, use_symm, iab, op, charges=None, omegas=None, origin=None):
         """op 6 dipoleMomentKernel, 7 momentumKernel, 8 angularMomentumKernel ([n][3][Sa][Sb]),
-        9 externalChargesErfKernel ([n][Sa][Sb]) for every pair of one class."""
+        9 externalChargesErfKernel ([n][Sa][Sb]), 10 externalChargesErfD1Kernel ([n][6][Sa][Sb]),
+        11 / 12 externalChargesOperator(Erf)D1Kernel ([n][n_charges * 3][Sa][Sb]), 13 / 14
+        potentialAtExternalCharges(Erf)Kernel ([n][n_charges][Sa][Sb]) for every pair of one class."""
         la, lb, na, _ = self.pair_classes(use_symm)[iab]
-        nb = 1 if op == 9 else 3
-        out = np.empty((na, nb, 2 * la + 1, 2 * lb + 1))
         q = np.ascontiguousarray(charges if charges is not None else np.zeros((0, 4)), dtype=np.float64)
+        nq = len(q)
+        nb = 1 if op == 9 else 6 if op == 10 else 3 * nq if op in (11, 12) else nq if op in (13, 14) else 3
+        out = np.empty((na, nb, 2 * la + 1, 2 * lb + 1))
         w = None if omegas is None else np.ascontiguousarray(omegas, dtype=np.float64)
         o = None if origin is None else np.ascontiguousarray(origin, dtype=np.float64)
         self._chk(lib().ref_one_electron_class_ex(self.h, int(use_symm), iab, op, _p(q),

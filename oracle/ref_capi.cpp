@@ -365,8 +365,12 @@ int ref_one_electron(void *h, int which, const double *charges, int n_charges, d
 
 // The reference's remaining per-pair one-electron kernels for every pair of one class:
 // op 6 dipoleMomentKernel, 7 momentumKernel, 8 angularMomentumKernel ([n_pairs][3][Sa Sb]; origin
-// for 6 and 8), 9 externalChargesErfKernel ([n_pairs][Sa Sb]; one omega per charge)
-// (oneelints.cpp:379-473, 587-680, 1513-1577, 1617-1701).
+// for 6 and 8), 9 externalChargesErfKernel ([n_pairs][Sa Sb]; one omega per charge),
+// 10 externalChargesErfD1Kernel ([n_pairs][6][Sa Sb]), 11 externalChargesOperatorD1Kernel and
+// 12 externalChargesOperatorErfD1Kernel ([n_pairs][n_charges][3][Sa Sb]), 13
+// potentialAtExternalChargesKernel and 14 potentialAtExternalChargesErfKernel
+// ([n_pairs][n_charges][Sa Sb]), 15 spinOrbitCoupling1ElKernel ([n_pairs][3][Sa Sb]) (oneelints.cpp:
+// 379-473, 587-680, 791-1086, 1209-1316, 1513-1577, 1617-1701, 1844-2060).
 int ref_one_electron_class_ex(void *h, int use_symm, int iab, int op, const double *charges, const double *omegas,
                               int n_charges, const double *origin, double *out)
 {
@@ -380,9 +384,11 @@ int ref_one_electron_class_ex(void *h, int use_symm, int iab, int op, const doub
         std::vector<double> w(omegas ? omegas : charges, omegas ? omegas + n_charges : charges);
         const std::array<double, 3> o = origin ? std::array<double, 3>{origin[0], origin[1], origin[2]}
                                                : std::array<double, 3>{0, 0, 0};
-        lints::BoysGrid grid(ab.la_ + ab.lb_);
+        const bool d1 = op == 10 || op == 11 || op == 12 || op == 15;
+        lints::BoysGrid grid(ab.la_ + ab.lb_ + (d1 ? 1 : 0));
         const size_t blk = lints::numSphericals(ab.la_) * lints::numSphericals(ab.lb_);
-        const int nb = op == 9 ? 1 : 3;
+        const size_t nq = (size_t)n_charges;
+        const size_t nb = op == 9 ? 1 : op == 10 ? 6 : (op == 11 || op == 12) ? 3 * nq : (op == 13 || op == 14) ? nq : 3;
         for (size_t i = 0; i < ab.n_pairs_; i++)
         {
             double *dst = out + i * nb * blk;
@@ -390,6 +396,38 @@ int ref_one_electron_class_ex(void *h, int use_symm, int iab, int op, const doub
             {
                 lible::vec2d v = lints::externalChargesErfKernel(i, q, w, grid, ab);
                 std::memcpy(dst, v.memptr(), blk * sizeof(double));
+                continue;
+            }
+            if (op == 10)
+            {
+                std::array<lible::vec2d, 6> v = lints::externalChargesErfD1Kernel(i, q, w, grid, ab);
+                for (int d = 0; d < 6; d++)
+                    std::memcpy(dst + d * blk, v[d].memptr(), blk * sizeof(double));
+                continue;
+            }
+            if (op == 11 || op == 12)
+            {
+                std::vector<std::array<lible::vec2d, 3>> v =
+                    op == 11 ? lints::externalChargesOperatorD1Kernel(i, q, grid, ab)
+                             : lints::externalChargesOperatorErfD1Kernel(i, q, w, grid, ab);
+                for (size_t c = 0; c < nq; c++)
+                    for (int d = 0; d < 3; d++)
+                        std::memcpy(dst + (3 * c + d) * blk, v[c][d].memptr(), blk * sizeof(double));
+                continue;
+            }
+            if (op == 15)
+            {
+                std::array<lible::vec2d, 3> v = lints::spinOrbitCoupling1ElKernel(i, q, grid, ab);
+                for (int d = 0; d < 3; d++)
+                    std::memcpy(dst + d * blk, v[d].memptr(), blk * sizeof(double));
+                continue;
+            }
+            if (op >= 13)
+            {
+                std::vector<lible::vec2d> v = op == 13 ? lints::potentialAtExternalChargesKernel(i, q, grid, ab)
+                                                       : lints::potentialAtExternalChargesErfKernel(i, q, w, grid, ab);
+                for (size_t c = 0; c < nq; c++)
+                    std::memcpy(dst + c * blk, v[c].memptr(), blk * sizeof(double));
                 continue;
             }
             std::array<lible::vec2d, 3> v = op == 6 ? lints::dipoleMomentKernel(i, o, ab)
@@ -401,9 +439,10 @@ int ref_one_electron_class_ex(void *h, int use_symm, int iab, int op, const doub
     });
 }
 
-// The reference's whole-matrix drivers: 4 dipoleMoment, 5 momentum, 6 angularMomentum ([3][nao][nao];
-// origin for 4 and 6), 7 nuclearAttractionErf (one omega per atom), 8 externalChargesErf (one omega
-// per charge) (oneelints.cpp:475-505, 1477-1511, 1579-1615, 1746-1791, 1122-1162).
+// The reference's whole-matrix drivers: 4 dipoleMoment, 5 momentum, 6 angularMomentum, 9
+// spinOrbitCoupling1El ([3][nao][nao]; origin for 4 and 6), 7 nuclearAttractionErf (one omega per
+// atom), 8 externalChargesErf (one omega per charge) (oneelints.cpp:475-505, 1122-1162, 1164-1207,
+// 1477-1511, 1579-1615, 1746-1791).
 int ref_one_electron_ex(void *h, int which, const double *charges, const double *omegas, int n_charges,
                         const double *origin, double *out)
 {
@@ -412,11 +451,12 @@ int ref_one_electron_ex(void *h, int which, const double *charges, const double 
         const lints::Structure &st = *static_cast<RefStructure *>(h)->s;
         const std::array<double, 3> o = origin ? std::array<double, 3>{origin[0], origin[1], origin[2]}
                                                : std::array<double, 3>{0, 0, 0};
-        if (which >= 4 && which <= 6)
+        if ((which >= 4 && which <= 6) || which == 9)
         {
-            std::array<lible::vec2d, 3> v = which == 4 ? lints::dipoleMoment(o, st)
+            std::array<lible::vec2d, 3> v = which == 4   ? lints::dipoleMoment(o, st)
                                             : which == 5 ? lints::momentum(st)
-                                                         : lints::angularMomentum(o, st);
+                                            : which == 6 ? lints::angularMomentum(o, st)
+                                                         : lints::spinOrbitCoupling1El(st);
             const size_t n = v[0].size();
             for (int d = 0; d < 3; d++)
                 std::memcpy(out + d * n, v[d].memptr(), n * sizeof(double));

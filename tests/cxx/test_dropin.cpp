@@ -210,6 +210,11 @@ int main(int argc, char **argv)
         }
         report("dipoleMoment(origin, Structure)", dd);
         report("angularMomentum(origin, Structure)", da);
+        const auto sg = lints::gpu::spinOrbitCoupling1El(ce), sr = lints::spinOrbitCoupling1El(se);
+        double ds = 0;
+        for (int k = 0; k < 3; k++)
+            ds = std::max(ds, maxDiff(sg[k], sr[k]));
+        report("spinOrbitCoupling1El(Structure)", ds);
     }
     catch (const std::exception &e)
     {

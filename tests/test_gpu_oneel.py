@@ -205,6 +205,18 @@ def test_momentum_and_angular_momentum_vs_reference():
     assert np.abs(np.diagonal(P, axis1=1, axis2=2)).max() == 0.0
 
 
+def test_spin_orbit_coupling_1el_vs_reference():
+    """spinOrbitCoupling1El of the nuclei against the reference's driver, which evaluates every
+    ordered shell pair (ethane cc-pVDZ, cc-pVTZ water dimer); the matrices are antisymmetric."""
+    Z2, xyz2, _ = water_cluster(2, 7)
+    for s, r in ((L.Structure("cc-pvdz", C2H6_Z, C2H6_ANG), R.RefStructure("cc-pvdz", C2H6_Z, C2H6_ANG, units="angstrom")),
+                 (L.Structure("cc-pvtz", Z2, xyz2, units="bohr"), R.RefStructure("cc-pvtz", Z2, xyz2))):
+        M, Mr = L.spinOrbitCoupling1El(s), r.one_electron_ex(9)
+        scale = max(1.0, np.abs(Mr).max())
+        assert np.abs(M - Mr).max() <= 1e-12 * scale
+        assert np.abs(M + M.transpose(0, 2, 1)).max() == 0.0
+
+
 def test_new_per_pair_kernels_vs_reference_elementwise():
     """dipoleMomentKernel, momentumKernel, angularMomentumKernel and externalChargesErfKernel for every
     class with and without symmetry (la < lb classes, stored swapped, included) against the
@@ -223,10 +235,51 @@ def test_new_per_pair_kernels_vs_reference_elementwise():
                 idx = list(range(sp.n_pairs_))
                 for op, got in ((6, L.dipoleMomentKernel(idx, o, sp)), (7, L.momentumKernel(idx, sp)),
                                 (8, L.angularMomentumKernel(idx, o, sp)),
-                                (9, L.externalChargesErfKernel(idx, q, w, sp))):
+                                (9, L.externalChargesErfKernel(idx, q, w, sp)),
+                                (15, L.spinOrbitCoupling1ElKernel(idx, q, sp))):
                     want = r.one_electron_class_ex(use_symm, i, op, charges=q, omegas=w, origin=o)
                     assert np.abs(got - want.reshape(got.shape)).max() <= 1e-12 * max(1.0, np.abs(want).max()), \
                         (use_symm, i, op)
     # a single pair returns the three blocks
     sp = L.shellPairData(True, cases[0][0])[0]
     assert len(L.momentumKernel(0, sp)) == 3
+
+
+def test_charge_kernels_golden_co2():
+    """The reference's kernel-API golden sums for the attenuated and per-charge Coulomb kernels
+    (test/tests_ints.cpp:414-596; CO2 6-31+G), summed in class / pair / charge / component / element
+    order as the reference's loops do."""
+    co2 = L.Structure("6-31+g", CO2_Z, CO2_ANG)
+    q = np.array([[x / 0.5291772083 for x in c] + [z] for c, z in zip(CO2_ANG, CO2_Z)])
+    assert golden(seqsum(_kernel_blocks(co2, False, L.externalChargesErfKernel, q, [1.2, -10.5, 0.031])),
+                  419.197077258844)
+    assert golden(seqsum(_kernel_blocks(co2, True, L.externalChargesOperatorD1Kernel, q)), 1067.752096834267)
+    assert golden(seqsum(_kernel_blocks(co2, True, L.potentialAtExternalChargesKernel, q)), 1357.142718060126)
+    q4 = np.array([[0.0, -0.025, 0.05, 1.0], [1.0, -0.025, 0.05, -1.0], [-1.0, 0.5, 0.6, 0.25],
+                   [0.0, -0.5, 0.24, -0.3]])
+    assert golden(seqsum(_kernel_blocks(co2, True, L.potentialAtExternalChargesErfKernel, q4,
+                                        [0.1, -0.5, 0.61, 0.000015])), 66.950210612294)
+
+
+def test_charge_kernels_vs_reference_elementwise():
+    """externalChargesErfD1Kernel, externalChargesOperator(Erf)D1Kernel and
+    potentialAtExternalCharges(Erf)Kernel for every class with and without symmetry against the
+    reference's kernels (cc-pVTZ water dimer, f shells; three charges with range parameters)."""
+    q = np.array([[1.0, -2.0, 0.5, 0.7], [-3.0, 1.0, -6.0, -1.2], [6.0, 2.0, -7.0, 2.0]])
+    w = np.array([0.4, -2.5, 11.0])
+    Z, xyz, _ = water_cluster(2, 7)
+    s, r = L.Structure("cc-pvtz", Z, xyz, units="bohr"), R.RefStructure("cc-pvtz", Z, xyz)
+    for use_symm in (True, False):
+        for i, sp in enumerate(L.shellPairData(use_symm, s)):
+            if not sp.n_pairs_:
+                continue
+            idx = list(range(sp.n_pairs_))
+            for op, got in ((10, L.externalChargesErfD1Kernel(idx, q, w, sp)),
+                            (11, L.externalChargesOperatorD1Kernel(idx, q, sp)),
+                            (12, L.externalChargesOperatorErfD1Kernel(idx, q, w, sp)),
+                            (13, L.potentialAtExternalChargesKernel(idx, q, sp)),
+                            (14, L.potentialAtExternalChargesErfKernel(idx, q, w, sp))):
+                want = r.one_electron_class_ex(use_symm, i, op, charges=q, omegas=w)
+                got = np.asarray(got)
+                assert np.abs(got.reshape(want.shape) - want).max() <= 1e-12 * max(1.0, np.abs(want).max()), \
+                    (use_symm, i, op)
