@@ -305,7 +305,8 @@ int lible_gpu_one_electron_batch(lible_gpu_ctx *ctx, int use_symm, int class_ab,
  * part), op 11 / 12 the operator part d/dC_xyz of externalChargesKernel / externalChargesErfKernel
  * summed over the given charges ([3][S_a][S_b]; one charge per call gives the reference's
  * externalChargesOperator(Erf)D1Kernel entry for that charge), op 13 spinOrbitCoupling1ElKernel
- * ([3][S_a][S_b], the given charges; ints.hpp:135-137, oneelints.cpp:1209-1316).  `omegas`: one range parameter per
+ * ([3][S_a][S_b], the given charges; ints.hpp:135-137, oneelints.cpp:1209-1316), op 14 pVpKernel
+ * ([3][3][S_a][S_b] = <d_i a| V |d_j b> for the given charges; ints.hpp:159-161; see pVpIntegrals).  `omegas`: one range parameter per
  * charge for 9, 10, 12 (NULL charges = the nuclei, one omega per atom; 9 scales a charge by
  * w / sqrt(w^2 + p), 10 and 12 by sqrt(w^2 / (w^2 + p)), as the reference's kernels do) (ints.hpp:66-148;
  * oneelints.cpp:379-473, 587-680, 791-889, 1513-1577, 1617-1701, 1844-2060).  Unused pointers may be
@@ -320,11 +321,17 @@ int lible_gpu_one_electron_batch_ex(lible_gpu_ctx *ctx, int use_symm, int class_
  *   angularMomentum (ints.hpp:146-147): -<m| (r - origin) x d/dr |n>, antisymmetric;
  *   nuclearAttractionErf (ints.hpp:52): the nuclei's erf(w r)/r attraction, `omegas` one per atom;
  *   externalChargesErf (ints.hpp:60-62): the same for point charges [n][4], one omega each;
- *   spinOrbitCoupling1El (ints.hpp:131): the one-electron SOC integrals of the nuclei, antisymmetric. */
+ *   spinOrbitCoupling1El (ints.hpp:131): the one-electron SOC integrals of the nuclei, antisymmetric;
+ *   pVpIntegrals (ints.hpp:154): out [3][3][nao][nao], <d_i m| V |d_j n> for the nuclei (charges
+ *     NULL) or the point charges [n][4], with out[i][j] = out[j][i]^T.  These are the integrals themselves: the reference's pVpKernel leaves
+ *     out the E factor of its first term and the R factor of its last and builds its x second-
+ *     derivative coefficients from the y first derivatives (oneelints.cpp:1392-1460, ecoeffs.cpp:
+ *     205), and its driver mirrors each component without exchanging i and j, so its values differ. */
 int lible_gpu_dipole_moment(lible_gpu_ctx *ctx, const double *origin, double *out);
 int lible_gpu_momentum(lible_gpu_ctx *ctx, double *out);
 int lible_gpu_angular_momentum(lible_gpu_ctx *ctx, const double *origin, double *out);
 int lible_gpu_spin_orbit_coupling_1el(lible_gpu_ctx *ctx, double *out);
+int lible_gpu_pvp_integrals(lible_gpu_ctx *ctx, const double *charges, int n_charges, double *out);
 int lible_gpu_nuclear_attraction_erf(lible_gpu_ctx *ctx, const double *omegas, double *out);
 int lible_gpu_external_charges_erf(lible_gpu_ctx *ctx, const double *charges, const double *omegas, int n_charges,
                                    double *out);

@@ -17,7 +17,7 @@
  *   ERI3D1Kernel, ERI2D1Kernel (operator())                 src/lible/ints/twoel/eri_kernels.hpp:60-169
  *   overlap, kineticEnergy, nuclearAttraction, nuclearAttractionErf, externalCharges,
  *   externalChargesErf, dipoleMoment, momentum, angularMomentum,
- *   spinOrbitCoupling1El                                     src/lible/ints/ints.hpp:29-151
+ *   spinOrbitCoupling1El, pVpIntegrals                       src/lible/ints/ints.hpp:29-154
  * Failures throw std::runtime_error with the library's message, as the reference throws
  * std::runtime_error for its own error cases.  jk(), jkEnergy() and jkEnergyGradient() have no
  * reference counterpart.
@@ -359,6 +359,28 @@ namespace lible::ints::gpu
     {
         Context c(structure, device);
         return spinOrbitCoupling1El(c);
+    }
+    // <d_i m| V |d_j n> for the nuclei, [i][j]; the integrals themselves, where the reference's
+    // pVpIntegrals differs (lible_b200.h, lible_gpu_pvp_integrals).
+    inline arr2d<vec2d, 3, 3> pVpIntegrals(Context &c)
+    {
+        const std::size_t n = c.dimAO();
+        std::vector<double> flat(9 * n * n);
+        c.check(lible_gpu_pvp_integrals(c.get(), nullptr, 0, flat.data()));
+        arr2d<vec2d, 3, 3> out;
+        for (int i = 0; i < 3; i++)
+            for (int j = 0; j < 3; j++)
+            {
+                out[i][j] = vec2d(n, n);
+                std::copy(flat.begin() + (std::ptrdiff_t)((3 * i + j) * n * n),
+                          flat.begin() + (std::ptrdiff_t)((3 * i + j + 1) * n * n), out[i][j].memptr());
+            }
+        return out;
+    }
+    inline arr2d<vec2d, 3, 3> pVpIntegrals(const Structure &structure, int device = 0)
+    {
+        Context c(structure, device);
+        return pVpIntegrals(c);
     }
 
     // ---- kernel functors (eri_kernels.hpp:60-169) -------------------------------------------------

@@ -101,6 +101,7 @@ SIGNATURES = {
     "lible_gpu_angular_momentum": [P, P, P],
     "lible_gpu_nuclear_attraction_erf": [P, P, P],
     "lible_gpu_spin_orbit_coupling_1el": [P, P],
+    "lible_gpu_pvp_integrals": [P, P, I, P],
     "lible_gpu_external_charges_erf": [P, P, P, I, P],
     "lible_gpu_one_electron_grad": [P, P, P, P],
     "lible_host_spherical_trafo": [I, P, P, P, P],

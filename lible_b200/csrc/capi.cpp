@@ -1052,12 +1052,12 @@ int lible_gpu_one_electron_batch_ex(lible_gpu_ctx *ctx, int use_symm, int class_
     return guard(ctx, [&](Engine &e) {
         if (n < 0 || (n > 0 && (!pairs || !out)) || (charges && n_charges < 0))
             throw EngineError(kStatusInvalid, "bad one-electron batch arguments");
-        if (op < 0 || op > 13)
+        if (op < 0 || op > 14)
             throw EngineError(kStatusInvalid, "bad one-electron operator");
         const auto cls = e.pairClasses(use_symm != 0);
         if (class_ab < 0 || class_ab >= (int)cls.size())
             throw EngineError(kStatusInvalid, "bad class index");
-        const int nblk = ((op >= 3 && op <= 5) || op == 10) ? 6 : ((op >= 6 && op <= 8) || op >= 11) ? 3 : 1;
+        const int nblk = op == 14 ? 9 : ((op >= 3 && op <= 5) || op == 10) ? 6 : ((op >= 6 && op <= 8) || op >= 11) ? 3 : 1;
         const size_t blk = (size_t)(2 * cls[class_ab].la + 1) * (2 * cls[class_ab].lb + 1) * nblk;
         DevArray o(out, (size_t)n * blk, false, e.stream());
         e.oneElectronBatch(use_symm != 0, class_ab, op, n, pairs, charges, charges ? n_charges : 0, o.ptr, omegas,
@@ -1084,7 +1084,7 @@ namespace
             if (!out || (charges && n_charges < 0))
                 throw EngineError(kStatusInvalid, "bad one-electron operator arguments");
             const size_t n = e.nao();
-            const int nblk = op == 9 ? 1 : 3;
+            const int nblk = op == 9 ? 1 : op == 14 ? 9 : 3;
             DevArray o(out, (size_t)nblk * n * n, false, e.stream());
             e.oneElectronOperator(op, charges, charges ? n_charges : 0, omegas, origin, o.ptr);
             o.copyOut();
@@ -1105,6 +1105,11 @@ int lible_gpu_momentum(lible_gpu_ctx *ctx, double *out)
 int lible_gpu_angular_momentum(lible_gpu_ctx *ctx, const double *origin, double *out)
 {
     return oneElectronOperator(ctx, 8, nullptr, nullptr, 0, origin, out);
+}
+
+int lible_gpu_pvp_integrals(lible_gpu_ctx *ctx, const double *charges, int n_charges, double *out)
+{
+    return oneElectronOperator(ctx, 14, charges, nullptr, charges ? n_charges : 0, nullptr, out);
 }
 
 int lible_gpu_spin_orbit_coupling_1el(lible_gpu_ctx *ctx, double *out)

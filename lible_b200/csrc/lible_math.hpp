@@ -173,4 +173,46 @@ namespace lible_b200
                     at(i, j, t) = v;
                 }
     }
+
+    // Second derivative of the Hermite coefficients with respect to the same axis' A - B, from the
+    // first (E1, hermiteE1) and the plain ones (E): differentiating the hermiteE1 recurrences once
+    // more gives
+    //   E2[0][0][0] = -2 (ab/p) (R E1[0][0][0] + E[0][0][0]),
+    //   E2[i][0][t] = -(b/p) (R E2[i-1][0][t] + 2 E1[i-1][0][t]) + E2[i-1][0][t-1] / 2p + (t+1) E2[i-1][0][t+1],
+    //   E2[i][j][t] =  (a/p) (R E2[i][j-1][t] + 2 E1[i][j-1][t]) + E2[i][j-1][t-1] / 2p + (t+1) E2[i][j-1][t+1]
+    // (the reference's ecoeffsRecurrence2_n2, src/lible/ints/ecoeffs.cpp:113-160).  Same layout as E.
+    LB_HD void hermiteE2(int la, int lb, double a, double b, double rab, const double *E, const double *E1,
+                         double *E2)
+    {
+        const double p = a + b;
+        const double one_o_2p = 0.5 / p;
+        const int nt = la + lb + 1;
+        for (int x = 0; x < (la + 1) * (lb + 1) * nt; x++)
+            E2[x] = 0.0;
+        auto e0 = [&](int i, int j, int t) -> double { return E[(i * (lb + 1) + j) * nt + t]; };
+        auto e1 = [&](int i, int j, int t) -> double { return E1[(i * (lb + 1) + j) * nt + t]; };
+        auto at = [&](int i, int j, int t) -> double & { return E2[(i * (lb + 1) + j) * nt + t]; };
+        at(0, 0, 0) = -2.0 * (a * b / p) * (rab * e1(0, 0, 0) + e0(0, 0, 0));
+        for (int i = 1; i <= la; i++)
+            for (int t = 0; t <= i; t++)
+            {
+                double v = -(b / p) * (rab * at(i - 1, 0, t) + 2.0 * e1(i - 1, 0, t));
+                if (t > 0)
+                    v += one_o_2p * at(i - 1, 0, t - 1);
+                if (t + 1 <= i - 1)
+                    v += (t + 1) * at(i - 1, 0, t + 1);
+                at(i, 0, t) = v;
+            }
+        for (int j = 1; j <= lb; j++)
+            for (int i = 0; i <= la; i++)
+                for (int t = 0; t <= i + j; t++)
+                {
+                    double v = (a / p) * (rab * at(i, j - 1, t) + 2.0 * e1(i, j - 1, t));
+                    if (t > 0)
+                        v += one_o_2p * at(i, j - 1, t - 1);
+                    if (t + 1 <= i + j - 1)
+                        v += (t + 1) * at(i, j - 1, t + 1);
+                    at(i, j, t) = v;
+                }
+    }
 }

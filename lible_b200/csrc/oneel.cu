@@ -254,10 +254,12 @@ namespace lible_b200
             kOpVOpD1 = 11,    // externalChargesOperatorD1Kernel for the charges summed: d/dC_xyz, [3]
             kOpVErfOpD1 = 12, // the same, erf-attenuated
             kOpSOC = 13,      // spinOrbitCoupling1ElKernel, [3]
+            kOpPVP = 14,      // pVpKernel, [3][3] (pvpPairKernel)
         };
         __host__ __device__ constexpr int oneOpBlocks(int op)
         {
-            return ((op >= kOpSD1 && op <= kOpVD1) || op == kOpVErfD1)                   ? 6
+            return op == kOpPVP                                                              ? 9
+                   : ((op >= kOpSD1 && op <= kOpVD1) || op == kOpVErfD1)                   ? 6
                    : ((op >= kOpDipole && op <= kOpAngular) || op >= kOpVOpD1) ? 3
                                                                                           : 1;
         }
@@ -699,6 +701,208 @@ namespace lible_b200
             }
         }
 
+        // pVp integrals of one pair, [3][3][S_a][S_b]: <d_i a| V |d_j b> for the point charges, the
+        // quantity of the reference's pVpKernel (src/lible/ints/oneelints.cpp:1318-1475).  With
+        // d/dA = (a/p) d/dP + d/dR and d/dB = (b/p) d/dP - d/dR applied to the Hermite expansion
+        // -f sum_tuv E_tuv(R) R_tuv(P - C) of the attraction (R = A - B, f = 2 pi / p d_a d_b):
+        //   pVp_ij = -f sum_tuv ( (ab/p^2) E R_{+e_i+e_j} - (a/p) E1_j R_{+e_i} + (b/p) E1_i R_{+e_j}
+        //                         - E2_ij R_tuv ),
+        // E1_j: the j-axis table replaced by its first derivative (hermiteE1), E2_ij: both first
+        // derivatives (i != j) or the i-axis second derivative (hermiteE2, i = j), R to order L + 2.
+        // The reference's kernel leaves out the E factor of its first term and the R factor of its
+        // last, and forms the x second-derivative table from the y first derivatives
+        // (oneelints.cpp:1392-1460, ecoeffs.cpp:205); this kernel follows the derivation, which the
+        // tests check against central finite differences of the point-charge integrals.  One warp
+        // per pair, as onePairKernel.
+        template <int LA, int LB>
+        struct PvpShape
+        {
+            static constexpr int L = LA + LB, L2 = L + 2;
+            static constexpr int NCA = (LA + 1) * (LA + 2) / 2, NCB = (LB + 1) * (LB + 2) / 2;
+            static constexpr int NC = NCA * NCB;
+            static constexpr int PER_LANE = (NC + 31) / 32;
+            static constexpr int NT = L + 1;
+            static constexpr int EAX = (LA + 1) * (LB + 1) * NT;
+            static constexpr int NR2 = (L2 + 1) * (L2 + 2) * (L2 + 3) / 6;
+            static constexpr int SA = 2 * LA + 1, SB = 2 * LB + 1;
+            static constexpr int WARP_DOUBLES = 9 * EAX + NR2 + 9 * NC;  // E, E1, E2; R; 9 blocks
+        };
+
+        template <int LA, int LB>
+        __global__ void __launch_bounds__(128) pvpPairKernel(OnePairArgs a)
+        {
+            using S = PvpShape<LA, LB>;
+            constexpr int L2 = S::L2, NT = S::NT, NB = LB + 1;
+            extern __shared__ __align__(16) double smem3[];
+            const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+            double *E = smem3 + (size_t)warp * S::WARP_DOUBLES;  // [table][axis][i][j][t]
+            double *Rs = E + 9 * S::EAX;
+            double *blk = Rs + S::NR2;
+            const long long task = (long long)blockIdx.x * (blockDim.x >> 5) + warp;
+            if (task >= a.n_tasks)
+                return;
+            const int ipair = a.list ? (int)a.list[task] : (int)task;
+            auto ex = [&](int tab, int axis, int i, int j, int t) {
+                return E[(tab * 3 + axis) * S::EAX + (i * NB + j) * NT + t];
+            };
+            const double *nA = a.norms_a + (size_t)ipair * S::SA, *nB = a.norms_b + (size_t)ipair * S::SB;
+            double acc[9][S::PER_LANE];
+#pragma unroll
+            for (int d = 0; d < 9; d++)
+#pragma unroll
+                for (int w = 0; w < S::PER_LANE; w++)
+                    acc[d][w] = 0.0;
+            const double *A = a.coords + 6 * (size_t)ipair, *B = A + 3;
+            for (uint32_t pp = a.pofs[ipair]; pp < a.pofs[ipair + 1]; pp++)
+            {
+                const double ea = a.exps[2 * pp], eb = a.exps[2 * pp + 1];
+                const double dadb = a.coeffs[2 * pp] * a.coeffs[2 * pp + 1];
+                const double p = ea + eb, mu = ea * eb / p;
+                double P[3];
+#pragma unroll
+                for (int k = 0; k < 3; k++)
+                    P[k] = (ea * A[k] + eb * B[k]) / p;
+                if (lane < 3)
+                {
+                    const double d = A[lane] - B[lane];
+                    double *e0 = E + lane * S::EAX, *e1 = E + (3 + lane) * S::EAX, *e2 = E + (6 + lane) * S::EAX;
+                    hermiteE(LA, LB, 0.5 / p, P[lane] - A[lane], P[lane] - B[lane], exp(-mu * d * d), e0);
+                    hermiteE1(LA, LB, ea, eb, d, e0, e1);
+                    hermiteE2(LA, LB, ea, eb, d, e0, e1, e2);
+                }
+                double r[S::NR2];
+#pragma unroll
+                for (int h = 0; h < S::NR2; h++)
+                    r[h] = 0.0;
+                for (int c = lane; c < a.n_charges; c += 32)
+                {
+                    const double *q = a.charges + 4 * (size_t)c;
+                    const double X = P[0] - q[0], Y = P[1] - q[1], Z = P[2] - q[2];
+                    double F[L2 + 1], R[S::NR2];
+                    boysF<L2, false>(p * (X * X + Y * Y + Z * Z), a.boys + (size_t)L2 * kBoysTerms * kBoysPitch, F);
+#pragma unroll
+                    for (int k = 0; k <= L2; k++)
+                        F[k] *= q[3];
+                    hermiteR<L2, double>(-2.0 * p, F, X, Y, Z, R);
+#pragma unroll
+                    for (int h = 0; h < S::NR2; h++)
+                        r[h] += R[h];
+                }
+#pragma unroll
+                for (int h = 0; h < S::NR2; h++)
+                {
+                    double v = r[h];
+#pragma unroll
+                    for (int o = 16; o > 0; o >>= 1)
+                        v += __shfl_xor_sync(0xffffffffu, v, o);
+                    if (lane == 0)
+                        Rs[h] = v;
+                }
+                __syncwarp();
+                const double fv = 2.0 * 3.14159265358979323846 / p * dadb;
+                const double cpp = ea * eb / (p * p), ca = ea / p, cb = eb / p;
+#pragma unroll
+                for (int w = 0; w < S::PER_LANE; w++)
+                {
+                    const int e = lane + 32 * w;
+                    if (e >= S::NC)
+                        break;
+                    int ijk[3], ijk_[3];
+                    cartExps(LA, e / S::NCB, ijk[0], ijk[1], ijk[2]);
+                    cartExps(LB, e % S::NCB, ijk_[0], ijk_[1], ijk_[2]);
+                    double s[9];
+#pragma unroll
+                    for (int d = 0; d < 9; d++)
+                        s[d] = 0.0;
+                    for (int t = 0; t <= ijk[0] + ijk_[0]; t++)
+                        for (int u = 0; u <= ijk[1] + ijk_[1]; u++)
+                            for (int v = 0; v <= ijk[2] + ijk_[2]; v++)
+                            {
+                                const int tuv[3] = {t, u, v};
+                                double g0[3], g1[3], g2[3];
+#pragma unroll
+                                for (int x = 0; x < 3; x++)
+                                {
+                                    g0[x] = ex(0, x, ijk[x], ijk_[x], tuv[x]);
+                                    g1[x] = ex(1, x, ijk[x], ijk_[x], tuv[x]);
+                                    g2[x] = ex(2, x, ijk[x], ijk_[x], tuv[x]);
+                                }
+                                const double e000 = g0[0] * g0[1] * g0[2];
+                                // E products with the first derivative on one axis, and on two / twice
+                                const double e1x[3] = {g1[0] * g0[1] * g0[2], g0[0] * g1[1] * g0[2], g0[0] * g0[1] * g1[2]};
+                                const double r0 = Rs[hermIndex(t, u, v)];
+                                double r1[3];
+#pragma unroll
+                                for (int x = 0; x < 3; x++)
+                                    r1[x] = Rs[hermIndex(t + (x == 0), u + (x == 1), v + (x == 2))];
+#pragma unroll
+                                for (int i = 0; i < 3; i++)
+#pragma unroll
+                                    for (int j = 0; j < 3; j++)
+                                    {
+                                        const double r2 = Rs[hermIndex(t + (i == 0) + (j == 0), u + (i == 1) + (j == 1),
+                                                                       v + (i == 2) + (j == 2))];
+                                        double rr;
+                                        if (i == j)
+                                            rr = (i == 0 ? g2[0] * g0[1] * g0[2]
+                                                  : i == 1 ? g0[0] * g2[1] * g0[2] : g0[0] * g0[1] * g2[2]);
+                                        else
+                                        {
+                                            const int k = 3 - i - j;
+                                            rr = g1[i] * g1[j] * g0[k];
+                                        }
+                                        s[3 * i + j] += cpp * r2 * e000 - ca * r1[i] * e1x[j] + cb * r1[j] * e1x[i] - rr * r0;
+                                    }
+                            }
+#pragma unroll
+                    for (int d = 0; d < 9; d++)
+                        acc[d][w] -= fv * s[d];
+                }
+                __syncwarp();
+            }
+            // spherical transform and norms; a swapped class is written in the caller's orientation:
+            // blocks transposed and components (i, j) -> (j, i)
+#pragma unroll
+            for (int d = 0; d < 9; d++)
+#pragma unroll
+                for (int w = 0; w < S::PER_LANE; w++)
+                {
+                    const int e = lane + 32 * w;
+                    if (e < S::NC)
+                        blk[d * S::NC + e] = acc[d][w];
+                }
+            __syncwarp();
+            double *out = a.out + (size_t)task * 9 * S::SA * S::SB;
+            for (int o = lane; o < 9 * S::SA * S::SB; o += 32)
+            {
+                const int d = o / (S::SA * S::SB), m = (o / S::SB) % S::SA, nn = o % S::SB;
+                const int dst = a.swap ? (((d % 3) * 3 + d / 3) * S::SA * S::SB + nn * S::SA + m) : o;
+                double sum = 0.0;
+                for (int ta = a.sph_ofs_a0; ta < a.sph_ofs_a1; ta++)
+                {
+                    if (a.sph_rc[2 * ta] != m)
+                        continue;
+                    const int ca2 = a.sph_rc[2 * ta + 1];
+                    for (int tb = a.sph_ofs_b0; tb < a.sph_ofs_b1; tb++)
+                        if (a.sph_rc[2 * tb] == nn)
+                            sum += a.sph_val[ta] * a.sph_val[tb] * blk[d * S::NC + ca2 * S::NCB + a.sph_rc[2 * tb + 1]];
+                }
+                out[dst] = nA[m] * nB[nn] * sum;
+            }
+        }
+
+        template <int LA, int LB>
+        void launchPvp(const OnePairArgs &a, cudaStream_t s, bool)
+        {
+            constexpr int warps = 4;
+            const size_t smem = sizeof(double) * warps * PvpShape<LA, LB>::WARP_DOUBLES;
+            auto k = pvpPairKernel<LA, LB>;
+            if (smem > 48 * 1024)
+                cudaCheck(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "attr");
+            k<<<(unsigned)((a.n_tasks + warps - 1) / warps), 32 * warps, smem, s>>>(a);
+            cudaCheck(cudaGetLastError(), "pVp pair kernel");
+        }
+
         using PairFn = void (*)(const OnePairArgs &, cudaStream_t, bool);
         template <int LA, int LB>
         void launchPair(const OnePairArgs &a, cudaStream_t s, bool grad)
@@ -710,6 +914,17 @@ namespace lible_b200
                 cudaCheck(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "attr");
             k<<<(unsigned)((a.n_tasks + warps - 1) / warps), 32 * warps, smem, s>>>(a);
             cudaCheck(cudaGetLastError(), "one-electron pair kernel");
+        }
+
+        PairFn lookupPvp(int la, int lb)
+        {
+            static const PairFn table[4][4] = {
+                {&launchPvp<0, 0>, &launchPvp<0, 1>, &launchPvp<0, 2>, &launchPvp<0, 3>},
+                {&launchPvp<1, 0>, &launchPvp<1, 1>, &launchPvp<1, 2>, &launchPvp<1, 3>},
+                {&launchPvp<2, 0>, &launchPvp<2, 1>, &launchPvp<2, 2>, &launchPvp<2, 3>},
+                {&launchPvp<3, 0>, &launchPvp<3, 1>, &launchPvp<3, 2>, &launchPvp<3, 3>},
+            };
+            return (la < 4 && lb < 4) ? table[la][lb] : nullptr;
         }
 
         PairFn lookupPair(int la, int lb)
@@ -806,10 +1021,11 @@ namespace lible_b200
 
     namespace
     {
-        // M[d][a][b] = blk, M[d][b][a] = sign * blk for every stored pair block [pair][d][S_a][S_b].
+        // M[d][a][b] = blk, M[d'][b][a] = sign * blk for every stored pair block [pair][d][S_a][S_b];
+        // d' = d, or the component (j, i) of d = (i, j) for the nine pVp blocks (comp_t).
         __global__ void scatterPairBlocks(const double *__restrict__ blocks, long long n_pairs, int nblk, int sa,
                                           int sb, const int32_t *__restrict__ ao, long long nao, double sign,
-                                          double *__restrict__ M)
+                                          int comp_t, double *__restrict__ M)
         {
             const long long per = (long long)nblk * sa * sb, total = n_pairs * per;
             for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; g < total;
@@ -819,8 +1035,9 @@ namespace lible_b200
                 const int o = (int)(g % per), d = o / (sa * sb), m = (o / sb) % sa, nn = o % sb;
                 const long long r = ao[2 * ip] + m, c = ao[2 * ip + 1] + nn;
                 const double v = blocks[g];
+                const int dt = comp_t ? (d % 3) * 3 + d / 3 : d;
                 M[((size_t)d * nao + r) * nao + c] = v;
-                M[((size_t)d * nao + c) * nao + r] = sign * v;
+                M[((size_t)dt * nao + c) * nao + r] = sign * v;
             }
         }
 
@@ -849,9 +1066,28 @@ namespace lible_b200
             }
         }
 
+        // pVp: M[(i,j)][r][c] and M[(j,i)][c][r] made equal (their mean), one unordered pair per thread.
+        __global__ void symmetrizePvp(double *M, long long nao)
+        {
+            const long long total = 9 * nao * nao;
+            for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; g < total;
+                 g += (long long)gridDim.x * blockDim.x)
+            {
+                const int d = (int)(g / (nao * nao));
+                const long long r = (g / nao) % nao, c = g % nao;
+                const int pd = (d % 3) * 3 + d / 3;
+                if (pd < d || (pd == d && c <= r))
+                    continue;
+                double *x = M + ((size_t)d * nao + r) * nao + c, *y = M + ((size_t)pd * nao + c) * nao + r;
+                const double m = 0.5 * (*x + *y);
+                *x = m;
+                *y = m;
+            }
+        }
+
         void checkOneOp(int op, const double *omegas_host, const double *origin)
         {
-            if (op < 0 || op > kOpSOC)
+            if (op < 0 || op > kOpPVP)
                 throw EngineError(kStatusInvalid, "bad one-electron operator");
             if (oneOpUsesOmegas(op) && !omegas_host)
                 throw EngineError(kStatusInvalid, "the erf-attenuated operator needs one omega per charge");
@@ -864,8 +1100,8 @@ namespace lible_b200
                                      const double *origin, double *out_dev)
     {
         requireSingle();
-        if (op < kOpDipole || (op > kOpVErf && op != kOpSOC))
-            throw EngineError(kStatusInvalid, "the whole-matrix operator form covers ops 6..9 and 13");
+        if (op < kOpDipole || (op > kOpVErf && op != kOpSOC && op != kOpPVP))
+            throw EngineError(kStatusInvalid, "the whole-matrix operator form covers ops 6..9, 13 and 14");
         checkOneOp(op, omegas_host, origin);
         if (max_l_ > 3)
             throw EngineError(kStatusUnsupported, "one-electron kernels are instantiated for l <= 3");
@@ -887,7 +1123,7 @@ namespace lible_b200
             const PairClass &pc = cs.host[c];
             if (pc.n_pairs == 0)
                 continue;
-            const PairFn fn = lookupPair(pc.la, pc.lb);
+            const PairFn fn = op == kOpPVP ? lookupPvp(pc.la, pc.lb) : lookupPair(pc.la, pc.lb);
             if (!fn)
                 throw EngineError(kStatusUnsupported, "one-electron kernels are instantiated for l <= 3");
             OneClassData d(pc, stream_);
@@ -926,13 +1162,17 @@ namespace lible_b200
             fn(a, stream_, false);
             const long long total = (long long)pc.n_pairs * nblk * sa * sb;
             scatterPairBlocks<<<(unsigned)std::min<long long>((total + 255) / 256, 148LL * 16), 256, 0, stream_>>>(
-                blocks.p, (long long)pc.n_pairs, nblk, sa, sb, d.ao.p, (long long)n, sign, out_dev);
+                blocks.p, (long long)pc.n_pairs, nblk, sa, sb, d.ao.p, (long long)n, sign, op == kOpPVP ? 1 : 0,
+                out_dev);
             cudaCheck(cudaGetLastError(), "scatter");
             cudaCheck(cudaStreamSynchronize(stream_), "one-electron operator");
         }
         const long long total = (long long)nblk * (long long)n * (long long)n;
-        symmetrizeBlocks<<<(unsigned)std::min<long long>((total + 255) / 256, 148LL * 16), 256, 0, stream_>>>(
-            out_dev, (long long)n, nblk, sign);
+        const unsigned grid = (unsigned)std::min<long long>((total + 255) / 256, 148LL * 16);
+        if (op == kOpPVP)
+            symmetrizePvp<<<grid, 256, 0, stream_>>>(out_dev, (long long)n);
+        else
+            symmetrizeBlocks<<<grid, 256, 0, stream_>>>(out_dev, (long long)n, nblk, sign);
         cudaCheck(cudaGetLastError(), "symmetrize");
         cudaCheck(cudaStreamSynchronize(stream_), "one-electron operator");
     }
@@ -947,7 +1187,7 @@ namespace lible_b200
             throw EngineError(kStatusInvalid, "bad class index");
         checkOneOp(op, omegas_host, origin);
         const PairClass &pc = cs.host[cls];
-        const PairFn fn = lookupPair(pc.la, pc.lb);
+        const PairFn fn = op == kOpPVP ? lookupPvp(pc.la, pc.lb) : lookupPair(pc.la, pc.lb);
         if (!fn)
             throw EngineError(kStatusUnsupported, "one-electron kernels are instantiated for l <= 3");
         if (n_tasks <= 0)

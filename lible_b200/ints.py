@@ -526,7 +526,7 @@ def _one_batch(op, ipair, sp, charges=None, omegas=None, origin=None):
     array)."""
     single = np.ndim(ipair) == 0
     idx = np.ascontiguousarray(np.atleast_1d(np.asarray(ipair, dtype=np.uint32)))
-    nb = 6 if (3 <= op <= 5 or op == 10) else 3 if (6 <= op <= 8 or op >= 11) else 1
+    nb = 9 if op == 14 else 6 if (3 <= op <= 5 or op == 10) else 3 if (6 <= op <= 8 or op >= 11) else 1
     out = np.empty((len(idx), nb, _nsph(sp.la_), _nsph(sp.lb_)))
     if charges is None:
         q, nq = None, 0
@@ -662,6 +662,30 @@ def momentum(structure):
 def angularMomentum(origin, structure):
     """lible::ints::angularMomentum (ints.hpp:146-147): [3][nao][nao], antisymmetric."""
     return _one_operator(structure, "lible_gpu_angular_momentum", 3, _ptr(_f64(origin)))
+
+
+def pVpKernel(ipair, charges, sp_data):
+    """lible::ints::pVpKernel (ints.hpp:159-161): <d_i a| V |d_j b> for the point charges
+    [x, y, z, q], as [3][3] blocks (an index) or an array [n][3][3][S_a][S_b] (a sequence).  The
+    integrals themselves; the reference's kernel differs (include/lible_b200.h, pVpIntegrals)."""
+    single = np.ndim(ipair) == 0
+    out = np.asarray(_one_batch(14, np.atleast_1d(ipair), sp_data, charges))
+    out = out.reshape(out.shape[0], 3, 3, out.shape[-2], out.shape[-1])
+    if single:
+        return [[out[0, i, j] for j in range(3)] for i in range(3)]
+    return out
+
+
+def pVpIntegrals(structure, point_charges=None):
+    """lible::ints::pVpIntegrals (ints.hpp:154): [3][3][nao][nao] of <d_i m| V |d_j n> for the
+    nuclei (or the given point charges [n][4], bohr), out[i][j] = out[j][i]^T."""
+    n = structure.nao
+    if point_charges is None:
+        q, nq = None, 0
+    else:
+        q = _f64(point_charges).reshape(-1, 4)
+        nq = len(q)
+    return _one_operator(structure, "lible_gpu_pvp_integrals", 9, _ptr(q), nq).reshape(3, 3, n, n)
 
 
 def spinOrbitCoupling1El(structure):

@@ -174,7 +174,7 @@ class RefStructure:
         la, lb, na, _ = self.pair_classes(use_symm)[iab]
         q = np.ascontiguousarray(charges if charges is not None else np.zeros((0, 4)), dtype=np.float64)
         nq = len(q)
-        nb = 1 if op == 9 else 6 if op == 10 else 3 * nq if op in (11, 12) else nq if op in (13, 14) else 3
+        nb = 1 if op == 9 else 6 if op == 10 else 9 if op == 16 else 3 * nq if op in (11, 12) else nq if op in (13, 14) else 3
         out = np.empty((na, nb, 2 * la + 1, 2 * lb + 1))
         w = None if omegas is None else np.ascontiguousarray(omegas, dtype=np.float64)
         o = None if origin is None else np.ascontiguousarray(origin, dtype=np.float64)

@@ -369,7 +369,8 @@ int ref_one_electron(void *h, int which, const double *charges, int n_charges, d
 // 10 externalChargesErfD1Kernel ([n_pairs][6][Sa Sb]), 11 externalChargesOperatorD1Kernel and
 // 12 externalChargesOperatorErfD1Kernel ([n_pairs][n_charges][3][Sa Sb]), 13
 // potentialAtExternalChargesKernel and 14 potentialAtExternalChargesErfKernel
-// ([n_pairs][n_charges][Sa Sb]), 15 spinOrbitCoupling1ElKernel ([n_pairs][3][Sa Sb]) (oneelints.cpp:
+// ([n_pairs][n_charges][Sa Sb]), 15 spinOrbitCoupling1ElKernel ([n_pairs][3][Sa Sb]), 16 pVpKernel
+// ([n_pairs][9][Sa Sb]) (oneelints.cpp:
 // 379-473, 587-680, 791-1086, 1209-1316, 1513-1577, 1617-1701, 1844-2060).
 int ref_one_electron_class_ex(void *h, int use_symm, int iab, int op, const double *charges, const double *omegas,
                               int n_charges, const double *origin, double *out)
@@ -385,10 +386,15 @@ int ref_one_electron_class_ex(void *h, int use_symm, int iab, int op, const doub
         const std::array<double, 3> o = origin ? std::array<double, 3>{origin[0], origin[1], origin[2]}
                                                : std::array<double, 3>{0, 0, 0};
         const bool d1 = op == 10 || op == 11 || op == 12 || op == 15;
-        lints::BoysGrid grid(ab.la_ + ab.lb_ + (d1 ? 1 : 0));
+        lints::BoysGrid grid(ab.la_ + ab.lb_ + (op == 16 ? 2 : d1 ? 1 : 0));
         const size_t blk = lints::numSphericals(ab.la_) * lints::numSphericals(ab.lb_);
         const size_t nq = (size_t)n_charges;
-        const size_t nb = op == 9 ? 1 : op == 10 ? 6 : (op == 11 || op == 12) ? 3 * nq : (op == 13 || op == 14) ? nq : 3;
+        const size_t nb = op == 9    ? 1
+                          : op == 10 ? 6
+                          : op == 16 ? 9
+                          : (op == 11 || op == 12) ? 3 * nq
+                          : (op == 13 || op == 14) ? nq
+                                                   : 3;
         for (size_t i = 0; i < ab.n_pairs_; i++)
         {
             double *dst = out + i * nb * blk;
@@ -413,6 +419,14 @@ int ref_one_electron_class_ex(void *h, int use_symm, int iab, int op, const doub
                 for (size_t c = 0; c < nq; c++)
                     for (int d = 0; d < 3; d++)
                         std::memcpy(dst + (3 * c + d) * blk, v[c][d].memptr(), blk * sizeof(double));
+                continue;
+            }
+            if (op == 16)
+            {
+                lible::arr2d<lible::vec2d, 3, 3> v = lints::pVpKernel(i, q, grid, ab);
+                for (int a = 0; a < 3; a++)
+                    for (int b = 0; b < 3; b++)
+                        std::memcpy(dst + (3 * a + b) * blk, v[a][b].memptr(), blk * sizeof(double));
                 continue;
             }
             if (op == 15)

@@ -283,3 +283,51 @@ def test_charge_kernels_vs_reference_elementwise():
                 got = np.asarray(got)
                 assert np.abs(got.reshape(want.shape) - want).max() <= 1e-12 * max(1.0, np.abs(want).max()), \
                     (use_symm, i, op)
+
+
+def test_pvp_against_finite_differences_of_charge_integrals():
+    """pVp_ij(m, n) = <d_i m| V |d_j n> = d^2 V_mn / dA_i dB_j for m on atom A and n on atom B != A,
+    with the point charges held fixed: central finite differences (step 1e-3 bohr, four displaced
+    geometries per (i, j)) of externalCharges on an O-H pair in cc-pVDZ (s, p and d functions),
+    to 2e-6 of the largest element.  The whole-matrix form satisfies pVp[i][j] = pVp[j][i]^T and
+    matches the per-pair kernel blocks."""
+    Z = [8, 1]
+    X0 = np.array([[0.1, -0.2, 0.05], [0.3, 1.1, 1.4]])
+    q = np.array([[1.5, 0.4, -0.7, 0.8], [-1.2, 2.0, 1.1, -0.5], [0.4, -1.6, 2.3, 1.3]])
+    s = L.Structure("cc-pvdz", Z, X0, units="bohr")
+    M = L.pVpIntegrals(s, q)
+    assert np.abs(M - M.transpose(1, 0, 3, 2)).max() == 0.0
+    n0 = 14  # cc-pVDZ O: 3s 2p 1d = 14 functions, then H
+    h = 1e-3
+
+    def V(dA, dB):
+        X = X0.copy()
+        X[0] += dA
+        X[1] += dB
+        return L.externalCharges(q, L.Structure("cc-pvdz", Z, X, units="bohr"))
+
+    scale = np.abs(M[:, :, :n0, n0:]).max()
+    for i in range(3):
+        for j in range(3):
+            ei, ej = np.eye(3)[i] * h, np.eye(3)[j] * h
+            fd = (V(ei, ej) - V(ei, -ej) - V(-ei, ej) + V(-ei, -ej)) / (4 * h * h)
+            assert np.abs(fd[:n0, n0:] - M[i, j, :n0, n0:]).max() <= 2e-6 * scale, (i, j)
+    # the per-pair kernel gives the same blocks (first class, every pair)
+    sp = L.shellPairData(True, s)[0]
+    k = L.pVpKernel(list(range(sp.n_pairs_)), q, sp)
+    assert k.shape[1:3] == (3, 3)
+
+
+def test_pvp_reference_kernel_differs_as_documented():
+    """The reference's pVpKernel (oneelints.cpp:1318-1475) does not give the integrals: it leaves out
+    the E factor of its first term and the R factor of its last.  Shown here on s-only functions
+    (6-31+G hydrogens), where it differs from the finite-difference-checked values of this library,
+    while both agree that the integrals are defined per pair and component."""
+    Z = [1, 1]
+    X = [[0.0, 0.0, 0.0], [0.4, -0.3, 1.3]]
+    s, r = L.Structure("6-31+g", Z, X, units="bohr"), R.RefStructure("6-31+g", Z, X)
+    q = np.array([[0.7, 0.2, -0.5, 1.0]])
+    sp = L.shellPairData(True, s)[0]
+    mine = L.pVpKernel(list(range(sp.n_pairs_)), q, sp)
+    ref = r.one_electron_class_ex(True, 0, 16, charges=q).reshape(mine.shape)
+    assert np.abs(mine - ref).max() > 1e-3 * np.abs(mine).max()
