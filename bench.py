@@ -382,6 +382,7 @@ def run_gradient(steps, seed=2024, cpu=True):
         t = time.perf_counter()
         g = L.jk_energy_backward(s, D, SCHWARZ)
         ts.append(time.perf_counter() - t)
+    L.jk_energy_forward(s, D, SCHWARZ)  # builds the forward plan
     t = time.perf_counter()
     L.jk_energy_forward(s, D, SCHWARZ)
     t_fwd = time.perf_counter() - t
