@@ -171,8 +171,9 @@ int lible_gpu_batch_layout(lible_gpu_ctx *ctx, int *n_mol, long long *nao, long 
  * candidate on D/J/K with CUDA events and keeps the fastest.  Candidates: the kernel's tile shape
  * (the default, and where it differs the alternative: twice the warps per quartet on the group
  * paths, the next larger thread group per quartet on the register path, or the default register
- * bound for classes compiled with a raised occupancy bound), resident blocks per SM (all or half)
- * and work-queue chunks of 2, 8 or 32 work units.  J and K are overwritten with
+ * bound for classes compiled with a raised occupancy bound), the class in the other orientation
+ * ((cd|ab) for (ab|cd), where that orientation takes the register path), resident blocks per SM
+ * (all or half) and work-queue chunks of 2, 8 or 32 work units.  J and K are overwritten with
  * meaningless values.  When cache_path is non-empty the choices are appended to that text file;
  * lible_gpu_set_tune_cache(ctx, path) makes later plans start from a cache.  summary (may be NULL)
  * receives one line per class pair. */
@@ -184,8 +185,9 @@ int lible_gpu_set_tune_cache(lible_gpu_ctx *ctx, const char *path);
  * is eri4Benchmark, src/lible/ints/twoel/eri4.cpp:97-150): every class launch runs serialised on
  * the context stream between two CUDA events.  On entry *n is the capacity of the arrays (any of
  * which may be NULL); on return *n is the number of launches.  Per launch: ls[4i..4i+3] = (la, lb,
- * lc, ld), fp32[i] (bit 0: FP32 arithmetic; bit 1: the class's alternative tile shape, chosen by
- * the autotuner), ms[i], algorithmic FLOPs flops[i] and quartets tasks[i].  J, K receive the
+ * lc, ld), fp32[i] (bit 0: FP32 arithmetic; bits 1-2: the shape the autotuner chose, 1 = the
+ * alternative tile shape, 2 = the other orientation), ms[i], algorithmic FLOPs flops[i] and
+ * quartets tasks[i].  J, K receive the
  * build's result. */
 int lible_gpu_jk_profile(lible_gpu_ctx *ctx, const double *D, double *J, double *K, const lible_gpu_jk_opts *opts,
                          int *n, int *ls, int *fp32, double *ms, double *flops, long long *tasks);

@@ -1562,6 +1562,28 @@ namespace lible_b200
         }
     };
 
+    // Shape 2 runs a J/K class pair in the other orientation: the kernel's bra is the plan's ket class
+    // and its ket the plan's bra class, (cd|ab) for (ab|cd), which the final A + A^T of J and K makes
+    // equivalent.  The plan's tasks stay as they are (major = ket pair, minor = bra pair) and are
+    // decoded with major_ket = 0; the bra-side copies in Schwarz order and the per-position Q of the
+    // minor list belong to the plan's bra class and are left unused.
+    static void flipOrientation(QuartetArgs &a, const double *bra_etp)
+    {
+        std::swap(a.bra, a.ket);
+        std::swap(a.bra_qpair, a.ket_qpair);
+        a.major_ket = 0;
+        a.bra_qpos = nullptr;
+        a.bra_soa = nullptr;
+        a.bra_pPs = nullptr;
+        a.bra_Es = nullptr;
+        a.bra_Efs = nullptr;
+        a.bra_pPfs = nullptr;
+        a.bra_soa2 = nullptr;
+        a.bra_Dab = nullptr;
+        a.bra_npos = 0;
+        a.ket_EtP = bra_etp;
+    }
+
     // Launches one J/K build of `plan` (memsets, class kernels over the stream branches, block
     // symmetrisation) on stream_; usable inside a stream capture.  With a timer every class launch
     // goes to stream_ itself, bracketed by events.
@@ -1635,7 +1657,12 @@ namespace lible_b200
                 timer->before(st);
                 timer->info.push_back({{Bh.la, Bh.lb, Kh.la, Kh.lb}, 2 * cp.shape64, 0.0, cp.flops64, cp.n64});
             }
-            cudaCheck(f64(a, st, num_sms_), "jk kernel");
+            {
+                QuartetArgs a64 = a;
+                if (cp.shape64 == 2)
+                    flipOrientation(a64, B.EtP);
+                cudaCheck(f64(a64, st, num_sms_), "jk kernel");
+            }
             if (timer && cp.t64 > 0)
                 timer->after(st);
             if (mixed && cp.t32 > 0)
@@ -1657,7 +1684,10 @@ namespace lible_b200
                     timer->before(st);
                     timer->info.push_back({{Bh.la, Bh.lb, Kh.la, Kh.lb}, 1 + 2 * cp.shape32, 0.0, cp.flops32, cp.n32});
                 }
-                cudaCheck(f32(a, st, num_sms_), "jk kernel fp32");
+                QuartetArgs a32 = a;
+                if (cp.shape32 == 2)
+                    flipOrientation(a32, B.EtP);
+                cudaCheck(f32(a32, st, num_sms_), "jk kernel fp32");
                 if (timer)
                     timer->after(st);
             }
@@ -1792,7 +1822,7 @@ namespace lible_b200
                 continue;
             int gd = 0, cm = 0, shape = 0;  // lines without the shape field are the default shape
             const int got = sscanf(l.c_str() + bar + 1, "%d %d %d", &gd, &cm, &shape);
-            if (got >= 2 && gd > 0 && cm > 0 && (shape == 0 || shape == 1))
+            if (got >= 2 && gd > 0 && cm > 0 && shape >= 0 && shape <= 2)
                 entries[l.substr(0, bar)] = {gd, cm, got == 3 ? shape : 0};
         }
         fclose(f);
@@ -1811,7 +1841,7 @@ namespace lible_b200
                 if (it == entries.end())
                     continue;
                 const Choice &ch = it->second;
-                const int shape = (ch.shape == 1 && hasFwdVariant(cp.tb, cp.tk, fp32 == 1)) ? 1 : 0;
+                const int shape = (ch.shape >= 1 && hasFwdVariant(cp.tb, cp.tk, fp32 == 1, ch.shape)) ? ch.shape : 0;
                 (fp32 ? cp.grid_div32 : cp.grid_div64) = ch.gd;
                 (fp32 ? cp.shape32 : cp.shape64) = shape;
                 rebuildChunks(cp, fp32 == 1, ch.cm);
@@ -1845,12 +1875,17 @@ namespace lible_b200
                 const long long n = fp32 ? cp.t32 : cp.t64;
                 if (n == 0)
                     continue;
-                const int n_shapes = hasFwdVariant(cp.tb, cp.tk, fp32 == 1) ? 2 : 1;
+                // shapes: the default, the alternative tile shape, the other orientation
+                int shapes[3] = {0, 0, 0}, n_shapes = 1;
+                for (int s2 = 1; s2 <= 2; s2++)
+                    if (hasFwdVariant(cp.tb, cp.tk, fp32 == 1, s2))
+                        shapes[n_shapes++] = s2;
                 float best = 1e30f;
                 int best_gd = 1, best_cm = 8, best_shape = 0;
-                for (int shape = 0; shape < n_shapes; shape++)
+                for (int si = 0; si < n_shapes; si++)
                 for (int cm : mults)
                 {
+                    const int shape = shapes[si];
                     LaunchFn fn = fp32 ? lookupFwd32(cp.tb, cp.tk, shape) : lookupFwd64(cp.tb, cp.tk, shape);
                     if (!fn)
                         throw EngineError(kStatusUnsupported, "quartet class not instantiated");
@@ -1895,6 +1930,8 @@ namespace lible_b200
                         a.bra_npos = (int)B.n_pairs;
                         a.ket_EtP = Kc.EtP;
                         a.status = d_status_;
+                        if (shape == 2)
+                            flipOrientation(a, B.EtP);
                         // a second timing only for short launches, where one sample is noisy
                         float t_min = 1e30f;
                         for (int rep = 0; rep < 2 && (rep == 0 || t_min < 2.0f); rep++)

@@ -1466,6 +1466,14 @@ namespace lible_b200
         using S1 = Shape<LA, LB, LC, LD, T, 1>;
         return S0::GT != S1::GT || S0::W != S1::W || minBlocksPerSM<LA, LB, LC, LD, T, 0>() > 1;
     }
+    // Whether a J/K class (la lb | lc ld) with distinct pair types may also run in the other
+    // orientation, (lc ld | la lb), the bra and ket exchanged: instantiated where that orientation
+    // takes the register path.  The launch autotuner times it as shape 2 against shapes 0 and 1.
+    template <int LA, int LB, int LC, int LD, typename T>
+    constexpr bool hasFlippedShape()
+    {
+        return (LA != LC || LB != LD) && Shape<LC, LD, LA, LB, T, 0>::GT > 0;
+    }
 
     template <int LA, int LB, int LC, int LD, typename T, int SV = 0>
     constexpr auto eriKernelFor()

@@ -25,5 +25,5 @@ namespace lible_b200
     LaunchFn lookupFwd32(int bra_type, int ket_type, int shape = 0);
     LaunchFn lookupD1(int bra_type, int ket_type);
     int unitFwd(int bra_type, int ket_type, bool fp32, int shape = 0);
-    bool hasFwdVariant(int bra_type, int ket_type, bool fp32);
+    bool hasFwdVariant(int bra_type, int ket_type, bool fp32, int shape = 1);
 }

@@ -14,6 +14,13 @@ namespace lible_b200
         else
             return cudaErrorNotSupported;
     }
+    cudaError_t launch_fwd32_00_00_f(const QuartetArgs &a, cudaStream_t s, int n)
+    {
+        if constexpr (hasFlippedShape<0,0,0,0,float>())
+            return launchFwd<0,0,0,0,float>(a, s, n);
+        else
+            return cudaErrorNotSupported;
+    }
     cudaError_t launch_fwd32_01_00(const QuartetArgs &a, cudaStream_t s, int n)
     {
         return launchFwd<1,0,0,0,float>(a, s, n);
@@ -22,6 +29,13 @@ namespace lible_b200
     {
         if constexpr (hasShapeVariant<1,0,0,0,float>())
             return launchFwd<1,0,0,0,float,1>(a, s, n);
+        else
+            return cudaErrorNotSupported;
+    }
+    cudaError_t launch_fwd32_01_00_f(const QuartetArgs &a, cudaStream_t s, int n)
+    {
+        if constexpr (hasFlippedShape<1,0,0,0,float>())
+            return launchFwd<0,0,1,0,float>(a, s, n);
         else
             return cudaErrorNotSupported;
     }

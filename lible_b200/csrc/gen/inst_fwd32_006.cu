@@ -14,6 +14,13 @@ namespace lible_b200
         else
             return cudaErrorNotSupported;
     }
+    cudaError_t launch_fwd32_04_02_f(const QuartetArgs &a, cudaStream_t s, int n)
+    {
+        if constexpr (hasFlippedShape<2,1,1,1,float>())
+            return launchFwd<1,1,2,1,float>(a, s, n);
+        else
+            return cudaErrorNotSupported;
+    }
     cudaError_t launch_fwd32_04_03(const QuartetArgs &a, cudaStream_t s, int n)
     {
         return launchFwd<2,1,2,0,float>(a, s, n);
@@ -22,6 +29,13 @@ namespace lible_b200
     {
         if constexpr (hasShapeVariant<2,1,2,0,float>())
             return launchFwd<2,1,2,0,float,1>(a, s, n);
+        else
+            return cudaErrorNotSupported;
+    }
+    cudaError_t launch_fwd32_04_03_f(const QuartetArgs &a, cudaStream_t s, int n)
+    {
+        if constexpr (hasFlippedShape<2,1,2,0,float>())
+            return launchFwd<2,0,2,1,float>(a, s, n);
         else
             return cudaErrorNotSupported;
     }

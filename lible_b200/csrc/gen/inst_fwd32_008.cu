@@ -14,6 +14,13 @@ namespace lible_b200
         else
             return cudaErrorNotSupported;
     }
+    cudaError_t launch_fwd32_05_01_f(const QuartetArgs &a, cudaStream_t s, int n)
+    {
+        if constexpr (hasFlippedShape<2,2,1,0,float>())
+            return launchFwd<1,0,2,2,float>(a, s, n);
+        else
+            return cudaErrorNotSupported;
+    }
     cudaError_t launch_fwd32_05_02(const QuartetArgs &a, cudaStream_t s, int n)
     {
         return launchFwd<2,2,1,1,float>(a, s, n);
@@ -22,6 +29,13 @@ namespace lible_b200
     {
         if constexpr (hasShapeVariant<2,2,1,1,float>())
             return launchFwd<2,2,1,1,float,1>(a, s, n);
+        else
+            return cudaErrorNotSupported;
+    }
+    cudaError_t launch_fwd32_05_02_f(const QuartetArgs &a, cudaStream_t s, int n)
+    {
+        if constexpr (hasFlippedShape<2,2,1,1,float>())
+            return launchFwd<1,1,2,2,float>(a, s, n);
         else
             return cudaErrorNotSupported;
     }

@@ -14,6 +14,13 @@ namespace lible_b200
         else
             return cudaErrorNotSupported;
     }
+    cudaError_t launch_fwd32_07_00_f(const QuartetArgs &a, cudaStream_t s, int n)
+    {
+        if constexpr (hasFlippedShape<3,1,0,0,float>())
+            return launchFwd<0,0,3,1,float>(a, s, n);
+        else
+            return cudaErrorNotSupported;
+    }
     cudaError_t launch_fwd32_07_01(const QuartetArgs &a, cudaStream_t s, int n)
     {
         return launchFwd<3,1,1,0,float>(a, s, n);
@@ -22,6 +29,13 @@ namespace lible_b200
     {
         if constexpr (hasShapeVariant<3,1,1,0,float>())
             return launchFwd<3,1,1,0,float,1>(a, s, n);
+        else
+            return cudaErrorNotSupported;
+    }
+    cudaError_t launch_fwd32_07_01_f(const QuartetArgs &a, cudaStream_t s, int n)
+    {
+        if constexpr (hasFlippedShape<3,1,1,0,float>())
+            return launchFwd<1,0,3,1,float>(a, s, n);
         else
             return cudaErrorNotSupported;
     }

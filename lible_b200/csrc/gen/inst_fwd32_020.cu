@@ -14,6 +14,13 @@ namespace lible_b200
         else
             return cudaErrorNotSupported;
     }
+    cudaError_t launch_fwd32_08_04_f(const QuartetArgs &a, cudaStream_t s, int n)
+    {
+        if constexpr (hasFlippedShape<3,2,2,1,float>())
+            return launchFwd<2,1,3,2,float>(a, s, n);
+        else
+            return cudaErrorNotSupported;
+    }
     cudaError_t launch_fwd32_08_05(const QuartetArgs &a, cudaStream_t s, int n)
     {
         return launchFwd<3,2,2,2,float>(a, s, n);
@@ -22,6 +29,13 @@ namespace lible_b200
     {
         if constexpr (hasShapeVariant<3,2,2,2,float>())
             return launchFwd<3,2,2,2,float,1>(a, s, n);
+        else
+            return cudaErrorNotSupported;
+    }
+    cudaError_t launch_fwd32_08_05_f(const QuartetArgs &a, cudaStream_t s, int n)
+    {
+        if constexpr (hasFlippedShape<3,2,2,2,float>())
+            return launchFwd<2,2,3,2,float>(a, s, n);
         else
             return cudaErrorNotSupported;
     }

@@ -14,6 +14,13 @@ namespace lible_b200
         else
             return cudaErrorNotSupported;
     }
+    cudaError_t launch_fwd32_09_01_f(const QuartetArgs &a, cudaStream_t s, int n)
+    {
+        if constexpr (hasFlippedShape<3,3,1,0,float>())
+            return launchFwd<1,0,3,3,float>(a, s, n);
+        else
+            return cudaErrorNotSupported;
+    }
     cudaError_t launch_fwd32_09_02(const QuartetArgs &a, cudaStream_t s, int n)
     {
         return launchFwd<3,3,1,1,float>(a, s, n);
@@ -22,6 +29,13 @@ namespace lible_b200
     {
         if constexpr (hasShapeVariant<3,3,1,1,float>())
             return launchFwd<3,3,1,1,float,1>(a, s, n);
+        else
+            return cudaErrorNotSupported;
+    }
+    cudaError_t launch_fwd32_09_02_f(const QuartetArgs &a, cudaStream_t s, int n)
+    {
+        if constexpr (hasFlippedShape<3,3,1,1,float>())
+            return launchFwd<1,1,3,3,float>(a, s, n);
         else
             return cudaErrorNotSupported;
     }

@@ -14,4 +14,11 @@ namespace lible_b200
         else
             return cudaErrorNotSupported;
     }
+    cudaError_t launch_fwd32_09_09_f(const QuartetArgs &a, cudaStream_t s, int n)
+    {
+        if constexpr (hasFlippedShape<3,3,3,3,float>())
+            return launchFwd<3,3,3,3,float>(a, s, n);
+        else
+            return cudaErrorNotSupported;
+    }
 }

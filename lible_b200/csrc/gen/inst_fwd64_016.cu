@@ -14,6 +14,13 @@ namespace lible_b200
         else
             return cudaErrorNotSupported;
     }
+    cudaError_t launch_fwd64_07_04_f(const QuartetArgs &a, cudaStream_t s, int n)
+    {
+        if constexpr (hasFlippedShape<3,1,2,1,double>())
+            return launchFwd<2,1,3,1,double>(a, s, n);
+        else
+            return cudaErrorNotSupported;
+    }
     cudaError_t launch_fwd64_07_05(const QuartetArgs &a, cudaStream_t s, int n)
     {
         return launchFwd<3,1,2,2,double>(a, s, n);
@@ -22,6 +29,13 @@ namespace lible_b200
     {
         if constexpr (hasShapeVariant<3,1,2,2,double>())
             return launchFwd<3,1,2,2,double,1>(a, s, n);
+        else
+            return cudaErrorNotSupported;
+    }
+    cudaError_t launch_fwd64_07_05_f(const QuartetArgs &a, cudaStream_t s, int n)
+    {
+        if constexpr (hasFlippedShape<3,1,2,2,double>())
+            return launchFwd<2,2,3,1,double>(a, s, n);
         else
             return cudaErrorNotSupported;
     }

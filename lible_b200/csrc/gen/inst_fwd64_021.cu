@@ -14,6 +14,13 @@ namespace lible_b200
         else
             return cudaErrorNotSupported;
     }
+    cudaError_t launch_fwd64_08_06_f(const QuartetArgs &a, cudaStream_t s, int n)
+    {
+        if constexpr (hasFlippedShape<3,2,3,0,double>())
+            return launchFwd<3,0,3,2,double>(a, s, n);
+        else
+            return cudaErrorNotSupported;
+    }
     cudaError_t launch_fwd64_08_07(const QuartetArgs &a, cudaStream_t s, int n)
     {
         return launchFwd<3,2,3,1,double>(a, s, n);
@@ -22,6 +29,13 @@ namespace lible_b200
     {
         if constexpr (hasShapeVariant<3,2,3,1,double>())
             return launchFwd<3,2,3,1,double,1>(a, s, n);
+        else
+            return cudaErrorNotSupported;
+    }
+    cudaError_t launch_fwd64_08_07_f(const QuartetArgs &a, cudaStream_t s, int n)
+    {
+        if constexpr (hasFlippedShape<3,2,3,1,double>())
+            return launchFwd<3,1,3,2,double>(a, s, n);
         else
             return cudaErrorNotSupported;
     }

@@ -14,6 +14,13 @@ namespace lible_b200
         else
             return cudaErrorNotSupported;
     }
+    cudaError_t launch_fwd64_09_09_f(const QuartetArgs &a, cudaStream_t s, int n)
+    {
+        if constexpr (hasFlippedShape<3,3,3,3,double>())
+            return launchFwd<3,3,3,3,double>(a, s, n);
+        else
+            return cudaErrorNotSupported;
+    }
     cudaError_t launch_fwd64_10_00(const QuartetArgs &a, cudaStream_t s, int n)
     {
         return launchFwd<4,0,0,0,double>(a, s, n);
@@ -22,6 +29,13 @@ namespace lible_b200
     {
         if constexpr (hasShapeVariant<4,0,0,0,double>())
             return launchFwd<4,0,0,0,double,1>(a, s, n);
+        else
+            return cudaErrorNotSupported;
+    }
+    cudaError_t launch_fwd64_10_00_f(const QuartetArgs &a, cudaStream_t s, int n)
+    {
+        if constexpr (hasFlippedShape<4,0,0,0,double>())
+            return launchFwd<0,0,4,0,double>(a, s, n);
         else
             return cudaErrorNotSupported;
     }

@@ -14,6 +14,13 @@ namespace lible_b200
         else
             return cudaErrorNotSupported;
     }
+    cudaError_t launch_fwd64_10_05_f(const QuartetArgs &a, cudaStream_t s, int n)
+    {
+        if constexpr (hasFlippedShape<4,0,2,2,double>())
+            return launchFwd<2,2,4,0,double>(a, s, n);
+        else
+            return cudaErrorNotSupported;
+    }
     cudaError_t launch_fwd64_10_06(const QuartetArgs &a, cudaStream_t s, int n)
     {
         return launchFwd<4,0,3,0,double>(a, s, n);
@@ -22,6 +29,13 @@ namespace lible_b200
     {
         if constexpr (hasShapeVariant<4,0,3,0,double>())
             return launchFwd<4,0,3,0,double,1>(a, s, n);
+        else
+            return cudaErrorNotSupported;
+    }
+    cudaError_t launch_fwd64_10_06_f(const QuartetArgs &a, cudaStream_t s, int n)
+    {
+        if constexpr (hasFlippedShape<4,0,3,0,double>())
+            return launchFwd<3,0,4,0,double>(a, s, n);
         else
             return cudaErrorNotSupported;
     }

@@ -14,6 +14,13 @@ namespace lible_b200
         else
             return cudaErrorNotSupported;
     }
+    cudaError_t launch_fwd64_11_08_f(const QuartetArgs &a, cudaStream_t s, int n)
+    {
+        if constexpr (hasFlippedShape<5,0,3,2,double>())
+            return launchFwd<3,2,5,0,double>(a, s, n);
+        else
+            return cudaErrorNotSupported;
+    }
     cudaError_t launch_fwd64_11_09(const QuartetArgs &a, cudaStream_t s, int n)
     {
         return launchFwd<5,0,3,3,double>(a, s, n);
@@ -22,6 +29,13 @@ namespace lible_b200
     {
         if constexpr (hasShapeVariant<5,0,3,3,double>())
             return launchFwd<5,0,3,3,double,1>(a, s, n);
+        else
+            return cudaErrorNotSupported;
+    }
+    cudaError_t launch_fwd64_11_09_f(const QuartetArgs &a, cudaStream_t s, int n)
+    {
+        if constexpr (hasFlippedShape<5,0,3,3,double>())
+            return launchFwd<3,3,5,0,double>(a, s, n);
         else
             return cudaErrorNotSupported;
     }

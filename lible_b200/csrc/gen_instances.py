@@ -2,8 +2,9 @@
 
 Each file holds a small group of classes of one kernel kind, so the build runs in parallel;
 inst_table.cu maps (bra pair type, ket pair type) to the launch wrappers.  A quartet class is
-always instantiated with the larger pair type in the bra; the host swaps bra and ket (and
-transposes the output) for the other orientation.
+instantiated with the larger pair type in the bra; the host swaps bra and ket (and transposes the
+output) for the other orientation.  For J/K the classes whose other orientation takes the register
+path are also instantiated that way round (shape 2, chosen by the launch autotuner).
 """
 import os
 
@@ -51,6 +52,11 @@ def main():
                              '    {', f'        if constexpr (hasShapeVariant<{la},{lb},{lc},{ld}{T}>())',
                              f'            return {launcher}<{la},{lb},{lc},{ld}{T},1>(a, s, n);',
                              '        else', '            return cudaErrorNotSupported;', '    }']
+                    # shape 2: the class in the other orientation (ket types above bra types)
+                    body += [f'    cudaError_t {name_of(bt, kt)}_f(const QuartetArgs &a, cudaStream_t s, int n)',
+                             '    {', f'        if constexpr (hasFlippedShape<{la},{lb},{lc},{ld}{T}>())',
+                             f'            return {launcher}<{lc},{ld},{la},{lb}{T}>(a, s, n);',
+                             '        else', '            return cudaErrorNotSupported;', '    }']
             body += ['}', '']
             name = f"inst_{kind}_{g // GROUP[kind]:03d}.cu"
             path = os.path.join(out, name)
@@ -63,6 +69,8 @@ def main():
         if kind.startswith("fwd"):
             table += [f'    cudaError_t {name_of(bt, kt)}_v1(const QuartetArgs &, cudaStream_t, int);'
                       for bt, kt in classes]
+            table += [f'    cudaError_t {name_of(bt, kt)}_f(const QuartetArgs &, cudaStream_t, int);'
+                      for bt, kt in classes]
         cls = lambda bt, kt: "%d,%d,%d,%d%s" % (PAIR_TYPES[bt] + PAIR_TYPES[kt] + (T,))
         for bt in range(ntypes):
             table.append(f'    static const LaunchFn k_{kind}_{bt:02d}[{bt + 1}] = {{' +
@@ -71,15 +79,24 @@ def main():
                 table.append(f'    static const LaunchFn k_{kind}v_{bt:02d}[{bt + 1}] = {{' +
                              ", ".join(f"hasShapeVariant<{cls(bt, kt)}>() ? &{name_of(bt, kt)}_v1 : nullptr"
                                        for kt in range(bt + 1)) + '};')
+                table.append(f'    static const LaunchFn k_{kind}f_{bt:02d}[{bt + 1}] = {{' +
+                             ", ".join(f"hasFlippedShape<{cls(bt, kt)}>() ? &{name_of(bt, kt)}_f : nullptr"
+                                       for kt in range(bt + 1)) + '};')
                 for v in (0, 1):
                     table.append(f'    static const int u_{kind}_{v}_{bt:02d}[{bt + 1}] = {{' +
                                  ", ".join(f"workUnit<{cls(bt, kt)},{v}>()" for kt in range(bt + 1)) + '};')
+                flip = lambda bt, kt: "%d,%d,%d,%d%s" % (PAIR_TYPES[kt] + PAIR_TYPES[bt] + (T,))
+                table.append(f'    static const int u_{kind}_2_{bt:02d}[{bt + 1}] = {{' +
+                             ", ".join(f"hasFlippedShape<{cls(bt, kt)}>() ? workUnit<{flip(bt, kt)},0>() : 0"
+                                       for kt in range(bt + 1)) + '};')
         if kind.startswith("fwd"):
-            for v in (0, 1):
+            for v in (0, 1, 2):
                 table.append(f'    static const int *const u_{kind}_{v}[{ntypes}] = {{' +
                              ", ".join(f"u_{kind}_{v}_{bt:02d}" for bt in range(ntypes)) + '};')
             table.append(f'    static const LaunchFn *const k_{kind}v[{ntypes}] = {{' +
                          ", ".join(f"k_{kind}v_{bt:02d}" for bt in range(ntypes)) + '};')
+            table.append(f'    static const LaunchFn *const k_{kind}f[{ntypes}] = {{' +
+                         ", ".join(f"k_{kind}f_{bt:02d}" for bt in range(ntypes)) + '};')
         table.append(f'    static const LaunchFn *const k_{kind}[{ntypes}] = {{' +
                      ", ".join(f"k_{kind}_{bt:02d}" for bt in range(ntypes)) + '};')
     for kind, _, ntypes in kinds():
@@ -91,15 +108,19 @@ def main():
         else:
             table += [f'    LaunchFn {fn}(int bt, int kt, int shape)', '    {',
                       f'        if (bt < 0 || bt >= {ntypes} || kt < 0 || kt > bt)',
-                      '            return nullptr;', f'        return shape ? k_{kind}v[bt][kt] : k_{kind}[bt][kt];', '    }']
+                      '            return nullptr;',
+                      f'        return shape == 2 ? k_{kind}f[bt][kt] : shape ? k_{kind}v[bt][kt] : k_{kind}[bt][kt];',
+                      '    }']
     table += ['    int unitFwd(int bt, int kt, bool fp32, int shape)', '    {',
               '        if (bt < 0 || kt < 0 || kt > bt || bt >= (fp32 ? %d : %d))' % (FP32_MAX_TYPE + 1, len(PAIR_TYPES)),
               '            return 0;',
+              '        if (shape == 2)',
+              '            return fp32 ? u_fwd32_2[bt][kt] : u_fwd64_2[bt][kt];',
               '        if (shape)',
               '            return fp32 ? u_fwd32_1[bt][kt] : u_fwd64_1[bt][kt];',
               '        return fp32 ? u_fwd32_0[bt][kt] : u_fwd64_0[bt][kt];', '    }',
-              '    bool hasFwdVariant(int bt, int kt, bool fp32)', '    {',
-              '        return (fp32 ? lookupFwd32(bt, kt, 1) : lookupFwd64(bt, kt, 1)) != nullptr;', '    }']
+              '    bool hasFwdVariant(int bt, int kt, bool fp32, int shape)', '    {',
+              '        return (fp32 ? lookupFwd32(bt, kt, shape) : lookupFwd64(bt, kt, shape)) != nullptr;', '    }']
     table += ['}', '']
     path = os.path.join(out, "inst_table.cu")
     text = "\n".join(table)

@@ -415,7 +415,8 @@ def jk_autotune(structure, D, schwarz=1e-12, precision="fp64", fp32_threshold=1e
 
 def jk_profile(structure, D, schwarz=1e-12, precision="fp64", fp32_threshold=1e-4, J=None, K=None):
     """One J/K build with every class launch serialised and timed by CUDA events.  Returns a list of
-    dicts (classes, fp32, shape = the launch's tile-shape variant, ms, flops, tasks) in launch order."""
+    dicts (classes, fp32, shape = the launch's shape: 0 default, 1 alternative tile shape, 2 the class
+    in the other orientation; ms, flops, tasks) in launch order."""
     Dh = D if hasattr(D, "data_ptr") else _f64(D)
     J = np.empty(_jk_shape(structure)) if J is None else J
     K = np.empty(_jk_shape(structure)) if K is None else K

@@ -103,7 +103,7 @@ def test_autotune_keeps_results_and_cache_round_trips(tmp_path):
     for e in entries:
         gpu, cls, fp32, bucket, choice = e.split("|")
         gd, cm, shape = (int(x) for x in choice.split())
-        assert gd in (1, 2) and cm in (2, 8, 32) and shape in (0, 1) and fp32 == "0"
+        assert gd in (1, 2) and cm in (2, 8, 32) and shape in (0, 1, 2) and fp32 == "0"
     # a fresh batch built with the cache reproduces the same results
     b2 = L.Batch(mols)
     L.set_tune_cache(b2, cache)
@@ -111,11 +111,14 @@ def test_autotune_keeps_results_and_cache_round_trips(tmp_path):
     assert np.abs(J2 - J).max() <= 1e-12 and np.abs(K2 - K).max() <= 1e-12
 
 
-@pytest.mark.parametrize("basis,precision", [("cc-pvdz", "mixed"), ("cc-pvtz", "mixed"), ("cc-pvtz", "fp64")])
-def test_alternative_tile_shapes_give_the_same_jk(tmp_path, basis, precision):
-    # every class forced to its alternative tile shape (where it has one) through a tune cache:
+@pytest.mark.parametrize("basis,precision,shape", [("cc-pvdz", "mixed", 1), ("cc-pvtz", "mixed", 1),
+                                                  ("cc-pvtz", "fp64", 1), ("cc-pvtz", "fp64", 2),
+                                                  ("cc-pvtz", "mixed", 2), ("cc-pvdz", "fp64", 2)])
+def test_alternative_tile_shapes_give_the_same_jk(tmp_path, basis, precision, shape):
+    # every class forced to its alternative shape (where it has one) through a tune cache; shape 1:
     # the register path with the next larger thread group, the group paths with twice the warps,
-    # the occupancy-bounded classes with the default bound; the J/K must not change
+    # the occupancy-bounded classes with the default bound; shape 2: the class in the other
+    # orientation (bra and ket exchanged) where that takes the register path; the J/K must not change
     Z, xyz, rng = water_cluster(3, 23)
     s = L.Structure(basis, Z, xyz, units="bohr")
     D = random_density(s.nao, 15, rng)
@@ -127,13 +130,13 @@ def test_alternative_tile_shapes_give_the_same_jk(tmp_path, basis, precision):
     for e in lines:
         head, choice = e.rsplit("|", 1)
         gd, cm, _ = choice.split()
-        forced.append(f"{head}|{gd} {cm} 1")
+        forced.append(f"{head}|{gd} {cm} {shape}")
     open(cache, "w").write("\n".join(forced) + "\n")
     s2 = L.Structure(basis, Z, xyz, units="bohr")
     L.set_tune_cache(s2, cache)
     J2, K2, _ = L.jk(s2, D, 1e-12, precision)
     prof = L.jk_profile(s2, D, 1e-12, precision)
-    assert any(r["shape"] == 1 for r in prof)
+    assert any(r["shape"] == shape for r in prof)
     tol = 1e-12 if precision == "fp64" else 1e-9
     assert np.abs(J2 - J).max() <= tol and np.abs(K2 - K).max() <= tol
 
