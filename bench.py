@@ -262,8 +262,9 @@ def run_rij(Z, xyz, D, J64, steps):
     """RI-J of the (H2O)_32 workload with the even-tempered s-f auxiliary basis (0.1 * 2.5^k,
     k = 0..11 per l and atom): wall time of one lible_gpu_rij call from host D to host J (both
     contractions over the kept three-centre tensor, and the solve with the cached metric factor;
-    the first call, which builds both, is timed separately), the rate at which a call reads the
-    tensor (two passes, whole-call time), and the RI error against the direct FP64 J of the same run."""
+    the first call, which builds both, is timed separately; the median of at least five calls, all
+    listed), the rate at which a call reads the tensor (two passes, whole-call time), and the RI
+    error against the direct FP64 J of the same run."""
     from lible_b200 import ints as L
     from lible_b200.workloads import even_tempered_aux
 
@@ -276,15 +277,15 @@ def run_rij(Z, xyz, D, J64, steps):
     Jri, _, _ = L.rij(s, D, SCHWARZ)
     first = time.perf_counter() - t0
     ts = []
-    for _ in range(max(1, steps)):
+    for _ in range(max(5, steps)):
         t = time.perf_counter()
         Jri, _, _ = L.rij(s, D, SCHWARZ)
         ts.append(time.perf_counter() - t)
     tensor_bytes = 8.0 * s.naux * s.nao * s.nao
     return {"workload": "RI-J, (H2O)_32 cc-pVDZ, even-tempered s-f auxiliary basis, FP64", "naux": s.naux,
-            "setup_s": setup, "first_call_s": first, "rij_s": float(np.mean(ts)), "rij_samples_s": ts,
+            "setup_s": setup, "first_call_s": first, "rij_s": float(np.median(ts)), "rij_samples_s": ts,
             "tensor_bytes": tensor_bytes,
-            "tensor_read_gbs": 2 * tensor_bytes / float(np.mean(ts)) / 1e9,
+            "tensor_read_gbs": 2 * tensor_bytes / float(np.median(ts)) / 1e9,
             "solve": L.rij_last_solve(s),
             "dEJ_Eh_vs_direct": float(0.5 * np.sum(D * (Jri - J64))),
             "dJ_fro_vs_direct": float(np.linalg.norm(Jri - J64))}
@@ -296,7 +297,8 @@ def run_rijk(Z, xyz, D, J64, K64, occ, steps):
     the occupied factor C
     (host C -> host K; D = C C^T, C from the eigenvectors of D), with the per-stage device times
     and rates of the exchange build, and the RI errors against the direct FP64 J and K of the same
-    run.  The first call of each builds and factorises (P|Q), which later calls reuse."""
+    run.  The first call of each builds and factorises (P|Q), which later calls reuse; the RI-J and
+    RI-K times are medians of at least five alternating calls, all listed."""
     from lible_b200 import ints as L
 
     w, V = np.linalg.eigh(D)
@@ -309,7 +311,7 @@ def run_rijk(Z, xyz, D, J64, K64, occ, steps):
     Kri = L.rik(s, C=C, schwarz=SCHWARZ)
     first = time.perf_counter() - t0
     tj, tk = [], []
-    for _ in range(max(1, steps)):
+    for _ in range(max(5, steps)):
         t = time.perf_counter()
         Jri, _, _ = L.rij(s, D, SCHWARZ)
         tj.append(time.perf_counter() - t)
@@ -325,8 +327,8 @@ def run_rijk(Z, xyz, D, J64, K64, occ, steps):
     t_grad = time.perf_counter() - t
     rates = {k: info["flops_" + k] / max(info["t_" + k], 1e-12) / 1e12 for k in ("gemm", "solve", "syrk")}
     return {"workload": "RI-JK, (H2O)_32 cc-pVDZ / def2-universal-jkfit, FP64, occupied factor C (160)",
-            "naux": s.naux, "setup_s": setup, "first_call_s": first, "rij_s": float(np.mean(tj)),
-            "rik_s": float(np.mean(tk)), "rij_samples_s": tj, "rik_samples_s": tk, "rik_from_D_s": t_dpath,
+            "naux": s.naux, "setup_s": setup, "first_call_s": first, "rij_s": float(np.median(tj)),
+            "rik_s": float(np.median(tk)), "rij_samples_s": tj, "rik_samples_s": tk, "rik_from_D_s": t_dpath,
             "rij_gradient_s": t_grad,
             "rij_gradient_translational_residual": float(np.abs(gJ.sum(axis=0)).max()),
             "solve": L.rij_last_solve(s),

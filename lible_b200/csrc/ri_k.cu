@@ -601,7 +601,12 @@ namespace lible_b200
         const long long ldz = k + (k & 1);
         if (ldz > INT32_MAX)
             throw EngineError(kStatusUnsupported, "RI-K: naux * occ exceeds the 32-bit cuBLAS dimension range");
-        DevBuf<double> Z((size_t)(n * ldz));
+        if (ft.Z.n < (size_t)(n * ldz))
+        {
+            ft.Z.clear();
+            ft.Z.reset((size_t)(n * ldz));
+        }
+        DevBuf<double> &Z = ft.Z;
         EventPair ev_gemm, ev_syrk;
         const double one = 1.0, zero = 0.0;
         cudaCheck(cudaEventRecord(ev_gemm.a, s), "event");

@@ -116,13 +116,16 @@ namespace lible_b200
     // The fitted three-centre tensor B[R][m][n] = sum_P F_PR (mn|P), F = L^{-T} (Cholesky) or G
     // (eigendecomposition), so that sum_R B_R,mn B_R,ls = sum_PQ (mn|P) M^{-1}_PQ (Q|ls).  Built once
     // per structure and Schwarz threshold (naux * nao^2 doubles) and kept in HBM; every later
-    // exchange build is then one strided-batched DGEMM and one DSYRK.
+    // exchange build is then one strided-batched DGEMM and one symmetric rank-k product.
     struct FittedTensor
     {
         DevBuf<double> B;
         double schwarz = -1;
         size_t naux = 0, nao = 0;
         double t_build = 0;  // seconds of the build (integrals + fit)
+        // the exchange operand Z of the last call, kept so that later calls with at most as many
+        // occupied columns reuse it instead of allocating and freeing naux * nao * occ doubles
+        mutable DevBuf<double> Z;
     };
     void buildFitted(Engine &e, BlasHandle &bh, const MetricFactor &mf, double schwarz, FittedTensor &ft);
     // K += sign * sum_R (B_R C)(B_R C)^T with the cached tensor (same contract as riExchange).
