@@ -3,13 +3,15 @@
     python -m lible_b200.jk_run --waters 8 --basis cc-pvdz --precision fp64 --repeat 2
     python -m lible_b200.jk_run --waters 2 --basis cc-pvtz --gradient --repeat 2
     python -m lible_b200.jk_run --waters 8 --rik def2-universal-jkfit --occ 40 --repeat 2
+    python -m lible_b200.jk_run --waters 8 --basis cc-pvtz --autotune --repeat 2
 
 The cluster and density follow lible_b200.workloads (5.7 bohr lattice, random rotations, +-0.6 bohr
 jitter, D = C C^T with occupation 5 per water unless --occ is given).  Every build is a separate
 lible_gpu_jk call on the structure's stream; the first one also builds the Schwarz factors and the
 screening plan.  --gradient runs the J/K energy gradient (lible_gpu_jk_energy_backward) instead;
 --rik AUX runs RI-K with that auxiliary basis from an orthonormal occupied factor C (the first call
-builds and keeps the fitted three-centre tensor).
+builds and keeps the fitted three-centre tensor); --autotune runs the launch autotuner once on the
+J/K plan before the timed builds (the choices apply to this structure's plan).
 Small cases of this command are what kernel profiles are taken on.
 """
 import argparse
@@ -30,6 +32,7 @@ def main(argv=None):
     ap.add_argument("--repeat", type=int, default=2)
     ap.add_argument("--gradient", action="store_true")
     ap.add_argument("--rik", default=None, metavar="AUX")
+    ap.add_argument("--autotune", action="store_true")
     args = ap.parse_args(argv)
 
     import torch
@@ -55,6 +58,8 @@ def main(argv=None):
     D = random_density(s.nao, args.occ or 5 * args.waters, rng)
     Dd = torch.tensor(D, device="cuda")
     J, K = torch.empty_like(Dd), torch.empty_like(Dd)
+    if args.autotune and not args.gradient:
+        L.jk_autotune(s, D, args.schwarz, args.precision, args.fp32_threshold)
     times = []
     for _ in range(args.repeat):
         torch.cuda.synchronize()
