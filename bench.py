@@ -261,7 +261,8 @@ def run_batch(steps, warmup, dev):
 def run_rij(Z, xyz, D, J64, steps):
     """RI-J of the (H2O)_32 workload with the even-tempered s-f auxiliary basis (0.1 * 2.5^k,
     k = 0..11 per l and atom): wall time of one lible_gpu_rij call from host D to host J (both
-    contractions over the kept three-centre tensor, and the solve with the cached metric factor;
+    contractions over the kept three-centre tensor (its packed lower triangle), and the solve with
+    the cached metric factor;
     the first call, which builds both, is timed separately; the median of at least five calls, all
     listed), the rate at which a call reads the tensor (two passes, whole-call time), and the RI
     error against the direct FP64 J of the same run."""
@@ -281,7 +282,7 @@ def run_rij(Z, xyz, D, J64, steps):
         t = time.perf_counter()
         Jri, _, _ = L.rij(s, D, SCHWARZ)
         ts.append(time.perf_counter() - t)
-    tensor_bytes = 8.0 * s.naux * s.nao * s.nao
+    tensor_bytes = 8.0 * s.naux * s.nao * (s.nao + 1) / 2  # the packed lower triangle of (mn|P)
     return {"workload": "RI-J, (H2O)_32 cc-pVDZ, even-tempered s-f auxiliary basis, FP64", "naux": s.naux,
             "setup_s": setup, "first_call_s": first, "rij_s": float(np.median(ts)), "rij_samples_s": ts,
             "tensor_bytes": tensor_bytes,

@@ -973,15 +973,15 @@ int lible_gpu_rij(lible_gpu_ctx *ctx, const double *D, double schwarz_threshold,
         DevArray j(J, n * n, false, e.stream());
         DevBuf<double> rhs_b(na);
         double *rhs = rhs_b.p;
-        // the tensor (naux * nao^2 doubles) is built by the first call when it takes at most 60% of
-        // the free memory and kept until the structure, the threshold or the mode changes
+        // the tensor (naux * nao (nao + 1) / 2 doubles) is built by the first call when it takes at
+        // most 60% of the free memory and kept until the structure, the threshold or the mode changes
         if (ctx->t3 && (ctx->t3->schwarz != schwarz_threshold || ctx->rij_cached_mode == 0))
             ctx->t3.reset();
         if (!ctx->t3 && ctx->rij_cached_mode == 1)
         {
             size_t free_b = 0, total_b = 0;
             cudaCheck(cudaMemGetInfo(&free_b, &total_b), "meminfo");
-            if (na * n * n * sizeof(double) <= (size_t)(0.6 * (double)free_b))
+            if (na * CachedT3::rowLength(n) * sizeof(double) <= (size_t)(0.6 * (double)free_b))
             {
                 auto t = std::make_unique<CachedT3>();
                 buildT3(e, schwarz_threshold, *t);

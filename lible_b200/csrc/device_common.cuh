@@ -44,9 +44,11 @@ namespace lible_b200
         kRIJ = 3,        // J_mn += sum_P (mn|P) d_P
         kD1Store = 4,    // write the 12 derivative blocks
         kD1Grad = 5,     // contract the derivative blocks with the two-particle density
-        kRIStore = 6,    // out[P - ri_lo][m][n] = out[P - ri_lo][n][m] = (mn|P), P in [ri_lo, ri_hi)
+        kRIStore = 6,    // out[P - ri_lo][m][n] = out[P - ri_lo][n][m] = (mn|P), P in [ri_lo, ri_hi); with
+                         // flags & kRIPacked only the lower triangle, out[P - ri_lo][i(i+1)/2 + j], j <= i
         kD1GradRI = 7,   // RI-J gradient: derivative blocks contracted with D_mn d_P (3c) or d_P d_Q (2c)
     };
+    constexpr int kRIPacked = 8;  // kRIStore flag: packed lower-triangle rows of nao (nao + 1) / 2
 
     struct QuartetArgs
     {
@@ -96,7 +98,8 @@ namespace lible_b200
         const double *ket_EtP;
         // epilogue
         int mode;
-        int flags;                        // kStore: bit0 swap bra shells, bit1 swap ket shells, bit2 swap bra/ket
+        int flags;                        // kStore: bit0 swap bra shells, bit1 swap ket shells, bit2 swap bra/ket;
+                                          // kRIStore: kRIPacked
         int aux_side;                     // RI modes: 0 = ket is the auxiliary side, 1 = bra, 2 = both
         int ri_lo, ri_hi;                 // kRIStore: the block of auxiliary functions written
         double *out;

@@ -2292,12 +2292,12 @@ namespace lible_b200
         return v;
     }
 
-    void Engine::riStore(int P_lo, int P_hi, double *T_dev, double schwarz)
+    void Engine::riStore(int P_lo, int P_hi, double *T_dev, double schwarz, bool packed)
     {
         requireSingle();
         JKPlan &plan = riPlan(schwarz);
-        const size_t n = nao_;
-        cudaCheck(cudaMemsetAsync(T_dev, 0, (size_t)(P_hi - P_lo) * n * n * sizeof(double), stream_), "memset");
+        const size_t n = nao_, row = packed ? n * (n + 1) / 2 : n * n;
+        cudaCheck(cudaMemsetAsync(T_dev, 0, (size_t)(P_hi - P_lo) * row * sizeof(double), stream_), "memset");
         cudaCheck(cudaMemsetAsync(plan.counters, 0, 2 * plan.pairs.size() * sizeof(unsigned long long), stream_),
                   "memset");
         for (size_t ip = 0; ip < plan.pairs.size(); ip++)
@@ -2306,6 +2306,7 @@ namespace lible_b200
             a.out = T_dev;
             a.ri_lo = P_lo;
             a.ri_hi = P_hi;
+            a.flags = packed ? kRIPacked : 0;
             a.counter = plan.counters + 2 * ip;
             a.mode = kRIStore;
             cudaCheck(riLaunchFn(plan, ip)(a, stream_, num_sms_), "ri store");

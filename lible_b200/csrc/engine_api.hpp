@@ -171,8 +171,9 @@ namespace lible_b200
                         double schwarz);
         // Dense block of three-centre integrals: T[P - P_lo][m][n] = (mn|P) for the auxiliary
         // functions P in [P_lo, P_hi) (block ends on shell boundaries, see auxShellStarts), with the
-        // Schwarz test of the RI plan; enqueued on the context stream.
-        void riStore(int P_lo, int P_hi, double *T_dev, double schwarz);
+        // Schwarz test of the RI plan; enqueued on the context stream.  packed: rows of the lower
+        // triangle only, T[P - P_lo][i (i + 1) / 2 + j] = (ij|P) for j <= i (nao (nao + 1) / 2 each).
+        void riStore(int P_lo, int P_hi, double *T_dev, double schwarz, bool packed = false);
         // Gradient of the RI-J energy 1/2 gamma^T (P|Q)^{-1} gamma given d = (P|Q)^{-1} gamma (device
         // vector): sum_P d_P sum_mn D_mn d(mn|P)/dR - 1/2 sum_PQ d_P d_Q d(P|Q)/dR, [n_atoms][3].
         void riGradient(const double *D_dev, const double *dcoef_dev, double *grad_dev, double schwarz);

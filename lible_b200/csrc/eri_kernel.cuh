@@ -496,15 +496,23 @@ namespace lible_b200
         };
         if (a.mode == kRIStore)
         {
-            // both orientations of the main pair; consecutive threads write consecutive n
-            const size_t nn2 = (size_t)n * n;
+            // both orientations of the main pair, or its packed lower-triangle element; consecutive
+            // threads write consecutive n
+            const bool packed = a.flags & kRIPacked;
+            const size_t row = packed ? (size_t)n * (n + 1) / 2 : (size_t)n * n;
             for (int o = tid; o < SX * S0 * S1; o += stride)
             {
                 const int nn = o % S1, m = (o / S1) % S0, x = o / (S0 * S1);
                 const double v = V(m, nn, x);
-                double *blk = a.out + (size_t)(ox + x - a.ri_lo) * nn2;
-                blk[(size_t)(o0 + m) * n + o1 + nn] = v;
-                blk[(size_t)(o1 + nn) * n + o0 + m] = v;
+                double *blk = a.out + (size_t)(ox + x - a.ri_lo) * row;
+                const size_t i = (size_t)(o0 + m), j = (size_t)(o1 + nn);
+                if (packed)
+                    blk[i >= j ? i * (i + 1) / 2 + j : j * (j + 1) / 2 + i] = v;
+                else
+                {
+                    blk[i * n + j] = v;
+                    blk[j * n + i] = v;
+                }
             }
         }
         else if (a.mode == kRIGamma)

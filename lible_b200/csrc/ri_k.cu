@@ -10,11 +10,13 @@
 //      Z[P][m][i] = sum_n T[P][m][n] C[n][i] as one DGEMM over the whole block;
 //   3. W = L^{-1} Z along P: one DTRSM with nao*occ right-hand sides (or W = Z G);
 //   4. K = sum_R W_R W_R^T: W is re-laid out as A[m][R][i] block by block and each block is one
-//      DSYRK with k = R_block * occ.
+//      symmetric rank-k product with k = R_block * occ (syrkUpper, this file's split-K FP64 DMMA
+//      kernel; cuBLAS DSYRK when k is odd).
 // The three-centre tensor is never held in full: only Z (naux x nao x occ) and one block of T.
 // When the fitted tensor B = L^{-1} (mn|P) fits in device memory it is instead built once per
-// structure (buildFitted) and every call is one strided-batched DGEMM and one DSYRK
+// structure (buildFitted) and every call is one strided-batched DGEMM and one syrkUpper
 // (riExchangeFitted): no integrals and no triangular solve per call.
+// RI-J keeps the packed lower triangle of (mn|P) instead (buildT3, t3Gamma, t3Coulomb).
 #include "ri_solve.hpp"
 
 #include <cmath>
@@ -630,9 +632,9 @@ namespace lible_b200
 
     namespace
     {
-        // gamma[P] = sum_e T[P][e] D[e], e over the n^2 elements: one block per row P (rows of n^2
-        // doubles streamed once from HBM, D read from L2), a block reduction of 256 partial sums.
-        // Rows are read as double2 when n^2 is even (every row then starts on 16 bytes).
+        // gamma[P] = sum_e T[P][e] D[e], e over the n2 elements of a row: one block per row P (rows
+        // streamed once from HBM, D read from L2), a block reduction of 256 partial sums.  Rows are
+        // read as double2 when n2 is even (every row then starts on 16 bytes).
         template <bool VEC>
         __global__ void __launch_bounds__(256) t3GammaKernel(const double *__restrict__ T, const double *__restrict__ D,
                                                              long long n2, long long naux, double *__restrict__ gamma)
@@ -675,8 +677,8 @@ namespace lible_b200
             }
         }
 
-        // J[e] += sum_{P in the block's range} d[P] T[P][e]: blocks tile the n^2 elements (a double2
-        // per thread when n^2 is even, else one double) and split the auxiliary range in slices of
+        // J[e] += sum_{P in the block's range} d[P] T[P][e]: blocks tile the n2 elements (a double2
+        // per thread when n2 is even, else one double) and split the auxiliary range in slices of
         // `per`; each element of T is read once, two rows in flight per step.
         template <bool VEC>
         __global__ void __launch_bounds__(256) t3CoulombKernel(const double *__restrict__ T, const double *__restrict__ dcoef,
@@ -721,15 +723,37 @@ namespace lible_b200
                 atomicAdd(J + e, a0);
             }
         }
+
+        // Dp[i (i + 1) / 2 + j] = D_ij + D_ji for j < i, D_ii for j = i (one thread per element).
+        __global__ void packDensityKernel(const double *__restrict__ D, long long n, double *__restrict__ Dp)
+        {
+            const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+            if (e >= n * n)
+                return;
+            const long long i = e / n, j = e % n;
+            if (j > i)
+                return;
+            Dp[i * (i + 1) / 2 + j] = i == j ? D[e] : D[e] + D[j * n + i];
+        }
+
+        // J_ij = J_ji = Jp[max (max + 1) / 2 + min] (one thread per element of J).
+        __global__ void unpackTriangleKernel(const double *__restrict__ Jp, long long n, double *__restrict__ J)
+        {
+            const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+            if (e >= n * n)
+                return;
+            const long long i = e / n, j = e % n;
+            J[e] = i >= j ? Jp[i * (i + 1) / 2 + j] : Jp[j * (j + 1) / 2 + i];
+        }
     }
 
     void buildT3(Engine &e, double schwarz, CachedT3 &t3)
     {
         const size_t n = e.nao(), na = e.naux();
-        t3.T.reset(na * n * n);
+        t3.T.reset(na * CachedT3::rowLength(n));
         EventPair ev;
         cudaCheck(cudaEventRecord(ev.a, e.stream()), "event");
-        e.riStore(0, (int)na, t3.T.p, schwarz);
+        e.riStore(0, (int)na, t3.T.p, schwarz, true);
         e.checkStatus();
         cudaCheck(cudaEventRecord(ev.b, e.stream()), "event");
         cudaCheck(cudaEventSynchronize(ev.b), "three-centre tensor");
@@ -741,18 +765,25 @@ namespace lible_b200
 
     void t3Gamma(Engine &e, const CachedT3 &t3, const double *D_dev, double *gamma_dev)
     {
-        const long long n2 = (long long)(t3.nao * t3.nao), na = (long long)t3.naux;
+        const long long n = (long long)t3.nao, n2 = (long long)CachedT3::rowLength(t3.nao), na = (long long)t3.naux;
+        if (t3.Dp.n < (size_t)n2)
+            t3.Dp.reset((size_t)n2);
+        packDensityKernel<<<(unsigned)((n * n + 255) / 256), 256, 0, e.stream()>>>(D_dev, n, t3.Dp.p);
+        cudaCheck(cudaGetLastError(), "t3 pack");
         const int grid = (int)std::min<long long>(na, 148LL * 8);
         if (n2 % 2 == 0)
-            t3GammaKernel<true><<<grid, 256, 0, e.stream()>>>(t3.T.p, D_dev, n2, na, gamma_dev);
+            t3GammaKernel<true><<<grid, 256, 0, e.stream()>>>(t3.T.p, t3.Dp.p, n2, na, gamma_dev);
         else
-            t3GammaKernel<false><<<grid, 256, 0, e.stream()>>>(t3.T.p, D_dev, n2, na, gamma_dev);
+            t3GammaKernel<false><<<grid, 256, 0, e.stream()>>>(t3.T.p, t3.Dp.p, n2, na, gamma_dev);
         cudaCheck(cudaGetLastError(), "t3 gamma");
     }
 
-    void t3Coulomb(Engine &e, const CachedT3 &t3, const double *d_dev, double *J_dev)
+    void t3Coulomb(Engine &e, const CachedT3 &t3, const double *d_dev, double *J_out)
     {
-        const long long n2 = (long long)(t3.nao * t3.nao), na = (long long)t3.naux;
+        const long long n = (long long)t3.nao, n2 = (long long)CachedT3::rowLength(t3.nao), na = (long long)t3.naux;
+        if (t3.Jp.n < (size_t)n2)
+            t3.Jp.reset((size_t)n2);
+        double *J_dev = t3.Jp.p;
         cudaCheck(cudaMemsetAsync(J_dev, 0, (size_t)n2 * sizeof(double), e.stream()), "memset");
         const bool vec = n2 % 2 == 0;
         const long long blocks = ((vec ? n2 / 2 : n2) + 255) / 256;
@@ -765,6 +796,8 @@ namespace lible_b200
         else
             t3CoulombKernel<false><<<grid, 256, 0, e.stream()>>>(t3.T.p, d_dev, n2, na, per, J_dev);
         cudaCheck(cudaGetLastError(), "t3 coulomb");
+        unpackTriangleKernel<<<(unsigned)((n * n + 255) / 256), 256, 0, e.stream()>>>(J_dev, n, J_out);
+        cudaCheck(cudaGetLastError(), "t3 unpack");
     }
 
     void splitDensity(Engine &e, const double *D_dev, long long n, DevBuf<double> &Cp, long long &n_pos,

@@ -132,19 +132,23 @@ namespace lible_b200
     void riExchangeFitted(Engine &e, BlasHandle &bh, const FittedTensor &ft, const double *C_dev, long long occ,
                           double sign, double *K_dev, RIKStats *stats);
 
-    // The raw three-centre tensor T[P][m][n] = (mn|P) (both orientations of each pair, Schwarz
-    // screened), kept in HBM by the RI-J calls when it fits; each RI-J is then two passes over it.
+    // The raw three-centre tensor (mn|P) (Schwarz screened), kept in HBM by the RI-J calls when it
+    // fits; each RI-J is then two passes over it.  (mn|P) is symmetric in m, n, so only the lower
+    // triangle is kept: T[P][i (i + 1) / 2 + j] = (ij|P), j <= i, naux * nao (nao + 1) / 2 doubles.
     struct CachedT3
     {
         DevBuf<double> T;
         double schwarz = -1;
         size_t naux = 0, nao = 0;
         double t_build = 0;  // seconds of the build
+        // packed operands of the two passes: D_ij + D_ji (D_ii on the diagonal), and J's triangle
+        mutable DevBuf<double> Dp, Jp;
+        static size_t rowLength(size_t nao) { return nao * (nao + 1) / 2; }
     };
     void buildT3(Engine &e, double schwarz, CachedT3 &t3);
-    // gamma_P = sum_mn T[P][mn] D_mn (full sum over both triangles).
+    // gamma_P = sum_mn (mn|P) D_mn (full sum over both triangles; D need not be symmetric).
     void t3Gamma(Engine &e, const CachedT3 &t3, const double *D_dev, double *gamma_dev);
-    // J_mn = sum_P T[P][mn] d_P (symmetric by construction).
+    // J_mn = sum_P (mn|P) d_P (symmetric by construction).
     void t3Coulomb(Engine &e, const CachedT3 &t3, const double *d_dev, double *J_dev);
 
     // Mirrors the row-major upper triangle of the n x n matrix into the lower one.

@@ -469,6 +469,32 @@ def test_mixed_precision_jk_ccpvtz():
     assert np.linalg.norm(Jm2 - J) <= 1e-4 and np.linalg.norm(Km2 - K) <= 1e-4
 
 
+def test_rij_cached_packed_rows_odd_length():
+    """The cached RI-J tensor keeps the packed lower triangle, nao (nao + 1) / 2 elements per
+    auxiliary function.  H2 / cc-pVDZ has 10 AOs, so a row holds 55 elements and the passes take
+    their scalar (unvectorised) form; the cached call matches the evaluating one and the
+    reference's gamma, also for a density that is not symmetric."""
+    xyz = np.array([[0.0, 0.0, 0.0], [0.0, 0.3, 1.4]])
+    s = L.Structure("cc-pvdz", [1, 1], xyz, "def2-universal-jkfit", units="bohr")
+    assert (s.nao * (s.nao + 1) // 2) % 2 == 1
+    r = R.RefStructure("cc-pvdz", [1, 1], xyz, aux="def2-universal-jkfit")
+    rng = np.random.default_rng(11)
+    D = random_density(s.nao, 1, rng)
+    J, g, d = L.rij(s, D, schwarz=0.0)  # the first call builds and uses the cached tensor
+    gr = r.rij_gamma(D)
+    assert np.abs(g - gr).max() <= 1e-12 * max(1.0, np.abs(gr).max())
+    L.rij_set_cached(s, 0)
+    Jn, gn, dn = L.rij(s, D, schwarz=0.0)
+    L.rij_set_cached(s, 1)
+    assert np.abs(J - Jn).max() <= 1e-12 and np.abs(J - J.T).max() == 0.0
+    assert np.abs(g - gn).max() <= 1e-12 * max(1.0, np.abs(gn).max())
+    # a non-symmetric density: the cached pass sums both triangles, (mn|P) (D_mn + D_nm)
+    A = D + 0.1 * rng.standard_normal(D.shape)
+    _, ga, _ = L.rij(s, A, schwarz=0.0)
+    _, gs, _ = L.rij(s, 0.5 * (A + A.T), schwarz=0.0)
+    assert np.abs(ga - gs).max() <= 1e-12 * max(1.0, np.abs(gs).max())
+
+
 def test_rij_even_tempered_aux_vs_reference():
     # the s-f even-tempered auxiliary basis of the mixed-precision RI-J workload (0.1 * 2.5^k,
     # k = 0..11 per l), on one water
