@@ -204,11 +204,12 @@ namespace lible_b200
                     const double *e1cd = a.ket.E1t + (size_t)q * 3 * C::HCD * C::SCD;
                     if constexpr (S::STAGE)
                     {
+                        // copies land during the R build; waited for before the first product
                         double *ek = reinterpret_cast<double *>(smem + S::off_ek);
                         for (int e = tid; e < C::HCD * C::SCD; e += G)
-                            ek[e] = __ldg(ecd + e);
+                            cpAsync8(ek + e, ecd + e);
                         for (int e = tid; e < 3 * C::HCD * C::SCD; e += G)
-                            ek[C::HCD * C::SCD + e] = __ldg(e1cd + e);
+                            cpAsync8(ek + C::HCD * C::SCD + e, e1cd + e);
                         ecd = ek;
                         e1cd = ek + C::HCD * C::SCD;
                     }
@@ -278,6 +279,8 @@ namespace lible_b200
                             const double r = cur[hermIndex(s4.x + dx, s4.y + dy, s4.z + dz)];
                             rm[e] = s4.w ? -r : r;
                         }
+                        if constexpr (S::STAGE)
+                            cpAsyncWaitAll();  // the staged ket tiles (no-op after the first pass)
                         __syncthreads();
 #pragma unroll
                         for (int k = 0; k < S::IK; k++)
@@ -912,13 +915,14 @@ namespace lible_b200
                     {
                         const double *ecd = a.ket.Et + (size_t)q * C::HCD * C::SCD;
                         const double *e1cd = a.ket.E1t + (size_t)q * 3 * C::HCD * C::SCD;
+                        // copies land during the R build; waited for before the W products
                         for (int e = tid; e < C::HCD * C::SCD; e += G)
                         {
                             const int o = (e / C::SCD) * S::P_EC + e % C::SCD;
-                            ec[o] = __ldg(ecd + e);
-                            ec[EC_SZ + o] = __ldg(e1cd + e);
-                            ec[2 * EC_SZ + o] = __ldg(e1cd + C::HCD * C::SCD + e);
-                            ec[3 * EC_SZ + o] = __ldg(e1cd + 2 * C::HCD * C::SCD + e);
+                            cpAsync8(ec + o, ecd + e);
+                            cpAsync8(ec + EC_SZ + o, e1cd + e);
+                            cpAsync8(ec + 2 * EC_SZ + o, e1cd + C::HCD * C::SCD + e);
+                            cpAsync8(ec + 3 * EC_SZ + o, e1cd + 2 * C::HCD * C::SCD + e);
                         }
                     }
                     // R to order L + 1 (closed form, or levels split over the block)
@@ -982,6 +986,8 @@ namespace lible_b200
                         nxt = tmp;
                     }
                     }
+                    cpAsyncWaitAll();
+                    __syncthreads();  // the ket tiles are visible to every warp
                     // the seven W products per tile, consumed in registers
                     double ax = 0, ay = 0, az = 0, c2x = 0, c2y = 0, c2z = 0;
                     for (int t = warp; t < S::TILES2; t += WD)

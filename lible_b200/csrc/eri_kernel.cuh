@@ -157,6 +157,29 @@ namespace lible_b200
 
     // Waits for the barrier phase with parity `phase`; gives up after `polls` polls, records
     // kStatusTimeout-style failure in *status and returns false.
+    // Asynchronous 8-byte global -> shared copy (no register staging); completed by cpAsyncWaitAll
+    // in the issuing thread, then published to the block by a barrier.
+    __device__ __forceinline__ void cpAsync8(void *dst_smem, const void *src_gmem)
+    {
+        const unsigned d = (unsigned)__cvta_generic_to_shared(dst_smem);
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src_gmem) : "memory");
+    }
+    __device__ __forceinline__ void cpAsync4(void *dst_smem, const void *src_gmem)
+    {
+        const unsigned d = (unsigned)__cvta_generic_to_shared(dst_smem);
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(src_gmem) : "memory");
+    }
+    template <typename T>
+    __device__ __forceinline__ void cpAsyncElem(T *dst_smem, const T *src_gmem)
+    {
+        static_assert(sizeof(T) == 4 || sizeof(T) == 8, "4- or 8-byte elements");
+        if constexpr (sizeof(T) == 8)
+            cpAsync8(dst_smem, src_gmem);
+        else
+            cpAsync4(dst_smem, src_gmem);
+    }
+    __device__ __forceinline__ void cpAsyncWaitAll() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
     __device__ __forceinline__ bool mbarWait(uint64_t *mbar, unsigned phase, int *status, int polls = kWaitPolls)
     {
         const unsigned m = (unsigned)__cvta_generic_to_shared(mbar);
@@ -726,14 +749,18 @@ namespace lible_b200
         for (uint32_t p = p0; p < p1; p++)
         {
             const PQ4 P = loadPQ(a.bra.pP, p);
+            // the bra E tile lands while the ket loop runs (waited for before the second product)
             for (int e = tid; e < C::SAB * C::HAB; e += G)
-                eas[e] = Eb[(size_t)p * C::SAB * C::HAB + e];
+                cpAsyncElem(eas + e, Eb + (size_t)p * C::SAB * C::HAB + e);
             T rxe[S::IK];
 #pragma unroll
             for (int k = 0; k < S::IK; k++)
                 rxe[k] = T(0);
             for (uint32_t q = q0; q < q1; q++)
             {
+                // the ket E tile of this primitive lands during the Boys function and the R build
+                for (int e = tid; e < C::HCD * C::SCD; e += G)
+                    cpAsyncElem(ecs + e, Ek + (size_t)q * C::HCD * C::SCD + e);
                 const PQ4 Q = loadPQ(a.ket.pP, q);
                 const double rs = rsqrt(P.x + Q.x);
                 const double alpha = P.x * Q.x * (rs * rs);
@@ -800,15 +827,14 @@ namespace lible_b200
                     nxt = tmp;
                 }
                 }
-                // signed R matrix [h'][h] and the staged ket E[q] [h'][cd]
+                // signed R matrix [h'][h]; the ket E[q] [h'][cd] copies complete
                 for (int e = tid; e < C::HCD * C::HAB; e += G)
                 {
                     const short ix = rix[e];
                     const T r = cur[ix & 0x7fff];
                     rm[e] = (ix & 0x8000) ? -r : r;
                 }
-                for (int e = tid; e < C::HCD * C::SCD; e += G)
-                    ecs[e] = Ek[(size_t)q * C::HCD * C::SCD + e];
+                cpAsyncWaitAll();
                 groupSync(G);
 #pragma unroll
                 for (int k = 0; k < S::IK; k++)
@@ -833,6 +859,7 @@ namespace lible_b200
                 if (e < C::HAB * C::SCD)
                     rxs[e] = rxe[k];
             }
+            cpAsyncWaitAll();  // the bra E tile (already complete unless the ket loop was empty)
             groupSync(G);
 #pragma unroll
             for (int k = 0; k < S::IB; k++)
@@ -892,8 +919,10 @@ namespace lible_b200
         for (uint32_t p = p0; p < p1; p++)
         {
             const PQ4 P = p == p0 ? g.P : loadPQ(a.bra.pP, p);
+            // the bra E tile of this primitive lands while the ket loop runs; it is first read by
+            // the second product, after the wait and the barrier in front of it
             for (int e = tid; e < C::SAB * C::HAB; e += G)
-                ea[(e / C::HAB) * S::P_EA + e % C::HAB] = __ldg(a.bra.E + (size_t)p * C::SAB * C::HAB + e);
+                cpAsync8(ea + (e / C::HAB) * S::P_EA + e % C::HAB, a.bra.E + (size_t)p * C::SAB * C::HAB + e);
             double acc[S::TPW][2];
 #pragma unroll
             for (int i = 0; i < S::TPW; i++)
@@ -986,6 +1015,7 @@ namespace lible_b200
                     {
                         if (tid == 0 && !a.wait_inject)
                             mbarWait(mbar, ph, nullptr);  // a late copy lands before the block exits
+                        cpAsyncWaitAll();                 // and so do the bra E copies
                         return false;
                     }
                 }
@@ -1023,6 +1053,7 @@ namespace lible_b200
                     o[1] = acc[i][1];
                 }
             }
+            cpAsyncWaitAll();
             groupSync(G);
             // v[tile] += E_bra[m][h] (R.E)[h][c] over h
 #pragma unroll
