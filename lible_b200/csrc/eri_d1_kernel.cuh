@@ -769,14 +769,21 @@ namespace lible_b200
         static constexpr size_t off_ht = a16(off_rd + 8 * 9 * WD);                        // NR1 char4
         static constexpr size_t off_hab = a16(off_ht + 4 * C::NR1);                       // HAB char4
         static constexpr size_t off_hcd = a16(off_hab + 4 * C::HAB);                      // HCD char4
-        static constexpr size_t smem = a16(off_hcd + 4 * C::HCD);
+        static constexpr size_t smem1 = a16(off_hcd + 4 * C::HCD);
+        // a second E_ab buffer (double buffering of the four E matrices of a bra primitive), kept
+        // when it costs no resident block per SM (228 KB per SM, 1 KB reserved per block)
+        static constexpr size_t off_ea2 = smem1;
+        static constexpr size_t smem2 = a16(off_ea2 + 8 * (size_t)KT1 * 4 * P_EA);
+        static constexpr size_t perSM(size_t x) { return (228 * 1024) / (x + 1024); }
+        static constexpr bool DB = smem2 <= 200 * 1024 && perSM(smem2) >= perSM(smem1);
+        static constexpr size_t smem = DB ? smem2 : smem1;
         // the classes this form serves, as measured on the (H2O)_8 cc-pVTZ gradient: not a register
         // class, a ket of at least S_cd = 5 spherical and H_cd = 10 Hermite functions (with smaller
         // kets the W products are too thin to pay for the GE products and the staging; (dd|ss), (fp|ss)
         // and (dd|ps) ran up to 2.3x slower than in the block form), and a layout that fits one block
         // per SM
         static constexpr bool USE = !d1RegisterClass(LA, LB, LC, LD) && C::SCD >= 5 && C::HCD >= 10 &&
-                                    smem <= 200 * 1024;
+                                    smem1 <= 200 * 1024;
     };
 
     template <int LA, int LB, int LC, int LD>
@@ -799,12 +806,16 @@ namespace lible_b200
         const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, r8 = lane >> 2, k4 = lane & 3;
         constexpr size_t GE_SZ = (size_t)S::MT * 8 * S::P_GE, EC_SZ = (size_t)S::NT2 * 8 * S::P_EC;
 
+        double *ea2 = reinterpret_cast<double *>(smem + S::off_ea2);  // second E_ab buffer (S::DB)
         // once per block: zero every operand tile (padding rows and columns are never written
         // afterwards, so they stay zero) and the Hermite (t, u, v, order) tables
         {
             const int nz = (int)((S::off_rd - S::off_ea) / 8);
             for (int e = tid; e < nz; e += G)
                 ea[e] = 0.0;
+            if constexpr (S::DB)
+                for (int e = tid; e < S::KT1 * 4 * S::P_EA; e += G)
+                    ea2[e] = 0.0;
             for (int e = tid; e < C::NR1; e += G)
             {
                 int t, u, v;
@@ -826,9 +837,22 @@ namespace lible_b200
         }
         __syncthreads();
 
+        // E (x4 = 0) or E1_x (x4 = 1..3) of bra primitive p into a staged E_ab buffer, by cp.async
+        auto issueE = [&](uint32_t p, int x4, double *dst) {
+            const double *src = x4 == 0 ? a.bra.E + (size_t)p * C::SAB * C::HAB
+                                        : a.bra.E1 + ((size_t)p * 3 + (x4 - 1)) * C::SAB * C::HAB;
+            for (int e = tid; e < C::SAB * C::HAB; e += G)
+                cpAsync8(dst + (e / C::HAB) * S::P_EA + e % C::HAB, src + e);
+        };
+
         auto processTask = [&](uint32_t ib, uint32_t ik) {
             const int32_t *bi = a.bra.info + 8 * ib;
             const int32_t *ki = a.ket.info + 8 * ik;
+            const uint32_t p0 = a.bra.pofs[ib], p1 = a.bra.pofs[ib + 1];
+            // the first E matrix lands while Gamma is formed (the first buffer was last read by a
+            // product that every thread finished before a later barrier)
+            if constexpr (S::DB)
+                issueE(p0, 0, ea);
             // Gamma[m][c] of the quartet (as in the block kernel's epilogues)
             {
                 const int n = a.nao;
@@ -868,27 +892,44 @@ namespace lible_b200
 #pragma unroll
             for (int x = 0; x < 9; x++)
                 g[x] = 0.0;
-            const uint32_t p0 = a.bra.pofs[ib], p1 = a.bra.pofs[ib + 1];
             const uint32_t q0 = a.ket.pofs[ik], q1 = a.ket.pofs[ik + 1];
             for (uint32_t p = p0; p < p1; p++)
             {
                 const PQ4 P = loadPQ(a.bra.pP, p);
                 const double2 AB = __ldg(reinterpret_cast<const double2 *>(a.bra.ab) + p);
-                // GE (x4 = 0) and GE1_x (x4 = 1..3) = E^T Gamma, one staged E matrix at a time
+                // the first buffer's last reader (the x4 = 2 product of the previous primitive)
+                // finished before the barriers of the ket loop
+                if constexpr (S::DB)
+                    if (p != p0)
+                        issueE(p, 0, ea);
+                // GE (x4 = 0) and GE1_x (x4 = 1..3) = E^T Gamma: with two buffers the next E matrix
+                // lands during this product, else one staged E matrix at a time
                 for (int x4 = 0; x4 < 4; x4++)
                 {
-                    const double *src = x4 == 0 ? a.bra.E + (size_t)p * C::SAB * C::HAB
-                                                : a.bra.E1 + ((size_t)p * 3 + (x4 - 1)) * C::SAB * C::HAB;
-                    __syncthreads();  // the previous product has read ea (and, first time, gs is written)
-                    for (int e = tid; e < C::SAB * C::HAB; e += G)
-                        ea[(e / C::HAB) * S::P_EA + e % C::HAB] = __ldg(src + e);
-                    __syncthreads();
+                    const double *eb = ea;
+                    if constexpr (S::DB)
+                    {
+                        cpAsyncWaitAll();  // E of this x4 (the only copy in flight)
+                        __syncthreads();   // it is visible, Gamma is written, the product x4 - 1 is done
+                        if (x4 < 3)
+                            issueE(p, x4 + 1, (x4 & 1) ? ea : ea2);
+                        eb = (x4 & 1) ? ea2 : ea;
+                    }
+                    else
+                    {
+                        const double *src = x4 == 0 ? a.bra.E + (size_t)p * C::SAB * C::HAB
+                                                    : a.bra.E1 + ((size_t)p * 3 + (x4 - 1)) * C::SAB * C::HAB;
+                        __syncthreads();  // the previous product has read ea (and, first time, gs is written)
+                        for (int e = tid; e < C::SAB * C::HAB; e += G)
+                            ea[(e / C::HAB) * S::P_EA + e % C::HAB] = __ldg(src + e);
+                        __syncthreads();
+                    }
                     double *out = ge + x4 * GE_SZ;
                     for (int t = warp; t < S::TILES1; t += WD)
                     {
                         const int mt = t / S::NT1, nt = t % S::NT1;
                         double d0 = 0.0, d1 = 0.0;
-                        const double *A = ea + k4 * S::P_EA + mt * 8 + r8;
+                        const double *A = eb + k4 * S::P_EA + mt * 8 + r8;
                         const double *B = gs + k4 * S::P_G + nt * 8 + r8;
 #pragma unroll 4
                         for (int ks = 0; ks < S::KT1; ks++)

@@ -1142,11 +1142,24 @@ namespace lible_b200
     // register-path classes where a higher occupancy measured faster on the (H2O)_32 cc-pVDZ J/K build
     // than the default bound (which lets the compiler use more registers): FP64 (dp|ps), (ds|ps),
     // (dp|ss) at 3 blocks and (ps|ss) at 6; FP32 (dp|ps), (ds|pp) at 3, (pp|ps) at 4, (ps|ps) at 6,
-    // (ds|ss) at 8.  1 = the default bound.
+    // (ds|ss) at 8; and the DMMA group-path classes at 128 registers per thread where their shared
+    // memory allows the blocks ((dd|dd): 166 -> 128 registers, 3 -> 4 blocks, 1.34 -> 1.15 ms on
+    // (H2O)_8 cc-pVTZ).  1 = the default bound.
     template <int LA, int LB, int LC, int LD, typename T, int SV = 0>
     constexpr int minBlocksPerSM()
     {
-        if (SV != 0 || Shape<LA, LB, LC, LD, T, SV>::W != 0)
+        using S = Shape<LA, LB, LC, LD, T, SV>;
+        if (SV != 0)
+            return 1;
+        if constexpr (S::MMA)
+        {
+            // DMMA group path: 128 registers per thread (4 blocks of 128 threads, 8 of 64, 2 of
+            // 256), where the shared-memory layout lets that many blocks reside
+            const int want = S::block <= 64 ? 8 : S::block <= 128 ? 4 : 2;
+            const int fit = (int)((228 * 1024) / (S::m_smem + 1024));
+            return want < fit ? want : fit;
+        }
+        if (S::W != 0)
             return 1;
         constexpr int c = LA * 1000 + LB * 100 + LC * 10 + LD;
         if (sizeof(T) == 8)
