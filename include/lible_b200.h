@@ -253,10 +253,11 @@ int lible_gpu_jk_energy_backward(lible_gpu_ctx *ctx, const double *D, const libl
 /* ---- RI-J ------------------------------------------------------------------------------------
  * gamma_P = sum_mn (mn|P) D_mn; (P|Q) d = gamma (Cholesky, FP64); J_mn = sum_P (mn|P) d_P.
  * Three-centre quartets with Q_mn Q_P < schwarz_threshold are skipped (Q_P = sqrt (P|P)).
- * gamma / dcoef outputs may be NULL.  The first call builds the tensor (mn|P) (naux * nao^2
- * doubles) in device memory when it takes at most 60% of the free memory and keeps it while the
- * structure and the threshold stay the same; later calls then contract that tensor instead of
- * evaluating the integrals twice.  The metric factor is kept the same way. */
+ * gamma / dcoef outputs may be NULL.  The first call builds the tensor (mn|P), its lower
+ * triangle in m, n (naux * nao (nao + 1) / 2 doubles), in device memory when it takes at most 60%
+ * of the free memory and keeps it while the structure and the threshold stay the same; later calls
+ * then contract that tensor instead of evaluating the integrals twice.  The metric factor is kept
+ * the same way. */
 int lible_gpu_rij(lible_gpu_ctx *ctx, const double *D, double schwarz_threshold, double *J, double *gamma,
                   double *dcoef);
 /* mode 1 (default): lible_gpu_rij keeps the three-centre tensor when it fits; 0: never build it
