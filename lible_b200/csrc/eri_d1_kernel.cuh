@@ -777,6 +777,10 @@ namespace lible_b200
         static constexpr size_t perSM(size_t x) { return (228 * 1024) / (x + 1024); }
         static constexpr bool DB = smem2 <= 200 * 1024 && perSM(smem2) >= perSM(smem1);
         static constexpr size_t smem = DB ? smem2 : smem1;
+        // resident blocks per SM the register allocation must allow: as many as the shared memory
+        // admits, at no fewer than 128 registers per thread
+        static constexpr int MINB0 = (int)perSM(smem) < 65536 / (G * 128) ? (int)perSM(smem) : 65536 / (G * 128);
+        static constexpr int MINB = MINB0 < 1 ? 1 : MINB0;
         // the classes this form serves, as measured on the (H2O)_8 cc-pVTZ gradient: not a register
         // class, a ket of at least S_cd = 5 spherical and H_cd = 10 Hermite functions (with smaller
         // kets the W products are too thin to pay for the GE products and the staging; (dd|ss), (fp|ss)
@@ -787,7 +791,8 @@ namespace lible_b200
     };
 
     template <int LA, int LB, int LC, int LD>
-    __global__ void __launch_bounds__(ShapeD1M<LA, LB, LC, LD>::G) eriD1MmaKernel(QuartetArgs a)
+    __global__ void __launch_bounds__(ShapeD1M<LA, LB, LC, LD>::G, ShapeD1M<LA, LB, LC, LD>::MINB)
+    eriD1MmaKernel(QuartetArgs a)
     {
         using C = Cls<LA, LB, LC, LD>;
         using S = ShapeD1M<LA, LB, LC, LD>;
