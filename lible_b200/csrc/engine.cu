@@ -1305,6 +1305,19 @@ namespace lible_b200
     // step.  With mixed precision a second (prefix, begin) pair covers the FP32 part of each range
     // (Q_bra Q_ket < thr32).  Segments are visited heaviest first (decreasing K_ab K_cd) and each task
     // sequence is cut into work-queue chunks (costChunks) that the kernels claim dynamically.
+    // Whether a mixed-precision plan keeps every quartet of the class (la lb | lc ld) in FP64: when
+    // its FP64 kernel is the DMMA group path, its ket has at least 15 spherical functions and its
+    // total angular momentum is at least 8.  Measured per class on (H2O)_8 cc-pVTZ, the FP32
+    // register or group kernels of those classes plus the FP64 launch of their large quartets took
+    // longer than the DMMA kernel running all of their quartets ((fd|dp) 5.3 against 3.6 ms, (fp|dd)
+    // 3.5 against 2.0 ms, (fd|fp) 2.5 against 1.4 ms).
+    static bool fp32InFp64(int la, int lb, int lc, int ld)
+    {
+        const int sab = nsph(la) * nsph(lb), scd = nsph(lc) * nsph(ld);
+        const int hab = nherm(la + lb), nr = nherm(la + lb + lc + ld);
+        return pickRegGroup<double>(sab, scd, hab, nr) == 0 && scd >= 15 && la + lb + lc + ld >= 8;
+    }
+
     Engine::JKClassPair Engine::buildClassPair(const ClassSet &bs, int cb, const ClassSet &ks, int ck, bool triangle,
                                                double thr, double thr32, bool mixed)
     {
@@ -1321,6 +1334,9 @@ namespace lible_b200
         JKClassPair cp;
         cp.cb = cb;
         cp.ck = ck;
+        cp.all64 = mixed && fp32InFp64(bs.host[cb].la, bs.host[cb].lb, ks.host[ck].la, ks.host[ck].lb);
+        if (cp.all64)
+            mixed = false;  // one FP64 task sequence over every surviving quartet
         std::vector<uint32_t> majors, b64, b32;
         std::vector<unsigned long long> p64(1, 0), p32(1, 0);
         auto &run64 = cp.run64, &run32 = cp.run32;  // tasks per major entry
@@ -1637,7 +1653,7 @@ namespace lible_b200
             a.bra_qpos = cs.orders[cp.cb].d_q;
             a.bra_qpair = B.Q;
             a.ket_qpair = Kc.Q;
-            a.q_lo = mixed ? plan.thr32 : plan.thr;
+            a.q_lo = (mixed && !cp.all64) ? plan.thr32 : plan.thr;
             a.q_hi = HUGE_VAL;
             a.bra_soa = B.soa;
             a.bra_pPs = B.pPs;
@@ -1918,7 +1934,7 @@ namespace lible_b200
                         a.bra_qpos = cs.orders[cp.cb].d_q;
                         a.bra_qpair = B.Q;
                         a.ket_qpair = Kc.Q;
-                        a.q_lo = fp32 ? plan.thr : (mixed ? plan.thr32 : plan.thr);
+                        a.q_lo = fp32 ? plan.thr : ((mixed && !cp.all64) ? plan.thr32 : plan.thr);
                         a.q_hi = fp32 ? plan.thr32 : HUGE_VAL;
                         a.bra_soa = B.soa;
                         a.bra_pPs = B.pPs;

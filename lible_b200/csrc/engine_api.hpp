@@ -252,6 +252,7 @@ namespace lible_b200
             bool swap = false;  // RI plans: bra is the auxiliary class
             long long n64 = 0, n32 = 0;  // surviving quartets
             long long t64 = 0, t32 = 0;  // launched tasks (whole bra groups; the kernels test each)
+            bool all64 = false;          // mixed plan, but every quartet of this pair in FP64
             double prim64 = 0, prim32 = 0, flops64 = 0, flops32 = 0;
             unsigned long long *prefix64 = nullptr, *prefix32 = nullptr;
             uint32_t *begin64 = nullptr, *begin32 = nullptr, *majors = nullptr;
